@@ -1,0 +1,211 @@
+/*
+ * mam4b.h -- C ABI of the B200-native MAM4 gas-aerosol microphysics step.
+ *
+ * One "step" advances every grid cell (column x level) through the
+ * sequence that mam4xx's host model runs per cell:
+ *
+ *   calcsize     mam4::modal_aero_calcsize::modal_aero_calcsize_sub
+ *                (src/mam4xx/modal_aero_calcsize.hpp:750)
+ *   water uptake mam4::water_uptake::modal_aero_water_uptake_dr
+ *                (src/mam4xx/water_uptake.hpp:481)
+ *   amicphys     mam4::microphysics::modal_aero_amicphys_intr
+ *                (src/mam4xx/mam4_amicphys.hpp:2120): H2SO4/SOAG
+ *                condensation, Aitken->accumulation renaming, H2SO4-H2O
+ *                nucleation, Brownian coagulation, primary-carbon aging,
+ *                over clear and cloudy subareas.
+ *
+ * The entry points replace the host's team dispatch
+ *   Kokkos::parallel_for(team_policy, ... process.compute_tendencies(...))
+ * (src/validation/aero_process.hpp:114-122, the AeroProcess plug-in API):
+ * one call processes a whole batch of columns on a CUDA stream.
+ *
+ * Data layout ("state" and "tendency" views). Every field is a plain
+ * array of doubles with one entry per cell, cell index = col*nlev + lev
+ * (the same flattening as a ColumnView per column laid end to end).
+ * Fields are passed as a table of pointers so that each field can live in
+ * its own allocation (a Prognostics-style view per species) or inside one
+ * slab with a leading dimension; reads and writes are coalesced per field.
+ *
+ * Units follow mam4::Prognostics: aerosol and gas mass mixing ratios in
+ * kg/kg, aerosol numbers in #/kg; tendencies in the same units per second.
+ *
+ * Error behaviour: every entry point returns a mam4b_status; nothing is
+ * thrown across the boundary and no device trap is ever raised. Per-cell
+ * conditions found on the device (non-finite input, condensation sub-step
+ * limit reached) are OR-ed into a status word that mam4b_last_status()
+ * returns after the stream has been synchronised.
+ */
+#ifndef MAM4B_H
+#define MAM4B_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MAM4B_ABI_VERSION 1
+
+/* ---------------------------------------------------------------- sizes */
+#define MAM4B_NUM_MODES 4     /* accumulation, aitken, coarse, primary C  */
+#define MAM4B_NUM_AERO 7      /* SOA, SO4, POM, BC, NaCl, DST, MOM          */
+#define MAM4B_NUM_POPS 25     /* 21 species-in-mode masses + 4 numbers      */
+#define MAM4B_GAS_PCNST 31    /* amicphys tracer work array length          */
+#define MAM4B_NUM_PROG 52     /* H2SO4, SOAG, 25 interstitial, 25 cloud     */
+
+/*
+ * Input fields (MAM4B_NIN per cell).
+ * Aerosol populations follow the E3SM state_q order of indices 15..39
+ * (src/mam4xx/utils.hpp:222-259): for each mode (accumulation, aitken,
+ * coarse, primary carbon) the species masses in mam4::mode_aero_species
+ * order (src/mam4xx/aero_modes.hpp:214-243), then the mode number:
+ *   0-6  acc  SO4 POM SOA BC DST NaCl MOM, 7 acc number
+ *   8-11 ait  SO4 SOA NaCl MOM,            12 ait number
+ *   13-19 cor DST NaCl SO4 BC POM SOA MOM, 20 coarse number
+ *   21-23 pca POM BC MOM,                  24 pca number
+ */
+enum {
+  MAM4B_IN_T = 0,      /* temperature [K]                                  */
+  MAM4B_IN_P = 1,      /* mid-level pressure [Pa]                          */
+  MAM4B_IN_ZM = 2,     /* mid-level height above surface [m]               */
+  MAM4B_IN_QV = 3,     /* water vapour mixing ratio [kg/kg]                */
+  MAM4B_IN_CLD = 4,    /* cloud fraction [-]                               */
+  MAM4B_IN_H2SO4 = 5,  /* H2SO4 gas [kg/kg]                                */
+  MAM4B_IN_SOAG = 6,   /* SOA precursor gas [kg/kg]                        */
+  MAM4B_IN_AER_I = 7,  /* 25 interstitial populations                      */
+  MAM4B_IN_AER_C = 32, /* 25 cloud-borne populations                       */
+  MAM4B_NIN = 57
+};
+
+/*
+ * Output fields (MAM4B_NOUT per cell).
+ *   0..51  tendency of the 52 prognostics in input order
+ *          (H2SO4, SOAG, 25 interstitial, 25 cloud-borne), per second,
+ *          = (value after the step - value before) / dt
+ *   52..55 dry geometric-mean diameter of the interstitial modes [m]
+ *   56..59 wet geometric-mean diameter [m]
+ *   60..63 wet density [kg/m3]
+ *   64..67 aerosol water [kg/kg]
+ */
+enum {
+  MAM4B_OUT_TEND = 0,
+  MAM4B_OUT_DGN_A = 52,
+  MAM4B_OUT_DGN_AWET = 56,
+  MAM4B_OUT_WETDENS = 60,
+  MAM4B_OUT_QAERWAT = 64,
+  MAM4B_NOUT = 68
+};
+
+/*
+ * Optional per-process diagnostics: the grid-cell mean tendencies of the
+ * 31 amicphys tracers [mol/mol/s or #/kmol/s] for condensation, renaming,
+ * nucleation, coagulation and cloud-borne renaming, as written by
+ * modal_aero_amicphys_intr into gas_aero_exchange_* (mam4_amicphys.hpp:
+ * 2355-2374). Field index = process*31 + tracer.
+ */
+enum { MAM4B_NDIAG = 5 * MAM4B_GAS_PCNST };
+
+typedef enum mam4b_status {
+  MAM4B_OK = 0,
+  MAM4B_ERR_INVALID_ARGUMENT = 1, /* null pointer, bad size, bad config    */
+  MAM4B_ERR_CUDA = 2,             /* a CUDA runtime call failed            */
+  MAM4B_ERR_NOT_SUPPORTED = 3,    /* option not built into this library    */
+  MAM4B_ERR_DEVICE_FLAGS = 4      /* cell-level flags raised on the device */
+} mam4b_status;
+
+/* Cell-level condition bits reported by mam4b_last_status(). */
+#define MAM4B_FLAG_NONFINITE_INPUT 0x1u
+#define MAM4B_FLAG_SOA_NITER_LIMIT 0x2u
+#define MAM4B_FLAG_NONFINITE_OUTPUT 0x4u
+
+/* Arithmetic of the step. */
+typedef enum mam4b_precision {
+  MAM4B_FP64 = 0,  /* plain double precision throughout                  */
+  MAM4B_MIXED = 1  /* FP32 bulk; FP64 in the condensation update, the
+                      renaming transfer fractions and conservation sums  */
+} mam4b_precision;
+
+/*
+ * Process switches and options; mirrors mam4::microphysics::AmicPhysConfig
+ * (src/mam4xx/mam4_amicphys.hpp:223-237) plus the aging parameter
+ * n_so4_monolayers_pcage (src/mam4xx/aging.hpp:31).
+ */
+typedef struct mam4b_config {
+  int do_cond;
+  int do_rename;
+  int do_newnuc;
+  int do_coag;
+  int gaexch_h2so4_uptake_optaa; /* 1 sequential, 2 simultaneous          */
+  int newnuc_h2so4_conc_optaa;   /* accepted, unused (as in the reference) */
+  unsigned n_so4_monolayers_pcage;
+} mam4b_config;
+
+/* Pointer tables. in[f] / out[f] point at ncell doubles (device memory). */
+typedef struct mam4b_state_view {
+  const double *field[MAM4B_NIN];
+  const double *pblh; /* planetary boundary layer height per column [m]  */
+} mam4b_state_view;
+
+typedef struct mam4b_tend_view {
+  double *field[MAM4B_NOUT];
+  double *diag[MAM4B_NDIAG]; /* all NULL: diagnostics not written        */
+} mam4b_tend_view;
+
+typedef struct mam4b_ctx mam4b_ctx;
+
+/* Fills *cfg with the defaults used by E3SM (all processes on,
+ * options 2/2, 8 monolayers). */
+void mam4b_default_config(mam4b_config *cfg);
+
+/* Creates a context bound to the current CUDA device. The context owns the
+ * device status word; one context per stream. */
+mam4b_status mam4b_create(mam4b_ctx **ctx, const mam4b_config *cfg);
+mam4b_status mam4b_destroy(mam4b_ctx *ctx);
+
+/*
+ * Runs one step over ncol*nlev cells, asynchronously on `stream`
+ * (a cudaStream_t; NULL = legacy default stream). All pointers are device
+ * pointers. Replaces AeroProcess<MicrophysicsProcess>::compute_tendencies
+ * dispatched over all columns (src/validation/aero_process.hpp:114).
+ */
+mam4b_status mam4b_step(mam4b_ctx *ctx, const mam4b_state_view *in,
+                        const mam4b_tend_view *out, int ncol, int nlev,
+                        double dt, int precision, void *stream);
+
+/*
+ * Same step on a slab: in_slab holds MAM4B_NIN fields of ld doubles each,
+ * out_slab MAM4B_NOUT fields of ld doubles each, pblh ncol doubles.
+ */
+mam4b_status mam4b_step_slab(mam4b_ctx *ctx, const double *in_slab,
+                             const double *pblh, double *out_slab, size_t ld,
+                             int ncol, int nlev, double dt, int precision,
+                             void *stream);
+
+/*
+ * Host-buffer convenience: copies the host slabs to the device, runs the
+ * step and copies the results back, all on `stream`, then synchronises.
+ * Scratch device memory is kept in ctx and reused across calls.
+ */
+mam4b_status mam4b_step_host(mam4b_ctx *ctx, const double *in_slab,
+                             const double *pblh, double *out_slab, size_t ld,
+                             int ncol, int nlev, double dt, int precision,
+                             void *stream);
+
+/* Synchronises the context's last stream and returns the OR of the
+ * MAM4B_FLAG_* bits raised since the previous call (then clears them). */
+mam4b_status mam4b_last_status(mam4b_ctx *ctx, uint32_t *flags);
+
+/* Copies a description of the last error into buf (NUL-terminated). */
+void mam4b_last_error(mam4b_ctx *ctx, char *buf, size_t len);
+
+/* Number of kernels launched by this context since creation. */
+uint64_t mam4b_launch_count(mam4b_ctx *ctx);
+
+int mam4b_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MAM4B_H */

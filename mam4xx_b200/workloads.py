@@ -1,0 +1,177 @@
+"""Seeded synthetic workloads for the microphysics step.
+
+No public dataset exists for this path, so each named configuration is a
+seeded draw (NumPy PCG64, seed = 20261203 + configuration index) with the
+shapes and value distributions of the step's benchmark configurations:
+
+  c1  8 x 72 columns x levels, clear sky, no cloud-borne aerosol
+  c2  4096 x 72, cloud fraction U(0, 1), cloud-borne aerosol drawn like the
+      interstitial aerosol
+  c3  65536 x 72, like c2 but 30% of cells get an Aitken number that puts the
+      Aitken dry diameter within +-10% of the renaming cut-off diameter
+  c4  65536 x 72, H2SO4 log-uniform 1e-15..1e-8 mol/mol, cloud fraction 0 for
+      60% of cells and U(0.2, 1) for 40% (uneven condensation sub-stepping)
+  c5  16384 x 72, like c2 (adjoint configuration)
+
+Common distributions (per cell): T ~ U(200, 310) K; RH ~ U(0.05, 0.99)
+converted to a vapour mixing ratio with the Magnus saturation formula used
+by amicphys (src/mam4xx/conversions.hpp:148-180, mam4_amicphys.hpp:2199-2205);
+H2SO4 ~ logU(1e-14, 1e-10) and SOAG ~ logU(1e-12, 1e-9) mol/mol; mode numbers
+~ logU(1e5, 1e10) #/kg; species masses ~ logU(1e-14, 1e-8) kg/kg for the
+species present in each mode. Pressure is geometric from 10 to 1000 hPa over
+the levels (level 0 at the top), heights follow the hypsometric equation with
+the drawn temperatures, and the boundary-layer height is 1000 m.
+
+The arrays use the field-major layout of include/mam4b.h: in_slab has shape
+(MAM4B_NIN, ncell) with cell = col*nlev + lev.
+"""
+
+import numpy as np
+
+NIN = 57
+NOUT = 68
+NDIAG = 155
+IN_T, IN_P, IN_ZM, IN_QV, IN_CLD, IN_H2SO4, IN_SOAG = range(7)
+IN_AER_I = 7
+IN_AER_C = 32
+OUT_DGN_A, OUT_DGN_AWET, OUT_WETDENS, OUT_QAERWAT = 52, 56, 60, 64
+
+# Population layout of the 25 aerosol entries (E3SM state_q 15..39):
+# (mode, species name) or (mode, "num").
+POPULATIONS = (
+    [(0, s) for s in ("SO4", "POM", "SOA", "BC", "DST", "NaCl", "MOM")] + [(0, "num")]
+    + [(1, s) for s in ("SO4", "SOA", "NaCl", "MOM")] + [(1, "num")]
+    + [(2, s) for s in ("DST", "NaCl", "SO4", "BC", "POM", "SOA", "MOM")] + [(2, "num")]
+    + [(3, s) for s in ("POM", "BC", "MOM")] + [(3, "num")]
+)
+NUMBER_SLOTS = tuple(i for i, (_, s) in enumerate(POPULATIONS) if s == "num")
+MODE_SPECIES_SLOTS = {m: tuple(i for i, (mm, s) in enumerate(POPULATIONS)
+                               if mm == m and s != "num") for m in range(4)}
+
+# Chemistry-mechanism molecular weights [g/mol] of the 31 amicphys tracers
+# (src/mam4xx/gas_chem_mechanism.hpp:31-38).
+ADV_MASS = np.array([
+    47.998200, 34.013600, 98.078400, 64.064800, 62.132400, 12.011000,
+    115.107340, 12.011000, 12.011000, 12.011000, 135.064039, 58.442468,
+    250092.672000, 1.007400, 115.107340, 12.011000, 58.442468, 250092.672000,
+    1.007400, 135.064039, 58.442468, 115.107340, 12.011000, 12.011000,
+    12.011000, 250092.672000, 1.007400, 12.011000, 12.011000, 250092.672000,
+    1.007400])
+MW_DRY_AIR = 28.966  # kg/kmol
+
+# Aitken-mode constants used to place cells near the renaming cut-off
+# (src/mam4xx/aero_modes.hpp:76-123, rename.hpp:452-465).
+_SIG = [1.8, 1.6, 1.8, 1.60000002384186]
+_DGN_NOM = [1.1e-7, 2.6e-8, 2e-6, 5e-8]
+_DENS = {"SOA": 1000.0, "SO4": 1770.0, "POM": 1000.0, "BC": 1700.0,
+         "NaCl": 1900.0, "DST": 2600.0, "MOM": 1601.0}
+
+CONFIGS = {
+    "c1": dict(index=0, ncol=8, nlev=72, clouds="none"),
+    "c2": dict(index=1, ncol=4096, nlev=72, clouds="uniform"),
+    "c3": dict(index=2, ncol=65536, nlev=72, clouds="uniform", near_cutoff=0.3),
+    "c4": dict(index=3, ncol=65536, nlev=72, clouds="bimodal",
+               h2so4_range=(1e-15, 1e-8)),
+    "c5": dict(index=4, ncol=16384, nlev=72, clouds="uniform"),
+}
+
+DT = 1800.0
+
+
+def rename_cutoff_diameter():
+    """Aitken->accumulation cut-off diameter (rename.hpp:462-465)."""
+    la, lc = np.log(_SIG[1]), np.log(_SIG[0])
+    return np.sqrt(_DGN_NOM[1] * np.exp(1.5 * la * la) * _DGN_NOM[0] * np.exp(1.5 * lc * lc))
+
+
+def magnus_qv_sat(temp, pmid):
+    """Saturation specific humidity of the amicphys RH diagnosis."""
+    eps = 0.018016 / 0.028966
+    tc = temp - 273.15
+    ew = 610.94 * np.exp(17.625 * tc / (234.04 + tc))
+    es = 1.00071 * np.exp(4.5e-8 * pmid) * ew
+    return eps * es / (pmid - (1.0 - eps) * es)
+
+
+def _logu(rng, lo, hi, n):
+    return np.exp(rng.uniform(np.log(lo), np.log(hi), n))
+
+
+def make_workload(name="c1", ncol=None, nlev=None, seed=None):
+    """Draws configuration `name`; ncol/nlev/seed override its defaults.
+
+    Returns a dict with in_slab (NIN, ncell) float64, pblh (ncol,),
+    ncol, nlev, dt and the configuration name."""
+    cfg = dict(CONFIGS[name])
+    ncol = cfg["ncol"] if ncol is None else int(ncol)
+    nlev = cfg["nlev"] if nlev is None else int(nlev)
+    seed = 20261203 + cfg["index"] if seed is None else int(seed)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    n = ncol * nlev
+    x = np.zeros((NIN, n), dtype=np.float64)
+
+    temp = rng.uniform(200.0, 310.0, n)
+    plev = np.geomspace(1000.0, 100000.0, nlev)  # Pa, level 0 at the top
+    pmid = np.tile(plev, ncol)
+    # hypsometric heights, integrating from the bottom level upward
+    tcol = temp.reshape(ncol, nlev)
+    zm = np.zeros((ncol, nlev))
+    rd_over_g = 287.04 / 9.80616
+    zm[:, -1] = rd_over_g * tcol[:, -1] * np.log(101325.0 / plev[-1])
+    for k in range(nlev - 2, -1, -1):
+        tbar = 0.5 * (tcol[:, k] + tcol[:, k + 1])
+        zm[:, k] = zm[:, k + 1] + rd_over_g * tbar * np.log(plev[k + 1] / plev[k])
+    rh = rng.uniform(0.05, 0.99, n)
+    qv = rh * magnus_qv_sat(temp, pmid)
+
+    if cfg["clouds"] == "none":
+        cld = np.zeros(n)
+    elif cfg["clouds"] == "uniform":
+        cld = rng.uniform(0.0, 1.0, n)
+    else:  # bimodal
+        cld = np.where(rng.uniform(0.0, 1.0, n) < 0.6, 0.0, rng.uniform(0.2, 1.0, n))
+
+    h2lo, h2hi = cfg.get("h2so4_range", (1e-14, 1e-10))
+    h2so4_vmr = _logu(rng, h2lo, h2hi, n)
+    soag_vmr = _logu(rng, 1e-12, 1e-9, n)
+
+    x[IN_T] = temp
+    x[IN_P] = pmid
+    x[IN_ZM] = zm.reshape(-1)
+    x[IN_QV] = qv
+    x[IN_CLD] = cld
+    x[IN_H2SO4] = h2so4_vmr * ADV_MASS[2] / MW_DRY_AIR
+    x[IN_SOAG] = soag_vmr * ADV_MASS[5] / MW_DRY_AIR
+
+    for base, cloudy in ((IN_AER_I, False), (IN_AER_C, True)):
+        for slot, (mode, spec) in enumerate(POPULATIONS):
+            if spec == "num":
+                v = _logu(rng, 1e5, 1e10, n)
+            else:
+                v = _logu(rng, 1e-14, 1e-8, n)
+            if cloudy and cfg["clouds"] == "none":
+                v = np.zeros(n)
+            x[base + slot] = v
+
+    frac = cfg.get("near_cutoff")
+    if frac:
+        # For a fraction of cells choose the Aitken number so that the dry
+        # number-median diameter from volume/number is within +-10% of the
+        # renaming cut-off (mean_particle_diameter_from_volume inverted).
+        pick = rng.uniform(0.0, 1.0, n) < frac
+        dtarget = rename_cutoff_diameter() * rng.uniform(0.9, 1.1, n)
+        vol = np.zeros(n)
+        for slot in MODE_SPECIES_SLOTS[1]:
+            vol += x[IN_AER_I + slot] / _DENS[POPULATIONS[slot][1]]
+        lsg = np.log(_SIG[1])
+        vpart = (np.pi / 6.0) * dtarget ** 3 * np.exp(4.5 * lsg * lsg)
+        num_ait = vol / vpart
+        x[IN_AER_I + NUMBER_SLOTS[1]] = np.where(pick, num_ait, x[IN_AER_I + NUMBER_SLOTS[1]])
+
+    pblh = np.full(ncol, 1000.0)
+    return {"name": name, "in_slab": x, "pblh": pblh, "ncol": ncol,
+            "nlev": nlev, "dt": DT}
+
+
+def pblh_per_cell(w):
+    return np.repeat(w["pblh"], w["nlev"])

@@ -1,0 +1,163 @@
+"""ctypes bindings of the two CPU oracles (test infrastructure only).
+
+  ReferenceOracle  oracle/_ref/libmam4ref.so -- mam4xx's own headers compiled
+                   unchanged against the host shim (exists only where the
+                   reference tree was available at build time).
+  PortOracle       oracle/libmam4oracle.so -- the plain-C restatement.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use
+this module; the product package never imports it.
+"""
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_SO = os.path.join(HERE, "_ref", "libmam4ref.so")
+PORT_SO = os.path.join(HERE, "libmam4oracle.so")
+
+NIN, NOUT, NDIAG = 57, 68, 155
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("do_cond", ctypes.c_int), ("do_rename", ctypes.c_int),
+                ("do_newnuc", ctypes.c_int), ("do_coag", ctypes.c_int),
+                ("gaexch_h2so4_uptake_optaa", ctypes.c_int),
+                ("newnuc_h2so4_conc_optaa", ctypes.c_int),
+                ("n_so4_monolayers_pcage", ctypes.c_uint)]
+
+
+def default_config(**kw):
+    c = dict(do_cond=1, do_rename=1, do_newnuc=1, do_coag=1,
+             gaexch_h2so4_uptake_optaa=2, newnuc_h2so4_conc_optaa=2,
+             n_so4_monolayers_pcage=8)
+    c.update(kw)
+    return Config(**c)
+
+
+_P = ctypes.c_void_p
+_D = ctypes.c_double
+_I = ctypes.c_int
+_S = ctypes.c_size_t
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+class _Oracle:
+    prefix = None
+    path = None
+
+    def __init__(self):
+        if not os.path.exists(self.path):
+            raise FileNotFoundError(self.path)
+        self.lib = ctypes.CDLL(self.path)
+        p = self.prefix
+        f = getattr(self.lib, p + "_step")
+        f.argtypes = [_I, _P, _S, _P, _P, _S, _P, _S, _D, ctypes.POINTER(Config), _I]
+        f.restype = _I
+        getattr(self.lib, p + "_calcsize").argtypes = [_I, _P, _P, _D, _P, _P, _P, _P]
+        getattr(self.lib, p + "_water_uptake").argtypes = [_I, _P, _P, _P, _P, _P, _P, _P, _P]
+        getattr(self.lib, p + "_amicphys").argtypes = [
+            _I, ctypes.POINTER(Config), _D, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]
+        getattr(self.lib, p + "_h2so4_update").argtypes = [_D, _D, _P, _P, _P, _P]
+        for t in ("_bm0ij", "_bm3i"):
+            g = getattr(self.lib, p + t)
+            g.argtypes = [_I, _I, _I]
+            g.restype = _D
+        getattr(self.lib, p + "_aging").argtypes = [ctypes.c_uint] + [_P] * 8
+
+    def step(self, in_slab, pblh_cell, dt, cfg=None, diag=False, nthreads=0):
+        x = np.ascontiguousarray(in_slab, dtype=np.float64)
+        n = x.shape[1]
+        pb = np.ascontiguousarray(pblh_cell, dtype=np.float64)
+        out = np.zeros((NOUT, n))
+        dg = np.zeros((NDIAG, n)) if diag else None
+        cfg = cfg or default_config()
+        rc = getattr(self.lib, self.prefix + "_step")(
+            n, _ptr(x), n, _ptr(pb), _ptr(out), n, _ptr(dg), n, dt, ctypes.byref(cfg), nthreads)
+        if rc != 0:
+            raise RuntimeError("oracle step failed: %d" % rc)
+        return (out, dg) if diag else out
+
+    def calcsize(self, state_q, qqcw, dt):
+        sq = np.ascontiguousarray(state_q, dtype=np.float64)
+        cw = np.ascontiguousarray(qqcw, dtype=np.float64)
+        n = sq.shape[0]
+        a, c = np.zeros((n, 4)), np.zeros((n, 4))
+        pt, dq = np.zeros((n, 40)), np.zeros((n, 40))
+        getattr(self.lib, self.prefix + "_calcsize")(n, _ptr(sq), _ptr(cw), dt, _ptr(a), _ptr(c),
+                                                     _ptr(pt), _ptr(dq))
+        return a, c, pt, dq
+
+    def water_uptake(self, state_q, temp, pmid, cld, dgncur_a):
+        arrs = [np.ascontiguousarray(v, dtype=np.float64) for v in (state_q, temp, pmid, cld, dgncur_a)]
+        n = arrs[0].shape[0]
+        w, q, d = np.zeros((n, 4)), np.zeros((n, 4)), np.zeros((n, 4))
+        getattr(self.lib, self.prefix + "_water_uptake")(n, *[_ptr(a) for a in arrs], _ptr(w), _ptr(q), _ptr(d))
+        return w, q, d
+
+    def amicphys(self, dt, temp, pmid, zm, pblh, qv, cld, qq, qqcw, dgncur_a, dgncur_awet,
+                 wetdens, cfg=None, diag=False):
+        ins = [np.ascontiguousarray(v, dtype=np.float64) for v in (temp, pmid, zm, pblh, qv, cld)]
+        q = np.array(qq, dtype=np.float64, order="C", copy=True)
+        cw = np.array(qqcw, dtype=np.float64, order="C", copy=True)
+        mo = [np.ascontiguousarray(v, dtype=np.float64) for v in (dgncur_a, dgncur_awet, wetdens)]
+        n = q.shape[0]
+        dg = np.zeros((n, 5, 31)) if diag else None
+        cfg = cfg or default_config()
+        getattr(self.lib, self.prefix + "_amicphys")(n, ctypes.byref(cfg), dt, *[_ptr(a) for a in ins],
+                                                     _ptr(q), _ptr(cw), *[_ptr(a) for a in mo], _ptr(dg))
+        return (q, cw, dg) if diag else (q, cw)
+
+    def h2so4_update(self, dt, netprod, uptkaer, qgas_cur, qaer_cur):
+        up = np.ascontiguousarray(uptkaer, dtype=np.float64)
+        qg = np.array([qgas_cur], dtype=np.float64)
+        av = np.zeros(1)
+        qa = np.array(qaer_cur, dtype=np.float64)
+        getattr(self.lib, self.prefix + "_h2so4_update")(dt, netprod, _ptr(up), _ptr(qg), _ptr(av), _ptr(qa))
+        return qg[0], av[0], qa
+
+    def bm0ij(self, n1, n2a, n2n):
+        return getattr(self.lib, self.prefix + "_bm0ij")(n1, n2a, n2n)
+
+    def bm3i(self, n1, n2a, n2n):
+        return getattr(self.lib, self.prefix + "_bm3i")(n1, n2a, n2n)
+
+    def aging(self, n_mono, dgn_a, qnum_cur, qnum_del_cond, qnum_del_coag, qaer_cur,
+              qaer_del_cond, qaer_del_coag, qaer_del_coag_in):
+        a = [np.array(v, dtype=np.float64, copy=True) for v in
+             (dgn_a, qnum_cur, qnum_del_cond, qnum_del_coag, qaer_cur, qaer_del_cond,
+              qaer_del_coag, qaer_del_coag_in)]
+        getattr(self.lib, self.prefix + "_aging")(n_mono, *[_ptr(v) for v in a])
+        return a[1:]
+
+
+class ReferenceOracle(_Oracle):
+    prefix = "mam4ref"
+    path = REF_SO
+
+
+class PortOracle(_Oracle):
+    prefix = "mam4orc"
+    path = PORT_SO
+
+    def __init__(self):
+        super().__init__()
+        self.lib.mam4orc_soa_niter.argtypes = [_I, _P, _S, _P, _D, ctypes.POINTER(Config), _P, _I]
+
+    def soa_niter(self, in_slab, pblh_cell, dt, cfg=None, nthreads=0):
+        x = np.ascontiguousarray(in_slab, dtype=np.float64)
+        n = x.shape[1]
+        pb = np.ascontiguousarray(pblh_cell, dtype=np.float64)
+        it = np.zeros(n, dtype=np.int32)
+        cfg = cfg or default_config()
+        self.lib.mam4orc_soa_niter(n, _ptr(x), n, _ptr(pb), dt, ctypes.byref(cfg), _ptr(it), nthreads)
+        return it
+
+
+def reference_available():
+    return os.path.exists(REF_SO)

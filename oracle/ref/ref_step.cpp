@@ -1,0 +1,293 @@
+// ref_step.cpp -- batched CPU driver around the mam4xx reference headers.
+//
+// TEST INFRASTRUCTURE ONLY (oracle/_ref/libmam4ref.so). The reference
+// headers are included read-only from the mam4xx source tree and compiled
+// unchanged against the host shim in oracle/shim; this file only composes
+// them into the microphysics step and exposes C entry points for tests and
+// for the CPU baseline timing.
+//
+// Step composition per cell (the host-model sequence the GPU kernel
+// replaces):
+//   1. pack state_q[40] / qqcw[40] (E3SM tracer order, kg/kg and #/kg,
+//      src/mam4xx/utils.hpp:222-259);
+//   2. modal_aero_calcsize_sub (src/mam4xx/modal_aero_calcsize.hpp:750)
+//      with CalcsizeData::initialize (:142);
+//   3. modal_aero_water_uptake_dr (src/mam4xx/water_uptake.hpp:481) on the
+//      same state_q and the calcsize dry diameters, as in
+//      src/validation/aero_model/aero_model_calcsize_water_uptake_dr.cpp:
+//      75-111;
+//   4. the calcsize tendencies applied for one step, q = max(0, q+tend*dt),
+//      to interstitial and cloud-borne aerosol entries (the update_mmr
+//      branch of the same driver, :112-118);
+//   5. mmr -> vmr with the chemistry mechanism molecular weights
+//      (src/mam4xx/gas_chem_mechanism.hpp:31-38; numbers x 28.966 kg/kmol);
+//   6. modal_aero_amicphys_intr (src/mam4xx/mam4_amicphys.hpp:2120) with
+//      q_pregaschem = q_precldchem = qq and qqcw_precldchem = qqcw;
+//   7. vmr -> mmr and tendency = (after - before)/dt.
+
+#include <mam4xx/mam4_amicphys.hpp>
+#include <mam4xx/modal_aero_calcsize.hpp>
+#include <mam4xx/water_uptake.hpp>
+
+#include "../oracle_api.h"
+
+#include <cstring>
+#include <omp.h>
+
+namespace {
+
+using mam4::Real;
+using CalcsizeData = mam4::modal_aero_calcsize::CalcsizeData;
+
+const CalcsizeData &calcsize_data() {
+  static const CalcsizeData d = [] {
+    CalcsizeData x;
+    x.initialize();
+    return x;
+  }();
+  return d;
+}
+
+constexpr double kMwDryAir = 28.966; // kg/kmol
+
+bool is_number_slot(int i31) {
+  return i31 == 13 || i31 == 18 || i31 == 26 || i31 == 30;
+}
+double to_vmr_factor(int i31) {
+  return is_number_slot(i31)
+             ? kMwDryAir
+             : kMwDryAir / mam4::gas_chemistry::adv_mass[i31];
+}
+double to_mmr_factor(int i31) {
+  return is_number_slot(i31)
+             ? 1.0 / kMwDryAir
+             : mam4::gas_chemistry::adv_mass[i31] / kMwDryAir;
+}
+
+mam4::microphysics::AmicPhysConfig amicphys_config(const mam4b_config &c) {
+  mam4::microphysics::AmicPhysConfig a;
+  a.do_cond = c.do_cond != 0;
+  a.do_rename = c.do_rename != 0;
+  a.do_newnuc = c.do_newnuc != 0;
+  a.do_coag = c.do_coag != 0;
+  a.gaexch_h2so4_uptake_optaa = c.gaexch_h2so4_uptake_optaa;
+  a.newnuc_h2so4_conc_optaa = c.newnuc_h2so4_conc_optaa;
+  return a;
+}
+
+void calcsize_cell(const Real (&state_q)[40], const Real (&qqcw)[40], Real dt,
+                   Real (&dgncur_a)[4], Real (&dgncur_c)[4], Real (&ptend)[40],
+                   Real (&dqqcwdt)[40]) {
+  for (int i = 0; i < 40; ++i) {
+    ptend[i] = 0;
+    dqqcwdt[i] = 0;
+  }
+  Real sq[40], cw[40];
+  std::memcpy(sq, state_q, sizeof(sq));
+  std::memcpy(cw, qqcw, sizeof(cw));
+  mam4::modal_aero_calcsize::modal_aero_calcsize_sub(
+      sq, cw, dt, calcsize_data(), dgncur_a, dgncur_c, ptend, dqqcwdt);
+}
+
+void water_uptake_cell(const Real (&state_q)[40], Real temp, Real pmid,
+                       Real cld, const Real (&dgncur_a)[4],
+                       Real (&dgncur_awet)[4], Real (&qaerwat)[4],
+                       Real (&wetdens)[4]) {
+  const CalcsizeData &cd = calcsize_data();
+  Real sq[40];
+  std::memcpy(sq, state_q, sizeof(sq));
+  Real dgn[4];
+  std::memcpy(dgn, dgncur_a, sizeof(dgn));
+  mam4::water_uptake::modal_aero_water_uptake_dr(
+      cd.nspec_amode, cd.specdens_amode, cd.spechygro, cd.lspectype_amode, sq,
+      temp, pmid, cld, dgn, dgncur_awet, qaerwat, wetdens);
+}
+
+void amicphys_cell(const mam4b_config &cfg, Real dt, Real temp, Real pmid,
+                   Real zm, Real pblh, Real qv, Real cld, Real (&qq)[31],
+                   Real (&qqcw)[31], const Real (&dgncur_a)[4],
+                   const Real (&dgncur_awet)[4], const Real (&wetdens)[4],
+                   Real *diag /* [5][31] or null */) {
+  using View2D = mam4::microphysics::View2D;
+  View2D d[5];
+  if (diag) {
+    for (int p = 0; p < 5; ++p)
+      d[p] = View2D("gas_aero_exchange", 31, 1);
+  }
+  Real q_pregaschem[31], q_precldchem[31], qqcw_precldchem[31];
+  std::memcpy(q_pregaschem, qq, sizeof(q_pregaschem));
+  std::memcpy(q_precldchem, qq, sizeof(q_precldchem));
+  std::memcpy(qqcw_precldchem, qqcw, sizeof(qqcw_precldchem));
+  const Real pdel_unused = 0.0; // passed through, never read by amicphys
+  mam4::microphysics::modal_aero_amicphys_intr(
+      amicphys_config(cfg), dt, cfg.n_so4_monolayers_pcage, temp, pmid,
+      pdel_unused, zm, pblh, qv, cld, qq, qqcw, 0, d[0], d[1], d[2], d[3], d[4],
+      q_pregaschem, q_precldchem, qqcw_precldchem, dgncur_a, dgncur_awet,
+      wetdens);
+  if (diag) {
+    for (int p = 0; p < 5; ++p)
+      for (int i = 0; i < 31; ++i)
+        diag[p * 31 + i] = d[p](i, 0);
+  }
+}
+
+void step_cell(const double *in, size_t ld, size_t c, double pblh, double *out,
+               size_t ldo, double *diag, size_t ldd, double dt,
+               const mam4b_config &cfg) {
+  auto IN = [&](int f) { return in[(size_t)f * ld + c]; };
+  Real state_q[40] = {}, qqcw[40] = {};
+  state_q[0] = IN(MAM4B_IN_QV);
+  state_q[11] = IN(MAM4B_IN_H2SO4);
+  state_q[14] = IN(MAM4B_IN_SOAG);
+  for (int p = 0; p < MAM4B_NUM_POPS; ++p) {
+    state_q[15 + p] = IN(MAM4B_IN_AER_I + p);
+    qqcw[15 + p] = IN(MAM4B_IN_AER_C + p);
+  }
+  const Real temp = IN(MAM4B_IN_T), pmid = IN(MAM4B_IN_P);
+  const Real cld = IN(MAM4B_IN_CLD);
+
+  Real dgncur_a[4], dgncur_c[4], ptend[40], dqqcwdt[40];
+  calcsize_cell(state_q, qqcw, dt, dgncur_a, dgncur_c, ptend, dqqcwdt);
+
+  Real dgncur_awet[4], qaerwat[4], wetdens[4];
+  water_uptake_cell(state_q, temp, pmid, cld, dgncur_a, dgncur_awet, qaerwat,
+                    wetdens);
+
+  for (int i = 15; i < 40; ++i) {
+    state_q[i] = mam4::max(0.0, state_q[i] + ptend[i] * dt);
+    qqcw[i] = mam4::max(0.0, qqcw[i] + dqqcwdt[i] * dt);
+  }
+
+  Real qq[31], qqcw31[31];
+  for (int i = 0; i < 31; ++i) {
+    qq[i] = state_q[9 + i] * to_vmr_factor(i);
+    qqcw31[i] = qqcw[9 + i] * to_vmr_factor(i);
+  }
+
+  Real dg[5 * 31];
+  amicphys_cell(cfg, dt, temp, pmid, IN(MAM4B_IN_ZM), pblh, IN(MAM4B_IN_QV),
+                cld, qq, qqcw31, dgncur_a, dgncur_awet, wetdens,
+                diag ? dg : nullptr);
+
+  auto OUT = [&](int f) -> double & { return out[(size_t)f * ldo + c]; };
+  OUT(MAM4B_OUT_TEND + 0) = (qq[2] * to_mmr_factor(2) - IN(MAM4B_IN_H2SO4)) / dt;
+  OUT(MAM4B_OUT_TEND + 1) = (qq[5] * to_mmr_factor(5) - IN(MAM4B_IN_SOAG)) / dt;
+  for (int p = 0; p < MAM4B_NUM_POPS; ++p) {
+    const int i31 = 6 + p;
+    OUT(MAM4B_OUT_TEND + 2 + p) =
+        (qq[i31] * to_mmr_factor(i31) - IN(MAM4B_IN_AER_I + p)) / dt;
+    OUT(MAM4B_OUT_TEND + 27 + p) =
+        (qqcw31[i31] * to_mmr_factor(i31) - IN(MAM4B_IN_AER_C + p)) / dt;
+  }
+  for (int m = 0; m < 4; ++m) {
+    OUT(MAM4B_OUT_DGN_A + m) = dgncur_a[m];
+    OUT(MAM4B_OUT_DGN_AWET + m) = dgncur_awet[m];
+    OUT(MAM4B_OUT_WETDENS + m) = wetdens[m];
+    OUT(MAM4B_OUT_QAERWAT + m) = qaerwat[m];
+  }
+  if (diag) {
+    for (int k = 0; k < 5 * 31; ++k)
+      diag[(size_t)k * ldd + c] = dg[k];
+  }
+}
+
+} // namespace
+
+extern "C" {
+
+int mam4ref_step(int ncell, const double *in, size_t ld_in,
+                 const double *pblh_cell, double *out, size_t ld_out,
+                 double *diag, size_t ld_diag, double dt,
+                 const mam4b_config *cfg, int nthreads) {
+  if (ncell < 0 || !in || !pblh_cell || !out || !cfg || dt <= 0)
+    return MAM4B_ERR_INVALID_ARGUMENT;
+  (void)calcsize_data();
+  const int nt = nthreads > 0 ? nthreads : omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nt)
+  for (int c = 0; c < ncell; ++c)
+    step_cell(in, ld_in, (size_t)c, pblh_cell[c], out, ld_out, diag, ld_diag,
+              dt, *cfg);
+  return MAM4B_OK;
+}
+
+void mam4ref_calcsize(int ncell, const double *state_q, const double *qqcw,
+                      double dt, double *dgncur_a, double *dgncur_c,
+                      double *ptend, double *dqqcwdt) {
+  for (int c = 0; c < ncell; ++c) {
+    Real sq[40], cw[40];
+    std::memcpy(sq, state_q + 40 * c, sizeof(sq));
+    std::memcpy(cw, qqcw + 40 * c, sizeof(cw));
+    Real a[4], b[4], pt[40], dq[40];
+    calcsize_cell(sq, cw, dt, a, b, pt, dq);
+    std::memcpy(dgncur_a + 4 * c, a, sizeof(a));
+    std::memcpy(dgncur_c + 4 * c, b, sizeof(b));
+    std::memcpy(ptend + 40 * c, pt, sizeof(pt));
+    std::memcpy(dqqcwdt + 40 * c, dq, sizeof(dq));
+  }
+}
+
+void mam4ref_water_uptake(int ncell, const double *state_q, const double *temp,
+                          const double *pmid, const double *cld,
+                          const double *dgncur_a, double *dgncur_awet,
+                          double *qaerwat, double *wetdens) {
+  for (int c = 0; c < ncell; ++c) {
+    Real sq[40], dg[4], w[4], q[4], d[4];
+    std::memcpy(sq, state_q + 40 * c, sizeof(sq));
+    std::memcpy(dg, dgncur_a + 4 * c, sizeof(dg));
+    water_uptake_cell(sq, temp[c], pmid[c], cld[c], dg, w, q, d);
+    std::memcpy(dgncur_awet + 4 * c, w, sizeof(w));
+    std::memcpy(qaerwat + 4 * c, q, sizeof(q));
+    std::memcpy(wetdens + 4 * c, d, sizeof(d));
+  }
+}
+
+void mam4ref_amicphys(int ncell, const mam4b_config *cfg, double dt,
+                      const double *temp, const double *pmid, const double *zm,
+                      const double *pblh, const double *qv, const double *cld,
+                      double *qq, double *qqcw, const double *dgncur_a,
+                      const double *dgncur_awet, const double *wetdens,
+                      double *diag) {
+  for (int c = 0; c < ncell; ++c) {
+    Real q[31], cw[31], a[4], w[4], d[4];
+    std::memcpy(q, qq + 31 * c, sizeof(q));
+    std::memcpy(cw, qqcw + 31 * c, sizeof(cw));
+    std::memcpy(a, dgncur_a + 4 * c, sizeof(a));
+    std::memcpy(w, dgncur_awet + 4 * c, sizeof(w));
+    std::memcpy(d, wetdens + 4 * c, sizeof(d));
+    amicphys_cell(*cfg, dt, temp[c], pmid[c], zm[c], pblh[c], qv[c], cld[c], q,
+                  cw, a, w, d, diag ? diag + 155 * c : nullptr);
+    std::memcpy(qq + 31 * c, q, sizeof(q));
+    std::memcpy(qqcw + 31 * c, cw, sizeof(cw));
+  }
+}
+
+void mam4ref_h2so4_update(double dt, double qgas_netprod_otrproc,
+                          const double *uptkaer, double *qgas_cur,
+                          double *qgas_avg, double *qaer_cur) {
+  mam4::gasaerexch::mam_gasaerexch_1subarea_1gas_nonvolatile(
+      dt, qgas_netprod_otrproc, uptkaer, *qgas_cur, *qgas_avg, qaer_cur);
+}
+
+double mam4ref_bm0ij(int n1, int n2a, int n2n) {
+  return mam4::coagulation::bm0ij_data(n1, n2a, n2n);
+}
+double mam4ref_bm3i(int n1, int n2a, int n2n) {
+  return mam4::coagulation::bm3i_data(n1, n2a, n2n);
+}
+
+void mam4ref_aging(unsigned n_so4_monolayers_pcage, const double *dgn_a,
+                   double *qnum_cur, double *qnum_del_cond,
+                   double *qnum_del_coag, double *qaer_cur,
+                   double *qaer_del_cond, double *qaer_del_coag,
+                   double *qaer_del_coag_in) {
+  mam4::aging::mam_pcarbon_aging_1subarea(
+      n_so4_monolayers_pcage, dgn_a, qnum_cur, qnum_del_cond, qnum_del_coag,
+      reinterpret_cast<Real(*)[4]>(qaer_cur),
+      reinterpret_cast<Real(*)[4]>(qaer_del_cond),
+      reinterpret_cast<Real(*)[4]>(qaer_del_coag),
+      reinterpret_cast<Real(*)[1]>(qaer_del_coag_in));
+}
+
+long mam4ref_assert_failures(void) { return mam4shim::assert_failures(); }
+
+} // extern "C"
