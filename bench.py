@@ -1,0 +1,319 @@
+"""Benchmark of the MAM4 microphysics step on B200.
+
+Workload: the uneven-batching configuration, 65,536 columns x 72 levels per
+GPU (4,718,592 cells), FP64, seeded synthetic inputs (mam4xx_b200.workloads
+'c4': H2SO4 1e-15..1e-8 mol/mol, cloud fraction 60% clear / 40% U(0.2, 1)).
+One step = calcsize + water uptake + amicphys over every cell, dt = 1800 s.
+
+  value  cells/s with inputs resident in HBM (one kernel launch per step),
+         whole job = all ranks' cells / max-over-ranks time
+  e2e    cells/s through the C ABI host entry (mam4b_step_host): pinned host
+         slabs copied in, step, results copied out, every step
+  roofline  algorithmic HBM bytes (57 input + 68 output doubles per cell plus
+         the per-column boundary-layer height) / measured kernel time, against
+         the measured copy bandwidth of MEASURED_PEAKS.json
+  cpu_baseline  the mam4xx reference headers compiled for the host
+         (oracle/_ref, OpenMP) on a bounded sample of the same cells
+
+--impl reference times that CPU implementation alone, as the reference arm.
+Multi-GPU: one process per GPU (torchrun); each rank owns its own 65,536
+columns, no data exchange (cells are independent); timing is max over ranks.
+"""
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NCOL_PER_GPU = 65536
+NLEV = 72
+WORKLOAD = "c4"
+BYTES_PER_CELL = (57 + 68) * 8  # + 8 bytes of boundary-layer height per column
+METRIC = "cells/s per amicphys step"
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _traffic_per_launch(ncell):
+    """DRAM bytes per launch from the committed ncu summary, scaled by cells."""
+    p = os.path.join(ROOT, "profiles", "step_kernel_c4_ncu.md")
+    if not os.path.exists(p):
+        return None
+    txt = open(p).read()
+    m = re.search(r"traffic_bytes_per_cell:\s*([0-9.eE+-]+)", txt)
+    return None if not m else float(m.group(1)) * ncell
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            import tempfile
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for k, n in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(x, pblh_cell, dt, target_s=12.0):
+    """Times the reference headers built for the host (or the restatement
+    where that build is absent) on a bounded sample of the workload."""
+    from oracle import pyoracle
+    orc = pyoracle.ReferenceOracle() if pyoracle.reference_available() else pyoracle.PortOracle()
+    kind = "reference" if pyoracle.reference_available() else "port"
+    cores = os.cpu_count() or 1
+    n0 = min(x.shape[1], 8 * 1024)
+    t = time.perf_counter()
+    orc.step(x[:, :n0], pblh_cell[:n0], dt, nthreads=cores)
+    rate0 = n0 / max(time.perf_counter() - t, 1e-6)
+    n = int(min(x.shape[1], max(n0, rate0 * target_s)))
+    t = time.perf_counter()
+    orc.step(x[:, :n], pblh_cell[:n], dt, nthreads=cores)
+    el = time.perf_counter() - t
+    return {"value": n / el, "unit": "cells/s", "cores": cores, "kind": kind,
+            "sample": "first %d cells of the %s workload (%.1f s, OpenMP over cells)" % (n, WORKLOAD, el)}
+
+
+def run_reference_arm(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    from mam4xx_b200.workloads import make_workload, pblh_per_cell
+    from oracle import pyoracle
+    orc = pyoracle.ReferenceOracle() if pyoracle.reference_available() else pyoracle.PortOracle()
+    kind = "reference" if pyoracle.reference_available() else "port"
+    cores = os.cpu_count() or 1
+    # a bounded sample per step: 1024 columns x 72 levels of the same workload
+    w = make_workload(WORKLOAD, ncol=1024)
+    x, pb, dt = w["in_slab"], pblh_per_cell(w), w["dt"]
+    n = x.shape[1]
+    for _ in range(args.warmup):
+        orc.step(x, pb, dt, nthreads=cores)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        orc.step(x, pb, dt, nthreads=cores)
+    el = time.perf_counter() - t
+    v = n * args.steps / el
+    line = {"metric": METRIC, "value": v, "unit": "cells/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "%s sample %d columns x %d levels" % (WORKLOAD, 1024, NLEV),
+                       "ncol": 1024, "nlev": NLEV, "dt_s": dt},
+            "cpu_baseline": {"value": v, "unit": "cells/s", "cores": cores, "kind": kind,
+                             "sample": "1024 columns x 72 levels per step, OpenMP over cells"},
+            "e2e": {"value": v, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--ncol", type=int, default=NCOL_PER_GPU, help="columns per GPU")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+    from mam4xx_b200 import native
+    from mam4xx_b200.workloads import make_workload, pblh_per_cell
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    ncol = args.ncol
+    w = make_workload(WORKLOAD, ncol=ncol, seed=20261203 + 3 + 1000 * rank)
+    x_host = w["in_slab"]
+    n = x_host.shape[1]
+    dt = w["dt"]
+    x = torch.from_numpy(x_host).to(dev)
+    pb = torch.from_numpy(w["pblh"]).to(dev)
+    out = torch.empty((native.NOUT, n), dtype=torch.float64, device=dev)
+    ctx = native.Context()
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        ctx.step_slab(x.data_ptr(), pb.data_ptr(), out.data_ptr(), n, ncol, NLEV, dt,
+                      stream=stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    flags = ctx.last_status()
+
+    # device-resident timing: every launch bracketed by events on its stream
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    sampler = ClockSampler(local)
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    launches0 = ctx.launch_count()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for i in range(args.steps):
+        evs[i][0].record(stream)
+        step()
+        evs[i][1].record(stream)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    launches = ctx.launch_count() - launches0
+    total_ms = t_start.elapsed_time(t_end)
+    kernel_ms = float(np.mean([a.elapsed_time(b) for a, b in evs]))
+    if ws > 1:
+        tt = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    ms_per_step = total_ms / args.steps
+    value = ws * n * args.steps / (total_ms * 1e-3)
+
+    # end-to-end through the host entry of the C ABI
+    e2e = None
+    if not args.no_e2e:
+        xin = torch.from_numpy(x_host).pin_memory()
+        pbh = torch.from_numpy(w["pblh"]).pin_memory()
+        oh = torch.empty((native.NOUT, n), dtype=torch.float64).pin_memory()
+        ectx = native.Context()
+        for _ in range(2):
+            ectx.step_host(xin.data_ptr(), pbh.data_ptr(), oh.data_ptr(), n, ncol, NLEV, dt,
+                           stream=stream.cuda_stream)
+        ke = max(2, min(args.steps, 5))
+        if ws > 1:
+            dist.barrier()
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for _ in range(ke):
+            ectx.step_host(xin.data_ptr(), pbh.data_ptr(), oh.data_ptr(), n, ncol, NLEV, dt,
+                           stream=stream.cuda_stream)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        e_ms = a0.elapsed_time(a1)
+        if ws > 1:
+            tt = torch.tensor([e_ms], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            e_ms = float(tt.item())
+        e2e = {"value": ws * n * ke / (e_ms * 1e-3), "unit": "cells/s",
+               "h2d_bytes_per_step": int(native.NIN * n * 8 + ncol * 8),
+               "d2h_bytes_per_step": int(native.NOUT * n * 8),
+               "steps": ke, "entry": "mam4b_step_host"}
+        ectx.close()
+
+    peak, peak_kind = _peaks()
+    alg_bytes = n * BYTES_PER_CELL + ncol * 8
+    achieved = alg_bytes / (kernel_ms * 1e-3) / 1e9
+    traffic = _traffic_per_launch(n)
+    line = {
+        "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded draws with the configuration's distributions)",
+        "config": {"workload": "%s: uneven batching, %d columns x %d levels per GPU, FP64, dt=1800 s"
+                               % (WORKLOAD, ncol, NLEV),
+                   "ncol_per_gpu": ncol, "nlev": NLEV, "cells_per_gpu": n,
+                   "parallelism": "column shards, one per GPU" if ws > 1 else "single GPU",
+                   "l2": "inputs (%.2f GB) larger than L2, no flush" % (native.NIN * n * 8 / 1e9)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": "%s copy bandwidth" % peak_kind,
+                     "kernel_ms": kernel_ms, "algorithmic_bytes_per_launch": alg_bytes},
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "device_flags": flags,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(x_host, pblh_per_cell(w), dt)
+        except Exception as e:  # reported, never silently replaced
+            line["cpu_baseline"] = {"error": str(e)}
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

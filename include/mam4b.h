@@ -114,10 +114,15 @@ typedef enum mam4b_status {
   MAM4B_ERR_DEVICE_FLAGS = 4      /* cell-level flags raised on the device */
 } mam4b_status;
 
-/* Cell-level condition bits reported by mam4b_last_status(). */
+/* Cell-level condition bits reported by mam4b_last_status().
+ * NONFINITE_* are errors. SOA_NITER_LIMIT is informational: the SOA
+ * condensation sub-stepping reached the reference's own cap of 1000
+ * iterations (gasaerexch_soaexch.hpp:93,172-173) in some cell; as in the
+ * reference, that cell keeps the state reached at the cap. */
 #define MAM4B_FLAG_NONFINITE_INPUT 0x1u
 #define MAM4B_FLAG_SOA_NITER_LIMIT 0x2u
 #define MAM4B_FLAG_NONFINITE_OUTPUT 0x4u
+#define MAM4B_FLAGS_ERROR_MASK (MAM4B_FLAG_NONFINITE_INPUT | MAM4B_FLAG_NONFINITE_OUTPUT)
 
 /* Arithmetic of the step. */
 typedef enum mam4b_precision {
@@ -192,8 +197,10 @@ mam4b_status mam4b_step_host(mam4b_ctx *ctx, const double *in_slab,
                              int ncol, int nlev, double dt, int precision,
                              void *stream);
 
-/* Synchronises the context's last stream and returns the OR of the
- * MAM4B_FLAG_* bits raised since the previous call (then clears them). */
+/* Synchronises the context's last stream, stores in *flags the OR of the
+ * MAM4B_FLAG_* bits raised since the previous call (then clears them), and
+ * returns MAM4B_ERR_DEVICE_FLAGS if any bit of MAM4B_FLAGS_ERROR_MASK is
+ * set, MAM4B_OK otherwise. */
 mam4b_status mam4b_last_status(mam4b_ctx *ctx, uint32_t *flags);
 
 /* Copies a description of the last error into buf (NUL-terminated). */

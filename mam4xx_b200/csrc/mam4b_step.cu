@@ -1,0 +1,964 @@
+// mam4b_step.cu -- sm_100a kernels and the C ABI (include/mam4b.h) of the
+// B200-native MAM4 microphysics step.
+//
+// One thread owns one grid cell for the whole step (calcsize -> water
+// uptake -> amicphys); inputs and outputs are structure-of-arrays fields,
+// so each load/store instruction of a warp touches 32 consecutive doubles.
+// Cells are independent: there is no inter-thread communication and no
+// shared memory; the coagulation correction tables are read through L1.
+#include <cuda_runtime.h>
+
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <atomic>
+#include <mutex>
+#include <new>
+
+#include "../../include/mam4b.h"
+#include "mam4b_physics.cuh"
+
+namespace mam4b {
+
+// ------------------------------------------------------- device constants
+__constant__ StepConsts c_k;
+
+#define COAG_TABLE_QUALIFIER __device__ const
+#include "coag_tables.inc"
+#undef COAG_TABLE_QUALIFIER
+
+struct StepArgs {
+  const double *in[MAM4B_NIN];
+  const double *pblh;
+  double *out[MAM4B_NOUT];
+  double *diag[MAM4B_NDIAG];
+  unsigned *flags;
+  long long ncell;
+  int nlev;
+  double dt;
+  int do_cond, do_rename, do_newnuc, do_coag, optaa;
+  unsigned nmono;
+};
+
+// ----------------------------------------------------- per-cell amicphys
+struct Diag {
+  // amicphys process tendencies for the grid cell, in the 31-tracer
+  // order: [process 0..3][tracer], cloud-borne renaming [tracer]
+  double t[NQTEND][31];
+  double cw[31];
+};
+
+__device__ __forceinline__ int pop_to_i31(int p) { return 6 + p; }
+// amicphys tracer index of the number of mode m (mam4_amicphys.hpp:36)
+__device__ __forceinline__ int num_i31(int m) { return m == 0 ? 13 : m == 1 ? 18 : m == 2 ? 26 : 30; }
+
+// Clear-subarea sequence: condensation, renaming, nucleation, coagulation,
+// aging (mam_amicphys_1subarea, mam4_amicphys.hpp:1127-1697). `s` holds the
+// subarea's incoming values and returns the outgoing ones. With DIAG the
+// per-process increments are added to dg scaled by afrac/(fcvt*deltat).
+template <bool DIAG>
+__device__ __forceinline__ int clear_subarea(const StepArgs &a, double deltat, double temp,
+                                             double pmid, double zmid, double pblh,
+                                             double relhum, const double (&dgn_a)[NMODE],
+                                             const double (&dgn_awet)[NMODE],
+                                             const double (&wetdens)[NMODE],
+                                             const double (&qgas1)[2], Sub &s, Diag *dg,
+                                             double afrac) {
+  const StepConsts &C = c_k;
+  const double aircon = pmid / (8314.46759100000 * temp);
+  double netprod1 = 0.0;
+  if (a.do_cond && a.optaa == 2) {
+    netprod1 = (s.gas[1] - qgas1[1]) / deltat;
+    s.gas[1] = (netprod1 >= 0) ? qgas1[1] : 0;
+  }
+  const double dtsub = (double)(int)(deltat / 1);
+  int niter = 0;
+  double qgas_avg1 = s.gas[1];
+  double uptkrate_h2so4 = 0.0;
+  double cond_so4_pc = 0.0, cond_soa_pc = 0.0;  // condensation gain of the pc mode
+  double dcond[NAER][NMODE], dcoag[NAER][NMODE], dncond[NMODE], dncoag[NMODE];
+  double gas_sv[2];
+  if (DIAG) {
+#pragma unroll
+    for (int x = 0; x < NAER; ++x)
+#pragma unroll
+      for (int m = 0; m < NMODE; ++m) {
+        dcond[x][m] = 0.0;
+        dcoag[x][m] = 0.0;
+      }
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      dncond[m] = 0.0;
+      dncoag[m] = 0.0;
+    }
+  }
+  double grow[NAER];
+#pragma unroll
+  for (int x = 0; x < NAER; ++x)
+    grow[x] = 0.0;
+
+  // ---------------------------------------------------- condensation
+  if (a.do_cond) {
+    gas_sv[0] = s.gas[0];
+    gas_sv[1] = s.gas[1];
+    double sv_ait[NAER], sv_pc_so4, sv_pc_soa;
+    double sv_all[NAER][NMODE];
+#pragma unroll
+    for (int x = 0; x < NAER; ++x) {
+      sv_ait[x] = s.aer[x][1];
+      if (DIAG) {
+#pragma unroll
+        for (int m = 0; m < NMODE; ++m)
+          sv_all[x][m] = s.aer[x][m];
+      }
+    }
+    sv_pc_so4 = s.aer[1][3];
+    sv_pc_soa = s.aer[0][3];
+    // H2SO4 gas diffusivity / mean free path (gasaerexch.hpp:223-253, 402-417)
+    const double p_in_atm = pmid / 1.013e5;
+    const double dgas = (1.0e-3 * pow(temp, 1.75) * sqrt(1. / 9.807840000000000E+01 + 0.035)) /
+                        (p_in_atm * pow((pow(4.288000000000000E+01, 1.0 / 3.0) + 2.7189), 2.0));
+    const double gas_diffus = dgas * 1.0e-4;
+    const double speed = 145.5 * sqrt(temp / 9.807840000000000E+01);
+    const double freepath = 3.0 * gas_diffus / speed;
+    double uptk1[NMODE], uptk0[NMODE];
+    uptake_rates(C, gas_diffus, freepath, dgn_awet, uptk1);
+#pragma unroll
+    for (int n = 0; n < NMODE; ++n) {
+      uptk1[n] = uptk1[n] * (s.num[n] * aircon);
+      uptk0[n] = uptk1[n] * 0.81;
+    }
+#pragma unroll
+    for (int n = 0; n < NMODE; ++n)
+      uptkrate_h2so4 += uptk1[n];
+    double avg0;
+    niter = soa_exchange(dtsub, temp, pmid, s, avg0, uptk0);
+    h2so4_update(dtsub, netprod1, s, uptk1, qgas_avg1);
+#pragma unroll
+    for (int x = 0; x < NAER; ++x)
+      grow[x] = s.aer[x][1] - sv_ait[x];
+    cond_so4_pc = s.aer[1][3] - sv_pc_so4;
+    cond_soa_pc = s.aer[0][3] - sv_pc_soa;
+    if (DIAG) {
+#pragma unroll
+      for (int x = 0; x < NAER; ++x)
+#pragma unroll
+        for (int m = 0; m < NMODE; ++m)
+          dcond[x][m] = s.aer[x][m] - sv_all[x][m];
+      // gas increment of condensation (mam4_amicphys.hpp:1434-1438)
+      dg->t[0][5] += ((0.0 + (s.gas[0] - (gas_sv[0] + 0.0 * dtsub))) / (C.fcvt_soag * deltat)) * afrac;
+      dg->t[0][2] += ((0.0 + (s.gas[1] - (gas_sv[1] + netprod1 * dtsub))) / (1.0 * deltat)) * afrac;
+    }
+  }
+
+  // -------------------------------------------------------- renaming
+  if (a.do_rename) {
+    double nsv[NMODE], asv[NAER][NMODE];
+    if (DIAG) {
+#pragma unroll
+      for (int m = 0; m < NMODE; ++m) {
+        nsv[m] = s.num[m];
+#pragma unroll
+        for (int x = 0; x < NAER; ++x)
+          asv[x][m] = s.aer[x][m];
+      }
+    }
+    const double zero7[NAER] = {0, 0, 0, 0, 0, 0, 0};
+    rename_subarea<false>(C, s, s, grow, zero7);
+    if (DIAG) {
+#pragma unroll
+      for (int m = 0; m < NMODE; ++m) {
+        dg->t[1][num_i31(m)] +=
+            ((0.0 + (s.num[m] - nsv[m])) / (1.0 * deltat)) * afrac;
+#pragma unroll
+        for (int x = 0; x < NAER; ++x) {
+          const int slot = K::aer_slot(x, m);
+          if (slot >= 0)
+            dg->t[1][pop_to_i31(slot)] +=
+                ((0.0 + (s.aer[x][m] - asv[x][m])) / (K::fcvt_aer(x) * deltat)) * afrac;
+        }
+      }
+    }
+  }
+
+  // ------------------------------------------------------ nucleation
+  if (a.do_newnuc) {
+    const double g1 = s.gas[1], n1 = s.num[1], a1 = s.aer[1][1];
+    nucleation(C, dtsub, temp, pmid, zmid, pblh, relhum, uptkrate_h2so4, qgas_avg1, s);
+    if (DIAG) {
+      dg->t[2][2] += ((0.0 + (s.gas[1] - g1)) / (1.0 * deltat)) * afrac;
+      dg->t[2][18] += ((0.0 + (s.num[1] - n1)) / (1.0 * deltat)) * afrac;
+      dg->t[2][14] += ((0.0 + (s.aer[1][1] - a1)) / (1.0 * deltat)) * afrac;
+    }
+  }
+
+  // ----------------------------------------------------- coagulation
+  double coag_in[NAER];
+  if (a.do_coag) {
+    double nsv[NMODE], asv[NAER][NMODE];
+    if (DIAG) {
+#pragma unroll
+      for (int m = 0; m < NMODE; ++m) {
+        nsv[m] = s.num[m];
+#pragma unroll
+        for (int x = 0; x < NAER; ++x)
+          asv[x][m] = s.aer[x][m];
+      }
+    }
+    const CoagTables T = {kCoagBm0ij, kCoagBm3i, kCoagBm0};
+    coagulation(C, T, dtsub, temp, pmid, aircon, dgn_awet, wetdens, s, coag_in);
+    if (DIAG) {
+#pragma unroll
+      for (int m = 0; m < NMODE; ++m) {
+        dncoag[m] = s.num[m] - nsv[m];
+#pragma unroll
+        for (int x = 0; x < NAER; ++x)
+          dcoag[x][m] = s.aer[x][m] - asv[x][m];
+      }
+#pragma unroll
+      for (int m = 0; m < NMODE; ++m) {
+        dg->t[3][num_i31(m)] +=
+            ((0.0 + dncoag[m]) / (1.0 * deltat)) * afrac;
+#pragma unroll
+        for (int x = 0; x < NAER; ++x) {
+          const int slot = K::aer_slot(x, m);
+          if (slot >= 0)
+            dg->t[3][pop_to_i31(slot)] += ((0.0 + dcoag[x][m]) / (K::fcvt_aer(x) * deltat)) * afrac;
+        }
+      }
+    }
+  } else {
+#pragma unroll
+    for (int x = 0; x < NAER; ++x)
+      coag_in[x] = 0.0;
+  }
+
+  // ----------------------------------------------------------- aging
+  if (DIAG) {
+    aging(C, a.nmono, dgn_a[3], s, dncond, dncoag, dcond, dcoag, coag_in);
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      if (a.do_cond)
+        dg->t[0][num_i31(m)] +=
+            ((0.0 + dncond[m]) / (1.0 * deltat)) * afrac;
+#pragma unroll
+      for (int x = 0; x < NAER; ++x) {
+        const int slot = K::aer_slot(x, m);
+        if (slot >= 0 && a.do_cond)
+          dg->t[0][pop_to_i31(slot)] += ((0.0 + dcond[x][m]) / (K::fcvt_aer(x) * deltat)) * afrac;
+      }
+    }
+  } else {
+    // Only the primary-carbon condensation gains of SO4/SOA enter the aging
+    // fraction; the other increments are bookkeeping for diagnostics.
+    double dn_c[NMODE] = {0, 0, 0, 0}, dn_g[NMODE] = {0, 0, 0, 0};
+    double dc[NAER][NMODE], dq[NAER][NMODE];
+#pragma unroll
+    for (int x = 0; x < NAER; ++x)
+#pragma unroll
+      for (int m = 0; m < NMODE; ++m) {
+        dc[x][m] = 0.0;
+        dq[x][m] = 0.0;
+      }
+    dc[1][3] = cond_so4_pc;
+    dc[0][3] = cond_soa_pc;
+    aging(C, a.nmono, dgn_a[3], s, dn_c, dn_g, dc, dq, coag_in);
+  }
+  return niter;
+}
+
+template <bool DIAG>
+__global__ void __launch_bounds__(128) step_kernel(const __grid_constant__ StepArgs a) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncell)
+    return;
+  const StepConsts &C = c_k;
+  const double temp = __ldg(a.in[MAM4B_IN_T] + c);
+  const double pmid = __ldg(a.in[MAM4B_IN_P] + c);
+  const double zm = __ldg(a.in[MAM4B_IN_ZM] + c);
+  const double qv = __ldg(a.in[MAM4B_IN_QV] + c);
+  const double cld = __ldg(a.in[MAM4B_IN_CLD] + c);
+  const double h2so4 = __ldg(a.in[MAM4B_IN_H2SO4] + c);
+  const double soag = __ldg(a.in[MAM4B_IN_SOAG] + c);
+  const double pblh = __ldg(a.pblh + c / a.nlev);
+  const double dt = a.dt;
+  double ai[NPOP], ac[NPOP];
+#pragma unroll
+  for (int p = 0; p < NPOP; ++p) {
+    ai[p] = __ldg(a.in[MAM4B_IN_AER_I + p] + c);
+    ac[p] = __ldg(a.in[MAM4B_IN_AER_C + p] + c);
+  }
+  {
+    double chk = temp + pmid + zm + qv + cld + h2so4 + soag + pblh;
+#pragma unroll
+    for (int p = 0; p < NPOP; ++p)
+      chk += ai[p] + ac[p];
+    if (!isfinite(chk))
+      atomicOr(a.flags, MAM4B_FLAG_NONFINITE_INPUT);
+  }
+
+  // ------------------------------------------------------- calcsize
+  double dgn_a[NMODE], pt_i[NPOP], pt_c[NPOP];
+  calcsize(C, ai, ac, dt, dgn_a, pt_i, pt_c);
+  // ---------------------------------------------------- water uptake
+  double dgn_awet[NMODE], qaerwat[NMODE], wetdens_wu[NMODE];
+  water_uptake(C, ai, qv, temp, pmid, cld, dgn_a, dgn_awet, qaerwat, wetdens_wu);
+
+  // calcsize tendencies applied for one step, then amicphys units
+  double qi[NPOP], qc[NPOP];
+#pragma unroll
+  for (int p = 0; p < NPOP; ++p) {
+    qi[p] = dmax(0.0, dmax(0.0, ai[p] + pt_i[p] * dt) * C.to_vmr[2 + p]);
+    qc[p] = dmax(0.0, dmax(0.0, ac[p] + pt_c[p] * dt) * C.to_vmr[2 + p]);
+  }
+  const double g_h2so4 = dmax(0.0, h2so4 * C.to_vmr[0]);
+  const double g_soag = dmax(0.0, soag * C.to_vmr[1]);
+
+  // -------------------------------------------------------- amicphys
+  // modal_aero_amicphys_intr (mam4_amicphys.hpp:2120-2376) with
+  // q_pregaschem = q_precldchem = qq and qqcw_precldchem = qqcw.
+  double wetdens[NMODE];
+#pragma unroll
+  for (int m = 0; m < NMODE; ++m)
+    wetdens[m] = dmax(1000.0, wetdens_wu[m]);
+  const double epsqs = 0.018016 / 0.028966;
+  const double tc = temp - 273.15;
+  const double ew = 610.94 * exp(17.625 * tc / (234.04 + tc));
+  const double ev_sat = 1.00071 * exp(4.5e-8 * pmid) * ew;
+  const double qv_sat = epsqs * ev_sat / (pmid - (1 - epsqs) * ev_sat);
+  const double relhumgcm = dmax(0.0, dmin(1.0, qv / qv_sat));
+
+  Diag dgv;
+  Diag *dg = DIAG ? &dgv : nullptr;
+  if (DIAG) {
+#pragma unroll
+    for (int k = 0; k < NQTEND; ++k)
+#pragma unroll
+      for (int i = 0; i < 31; ++i)
+        dgv.t[k][i] = 0.0;
+#pragma unroll
+    for (int i = 0; i < 31; ++i)
+      dgv.cw[i] = 0.0;
+  }
+
+  // outgoing grid-cell means (amicphys units): gases, interstitial, cloud
+  double o_h2so4, o_soag, oi[NPOP], oc[NPOP];
+  const double fsoag = C.fcvt_soag;
+
+  auto load_sub = [&](Sub &s, const double (&q)[NPOP], const double (&fac_num)[NMODE],
+                      const double (&fac_mass)[NMODE]) {
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      s.num[m] = (q[K::numslot(m)] * fac_num[m]) * 1;
+#pragma unroll
+      for (int x = 0; x < NAER; ++x) {
+        const int slot = K::aer_slot(x, m);
+        s.aer[x][m] = (slot >= 0) ? (q[slot] * fac_mass[m]) * K::fcvt_aer(x) : 0.0;
+      }
+    }
+  };
+
+  if (cld < 1.0e-5) {
+    // ------------------------------------------- clear grid cell
+    Sub s;
+    // qsub = qgcm exactly (category I copies the grid means)
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      s.num[m] = qi[K::numslot(m)] * 1;
+#pragma unroll
+      for (int x = 0; x < NAER; ++x) {
+        const int slot = K::aer_slot(x, m);
+        s.aer[x][m] = (slot >= 0) ? qi[slot] * K::fcvt_aer(x) : 0.0;
+      }
+    }
+    s.gas[0] = g_soag * fsoag;
+    s.gas[1] = g_h2so4 * 1.0;
+    const double qgas1[2] = {s.gas[0], s.gas[1]};
+    const int niter = clear_subarea<DIAG>(a, dt, temp, pmid, zm, pblh, relhumgcm, dgn_a,
+                                          dgn_awet, wetdens, qgas1, s, dg, 1.0);
+    if (niter > 1000)
+      atomicOr(a.flags, MAM4B_FLAG_SOA_NITER_LIMIT);
+    const double f = 1.0 - 0.0;
+    const bool map_gas = a.do_cond || a.do_newnuc;
+    o_soag = dmax(0.0, 0.0 + (map_gas ? s.gas[0] / fsoag : g_soag) * f);
+    o_h2so4 = dmax(0.0, 0.0 + (map_gas ? s.gas[1] / 1.0 : g_h2so4) * f);
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      oi[K::numslot(m)] = dmax(0.0, 0.0 + (s.num[m] / 1.0) * f);
+#pragma unroll
+      for (int x = 0; x < NAER; ++x) {
+        const int slot = K::aer_slot(x, m);
+        if (slot >= 0)
+          oi[slot] = dmax(0.0, 0.0 + (s.aer[x][m] / K::fcvt_aer(x)) * f);
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < NPOP; ++p)
+      oc[p] = qc[p];
+  } else if (cld > 0.999) {
+    // ------------------------------------------ cloudy grid cell
+    Sub si, sc;
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      si.num[m] = qi[K::numslot(m)] * 1;
+      sc.num[m] = qc[K::numslot(m)] * 1;
+#pragma unroll
+      for (int x = 0; x < NAER; ++x) {
+        const int slot = K::aer_slot(x, m);
+        si.aer[x][m] = (slot >= 0) ? qi[slot] * K::fcvt_aer(x) : 0.0;
+        sc.aer[x][m] = (slot >= 0) ? qc[slot] * K::fcvt_aer(x) : 0.0;
+      }
+    }
+    si.gas[0] = si.gas[1] = sc.gas[0] = sc.gas[1] = 0.0;
+    double nsv_i[NMODE], nsv_c[NMODE], asv_i[NAER][NMODE], asv_c[NAER][NMODE];
+    if (DIAG) {
+#pragma unroll
+      for (int m = 0; m < NMODE; ++m) {
+        nsv_i[m] = si.num[m];
+        nsv_c[m] = sc.num[m];
+#pragma unroll
+        for (int x = 0; x < NAER; ++x) {
+          asv_i[x][m] = si.aer[x][m];
+          asv_c[x][m] = sc.aer[x][m];
+        }
+      }
+    }
+    if (a.do_rename) {
+      const double zero7[NAER] = {0, 0, 0, 0, 0, 0, 0};
+      rename_subarea<true>(C, si, sc, zero7, zero7);
+    }
+    const double f = 1.0;
+    o_soag = dmax(0.0, 0.0 + g_soag * f);
+    o_h2so4 = dmax(0.0, 0.0 + g_h2so4 * f);
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      oi[K::numslot(m)] = dmax(0.0, 0.0 + (si.num[m] / 1.0) * f);
+      oc[K::numslot(m)] = 0.0 + (sc.num[m] / 1.0) * f;
+#pragma unroll
+      for (int x = 0; x < NAER; ++x) {
+        const int slot = K::aer_slot(x, m);
+        if (slot >= 0) {
+          oi[slot] = dmax(0.0, 0.0 + (si.aer[x][m] / K::fcvt_aer(x)) * f);
+          oc[slot] = 0.0 + (sc.aer[x][m] / K::fcvt_aer(x)) * f;
+        }
+      }
+    }
+    if (DIAG && a.do_rename) {
+#pragma unroll
+      for (int m = 0; m < NMODE; ++m) {
+        const int ln = num_i31(m);
+        dgv.t[1][ln] += ((0.0 + (si.num[m] - nsv_i[m])) / (1.0 * dt)) * f;
+        dgv.cw[ln] += ((0.0 + (sc.num[m] - nsv_c[m])) / (1.0 * dt)) * f;
+#pragma unroll
+        for (int x = 0; x < NAER; ++x) {
+          const int slot = K::aer_slot(x, m);
+          if (slot >= 0) {
+            dgv.t[1][pop_to_i31(slot)] +=
+                ((0.0 + (si.aer[x][m] - asv_i[x][m])) / (K::fcvt_aer(x) * dt)) * f;
+            dgv.cw[pop_to_i31(slot)] +=
+                ((0.0 + (sc.aer[x][m] - asv_c[x][m])) / (K::fcvt_aer(x) * dt)) * f;
+          }
+        }
+      }
+    }
+  } else {
+    // ------------------------------------- partly cloudy grid cell
+    const double fcldy = cld, fclea = 1.0 - fcldy;
+    // interstitial partition factors per mode (get_partition_factors,
+    // mam4_amicphys.hpp:414-449), number and mass separately
+    double fn_c[NMODE], fn_y[NMODE], fm_c[NMODE], fm_y[NMODE];
+    auto part = [&](double q_i, double q_c, double &fc, double &fy) {
+      const double cldbrn_cldy = q_c / fcldy;
+      const double intrst_cldy = dmax(0.0, ((q_i + q_c) - cldbrn_cldy));
+      const double intrst_clea = (q_i - fcldy * intrst_cldy) / fclea;
+      double r = dmax(1.e-35, intrst_clea * fclea) / dmax(1.e-35, q_i);
+      r = dmax(0.0, dmin(1.0, r));
+      fc = r / fclea;
+      fy = (1 - r) / fcldy;
+    };
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      part(qi[K::numslot(m)], qc[K::numslot(m)], fn_c[m], fn_y[m]);
+      double si_ = 0.0, sc_ = 0.0;
+#pragma unroll
+      for (int s = 0; s < K::nspec(m); ++s) {
+        si_ = si_ + qi[K::spec0(m) + s];
+        sc_ = sc_ + qc[K::spec0(m) + s];
+      }
+      part(si_, sc_, fm_c[m], fm_y[m]);
+    }
+    // gases: clear keeps the grid mean, cloudy gets the remainder
+    double gcl[2] = {g_soag, g_h2so4}, gcy[2];
+#pragma unroll
+    for (int g = 0; g < 2; ++g) {
+      gcy[g] = (gcl[g] - fclea * gcl[g]) / fcldy;
+      if (gcy[g] < 0) {
+        gcy[g] = 0;
+        gcl[g] = gcl[g] / fclea;
+      }
+    }
+    // clear subarea (jsub 1)
+    {
+      Sub s;
+      load_sub(s, qi, fn_c, fm_c);
+      s.gas[0] = gcl[0] * fsoag;
+      s.gas[1] = gcl[1] * 1.0;
+      const double qgas1[2] = {g_soag * fsoag, g_h2so4 * 1.0};
+      const double rhc = bound(0.0, 1.0, (relhumgcm - fcldy) / fclea);
+      const int niter = clear_subarea<DIAG>(a, dt, temp, pmid, zm, pblh, rhc, dgn_a, dgn_awet,
+                                            wetdens, qgas1, s, dg, fclea);
+      if (niter > 1000)
+        atomicOr(a.flags, MAM4B_FLAG_SOA_NITER_LIMIT);
+      const bool map_gas = a.do_cond || a.do_newnuc;
+      o_soag = 0.0 + (map_gas ? s.gas[0] / fsoag : gcl[0]) * fclea;
+      o_h2so4 = 0.0 + (map_gas ? s.gas[1] / 1.0 : gcl[1]) * fclea;
+#pragma unroll
+      for (int m = 0; m < NMODE; ++m) {
+        oi[K::numslot(m)] = 0.0 + (s.num[m] / 1.0) * fclea;
+        oc[K::numslot(m)] = 0.0 + 0.0 * fclea;
+#pragma unroll
+        for (int x = 0; x < NAER; ++x) {
+          const int slot = K::aer_slot(x, m);
+          if (slot >= 0) {
+            oi[slot] = 0.0 + (s.aer[x][m] / K::fcvt_aer(x)) * fclea;
+            oc[slot] = 0.0 + 0.0 * fclea;
+          }
+        }
+      }
+    }
+    // cloudy subarea (jsub 2): renaming only
+    {
+      Sub si, sc;
+      load_sub(si, qi, fn_y, fm_y);
+#pragma unroll
+      for (int m = 0; m < NMODE; ++m) {
+        sc.num[m] = (qc[K::numslot(m)] / fcldy) * 1;
+#pragma unroll
+        for (int x = 0; x < NAER; ++x) {
+          const int slot = K::aer_slot(x, m);
+          sc.aer[x][m] = (slot >= 0) ? (qc[slot] / fcldy) * K::fcvt_aer(x) : 0.0;
+        }
+      }
+      si.gas[0] = si.gas[1] = sc.gas[0] = sc.gas[1] = 0.0;
+      double nsv_i[NMODE], nsv_c[NMODE], asv_i[NAER][NMODE], asv_c[NAER][NMODE];
+      if (DIAG) {
+#pragma unroll
+        for (int m = 0; m < NMODE; ++m) {
+          nsv_i[m] = si.num[m];
+          nsv_c[m] = sc.num[m];
+#pragma unroll
+          for (int x = 0; x < NAER; ++x) {
+            asv_i[x][m] = si.aer[x][m];
+            asv_c[x][m] = sc.aer[x][m];
+          }
+        }
+      }
+      if (a.do_rename) {
+        const double zero7[NAER] = {0, 0, 0, 0, 0, 0, 0};
+        rename_subarea<true>(C, si, sc, zero7, zero7);
+      }
+      o_soag = dmax(0.0, o_soag + gcy[0] * fcldy);
+      o_h2so4 = dmax(0.0, o_h2so4 + gcy[1] * fcldy);
+#pragma unroll
+      for (int m = 0; m < NMODE; ++m) {
+        oi[K::numslot(m)] = dmax(0.0, oi[K::numslot(m)] + (si.num[m] / 1.0) * fcldy);
+        oc[K::numslot(m)] = oc[K::numslot(m)] + (sc.num[m] / 1.0) * fcldy;
+#pragma unroll
+        for (int x = 0; x < NAER; ++x) {
+          const int slot = K::aer_slot(x, m);
+          if (slot >= 0) {
+            oi[slot] = dmax(0.0, oi[slot] + (si.aer[x][m] / K::fcvt_aer(x)) * fcldy);
+            oc[slot] = oc[slot] + (sc.aer[x][m] / K::fcvt_aer(x)) * fcldy;
+          }
+        }
+      }
+      if (DIAG && a.do_rename) {
+#pragma unroll
+        for (int m = 0; m < NMODE; ++m) {
+          const int ln = num_i31(m);
+          dgv.t[1][ln] += ((0.0 + (si.num[m] - nsv_i[m])) / (1.0 * dt)) * fcldy;
+          dgv.cw[ln] += ((0.0 + (sc.num[m] - nsv_c[m])) / (1.0 * dt)) * fcldy;
+#pragma unroll
+          for (int x = 0; x < NAER; ++x) {
+            const int slot = K::aer_slot(x, m);
+            if (slot >= 0) {
+              dgv.t[1][pop_to_i31(slot)] +=
+                  ((0.0 + (si.aer[x][m] - asv_i[x][m])) / (K::fcvt_aer(x) * dt)) * fcldy;
+              dgv.cw[pop_to_i31(slot)] +=
+                  ((0.0 + (sc.aer[x][m] - asv_c[x][m])) / (K::fcvt_aer(x) * dt)) * fcldy;
+            }
+          }
+        }
+      }
+    }
+  }
+
+  // ---------------------------------------------------------- outputs
+  double *const *out = a.out;
+  out[MAM4B_OUT_TEND + 0][c] = (o_h2so4 * C.to_mmr[0] - h2so4) / dt;
+  out[MAM4B_OUT_TEND + 1][c] = (o_soag * C.to_mmr[1] - soag) / dt;
+#pragma unroll
+  for (int p = 0; p < NPOP; ++p) {
+    out[MAM4B_OUT_TEND + 2 + p][c] = (oi[p] * C.to_mmr[2 + p] - ai[p]) / dt;
+    out[MAM4B_OUT_TEND + 27 + p][c] = (oc[p] * C.to_mmr[2 + p] - ac[p]) / dt;
+  }
+#pragma unroll
+  for (int m = 0; m < NMODE; ++m) {
+    out[MAM4B_OUT_DGN_A + m][c] = dgn_a[m];
+    out[MAM4B_OUT_DGN_AWET + m][c] = dgn_awet[m];
+    out[MAM4B_OUT_WETDENS + m][c] = wetdens_wu[m];
+    out[MAM4B_OUT_QAERWAT + m][c] = qaerwat[m];
+  }
+  if (DIAG) {
+#pragma unroll
+    for (int k = 0; k < NQTEND; ++k)
+#pragma unroll
+      for (int i = 0; i < 31; ++i)
+        if (a.diag[k * 31 + i])
+          a.diag[k * 31 + i][c] = dgv.t[k][i];
+#pragma unroll
+    for (int i = 0; i < 31; ++i)
+      if (a.diag[4 * 31 + i])
+        a.diag[4 * 31 + i][c] = dgv.cw[i];
+  }
+}
+
+// ====================================================== derived constants
+// Evaluated once per device by a one-thread kernel, with the same
+// expressions the reference evaluates inline (and the same math library the
+// kernel uses), then copied into constant memory.
+__host__ __device__ static double h_vol_from_diam(double d, double sig) {
+  return (d * d * d) * exp(4.5 * (log(sig) * log(sig))) * K::pi_sixth;
+}
+
+__host__ __device__ static StepConsts make_consts() {
+  StepConsts C = {};
+  for (int m = 0; m < NMODE; ++m) {
+    C.n2v_nom[m] = 1.0 / h_vol_from_diam(K::dnom(m), K::sig(m));
+    C.n2v_min[m] = 1.0 / h_vol_from_diam(K::dmax(m), K::sig(m));
+    C.n2v_max[m] = 1.0 / h_vol_from_diam(K::dmin(m), K::sig(m));
+    for (int s = 0; s < K::nspec(m); ++s)
+      C.inv_density[m][s] = 1.0 / K::aero_dens(K::mode_spec(m, s));
+    C.log_sig[m] = log(K::sig(m));
+  }
+  // unit factors: H2SO4 (tracer 2), SOAG (tracer 5), populations 6..30
+  auto is_num = [](int i31) { return i31 == 13 || i31 == 18 || i31 == 26 || i31 == 30; };
+  const int tr[2] = {2, 5};
+  for (int k = 0; k < NPOP + 2; ++k) {
+    const int i31 = k < 2 ? tr[k] : 6 + (k - 2);
+    C.to_vmr[k] = is_num(i31) ? K::mw_dry_air : K::mw_dry_air / K::adv_mass(i31);
+    C.to_mmr[k] = is_num(i31) ? 1.0 / K::mw_dry_air : K::adv_mass(i31) / K::mw_dry_air;
+  }
+  C.fcvt_soag = K::adv_mass(5) / 150;
+  // renaming pair aitken -> accumulation (rename.hpp:393-476)
+  {
+    const double alnsg = log(K::sig(1));
+    C.rn_fac = sqrt(0.5) / alnsg;
+    C.rn_v2n_lo_rlx = 1.0 / h_vol_from_diam(K::dmin(1), K::sig(1)) * 27.0;
+    C.rn_v2n_hi_rlx = 1.0 / h_vol_from_diam(K::dmax(1), K::sig(1)) / 27.0;
+    C.rn_ln_tail_fac = 3.0 * (alnsg * alnsg);
+    const double alnsg_d = log(K::sig(0));
+    const double cutoff = sqrt(K::dnom(1) * exp(1.5 * (alnsg * alnsg)) * K::dnom(0) *
+                               exp(1.5 * (alnsg_d * alnsg_d)));
+    C.rn_ln_cutoff = log(cutoff);
+    C.rn_threshold = 0.99 * cutoff;
+  }
+  // nucleation size bounds (mam4_amicphys.hpp:990-1008)
+  C.nuc_dplom = exp(0.67 * log(K::dmin(1)) + 0.33 * log(K::dnom(1)));
+  {
+    const double tmpa = 1770.0 * K::pi / 6.0;
+    C.nuc_mass1p_lo = tmpa * (pow(C.nuc_dplom, 3.0));
+    C.nuc_mass1p_hi = tmpa * (pow(K::dmax(1), 3.0));
+  }
+  // aging (aging.hpp:82-150)
+  {
+    const double mw_soa = 150 / 1000.0, mw_so4 = 115 / 1000.0;
+    C.so4_vol = mw_so4 * 1000.0 / 1770.0;
+    const double soa_vol = mw_soa * 1000.0 / 1000.0;
+    C.soa_fac_eqvhyg = soa_vol * 0.14000000000000001 / 0.50700000000000001;
+    const double l = log(K::sig(3));
+    C.aging_fac_volsfc = exp(2.5 * (l * l));
+  }
+  C.geomean_ait_acc = sqrt(C.n2v_nom[1]) * sqrt(C.n2v_nom[0]);
+  C.hystfac = 1.0 / dmax(1.0e-5, (K::rh_deliq - K::rh_cryst));
+  C.kohler_aa = 2.0e4 * 18.0 * 76.0 / (8.3e7 * 273.0 * 1.0);
+  return C;
+}
+
+__global__ void init_consts_kernel(StepConsts *out) { *out = make_consts(); }
+
+}  // namespace mam4b
+
+// =============================================================== C ABI
+using namespace mam4b;
+
+struct mam4b_ctx {
+  mam4b_config cfg;
+  int device;
+  unsigned *d_flags;
+  cudaStream_t last_stream;
+  char err[256];
+  std::atomic<unsigned long long> launches;
+  // host-path scratch (device slabs), grown on demand
+  double *d_in, *d_out, *d_pblh;
+  size_t cap_in, cap_out, cap_pblh;
+};
+
+namespace {
+std::mutex g_init_mu;
+bool g_consts_ready[64];
+
+mam4b_status set_err(mam4b_ctx *ctx, mam4b_status st, const char *what, cudaError_t e) {
+  if (ctx)
+    snprintf(ctx->err, sizeof(ctx->err), "%s: %s", what,
+             e == cudaSuccess ? "invalid argument" : cudaGetErrorString(e));
+  return st;
+}
+
+cudaError_t ensure_consts(int dev) {
+  std::lock_guard<std::mutex> lk(g_init_mu);
+  if (dev < 0 || dev >= 64)
+    return cudaErrorInvalidDevice;
+  if (g_consts_ready[dev])
+    return cudaSuccess;
+  StepConsts *d_tmp = nullptr;
+  cudaError_t e = cudaMalloc(&d_tmp, sizeof(StepConsts));
+  if (e == cudaSuccess) {
+    init_consts_kernel<<<1, 1>>>(d_tmp);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess)
+    e = cudaDeviceSynchronize();
+  if (e == cudaSuccess)
+    e = cudaMemcpyToSymbol(c_k, d_tmp, sizeof(StepConsts), 0, cudaMemcpyDeviceToDevice);
+  if (e == cudaSuccess)
+    e = cudaDeviceSynchronize();
+  cudaFree(d_tmp);
+  if (e == cudaSuccess)
+    g_consts_ready[dev] = true;
+  return e;
+}
+
+bool valid_config(const mam4b_config *c) {
+  return c && (c->gaexch_h2so4_uptake_optaa == 1 || c->gaexch_h2so4_uptake_optaa == 2);
+}
+}  // namespace
+
+extern "C" {
+
+int mam4b_abi_version(void) { return MAM4B_ABI_VERSION; }
+
+void mam4b_default_config(mam4b_config *cfg) {
+  if (!cfg)
+    return;
+  cfg->do_cond = 1;
+  cfg->do_rename = 1;
+  cfg->do_newnuc = 1;
+  cfg->do_coag = 1;
+  cfg->gaexch_h2so4_uptake_optaa = 2;
+  cfg->newnuc_h2so4_conc_optaa = 2;
+  cfg->n_so4_monolayers_pcage = 8;
+}
+
+mam4b_status mam4b_create(mam4b_ctx **out, const mam4b_config *cfg) {
+  if (!out)
+    return MAM4B_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  mam4b_config c;
+  if (cfg)
+    c = *cfg;
+  else
+    mam4b_default_config(&c);
+  if (!valid_config(&c))
+    return MAM4B_ERR_INVALID_ARGUMENT;
+  mam4b_ctx *ctx = new (std::nothrow) mam4b_ctx();
+  if (!ctx)
+    return MAM4B_ERR_INVALID_ARGUMENT;
+  ctx->cfg = c;
+  ctx->launches = 0;
+  cudaError_t e = cudaGetDevice(&ctx->device);
+  if (e == cudaSuccess)
+    e = ensure_consts(ctx->device);
+  if (e == cudaSuccess)
+    e = cudaMalloc(&ctx->d_flags, sizeof(unsigned));
+  if (e == cudaSuccess)
+    e = cudaMemset(ctx->d_flags, 0, sizeof(unsigned));
+  if (e != cudaSuccess) {
+    if (ctx->d_flags)
+      cudaFree(ctx->d_flags);
+    delete ctx;
+    return MAM4B_ERR_CUDA;
+  }
+  *out = ctx;
+  return MAM4B_OK;
+}
+
+mam4b_status mam4b_destroy(mam4b_ctx *ctx) {
+  if (!ctx)
+    return MAM4B_ERR_INVALID_ARGUMENT;
+  cudaFree(ctx->d_flags);
+  cudaFree(ctx->d_in);
+  cudaFree(ctx->d_out);
+  cudaFree(ctx->d_pblh);
+  delete ctx;
+  return MAM4B_OK;
+}
+
+mam4b_status mam4b_step(mam4b_ctx *ctx, const mam4b_state_view *in, const mam4b_tend_view *out,
+                        int ncol, int nlev, double dt, int precision, void *stream) {
+  if (!ctx || !in || !out || ncol < 0 || nlev <= 0 || !(dt > 0.0) || !isfinite(dt))
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_step", cudaSuccess);
+  if (precision != MAM4B_FP64)
+    return set_err(ctx, MAM4B_ERR_NOT_SUPPORTED, "mam4b_step: precision", cudaSuccess);
+  StepArgs a;
+  memset(&a, 0, sizeof(a));
+  bool diag = false;
+  for (int f = 0; f < MAM4B_NIN; ++f) {
+    if (!in->field[f])
+      return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_step: null input field", cudaSuccess);
+    a.in[f] = in->field[f];
+  }
+  if (!in->pblh)
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_step: null pblh", cudaSuccess);
+  a.pblh = in->pblh;
+  for (int f = 0; f < MAM4B_NOUT; ++f) {
+    if (!out->field[f])
+      return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_step: null output field", cudaSuccess);
+    a.out[f] = out->field[f];
+  }
+  for (int f = 0; f < MAM4B_NDIAG; ++f) {
+    a.diag[f] = out->diag[f];
+    diag = diag || (out->diag[f] != nullptr);
+  }
+  a.flags = ctx->d_flags;
+  a.ncell = (long long)ncol * nlev;
+  a.nlev = nlev;
+  a.dt = dt;
+  a.do_cond = ctx->cfg.do_cond;
+  a.do_rename = ctx->cfg.do_rename;
+  a.do_newnuc = ctx->cfg.do_newnuc;
+  a.do_coag = ctx->cfg.do_coag;
+  a.optaa = ctx->cfg.gaexch_h2so4_uptake_optaa;
+  a.nmono = ctx->cfg.n_so4_monolayers_pcage;
+  cudaStream_t s = (cudaStream_t)stream;
+  ctx->last_stream = s;
+  if (a.ncell == 0)
+    return MAM4B_OK;
+  const int block = 128;
+  const long long grid = (a.ncell + block - 1) / block;
+  if (grid > 0x7fffffffLL)
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_step: too many cells", cudaSuccess);
+  if (diag)
+    step_kernel<true><<<(unsigned)grid, block, 0, s>>>(a);
+  else
+    step_kernel<false><<<(unsigned)grid, block, 0, s>>>(a);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_step launch", e);
+  ctx->launches++;
+  return MAM4B_OK;
+}
+
+mam4b_status mam4b_step_slab(mam4b_ctx *ctx, const double *in_slab, const double *pblh,
+                             double *out_slab, size_t ld, int ncol, int nlev, double dt,
+                             int precision, void *stream) {
+  if (!ctx || !in_slab || !pblh || !out_slab || ncol < 0 || nlev <= 0 ||
+      ld < (size_t)ncol * (size_t)nlev)
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_step_slab", cudaSuccess);
+  mam4b_state_view iv;
+  mam4b_tend_view ov;
+  memset(&iv, 0, sizeof(iv));
+  memset(&ov, 0, sizeof(ov));
+  for (int f = 0; f < MAM4B_NIN; ++f)
+    iv.field[f] = in_slab + (size_t)f * ld;
+  iv.pblh = pblh;
+  for (int f = 0; f < MAM4B_NOUT; ++f)
+    ov.field[f] = out_slab + (size_t)f * ld;
+  return mam4b_step(ctx, &iv, &ov, ncol, nlev, dt, precision, stream);
+}
+
+static cudaError_t grow(double **p, size_t *cap, size_t need) {
+  if (*cap >= need)
+    return cudaSuccess;
+  cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  cudaError_t e = cudaMalloc(p, need * sizeof(double));
+  if (e == cudaSuccess)
+    *cap = need;
+  return e;
+}
+
+mam4b_status mam4b_step_host(mam4b_ctx *ctx, const double *in_slab, const double *pblh,
+                             double *out_slab, size_t ld, int ncol, int nlev, double dt,
+                             int precision, void *stream) {
+  if (!ctx || !in_slab || !pblh || !out_slab || ncol < 0 || nlev <= 0 ||
+      ld < (size_t)ncol * (size_t)nlev)
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_step_host", cudaSuccess);
+  const size_t n = (size_t)ncol * (size_t)nlev;
+  cudaError_t e = grow(&ctx->d_in, &ctx->cap_in, (size_t)MAM4B_NIN * n);
+  if (e == cudaSuccess)
+    e = grow(&ctx->d_out, &ctx->cap_out, (size_t)MAM4B_NOUT * n);
+  if (e == cudaSuccess)
+    e = grow(&ctx->d_pblh, &ctx->cap_pblh, (size_t)(ncol > 0 ? ncol : 1));
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_step_host alloc", e);
+  cudaStream_t s = (cudaStream_t)stream;
+  // one copy per field when the host leading dimension differs from n
+  if (ld == n) {
+    e = cudaMemcpyAsync(ctx->d_in, in_slab, (size_t)MAM4B_NIN * n * sizeof(double),
+                        cudaMemcpyHostToDevice, s);
+  } else {
+    for (int f = 0; f < MAM4B_NIN && e == cudaSuccess; ++f)
+      e = cudaMemcpyAsync(ctx->d_in + (size_t)f * n, in_slab + (size_t)f * ld,
+                          n * sizeof(double), cudaMemcpyHostToDevice, s);
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(ctx->d_pblh, pblh, (size_t)ncol * sizeof(double), cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_step_host H2D", e);
+  mam4b_status st = mam4b_step_slab(ctx, ctx->d_in, ctx->d_pblh, ctx->d_out, n, ncol, nlev, dt,
+                                    precision, stream);
+  if (st != MAM4B_OK)
+    return st;
+  if (ld == n) {
+    e = cudaMemcpyAsync(out_slab, ctx->d_out, (size_t)MAM4B_NOUT * n * sizeof(double),
+                        cudaMemcpyDeviceToHost, s);
+  } else {
+    for (int f = 0; f < MAM4B_NOUT && e == cudaSuccess; ++f)
+      e = cudaMemcpyAsync(out_slab + (size_t)f * ld, ctx->d_out + (size_t)f * n,
+                          n * sizeof(double), cudaMemcpyDeviceToHost, s);
+  }
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_step_host D2H", e);
+  return MAM4B_OK;
+}
+
+mam4b_status mam4b_last_status(mam4b_ctx *ctx, uint32_t *flags) {
+  if (!ctx || !flags)
+    return MAM4B_ERR_INVALID_ARGUMENT;
+  cudaError_t e = cudaStreamSynchronize(ctx->last_stream);
+  unsigned h = 0;
+  if (e == cudaSuccess)
+    e = cudaMemcpy(&h, ctx->d_flags, sizeof(unsigned), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess)
+    e = cudaMemset(ctx->d_flags, 0, sizeof(unsigned));
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_last_status", e);
+  *flags = h;
+  return (h & MAM4B_FLAGS_ERROR_MASK) ? MAM4B_ERR_DEVICE_FLAGS : MAM4B_OK;
+}
+
+void mam4b_last_error(mam4b_ctx *ctx, char *buf, size_t len) {
+  if (!buf || len == 0)
+    return;
+  const char *m = ctx ? ctx->err : "null context";
+  snprintf(buf, len, "%s", m);
+}
+
+uint64_t mam4b_launch_count(mam4b_ctx *ctx) { return ctx ? (uint64_t)ctx->launches : 0; }
+
+}  // extern "C"

@@ -1,0 +1,155 @@
+"""ctypes binding of the C ABI in include/mam4b.h (libmam4b.so).
+
+The library is loaded from the package directory; there is no fallback: if
+the shared object is missing, or a call is made without a CUDA device, the
+call raises.
+"""
+
+import ctypes
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libmam4b.so")
+
+NIN, NOUT, NDIAG, NPOP = 57, 68, 155, 25
+FP64, MIXED = 0, 1
+STATUS = {0: "ok", 1: "invalid argument", 2: "cuda error", 3: "not supported",
+          4: "device flags"}
+FLAG_NONFINITE_INPUT = 0x1
+FLAG_SOA_NITER_LIMIT = 0x2
+FLAG_NONFINITE_OUTPUT = 0x4
+
+
+class Config(ctypes.Structure):
+    """mam4b_config: AmicPhysConfig (src/mam4xx/mam4_amicphys.hpp:223-237)
+    plus n_so4_monolayers_pcage (src/mam4xx/aging.hpp:31)."""
+    _fields_ = [("do_cond", ctypes.c_int), ("do_rename", ctypes.c_int),
+                ("do_newnuc", ctypes.c_int), ("do_coag", ctypes.c_int),
+                ("gaexch_h2so4_uptake_optaa", ctypes.c_int),
+                ("newnuc_h2so4_conc_optaa", ctypes.c_int),
+                ("n_so4_monolayers_pcage", ctypes.c_uint)]
+
+
+class StateView(ctypes.Structure):
+    _fields_ = [("field", ctypes.c_void_p * NIN), ("pblh", ctypes.c_void_p)]
+
+
+class TendView(ctypes.Structure):
+    _fields_ = [("field", ctypes.c_void_p * NOUT), ("diag", ctypes.c_void_p * NDIAG)]
+
+
+_lib = None
+
+
+def lib():
+    """Loads libmam4b.so once; raises if it was not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libmam4b.so not built: run python -m mam4xx_b200.build")
+        L = ctypes.CDLL(LIB_PATH)
+        P, I, D, S = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_size_t
+        L.mam4b_abi_version.restype = I
+        L.mam4b_default_config.argtypes = [ctypes.POINTER(Config)]
+        L.mam4b_create.argtypes = [ctypes.POINTER(P), ctypes.POINTER(Config)]
+        L.mam4b_create.restype = I
+        L.mam4b_destroy.argtypes = [P]
+        L.mam4b_destroy.restype = I
+        L.mam4b_step.argtypes = [P, ctypes.POINTER(StateView), ctypes.POINTER(TendView), I, I, D, I, P]
+        L.mam4b_step.restype = I
+        L.mam4b_step_slab.argtypes = [P, P, P, P, S, I, I, D, I, P]
+        L.mam4b_step_slab.restype = I
+        L.mam4b_step_host.argtypes = [P, P, P, P, S, I, I, D, I, P]
+        L.mam4b_step_host.restype = I
+        L.mam4b_last_status.argtypes = [P, ctypes.POINTER(ctypes.c_uint32)]
+        L.mam4b_last_status.restype = I
+        L.mam4b_last_error.argtypes = [P, ctypes.c_char_p, S]
+        L.mam4b_launch_count.argtypes = [P]
+        L.mam4b_launch_count.restype = ctypes.c_uint64
+        _lib = L
+    return _lib
+
+
+EXPORTED = ["mam4b_abi_version", "mam4b_default_config", "mam4b_create", "mam4b_destroy",
+            "mam4b_step", "mam4b_step_slab", "mam4b_step_host", "mam4b_last_status",
+            "mam4b_last_error", "mam4b_launch_count"]
+
+
+def default_config(**overrides):
+    c = Config()
+    lib().mam4b_default_config(ctypes.byref(c))
+    for k, v in overrides.items():
+        setattr(c, k, int(v))
+    return c
+
+
+class MicrophysicsError(RuntimeError):
+    pass
+
+
+class Context:
+    """Owns one mam4b_ctx (bound to the current CUDA device)."""
+
+    def __init__(self, config=None):
+        self._lib = lib()
+        self.config = config if config is not None else default_config()
+        h = ctypes.c_void_p()
+        st = self._lib.mam4b_create(ctypes.byref(h), ctypes.byref(self.config))
+        if st != 0:
+            raise MicrophysicsError("mam4b_create failed: %s" % STATUS.get(st, st))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.mam4b_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st, what):
+        if st != 0:
+            buf = ctypes.create_string_buffer(256)
+            self._lib.mam4b_last_error(self._h, buf, 256)
+            raise MicrophysicsError("%s: %s (%s)" % (what, STATUS.get(st, st), buf.value.decode()))
+
+    def step(self, in_ptrs, pblh_ptr, out_ptrs, ncol, nlev, dt, diag_ptrs=None,
+             precision=FP64, stream=0):
+        iv = StateView()
+        for f, p in enumerate(in_ptrs):
+            iv.field[f] = p
+        iv.pblh = pblh_ptr
+        ov = TendView()
+        for f, p in enumerate(out_ptrs):
+            ov.field[f] = p
+        if diag_ptrs is not None:
+            for f, p in enumerate(diag_ptrs):
+                ov.diag[f] = p
+        st = self._lib.mam4b_step(self._h, ctypes.byref(iv), ctypes.byref(ov), int(ncol),
+                                  int(nlev), float(dt), int(precision), ctypes.c_void_p(stream))
+        self._check(st, "mam4b_step")
+
+    def step_slab(self, in_ptr, pblh_ptr, out_ptr, ld, ncol, nlev, dt, precision=FP64, stream=0):
+        st = self._lib.mam4b_step_slab(self._h, in_ptr, pblh_ptr, out_ptr, int(ld), int(ncol),
+                                       int(nlev), float(dt), int(precision),
+                                       ctypes.c_void_p(stream))
+        self._check(st, "mam4b_step_slab")
+
+    def step_host(self, in_ptr, pblh_ptr, out_ptr, ld, ncol, nlev, dt, precision=FP64, stream=0):
+        st = self._lib.mam4b_step_host(self._h, in_ptr, pblh_ptr, out_ptr, int(ld), int(ncol),
+                                       int(nlev), float(dt), int(precision),
+                                       ctypes.c_void_p(stream))
+        self._check(st, "mam4b_step_host")
+
+    def last_status(self):
+        f = ctypes.c_uint32(0)
+        st = self._lib.mam4b_last_status(self._h, ctypes.byref(f))
+        if st not in (0, 4):
+            self._check(st, "mam4b_last_status")
+        return int(f.value)
+
+    def launch_count(self):
+        return int(self._lib.mam4b_launch_count(self._h))

@@ -1,0 +1,76 @@
+"""Build recipe of the CPU checkers (test infrastructure only).
+
+  oracle/libmam4oracle.so    gcc, plain C restatement (oracle/mam4_oracle.c)
+  oracle/libmam4oracle_ulp.so the same with every libm result moved by a few
+                             ulps (seeded): the algorithm's own sensitivity
+  oracle/libmam4oracle_gpu.so the same source compiled for the GPU with nvcc
+                             (CUDA libm, no FMA contraction): the libm-matched
+                             diagnostic oracle
+  oracle/_ref/libmam4ref.so  g++, the mam4xx reference headers included
+                             read-only from <ref>/src and compiled unchanged
+                             against the host shim in oracle/shim; built only
+                             when the reference tree exists (no cmake, no
+                             Kokkos/EKAT: the shim stands in for the small
+                             surface the headers use)
+
+Both use -O3 -ffp-contract=off so that every expression rounds in source
+order, and OpenMP for the multi-core CPU baseline. No -march=native: the
+libraries travel to other hosts.
+"""
+
+import os
+import subprocess
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+PORT_SO = os.path.join(HERE, "libmam4oracle.so")
+ULP_SO = os.path.join(HERE, "libmam4oracle_ulp.so")
+REF_SO = os.path.join(HERE, "_ref", "libmam4ref.so")
+GPU_SO = os.path.join(HERE, "libmam4oracle_gpu.so")
+DEFAULT_REF = "/root/reference"
+
+COMMON = ["-O3", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off"]
+
+
+def _run(cmd):
+    print("+", " ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(ref=None, force=False):
+    deps = [os.path.join(HERE, "mam4_oracle.c"), os.path.join(HERE, "oracle_api.h"),
+            os.path.join(ROOT, "include", "mam4b.h"),
+            os.path.join(ROOT, "mam4xx_b200", "csrc", "coag_tables.inc")]
+    if force or _stale(PORT_SO, deps):
+        _run(["gcc", "-std=c99"] + COMMON + [os.path.join(HERE, "mam4_oracle.c"), "-o", PORT_SO, "-lm"])
+    if force or _stale(ULP_SO, deps):
+        # same restatement with each libm result moved by one ulp (seeded):
+        # measures the algorithm's own sensitivity to last-bit differences
+        _run(["gcc", "-std=gnu99", "-DORACLE_ULP_NOISE"] + COMMON +
+             [os.path.join(HERE, "mam4_oracle.c"), "-o", ULP_SO, "-lm"])
+    if force or _stale(GPU_SO, deps + [os.path.join(HERE, "mam4_oracle_gpu.cu")]):
+        # the same restatement as device code (CUDA libm, no FMA contraction)
+        _run([os.environ.get("NVCC", "nvcc"), "-x", "cu", "-gencode", "arch=compute_100a,code=sm_100a",
+              "-O3", "-std=c++17", "--fmad=false", "-Xcompiler", "-fPIC", "-shared",
+              os.path.join(HERE, "mam4_oracle_gpu.cu"), "-o", GPU_SO])
+    ref = ref or DEFAULT_REF
+    src = os.path.join(ref, "src")
+    if os.path.isdir(os.path.join(src, "mam4xx")):
+        shim = os.path.join(HERE, "shim")
+        rdeps = [os.path.join(HERE, "ref", "ref_step.cpp"), os.path.join(shim, "kokkos_ekat_shim.hpp")]
+        if force or _stale(REF_SO, rdeps):
+            os.makedirs(os.path.dirname(REF_SO), exist_ok=True)
+            _run(["g++", "-std=c++17"] + COMMON + ["-I", shim, "-I", src,
+                  os.path.join(HERE, "ref", "ref_step.cpp"), "-o", REF_SO])
+    return PORT_SO
+
+
+if __name__ == "__main__":
+    build(force=True)

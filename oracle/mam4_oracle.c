@@ -32,6 +32,79 @@
 #include <omp.h>
 #endif
 
+/* The same source compiles for the host (gcc) and, as the libm-matched
+ * diagnostic oracle, for the GPU (oracle/mam4_oracle_gpu.cu, nvcc): there
+ * every function is device code and every table lives in device memory. */
+#ifdef ORACLE_GPU
+#define ORC_FN static __device__
+#define ORC_TABLE static __device__ const
+#else
+#define ORC_FN static
+#define ORC_TABLE static const
+#endif
+
+#ifdef ORACLE_ULP_NOISE
+/* Rounding-sensitivity build (libmam4oracle_ulp.so): every libm result is
+ * moved by one ulp up or down, the direction drawn from a xorshift stream
+ * seeded per cell, so the run is deterministic under any thread schedule.
+ * The spread of such runs around the canonical build measures how much the
+ * reference algorithm itself amplifies last-bit differences of its math
+ * library; the CUDA kernel is held to that spread on rounding-sensitive
+ * cells and to 1e-12 everywhere else. */
+#include <stdint.h>
+static uint64_t g_noise_seed = 0;
+static __thread uint64_t t_noise;
+static void noise_seed_cell(size_t c) {
+  uint64_t z = (uint64_t)c + 0x9E3779B97F4A7C15ull * (g_noise_seed + 1);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  t_noise = (z ^ (z >> 31)) | 1ull;
+}
+static double nudge(double v, int k) {
+  for (int i = 0; i < k; ++i)
+    v = nextafter(v, INFINITY);
+  for (int i = 0; i > k; --i)
+    v = nextafter(v, -INFINITY);
+  return v;
+}
+/* moves v by a nonzero number of ulps in [-maxulp, maxulp] */
+static double noisy_k(double v, int maxulp) {
+  if (g_noise_seed == 0 || !isfinite(v) || v == 0.0)
+    return v;
+  t_noise ^= t_noise << 13;
+  t_noise ^= t_noise >> 7;
+  t_noise ^= t_noise << 17;
+  const int k = 1 + (int)((t_noise >> 1) % (uint64_t)maxulp);
+  return nudge(v, (t_noise & 1) ? k : -k);
+}
+/* ulp bounds of the GPU math library for these functions: 2 ulp, erfc 5 */
+static double noisy(double v) { return noisy_k(v, 2); }
+static double n_exp(double x) { return noisy(exp(x)); }
+static double n_log(double x) { return noisy(log(x)); }
+static double n_pow(double x, double y) { return noisy(pow(x, y)); }
+static double n_cbrt(double x) { return noisy(cbrt(x)); }
+static double n_erfc(double x) { return noisy_k(erfc(x), 5); }
+static double n_log10(double x) { return noisy(log10(x)); }
+static double n_atan2(double y, double x) { return noisy(atan2(y, x)); }
+static double n_hypot(double x, double y) { return noisy(hypot(x, y)); }
+static double n_sin(double x) { return noisy(sin(x)); }
+static double n_cos(double x) { return noisy(cos(x)); }
+#define exp n_exp
+#define log n_log
+#define pow n_pow
+#define cbrt n_cbrt
+#define erfc n_erfc
+#define log10 n_log10
+#define atan2 n_atan2
+#define hypot n_hypot
+#define sin n_sin
+#define cos n_cos
+void mam4orc_set_ulp_noise(unsigned long long seed) { g_noise_seed = seed; }
+#define NOISE_SEED_CELL(c) noise_seed_cell(c)
+#else
+#define NOISE_SEED_CELL(c) ((void)0)
+#endif
+
 typedef double real;
 
 #define NMODE 4
@@ -41,82 +114,82 @@ typedef double real;
 #define NSUB 3
 #define NQTEND 4
 
-static const real PI = 3.14159265358979323846264;
+ORC_TABLE real PI = 3.14159265358979323846264;
 #define PI_SIXTH (3.14159265358979323846264 / 6)
 #define EPS DBL_EPSILON
 
-static real rmax(real a, real b) { return (a < b) ? b : a; }
-static real rmin(real a, real b) { return (b < a) ? b : a; }
-static real square(real x) { return x * x; }
-static real cube(real x) { return x * x * x; }
+ORC_FN real rmax(real a, real b) { return (a < b) ? b : a; }
+ORC_FN real rmin(real a, real b) { return (b < a) ? b : a; }
+ORC_FN real square(real x) { return x * x; }
+ORC_FN real cube(real x) { return x * x * x; }
 /* utils.hpp:24 */
-static real min_max_bound(real lo, real hi, real x) { return rmax(lo, rmin(hi, x)); }
+ORC_FN real min_max_bound(real lo, real hi, real x) { return rmax(lo, rmin(hi, x)); }
 /* floating_point.hpp:79 */
-static real safe_denominator(real x) { return x / (x * x + EPS * EPS); }
+ORC_FN real safe_denominator(real x) { return x / (x * x + EPS * EPS); }
 
 /* ------------------------------------------------------------ constants */
 /* aero_modes.hpp:76-123 (accumulation, aitken, coarse, primary carbon) */
-static const real MODE_DMIN[NMODE] = {5.35e-8, 8.7e-9, 1e-6, 1e-8};
-static const real MODE_DNOM[NMODE] = {1.1e-7, 2.6e-8, 2e-6, 5e-8};
-static const real MODE_DMAX[NMODE] = {4.4e-7, 5.2e-8, 4e-6, 1e-7};
-static const real MODE_SIG[NMODE] = {1.8, 1.6, 1.8, 1.60000002384186};
-static const real RH_CRYST = 0.35, RH_DELIQ = 0.8;
+ORC_TABLE real MODE_DMIN[NMODE] = {5.35e-8, 8.7e-9, 1e-6, 1e-8};
+ORC_TABLE real MODE_DNOM[NMODE] = {1.1e-7, 2.6e-8, 2e-6, 5e-8};
+ORC_TABLE real MODE_DMAX[NMODE] = {4.4e-7, 5.2e-8, 4e-6, 1e-7};
+ORC_TABLE real MODE_SIG[NMODE] = {1.8, 1.6, 1.8, 1.60000002384186};
+ORC_TABLE real RH_CRYST = 0.35, RH_DELIQ = 0.8;
 /* aero_modes.hpp:214-243; AeroId: SOA 0 SO4 1 POM 2 BC 3 NaCl 4 DST 5 MOM 6 */
-static const int NSPEC[NMODE] = {7, 4, 7, 3};
-static const int MODE_SPEC[NMODE][7] = {{1, 2, 0, 3, 5, 4, 6},
+ORC_TABLE int NSPEC[NMODE] = {7, 4, 7, 3};
+ORC_TABLE int MODE_SPEC[NMODE][7] = {{1, 2, 0, 3, 5, 4, 6},
                                         {1, 0, 4, 6, -1, -1, -1},
                                         {5, 4, 1, 3, 2, 0, 6},
                                         {2, 3, 6, -1, -1, -1, -1}};
 /* aero_modes.hpp:140-150 densities by AeroId */
-static const real AERO_DENS[NAER] = {1000.0, 1770.0, 1000.0, 1700.0, 1900.0, 2600.0, 1601.0};
+ORC_TABLE real AERO_DENS[NAER] = {1000.0, 1770.0, 1000.0, 1700.0, 1900.0, 2600.0, 1601.0};
 /* state_q indices (0-based): number of each mode (utils.hpp:205-218) and the
  * first species slot of each mode (ndrop.hpp:77-80, minus one) */
-static const int NUM_IDX[NMODE] = {22, 27, 35, 39};
-static const int SPEC0_IDX[NMODE] = {15, 23, 28, 36};
+ORC_TABLE int NUM_IDX[NMODE] = {22, 27, 35, 39};
+ORC_TABLE int SPEC0_IDX[NMODE] = {15, 23, 28, 36};
 /* water uptake species types (water_uptake.hpp:314-344 /
  * ndrop.hpp:59-80): density and hygroscopicity by type 1..9 */
-static const real SPECDENS[14] = {0.1770000000E+04, 0.1797693135 + 309, 0.1797693135 + 309,
+ORC_TABLE real SPECDENS[14] = {0.1770000000E+04, 0.1797693135 + 309, 0.1797693135 + 309,
                                   0.1000000000E+04, 0.1000000000E+04, 0.1700000000E+04,
                                   0.1900000000E+04, 0.2600000000E+04, 0.1601000000E+04,
                                   0, 0, 0, 0, 0};
-static const real SPECHYGRO[14] = {0.5070000000E+00, 0.1797693135 + 309, 0.1797693135 + 309,
+ORC_TABLE real SPECHYGRO[14] = {0.5070000000E+00, 0.1797693135 + 309, 0.1797693135 + 309,
                                    0.1000000083E-09, 0.1400000000E+00, 0.1000000013E-09,
                                    0.1160000000E+01, 0.6800000000E-01, 0.1000000015E+00,
                                    0, 0, 0, 0, 0};
-static const int LSPECTYPE[NMODE][7] = {{1, 4, 5, 6, 8, 7, 9},
+ORC_TABLE int LSPECTYPE[NMODE][7] = {{1, 4, 5, 6, 8, 7, 9},
                                         {1, 5, 7, 9, 0, 0, 0},
                                         {8, 7, 1, 6, 4, 5, 9},
                                         {4, 6, 9, 0, 0, 0, 0}};
 /* chemistry mechanism molecular weights (gas_chem_mechanism.hpp:31-38) */
-static const real ADV_MASS[PCNST] = {
+ORC_TABLE real ADV_MASS[PCNST] = {
     47.998200, 34.013600, 98.078400, 64.064800, 62.132400, 12.011000, 115.107340, 12.011000,
     12.011000, 12.011000, 135.064039, 58.442468, 250092.672000, 1.007400, 115.107340,
     12.011000, 58.442468, 250092.672000, 1.007400, 135.064039, 58.442468, 115.107340,
     12.011000, 12.011000, 12.011000, 250092.672000, 1.007400, 12.011000, 12.011000,
     250092.672000, 1.007400};
 /* mam4_amicphys.hpp:35-154 index maps and unit factors */
-static const int NUMPTR31[NMODE] = {13, 18, 26, 30};
-static const int LMASSPTR31[NAER][NMODE] = {{6, 14, 19, 27},  {7, 15, 20, 28},
+ORC_TABLE int NUMPTR31[NMODE] = {13, 18, 26, 30};
+ORC_TABLE int LMASSPTR31[NAER][NMODE] = {{6, 14, 19, 27},  {7, 15, 20, 28},
                                             {8, 16, 21, 29},  {9, 17, 22, -6},
                                             {10, -6, 23, -6}, {11, -6, 24, -6},
                                             {12, -6, 25, -6}};
-static const int LMAPCC_ALL[PCNST] = {0, 0, 1, 0, 0, 1, 2, 2, 2, 2, 2, 2, 2, 3, 2, 2,
+ORC_TABLE int LMAPCC_ALL[PCNST] = {0, 0, 1, 0, 0, 1, 2, 2, 2, 2, 2, 2, 2, 3, 2, 2,
                                       2, 2, 3, 2, 2, 2, 2, 2, 2, 2, 3, 2, 2, 2, 3};
-static const int LMAP_GAS[NGAS] = {5, 2};
-static const int LMAP_AER[NAER][NMODE] = {{8, 15, 24, -1},  {6, 14, 21, -1}, {7, -1, 23, 27},
+ORC_TABLE int LMAP_GAS[NGAS] = {5, 2};
+ORC_TABLE int LMAP_AER[NAER][NMODE] = {{8, 15, 24, -1},  {6, 14, 21, -1}, {7, -1, 23, 27},
                                           {9, -1, 22, 28},  {11, 16, 20, -1},
                                           {10, -1, 19, -1}, {12, 17, 25, 29}};
-static const real FCVT_AER[NAER] = {8.000000000000000E-002, 1, 8.000000000000000E-002, 1, 1, 1, 1};
+ORC_TABLE real FCVT_AER[NAER] = {8.000000000000000E-002, 1, 8.000000000000000E-002, 1, 1, 1, 1};
 /* rename / aging mass-to-volume factors (mam4_amicphys.hpp:1495-1502) */
-static const real MASS_2_VOL[NAER] = {0.15, 6.4971751412429377e-002, 0.15,
+ORC_TABLE real MASS_2_VOL[NAER] = {0.15, 6.4971751412429377e-002, 0.15,
                                       7.0588235294117650e-003, 3.0789473684210526e-002,
                                       5.1923076923076926e-002, 156.20986883198000};
 
 /* coagulation correction tables (coagulation.hpp:81, :330, :588) */
-#define COAG_TABLE_QUALIFIER static const
+#define COAG_TABLE_QUALIFIER ORC_TABLE
 #include "../mam4xx_b200/csrc/coag_tables.inc"
 
-static real fcvt_gas(int igas) { /* mam4_amicphys.hpp:137-153 */
+ORC_FN real fcvt_gas(int igas) { /* mam4_amicphys.hpp:137-153 */
   const real mw_gas = ADV_MASS[LMAP_GAS[igas]];
   real denom = mw_gas;
   if (igas < 1)
@@ -127,10 +200,10 @@ static real fcvt_gas(int igas) { /* mam4_amicphys.hpp:137-153 */
  * water of the subareas (:2248-2250), so every water entry stays zero. */
 
 /* conversions.hpp:299-315 */
-static real mean_particle_diameter_from_volume(real v, real sig) {
+ORC_FN real mean_particle_diameter_from_volume(real v, real sig) {
   return cbrt(v / PI_SIXTH) * exp(-1.5 * square(log(sig)));
 }
-static real mean_particle_volume_from_diameter(real d, real sig) {
+ORC_FN real mean_particle_volume_from_diameter(real d, real sig) {
   return cube(d) * exp(4.5 * square(log(sig))) * PI_SIXTH;
 }
 
@@ -141,7 +214,7 @@ typedef struct {
   real n2v_min[NMODE], n2v_max[NMODE], n2v_nom[NMODE];
 } calcsize_data;
 
-static void calcsize_init(calcsize_data *d) { /* modal_aero_calcsize.hpp:22-108 */
+ORC_FN void calcsize_init(calcsize_data *d) { /* modal_aero_calcsize.hpp:22-108 */
   for (int m = 0; m < NMODE; ++m) {
     d->n2v_nom[m] = 1.0 / mean_particle_volume_from_diameter(MODE_DNOM[m], MODE_SIG[m]);
     d->n2v_min[m] = 1.0 / mean_particle_volume_from_diameter(MODE_DMAX[m], MODE_SIG[m]);
@@ -152,7 +225,7 @@ static void calcsize_init(calcsize_data *d) { /* modal_aero_calcsize.hpp:22-108 
 }
 
 /* calcsize.hpp:56-78 */
-static void update_diameter_and_vol2num(real drv, real num, real v2nmin, real v2nmax,
+ORC_FN void update_diameter_and_vol2num(real drv, real num, real v2nmin, real v2nmax,
                                         real dgnmin, real dgnmax, real sig, real *dgncur,
                                         real *v2ncur) {
   if (!(drv > 0.0))
@@ -170,7 +243,7 @@ static void update_diameter_and_vol2num(real drv, real num, real v2nmin, real v2
 }
 
 /* calcsize.hpp:95-310 */
-static void adjust_num_sizes(real drv_i, real drv_c, real init_num_i, real init_num_c, real dt,
+ORC_FN void adjust_num_sizes(real drv_i, real drv_c, real init_num_i, real init_num_c, real dt,
                              real v2nmin, real v2nmax, real adj_tscale_inv, real *num_i,
                              real *num_c, real *dqdt, real *dqqcwdt) {
   const real frac = rmax(0.0, rmin(1.0, dt * adj_tscale_inv));
@@ -236,7 +309,7 @@ static void adjust_num_sizes(real drv_i, real drv_c, real init_num_i, real init_
 }
 
 /* calcsize.hpp:481-515 */
-static void compute_new_sz_after_transfer(real drv, real num, real v2n_hi, real v2n_lo, real v2n,
+ORC_FN void compute_new_sz_after_transfer(real drv, real num, real v2n_hi, real v2n_lo, real v2n,
                                           real dgn_hi, real dgn_lo, real dgn_nom, real sig,
                                           real *dgncur, real *v2ncur) {
   if (drv > 0.0) {
@@ -257,7 +330,7 @@ static void compute_new_sz_after_transfer(real drv, real num, real v2n_hi, real 
 }
 
 /* modal_aero_calcsize.hpp:448-497 (update_tends_flx) */
-static void update_tends_flx(int jmode, int src, int dest, const int *src_idx,
+ORC_FN void update_tends_flx(int jmode, int src, int dest, const int *src_idx,
                              const int *dest_idx, const real xfertend_num[2][2], real xfercoef,
                              const real *state_q, const real *qqcw, real *ptend, real *dqqcwdt) {
   ptend[src] -= xfertend_num[jmode][0];
@@ -277,7 +350,7 @@ static void update_tends_flx(int jmode, int src, int dest, const int *src_idx,
 /* modal_aero_calcsize.hpp:750-932 (modal_aero_calcsize_sub with
  * size_adjustment :263, compute_dry_volume :421, aitken_accum_exchange :499,
  * compute_coef_acc_ait_transfer :162, calcsize.hpp:314) */
-static void calcsize_sub(const calcsize_data *cd, const real *state_q, const real *qqcw, real dt,
+ORC_FN void calcsize_sub(const calcsize_data *cd, const real *state_q, const real *qqcw, real dt,
                          real dgncur_i[NMODE], real dgncur_c[NMODE], real ptend[40],
                          real dqqcwdt[40]) {
   const int ait = 1, acc = 0;
@@ -364,7 +437,7 @@ static void calcsize_sub(const calcsize_data *cd, const real *state_q, const rea
   int acc2ait = 0;
   real xfc_num_acc2ait = 0, xfc_vol_acc2ait = 0, drv_i_noxf = 0, drv_c_noxf = 0;
   {
-    static const int noxf[7] = {0, 1, 0, 1, 1, 0, 0};
+    const int noxf[7] = {0, 1, 0, 1, 1, 0, 0};
     real drv_t = dv_i_accsv + dv_c_accsv;
     real num_t = n_i_accsv + n_c_accsv;
     real num_t0 = 0;
@@ -436,8 +509,8 @@ static void calcsize_sub(const calcsize_data *cd, const real *state_q, const rea
                                   MODE_DNOM[acc], MODE_SIG[acc], &dgncur_c[acc], &tmp);
     /* common species: accumulation slots SO4, SOA, NaCl, MOM and their
      * aitken counterparts (modal_aero_calcsize.hpp:46-70) */
-    static const int acc_in_ait[4] = {15, 17, 20, 21};
-    static const int ait_in_acc[4] = {23, 24, 25, 26};
+    const int acc_in_ait[4] = {15, 17, 20, 21};
+    const int ait_in_acc[4] = {23, 24, 25, 26};
     if (ait2acc > 0)
       update_tends_flx(0, 27, 22, ait_in_acc, acc_in_ait, xfertend_num, xfc_vol_ait2acc,
                        state_q, qqcw, ptend, dqqcwdt);
@@ -452,18 +525,18 @@ static void calcsize_sub(const calcsize_data *cd, const real *state_q, const rea
 typedef struct {
   real re, im;
 } cplx;
-static cplx cmk(real r, real i) {
+ORC_FN cplx cmk(real r, real i) {
   cplx z = {r, i};
   return z;
 }
-static cplx cadd(cplx a, cplx b) { return cmk(a.re + b.re, a.im + b.im); }
-static cplx csub(cplx a, cplx b) { return cmk(a.re - b.re, a.im - b.im); }
-static cplx cmul(cplx a, cplx b) {
+ORC_FN cplx cadd(cplx a, cplx b) { return cmk(a.re + b.re, a.im + b.im); }
+ORC_FN cplx csub(cplx a, cplx b) { return cmk(a.re - b.re, a.im - b.im); }
+ORC_FN cplx cmul(cplx a, cplx b) {
   return cmk(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re);
 }
-static cplx cscale(real s, cplx a) { return cmk(s * a.re, s * a.im); }
-static cplx cdivr(cplx a, real s) { return cmk(a.re / s, a.im / s); }
-static cplx cdiv(cplx x, cplx y) {
+ORC_FN cplx cscale(real s, cplx a) { return cmk(s * a.re, s * a.im); }
+ORC_FN cplx cdivr(cplx a, real s) { return cmk(a.re / s, a.im / s); }
+ORC_FN cplx cdiv(cplx x, cplx y) {
   const real s = fabs(y.re) + fabs(y.im);
   if (s == 0.0)
     return cmk(x.re / s, x.im / s);
@@ -473,7 +546,7 @@ static cplx cdiv(cplx x, cplx y) {
   const cplx r = cmul(xs, ycs);
   return cmk(r.re / yabs2, r.im / yabs2);
 }
-static cplx csqrt_k(cplx x) {
+ORC_FN cplx csqrt_k(cplx x) {
   const real r = x.re, i = x.im;
   if (r == 0.0) {
     const real t = sqrt(fabs(i) / 2);
@@ -483,7 +556,7 @@ static cplx csqrt_k(cplx x) {
   const real u = t / 2;
   return r > 0.0 ? cmk(u, i / t) : cmk(fabs(i) / t, i < 0.0 ? -u : u);
 }
-static cplx cpow_k(cplx x, real y) {
+ORC_FN cplx cpow_k(cplx x, real y) {
   const real r = hypot(x.re, x.im);
   const real th = atan2(x.im, x.re);
   const real rho = pow(r, y), ang = y * th;
@@ -491,7 +564,7 @@ static cplx cpow_k(cplx x, real y) {
 }
 
 /* water_uptake.hpp:131-171 */
-static void makoh_quartic(cplx cx[4], real p3, real p2, real p1, real p0) {
+ORC_FN void makoh_quartic(cplx cx[4], real p3, real p2, real p1, real p0) {
   const real qq = -p2 * p2 / 36.0 + (p3 * p1 - 4.0 * p0) / 12.0;
   const real rr = -cube(p2 / 6.0) + p2 * (p3 * p1 - 4.0 * p0) / 48.0 +
                   (4.0 * p0 * p2 - p0 * p3 * p3 - p1 * p1) / 16.0;
@@ -519,7 +592,7 @@ static void makoh_quartic(cplx cx[4], real p3, real p2, real p1, real p0) {
 }
 
 /* water_uptake.hpp:101-125 */
-static real find_real_solution(real rdry, const cplx cx[4]) {
+ORC_FN real find_real_solution(real rdry, const cplx cx[4]) {
   const real eps = 1e-4;
   real rwet = 1000.0 * rdry;
   for (int n = 0; n < 4; ++n) {
@@ -538,7 +611,7 @@ static real find_real_solution(real rdry, const cplx cx[4]) {
 }
 
 /* water_uptake.hpp:180-230 */
-static real kohler(real rdry_in, real hygro, real rh) {
+ORC_FN real kohler(real rdry_in, real hygro, real rh) {
   const real rhow = 1.0, surften = 76.0, mw = 18.0, tair = 273.0, ugascon = 8.3e7;
   const real eps = 1e-4;
   const real aa = 2.0e4 * mw * surften / (ugascon * tair * rhow);
@@ -565,7 +638,7 @@ static real kohler(real rdry_in, real hygro, real rh) {
 }
 
 /* wv_sat_methods.hpp:14-46, 94-131 */
-static real goffgratch_svp_water(real t) {
+ORC_FN real goffgratch_svp_water(real t) {
   const real tboil = 373.16, ten = 10, one = 1;
   return pow(ten, -7.90298 * (tboil / t - one) + 5.02808 * log10(tboil / t) -
                       1.3816e-7 * (pow(ten, 11.344 * (one - t / tboil)) - one) +
@@ -573,7 +646,7 @@ static real goffgratch_svp_water(real t) {
                       log10(1013.246)) *
          ten * ten;
 }
-static real qsat_water(real t, real p) {
+ORC_FN real qsat_water(real t, real p) {
   const real es = goffgratch_svp_water(t);
   const real epsilo = 0.018016 / 0.028966;
   const real omeps = 1 - epsilo;
@@ -583,7 +656,7 @@ static real qsat_water(real t, real p) {
 }
 
 /* water_uptake.hpp:362-480 (dryaer, rh_clearair, wetaer, wetdens) */
-static void water_uptake_dr(const real *state_q, real temp, real pmid, real cldn,
+ORC_FN void water_uptake_dr(const real *state_q, real temp, real pmid, real cldn,
                             const real dgncur_a[NMODE], real dgncur_awet[NMODE],
                             real qaerwat[NMODE], real wetdens[NMODE]) {
   real hygro[NMODE], naer[NMODE], dryrad[NMODE], dryvol[NMODE], drymass[NMODE];
@@ -659,13 +732,13 @@ static void water_uptake_dr(const real *state_q, real temp, real pmid, real cldn
  * gasaerexch.hpp, gasaerexch_soaexch.hpp */
 
 /* gasaerexch.hpp:255-268 */
-static real fuchs_sutugin(real d_p, real freepath, real a283, real a75) {
+ORC_FN real fuchs_sutugin(real d_p, real freepath, real a283, real a75) {
   const real kn = 2.0 * freepath / d_p;
   return (a75 * (1.0 + kn)) / (kn * (kn + 1.0 + a283) + a75);
 }
 
 /* gasaerexch.hpp:270-353 */
-static void gas_aer_uptkrates_1box1gas(real accom, real gasdiffus, real freepath,
+ORC_FN void gas_aer_uptkrates_1box1gas(real accom, real gasdiffus, real freepath,
                                        const real dgn_awet[NMODE], const real lnsg[NMODE],
                                        real uptk[NMODE]) {
   const real tworootpi = 2 * sqrt(PI);
@@ -694,7 +767,7 @@ static void gas_aer_uptkrates_1box1gas(real accom, real gasdiffus, real freepath
 
 /* gasaerexch_soaexch.hpp:80-341 (the 9-argument variant called by
  * mam_gasaerexch_1subarea); returns the number of sub-steps */
-static int soaexch_1subarea(real dtsubstep, real temp, real pmid, real qgas_cur[NGAS],
+ORC_FN int soaexch_1subarea(real dtsubstep, real temp, real pmid, real qgas_cur[NGAS],
                             real qgas_avg[NGAS], real qaer_cur[NAER][NMODE],
                             const real uptkaer[NGAS][NMODE]) {
   const int niter_max = 1000;
@@ -822,7 +895,7 @@ static int soaexch_1subarea(real dtsubstep, real temp, real pmid, real qgas_cur[
 }
 
 /* gasaerexch.hpp:355-557; returns SOA sub-step count */
-static int gasaerexch_1subarea(real dtsubstep, real temp, real pmid, real aircon,
+ORC_FN int gasaerexch_1subarea(real dtsubstep, real temp, real pmid, real aircon,
                                real qgas_cur[NGAS], real qgas_avg[NGAS],
                                const real qgas_netprod[NGAS], real qaer_cur[NAER][NMODE],
                                const real qnum_cur[NMODE], const real dgn_awet[NMODE],
@@ -897,7 +970,7 @@ static int gasaerexch_1subarea(real dtsubstep, real temp, real pmid, real aircon
 }
 
 /* gasaerexch.hpp:140-221 (the unit-tested single-gas form) */
-static void h2so4_nonvolatile(real dt, real netprod, const real uptk[NMODE], real *qgas_cur,
+ORC_FN void h2so4_nonvolatile(real dt, real netprod, const real uptk[NMODE], real *qgas_cur,
                               real *qgas_avg, real qaer_cur[NMODE]) {
   real qaer_prev[NMODE];
   for (int i = 0; i < NMODE; ++i)
@@ -931,13 +1004,13 @@ static void h2so4_nonvolatile(real dt, real netprod, const real uptk[NMODE], rea
 
 /* ---------------------------------------------------------------- rename
  * rename.hpp:138-170, 225-390, 711-790 */
-static real tail_fraction(real diameter, real ln_cutoff, real fac, real ln_tail_fac, int use_tail) {
+ORC_FN real tail_fraction(real diameter, real ln_cutoff, real fac, real ln_tail_fac, int use_tail) {
   const real ld = use_tail ? log(diameter) + ln_tail_fac : log(diameter);
   const real tail = (ln_cutoff - ld) * fac;
   return 0.5 * erfc(tail);
 }
 
-static void rename_1subarea(int is_cloudy, real qnum_i[NMODE], real qaer_i[NAER][NMODE],
+ORC_FN void rename_1subarea(int is_cloudy, real qnum_i[NMODE], real qaer_i[NAER][NMODE],
                             const real qdel_i[NAER][NMODE], real qnum_c[NMODE],
                             real qaer_c[NAER][NMODE], const real qdel_c[NAER][NMODE]) {
   /* find_renaming_pairs (rename.hpp:393-476) for the only pair aitken->acc */
@@ -1041,13 +1114,13 @@ static void rename_1subarea(int is_cloudy, real qnum_i[NMODE], real qaer_i[NAER]
 /* ------------------------------------------------------------ nucleation
  * nucleation.hpp:38-118 (pbl_nuc_wang2008), :128-160 (binary), :347-860
  * (mer07_veh02_nuc_mosaic_1box), vehkamaki2002.hpp:54-190 */
-static real veh02_x_crit(real n_a, real t, real rh) {
+ORC_FN real veh02_x_crit(real n_a, real t, real rh) {
   return 0.740997 - 0.00266379 * t - 0.00349998 * log(n_a) + 0.0000504022 * t * log(n_a) +
          0.00201048 * log(rh) - 0.000183289 * t * log(rh) + 0.00157407 * square(log(rh)) -
          0.0000179059 * t * square(log(rh)) + 0.000184403 * cube(log(rh)) -
          1.50345e-6 * t * cube(log(rh));
 }
-static real veh02_log_rate(real n_a, real t, real rh, real x) {
+ORC_FN real veh02_log_rate(real n_a, real t, real rh, real x) {
   const real a = 0.14309 + 2.21956 * t - 0.0273911 * square(t) + 0.0000722811 * cube(t) + 5.91822 / x;
   const real b = 0.117489 + 0.462532 * t - 0.0118059 * square(t) + 0.0000404196 * cube(t) + 15.7963 / x;
   const real c = -0.215554 - 0.0810269 * t + 0.00143581 * square(t) - 4.7758e-6 * cube(t) - 2.91297 / x;
@@ -1062,7 +1135,7 @@ static real veh02_log_rate(real n_a, real t, real rh, real x) {
          f * log(rh) * log(n_a) + g * square(log(rh)) * (log(n_a)) + h * square(log(n_a)) +
          i * log(rh) * square(log(n_a)) + j * cube(log(n_a));
 }
-static real veh02_ntot(real n_a, real t, real rh, real x) {
+ORC_FN real veh02_ntot(real n_a, real t, real rh, real x) {
   const real A = -0.00295413 - 0.0976834 * t + 0.00102485 * square(t) - 2.18646e-6 * cube(t) - 0.101717 / x;
   const real B = -0.00205064 - 0.00758504 * t + 0.000192654 * square(t) - 6.7043e-7 * cube(t) - 0.255774 / x;
   const real C = +0.00322308 + 0.000852637 * t - 0.0000154757 * square(t) + 5.66661e-8 * cube(t) + 0.0338444 / x;
@@ -1077,13 +1150,13 @@ static real veh02_ntot(real n_a, real t, real rh, real x) {
              F * log(rh) * log(n_a) + G * square(log(rh)) * log(n_a) + H * square(log(n_a)) +
              I * log(rh) * square(log(n_a)) + J * cube(log(n_a)));
 }
-static real veh02_radius(real x, real ntot) {
+ORC_FN real veh02_radius(real x, real ntot) {
   return exp(-1.6524245 + 0.42316402 * x + 0.3346648 * log(ntot));
 }
 
 /* mer07_veh02_nuc_mosaic_1box with newnuc_method_flagaa = 11, nsize = 1,
  * no NH3 (mam4_amicphys.hpp:965-995); outputs qnuma_del, qso4a_del */
-static void nuc_mosaic_1box(real dtnuc, real temp_in, real rh_in, real press_in, real zm_in,
+ORC_FN void nuc_mosaic_1box(real dtnuc, real temp_in, real rh_in, real press_in, real zm_in,
                             real pblh_in, real qh2so4_cur, real qh2so4_avg,
                             real h2so4_uptkrate, real mw_so4a_host, real dp_lo, real dp_hi,
                             real rgas, real avogad, real mw_nh4a, real mw_so4a,
@@ -1217,7 +1290,7 @@ static void nuc_mosaic_1box(real dtnuc, real temp_in, real rh_in, real press_in,
 }
 
 /* mam4_amicphys.hpp:917-1094 */
-static void newnuc_1subarea(real deltat, real temp, real pmid, real zmid, real pblh,
+ORC_FN void newnuc_1subarea(real deltat, real temp, real pmid, real zmid, real pblh,
                             real relhum, real uptkrate_h2so4, real qgas_cur[NGAS],
                             const real qgas_avg[NGAS], real qnum_cur[NMODE],
                             real qaer_cur[NAER][NMODE]) {
@@ -1270,7 +1343,7 @@ static void newnuc_1subarea(real deltat, real temp, real pmid, real zmid, real p
 
 /* ---------------------------------------------------------- coagulation
  * coagulation.hpp:298-817, 850-1119 */
-static void getcoags_wrapper(real airtemp, real airprs, real dgatk, real dgacc, real sgatk,
+ORC_FN void getcoags_wrapper(real airtemp, real airprs, real dgatk, real dgacc, real sgatk,
                              real sgacc, real xxlsgat, real xxlsgac, real pdensat,
                              real pdensac, real *betaij0, real *betaij3, real *betaii0,
                              real *betajj0) {
@@ -1354,7 +1427,7 @@ static void getcoags_wrapper(real airtemp, real airprs, real dgatk, real dgacc, 
   *betaij3 = rmax(0.0, qv12 / dumatk3);
 }
 
-static void qnum_intra_inter(real bijdtqnumj, real biidt, real qnumi_bgn, real *qnumi_end) {
+ORC_FN void qnum_intra_inter(real bijdtqnumj, real biidt, real qnumi_bgn, real *qnumi_end) {
   if (bijdtqnumj < 1.0e-5) {
     *qnumi_end = qnumi_bgn / (1.0 + (bijdtqnumj + biidt * qnumi_bgn) * (1.0 + 0.5 * bijdtqnumj));
   } else {
@@ -1364,7 +1437,7 @@ static void qnum_intra_inter(real bijdtqnumj, real biidt, real qnumi_bgn, real *
   }
 }
 
-static void coag_1subarea(real deltat, real temp, real pmid, real aircon,
+ORC_FN void coag_1subarea(real deltat, real temp, real pmid, real aircon,
                           const real dgn_awet[NMODE], const real wetdens[NMODE],
                           real qnum_cur[NMODE], real qaer_cur[NAER][NMODE],
                           real qaer_del_coag_out[NAER]) {
@@ -1445,7 +1518,7 @@ static void coag_1subarea(real deltat, real temp, real pmid, real aircon,
 
 /* ------------------------------------------------------------------ aging
  * aging.hpp:70-361 */
-static void pcarbon_aging_1subarea(unsigned n_so4_monolayers, const real dgn_a[NMODE],
+ORC_FN void pcarbon_aging_1subarea(unsigned n_so4_monolayers, const real dgn_a[NMODE],
                                    real qnum_cur[NMODE], real qnum_del_cond[NMODE],
                                    real qnum_del_coag[NMODE], real qaer_cur[NAER][NMODE],
                                    real qaer_del_cond[NAER][NMODE],
@@ -1477,8 +1550,8 @@ static void pcarbon_aging_1subarea(unsigned n_so4_monolayers, const real dgn_a[N
     xferfrac = xferfrac_max;
   else
     xferfrac = rmin(tmp1 / tmp2, xferfrac_max);
-  static const int to_acc[3] = {2, 3, 6};     /* POM, BC, MOM */
-  static const int all_to_acc[4] = {0, 1, 4, 5}; /* SOA, SO4, NaCl, DST */
+  const int to_acc[3] = {2, 3, 6};     /* POM, BC, MOM */
+  const int all_to_acc[4] = {0, 1, 4, 5}; /* SOA, SO4, NaCl, DST */
   for (int k = 0; k < 3; ++k) {
     const int s = to_acc[k];
     const real q = qaer_cur[s][pc] * xferfrac;
@@ -1515,7 +1588,7 @@ typedef struct {
   int do_cond, do_rename, do_newnuc, do_coag, optaa;
 } sub_flags;
 
-static int amicphys_1subarea(const sub_flags *f, real deltat, int iscldy, unsigned nmono,
+ORC_FN int amicphys_1subarea(const sub_flags *f, real deltat, int iscldy, unsigned nmono,
                              real temp, real pmid, real zmid, real pblh, real relhum,
                              const real dgn_a[NMODE], const real dgn_awet[NMODE],
                              const real wetdens[NMODE], const real qgas1[NGAS],
@@ -1671,7 +1744,7 @@ static int amicphys_1subarea(const sub_flags *f, real deltat, int iscldy, unsign
 
 /* ------------------------------------------------------ subarea set-up
  * mam4_amicphys.hpp:242-911 */
-static void get_partition_factors(real q_i, real q_c, real fcldy, real fclea, real *fac_clea,
+ORC_FN void get_partition_factors(real q_i, real q_c, real fcldy, real fclea, real *fac_clea,
                                   real *fac_cldy) {
   const real cldbrn_cldy = q_c / fcldy;
   const real intrst_cldy = rmax(0, ((q_i + q_c) - cldbrn_cldy));
@@ -1685,7 +1758,7 @@ static void get_partition_factors(real q_i, real q_c, real fcldy, real fclea, re
 
 typedef real qsub_t[PCNST][NSUB];
 
-static void set_subarea_intrst(int jclea, int jcldy, real fclea, real fcldy, const real *qgcm,
+ORC_FN void set_subarea_intrst(int jclea, int jcldy, real fclea, real fcldy, const real *qgcm,
                                const real *qqcwgcm, const real *qgcmx, qsub_t qsubx) {
   for (int m = 0; m < NMODE; ++m) {
     real fc, fy;
@@ -1710,7 +1783,7 @@ static void set_subarea_intrst(int jclea, int jcldy, real fclea, real fcldy, con
   }
 }
 
-static void set_subarea_cldbrn(int jclea, int jcldy, real fcldy, const real *qqcwgcm,
+ORC_FN void set_subarea_cldbrn(int jclea, int jcldy, real fcldy, const real *qqcwgcm,
                                qsub_t qqcwsub) {
   for (int m = 0; m < NMODE; ++m) {
     const int ic = NUMPTR31[m];
@@ -1726,7 +1799,7 @@ static void set_subarea_cldbrn(int jclea, int jcldy, real fcldy, const real *qqc
 }
 
 /* modal_aero_amicphys_intr (mam4_amicphys.hpp:2120-2376) for one cell */
-static int amicphys_intr(const mam4b_config *cfg, real deltat, real temp, real pmid, real zm,
+ORC_FN int amicphys_intr(const mam4b_config *cfg, real deltat, real temp, real pmid, real zm,
                          real pblh, real qv, real cld, real qq[PCNST], real qqcw[PCNST],
                          const real q_pregaschem[PCNST], const real q_precldchem[PCNST],
                          const real qqcw_precldchem[PCNST], const real dgncur_a[NMODE],
@@ -1993,6 +2066,7 @@ static int amicphys_intr(const mam4b_config *cfg, real deltat, real temp, real p
 }
 
 /* ============================================================ full step */
+#ifndef ORACLE_GPU
 static const calcsize_data *cdata(void) {
   static calcsize_data d;
   static int init = 0;
@@ -2002,19 +2076,22 @@ static const calcsize_data *cdata(void) {
   }
   return &d;
 }
+#endif
 
-static real to_vmr(int i31) {
+ORC_FN real to_vmr(int i31) {
   const int num = (i31 == 13 || i31 == 18 || i31 == 26 || i31 == 30);
   return num ? 28.966 : 28.966 / ADV_MASS[i31];
 }
-static real to_mmr(int i31) {
+ORC_FN real to_mmr(int i31) {
   const int num = (i31 == 13 || i31 == 18 || i31 == 26 || i31 == 30);
   return num ? 1.0 / 28.966 : ADV_MASS[i31] / 28.966;
 }
 
-static int step_cell(const double *in, size_t ld, size_t c, double pblh, double *out, size_t ldo,
-                     double *diag, size_t ldd, double dt, const mam4b_config *cfg) {
+ORC_FN int step_cell(const calcsize_data *cd, const double *in, size_t ld, size_t c, double pblh,
+                     double *out, size_t ldo, double *diag, size_t ldd, double dt,
+                     const mam4b_config *cfg) {
 #define IN(f) in[(size_t)(f) * ld + c]
+  NOISE_SEED_CELL(c);
   real state_q[40] = {0}, qqcw[40] = {0};
   state_q[0] = IN(MAM4B_IN_QV);
   state_q[11] = IN(MAM4B_IN_H2SO4);
@@ -2025,7 +2102,7 @@ static int step_cell(const double *in, size_t ld, size_t c, double pblh, double 
   }
   const real temp = IN(MAM4B_IN_T), pmid = IN(MAM4B_IN_P), cld = IN(MAM4B_IN_CLD);
   real dgncur_a[NMODE], dgncur_c[NMODE], ptend[40] = {0}, dqqcwdt[40] = {0};
-  calcsize_sub(cdata(), state_q, qqcw, dt, dgncur_a, dgncur_c, ptend, dqqcwdt);
+  calcsize_sub(cd, state_q, qqcw, dt, dgncur_a, dgncur_c, ptend, dqqcwdt);
   real dgncur_awet[NMODE], qaerwat[NMODE], wetdens[NMODE];
   water_uptake_dr(state_q, temp, pmid, cld, dgncur_a, dgncur_awet, qaerwat, wetdens);
   for (int i = 15; i < 40; ++i) {
@@ -2068,6 +2145,7 @@ static int step_cell(const double *in, size_t ld, size_t c, double pblh, double 
 }
 
 /* ============================================================== C entries */
+#ifndef ORACLE_GPU
 int mam4orc_step(int ncell, const double *in, size_t ld_in, const double *pblh_cell,
                  double *out, size_t ld_out, double *diag, size_t ld_diag, double dt,
                  const mam4b_config *cfg, int nthreads) {
@@ -2081,7 +2159,7 @@ int mam4orc_step(int ncell, const double *in, size_t ld_in, const double *pblh_c
   (void)nthreads;
 #endif
   for (int c = 0; c < ncell; ++c)
-    step_cell(in, ld_in, (size_t)c, pblh_cell[c], out, ld_out, diag, ld_diag, dt, cfg);
+    step_cell(cdata(), in, ld_in, (size_t)c, pblh_cell[c], out, ld_out, diag, ld_diag, dt, cfg);
   return MAM4B_OK;
 }
 
@@ -2095,7 +2173,7 @@ void mam4orc_soa_niter(int ncell, const double *in, size_t ld_in, const double *
   (void)nthreads;
 #endif
   for (int c = 0; c < ncell; ++c)
-    niter[c] = step_cell(in, ld_in, (size_t)c, pblh_cell[c], NULL, 0, NULL, 0, dt, cfg);
+    niter[c] = step_cell(cdata(), in, ld_in, (size_t)c, pblh_cell[c], NULL, 0, NULL, 0, dt, cfg);
 }
 
 void mam4orc_calcsize(int ncell, const double *state_q, const double *qqcw, double dt,
@@ -2146,3 +2224,4 @@ void mam4orc_aging(unsigned n_so4_monolayers_pcage, const double *dgn_a, double 
                          (real(*)[NMODE])qaer_cur, (real(*)[NMODE])qaer_del_cond,
                          (real(*)[NMODE])qaer_del_coag, qaer_del_coag_in);
 }
+#endif /* !ORACLE_GPU */

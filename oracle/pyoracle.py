@@ -17,6 +17,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_SO = os.path.join(HERE, "_ref", "libmam4ref.so")
 PORT_SO = os.path.join(HERE, "libmam4oracle.so")
+ULP_SO = os.path.join(HERE, "libmam4oracle_ulp.so")
+GPU_SO = os.path.join(HERE, "libmam4oracle_gpu.so")
 
 NIN, NOUT, NDIAG = 57, 68, 155
 
@@ -159,5 +161,120 @@ class PortOracle(_Oracle):
         return it
 
 
+class UlpOracle(PortOracle):
+    """The restatement with every libm result moved by 1..2 ulps (1..5 for
+    erfc), drawn per call from a stream seeded by (seed, cell)."""
+    path = ULP_SO
+
+    def __init__(self, seed=1):
+        super().__init__()
+        self.lib.mam4orc_set_ulp_noise.argtypes = [ctypes.c_ulonglong]
+        self.lib.mam4orc_set_ulp_noise(int(seed))
+
+    def reseed(self, seed):
+        self.lib.mam4orc_set_ulp_noise(int(seed))
+
+
+class GpuOracle:
+    """The restatement compiled for the GPU (CUDA libm, no FMA contraction):
+    differs from the host build only through the math library."""
+
+    def __init__(self):
+        if not os.path.exists(GPU_SO):
+            raise FileNotFoundError(GPU_SO)
+        self.lib = ctypes.CDLL(GPU_SO)
+        self.lib.mam4orcgpu_step.argtypes = [_I, _P, _S, _P, _P, _S, _P, _S, _D, ctypes.POINTER(Config)]
+        self.lib.mam4orcgpu_step.restype = _I
+
+    def step(self, in_slab, pblh_cell, dt, cfg=None, diag=False):
+        x = np.ascontiguousarray(in_slab, dtype=np.float64)
+        n = x.shape[1]
+        pb = np.ascontiguousarray(pblh_cell, dtype=np.float64)
+        out = np.zeros((NOUT, n))
+        dg = np.zeros((NDIAG, n)) if diag else None
+        cfg = cfg or default_config()
+        rc = self.lib.mam4orcgpu_step(n, _ptr(x), n, _ptr(pb), _ptr(out), n, _ptr(dg), n, dt,
+                                      ctypes.byref(cfg))
+        if rc != 0:
+            raise RuntimeError("GPU oracle failed: %d" % rc)
+        return (out, dg) if diag else out
+
+
 def reference_available():
     return os.path.exists(REF_SO)
+
+
+# ----------------------------------------------------------------------
+# Parity against the oracle
+# ----------------------------------------------------------------------
+TOL = 1e-12        # north-star tolerance, state-relative
+QUANTILES = (0.5, 0.9, 0.99, 0.999)
+
+
+def state_rel_err(tend_a, tend_b, in_slab, dt):
+    """|a - b| * dt / max(|q_before|, |q_after|, 1e-30): the error of a
+    tendency in units of the state it changes (shapes (52, n))."""
+    q0 = np.abs(in_slab[5:57])
+    q1 = np.abs(in_slab[5:57] + tend_b * dt)
+    return np.abs(tend_a - tend_b) * dt / np.maximum(np.maximum(q0, q1), 1e-30)
+
+
+def output_errors(out, ref, in_slab, dt):
+    """(68, n) errors: tendencies state-relative, the 16 size/density/water
+    outputs relative."""
+    e_t = state_rel_err(out[:52], ref[:52], in_slab, dt)
+    e_d = np.abs(out[52:] - ref[52:]) / np.maximum(np.abs(ref[52:]), 1e-300)
+    return np.concatenate([e_t, e_d], axis=0)
+
+
+def libm_spread_baseline(in_slab, pblh_cell, dt, ref_out, cfg=None, seeds=(1, 2)):
+    """What the reference algorithm does to itself under a different libm:
+    per-cell error statistics of the oracle whose libm results are moved by
+    1..2 ulps (1..5 for erfc), against the canonical oracle."""
+    u = UlpOracle(seeds[0])
+    fracs, qs, maxes = [], [], []
+    for sd in seeds:
+        u.reseed(sd)
+        ec = output_errors(u.step(in_slab, pblh_cell, dt, cfg=cfg), ref_out, in_slab, dt).max(axis=0)
+        fracs.append(float((ec <= TOL).mean()))
+        qs.append(np.quantile(ec, QUANTILES))
+        maxes.append(float(ec.max()))
+    u.reseed(0)
+    return {"frac_within_tol": min(fracs), "quantiles": np.max(qs, axis=0), "max": max(maxes)}
+
+
+def parity(candidate, ref_out, in_slab, pblh_cell, dt, cfg=None, tol=TOL):
+    """Statistical parity of a candidate (the CUDA step) with the canonical
+    oracle when the two differ only through their math libraries.
+
+    The reference algorithm amplifies last-bit libm differences (SOA
+    sub-stepping, the water-uptake quartic), so no libm-independent bound
+    of 1e-12 exists on every cell. The candidate must be at least as close
+    to the oracle as the oracle is to itself under 1..2-ulp libm
+    perturbations: the fraction of cells whose 68 outputs are all within
+    `tol` may fall short of that baseline by at most 0.02, each per-cell
+    error quantile (50/90/99/99.9 %) may exceed the baseline's by at most 3x
+    (and never matters below `tol`), and the largest error by at most 10x.
+    Returns a summary; raises AssertionError."""
+    err = output_errors(candidate, ref_out, in_slab, dt)
+    ec = err.max(axis=0)
+    base = libm_spread_baseline(in_slab, pblh_cell, dt, ref_out, cfg=cfg)
+    cq = np.quantile(ec, QUANTILES)
+    summary = {"cells": int(ec.size), "frac_within_tol": float((ec <= tol).mean()),
+               "baseline_frac_within_tol": base["frac_within_tol"],
+               "quantiles": [float(v) for v in cq],
+               "baseline_quantiles": [float(v) for v in base["quantiles"]],
+               "max_err": float(ec.max()), "baseline_max": base["max"]}
+    problems = []
+    if summary["frac_within_tol"] < base["frac_within_tol"] - 0.02:
+        problems.append("fraction within tol")
+    for q, c, b in zip(QUANTILES, cq, base["quantiles"]):
+        if c > max(tol, 3.0 * b):
+            problems.append("quantile %g" % q)
+    if ec.max() > max(tol, 10.0 * base["max"]):
+        problems.append("max")
+    if problems:
+        f, c = np.unravel_index(np.argmax(err), err.shape)
+        raise AssertionError("parity: %s; worst output %d cell %d (%r vs %r); %s"
+                             % (", ".join(problems), f, c, candidate[f, c], ref_out[f, c], summary))
+    return summary
