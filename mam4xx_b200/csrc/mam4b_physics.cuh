@@ -668,95 +668,129 @@ __device__ __forceinline__ void uptake_rates(const StepConsts &C, double gasdiff
   }
 }
 
-// mam_soaexch_1subarea (gasaerexch_soaexch.hpp:80-341); returns sub-steps.
-// Bounded by the reference's own limit of 1000 iterations.
-__device__ __forceinline__ int soa_exchange(double dtfull, double temp, double pmid, Sub &s,
-                                            double &qgas_avg0, const double (&uptk)[NMODE]) {
+// SOA gas-particle exchange: mam_soaexch_1subarea (gasaerexch_soaexch.hpp:
+// 80-341), semi-implicit with adaptive sub-steps dt = 0.05 / sum(k |phi|),
+// bounded by the reference's own cap of 1000 sub-steps. Split into the
+// loop state, its set-up and one sub-step so that the same arithmetic runs
+// inline or in the work-stealing solver kernel.
+struct SoaState {
+  double g;              // SOA gas (internal units)
+  double a[NMODE];       // particle SOA per mode
+  double opoa[NMODE];    // oxygenated POA per mode (0.1 x POM; 0 for pca)
+  double uptk[NMODE];    // SOAG uptake rate per mode [1/s]
+  double g0;             // equilibrium SOA gas without solute effect
+  double tcur, dtfull;
+  int niter;
+};
+
+__device__ __forceinline__ void soa_init(SoaState &st, double dtfull, double temp, double pmid,
+                                         const Sub &s, const double (&uptk)[NMODE]) {
   const double p0_soa = 1.0e-10 * exp(-(156.0e3 / 8.3144) * ((1.0 / temp) - (1.0 / 298.0)));
-  const double g0_soa = 1.01325e5 * p0_soa / pmid;
+  st.g0 = 1.01325e5 * p0_soa / pmid;
   constexpr double opoa_frac[NMODE] = {0.1, 0.1, 0.1, 0.0};
+  st.g = s.gas[0];
+#pragma unroll
+  for (int n = 0; n < NMODE; ++n) {
+    st.a[n] = s.aer[0][n];
+    st.uptk[n] = uptk[n];
+    st.opoa[n] = 0.0 + opoa_frac[n] * dmax(s.aer[2][n], 0.0);
+  }
+  st.tcur = 0.0;
+  st.dtfull = dtfull;
+  st.niter = 0;
+}
+
+// One pass of the reference's while loop; false once the loop has ended.
+__device__ __forceinline__ bool soa_step(SoaState &st) {
+  if (!(st.tcur < st.dtfull - 1.0e-3))
+    return false;
+  st.niter++;
+  if (st.niter > 1000)
+    return false;
+  const double qgas_prv = st.g;
+  double g_soa = dmax(qgas_prv, 0.0);
+  double tot_soa = g_soa;
+  double a_soa[NMODE], sat[NMODE], g_star[NMODE], beta[NMODE];
   bool skip[NMODE];
 #pragma unroll
-  for (int n = 0; n < NMODE; ++n)
-    skip[n] = !(uptk[n] > 1.0e-15);
-  double a_soa[NMODE] = {0.0, 0.0, 0.0, 0.0};
-  double tcur = 0.0, dtsum = 0.0, avg = 0.0;
-  int niter = 0;
-  while (tcur < dtfull - 1.0e-3) {
-    niter++;
-    if (niter > 1000)
-      break;
-    const double qgas_prv = s.gas[0];
-    double g_soa = dmax(qgas_prv, 0.0);
-    double tot_soa = g_soa;
-    double a_opoa[NMODE], sat[NMODE], g_star[NMODE], beta[NMODE];
-#pragma unroll
-    for (int n = 0; n < NMODE; ++n) {
-      if (skip[n])
-        continue;
-      a_soa[n] = dmax(s.aer[0][n], 0.0);
-      tot_soa += a_soa[n];
-    }
-    double tmpb = 0.0;
-#pragma unroll
-    for (int n = 0; n < NMODE; ++n) {
-      if (skip[n])
-        continue;
-      a_opoa[n] = 0.0 + opoa_frac[n] * dmax(s.aer[2][n], 0.0);
-      const double a_ooa = a_opoa[n] + a_soa[n];
-      sat[n] = g0_soa / dmax(a_ooa, 1.0e-20);
-      g_star[n] = sat[n] * a_soa[n];
-      const double phi = (g_soa - g_star[n]) / dmax(g_soa, dmax(g_star[n], 1.0e-20));
-      tmpb += uptk[n] * fabs(phi);
-    }
-    const double tmpa = dmax(0.0, tmpb);
-    double dtcur;
-    const double dtmax = dtfull - tcur;
-    if (dtmax * tmpa <= 0.05) {
-      dtcur = dtmax;
-      tcur = dtfull;
-    } else {
-      dtcur = 0.05 / tmpa;
-      tcur += dtcur;
-    }
-#pragma unroll
-    for (int n = 0; n < NMODE; ++n) {
-      if (skip[n])
-        continue;
-      double a_tmp = a_soa[n];
-      beta[n] = dtcur * uptk[n];
-      const double del_g = g_soa - g_star[n];
-      if (del_g > 0.0) {
-        a_tmp += beta[n] * del_g;
-        const double a_ooa = a_opoa[n] + a_tmp;
-        sat[n] = g0_soa / dmax(a_ooa, 1.0e-20);
-      }
-    }
-    double ta = 0.0, tb = 0.0;
-#pragma unroll
-    for (int n = 0; n < NMODE; ++n) {
-      if (skip[n])
-        continue;
-      ta += a_soa[n] / (1.0 + beta[n] * sat[n]);
-      tb += beta[n] / (1.0 + beta[n] * sat[n]);
-    }
-    g_soa = (tot_soa - ta) / (1.0 + tb);
-    g_soa = dmax(0.0, g_soa);
-#pragma unroll
-    for (int n = 0; n < NMODE; ++n) {
-      if (skip[n])
-        continue;
-      a_soa[n] = (a_soa[n] + beta[n] * g_soa) / (1.0 + beta[n] * sat[n]);
-    }
-    s.gas[0] = g_soa;
-    avg += dtcur * (qgas_prv + 0.5 * (g_soa - qgas_prv));
-#pragma unroll
-    for (int n = 0; n < NMODE; ++n)
-      s.aer[0][n] = a_soa[n];
-    dtsum += dtcur;
+  for (int n = 0; n < NMODE; ++n) {
+    skip[n] = !(st.uptk[n] > 1.0e-15);
+    a_soa[n] = 0.0;
+    if (skip[n])
+      continue;
+    a_soa[n] = dmax(st.a[n], 0.0);
+    tot_soa += a_soa[n];
   }
-  qgas_avg0 = dmax(0.0, avg / dtsum);
-  return niter;
+  double tmpb = 0.0;
+#pragma unroll
+  for (int n = 0; n < NMODE; ++n) {
+    if (skip[n])
+      continue;
+    const double a_ooa = st.opoa[n] + a_soa[n];
+    sat[n] = st.g0 / dmax(a_ooa, 1.0e-20);
+    g_star[n] = sat[n] * a_soa[n];
+    const double phi = (g_soa - g_star[n]) / dmax(g_soa, dmax(g_star[n], 1.0e-20));
+    tmpb += st.uptk[n] * fabs(phi);
+  }
+  const double tmpa = dmax(0.0, tmpb);
+  double dtcur;
+  const double dtmax = st.dtfull - st.tcur;
+  if (dtmax * tmpa <= 0.05) {
+    dtcur = dtmax;
+    st.tcur = st.dtfull;
+  } else {
+    dtcur = 0.05 / tmpa;
+    st.tcur += dtcur;
+  }
+#pragma unroll
+  for (int n = 0; n < NMODE; ++n) {
+    if (skip[n])
+      continue;
+    double a_tmp = a_soa[n];
+    beta[n] = dtcur * st.uptk[n];
+    const double del_g = g_soa - g_star[n];
+    if (del_g > 0.0) {
+      a_tmp += beta[n] * del_g;
+      const double a_ooa = st.opoa[n] + a_tmp;
+      sat[n] = st.g0 / dmax(a_ooa, 1.0e-20);
+    }
+  }
+  double ta = 0.0, tb = 0.0;
+#pragma unroll
+  for (int n = 0; n < NMODE; ++n) {
+    if (skip[n])
+      continue;
+    ta += a_soa[n] / (1.0 + beta[n] * sat[n]);
+    tb += beta[n] / (1.0 + beta[n] * sat[n]);
+  }
+  g_soa = (tot_soa - ta) / (1.0 + tb);
+  g_soa = dmax(0.0, g_soa);
+#pragma unroll
+  for (int n = 0; n < NMODE; ++n) {
+    if (skip[n])
+      continue;
+    a_soa[n] = (a_soa[n] + beta[n] * g_soa) / (1.0 + beta[n] * sat[n]);
+  }
+  st.g = g_soa;
+#pragma unroll
+  for (int n = 0; n < NMODE; ++n)
+    st.a[n] = a_soa[n];
+  return true;
+}
+
+// Inline form: runs the whole loop for one subarea; returns the sub-step
+// count (1001 when the cap was reached).
+__device__ __forceinline__ int soa_exchange(double dtfull, double temp, double pmid, Sub &s,
+                                            const double (&uptk)[NMODE]) {
+  SoaState st;
+  soa_init(st, dtfull, temp, pmid, s, uptk);
+  while (soa_step(st)) {
+  }
+  s.gas[0] = st.g;
+#pragma unroll
+  for (int n = 0; n < NMODE; ++n)
+    s.aer[0][n] = st.a[n];
+  return st.niter;
 }
 
 // H2SO4 quasi-analytic update (gasaerexch.hpp:486-537)

@@ -39,7 +39,20 @@ struct StepArgs {
   double dt;
   int do_cond, do_rename, do_newnuc, do_coag, optaa;
   unsigned nmono;
+  // SOA solver hand-off (see soa_kernel): per-cell loop state, the list of
+  // queued cells and two counters (queued, handed out)
+  double *soa;       // [SOA_FIELDS][ncell]
+  int *task;         // [ncell]
+  unsigned *counters;
 };
+
+// Phases of the step. PRE runs each cell up to the SOA condensation loop
+// (cells without one finish here) and queues the rest; soa_kernel runs the
+// queued loops with per-lane work stealing; POST recomputes the queued
+// cells' (deterministic) prefix, takes the loop result and finishes them.
+enum { PHASE_FULL = 0, PHASE_PRE = 1, PHASE_POST = 2 };
+enum { SOA_G = 0, SOA_A = 1, SOA_OPOA = 5, SOA_UPTK = 9, SOA_G0 = 13, SOA_FIELDS = 14 };
+constexpr int kDeferred = -1;
 
 // ----------------------------------------------------- per-cell amicphys
 struct Diag {
@@ -57,8 +70,9 @@ __device__ __forceinline__ int num_i31(int m) { return m == 0 ? 13 : m == 1 ? 18
 // aging (mam_amicphys_1subarea, mam4_amicphys.hpp:1127-1697). `s` holds the
 // subarea's incoming values and returns the outgoing ones. With DIAG the
 // per-process increments are added to dg scaled by afrac/(fcvt*deltat).
-template <bool DIAG>
-__device__ __forceinline__ int clear_subarea(const StepArgs &a, double deltat, double temp,
+template <bool DIAG, int PHASE>
+__device__ __forceinline__ int clear_subarea(const StepArgs &a, long long cell, double deltat,
+                                             double temp,
                                              double pmid, double zmid, double pblh,
                                              double relhum, const double (&dgn_a)[NMODE],
                                              const double (&dgn_awet)[NMODE],
@@ -132,8 +146,40 @@ __device__ __forceinline__ int clear_subarea(const StepArgs &a, double deltat, d
 #pragma unroll
     for (int n = 0; n < NMODE; ++n)
       uptkrate_h2so4 += uptk1[n];
-    double avg0;
-    niter = soa_exchange(dtsub, temp, pmid, s, avg0, uptk0);
+    if (PHASE == PHASE_FULL) {
+      niter = soa_exchange(dtsub, temp, pmid, s, uptk0);
+    } else if (PHASE == PHASE_PRE) {
+      // hand the loop to the solver kernel and stop here
+      SoaState st;
+      soa_init(st, dtsub, temp, pmid, s, uptk0);
+      const size_t n = (size_t)a.ncell;
+      double *q = a.soa + (size_t)cell;
+      q[SOA_G * n] = st.g;
+#pragma unroll
+      for (int k = 0; k < NMODE; ++k) {
+        q[(SOA_A + k) * n] = st.a[k];
+        q[(SOA_OPOA + k) * n] = st.opoa[k];
+        q[(SOA_UPTK + k) * n] = st.uptk[k];
+      }
+      q[SOA_G0 * n] = st.g0;
+      // warp-aggregated append to the task list
+      const unsigned m = __activemask();
+      const int lane = threadIdx.x & 31;
+      const int leader = __ffs(m) - 1;
+      unsigned base = 0;
+      if (lane == leader)
+        base = atomicAdd(&a.counters[0], (unsigned)__popc(m));
+      base = __shfl_sync(m, base, leader);
+      a.task[base + __popc(m & ((1u << lane) - 1))] = (int)cell;
+      return kDeferred;
+    } else {
+      const size_t n = (size_t)a.ncell;
+      const double *q = a.soa + (size_t)cell;
+      s.gas[0] = q[SOA_G * n];
+#pragma unroll
+      for (int k = 0; k < NMODE; ++k)
+        s.aer[0][k] = q[(SOA_A + k) * n];
+    }
     h2so4_update(dtsub, netprod1, s, uptk1, qgas_avg1);
 #pragma unroll
     for (int x = 0; x < NAER; ++x)
@@ -268,11 +314,8 @@ __device__ __forceinline__ int clear_subarea(const StepArgs &a, double deltat, d
   return niter;
 }
 
-template <bool DIAG>
-__global__ void __launch_bounds__(128) step_kernel(const __grid_constant__ StepArgs a) {
-  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= a.ncell)
-    return;
+template <bool DIAG, int PHASE>
+__device__ __forceinline__ void cell_step(const StepArgs &a, const long long c) {
   const StepConsts &C = c_k;
   const double temp = __ldg(a.in[MAM4B_IN_T] + c);
   const double pmid = __ldg(a.in[MAM4B_IN_P] + c);
@@ -289,7 +332,7 @@ __global__ void __launch_bounds__(128) step_kernel(const __grid_constant__ StepA
     ai[p] = __ldg(a.in[MAM4B_IN_AER_I + p] + c);
     ac[p] = __ldg(a.in[MAM4B_IN_AER_C + p] + c);
   }
-  {
+  if (PHASE != PHASE_POST) {
     double chk = temp + pmid + zm + qv + cld + h2so4 + soag + pblh;
 #pragma unroll
     for (int p = 0; p < NPOP; ++p)
@@ -375,8 +418,10 @@ __global__ void __launch_bounds__(128) step_kernel(const __grid_constant__ StepA
     s.gas[0] = g_soag * fsoag;
     s.gas[1] = g_h2so4 * 1.0;
     const double qgas1[2] = {s.gas[0], s.gas[1]};
-    const int niter = clear_subarea<DIAG>(a, dt, temp, pmid, zm, pblh, relhumgcm, dgn_a,
-                                          dgn_awet, wetdens, qgas1, s, dg, 1.0);
+    const int niter = clear_subarea<DIAG, PHASE>(a, c, dt, temp, pmid, zm, pblh, relhumgcm,
+                                                 dgn_a, dgn_awet, wetdens, qgas1, s, dg, 1.0);
+    if (niter == kDeferred)
+      return;
     if (niter > 1000)
       atomicOr(a.flags, MAM4B_FLAG_SOA_NITER_LIMIT);
     const double f = 1.0 - 0.0;
@@ -506,8 +551,10 @@ __global__ void __launch_bounds__(128) step_kernel(const __grid_constant__ StepA
       s.gas[1] = gcl[1] * 1.0;
       const double qgas1[2] = {g_soag * fsoag, g_h2so4 * 1.0};
       const double rhc = bound(0.0, 1.0, (relhumgcm - fcldy) / fclea);
-      const int niter = clear_subarea<DIAG>(a, dt, temp, pmid, zm, pblh, rhc, dgn_a, dgn_awet,
-                                            wetdens, qgas1, s, dg, fclea);
+      const int niter = clear_subarea<DIAG, PHASE>(a, c, dt, temp, pmid, zm, pblh, rhc, dgn_a,
+                                                   dgn_awet, wetdens, qgas1, s, dg, fclea);
+      if (niter == kDeferred)
+        return;
       if (niter > 1000)
         atomicOr(a.flags, MAM4B_FLAG_SOA_NITER_LIMIT);
       const bool map_gas = a.do_cond || a.do_newnuc;
@@ -624,6 +671,78 @@ __global__ void __launch_bounds__(128) step_kernel(const __grid_constant__ StepA
   }
 }
 
+
+template <bool DIAG>
+__global__ void __launch_bounds__(128) pre_kernel(const __grid_constant__ StepArgs a) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < a.ncell)
+    cell_step<DIAG, PHASE_PRE>(a, c);
+}
+
+template <bool DIAG>
+__global__ void __launch_bounds__(128) post_kernel(const __grid_constant__ StepArgs a) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < (long long)a.counters[0])
+    cell_step<DIAG, PHASE_POST>(a, a.task[i]);
+}
+
+// SOA sub-stepping of the queued cells. Persistent warps; every lane owns
+// one cell's loop and, as soon as that loop ends, takes the next queued
+// cell (one atomic per warp for all lanes that need work), so a warp never
+// idles behind one cell that needs hundreds of sub-steps.
+constexpr int kSoaBlock = 256;
+__global__ void __launch_bounds__(kSoaBlock) soa_kernel(const __grid_constant__ StepArgs a) {
+  const unsigned ntask = a.counters[0];
+  const int lane = threadIdx.x & 31;
+  const size_t n = (size_t)a.ncell;
+  SoaState st;
+  int cell = -1;
+  bool active = false, want = true;
+  while (true) {
+    const unsigned need = __ballot_sync(0xffffffffu, want);
+    if (need) {
+      const int leader = __ffs(need) - 1;
+      unsigned base = 0;
+      if (lane == leader)
+        base = atomicAdd(&a.counters[1], (unsigned)__popc(need));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (want) {
+        const unsigned t = base + __popc(need & ((1u << lane) - 1));
+        want = false;
+        if (t < ntask) {
+          cell = a.task[t];
+          const double *q = a.soa + (size_t)cell;
+          st.g = q[SOA_G * n];
+#pragma unroll
+          for (int k = 0; k < NMODE; ++k) {
+            st.a[k] = q[(SOA_A + k) * n];
+            st.opoa[k] = q[(SOA_OPOA + k) * n];
+            st.uptk[k] = q[(SOA_UPTK + k) * n];
+          }
+          st.g0 = q[SOA_G0 * n];
+          st.tcur = 0.0;
+          st.dtfull = (double)(int)(a.dt / 1);
+          st.niter = 0;
+          active = true;
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, active))
+      break;
+    if (active && !soa_step(st)) {
+      double *q = a.soa + (size_t)cell;
+      q[SOA_G * n] = st.g;
+#pragma unroll
+      for (int k = 0; k < NMODE; ++k)
+        q[(SOA_A + k) * n] = st.a[k];
+      if (st.niter > 1000)
+        atomicOr(a.flags, MAM4B_FLAG_SOA_NITER_LIMIT);
+      active = false;
+      want = true;
+    }
+  }
+}
+
 // ====================================================== derived constants
 // Evaluated once per device by a one-thread kernel, with the same
 // expressions the reference evaluates inline (and the same math library the
@@ -703,6 +822,12 @@ struct mam4b_ctx {
   // host-path scratch (device slabs), grown on demand
   double *d_in, *d_out, *d_pblh;
   size_t cap_in, cap_out, cap_pblh;
+  // SOA solver scratch: loop state, queued cells, counters (grown on demand)
+  double *d_soa;
+  int *d_task;
+  unsigned *d_counters;
+  size_t cap_cells;
+  int soa_grid;  // persistent solver blocks (SMs x resident blocks)
 };
 
 namespace {
@@ -742,6 +867,35 @@ cudaError_t ensure_consts(int dev) {
 
 bool valid_config(const mam4b_config *c) {
   return c && (c->gaexch_h2so4_uptake_optaa == 1 || c->gaexch_h2so4_uptake_optaa == 2);
+}
+
+cudaError_t ensure_solver_scratch(mam4b_ctx *ctx, size_t ncell) {
+  cudaError_t e = cudaSuccess;
+  if (!ctx->d_counters)
+    e = cudaMalloc(&ctx->d_counters, 2 * sizeof(unsigned));
+  if (e == cudaSuccess && ctx->soa_grid == 0) {
+    int dev = 0, sms = 0, per_sm = 0;
+    e = cudaGetDevice(&dev);
+    if (e == cudaSuccess)
+      e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, soa_kernel, kSoaBlock, 0);
+    if (e == cudaSuccess)
+      ctx->soa_grid = sms * (per_sm > 0 ? per_sm : 1);
+  }
+  if (e != cudaSuccess || ctx->cap_cells >= ncell)
+    return e;
+  cudaFree(ctx->d_soa);
+  cudaFree(ctx->d_task);
+  ctx->d_soa = nullptr;
+  ctx->d_task = nullptr;
+  ctx->cap_cells = 0;
+  e = cudaMalloc(&ctx->d_soa, (size_t)SOA_FIELDS * ncell * sizeof(double));
+  if (e == cudaSuccess)
+    e = cudaMalloc(&ctx->d_task, ncell * sizeof(int));
+  if (e == cudaSuccess)
+    ctx->cap_cells = ncell;
+  return e;
 }
 }  // namespace
 
@@ -801,6 +955,9 @@ mam4b_status mam4b_destroy(mam4b_ctx *ctx) {
   cudaFree(ctx->d_in);
   cudaFree(ctx->d_out);
   cudaFree(ctx->d_pblh);
+  cudaFree(ctx->d_soa);
+  cudaFree(ctx->d_task);
+  cudaFree(ctx->d_counters);
   delete ctx;
   return MAM4B_OK;
 }
@@ -847,16 +1004,30 @@ mam4b_status mam4b_step(mam4b_ctx *ctx, const mam4b_state_view *in, const mam4b_
     return MAM4B_OK;
   const int block = 128;
   const long long grid = (a.ncell + block - 1) / block;
-  if (grid > 0x7fffffffLL)
+  if (a.ncell > 0x7fffffffLL)
     return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_step: too many cells", cudaSuccess);
+  cudaError_t e = ensure_solver_scratch(ctx, (size_t)a.ncell);
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_step scratch", e);
+  a.soa = ctx->d_soa;
+  a.task = ctx->d_task;
+  a.counters = ctx->d_counters;
+  e = cudaMemsetAsync(ctx->d_counters, 0, 2 * sizeof(unsigned), s);
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_step counters", e);
   if (diag)
-    step_kernel<true><<<(unsigned)grid, block, 0, s>>>(a);
+    pre_kernel<true><<<(unsigned)grid, block, 0, s>>>(a);
   else
-    step_kernel<false><<<(unsigned)grid, block, 0, s>>>(a);
-  cudaError_t e = cudaGetLastError();
+    pre_kernel<false><<<(unsigned)grid, block, 0, s>>>(a);
+  soa_kernel<<<ctx->soa_grid, kSoaBlock, 0, s>>>(a);
+  if (diag)
+    post_kernel<true><<<(unsigned)grid, block, 0, s>>>(a);
+  else
+    post_kernel<false><<<(unsigned)grid, block, 0, s>>>(a);
+  e = cudaGetLastError();
   if (e != cudaSuccess)
     return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_step launch", e);
-  ctx->launches++;
+  ctx->launches += 3;
   return MAM4B_OK;
 }
 
