@@ -41,18 +41,21 @@ struct StepArgs {
   unsigned nmono;
   // SOA solver hand-off (see soa_kernel): per-cell loop state, the list of
   // queued cells and two counters (queued, handed out)
-  double *soa;       // [SOA_FIELDS][ncell]
-  int *task;         // [ncell]
+  double *soa;       // [SOA_FIELDS][ncell], indexed by queue slot
+  double *hand;      // [H_FIELDS][ncell], indexed by queue slot
+  int *task;         // [ncell]: cell of each queue slot
   unsigned *counters;
 };
 
-// Phases of the step. PRE runs each cell up to the SOA condensation loop
-// (cells without one finish here) and queues the rest; soa_kernel runs the
-// queued loops with per-lane work stealing; POST recomputes the queued
-// cells' (deterministic) prefix, takes the loop result and finishes them.
-enum { PHASE_FULL = 0, PHASE_PRE = 1, PHASE_POST = 2 };
+// Phases of the step. FULL runs each cell start to end in one thread (the
+// diagnostics path). PRE runs each cell up to the SOA condensation loop of
+// its clear subarea, writes the loop's initial state and the rest of the
+// cell's state at that point to slot-indexed scratch and queues the cell
+// (cells without the loop finish in PRE); soa_kernel runs the queued loops
+// with per-lane work stealing; post_kernel finishes the queued cells from
+// the hand-off and the loop result.
+enum { PHASE_FULL = 0, PHASE_PRE = 1 };
 enum { SOA_G = 0, SOA_A = 1, SOA_OPOA = 5, SOA_UPTK = 9, SOA_G0 = 13, SOA_FIELDS = 14 };
-constexpr int kDeferred = -1;
 
 // ----------------------------------------------------- per-cell amicphys
 struct Diag {
@@ -66,33 +69,98 @@ __device__ __forceinline__ int pop_to_i31(int p) { return 6 + p; }
 // amicphys tracer index of the number of mode m (mam4_amicphys.hpp:36)
 __device__ __forceinline__ int num_i31(int m) { return m == 0 ? 13 : m == 1 ? 18 : m == 2 ? 26 : 30; }
 
-// Clear-subarea sequence: condensation, renaming, nucleation, coagulation,
-// aging (mam_amicphys_1subarea, mam4_amicphys.hpp:1127-1697). `s` holds the
-// subarea's incoming values and returns the outgoing ones. With DIAG the
-// per-process increments are added to dg scaled by afrac/(fcvt*deltat).
-template <bool DIAG, int PHASE>
-__device__ __forceinline__ int clear_subarea(const StepArgs &a, long long cell, double deltat,
-                                             double temp,
-                                             double pmid, double zmid, double pblh,
-                                             double relhum, const double (&dgn_a)[NMODE],
-                                             const double (&dgn_awet)[NMODE],
-                                             const double (&wetdens)[NMODE],
-                                             const double (&qgas1)[2], Sub &s, Diag *dg,
-                                             double afrac) {
+// Hand-off of a queued cell from the pre to the post kernel: one double per
+// field and queue slot ([field][slot], coalesced in both kernels).
+enum {
+  H_GAS1 = 0,      // H2SO4 of the clear subarea at the loop
+  H_POP = 1,       // 25 numbers/masses of the clear subarea at the loop
+  H_UPTK = 26,     // 4 H2SO4 uptake rates
+  H_NETPROD = 30,  // H2SO4 net production of other processes
+  H_SV_SO4 = 31,   // aitken SO4 and SOA before condensation
+  H_SV_SOA = 32,
+  H_DGN_PC = 33,   // dry diameter of the primary-carbon mode
+  H_AWET = 34,     // 4 wet diameters
+  H_WETD = 38,     // 4 wet densities (>= 1000)
+  H_RELHUM = 42,   // relative humidity of the clear subarea
+  H_OC = 43,       // 25 outgoing cloud-borne grid means
+  H_CI = 68,       // 25 interstitial contributions of the cloudy subarea
+  H_CG = 93,       // 2 gas contributions of the cloudy subarea (SOAG, H2SO4)
+  H_FIELDS = 95
+};
+
+// State of the clear subarea between the start of condensation and the SOA
+// loop (everything the rest of mam_amicphys_1subarea needs from before it).
+struct ClearMid {
+  double netprod1;
+  double uptk1[NMODE];
+  double sv_so4_ait, sv_soa_ait;
+  // DIAG only: values before condensation
+  double gas_sv[2];
+  double sv_all[NAER][NMODE];
+};
+
+// Clear subarea, mam_amicphys_1subarea (mam4_amicphys.hpp:1127-1697), part 1:
+// optaa-2 production split, H2SO4 diffusivity and uptake rates. Returns the
+// SOAG uptake rates for the SOA loop.
+template <bool DIAG>
+__device__ __forceinline__ void clear_prefix(const StepArgs &a, double deltat, double temp,
+                                             double pmid, const double (&dgn_awet)[NMODE],
+                                             const double (&qgas1)[2], Sub &s, ClearMid &cm,
+                                             double (&uptk0)[NMODE]) {
   const StepConsts &C = c_k;
   const double aircon = pmid / (8314.46759100000 * temp);
-  double netprod1 = 0.0;
+  cm.netprod1 = 0.0;
   if (a.do_cond && a.optaa == 2) {
-    netprod1 = (s.gas[1] - qgas1[1]) / deltat;
-    s.gas[1] = (netprod1 >= 0) ? qgas1[1] : 0;
+    cm.netprod1 = (s.gas[1] - qgas1[1]) / deltat;
+    s.gas[1] = (cm.netprod1 >= 0) ? qgas1[1] : 0;
   }
+  if (!a.do_cond)
+    return;
+  cm.gas_sv[0] = s.gas[0];
+  cm.gas_sv[1] = s.gas[1];
+  cm.sv_so4_ait = s.aer[1][1];
+  cm.sv_soa_ait = s.aer[0][1];
+  if (DIAG) {
+#pragma unroll
+    for (int x = 0; x < NAER; ++x)
+#pragma unroll
+      for (int m = 0; m < NMODE; ++m)
+        cm.sv_all[x][m] = s.aer[x][m];
+  }
+  // H2SO4 gas diffusivity / mean free path (gasaerexch.hpp:223-253, 402-417)
+  const double p_in_atm = pmid / 1.013e5;
+  const double dgas = (1.0e-3 * pow(temp, 1.75) * sqrt(1. / 9.807840000000000E+01 + 0.035)) /
+                      (p_in_atm * pow((pow(4.288000000000000E+01, 1.0 / 3.0) + 2.7189), 2.0));
+  const double gas_diffus = dgas * 1.0e-4;
+  const double speed = 145.5 * sqrt(temp / 9.807840000000000E+01);
+  const double freepath = 3.0 * gas_diffus / speed;
+  uptake_rates(C, gas_diffus, freepath, dgn_awet, cm.uptk1);
+#pragma unroll
+  for (int n = 0; n < NMODE; ++n) {
+    cm.uptk1[n] = cm.uptk1[n] * (s.num[n] * aircon);
+    uptk0[n] = cm.uptk1[n] * 0.81;
+  }
+}
+
+// Part 2, after the SOA loop: H2SO4 update, renaming, nucleation,
+// coagulation, aging. With DIAG the per-process increments are added to dg
+// scaled by afrac/(fcvt*deltat).
+template <bool DIAG>
+__device__ __forceinline__ void clear_suffix(const StepArgs &a, double deltat, double temp,
+                                             double pmid, double zmid, double pblh,
+                                             double relhum, double dgn_a_pc,
+                                             const double (&dgn_awet)[NMODE],
+                                             const double (&wetdens)[NMODE], const ClearMid &cm,
+                                             Sub &s, Diag *dg, double afrac) {
+  const StepConsts &C = c_k;
+  const double aircon = pmid / (8314.46759100000 * temp);
   const double dtsub = (double)(int)(deltat / 1);
-  int niter = 0;
   double qgas_avg1 = s.gas[1];
   double uptkrate_h2so4 = 0.0;
-  double cond_so4_pc = 0.0, cond_soa_pc = 0.0;  // condensation gain of the pc mode
+  // the primary-carbon mode holds no SO4/SOA before condensation, so its
+  // condensation gains are its values after it
+  double cond_so4_pc = 0.0, cond_soa_pc = 0.0;
   double dcond[NAER][NMODE], dcoag[NAER][NMODE], dncond[NMODE], dncoag[NMODE];
-  double gas_sv[2];
   if (DIAG) {
 #pragma unroll
     for (int x = 0; x < NAER; ++x)
@@ -112,89 +180,25 @@ __device__ __forceinline__ int clear_subarea(const StepArgs &a, long long cell, 
   for (int x = 0; x < NAER; ++x)
     grow[x] = 0.0;
 
-  // ---------------------------------------------------- condensation
   if (a.do_cond) {
-    gas_sv[0] = s.gas[0];
-    gas_sv[1] = s.gas[1];
-    double sv_ait[NAER], sv_pc_so4, sv_pc_soa;
-    double sv_all[NAER][NMODE];
-#pragma unroll
-    for (int x = 0; x < NAER; ++x) {
-      sv_ait[x] = s.aer[x][1];
-      if (DIAG) {
-#pragma unroll
-        for (int m = 0; m < NMODE; ++m)
-          sv_all[x][m] = s.aer[x][m];
-      }
-    }
-    sv_pc_so4 = s.aer[1][3];
-    sv_pc_soa = s.aer[0][3];
-    // H2SO4 gas diffusivity / mean free path (gasaerexch.hpp:223-253, 402-417)
-    const double p_in_atm = pmid / 1.013e5;
-    const double dgas = (1.0e-3 * pow(temp, 1.75) * sqrt(1. / 9.807840000000000E+01 + 0.035)) /
-                        (p_in_atm * pow((pow(4.288000000000000E+01, 1.0 / 3.0) + 2.7189), 2.0));
-    const double gas_diffus = dgas * 1.0e-4;
-    const double speed = 145.5 * sqrt(temp / 9.807840000000000E+01);
-    const double freepath = 3.0 * gas_diffus / speed;
-    double uptk1[NMODE], uptk0[NMODE];
-    uptake_rates(C, gas_diffus, freepath, dgn_awet, uptk1);
-#pragma unroll
-    for (int n = 0; n < NMODE; ++n) {
-      uptk1[n] = uptk1[n] * (s.num[n] * aircon);
-      uptk0[n] = uptk1[n] * 0.81;
-    }
 #pragma unroll
     for (int n = 0; n < NMODE; ++n)
-      uptkrate_h2so4 += uptk1[n];
-    if (PHASE == PHASE_FULL) {
-      niter = soa_exchange(dtsub, temp, pmid, s, uptk0);
-    } else if (PHASE == PHASE_PRE) {
-      // hand the loop to the solver kernel and stop here
-      SoaState st;
-      soa_init(st, dtsub, temp, pmid, s, uptk0);
-      const size_t n = (size_t)a.ncell;
-      double *q = a.soa + (size_t)cell;
-      q[SOA_G * n] = st.g;
-#pragma unroll
-      for (int k = 0; k < NMODE; ++k) {
-        q[(SOA_A + k) * n] = st.a[k];
-        q[(SOA_OPOA + k) * n] = st.opoa[k];
-        q[(SOA_UPTK + k) * n] = st.uptk[k];
-      }
-      q[SOA_G0 * n] = st.g0;
-      // warp-aggregated append to the task list
-      const unsigned m = __activemask();
-      const int lane = threadIdx.x & 31;
-      const int leader = __ffs(m) - 1;
-      unsigned base = 0;
-      if (lane == leader)
-        base = atomicAdd(&a.counters[0], (unsigned)__popc(m));
-      base = __shfl_sync(m, base, leader);
-      a.task[base + __popc(m & ((1u << lane) - 1))] = (int)cell;
-      return kDeferred;
-    } else {
-      const size_t n = (size_t)a.ncell;
-      const double *q = a.soa + (size_t)cell;
-      s.gas[0] = q[SOA_G * n];
-#pragma unroll
-      for (int k = 0; k < NMODE; ++k)
-        s.aer[0][k] = q[(SOA_A + k) * n];
-    }
-    h2so4_update(dtsub, netprod1, s, uptk1, qgas_avg1);
-#pragma unroll
-    for (int x = 0; x < NAER; ++x)
-      grow[x] = s.aer[x][1] - sv_ait[x];
-    cond_so4_pc = s.aer[1][3] - sv_pc_so4;
-    cond_soa_pc = s.aer[0][3] - sv_pc_soa;
+      uptkrate_h2so4 += cm.uptk1[n];
+    h2so4_update(dtsub, cm.netprod1, s, cm.uptk1, qgas_avg1);
+    // growth of the aitken mode by condensation: only SO4 and SOA change
+    grow[1] = s.aer[1][1] - cm.sv_so4_ait;
+    grow[0] = s.aer[0][1] - cm.sv_soa_ait;
+    cond_so4_pc = s.aer[1][3] - 0.0;
+    cond_soa_pc = s.aer[0][3] - 0.0;
     if (DIAG) {
 #pragma unroll
       for (int x = 0; x < NAER; ++x)
 #pragma unroll
         for (int m = 0; m < NMODE; ++m)
-          dcond[x][m] = s.aer[x][m] - sv_all[x][m];
+          dcond[x][m] = s.aer[x][m] - cm.sv_all[x][m];
       // gas increment of condensation (mam4_amicphys.hpp:1434-1438)
-      dg->t[0][5] += ((0.0 + (s.gas[0] - (gas_sv[0] + 0.0 * dtsub))) / (C.fcvt_soag * deltat)) * afrac;
-      dg->t[0][2] += ((0.0 + (s.gas[1] - (gas_sv[1] + netprod1 * dtsub))) / (1.0 * deltat)) * afrac;
+      dg->t[0][5] += ((0.0 + (s.gas[0] - (cm.gas_sv[0] + 0.0 * dtsub))) / (C.fcvt_soag * deltat)) * afrac;
+      dg->t[0][2] += ((0.0 + (s.gas[1] - (cm.gas_sv[1] + cm.netprod1 * dtsub))) / (1.0 * deltat)) * afrac;
     }
   }
 
@@ -215,8 +219,7 @@ __device__ __forceinline__ int clear_subarea(const StepArgs &a, long long cell, 
     if (DIAG) {
 #pragma unroll
       for (int m = 0; m < NMODE; ++m) {
-        dg->t[1][num_i31(m)] +=
-            ((0.0 + (s.num[m] - nsv[m])) / (1.0 * deltat)) * afrac;
+        dg->t[1][num_i31(m)] += ((0.0 + (s.num[m] - nsv[m])) / (1.0 * deltat)) * afrac;
 #pragma unroll
         for (int x = 0; x < NAER; ++x) {
           const int slot = K::aer_slot(x, m);
@@ -264,8 +267,7 @@ __device__ __forceinline__ int clear_subarea(const StepArgs &a, long long cell, 
       }
 #pragma unroll
       for (int m = 0; m < NMODE; ++m) {
-        dg->t[3][num_i31(m)] +=
-            ((0.0 + dncoag[m]) / (1.0 * deltat)) * afrac;
+        dg->t[3][num_i31(m)] += ((0.0 + dncoag[m]) / (1.0 * deltat)) * afrac;
 #pragma unroll
         for (int x = 0; x < NAER; ++x) {
           const int slot = K::aer_slot(x, m);
@@ -282,12 +284,11 @@ __device__ __forceinline__ int clear_subarea(const StepArgs &a, long long cell, 
 
   // ----------------------------------------------------------- aging
   if (DIAG) {
-    aging(C, a.nmono, dgn_a[3], s, dncond, dncoag, dcond, dcoag, coag_in);
+    aging(C, a.nmono, dgn_a_pc, s, dncond, dncoag, dcond, dcoag, coag_in);
 #pragma unroll
     for (int m = 0; m < NMODE; ++m) {
       if (a.do_cond)
-        dg->t[0][num_i31(m)] +=
-            ((0.0 + dncond[m]) / (1.0 * deltat)) * afrac;
+        dg->t[0][num_i31(m)] += ((0.0 + dncond[m]) / (1.0 * deltat)) * afrac;
 #pragma unroll
       for (int x = 0; x < NAER; ++x) {
         const int slot = K::aer_slot(x, m);
@@ -309,11 +310,75 @@ __device__ __forceinline__ int clear_subarea(const StepArgs &a, long long cell, 
       }
     dc[1][3] = cond_so4_pc;
     dc[0][3] = cond_soa_pc;
-    aging(C, a.nmono, dgn_a[3], s, dn_c, dn_g, dc, dq, coag_in);
+    aging(C, a.nmono, dgn_a_pc, s, dn_c, dn_g, dc, dq, coag_in);
   }
+}
+
+// Whole clear subarea in one thread: part 1, the SOA loop inline (compiled
+// in only WITH_SOA; the pre kernel queues every cell that has one), part 2.
+// Returns the SOA sub-step count.
+template <bool DIAG, bool WITH_SOA>
+__device__ __forceinline__ int clear_subarea(const StepArgs &a, double deltat, double temp,
+                                             double pmid, double zmid, double pblh,
+                                             double relhum, const double (&dgn_a)[NMODE],
+                                             const double (&dgn_awet)[NMODE],
+                                             const double (&wetdens)[NMODE],
+                                             const double (&qgas1)[2], Sub &s, Diag *dg,
+                                             double afrac) {
+  ClearMid cm;
+  double uptk0[NMODE];
+  clear_prefix<DIAG>(a, deltat, temp, pmid, dgn_awet, qgas1, s, cm, uptk0);
+  int niter = 0;
+  if (WITH_SOA && a.do_cond)
+    niter = soa_exchange((double)(int)(deltat / 1), temp, pmid, s, uptk0);
+  clear_suffix<DIAG>(a, deltat, temp, pmid, zmid, pblh, relhum, dgn_a[3], dgn_awet, wetdens, cm, s,
+                     dg, afrac);
   return niter;
 }
 
+// population slot <-> Sub (mass slots in fcvt units, numbers as is)
+__device__ __forceinline__ void sub_to_pop(const Sub &s, double (&p)[NPOP]) {
+#pragma unroll
+  for (int m = 0; m < NMODE; ++m) {
+    p[K::numslot(m)] = s.num[m];
+#pragma unroll
+    for (int x = 0; x < NAER; ++x)
+      if (K::aer_slot(x, m) >= 0)
+        p[K::aer_slot(x, m)] = s.aer[x][m];
+  }
+}
+__device__ __forceinline__ void pop_to_sub(const double (&p)[NPOP], Sub &s) {
+#pragma unroll
+  for (int m = 0; m < NMODE; ++m) {
+    s.num[m] = p[K::numslot(m)];
+#pragma unroll
+    for (int x = 0; x < NAER; ++x)
+      s.aer[x][m] = (K::aer_slot(x, m) >= 0) ? p[K::aer_slot(x, m)] : 0.0;
+  }
+}
+
+__device__ __forceinline__ void store_outputs(const StepArgs &a, long long c, double o_h2so4,
+                                              double o_soag, const double (&oi)[NPOP],
+                                              const double (&oc)[NPOP], double h2so4, double soag,
+                                              const double (&ai)[NPOP], const double (&ac)[NPOP]) {
+  const StepConsts &C = c_k;
+  const double dt = a.dt;
+  double *const *out = a.out;
+  out[MAM4B_OUT_TEND + 0][c] = (o_h2so4 * C.to_mmr[0] - h2so4) / dt;
+  out[MAM4B_OUT_TEND + 1][c] = (o_soag * C.to_mmr[1] - soag) / dt;
+#pragma unroll
+  for (int p = 0; p < NPOP; ++p) {
+    out[MAM4B_OUT_TEND + 2 + p][c] = (oi[p] * C.to_mmr[2 + p] - ai[p]) / dt;
+    out[MAM4B_OUT_TEND + 27 + p][c] = (oc[p] * C.to_mmr[2 + p] - ac[p]) / dt;
+  }
+}
+
+// One grid cell: modal_aero_calcsize_sub, modal_aero_water_uptake_dr and
+// modal_aero_amicphys_intr (mam4_amicphys.hpp:2120-2376) with
+// q_pregaschem = q_precldchem = qq and qqcw_precldchem = qqcw.
+// PHASE_FULL: all of it. PHASE_PRE: cells with a clear subarea and
+// condensation stop at the SOA loop, hand their state to the solver and the
+// post kernel, and are queued; the others finish here.
 template <bool DIAG, int PHASE>
 __device__ __forceinline__ void cell_step(const StepArgs &a, const long long c) {
   const StepConsts &C = c_k;
@@ -332,7 +397,7 @@ __device__ __forceinline__ void cell_step(const StepArgs &a, const long long c) 
     ai[p] = __ldg(a.in[MAM4B_IN_AER_I + p] + c);
     ac[p] = __ldg(a.in[MAM4B_IN_AER_C + p] + c);
   }
-  if (PHASE != PHASE_POST) {
+  {
     double chk = temp + pmid + zm + qv + cld + h2so4 + soag + pblh;
 #pragma unroll
     for (int p = 0; p < NPOP; ++p)
@@ -347,6 +412,13 @@ __device__ __forceinline__ void cell_step(const StepArgs &a, const long long c) 
   // ---------------------------------------------------- water uptake
   double dgn_awet[NMODE], qaerwat[NMODE], wetdens_wu[NMODE];
   water_uptake(C, ai, qv, temp, pmid, cld, dgn_a, dgn_awet, qaerwat, wetdens_wu);
+#pragma unroll
+  for (int m = 0; m < NMODE; ++m) {
+    a.out[MAM4B_OUT_DGN_A + m][c] = dgn_a[m];
+    a.out[MAM4B_OUT_DGN_AWET + m][c] = dgn_awet[m];
+    a.out[MAM4B_OUT_WETDENS + m][c] = wetdens_wu[m];
+    a.out[MAM4B_OUT_QAERWAT + m][c] = qaerwat[m];
+  }
 
   // calcsize tendencies applied for one step, then amicphys units
   double qi[NPOP], qc[NPOP];
@@ -359,8 +431,6 @@ __device__ __forceinline__ void cell_step(const StepArgs &a, const long long c) 
   const double g_soag = dmax(0.0, soag * C.to_vmr[1]);
 
   // -------------------------------------------------------- amicphys
-  // modal_aero_amicphys_intr (mam4_amicphys.hpp:2120-2376) with
-  // q_pregaschem = q_precldchem = qq and qqcw_precldchem = qqcw.
   double wetdens[NMODE];
 #pragma unroll
   for (int m = 0; m < NMODE; ++m)
@@ -388,6 +458,8 @@ __device__ __forceinline__ void cell_step(const StepArgs &a, const long long c) 
   // outgoing grid-cell means (amicphys units): gases, interstitial, cloud
   double o_h2so4, o_soag, oi[NPOP], oc[NPOP];
   const double fsoag = C.fcvt_soag;
+  const bool map_gas = a.do_cond || a.do_newnuc;
+  const bool defer = (PHASE == PHASE_PRE) && a.do_cond && !(cld > 0.999);
 
   auto load_sub = [&](Sub &s, const double (&q)[NPOP], const double (&fac_num)[NMODE],
                       const double (&fac_mass)[NMODE]) {
@@ -401,11 +473,54 @@ __device__ __forceinline__ void cell_step(const StepArgs &a, const long long c) 
       }
     }
   };
+  // queue the cell: solver state and hand-off at the start of the SOA loop
+  auto hand_off = [&](const Sub &s, const ClearMid &cm, const double (&uptk0)[NMODE],
+                      double relhum) {
+    const unsigned m = __activemask();
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(m) - 1;
+    unsigned base = 0;
+    if (lane == leader)
+      base = atomicAdd(&a.counters[0], (unsigned)__popc(m));
+    base = __shfl_sync(m, base, leader);
+    const unsigned slot = base + __popc(m & ((1u << lane) - 1));
+    a.task[slot] = (int)c;
+    const size_t n = (size_t)a.ncell;
+    SoaState st;
+    soa_init(st, (double)(int)(dt / 1), temp, pmid, s, uptk0);
+    double *q = a.soa + slot;
+    q[SOA_G * n] = st.g;
+#pragma unroll
+    for (int k = 0; k < NMODE; ++k) {
+      q[(SOA_A + k) * n] = st.a[k];
+      q[(SOA_OPOA + k) * n] = st.opoa[k];
+      q[(SOA_UPTK + k) * n] = st.uptk[k];
+    }
+    q[SOA_G0 * n] = st.g0;
+    double *h = a.hand + slot;
+    h[H_GAS1 * n] = s.gas[1];
+    double pop[NPOP];
+    sub_to_pop(s, pop);
+#pragma unroll
+    for (int p = 0; p < NPOP; ++p)
+      h[(H_POP + p) * n] = pop[p];
+#pragma unroll
+    for (int k = 0; k < NMODE; ++k) {
+      h[(H_UPTK + k) * n] = cm.uptk1[k];
+      h[(H_AWET + k) * n] = dgn_awet[k];
+      h[(H_WETD + k) * n] = wetdens[k];
+    }
+    h[H_NETPROD * n] = cm.netprod1;
+    h[H_SV_SO4 * n] = cm.sv_so4_ait;
+    h[H_SV_SOA * n] = cm.sv_soa_ait;
+    h[H_DGN_PC * n] = dgn_a[3];
+    h[H_RELHUM * n] = relhum;
+    return slot;
+  };
 
   if (cld < 1.0e-5) {
     // ------------------------------------------- clear grid cell
     Sub s;
-    // qsub = qgcm exactly (category I copies the grid means)
 #pragma unroll
     for (int m = 0; m < NMODE; ++m) {
       s.num[m] = qi[K::numslot(m)] * 1;
@@ -418,14 +533,23 @@ __device__ __forceinline__ void cell_step(const StepArgs &a, const long long c) 
     s.gas[0] = g_soag * fsoag;
     s.gas[1] = g_h2so4 * 1.0;
     const double qgas1[2] = {s.gas[0], s.gas[1]};
-    const int niter = clear_subarea<DIAG, PHASE>(a, c, dt, temp, pmid, zm, pblh, relhumgcm,
-                                                 dgn_a, dgn_awet, wetdens, qgas1, s, dg, 1.0);
-    if (niter == kDeferred)
+    if (defer) {
+      ClearMid cm;
+      double uptk0[NMODE];
+      clear_prefix<false>(a, dt, temp, pmid, dgn_awet, qgas1, s, cm, uptk0);
+      const unsigned slot = hand_off(s, cm, uptk0, relhumgcm);
+      double *h = a.hand + slot;
+      const size_t n = (size_t)a.ncell;
+#pragma unroll
+      for (int p = 0; p < NPOP; ++p)
+        h[(H_OC + p) * n] = qc[p];
       return;
+    }
+    const int niter = clear_subarea<DIAG, PHASE == PHASE_FULL>(a, dt, temp, pmid, zm, pblh, relhumgcm, dgn_a,
+                                          dgn_awet, wetdens, qgas1, s, dg, 1.0);
     if (niter > 1000)
       atomicOr(a.flags, MAM4B_FLAG_SOA_NITER_LIMIT);
     const double f = 1.0 - 0.0;
-    const bool map_gas = a.do_cond || a.do_newnuc;
     o_soag = dmax(0.0, 0.0 + (map_gas ? s.gas[0] / fsoag : g_soag) * f);
     o_h2so4 = dmax(0.0, 0.0 + (map_gas ? s.gas[1] / 1.0 : g_h2so4) * f);
 #pragma unroll
@@ -543,38 +667,10 @@ __device__ __forceinline__ void cell_step(const StepArgs &a, const long long c) 
         gcl[g] = gcl[g] / fclea;
       }
     }
-    // clear subarea (jsub 1)
-    {
-      Sub s;
-      load_sub(s, qi, fn_c, fm_c);
-      s.gas[0] = gcl[0] * fsoag;
-      s.gas[1] = gcl[1] * 1.0;
-      const double qgas1[2] = {g_soag * fsoag, g_h2so4 * 1.0};
-      const double rhc = bound(0.0, 1.0, (relhumgcm - fcldy) / fclea);
-      const int niter = clear_subarea<DIAG, PHASE>(a, c, dt, temp, pmid, zm, pblh, rhc, dgn_a,
-                                                   dgn_awet, wetdens, qgas1, s, dg, fclea);
-      if (niter == kDeferred)
-        return;
-      if (niter > 1000)
-        atomicOr(a.flags, MAM4B_FLAG_SOA_NITER_LIMIT);
-      const bool map_gas = a.do_cond || a.do_newnuc;
-      o_soag = 0.0 + (map_gas ? s.gas[0] / fsoag : gcl[0]) * fclea;
-      o_h2so4 = 0.0 + (map_gas ? s.gas[1] / 1.0 : gcl[1]) * fclea;
-#pragma unroll
-      for (int m = 0; m < NMODE; ++m) {
-        oi[K::numslot(m)] = 0.0 + (s.num[m] / 1.0) * fclea;
-        oc[K::numslot(m)] = 0.0 + 0.0 * fclea;
-#pragma unroll
-        for (int x = 0; x < NAER; ++x) {
-          const int slot = K::aer_slot(x, m);
-          if (slot >= 0) {
-            oi[slot] = 0.0 + (s.aer[x][m] / K::fcvt_aer(x)) * fclea;
-            oc[slot] = 0.0 + 0.0 * fclea;
-          }
-        }
-      }
-    }
-    // cloudy subarea (jsub 2): renaming only
+    const double rhc = bound(0.0, 1.0, (relhumgcm - fcldy) / fclea);
+    // cloudy subarea (jsub 2): renaming only; its contributions to the
+    // grid means are added after the clear subarea's
+    double ci[NPOP], cg[2];
     {
       Sub si, sc;
       load_sub(si, qi, fn_y, fm_y);
@@ -605,18 +701,18 @@ __device__ __forceinline__ void cell_step(const StepArgs &a, const long long c) 
         const double zero7[NAER] = {0, 0, 0, 0, 0, 0, 0};
         rename_subarea<true>(C, si, sc, zero7, zero7);
       }
-      o_soag = dmax(0.0, o_soag + gcy[0] * fcldy);
-      o_h2so4 = dmax(0.0, o_h2so4 + gcy[1] * fcldy);
+      cg[0] = gcy[0] * fcldy;
+      cg[1] = gcy[1] * fcldy;
 #pragma unroll
       for (int m = 0; m < NMODE; ++m) {
-        oi[K::numslot(m)] = dmax(0.0, oi[K::numslot(m)] + (si.num[m] / 1.0) * fcldy);
-        oc[K::numslot(m)] = oc[K::numslot(m)] + (sc.num[m] / 1.0) * fcldy;
+        ci[K::numslot(m)] = (si.num[m] / 1.0) * fcldy;
+        oc[K::numslot(m)] = (0.0 + 0.0 * fclea) + (sc.num[m] / 1.0) * fcldy;
 #pragma unroll
         for (int x = 0; x < NAER; ++x) {
           const int slot = K::aer_slot(x, m);
           if (slot >= 0) {
-            oi[slot] = dmax(0.0, oi[slot] + (si.aer[x][m] / K::fcvt_aer(x)) * fcldy);
-            oc[slot] = oc[slot] + (sc.aer[x][m] / K::fcvt_aer(x)) * fcldy;
+            ci[slot] = (si.aer[x][m] / K::fcvt_aer(x)) * fcldy;
+            oc[slot] = (0.0 + 0.0 * fclea) + (sc.aer[x][m] / K::fcvt_aer(x)) * fcldy;
           }
         }
       }
@@ -639,24 +735,68 @@ __device__ __forceinline__ void cell_step(const StepArgs &a, const long long c) 
         }
       }
     }
+    // clear subarea (jsub 1); in the diagnostics path its increments are
+    // accumulated before the cloudy subarea's, as in the reference
+    {
+      Sub s;
+      load_sub(s, qi, fn_c, fm_c);
+      s.gas[0] = gcl[0] * fsoag;
+      s.gas[1] = gcl[1] * 1.0;
+      const double qgas1[2] = {g_soag * fsoag, g_h2so4 * 1.0};
+      if (defer) {
+        ClearMid cm;
+        double uptk0[NMODE];
+        clear_prefix<false>(a, dt, temp, pmid, dgn_awet, qgas1, s, cm, uptk0);
+        const unsigned slot = hand_off(s, cm, uptk0, rhc);
+        double *h = a.hand + slot;
+        const size_t n = (size_t)a.ncell;
+#pragma unroll
+        for (int p = 0; p < NPOP; ++p) {
+          h[(H_OC + p) * n] = oc[p];
+          h[(H_CI + p) * n] = ci[p];
+        }
+        h[H_CG * n] = cg[0];
+        h[(H_CG + 1) * n] = cg[1];
+        return;
+      }
+      Diag dclear;
+      Diag *dcp = DIAG ? &dclear : nullptr;
+      if (DIAG) {
+#pragma unroll
+        for (int k = 0; k < NQTEND; ++k)
+#pragma unroll
+          for (int i = 0; i < 31; ++i)
+            dclear.t[k][i] = 0.0;
+      }
+      const int niter = clear_subarea<DIAG, PHASE == PHASE_FULL>(a, dt, temp, pmid, zm, pblh, rhc, dgn_a, dgn_awet,
+                                            wetdens, qgas1, s, dcp, fclea);
+      if (niter > 1000)
+        atomicOr(a.flags, MAM4B_FLAG_SOA_NITER_LIMIT);
+      if (DIAG) {
+        // jsub 1 then jsub 2: t = (0 + clear) + cloudy
+#pragma unroll
+        for (int k = 0; k < NQTEND; ++k)
+#pragma unroll
+          for (int i = 0; i < 31; ++i)
+            dgv.t[k][i] = dclear.t[k][i] + dgv.t[k][i];
+      }
+      o_soag = dmax(0.0, (0.0 + (map_gas ? s.gas[0] / fsoag : gcl[0]) * fclea) + cg[0]);
+      o_h2so4 = dmax(0.0, (0.0 + (map_gas ? s.gas[1] / 1.0 : gcl[1]) * fclea) + cg[1]);
+#pragma unroll
+      for (int m = 0; m < NMODE; ++m) {
+        oi[K::numslot(m)] = dmax(0.0, (0.0 + (s.num[m] / 1.0) * fclea) + ci[K::numslot(m)]);
+#pragma unroll
+        for (int x = 0; x < NAER; ++x) {
+          const int slot = K::aer_slot(x, m);
+          if (slot >= 0)
+            oi[slot] = dmax(0.0, (0.0 + (s.aer[x][m] / K::fcvt_aer(x)) * fclea) + ci[slot]);
+        }
+      }
+    }
   }
 
   // ---------------------------------------------------------- outputs
-  double *const *out = a.out;
-  out[MAM4B_OUT_TEND + 0][c] = (o_h2so4 * C.to_mmr[0] - h2so4) / dt;
-  out[MAM4B_OUT_TEND + 1][c] = (o_soag * C.to_mmr[1] - soag) / dt;
-#pragma unroll
-  for (int p = 0; p < NPOP; ++p) {
-    out[MAM4B_OUT_TEND + 2 + p][c] = (oi[p] * C.to_mmr[2 + p] - ai[p]) / dt;
-    out[MAM4B_OUT_TEND + 27 + p][c] = (oc[p] * C.to_mmr[2 + p] - ac[p]) / dt;
-  }
-#pragma unroll
-  for (int m = 0; m < NMODE; ++m) {
-    out[MAM4B_OUT_DGN_A + m][c] = dgn_a[m];
-    out[MAM4B_OUT_DGN_AWET + m][c] = dgn_awet[m];
-    out[MAM4B_OUT_WETDENS + m][c] = wetdens_wu[m];
-    out[MAM4B_OUT_QAERWAT + m][c] = qaerwat[m];
-  }
+  store_outputs(a, c, o_h2so4, o_soag, oi, oc, h2so4, soag, ai, ac);
   if (DIAG) {
 #pragma unroll
     for (int k = 0; k < NQTEND; ++k)
@@ -671,19 +811,112 @@ __device__ __forceinline__ void cell_step(const StepArgs &a, const long long c) 
   }
 }
 
-
-template <bool DIAG>
-__global__ void __launch_bounds__(128) pre_kernel(const __grid_constant__ StepArgs a) {
-  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c < a.ncell)
-    cell_step<DIAG, PHASE_PRE>(a, c);
+// Second half of a queued cell: the state at the SOA loop (hand-off), the
+// loop's result (solver), the rest of the clear subarea, recombination with
+// the cloudy subarea's contributions, tendencies.
+__device__ __forceinline__ void cell_post(const StepArgs &a, unsigned slot) {
+  const StepConsts &C = c_k;
+  const size_t n = (size_t)a.ncell;
+  const long long c = a.task[slot];
+  const double temp = __ldg(a.in[MAM4B_IN_T] + c);
+  const double pmid = __ldg(a.in[MAM4B_IN_P] + c);
+  const double zm = __ldg(a.in[MAM4B_IN_ZM] + c);
+  const double cld = __ldg(a.in[MAM4B_IN_CLD] + c);
+  const double pblh = __ldg(a.pblh + c / a.nlev);
+  const double dt = a.dt;
+  const double *h = a.hand + slot;
+  const double *q = a.soa + slot;
+  Sub s;
+  {
+    double pop[NPOP];
+#pragma unroll
+    for (int p = 0; p < NPOP; ++p)
+      pop[p] = h[(H_POP + p) * n];
+    pop_to_sub(pop, s);
+  }
+  s.gas[0] = q[SOA_G * n];
+  s.gas[1] = h[H_GAS1 * n];
+#pragma unroll
+  for (int k = 0; k < NMODE; ++k)
+    s.aer[0][k] = q[(SOA_A + k) * n];
+  ClearMid cm;
+  cm.netprod1 = h[H_NETPROD * n];
+  cm.sv_so4_ait = h[H_SV_SO4 * n];
+  cm.sv_soa_ait = h[H_SV_SOA * n];
+  double dgn_awet[NMODE], wetdens[NMODE];
+#pragma unroll
+  for (int k = 0; k < NMODE; ++k) {
+    cm.uptk1[k] = h[(H_UPTK + k) * n];
+    dgn_awet[k] = h[(H_AWET + k) * n];
+    wetdens[k] = h[(H_WETD + k) * n];
+  }
+  clear_suffix<false>(a, dt, temp, pmid, zm, pblh, h[H_RELHUM * n], h[H_DGN_PC * n], dgn_awet,
+                      wetdens, cm, s, nullptr, 0.0);
+  // recombination (form_gcm_of_gases_and_aerosols_from_subareas)
+  const double fsoag = C.fcvt_soag;
+  double o_h2so4, o_soag, oi[NPOP], oc[NPOP];
+#pragma unroll
+  for (int p = 0; p < NPOP; ++p)
+    oc[p] = h[(H_OC + p) * n];
+  double po[NPOP];
+  sub_to_pop(s, po);
+  if (cld < 1.0e-5) {
+    const double f = 1.0 - 0.0;
+    o_soag = dmax(0.0, 0.0 + (s.gas[0] / fsoag) * f);
+    o_h2so4 = dmax(0.0, 0.0 + (s.gas[1] / 1.0) * f);
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      oi[K::numslot(m)] = dmax(0.0, 0.0 + (po[K::numslot(m)] / 1.0) * f);
+#pragma unroll
+      for (int x = 0; x < NAER; ++x) {
+        const int sl = K::aer_slot(x, m);
+        if (sl >= 0)
+          oi[sl] = dmax(0.0, 0.0 + (po[sl] / K::fcvt_aer(x)) * f);
+      }
+    }
+  } else {
+    const double fclea = 1.0 - cld;
+    o_soag = dmax(0.0, (0.0 + (s.gas[0] / fsoag) * fclea) + h[H_CG * n]);
+    o_h2so4 = dmax(0.0, (0.0 + (s.gas[1] / 1.0) * fclea) + h[(H_CG + 1) * n]);
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      oi[K::numslot(m)] = dmax(0.0, (0.0 + (po[K::numslot(m)] / 1.0) * fclea) +
+                                        h[(H_CI + K::numslot(m)) * n]);
+#pragma unroll
+      for (int x = 0; x < NAER; ++x) {
+        const int sl = K::aer_slot(x, m);
+        if (sl >= 0)
+          oi[sl] = dmax(0.0, (0.0 + (po[sl] / K::fcvt_aer(x)) * fclea) + h[(H_CI + sl) * n]);
+      }
+    }
+  }
+  double ai[NPOP], ac[NPOP];
+#pragma unroll
+  for (int p = 0; p < NPOP; ++p) {
+    ai[p] = __ldg(a.in[MAM4B_IN_AER_I + p] + c);
+    ac[p] = __ldg(a.in[MAM4B_IN_AER_C + p] + c);
+  }
+  store_outputs(a, c, o_h2so4, o_soag, oi, oc, __ldg(a.in[MAM4B_IN_H2SO4] + c),
+                __ldg(a.in[MAM4B_IN_SOAG] + c), ai, ac);
 }
 
 template <bool DIAG>
+__global__ void __launch_bounds__(128) full_kernel(const __grid_constant__ StepArgs a) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < a.ncell)
+    cell_step<DIAG, PHASE_FULL>(a, c);
+}
+
+__global__ void __launch_bounds__(128) pre_kernel(const __grid_constant__ StepArgs a) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < a.ncell)
+    cell_step<false, PHASE_PRE>(a, c);
+}
+
 __global__ void __launch_bounds__(128) post_kernel(const __grid_constant__ StepArgs a) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < (long long)a.counters[0])
-    cell_step<DIAG, PHASE_POST>(a, a.task[i]);
+    cell_post(a, (unsigned)i);
 }
 
 // SOA sub-stepping of the queued cells. Persistent warps; every lane owns
@@ -696,7 +929,7 @@ __global__ void __launch_bounds__(kSoaBlock) soa_kernel(const __grid_constant__ 
   const int lane = threadIdx.x & 31;
   const size_t n = (size_t)a.ncell;
   SoaState st;
-  int cell = -1;
+  unsigned slot = 0;
   bool active = false, want = true;
   while (true) {
     const unsigned need = __ballot_sync(0xffffffffu, want);
@@ -710,8 +943,8 @@ __global__ void __launch_bounds__(kSoaBlock) soa_kernel(const __grid_constant__ 
         const unsigned t = base + __popc(need & ((1u << lane) - 1));
         want = false;
         if (t < ntask) {
-          cell = a.task[t];
-          const double *q = a.soa + (size_t)cell;
+          slot = t;
+          const double *q = a.soa + slot;
           st.g = q[SOA_G * n];
 #pragma unroll
           for (int k = 0; k < NMODE; ++k) {
@@ -730,7 +963,7 @@ __global__ void __launch_bounds__(kSoaBlock) soa_kernel(const __grid_constant__ 
     if (!__any_sync(0xffffffffu, active))
       break;
     if (active && !soa_step(st)) {
-      double *q = a.soa + (size_t)cell;
+      double *q = a.soa + slot;
       q[SOA_G * n] = st.g;
 #pragma unroll
       for (int k = 0; k < NMODE; ++k)
@@ -822,8 +1055,10 @@ struct mam4b_ctx {
   // host-path scratch (device slabs), grown on demand
   double *d_in, *d_out, *d_pblh;
   size_t cap_in, cap_out, cap_pblh;
-  // SOA solver scratch: loop state, queued cells, counters (grown on demand)
+  // pipeline scratch: SOA loop state, hand-off, queued cells, counters
+  // (grown on demand)
   double *d_soa;
+  double *d_hand;
   int *d_task;
   unsigned *d_counters;
   size_t cap_cells;
@@ -886,11 +1121,15 @@ cudaError_t ensure_solver_scratch(mam4b_ctx *ctx, size_t ncell) {
   if (e != cudaSuccess || ctx->cap_cells >= ncell)
     return e;
   cudaFree(ctx->d_soa);
+  cudaFree(ctx->d_hand);
   cudaFree(ctx->d_task);
   ctx->d_soa = nullptr;
+  ctx->d_hand = nullptr;
   ctx->d_task = nullptr;
   ctx->cap_cells = 0;
   e = cudaMalloc(&ctx->d_soa, (size_t)SOA_FIELDS * ncell * sizeof(double));
+  if (e == cudaSuccess)
+    e = cudaMalloc(&ctx->d_hand, (size_t)H_FIELDS * ncell * sizeof(double));
   if (e == cudaSuccess)
     e = cudaMalloc(&ctx->d_task, ncell * sizeof(int));
   if (e == cudaSuccess)
@@ -956,6 +1195,7 @@ mam4b_status mam4b_destroy(mam4b_ctx *ctx) {
   cudaFree(ctx->d_out);
   cudaFree(ctx->d_pblh);
   cudaFree(ctx->d_soa);
+  cudaFree(ctx->d_hand);
   cudaFree(ctx->d_task);
   cudaFree(ctx->d_counters);
   delete ctx;
@@ -1006,24 +1246,29 @@ mam4b_status mam4b_step(mam4b_ctx *ctx, const mam4b_state_view *in, const mam4b_
   const long long grid = (a.ncell + block - 1) / block;
   if (a.ncell > 0x7fffffffLL)
     return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_step: too many cells", cudaSuccess);
-  cudaError_t e = ensure_solver_scratch(ctx, (size_t)a.ncell);
+  cudaError_t e;
+  if (diag) {
+    // per-process diagnostics: one thread per cell, start to end
+    full_kernel<true><<<(unsigned)grid, block, 0, s>>>(a);
+    e = cudaGetLastError();
+    if (e != cudaSuccess)
+      return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_step launch", e);
+    ctx->launches += 1;
+    return MAM4B_OK;
+  }
+  e = ensure_solver_scratch(ctx, (size_t)a.ncell);
   if (e != cudaSuccess)
     return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_step scratch", e);
   a.soa = ctx->d_soa;
+  a.hand = ctx->d_hand;
   a.task = ctx->d_task;
   a.counters = ctx->d_counters;
   e = cudaMemsetAsync(ctx->d_counters, 0, 2 * sizeof(unsigned), s);
   if (e != cudaSuccess)
     return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_step counters", e);
-  if (diag)
-    pre_kernel<true><<<(unsigned)grid, block, 0, s>>>(a);
-  else
-    pre_kernel<false><<<(unsigned)grid, block, 0, s>>>(a);
+  pre_kernel<<<(unsigned)grid, block, 0, s>>>(a);
   soa_kernel<<<ctx->soa_grid, kSoaBlock, 0, s>>>(a);
-  if (diag)
-    post_kernel<true><<<(unsigned)grid, block, 0, s>>>(a);
-  else
-    post_kernel<false><<<(unsigned)grid, block, 0, s>>>(a);
+  post_kernel<<<(unsigned)grid, block, 0, s>>>(a);
   e = cudaGetLastError();
   if (e != cudaSuccess)
     return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_step launch", e);
