@@ -111,7 +111,9 @@ typedef enum mam4b_status {
   MAM4B_ERR_INVALID_ARGUMENT = 1, /* null pointer, bad size, bad config    */
   MAM4B_ERR_CUDA = 2,             /* a CUDA runtime call failed            */
   MAM4B_ERR_NOT_SUPPORTED = 3,    /* option not built into this library    */
-  MAM4B_ERR_DEVICE_FLAGS = 4      /* cell-level flags raised on the device */
+  MAM4B_ERR_DEVICE_FLAGS = 4,     /* cell-level flags raised on the device */
+  MAM4B_ERR_TOO_MANY_CELLS = 5    /* batch larger than the fixed scratch of
+                                     mam4b_step_slab_noalloc              */
 } mam4b_status;
 
 /* Cell-level condition bits reported by mam4b_last_status().
@@ -196,6 +198,40 @@ mam4b_status mam4b_step_host(mam4b_ctx *ctx, const double *in_slab,
                              const double *pblh, double *out_slab, size_t ld,
                              int ncol, int nlev, double dt, int precision,
                              void *stream);
+
+/*
+ * Allocation-free step (no counterpart in the reference: mam4xx allocates
+ * its work views itself). For callers that cannot call cudaMalloc: host
+ * models whose memory pool has reserved the GPU's memory up front, and
+ * host models that forbid allocation after start-up because cudaMalloc and
+ * cudaFree can synchronise the whole device and stall their other streams.
+ * The same step as mam4b_step_slab (FP64, no diagnostics, same results),
+ * with the working memory of the SOA condensation solver in one fixed
+ * device array inside the library instead of context-owned allocations:
+ * MAM4B_NOALLOC_MAX_CELLS cells at most, about 14 MB, held on every GPU
+ * that loads the library until the process exits. No context is needed.
+ *
+ *   cfg      process switches (NULL = mam4b_default_config)
+ *   in_slab, pblh, out_slab, ld, ncol, nlev, dt  as for mam4b_step_slab
+ *   flags    optional device pointer to one word into which the step ORs
+ *            its MAM4B_FLAG_* bits; the caller clears it (NULL = dropped)
+ *   stream   cudaStream_t the step is queued on (NULL = legacy default)
+ *
+ * Returns MAM4B_ERR_TOO_MANY_CELLS, before touching the device, when
+ * ncol*nlev > MAM4B_NOALLOC_MAX_CELLS; split larger batches by columns.
+ * The first call on a device does a one-time set-up with that device
+ * current (finds the array's device address, fills the constant tables)
+ * and synchronises the device; make that first call, for instance with
+ * ncol = 0, which does only the set-up, before any stream capture. Every
+ * call shares the one array and leaves its contents behind: two calls
+ * whose work overlaps on a device (other streams, other host threads)
+ * race and give wrong results; serialise them.
+ */
+#define MAM4B_NOALLOC_MAX_CELLS 16384
+mam4b_status mam4b_step_slab_noalloc(const mam4b_config *cfg, const double *in_slab,
+                                     const double *pblh, double *out_slab, size_t ld,
+                                     int ncol, int nlev, double dt, uint32_t *flags,
+                                     void *stream);
 
 /* Synchronises the context's last stream, stores in *flags the OR of the
  * MAM4B_FLAG_* bits raised since the previous call (then clears them), and

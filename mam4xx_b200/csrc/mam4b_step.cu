@@ -1040,6 +1040,24 @@ __host__ __device__ static StepConsts make_consts() {
 
 __global__ void init_consts_kernel(StepConsts *out) { *out = make_consts(); }
 
+// ============================================ scratch of the no-alloc step
+// mam4b_step_slab_noalloc keeps the pipeline's working memory in this one
+// array instead of context allocations: SOA loop state [SOA_FIELDS][ncell],
+// hand-off [H_FIELDS][ncell], queue ([ncell] ints), and a 256-byte tail with
+// the two queue counters and a spare flag word. Host code must not pass the
+// name g_noalloc_scratch to a kernel (on the host it is a stand-in, not a
+// device address); it uses the address from cudaGetSymbolAddress.
+constexpr size_t kNoAllocCells = MAM4B_NOALLOC_MAX_CELLS;
+constexpr size_t kNoAllocSoa = 0;
+constexpr size_t kNoAllocHand = kNoAllocSoa + (size_t)SOA_FIELDS * kNoAllocCells;
+constexpr size_t kNoAllocTask = kNoAllocHand + (size_t)H_FIELDS * kNoAllocCells;
+constexpr size_t kNoAllocTail = kNoAllocTask + kNoAllocCells / 2;
+constexpr size_t kNoAllocDoubles = kNoAllocTail + 32;
+static_assert(kNoAllocCells % 64 == 0, "scratch regions stay 256-byte aligned");
+static_assert(sizeof(StepConsts) <= (size_t)SOA_FIELDS * kNoAllocCells * sizeof(double),
+              "constants staging fits in the SOA region");
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
 }  // namespace mam4b
 
 // =============================================================== C ABI
@@ -1135,6 +1153,53 @@ cudaError_t ensure_solver_scratch(mam4b_ctx *ctx, size_t ncell) {
   if (e == cudaSuccess)
     ctx->cap_cells = ncell;
   return e;
+}
+
+// Per-device state of mam4b_step_slab_noalloc, filled once per device by
+// noalloc_setup with that device current.
+struct NoAllocDevice {
+  bool ready;
+  double *scratch;  // device address of g_noalloc_scratch on this device
+  int soa_grid;
+};
+NoAllocDevice g_noalloc[64];
+
+cudaError_t noalloc_setup(int dev) {
+  std::lock_guard<std::mutex> lk(g_init_mu);
+  if (dev < 0 || dev >= 64)
+    return cudaErrorInvalidDevice;
+  if (g_noalloc[dev].ready)
+    return cudaSuccess;
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess)
+    return e;
+  if (!g_consts_ready[dev]) {
+    // derived constants without a temporary allocation: staged in the
+    // scratch array (no step can be using it before set-up ends)
+    StepConsts *stage = reinterpret_cast<StepConsts *>(p);
+    init_consts_kernel<<<1, 1>>>(stage);
+    e = cudaGetLastError();
+    if (e == cudaSuccess)
+      e = cudaDeviceSynchronize();
+    if (e == cudaSuccess)
+      e = cudaMemcpyToSymbol(c_k, stage, sizeof(StepConsts), 0, cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess)
+      e = cudaDeviceSynchronize();
+    if (e != cudaSuccess)
+      return e;
+    g_consts_ready[dev] = true;
+  }
+  int sms = 0, per_sm = 0;
+  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, soa_kernel, kSoaBlock, 0);
+  if (e != cudaSuccess)
+    return e;
+  g_noalloc[dev].scratch = static_cast<double *>(p);
+  g_noalloc[dev].soa_grid = sms * (per_sm > 0 ? per_sm : 1);
+  g_noalloc[dev].ready = true;
+  return cudaSuccess;
 }
 }  // namespace
 
@@ -1351,6 +1416,73 @@ mam4b_status mam4b_step_host(mam4b_ctx *ctx, const double *in_slab, const double
   if (e != cudaSuccess)
     return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_step_host D2H", e);
   return MAM4B_OK;
+}
+
+// Allocation-free step for callers that cannot call cudaMalloc (a host
+// model whose memory pool owns the GPU's memory, or that forbids the
+// device-wide synchronisation of cudaMalloc/cudaFree once it runs). Same
+// kernels as mam4b_step, with their scratch in g_noalloc_scratch. Nothing
+// here allocates: set-up uses cudaGetSymbolAddress, a kernel, copies into
+// the constant bank and occupancy queries; each step clears the counters
+// with cudaMemsetAsync and launches three kernels. All calls share the
+// array, so calls that overlap on the GPU race.
+mam4b_status mam4b_step_slab_noalloc(const mam4b_config *cfg, const double *in_slab,
+                                     const double *pblh, double *out_slab, size_t ld, int ncol,
+                                     int nlev, double dt, uint32_t *flags, void *stream) {
+  mam4b_config c;
+  if (cfg)
+    c = *cfg;
+  else
+    mam4b_default_config(&c);
+  if (!valid_config(&c) || !in_slab || !pblh || !out_slab || ncol < 0 || nlev <= 0 ||
+      !(dt > 0.0) || !isfinite(dt) || ld < (size_t)ncol * (size_t)nlev)
+    return MAM4B_ERR_INVALID_ARGUMENT;
+  const long long ncell = (long long)ncol * nlev;
+  if (ncell > (long long)MAM4B_NOALLOC_MAX_CELLS)
+    return MAM4B_ERR_TOO_MANY_CELLS;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess)
+    e = noalloc_setup(dev);
+  if (e != cudaSuccess)
+    return MAM4B_ERR_CUDA;
+  if (ncell == 0)
+    return MAM4B_OK;
+  const NoAllocDevice &nd = g_noalloc[dev];
+  StepArgs a;
+  memset(&a, 0, sizeof(a));
+  for (int f = 0; f < MAM4B_NIN; ++f)
+    a.in[f] = in_slab + (size_t)f * ld;
+  a.pblh = pblh;
+  for (int f = 0; f < MAM4B_NOUT; ++f)
+    a.out[f] = out_slab + (size_t)f * ld;
+  unsigned *tail = reinterpret_cast<unsigned *>(nd.scratch + kNoAllocTail);
+  a.counters = tail;                                 // [0] queued, [1] handed out
+  a.flags = flags ? reinterpret_cast<unsigned *>(flags) : tail + 2;
+  a.soa = nd.scratch + kNoAllocSoa;
+  a.hand = nd.scratch + kNoAllocHand;
+  a.task = reinterpret_cast<int *>(nd.scratch + kNoAllocTask);
+  a.ncell = ncell;
+  a.nlev = nlev;
+  a.dt = dt;
+  a.do_cond = c.do_cond;
+  a.do_rename = c.do_rename;
+  a.do_newnuc = c.do_newnuc;
+  a.do_coag = c.do_coag;
+  a.optaa = c.gaexch_h2so4_uptake_optaa;
+  a.nmono = c.n_so4_monolayers_pcage;
+  cudaStream_t s = (cudaStream_t)stream;
+  // the counters (and the spare flag word) must start every step at zero
+  e = cudaMemsetAsync(tail, 0, 4 * sizeof(unsigned), s);
+  if (e != cudaSuccess)
+    return MAM4B_ERR_CUDA;
+  const int block = 128;
+  const unsigned grid = (unsigned)((ncell + block - 1) / block);
+  pre_kernel<<<grid, block, 0, s>>>(a);
+  soa_kernel<<<nd.soa_grid, kSoaBlock, 0, s>>>(a);
+  post_kernel<<<grid, block, 0, s>>>(a);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? MAM4B_OK : MAM4B_ERR_CUDA;
 }
 
 mam4b_status mam4b_last_status(mam4b_ctx *ctx, uint32_t *flags) {

@@ -14,7 +14,8 @@ LIB_PATH = os.path.join(PKG, "libmam4b.so")
 NIN, NOUT, NDIAG, NPOP = 57, 68, 155, 25
 FP64, MIXED = 0, 1
 STATUS = {0: "ok", 1: "invalid argument", 2: "cuda error", 3: "not supported",
-          4: "device flags"}
+          4: "device flags", 5: "too many cells for the no-alloc scratch"}
+NOALLOC_MAX_CELLS = 16384  # MAM4B_NOALLOC_MAX_CELLS
 FLAG_NONFINITE_INPUT = 0x1
 FLAG_SOA_NITER_LIMIT = 0x2
 FLAG_NONFINITE_OUTPUT = 0x4
@@ -64,6 +65,8 @@ def lib():
         L.mam4b_last_status.argtypes = [P, ctypes.POINTER(ctypes.c_uint32)]
         L.mam4b_last_status.restype = I
         L.mam4b_last_error.argtypes = [P, ctypes.c_char_p, S]
+        L.mam4b_step_slab_noalloc.argtypes = [ctypes.POINTER(Config), P, P, P, S, I, I, D, P, P]
+        L.mam4b_step_slab_noalloc.restype = I
         L.mam4b_launch_count.argtypes = [P]
         L.mam4b_launch_count.restype = ctypes.c_uint64
         _lib = L
@@ -72,7 +75,7 @@ def lib():
 
 EXPORTED = ["mam4b_abi_version", "mam4b_default_config", "mam4b_create", "mam4b_destroy",
             "mam4b_step", "mam4b_step_slab", "mam4b_step_host", "mam4b_last_status",
-            "mam4b_last_error", "mam4b_launch_count"]
+            "mam4b_last_error", "mam4b_launch_count", "mam4b_step_slab_noalloc"]
 
 
 def default_config(**overrides):

@@ -1,0 +1,83 @@
+"""Allocation-free entry point mam4b_step_slab_noalloc.
+
+Some host models cannot call cudaMalloc while they run: their memory pool
+has reserved the GPU's memory up front, or they forbid allocation after
+start-up because cudaMalloc/cudaFree can synchronise the whole device. This
+entry point serves them: it keeps the solver's working memory in one fixed
+array inside the library (MAM4B_NOALLOC_MAX_CELLS cells at most) and needs
+no context. It runs the same kernels as mam4b_step_slab, so its outputs
+must equal that entry point's bit for bit (the exact-equality criterion of
+the other bitwise GPU tests), also on the second of two calls in a row,
+when the array still holds the first call's contents.
+
+The file is named to be collected last; the no-alloc call comes first in
+the GPU test so that, run alone in a fresh process, it also covers the
+one-time set-up (constant tables filled without an allocation).
+"""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from mam4xx_b200 import native
+from mam4xx_b200.workloads import make_workload
+
+
+def _call_noalloc(cfg, x, pb, out, ld, ncol, nlev, dt, flags_ptr):
+    return native.lib().mam4b_step_slab_noalloc(
+        ctypes.byref(cfg) if cfg is not None else None, x, pb, out, ld, ncol, nlev, dt,
+        flags_ptr, None)
+
+
+def test_noalloc_rejects_oversized_and_invalid_batches():
+    """Checked before any CUDA call, so no device is needed."""
+    dummy = ctypes.c_void_p(16)
+    cap = native.NOALLOC_MAX_CELLS
+    # one column of cap+1 levels: beyond the fixed scratch
+    assert _call_noalloc(None, dummy, dummy, dummy, cap + 1, 1, cap + 1, 1800.0, None) == 5
+    # exactly at the cap with a too-small leading dimension: invalid
+    assert _call_noalloc(None, dummy, dummy, dummy, cap - 1, 1, cap, 1800.0, None) == 1
+    assert _call_noalloc(None, None, dummy, dummy, 8, 1, 8, 1800.0, None) == 1
+    bad = native.Config(1, 1, 1, 1, 7, 2, 8)  # optaa must be 1 or 2
+    assert _call_noalloc(bad, dummy, dummy, dummy, 8, 1, 8, 1800.0, None) == 1
+    assert native.STATUS[5].startswith("too many cells")
+
+
+@pytest.mark.gpu
+def test_noalloc_matches_step_slab_on_two_calls_in_a_row():
+    import torch
+    dev = torch.device("cuda:0")
+    # first call: 227 columns x 72 levels = 16344 cells (near the cap);
+    # second call: a smaller, ragged batch of another configuration, run
+    # over the first call's leftovers in the scratch array
+    cases = [make_workload("c4", ncol=227, nlev=72, seed=91),
+             make_workload("c2", ncol=13, nlev=72, seed=92)]
+    assert cases[0]["ncol"] * cases[0]["nlev"] <= native.NOALLOC_MAX_CELLS
+    cfg = native.default_config()
+    flags = torch.zeros(1, dtype=torch.int32, device=dev)
+    got = []
+    for w in cases:
+        x = torch.from_numpy(w["in_slab"]).to(dev)
+        pb = torch.from_numpy(w["pblh"]).to(dev)
+        n = x.shape[1]
+        out = torch.full((native.NOUT, n), float("nan"), dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()
+        st = _call_noalloc(cfg, x.data_ptr(), pb.data_ptr(), out.data_ptr(), n,
+                           w["ncol"], w["nlev"], w["dt"], flags.data_ptr())
+        assert st == 0, native.STATUS.get(st, st)
+        torch.cuda.synchronize()
+        got.append(out.cpu().numpy())
+    assert int(flags.item()) & (native.FLAG_NONFINITE_INPUT | native.FLAG_NONFINITE_OUTPUT) == 0
+
+    ctx = native.Context(cfg)
+    for w, g in zip(cases, got):
+        x = torch.from_numpy(w["in_slab"]).to(dev)
+        pb = torch.from_numpy(w["pblh"]).to(dev)
+        n = x.shape[1]
+        ref = torch.full((native.NOUT, n), float("nan"), dtype=torch.float64, device=dev)
+        ctx.step_slab(x.data_ptr(), pb.data_ptr(), ref.data_ptr(), n, w["ncol"], w["nlev"], w["dt"])
+        torch.cuda.synchronize()
+        r = ref.cpu().numpy()
+        assert np.isfinite(g).all()
+        assert np.array_equal(g, r), "no-alloc step differs from mam4b_step_slab"
