@@ -700,6 +700,22 @@ __device__ __forceinline__ void soa_init(SoaState &st, double dtfull, double tem
   st.niter = 0;
 }
 
+// sum(uptake * |phi|) of the loop's first pass (the first sub-step is
+// 0.05 / this): a cheap predictor of how many passes the loop will take.
+__device__ __forceinline__ double soa_first_rate(const SoaState &st) {
+  const double g = dmax(st.g, 0.0);
+  double r = 0.0;
+#pragma unroll
+  for (int n = 0; n < NMODE; ++n) {
+    if (!(st.uptk[n] > 1.0e-15))
+      continue;
+    const double a = dmax(st.a[n], 0.0);
+    const double gs = (st.g0 / dmax(st.opoa[n] + a, 1.0e-20)) * a;
+    r += st.uptk[n] * fabs((g - gs) / dmax(g, dmax(gs, 1.0e-20)));
+  }
+  return r;
+}
+
 // One pass of the reference's while loop; false once the loop has ended.
 __device__ __forceinline__ bool soa_step(SoaState &st) {
   if (!(st.tcur < st.dtfull - 1.0e-3))

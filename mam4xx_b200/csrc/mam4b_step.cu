@@ -40,10 +40,12 @@ struct StepArgs {
   int do_cond, do_rename, do_newnuc, do_coag, optaa;
   unsigned nmono;
   // SOA solver hand-off (see soa_kernel): per-cell loop state, the list of
-  // queued cells and two counters (queued, handed out)
+  // queued cells, the solver's order and counters (CNT_*)
   double *soa;       // [SOA_FIELDS][ncell], indexed by queue slot
   double *hand;      // [H_FIELDS][ncell], indexed by queue slot
   int *task;         // [ncell]: cell of each queue slot
+  int *order;        // [ncell]: slots in solver order, long loops from the
+                     // front, short ones from the back
   unsigned *counters;
 };
 
@@ -56,6 +58,13 @@ struct StepArgs {
 // the hand-off and the loop result.
 enum { PHASE_FULL = 0, PHASE_PRE = 1 };
 enum { SOA_G = 0, SOA_A = 1, SOA_OPOA = 5, SOA_UPTK = 9, SOA_G0 = 13, SOA_FIELDS = 14 };
+// queue counters: queued slots, slots handed to the solver, long and short
+// loops in the order list
+enum { CNT_QUEUED = 0, CNT_TAKEN = 1, CNT_LONG = 2, CNT_SHORT = 3, CNT_WORDS = 4 };
+// A loop is started early when its first sub-step is shorter than
+// dt / kLongLoopSteps, i.e. when it is expected to take at least about that
+// many sub-steps (the SOA loop's step is 0.05 / sum(uptake * |phi|)).
+constexpr double kLongLoopSteps = 300.0;
 
 // ----------------------------------------------------- per-cell amicphys
 struct Diag {
@@ -476,18 +485,34 @@ __device__ __forceinline__ void cell_step(const StepArgs &a, const long long c) 
   // queue the cell: solver state and hand-off at the start of the SOA loop
   auto hand_off = [&](const Sub &s, const ClearMid &cm, const double (&uptk0)[NMODE],
                       double relhum) {
+    SoaState st;
+    soa_init(st, (double)(int)(dt / 1), temp, pmid, s, uptk0);
+    const bool long_loop = soa_first_rate(st) * st.dtfull > 0.05 * kLongLoopSteps;
+    // warp-aggregated appends: the slot (in discovery order, which keeps
+    // the post kernel's cell accesses coalesced) and the solver order entry
     const unsigned m = __activemask();
     const int lane = threadIdx.x & 31;
     const int leader = __ffs(m) - 1;
-    unsigned base = 0;
-    if (lane == leader)
-      base = atomicAdd(&a.counters[0], (unsigned)__popc(m));
+    const unsigned m_long = __ballot_sync(m, long_loop), m_short = m & ~m_long;
+    unsigned base = 0, b_long = 0, b_short = 0;
+    if (lane == leader) {
+      base = atomicAdd(&a.counters[CNT_QUEUED], (unsigned)__popc(m));
+      if (m_long)
+        b_long = atomicAdd(&a.counters[CNT_LONG], (unsigned)__popc(m_long));
+      if (m_short)
+        b_short = atomicAdd(&a.counters[CNT_SHORT], (unsigned)__popc(m_short));
+    }
     base = __shfl_sync(m, base, leader);
-    const unsigned slot = base + __popc(m & ((1u << lane) - 1));
+    b_long = __shfl_sync(m, b_long, leader);
+    b_short = __shfl_sync(m, b_short, leader);
+    const unsigned below = (1u << lane) - 1;
+    const unsigned slot = base + __popc(m & below);
     a.task[slot] = (int)c;
+    if (long_loop)
+      a.order[b_long + __popc(m_long & below)] = (int)slot;
+    else
+      a.order[a.ncell - 1 - (b_short + __popc(m_short & below))] = (int)slot;
     const size_t n = (size_t)a.ncell;
-    SoaState st;
-    soa_init(st, (double)(int)(dt / 1), temp, pmid, s, uptk0);
     double *q = a.soa + slot;
     q[SOA_G * n] = st.g;
 #pragma unroll
@@ -915,17 +940,21 @@ __global__ void __launch_bounds__(128) pre_kernel(const __grid_constant__ StepAr
 
 __global__ void __launch_bounds__(128) post_kernel(const __grid_constant__ StepArgs a) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < (long long)a.counters[0])
+  if (i < (long long)a.counters[CNT_QUEUED])
     cell_post(a, (unsigned)i);
 }
 
 // SOA sub-stepping of the queued cells. Persistent warps; every lane owns
 // one cell's loop and, as soon as that loop ends, takes the next queued
 // cell (one atomic per warp for all lanes that need work), so a warp never
-// idles behind one cell that needs hundreds of sub-steps.
+// idles behind one cell that needs hundreds of sub-steps. Cells are taken
+// long loops first, so that the last ones handed out are short. The loop
+// is bound by FP64 division latency: 4 blocks of 256 per SM (64 registers)
+// hide more of it than the unconstrained 93-register build.
 constexpr int kSoaBlock = 256;
-__global__ void __launch_bounds__(kSoaBlock) soa_kernel(const __grid_constant__ StepArgs a) {
-  const unsigned ntask = a.counters[0];
+__global__ void __launch_bounds__(kSoaBlock, 4) soa_kernel(const __grid_constant__ StepArgs a) {
+  const unsigned ntask = a.counters[CNT_QUEUED];
+  const unsigned nlong = a.counters[CNT_LONG];
   const int lane = threadIdx.x & 31;
   const size_t n = (size_t)a.ncell;
   SoaState st;
@@ -937,13 +966,13 @@ __global__ void __launch_bounds__(kSoaBlock) soa_kernel(const __grid_constant__ 
       const int leader = __ffs(need) - 1;
       unsigned base = 0;
       if (lane == leader)
-        base = atomicAdd(&a.counters[1], (unsigned)__popc(need));
+        base = atomicAdd(&a.counters[CNT_TAKEN], (unsigned)__popc(need));
       base = __shfl_sync(0xffffffffu, base, leader);
       if (want) {
         const unsigned t = base + __popc(need & ((1u << lane) - 1));
         want = false;
         if (t < ntask) {
-          slot = t;
+          slot = (unsigned)(t < nlong ? a.order[t] : a.order[a.ncell - 1 - (t - nlong)]);
           const double *q = a.soa + slot;
           st.g = q[SOA_G * n];
 #pragma unroll
@@ -1043,15 +1072,16 @@ __global__ void init_consts_kernel(StepConsts *out) { *out = make_consts(); }
 // ============================================ scratch of the no-alloc step
 // mam4b_step_slab_noalloc keeps the pipeline's working memory in this one
 // array instead of context allocations: SOA loop state [SOA_FIELDS][ncell],
-// hand-off [H_FIELDS][ncell], queue ([ncell] ints), and a 256-byte tail with
-// the two queue counters and a spare flag word. Host code must not pass the
+// hand-off [H_FIELDS][ncell], queue and solver order ([ncell] ints each), and
+// a 256-byte tail with the queue counters and a spare flag word. Host code must not pass the
 // name g_noalloc_scratch to a kernel (on the host it is a stand-in, not a
 // device address); it uses the address from cudaGetSymbolAddress.
 constexpr size_t kNoAllocCells = MAM4B_NOALLOC_MAX_CELLS;
 constexpr size_t kNoAllocSoa = 0;
 constexpr size_t kNoAllocHand = kNoAllocSoa + (size_t)SOA_FIELDS * kNoAllocCells;
 constexpr size_t kNoAllocTask = kNoAllocHand + (size_t)H_FIELDS * kNoAllocCells;
-constexpr size_t kNoAllocTail = kNoAllocTask + kNoAllocCells / 2;
+constexpr size_t kNoAllocOrder = kNoAllocTask + kNoAllocCells / 2;
+constexpr size_t kNoAllocTail = kNoAllocOrder + kNoAllocCells / 2;
 constexpr size_t kNoAllocDoubles = kNoAllocTail + 32;
 static_assert(kNoAllocCells % 64 == 0, "scratch regions stay 256-byte aligned");
 static_assert(sizeof(StepConsts) <= (size_t)SOA_FIELDS * kNoAllocCells * sizeof(double),
@@ -1077,7 +1107,7 @@ struct mam4b_ctx {
   // (grown on demand)
   double *d_soa;
   double *d_hand;
-  int *d_task;
+  int *d_task, *d_order;
   unsigned *d_counters;
   size_t cap_cells;
   int soa_grid;  // persistent solver blocks (SMs x resident blocks)
@@ -1125,7 +1155,7 @@ bool valid_config(const mam4b_config *c) {
 cudaError_t ensure_solver_scratch(mam4b_ctx *ctx, size_t ncell) {
   cudaError_t e = cudaSuccess;
   if (!ctx->d_counters)
-    e = cudaMalloc(&ctx->d_counters, 2 * sizeof(unsigned));
+    e = cudaMalloc(&ctx->d_counters, CNT_WORDS * sizeof(unsigned));
   if (e == cudaSuccess && ctx->soa_grid == 0) {
     int dev = 0, sms = 0, per_sm = 0;
     e = cudaGetDevice(&dev);
@@ -1141,15 +1171,19 @@ cudaError_t ensure_solver_scratch(mam4b_ctx *ctx, size_t ncell) {
   cudaFree(ctx->d_soa);
   cudaFree(ctx->d_hand);
   cudaFree(ctx->d_task);
+  cudaFree(ctx->d_order);
   ctx->d_soa = nullptr;
   ctx->d_hand = nullptr;
   ctx->d_task = nullptr;
+  ctx->d_order = nullptr;
   ctx->cap_cells = 0;
   e = cudaMalloc(&ctx->d_soa, (size_t)SOA_FIELDS * ncell * sizeof(double));
   if (e == cudaSuccess)
     e = cudaMalloc(&ctx->d_hand, (size_t)H_FIELDS * ncell * sizeof(double));
   if (e == cudaSuccess)
     e = cudaMalloc(&ctx->d_task, ncell * sizeof(int));
+  if (e == cudaSuccess)
+    e = cudaMalloc(&ctx->d_order, ncell * sizeof(int));
   if (e == cudaSuccess)
     ctx->cap_cells = ncell;
   return e;
@@ -1262,6 +1296,7 @@ mam4b_status mam4b_destroy(mam4b_ctx *ctx) {
   cudaFree(ctx->d_soa);
   cudaFree(ctx->d_hand);
   cudaFree(ctx->d_task);
+  cudaFree(ctx->d_order);
   cudaFree(ctx->d_counters);
   delete ctx;
   return MAM4B_OK;
@@ -1327,8 +1362,9 @@ mam4b_status mam4b_step(mam4b_ctx *ctx, const mam4b_state_view *in, const mam4b_
   a.soa = ctx->d_soa;
   a.hand = ctx->d_hand;
   a.task = ctx->d_task;
+  a.order = ctx->d_order;
   a.counters = ctx->d_counters;
-  e = cudaMemsetAsync(ctx->d_counters, 0, 2 * sizeof(unsigned), s);
+  e = cudaMemsetAsync(ctx->d_counters, 0, CNT_WORDS * sizeof(unsigned), s);
   if (e != cudaSuccess)
     return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_step counters", e);
   pre_kernel<<<(unsigned)grid, block, 0, s>>>(a);
@@ -1457,11 +1493,12 @@ mam4b_status mam4b_step_slab_noalloc(const mam4b_config *cfg, const double *in_s
   for (int f = 0; f < MAM4B_NOUT; ++f)
     a.out[f] = out_slab + (size_t)f * ld;
   unsigned *tail = reinterpret_cast<unsigned *>(nd.scratch + kNoAllocTail);
-  a.counters = tail;                                 // [0] queued, [1] handed out
-  a.flags = flags ? reinterpret_cast<unsigned *>(flags) : tail + 2;
+  a.counters = tail;  // CNT_WORDS queue counters, then the spare flag word
+  a.flags = flags ? reinterpret_cast<unsigned *>(flags) : tail + CNT_WORDS;
   a.soa = nd.scratch + kNoAllocSoa;
   a.hand = nd.scratch + kNoAllocHand;
   a.task = reinterpret_cast<int *>(nd.scratch + kNoAllocTask);
+  a.order = reinterpret_cast<int *>(nd.scratch + kNoAllocOrder);
   a.ncell = ncell;
   a.nlev = nlev;
   a.dt = dt;
@@ -1473,7 +1510,7 @@ mam4b_status mam4b_step_slab_noalloc(const mam4b_config *cfg, const double *in_s
   a.nmono = c.n_so4_monolayers_pcage;
   cudaStream_t s = (cudaStream_t)stream;
   // the counters (and the spare flag word) must start every step at zero
-  e = cudaMemsetAsync(tail, 0, 4 * sizeof(unsigned), s);
+  e = cudaMemsetAsync(tail, 0, (CNT_WORDS + 1) * sizeof(unsigned), s);
   if (e != cudaSuccess)
     return MAM4B_ERR_CUDA;
   const int block = 128;
