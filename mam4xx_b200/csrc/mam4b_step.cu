@@ -1093,6 +1093,14 @@ static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 // =============================================================== C ABI
 using namespace mam4b;
 
+// Host-buffer path: columns are processed in chunks of about kHostChunkCells
+// cells, round-robin over kHostStreams streams, so that the host->device
+// copy of one chunk, the kernels of another and the device->host copy of a
+// third run at the same time.
+constexpr int kHostStreams = 3;
+constexpr long long kHostChunkCells = 1LL << 19;
+constexpr int kMaxChunks = 64;
+
 struct mam4b_ctx {
   mam4b_config cfg;
   int device;
@@ -1108,9 +1116,13 @@ struct mam4b_ctx {
   double *d_soa;
   double *d_hand;
   int *d_task, *d_order;
-  unsigned *d_counters;
+  unsigned *d_counters;  // CNT_WORDS per chunk of the host path
   size_t cap_cells;
   int soa_grid;  // persistent solver blocks (SMs x resident blocks)
+  // host path: copy/compute streams and their events (created on first use)
+  cudaStream_t hs[kHostStreams];
+  cudaEvent_t ev_start, ev_done[kHostStreams];
+  bool host_streams;
 };
 
 namespace {
@@ -1155,7 +1167,7 @@ bool valid_config(const mam4b_config *c) {
 cudaError_t ensure_solver_scratch(mam4b_ctx *ctx, size_t ncell) {
   cudaError_t e = cudaSuccess;
   if (!ctx->d_counters)
-    e = cudaMalloc(&ctx->d_counters, CNT_WORDS * sizeof(unsigned));
+    e = cudaMalloc(&ctx->d_counters, (size_t)CNT_WORDS * kMaxChunks * sizeof(unsigned));
   if (e == cudaSuccess && ctx->soa_grid == 0) {
     int dev = 0, sms = 0, per_sm = 0;
     e = cudaGetDevice(&dev);
@@ -1187,6 +1199,70 @@ cudaError_t ensure_solver_scratch(mam4b_ctx *ctx, size_t ncell) {
   if (e == cudaSuccess)
     ctx->cap_cells = ncell;
   return e;
+}
+
+void set_step_config(const mam4b_ctx *ctx, StepArgs &a, long long ncell, int nlev, double dt) {
+  a.flags = ctx->d_flags;
+  a.ncell = ncell;
+  a.nlev = nlev;
+  a.dt = dt;
+  a.do_cond = ctx->cfg.do_cond;
+  a.do_rename = ctx->cfg.do_rename;
+  a.do_newnuc = ctx->cfg.do_newnuc;
+  a.do_coag = ctx->cfg.do_coag;
+  a.optaa = ctx->cfg.gaexch_h2so4_uptake_optaa;
+  a.nmono = ctx->cfg.n_so4_monolayers_pcage;
+}
+
+// Pipeline scratch of the cells [c0, c0 + a.ncell) of a batch (one host
+// chunk; c0 = 0 for a whole batch); chunk selects its counters.
+void set_step_scratch(const mam4b_ctx *ctx, StepArgs &a, size_t c0, int chunk) {
+  a.soa = ctx->d_soa + (size_t)SOA_FIELDS * c0;
+  a.hand = ctx->d_hand + (size_t)H_FIELDS * c0;
+  a.task = ctx->d_task + c0;
+  a.order = ctx->d_order + c0;
+  a.counters = ctx->d_counters + (size_t)CNT_WORDS * chunk;
+}
+
+// Clears the counters and queues the three pipeline kernels on s.
+cudaError_t launch_pipeline(mam4b_ctx *ctx, const StepArgs &a, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(a.counters, 0, CNT_WORDS * sizeof(unsigned), s);
+  if (e != cudaSuccess)
+    return e;
+  const int block = 128;
+  const unsigned grid = (unsigned)((a.ncell + block - 1) / block);
+  pre_kernel<<<grid, block, 0, s>>>(a);
+  soa_kernel<<<ctx->soa_grid, kSoaBlock, 0, s>>>(a);
+  post_kernel<<<grid, block, 0, s>>>(a);
+  e = cudaGetLastError();
+  if (e == cudaSuccess)
+    ctx->launches += 3;
+  return e;
+}
+
+cudaError_t ensure_host_streams(mam4b_ctx *ctx) {
+  if (ctx->host_streams)
+    return cudaSuccess;
+  cudaError_t e = cudaEventCreateWithFlags(&ctx->ev_start, cudaEventDisableTiming);
+  int k = 0;
+  for (; k < kHostStreams && e == cudaSuccess; ++k) {
+    e = cudaStreamCreateWithFlags(&ctx->hs[k], cudaStreamNonBlocking);
+    if (e == cudaSuccess) {
+      e = cudaEventCreateWithFlags(&ctx->ev_done[k], cudaEventDisableTiming);
+      if (e != cudaSuccess)
+        cudaStreamDestroy(ctx->hs[k]);
+    }
+  }
+  if (e != cudaSuccess) {
+    for (int j = 0; j < k - 1; ++j) {
+      cudaStreamDestroy(ctx->hs[j]);
+      cudaEventDestroy(ctx->ev_done[j]);
+    }
+    cudaEventDestroy(ctx->ev_start);
+    return e;
+  }
+  ctx->host_streams = true;
+  return cudaSuccess;
 }
 
 // Per-device state of mam4b_step_slab_noalloc, filled once per device by
@@ -1298,6 +1374,13 @@ mam4b_status mam4b_destroy(mam4b_ctx *ctx) {
   cudaFree(ctx->d_task);
   cudaFree(ctx->d_order);
   cudaFree(ctx->d_counters);
+  if (ctx->host_streams) {
+    for (int k = 0; k < kHostStreams; ++k) {
+      cudaStreamDestroy(ctx->hs[k]);
+      cudaEventDestroy(ctx->ev_done[k]);
+    }
+    cudaEventDestroy(ctx->ev_start);
+  }
   delete ctx;
   return MAM4B_OK;
 }
@@ -1328,16 +1411,7 @@ mam4b_status mam4b_step(mam4b_ctx *ctx, const mam4b_state_view *in, const mam4b_
     a.diag[f] = out->diag[f];
     diag = diag || (out->diag[f] != nullptr);
   }
-  a.flags = ctx->d_flags;
-  a.ncell = (long long)ncol * nlev;
-  a.nlev = nlev;
-  a.dt = dt;
-  a.do_cond = ctx->cfg.do_cond;
-  a.do_rename = ctx->cfg.do_rename;
-  a.do_newnuc = ctx->cfg.do_newnuc;
-  a.do_coag = ctx->cfg.do_coag;
-  a.optaa = ctx->cfg.gaexch_h2so4_uptake_optaa;
-  a.nmono = ctx->cfg.n_so4_monolayers_pcage;
+  set_step_config(ctx, a, (long long)ncol * nlev, nlev, dt);
   cudaStream_t s = (cudaStream_t)stream;
   ctx->last_stream = s;
   if (a.ncell == 0)
@@ -1359,21 +1433,10 @@ mam4b_status mam4b_step(mam4b_ctx *ctx, const mam4b_state_view *in, const mam4b_
   e = ensure_solver_scratch(ctx, (size_t)a.ncell);
   if (e != cudaSuccess)
     return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_step scratch", e);
-  a.soa = ctx->d_soa;
-  a.hand = ctx->d_hand;
-  a.task = ctx->d_task;
-  a.order = ctx->d_order;
-  a.counters = ctx->d_counters;
-  e = cudaMemsetAsync(ctx->d_counters, 0, CNT_WORDS * sizeof(unsigned), s);
-  if (e != cudaSuccess)
-    return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_step counters", e);
-  pre_kernel<<<(unsigned)grid, block, 0, s>>>(a);
-  soa_kernel<<<ctx->soa_grid, kSoaBlock, 0, s>>>(a);
-  post_kernel<<<(unsigned)grid, block, 0, s>>>(a);
-  e = cudaGetLastError();
+  set_step_scratch(ctx, a, 0, 0);
+  e = launch_pipeline(ctx, a, s);
   if (e != cudaSuccess)
     return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_step launch", e);
-  ctx->launches += 3;
   return MAM4B_OK;
 }
 
@@ -1411,46 +1474,80 @@ mam4b_status mam4b_step_host(mam4b_ctx *ctx, const double *in_slab, const double
                              double *out_slab, size_t ld, int ncol, int nlev, double dt,
                              int precision, void *stream) {
   if (!ctx || !in_slab || !pblh || !out_slab || ncol < 0 || nlev <= 0 ||
-      ld < (size_t)ncol * (size_t)nlev)
+      ld < (size_t)ncol * (size_t)nlev || !(dt > 0.0) || !isfinite(dt))
     return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_step_host", cudaSuccess);
+  if (precision != MAM4B_FP64)
+    return set_err(ctx, MAM4B_ERR_NOT_SUPPORTED, "mam4b_step_host: precision", cudaSuccess);
   const size_t n = (size_t)ncol * (size_t)nlev;
+  if (n > 0x7fffffffULL)
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_step_host: too many cells", cudaSuccess);
+  cudaStream_t us = (cudaStream_t)stream;
+  ctx->last_stream = us;
+  if (n == 0)
+    return MAM4B_OK;
   cudaError_t e = grow(&ctx->d_in, &ctx->cap_in, (size_t)MAM4B_NIN * n);
   if (e == cudaSuccess)
     e = grow(&ctx->d_out, &ctx->cap_out, (size_t)MAM4B_NOUT * n);
   if (e == cudaSuccess)
-    e = grow(&ctx->d_pblh, &ctx->cap_pblh, (size_t)(ncol > 0 ? ncol : 1));
-  if (e != cudaSuccess)
-    return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_step_host alloc", e);
-  cudaStream_t s = (cudaStream_t)stream;
-  // one copy per field when the host leading dimension differs from n
-  if (ld == n) {
-    e = cudaMemcpyAsync(ctx->d_in, in_slab, (size_t)MAM4B_NIN * n * sizeof(double),
-                        cudaMemcpyHostToDevice, s);
-  } else {
-    for (int f = 0; f < MAM4B_NIN && e == cudaSuccess; ++f)
-      e = cudaMemcpyAsync(ctx->d_in + (size_t)f * n, in_slab + (size_t)f * ld,
-                          n * sizeof(double), cudaMemcpyHostToDevice, s);
-  }
+    e = grow(&ctx->d_pblh, &ctx->cap_pblh, (size_t)ncol);
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(ctx->d_pblh, pblh, (size_t)ncol * sizeof(double), cudaMemcpyHostToDevice, s);
-  if (e != cudaSuccess)
-    return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_step_host H2D", e);
-  mam4b_status st = mam4b_step_slab(ctx, ctx->d_in, ctx->d_pblh, ctx->d_out, n, ncol, nlev, dt,
-                                    precision, stream);
-  if (st != MAM4B_OK)
-    return st;
-  if (ld == n) {
-    e = cudaMemcpyAsync(out_slab, ctx->d_out, (size_t)MAM4B_NOUT * n * sizeof(double),
-                        cudaMemcpyDeviceToHost, s);
-  } else {
-    for (int f = 0; f < MAM4B_NOUT && e == cudaSuccess; ++f)
-      e = cudaMemcpyAsync(out_slab + (size_t)f * ld, ctx->d_out + (size_t)f * n,
-                          n * sizeof(double), cudaMemcpyDeviceToHost, s);
-  }
+    e = ensure_solver_scratch(ctx, n);
   if (e == cudaSuccess)
-    e = cudaStreamSynchronize(s);
+    e = ensure_host_streams(ctx);
   if (e != cudaSuccess)
-    return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_step_host D2H", e);
+    return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_step_host scratch", e);
+  // chunks of whole columns
+  int chunk_cols = (int)(kHostChunkCells / nlev);
+  if (chunk_cols < 1)
+    chunk_cols = 1;
+  if ((ncol + chunk_cols - 1) / chunk_cols > kMaxChunks)
+    chunk_cols = (ncol + kMaxChunks - 1) / kMaxChunks;
+  const int nchunk = (ncol + chunk_cols - 1) / chunk_cols;
+  // the internal streams start after the work already queued on us
+  e = cudaEventRecord(ctx->ev_start, us);
+  for (int k = 0; k < kHostStreams && e == cudaSuccess; ++k)
+    e = cudaStreamWaitEvent(ctx->hs[k], ctx->ev_start, 0);
+  const size_t dp = n * sizeof(double), hp = ld * sizeof(double);
+  for (int i = 0; i < nchunk && e == cudaSuccess; ++i) {
+    cudaStream_t s = ctx->hs[i % kHostStreams];
+    const int col0 = i * chunk_cols;
+    const int ncc = (col0 + chunk_cols <= ncol) ? chunk_cols : ncol - col0;
+    const size_t c0 = (size_t)col0 * nlev, nc = (size_t)ncc * nlev;
+    // field f of the chunk: nc doubles at f*ld + c0 on the host, f*n + c0 on the device
+    e = cudaMemcpy2DAsync(ctx->d_in + c0, dp, in_slab + c0, hp, nc * sizeof(double), MAM4B_NIN,
+                          cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(ctx->d_pblh + col0, pblh + col0, (size_t)ncc * sizeof(double),
+                          cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess)
+      break;
+    StepArgs a;
+    memset(&a, 0, sizeof(a));
+    for (int f = 0; f < MAM4B_NIN; ++f)
+      a.in[f] = ctx->d_in + (size_t)f * n + c0;
+    a.pblh = ctx->d_pblh + col0;
+    for (int f = 0; f < MAM4B_NOUT; ++f)
+      a.out[f] = ctx->d_out + (size_t)f * n + c0;
+    set_step_config(ctx, a, (long long)nc, nlev, dt);
+    set_step_scratch(ctx, a, c0, i);
+    e = launch_pipeline(ctx, a, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpy2DAsync(out_slab + c0, hp, ctx->d_out + c0, dp, nc * sizeof(double),
+                            MAM4B_NOUT, cudaMemcpyDeviceToHost, s);
+  }
+  // us waits for every internal stream, then the call returns
+  for (int k = 0; k < kHostStreams; ++k) {
+    cudaError_t e2 = cudaEventRecord(ctx->ev_done[k], ctx->hs[k]);
+    if (e2 == cudaSuccess)
+      e2 = cudaStreamWaitEvent(us, ctx->ev_done[k], 0);
+    if (e == cudaSuccess)
+      e = e2;
+  }
+  cudaError_t e3 = cudaStreamSynchronize(us);
+  if (e == cudaSuccess)
+    e = e3;
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_step_host", e);
   return MAM4B_OK;
 }
 

@@ -178,6 +178,26 @@ def test_host_entry_matches_device_entry(cuda_device):
     np.testing.assert_array_equal(out, dev)
 
 
+def test_host_entry_chunked_pipeline(cuda_device):
+    """The host entry streams columns in chunks of ~2^19 cells over several
+    streams: 16,000 x 72 cells make 3 chunks, the last one ragged. A padded
+    host leading dimension and a second, smaller call on the same context
+    (chunk scratch reused) must give the device entry's results bit for bit."""
+    ctx = native.Context()
+    for ncol, pad in ((16000, 7), (9000, 0)):
+        w = make_workload("c4", ncol=ncol, seed=40 + ncol)
+        dev = run_gpu(w)
+        n = w["in_slab"].shape[1]
+        ld = n + pad
+        x = np.zeros((native.NIN, ld))
+        x[:, :n] = w["in_slab"]
+        out = np.full((native.NOUT, ld), -7.0)
+        ctx.step_host(x.ctypes.data, w["pblh"].ctypes.data, out.ctypes.data, ld,
+                      w["ncol"], w["nlev"], w["dt"])
+        np.testing.assert_array_equal(out[:, :n], dev)
+        assert (out[:, n:] == -7.0).all()  # padding untouched
+
+
 def test_full_size_properties(cuda_device):
     """At 65,536 x 72 cells (too many for the oracle): finite outputs,
     bitwise-deterministic reruns, non-negative post-step state, and
