@@ -49,14 +49,14 @@ struct StepArgs {
   unsigned *counters;
 };
 
-// Phases of the step. FULL runs each cell start to end in one thread (the
-// diagnostics path). PRE runs each cell up to the SOA condensation loop of
-// its clear subarea, writes the loop's initial state and the rest of the
-// cell's state at that point to slot-indexed scratch and queues the cell
-// (cells without the loop finish in PRE); soa_kernel runs the queued loops
-// with per-lane work stealing; post_kernel finishes the queued cells from
-// the hand-off and the loop result.
-enum { PHASE_FULL = 0, PHASE_PRE = 1 };
+// The step runs as a pipeline of three kernels when condensation is on and
+// no diagnostics are asked for: pre_kernel runs each cell up to the SOA
+// condensation loop of its clear subarea, writes the loop's initial state
+// and the rest of the cell's state at that point to slot-indexed scratch
+// and queues the cell (cloudy cells finish there); soa_kernel runs the
+// queued loops with per-lane work stealing; post_kernel finishes the queued
+// cells from the hand-off and the loop result. Otherwise full_kernel runs
+// each cell start to end in one thread.
 enum { SOA_G = 0, SOA_A = 1, SOA_OPOA = 5, SOA_UPTK = 9, SOA_G0 = 13, SOA_FIELDS = 14 };
 // queue counters: queued slots, slots handed to the solver, long and short
 // loops in the order list
@@ -323,10 +323,9 @@ __device__ __forceinline__ void clear_suffix(const StepArgs &a, double deltat, d
   }
 }
 
-// Whole clear subarea in one thread: part 1, the SOA loop inline (compiled
-// in only WITH_SOA; the pre kernel queues every cell that has one), part 2.
+// Whole clear subarea in one thread: part 1, the SOA loop inline, part 2.
 // Returns the SOA sub-step count.
-template <bool DIAG, bool WITH_SOA>
+template <bool DIAG>
 __device__ __forceinline__ int clear_subarea(const StepArgs &a, double deltat, double temp,
                                              double pmid, double zmid, double pblh,
                                              double relhum, const double (&dgn_a)[NMODE],
@@ -338,7 +337,7 @@ __device__ __forceinline__ int clear_subarea(const StepArgs &a, double deltat, d
   double uptk0[NMODE];
   clear_prefix<DIAG>(a, deltat, temp, pmid, dgn_awet, qgas1, s, cm, uptk0);
   int niter = 0;
-  if (WITH_SOA && a.do_cond)
+  if (a.do_cond)
     niter = soa_exchange((double)(int)(deltat / 1), temp, pmid, s, uptk0);
   clear_suffix<DIAG>(a, deltat, temp, pmid, zmid, pblh, relhum, dgn_a[3], dgn_awet, wetdens, cm, s,
                      dg, afrac);
@@ -382,75 +381,264 @@ __device__ __forceinline__ void store_outputs(const StepArgs &a, long long c, do
   }
 }
 
-// One grid cell: modal_aero_calcsize_sub, modal_aero_water_uptake_dr and
-// modal_aero_amicphys_intr (mam4_amicphys.hpp:2120-2376) with
-// q_pregaschem = q_precldchem = qq and qqcw_precldchem = qqcw.
-// PHASE_FULL: all of it. PHASE_PRE: cells with a clear subarea and
-// condensation stop at the SOA loop, hand their state to the solver and the
-// post kernel, and are queued; the others finish here.
-template <bool DIAG, int PHASE>
-__device__ __forceinline__ void cell_step(const StepArgs &a, const long long c) {
+// Per-cell state after calcsize and water uptake (modal_aero_calcsize_sub,
+// modal_aero_water_uptake_dr), in amicphys units where amicphys reads it.
+struct Front {
+  double temp, pmid, zm, qv, cld, h2so4, soag, pblh;
+  double ai[NPOP], ac[NPOP];          // populations as passed in (mmr)
+  double dgn_a[NMODE], dgn_awet[NMODE], wetdens[NMODE];
+  double qi[NPOP], qc[NPOP];          // after the calcsize update (vmr)
+  double g_h2so4, g_soag;             // gases (vmr)
+  double relhumgcm;
+};
+
+// Loads the cell, checks it, runs calcsize and water uptake, writes the
+// size outputs and prepares the amicphys inputs: the part of
+// modal_aero_amicphys_intr (mam4_amicphys.hpp:2120-2260) before the
+// subarea loop, with q_pregaschem = q_precldchem = qq and
+// qqcw_precldchem = qqcw.
+__device__ __forceinline__ void cell_front(const StepArgs &a, const long long c, Front &f) {
   const StepConsts &C = c_k;
-  const double temp = __ldg(a.in[MAM4B_IN_T] + c);
-  const double pmid = __ldg(a.in[MAM4B_IN_P] + c);
-  const double zm = __ldg(a.in[MAM4B_IN_ZM] + c);
-  const double qv = __ldg(a.in[MAM4B_IN_QV] + c);
-  const double cld = __ldg(a.in[MAM4B_IN_CLD] + c);
-  const double h2so4 = __ldg(a.in[MAM4B_IN_H2SO4] + c);
-  const double soag = __ldg(a.in[MAM4B_IN_SOAG] + c);
-  const double pblh = __ldg(a.pblh + c / a.nlev);
+  f.temp = __ldg(a.in[MAM4B_IN_T] + c);
+  f.pmid = __ldg(a.in[MAM4B_IN_P] + c);
+  f.zm = __ldg(a.in[MAM4B_IN_ZM] + c);
+  f.qv = __ldg(a.in[MAM4B_IN_QV] + c);
+  f.cld = __ldg(a.in[MAM4B_IN_CLD] + c);
+  f.h2so4 = __ldg(a.in[MAM4B_IN_H2SO4] + c);
+  f.soag = __ldg(a.in[MAM4B_IN_SOAG] + c);
+  f.pblh = __ldg(a.pblh + c / a.nlev);
   const double dt = a.dt;
-  double ai[NPOP], ac[NPOP];
 #pragma unroll
   for (int p = 0; p < NPOP; ++p) {
-    ai[p] = __ldg(a.in[MAM4B_IN_AER_I + p] + c);
-    ac[p] = __ldg(a.in[MAM4B_IN_AER_C + p] + c);
+    f.ai[p] = __ldg(a.in[MAM4B_IN_AER_I + p] + c);
+    f.ac[p] = __ldg(a.in[MAM4B_IN_AER_C + p] + c);
   }
   {
-    double chk = temp + pmid + zm + qv + cld + h2so4 + soag + pblh;
+    double chk = f.temp + f.pmid + f.zm + f.qv + f.cld + f.h2so4 + f.soag + f.pblh;
 #pragma unroll
     for (int p = 0; p < NPOP; ++p)
-      chk += ai[p] + ac[p];
+      chk += f.ai[p] + f.ac[p];
     if (!isfinite(chk))
       atomicOr(a.flags, MAM4B_FLAG_NONFINITE_INPUT);
   }
-
-  // ------------------------------------------------------- calcsize
-  double dgn_a[NMODE], pt_i[NPOP], pt_c[NPOP];
-  calcsize(C, ai, ac, dt, dgn_a, pt_i, pt_c);
-  // ---------------------------------------------------- water uptake
-  double dgn_awet[NMODE], qaerwat[NMODE], wetdens_wu[NMODE];
-  water_uptake(C, ai, qv, temp, pmid, cld, dgn_a, dgn_awet, qaerwat, wetdens_wu);
+  double pt_i[NPOP], pt_c[NPOP];
+  calcsize(C, f.ai, f.ac, dt, f.dgn_a, pt_i, pt_c);
+  double qaerwat[NMODE], wetdens_wu[NMODE];
+  water_uptake(C, f.ai, f.qv, f.temp, f.pmid, f.cld, f.dgn_a, f.dgn_awet, qaerwat, wetdens_wu);
 #pragma unroll
   for (int m = 0; m < NMODE; ++m) {
-    a.out[MAM4B_OUT_DGN_A + m][c] = dgn_a[m];
-    a.out[MAM4B_OUT_DGN_AWET + m][c] = dgn_awet[m];
+    a.out[MAM4B_OUT_DGN_A + m][c] = f.dgn_a[m];
+    a.out[MAM4B_OUT_DGN_AWET + m][c] = f.dgn_awet[m];
     a.out[MAM4B_OUT_WETDENS + m][c] = wetdens_wu[m];
     a.out[MAM4B_OUT_QAERWAT + m][c] = qaerwat[m];
   }
-
   // calcsize tendencies applied for one step, then amicphys units
-  double qi[NPOP], qc[NPOP];
 #pragma unroll
   for (int p = 0; p < NPOP; ++p) {
-    qi[p] = dmax(0.0, dmax(0.0, ai[p] + pt_i[p] * dt) * C.to_vmr[2 + p]);
-    qc[p] = dmax(0.0, dmax(0.0, ac[p] + pt_c[p] * dt) * C.to_vmr[2 + p]);
+    f.qi[p] = dmax(0.0, dmax(0.0, f.ai[p] + pt_i[p] * dt) * C.to_vmr[2 + p]);
+    f.qc[p] = dmax(0.0, dmax(0.0, f.ac[p] + pt_c[p] * dt) * C.to_vmr[2 + p]);
   }
-  const double g_h2so4 = dmax(0.0, h2so4 * C.to_vmr[0]);
-  const double g_soag = dmax(0.0, soag * C.to_vmr[1]);
-
-  // -------------------------------------------------------- amicphys
-  double wetdens[NMODE];
+  f.g_h2so4 = dmax(0.0, f.h2so4 * C.to_vmr[0]);
+  f.g_soag = dmax(0.0, f.soag * C.to_vmr[1]);
 #pragma unroll
   for (int m = 0; m < NMODE; ++m)
-    wetdens[m] = dmax(1000.0, wetdens_wu[m]);
+    f.wetdens[m] = dmax(1000.0, wetdens_wu[m]);
   const double epsqs = 0.018016 / 0.028966;
-  const double tc = temp - 273.15;
+  const double tc = f.temp - 273.15;
   const double ew = 610.94 * exp(17.625 * tc / (234.04 + tc));
-  const double ev_sat = 1.00071 * exp(4.5e-8 * pmid) * ew;
-  const double qv_sat = epsqs * ev_sat / (pmid - (1 - epsqs) * ev_sat);
-  const double relhumgcm = dmax(0.0, dmin(1.0, qv / qv_sat));
+  const double ev_sat = 1.00071 * exp(4.5e-8 * f.pmid) * ew;
+  const double qv_sat = epsqs * ev_sat / (f.pmid - (1 - epsqs) * ev_sat);
+  f.relhumgcm = dmax(0.0, dmin(1.0, f.qv / qv_sat));
+}
 
+// Sub-area fields of a Sub from populations with per-mode factors
+// (number, mass), as the subarea set-up does (mam4_amicphys.hpp:460-560).
+__device__ __forceinline__ void load_sub(Sub &s, const double (&q)[NPOP],
+                                         const double (&fac_num)[NMODE],
+                                         const double (&fac_mass)[NMODE]) {
+#pragma unroll
+  for (int m = 0; m < NMODE; ++m) {
+    s.num[m] = (q[K::numslot(m)] * fac_num[m]) * 1;
+#pragma unroll
+    for (int x = 0; x < NAER; ++x) {
+      const int slot = K::aer_slot(x, m);
+      s.aer[x][m] = (slot >= 0) ? (q[slot] * fac_mass[m]) * K::fcvt_aer(x) : 0.0;
+    }
+  }
+}
+__device__ __forceinline__ void load_sub_plain(Sub &s, const double (&q)[NPOP]) {
+#pragma unroll
+  for (int m = 0; m < NMODE; ++m) {
+    s.num[m] = q[K::numslot(m)] * 1;
+#pragma unroll
+    for (int x = 0; x < NAER; ++x) {
+      const int slot = K::aer_slot(x, m);
+      s.aer[x][m] = (slot >= 0) ? q[slot] * K::fcvt_aer(x) : 0.0;
+    }
+  }
+}
+
+// Renaming of a cloudy (sub)area, interstitial si and cloud-borne sc,
+// weighted by f; adds the renaming diagnostics when DIAG.
+template <bool DIAG>
+__device__ __forceinline__ void cloudy_rename(const StepArgs &a, Sub &si, Sub &sc, double f,
+                                              Diag *dg) {
+  const StepConsts &C = c_k;
+  si.gas[0] = si.gas[1] = sc.gas[0] = sc.gas[1] = 0.0;
+  double nsv_i[NMODE], nsv_c[NMODE], asv_i[NAER][NMODE], asv_c[NAER][NMODE];
+  if (DIAG) {
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      nsv_i[m] = si.num[m];
+      nsv_c[m] = sc.num[m];
+#pragma unroll
+      for (int x = 0; x < NAER; ++x) {
+        asv_i[x][m] = si.aer[x][m];
+        asv_c[x][m] = sc.aer[x][m];
+      }
+    }
+  }
+  if (a.do_rename) {
+    const double zero7[NAER] = {0, 0, 0, 0, 0, 0, 0};
+    rename_subarea<true>(C, si, sc, zero7, zero7);
+  }
+  if (DIAG && a.do_rename) {
+    const double dt = a.dt;
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      const int ln = num_i31(m);
+      dg->t[1][ln] += ((0.0 + (si.num[m] - nsv_i[m])) / (1.0 * dt)) * f;
+      dg->cw[ln] += ((0.0 + (sc.num[m] - nsv_c[m])) / (1.0 * dt)) * f;
+#pragma unroll
+      for (int x = 0; x < NAER; ++x) {
+        const int slot = K::aer_slot(x, m);
+        if (slot >= 0) {
+          dg->t[1][pop_to_i31(slot)] +=
+              ((0.0 + (si.aer[x][m] - asv_i[x][m])) / (K::fcvt_aer(x) * dt)) * f;
+          dg->cw[pop_to_i31(slot)] +=
+              ((0.0 + (sc.aer[x][m] - asv_c[x][m])) / (K::fcvt_aer(x) * dt)) * f;
+        }
+      }
+    }
+  }
+}
+
+// Cloudy grid cell (cloud fraction > 0.999): renaming only.
+template <bool DIAG>
+__device__ __forceinline__ void cloudy_cell(const StepArgs &a, const Front &f, double &o_h2so4,
+                                            double &o_soag, double (&oi)[NPOP],
+                                            double (&oc)[NPOP], Diag *dg) {
+  Sub si, sc;
+  load_sub_plain(si, f.qi);
+  load_sub_plain(sc, f.qc);
+  const double w = 1.0;
+  cloudy_rename<DIAG>(a, si, sc, w, dg);
+  o_soag = dmax(0.0, 0.0 + f.g_soag * w);
+  o_h2so4 = dmax(0.0, 0.0 + f.g_h2so4 * w);
+#pragma unroll
+  for (int m = 0; m < NMODE; ++m) {
+    oi[K::numslot(m)] = dmax(0.0, 0.0 + (si.num[m] / 1.0) * w);
+    oc[K::numslot(m)] = 0.0 + (sc.num[m] / 1.0) * w;
+#pragma unroll
+    for (int x = 0; x < NAER; ++x) {
+      const int slot = K::aer_slot(x, m);
+      if (slot >= 0) {
+        oi[slot] = dmax(0.0, 0.0 + (si.aer[x][m] / K::fcvt_aer(x)) * w);
+        oc[slot] = 0.0 + (sc.aer[x][m] / K::fcvt_aer(x)) * w;
+      }
+    }
+  }
+}
+
+// Partly cloudy grid cell, set-up of both subareas and the cloudy one
+// (jsub 2, renaming only): the clear subarea's incoming state s, its gases
+// and relative humidity, and the cloudy subarea's contributions to the
+// grid means (ci interstitial, cg gases SOAG/H2SO4, oc cloud-borne).
+// Partition factors: get_partition_factors (mam4_amicphys.hpp:414-449).
+template <bool DIAG>
+__device__ __forceinline__ void partly_cloudy_setup(const StepArgs &a, const Front &f, Sub &s,
+                                                    double (&gcl)[2], double &rhc,
+                                                    double (&ci)[NPOP], double (&cg)[2],
+                                                    double (&oc)[NPOP], Diag *dg) {
+  const StepConsts &C = c_k;
+  const double fcldy = f.cld, fclea = 1.0 - fcldy;
+  double fn_c[NMODE], fn_y[NMODE], fm_c[NMODE], fm_y[NMODE];
+  auto part = [&](double q_i, double q_c, double &fc, double &fy) {
+    const double cldbrn_cldy = q_c / fcldy;
+    const double intrst_cldy = dmax(0.0, ((q_i + q_c) - cldbrn_cldy));
+    const double intrst_clea = (q_i - fcldy * intrst_cldy) / fclea;
+    double r = dmax(1.e-35, intrst_clea * fclea) / dmax(1.e-35, q_i);
+    r = dmax(0.0, dmin(1.0, r));
+    fc = r / fclea;
+    fy = (1 - r) / fcldy;
+  };
+#pragma unroll
+  for (int m = 0; m < NMODE; ++m) {
+    part(f.qi[K::numslot(m)], f.qc[K::numslot(m)], fn_c[m], fn_y[m]);
+    double si_ = 0.0, sc_ = 0.0;
+#pragma unroll
+    for (int k = 0; k < K::nspec(m); ++k) {
+      si_ = si_ + f.qi[K::spec0(m) + k];
+      sc_ = sc_ + f.qc[K::spec0(m) + k];
+    }
+    part(si_, sc_, fm_c[m], fm_y[m]);
+  }
+  // gases: clear keeps the grid mean, cloudy gets the remainder
+  double gcy[2];
+  gcl[0] = f.g_soag;
+  gcl[1] = f.g_h2so4;
+#pragma unroll
+  for (int g = 0; g < 2; ++g) {
+    gcy[g] = (gcl[g] - fclea * gcl[g]) / fcldy;
+    if (gcy[g] < 0) {
+      gcy[g] = 0;
+      gcl[g] = gcl[g] / fclea;
+    }
+  }
+  rhc = bound(0.0, 1.0, (f.relhumgcm - fcldy) / fclea);
+  {
+    Sub si, sc;
+    load_sub(si, f.qi, fn_y, fm_y);
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      sc.num[m] = (f.qc[K::numslot(m)] / fcldy) * 1;
+#pragma unroll
+      for (int x = 0; x < NAER; ++x) {
+        const int slot = K::aer_slot(x, m);
+        sc.aer[x][m] = (slot >= 0) ? (f.qc[slot] / fcldy) * K::fcvt_aer(x) : 0.0;
+      }
+    }
+    cloudy_rename<DIAG>(a, si, sc, fcldy, dg);
+    cg[0] = gcy[0] * fcldy;
+    cg[1] = gcy[1] * fcldy;
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      ci[K::numslot(m)] = (si.num[m] / 1.0) * fcldy;
+      oc[K::numslot(m)] = (0.0 + 0.0 * fclea) + (sc.num[m] / 1.0) * fcldy;
+#pragma unroll
+      for (int x = 0; x < NAER; ++x) {
+        const int slot = K::aer_slot(x, m);
+        if (slot >= 0) {
+          ci[slot] = (si.aer[x][m] / K::fcvt_aer(x)) * fcldy;
+          oc[slot] = (0.0 + 0.0 * fclea) + (sc.aer[x][m] / K::fcvt_aer(x)) * fcldy;
+        }
+      }
+    }
+  }
+  load_sub(s, f.qi, fn_c, fm_c);
+  s.gas[0] = gcl[0] * C.fcvt_soag;
+  s.gas[1] = gcl[1] * 1.0;
+}
+
+// One grid cell start to end in one thread (modal_aero_amicphys_intr,
+// mam4_amicphys.hpp:2120-2376): the diagnostics path, and the whole step
+// when condensation is off (no SOA loop to pipeline).
+template <bool DIAG>
+__device__ __forceinline__ void cell_step(const StepArgs &a, const long long c) {
+  const StepConsts &C = c_k;
+  Front f;
+  cell_front(a, c, f);
+  const double dt = a.dt;
   Diag dgv;
   Diag *dg = DIAG ? &dgv : nullptr;
   if (DIAG) {
@@ -463,365 +651,83 @@ __device__ __forceinline__ void cell_step(const StepArgs &a, const long long c) 
     for (int i = 0; i < 31; ++i)
       dgv.cw[i] = 0.0;
   }
-
   // outgoing grid-cell means (amicphys units): gases, interstitial, cloud
   double o_h2so4, o_soag, oi[NPOP], oc[NPOP];
   const double fsoag = C.fcvt_soag;
   const bool map_gas = a.do_cond || a.do_newnuc;
-  const bool defer = (PHASE == PHASE_PRE) && a.do_cond && !(cld > 0.999);
+  const double qgas1[2] = {f.g_soag * fsoag, f.g_h2so4 * 1.0};
 
-  auto load_sub = [&](Sub &s, const double (&q)[NPOP], const double (&fac_num)[NMODE],
-                      const double (&fac_mass)[NMODE]) {
-#pragma unroll
-    for (int m = 0; m < NMODE; ++m) {
-      s.num[m] = (q[K::numslot(m)] * fac_num[m]) * 1;
-#pragma unroll
-      for (int x = 0; x < NAER; ++x) {
-        const int slot = K::aer_slot(x, m);
-        s.aer[x][m] = (slot >= 0) ? (q[slot] * fac_mass[m]) * K::fcvt_aer(x) : 0.0;
-      }
-    }
-  };
-  // queue the cell: solver state and hand-off at the start of the SOA loop
-  auto hand_off = [&](const Sub &s, const ClearMid &cm, const double (&uptk0)[NMODE],
-                      double relhum) {
-    SoaState st;
-    soa_init(st, (double)(int)(dt / 1), temp, pmid, s, uptk0);
-    const bool long_loop = soa_first_rate(st) * st.dtfull > 0.05 * kLongLoopSteps;
-    // warp-aggregated appends: the slot (in discovery order, which keeps
-    // the post kernel's cell accesses coalesced) and the solver order entry
-    const unsigned m = __activemask();
-    const int lane = threadIdx.x & 31;
-    const int leader = __ffs(m) - 1;
-    const unsigned m_long = __ballot_sync(m, long_loop), m_short = m & ~m_long;
-    unsigned base = 0, b_long = 0, b_short = 0;
-    if (lane == leader) {
-      base = atomicAdd(&a.counters[CNT_QUEUED], (unsigned)__popc(m));
-      if (m_long)
-        b_long = atomicAdd(&a.counters[CNT_LONG], (unsigned)__popc(m_long));
-      if (m_short)
-        b_short = atomicAdd(&a.counters[CNT_SHORT], (unsigned)__popc(m_short));
-    }
-    base = __shfl_sync(m, base, leader);
-    b_long = __shfl_sync(m, b_long, leader);
-    b_short = __shfl_sync(m, b_short, leader);
-    const unsigned below = (1u << lane) - 1;
-    const unsigned slot = base + __popc(m & below);
-    a.task[slot] = (int)c;
-    if (long_loop)
-      a.order[b_long + __popc(m_long & below)] = (int)slot;
-    else
-      a.order[a.ncell - 1 - (b_short + __popc(m_short & below))] = (int)slot;
-    const size_t n = (size_t)a.ncell;
-    double *q = a.soa + slot;
-    q[SOA_G * n] = st.g;
-#pragma unroll
-    for (int k = 0; k < NMODE; ++k) {
-      q[(SOA_A + k) * n] = st.a[k];
-      q[(SOA_OPOA + k) * n] = st.opoa[k];
-      q[(SOA_UPTK + k) * n] = st.uptk[k];
-    }
-    q[SOA_G0 * n] = st.g0;
-    double *h = a.hand + slot;
-    h[H_GAS1 * n] = s.gas[1];
-    double pop[NPOP];
-    sub_to_pop(s, pop);
-#pragma unroll
-    for (int p = 0; p < NPOP; ++p)
-      h[(H_POP + p) * n] = pop[p];
-#pragma unroll
-    for (int k = 0; k < NMODE; ++k) {
-      h[(H_UPTK + k) * n] = cm.uptk1[k];
-      h[(H_AWET + k) * n] = dgn_awet[k];
-      h[(H_WETD + k) * n] = wetdens[k];
-    }
-    h[H_NETPROD * n] = cm.netprod1;
-    h[H_SV_SO4 * n] = cm.sv_so4_ait;
-    h[H_SV_SOA * n] = cm.sv_soa_ait;
-    h[H_DGN_PC * n] = dgn_a[3];
-    h[H_RELHUM * n] = relhum;
-    return slot;
-  };
-
-  if (cld < 1.0e-5) {
-    // ------------------------------------------- clear grid cell
+  if (f.cld > 0.999) {
+    cloudy_cell<DIAG>(a, f, o_h2so4, o_soag, oi, oc, dg);
+  } else if (f.cld < 1.0e-5) {
+    // clear grid cell: the subarea is the grid mean
     Sub s;
-#pragma unroll
-    for (int m = 0; m < NMODE; ++m) {
-      s.num[m] = qi[K::numslot(m)] * 1;
-#pragma unroll
-      for (int x = 0; x < NAER; ++x) {
-        const int slot = K::aer_slot(x, m);
-        s.aer[x][m] = (slot >= 0) ? qi[slot] * K::fcvt_aer(x) : 0.0;
-      }
-    }
-    s.gas[0] = g_soag * fsoag;
-    s.gas[1] = g_h2so4 * 1.0;
-    const double qgas1[2] = {s.gas[0], s.gas[1]};
-    if (defer) {
-      ClearMid cm;
-      double uptk0[NMODE];
-      clear_prefix<false>(a, dt, temp, pmid, dgn_awet, qgas1, s, cm, uptk0);
-      const unsigned slot = hand_off(s, cm, uptk0, relhumgcm);
-      double *h = a.hand + slot;
-      const size_t n = (size_t)a.ncell;
-#pragma unroll
-      for (int p = 0; p < NPOP; ++p)
-        h[(H_OC + p) * n] = qc[p];
-      return;
-    }
-    const int niter = clear_subarea<DIAG, PHASE == PHASE_FULL>(a, dt, temp, pmid, zm, pblh, relhumgcm, dgn_a,
-                                          dgn_awet, wetdens, qgas1, s, dg, 1.0);
+    load_sub_plain(s, f.qi);
+    s.gas[0] = f.g_soag * fsoag;
+    s.gas[1] = f.g_h2so4 * 1.0;
+    const int niter = clear_subarea<DIAG>(a, dt, f.temp, f.pmid, f.zm, f.pblh, f.relhumgcm,
+                                                f.dgn_a, f.dgn_awet, f.wetdens, qgas1, s, dg, 1.0);
     if (niter > 1000)
       atomicOr(a.flags, MAM4B_FLAG_SOA_NITER_LIMIT);
-    const double f = 1.0 - 0.0;
-    o_soag = dmax(0.0, 0.0 + (map_gas ? s.gas[0] / fsoag : g_soag) * f);
-    o_h2so4 = dmax(0.0, 0.0 + (map_gas ? s.gas[1] / 1.0 : g_h2so4) * f);
+    const double w = 1.0 - 0.0;
+    o_soag = dmax(0.0, 0.0 + (map_gas ? s.gas[0] / fsoag : f.g_soag) * w);
+    o_h2so4 = dmax(0.0, 0.0 + (map_gas ? s.gas[1] / 1.0 : f.g_h2so4) * w);
 #pragma unroll
     for (int m = 0; m < NMODE; ++m) {
-      oi[K::numslot(m)] = dmax(0.0, 0.0 + (s.num[m] / 1.0) * f);
+      oi[K::numslot(m)] = dmax(0.0, 0.0 + (s.num[m] / 1.0) * w);
 #pragma unroll
       for (int x = 0; x < NAER; ++x) {
         const int slot = K::aer_slot(x, m);
         if (slot >= 0)
-          oi[slot] = dmax(0.0, 0.0 + (s.aer[x][m] / K::fcvt_aer(x)) * f);
+          oi[slot] = dmax(0.0, 0.0 + (s.aer[x][m] / K::fcvt_aer(x)) * w);
       }
     }
 #pragma unroll
     for (int p = 0; p < NPOP; ++p)
-      oc[p] = qc[p];
-  } else if (cld > 0.999) {
-    // ------------------------------------------ cloudy grid cell
-    Sub si, sc;
-#pragma unroll
-    for (int m = 0; m < NMODE; ++m) {
-      si.num[m] = qi[K::numslot(m)] * 1;
-      sc.num[m] = qc[K::numslot(m)] * 1;
-#pragma unroll
-      for (int x = 0; x < NAER; ++x) {
-        const int slot = K::aer_slot(x, m);
-        si.aer[x][m] = (slot >= 0) ? qi[slot] * K::fcvt_aer(x) : 0.0;
-        sc.aer[x][m] = (slot >= 0) ? qc[slot] * K::fcvt_aer(x) : 0.0;
-      }
-    }
-    si.gas[0] = si.gas[1] = sc.gas[0] = sc.gas[1] = 0.0;
-    double nsv_i[NMODE], nsv_c[NMODE], asv_i[NAER][NMODE], asv_c[NAER][NMODE];
+      oc[p] = f.qc[p];
+  } else {
+    // partly cloudy grid cell: cloudy subarea first (its contributions are
+    // added after the clear subarea's, as in the reference's jsub order)
+    const double fclea = 1.0 - f.cld;
+    Sub s;
+    double gcl[2], rhc, ci[NPOP], cg[2];
+    partly_cloudy_setup<DIAG>(a, f, s, gcl, rhc, ci, cg, oc, dg);
+    Diag dclear;
+    Diag *dcp = DIAG ? &dclear : nullptr;
     if (DIAG) {
 #pragma unroll
-      for (int m = 0; m < NMODE; ++m) {
-        nsv_i[m] = si.num[m];
-        nsv_c[m] = sc.num[m];
+      for (int k = 0; k < NQTEND; ++k)
 #pragma unroll
-        for (int x = 0; x < NAER; ++x) {
-          asv_i[x][m] = si.aer[x][m];
-          asv_c[x][m] = sc.aer[x][m];
-        }
-      }
+        for (int i = 0; i < 31; ++i)
+          dclear.t[k][i] = 0.0;
     }
-    if (a.do_rename) {
-      const double zero7[NAER] = {0, 0, 0, 0, 0, 0, 0};
-      rename_subarea<true>(C, si, sc, zero7, zero7);
+    const int niter = clear_subarea<DIAG>(a, dt, f.temp, f.pmid, f.zm, f.pblh, rhc, f.dgn_a,
+                                                f.dgn_awet, f.wetdens, qgas1, s, dcp, fclea);
+    if (niter > 1000)
+      atomicOr(a.flags, MAM4B_FLAG_SOA_NITER_LIMIT);
+    if (DIAG) {
+      // jsub 1 then jsub 2: t = (0 + clear) + cloudy
+#pragma unroll
+      for (int k = 0; k < NQTEND; ++k)
+#pragma unroll
+        for (int i = 0; i < 31; ++i)
+          dgv.t[k][i] = dclear.t[k][i] + dgv.t[k][i];
     }
-    const double f = 1.0;
-    o_soag = dmax(0.0, 0.0 + g_soag * f);
-    o_h2so4 = dmax(0.0, 0.0 + g_h2so4 * f);
+    o_soag = dmax(0.0, (0.0 + (map_gas ? s.gas[0] / fsoag : gcl[0]) * fclea) + cg[0]);
+    o_h2so4 = dmax(0.0, (0.0 + (map_gas ? s.gas[1] / 1.0 : gcl[1]) * fclea) + cg[1]);
 #pragma unroll
     for (int m = 0; m < NMODE; ++m) {
-      oi[K::numslot(m)] = dmax(0.0, 0.0 + (si.num[m] / 1.0) * f);
-      oc[K::numslot(m)] = 0.0 + (sc.num[m] / 1.0) * f;
+      oi[K::numslot(m)] = dmax(0.0, (0.0 + (s.num[m] / 1.0) * fclea) + ci[K::numslot(m)]);
 #pragma unroll
       for (int x = 0; x < NAER; ++x) {
         const int slot = K::aer_slot(x, m);
-        if (slot >= 0) {
-          oi[slot] = dmax(0.0, 0.0 + (si.aer[x][m] / K::fcvt_aer(x)) * f);
-          oc[slot] = 0.0 + (sc.aer[x][m] / K::fcvt_aer(x)) * f;
-        }
-      }
-    }
-    if (DIAG && a.do_rename) {
-#pragma unroll
-      for (int m = 0; m < NMODE; ++m) {
-        const int ln = num_i31(m);
-        dgv.t[1][ln] += ((0.0 + (si.num[m] - nsv_i[m])) / (1.0 * dt)) * f;
-        dgv.cw[ln] += ((0.0 + (sc.num[m] - nsv_c[m])) / (1.0 * dt)) * f;
-#pragma unroll
-        for (int x = 0; x < NAER; ++x) {
-          const int slot = K::aer_slot(x, m);
-          if (slot >= 0) {
-            dgv.t[1][pop_to_i31(slot)] +=
-                ((0.0 + (si.aer[x][m] - asv_i[x][m])) / (K::fcvt_aer(x) * dt)) * f;
-            dgv.cw[pop_to_i31(slot)] +=
-                ((0.0 + (sc.aer[x][m] - asv_c[x][m])) / (K::fcvt_aer(x) * dt)) * f;
-          }
-        }
-      }
-    }
-  } else {
-    // ------------------------------------- partly cloudy grid cell
-    const double fcldy = cld, fclea = 1.0 - fcldy;
-    // interstitial partition factors per mode (get_partition_factors,
-    // mam4_amicphys.hpp:414-449), number and mass separately
-    double fn_c[NMODE], fn_y[NMODE], fm_c[NMODE], fm_y[NMODE];
-    auto part = [&](double q_i, double q_c, double &fc, double &fy) {
-      const double cldbrn_cldy = q_c / fcldy;
-      const double intrst_cldy = dmax(0.0, ((q_i + q_c) - cldbrn_cldy));
-      const double intrst_clea = (q_i - fcldy * intrst_cldy) / fclea;
-      double r = dmax(1.e-35, intrst_clea * fclea) / dmax(1.e-35, q_i);
-      r = dmax(0.0, dmin(1.0, r));
-      fc = r / fclea;
-      fy = (1 - r) / fcldy;
-    };
-#pragma unroll
-    for (int m = 0; m < NMODE; ++m) {
-      part(qi[K::numslot(m)], qc[K::numslot(m)], fn_c[m], fn_y[m]);
-      double si_ = 0.0, sc_ = 0.0;
-#pragma unroll
-      for (int s = 0; s < K::nspec(m); ++s) {
-        si_ = si_ + qi[K::spec0(m) + s];
-        sc_ = sc_ + qc[K::spec0(m) + s];
-      }
-      part(si_, sc_, fm_c[m], fm_y[m]);
-    }
-    // gases: clear keeps the grid mean, cloudy gets the remainder
-    double gcl[2] = {g_soag, g_h2so4}, gcy[2];
-#pragma unroll
-    for (int g = 0; g < 2; ++g) {
-      gcy[g] = (gcl[g] - fclea * gcl[g]) / fcldy;
-      if (gcy[g] < 0) {
-        gcy[g] = 0;
-        gcl[g] = gcl[g] / fclea;
-      }
-    }
-    const double rhc = bound(0.0, 1.0, (relhumgcm - fcldy) / fclea);
-    // cloudy subarea (jsub 2): renaming only; its contributions to the
-    // grid means are added after the clear subarea's
-    double ci[NPOP], cg[2];
-    {
-      Sub si, sc;
-      load_sub(si, qi, fn_y, fm_y);
-#pragma unroll
-      for (int m = 0; m < NMODE; ++m) {
-        sc.num[m] = (qc[K::numslot(m)] / fcldy) * 1;
-#pragma unroll
-        for (int x = 0; x < NAER; ++x) {
-          const int slot = K::aer_slot(x, m);
-          sc.aer[x][m] = (slot >= 0) ? (qc[slot] / fcldy) * K::fcvt_aer(x) : 0.0;
-        }
-      }
-      si.gas[0] = si.gas[1] = sc.gas[0] = sc.gas[1] = 0.0;
-      double nsv_i[NMODE], nsv_c[NMODE], asv_i[NAER][NMODE], asv_c[NAER][NMODE];
-      if (DIAG) {
-#pragma unroll
-        for (int m = 0; m < NMODE; ++m) {
-          nsv_i[m] = si.num[m];
-          nsv_c[m] = sc.num[m];
-#pragma unroll
-          for (int x = 0; x < NAER; ++x) {
-            asv_i[x][m] = si.aer[x][m];
-            asv_c[x][m] = sc.aer[x][m];
-          }
-        }
-      }
-      if (a.do_rename) {
-        const double zero7[NAER] = {0, 0, 0, 0, 0, 0, 0};
-        rename_subarea<true>(C, si, sc, zero7, zero7);
-      }
-      cg[0] = gcy[0] * fcldy;
-      cg[1] = gcy[1] * fcldy;
-#pragma unroll
-      for (int m = 0; m < NMODE; ++m) {
-        ci[K::numslot(m)] = (si.num[m] / 1.0) * fcldy;
-        oc[K::numslot(m)] = (0.0 + 0.0 * fclea) + (sc.num[m] / 1.0) * fcldy;
-#pragma unroll
-        for (int x = 0; x < NAER; ++x) {
-          const int slot = K::aer_slot(x, m);
-          if (slot >= 0) {
-            ci[slot] = (si.aer[x][m] / K::fcvt_aer(x)) * fcldy;
-            oc[slot] = (0.0 + 0.0 * fclea) + (sc.aer[x][m] / K::fcvt_aer(x)) * fcldy;
-          }
-        }
-      }
-      if (DIAG && a.do_rename) {
-#pragma unroll
-        for (int m = 0; m < NMODE; ++m) {
-          const int ln = num_i31(m);
-          dgv.t[1][ln] += ((0.0 + (si.num[m] - nsv_i[m])) / (1.0 * dt)) * fcldy;
-          dgv.cw[ln] += ((0.0 + (sc.num[m] - nsv_c[m])) / (1.0 * dt)) * fcldy;
-#pragma unroll
-          for (int x = 0; x < NAER; ++x) {
-            const int slot = K::aer_slot(x, m);
-            if (slot >= 0) {
-              dgv.t[1][pop_to_i31(slot)] +=
-                  ((0.0 + (si.aer[x][m] - asv_i[x][m])) / (K::fcvt_aer(x) * dt)) * fcldy;
-              dgv.cw[pop_to_i31(slot)] +=
-                  ((0.0 + (sc.aer[x][m] - asv_c[x][m])) / (K::fcvt_aer(x) * dt)) * fcldy;
-            }
-          }
-        }
-      }
-    }
-    // clear subarea (jsub 1); in the diagnostics path its increments are
-    // accumulated before the cloudy subarea's, as in the reference
-    {
-      Sub s;
-      load_sub(s, qi, fn_c, fm_c);
-      s.gas[0] = gcl[0] * fsoag;
-      s.gas[1] = gcl[1] * 1.0;
-      const double qgas1[2] = {g_soag * fsoag, g_h2so4 * 1.0};
-      if (defer) {
-        ClearMid cm;
-        double uptk0[NMODE];
-        clear_prefix<false>(a, dt, temp, pmid, dgn_awet, qgas1, s, cm, uptk0);
-        const unsigned slot = hand_off(s, cm, uptk0, rhc);
-        double *h = a.hand + slot;
-        const size_t n = (size_t)a.ncell;
-#pragma unroll
-        for (int p = 0; p < NPOP; ++p) {
-          h[(H_OC + p) * n] = oc[p];
-          h[(H_CI + p) * n] = ci[p];
-        }
-        h[H_CG * n] = cg[0];
-        h[(H_CG + 1) * n] = cg[1];
-        return;
-      }
-      Diag dclear;
-      Diag *dcp = DIAG ? &dclear : nullptr;
-      if (DIAG) {
-#pragma unroll
-        for (int k = 0; k < NQTEND; ++k)
-#pragma unroll
-          for (int i = 0; i < 31; ++i)
-            dclear.t[k][i] = 0.0;
-      }
-      const int niter = clear_subarea<DIAG, PHASE == PHASE_FULL>(a, dt, temp, pmid, zm, pblh, rhc, dgn_a, dgn_awet,
-                                            wetdens, qgas1, s, dcp, fclea);
-      if (niter > 1000)
-        atomicOr(a.flags, MAM4B_FLAG_SOA_NITER_LIMIT);
-      if (DIAG) {
-        // jsub 1 then jsub 2: t = (0 + clear) + cloudy
-#pragma unroll
-        for (int k = 0; k < NQTEND; ++k)
-#pragma unroll
-          for (int i = 0; i < 31; ++i)
-            dgv.t[k][i] = dclear.t[k][i] + dgv.t[k][i];
-      }
-      o_soag = dmax(0.0, (0.0 + (map_gas ? s.gas[0] / fsoag : gcl[0]) * fclea) + cg[0]);
-      o_h2so4 = dmax(0.0, (0.0 + (map_gas ? s.gas[1] / 1.0 : gcl[1]) * fclea) + cg[1]);
-#pragma unroll
-      for (int m = 0; m < NMODE; ++m) {
-        oi[K::numslot(m)] = dmax(0.0, (0.0 + (s.num[m] / 1.0) * fclea) + ci[K::numslot(m)]);
-#pragma unroll
-        for (int x = 0; x < NAER; ++x) {
-          const int slot = K::aer_slot(x, m);
-          if (slot >= 0)
-            oi[slot] = dmax(0.0, (0.0 + (s.aer[x][m] / K::fcvt_aer(x)) * fclea) + ci[slot]);
-        }
+        if (slot >= 0)
+          oi[slot] = dmax(0.0, (0.0 + (s.aer[x][m] / K::fcvt_aer(x)) * fclea) + ci[slot]);
       }
     }
   }
 
-  // ---------------------------------------------------------- outputs
-  store_outputs(a, c, o_h2so4, o_soag, oi, oc, h2so4, soag, ai, ac);
+  store_outputs(a, c, o_h2so4, o_soag, oi, oc, f.h2so4, f.soag, f.ai, f.ac);
   if (DIAG) {
 #pragma unroll
     for (int k = 0; k < NQTEND; ++k)
@@ -833,6 +739,112 @@ __device__ __forceinline__ void cell_step(const StepArgs &a, const long long c) 
     for (int i = 0; i < 31; ++i)
       if (a.diag[4 * 31 + i])
         a.diag[4 * 31 + i][c] = dgv.cw[i];
+  }
+}
+
+// First half of the pipelined step (condensation on, no diagnostics): the
+// cell's front; cloudy cells finish here; every other cell sets up its
+// clear subarea (and, when partly cloudy, runs the cloudy one), runs the
+// clear subarea up to the SOA loop and hands the state at that point to the
+// solver and the post kernel. The clear-subarea part runs converged for
+// clear and partly cloudy cells alike.
+__device__ __forceinline__ void cell_pre(const StepArgs &a, const long long c) {
+  const StepConsts &C = c_k;
+  Front f;
+  cell_front(a, c, f);
+  const double dt = a.dt;
+  const double fsoag = C.fcvt_soag;
+  if (f.cld > 0.999) {
+    double o_h2so4, o_soag, oi[NPOP], oc[NPOP];
+    cloudy_cell<false>(a, f, o_h2so4, o_soag, oi, oc, nullptr);
+    store_outputs(a, c, o_h2so4, o_soag, oi, oc, f.h2so4, f.soag, f.ai, f.ac);
+    return;
+  }
+  const bool partly = !(f.cld < 1.0e-5);
+  Sub s;
+  double rh, oc[NPOP], ci[NPOP], cg[2];
+  if (!partly) {
+    load_sub_plain(s, f.qi);
+    s.gas[0] = f.g_soag * fsoag;
+    s.gas[1] = f.g_h2so4 * 1.0;
+    rh = f.relhumgcm;
+#pragma unroll
+    for (int p = 0; p < NPOP; ++p)
+      oc[p] = f.qc[p];
+  } else {
+    double gcl[2];
+    partly_cloudy_setup<false>(a, f, s, gcl, rh, ci, cg, oc, nullptr);
+  }
+  const double qgas1[2] = {f.g_soag * fsoag, f.g_h2so4 * 1.0};
+  ClearMid cm;
+  double uptk0[NMODE];
+  clear_prefix<false>(a, dt, f.temp, f.pmid, f.dgn_awet, qgas1, s, cm, uptk0);
+
+  // queue the cell: solver state and hand-off at the start of the SOA loop
+  SoaState st;
+  soa_init(st, (double)(int)(dt / 1), f.temp, f.pmid, s, uptk0);
+  const bool long_loop = soa_first_rate(st) * st.dtfull > 0.05 * kLongLoopSteps;
+  // warp-aggregated appends: the slot (in discovery order, which keeps the
+  // post kernel's cell accesses coalesced) and the solver order entry
+  const unsigned m = __activemask();
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(m) - 1;
+  const unsigned m_long = __ballot_sync(m, long_loop), m_short = m & ~m_long;
+  unsigned base = 0, b_long = 0, b_short = 0;
+  if (lane == leader) {
+    base = atomicAdd(&a.counters[CNT_QUEUED], (unsigned)__popc(m));
+    if (m_long)
+      b_long = atomicAdd(&a.counters[CNT_LONG], (unsigned)__popc(m_long));
+    if (m_short)
+      b_short = atomicAdd(&a.counters[CNT_SHORT], (unsigned)__popc(m_short));
+  }
+  base = __shfl_sync(m, base, leader);
+  b_long = __shfl_sync(m, b_long, leader);
+  b_short = __shfl_sync(m, b_short, leader);
+  const unsigned below = (1u << lane) - 1;
+  const unsigned slot = base + __popc(m & below);
+  a.task[slot] = (int)c;
+  if (long_loop)
+    a.order[b_long + __popc(m_long & below)] = (int)slot;
+  else
+    a.order[a.ncell - 1 - (b_short + __popc(m_short & below))] = (int)slot;
+  const size_t n = (size_t)a.ncell;
+  double *q = a.soa + slot;
+  q[SOA_G * n] = st.g;
+#pragma unroll
+  for (int k = 0; k < NMODE; ++k) {
+    q[(SOA_A + k) * n] = st.a[k];
+    q[(SOA_OPOA + k) * n] = st.opoa[k];
+    q[(SOA_UPTK + k) * n] = st.uptk[k];
+  }
+  q[SOA_G0 * n] = st.g0;
+  double *h = a.hand + slot;
+  h[H_GAS1 * n] = s.gas[1];
+  double pop[NPOP];
+  sub_to_pop(s, pop);
+#pragma unroll
+  for (int p = 0; p < NPOP; ++p)
+    h[(H_POP + p) * n] = pop[p];
+#pragma unroll
+  for (int k = 0; k < NMODE; ++k) {
+    h[(H_UPTK + k) * n] = cm.uptk1[k];
+    h[(H_AWET + k) * n] = f.dgn_awet[k];
+    h[(H_WETD + k) * n] = f.wetdens[k];
+  }
+  h[H_NETPROD * n] = cm.netprod1;
+  h[H_SV_SO4 * n] = cm.sv_so4_ait;
+  h[H_SV_SOA * n] = cm.sv_soa_ait;
+  h[H_DGN_PC * n] = f.dgn_a[3];
+  h[H_RELHUM * n] = rh;
+#pragma unroll
+  for (int p = 0; p < NPOP; ++p)
+    h[(H_OC + p) * n] = oc[p];
+  if (partly) {
+#pragma unroll
+    for (int p = 0; p < NPOP; ++p)
+      h[(H_CI + p) * n] = ci[p];
+    h[H_CG * n] = cg[0];
+    h[(H_CG + 1) * n] = cg[1];
   }
 }
 
@@ -929,13 +941,13 @@ template <bool DIAG>
 __global__ void __launch_bounds__(128) full_kernel(const __grid_constant__ StepArgs a) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c < a.ncell)
-    cell_step<DIAG, PHASE_FULL>(a, c);
+    cell_step<DIAG>(a, c);
 }
 
 __global__ void __launch_bounds__(128) pre_kernel(const __grid_constant__ StepArgs a) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c < a.ncell)
-    cell_step<false, PHASE_PRE>(a, c);
+    cell_pre(a, c);
 }
 
 __global__ void __launch_bounds__(128) post_kernel(const __grid_constant__ StepArgs a) {
@@ -1231,6 +1243,14 @@ cudaError_t launch_pipeline(mam4b_ctx *ctx, const StepArgs &a, cudaStream_t s) {
     return e;
   const int block = 128;
   const unsigned grid = (unsigned)((a.ncell + block - 1) / block);
+  if (!a.do_cond) {
+    // no SOA loop to pipeline
+    full_kernel<false><<<grid, block, 0, s>>>(a);
+    e = cudaGetLastError();
+    if (e == cudaSuccess)
+      ctx->launches += 1;
+    return e;
+  }
   pre_kernel<<<grid, block, 0, s>>>(a);
   soa_kernel<<<ctx->soa_grid, kSoaBlock, 0, s>>>(a);
   post_kernel<<<grid, block, 0, s>>>(a);
@@ -1612,9 +1632,14 @@ mam4b_status mam4b_step_slab_noalloc(const mam4b_config *cfg, const double *in_s
     return MAM4B_ERR_CUDA;
   const int block = 128;
   const unsigned grid = (unsigned)((ncell + block - 1) / block);
-  pre_kernel<<<grid, block, 0, s>>>(a);
-  soa_kernel<<<nd.soa_grid, kSoaBlock, 0, s>>>(a);
-  post_kernel<<<grid, block, 0, s>>>(a);
+  if (!a.do_cond) {
+    // no SOA loop to pipeline (and no scratch used)
+    full_kernel<false><<<grid, block, 0, s>>>(a);
+  } else {
+    pre_kernel<<<grid, block, 0, s>>>(a);
+    soa_kernel<<<nd.soa_grid, kSoaBlock, 0, s>>>(a);
+    post_kernel<<<grid, block, 0, s>>>(a);
+  }
   e = cudaGetLastError();
   return e == cudaSuccess ? MAM4B_OK : MAM4B_ERR_CUDA;
 }
