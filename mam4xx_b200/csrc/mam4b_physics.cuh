@@ -563,67 +563,88 @@ __device__ __forceinline__ double qsat_water(double t, double p) {
 
 // modal_aero_water_uptake_dr with wet density (water_uptake.hpp:362-480);
 // uses the state before the calcsize update, like the reference driver.
+// Relative humidity of the clear part of the cell:
+__device__ __forceinline__ double water_uptake_rh(double qv, double temp, double pmid,
+                                                  double cldn) {
+  const double qs = qsat_water(temp, pmid);
+  const double rh_max = 0.98;
+  double rh = (qs > qv) ? qv / qs : rh_max;
+  rh = bound(0.0, rh_max, rh);
+  if (cldn < 1.0)
+    rh = (rh - cldn) / (1.0 - cldn);
+  return dmax(rh, 0.0);
+}
+
+// One mode: sp holds its species masses in mode order (sp[0..nspec(m)-1]).
+template <int M>
+__device__ __forceinline__ void water_uptake_mode(const StepConsts &C, const double (&sp)[7],
+                                                  double rh, double dgn_a, double &dgn_awet,
+                                                  double &qaerwat, double &wetdens) {
+  double hygro = 0.0, dryvolmr = 0.0, maer = 0.0;
+#pragma unroll
+  for (int s = 0; s < K::nspec(M); ++s) {
+    const int w = K::spec0(M) + s - M;  // species index among the 21 masses
+    const double raer = sp[s];
+    const double vol_tmp = raer / K::wu_dens(w);
+    maer = maer + raer;
+    dryvolmr += vol_tmp;
+    hygro += vol_tmp * K::wu_hygro(w);
+  }
+  const int w0 = K::spec0(M) - M;
+  if (dryvolmr > 1e-30)
+    hygro = hygro / dryvolmr;
+  else
+    hygro = K::wu_hygro(w0);
+  const double v2ncur_a = 1.0 / ((K::pi / 6.0) * cube(dgn_a) * exp(4.5 * sq(C.log_sig[M])));
+  const double naer = dryvolmr * v2ncur_a;
+  const double drydens = (maer > 1e-31) ? maer / dryvolmr : 1.0;
+  const double dryvol = 1.0 / v2ncur_a;
+  const double drymass = drydens * dryvol;
+  const double dryrad = cbrt(dryvol / (K::pi * 4.0 / 3.0));
+  double wetrad = kohler(C, dryrad, hygro, rh);
+  wetrad = dmax(wetrad, dryrad);
+  double wetvol = (K::pi * 4.0 / 3.0) * cube(wetrad);
+  wetvol = dmax(wetvol, dryvol);
+  double wtrvol = wetvol - dryvol;
+  wtrvol = dmax(wtrvol, 0.0);
+  if (rh < K::rh_cryst) {
+    wetrad = dryrad;
+    wetvol = dryvol;
+    wtrvol = 0.0;
+  } else if (rh < K::rh_deliq) {
+    wtrvol = wtrvol * C.hystfac * (rh - K::rh_cryst);
+    wtrvol = dmax(wtrvol, 0.0);
+    wetvol = dryvol + wtrvol;
+    wetrad = cbrt(wetvol / (4.0 / 3.0 * K::pi));
+  }
+  dgn_awet = dgn_a * (wetrad / dryrad);
+  qaerwat = 1.0e3 * naer * wtrvol;
+  wetdens = (wetvol > 1.0e-30) ? (drymass + 1.0e3 * wtrvol) / wetvol : K::wu_dens(w0);
+}
+
+template <int M>
+__device__ __forceinline__ void mode_species(const double (&ai)[NPOP], double (&sp)[7]) {
+#pragma unroll
+  for (int s = 0; s < 7; ++s)
+    sp[s] = (s < K::nspec(M)) ? ai[K::spec0(M) + (s < K::nspec(M) ? s : 0)] : 0.0;
+}
+
 __device__ __forceinline__ void water_uptake(const StepConsts &C, const double (&ai)[NPOP],
                                              double qv, double temp, double pmid, double cldn,
                                              const double (&dgn_a)[NMODE],
                                              double (&dgn_awet)[NMODE],
                                              double (&qaerwat)[NMODE],
                                              double (&wetdens)[NMODE]) {
-  double rh;
-  {
-    const double qs = qsat_water(temp, pmid);
-    const double rh_max = 0.98;
-    rh = (qs > qv) ? qv / qs : rh_max;
-    rh = bound(0.0, rh_max, rh);
-    if (cldn < 1.0)
-      rh = (rh - cldn) / (1.0 - cldn);
-    rh = dmax(rh, 0.0);
-  }
-#pragma unroll
-  for (int m = 0; m < NMODE; ++m) {
-    double hygro = 0.0, dryvolmr = 0.0, maer = 0.0;
-#pragma unroll
-    for (int s = 0; s < K::nspec(m); ++s) {
-      const int slot = K::spec0(m) + s;
-      const int w = slot - m;  // species index among the 21 masses
-      const double raer = ai[slot];
-      const double vol_tmp = raer / K::wu_dens(w);
-      maer = maer + raer;
-      dryvolmr += vol_tmp;
-      hygro += vol_tmp * K::wu_hygro(w);
-    }
-    const int w0 = K::spec0(m) - m;
-    if (dryvolmr > 1e-30)
-      hygro = hygro / dryvolmr;
-    else
-      hygro = K::wu_hygro(w0);
-    const double v2ncur_a =
-        1.0 / ((K::pi / 6.0) * cube(dgn_a[m]) * exp(4.5 * sq(C.log_sig[m])));
-    const double naer = dryvolmr * v2ncur_a;
-    const double drydens = (maer > 1e-31) ? maer / dryvolmr : 1.0;
-    const double dryvol = 1.0 / v2ncur_a;
-    const double drymass = drydens * dryvol;
-    const double dryrad = cbrt(dryvol / (K::pi * 4.0 / 3.0));
-    double wetrad = kohler(C, dryrad, hygro, rh);
-    wetrad = dmax(wetrad, dryrad);
-    double wetvol = (K::pi * 4.0 / 3.0) * cube(wetrad);
-    wetvol = dmax(wetvol, dryvol);
-    double wtrvol = wetvol - dryvol;
-    wtrvol = dmax(wtrvol, 0.0);
-    if (rh < K::rh_cryst) {
-      wetrad = dryrad;
-      wetvol = dryvol;
-      wtrvol = 0.0;
-    } else if (rh < K::rh_deliq) {
-      wtrvol = wtrvol * C.hystfac * (rh - K::rh_cryst);
-      wtrvol = dmax(wtrvol, 0.0);
-      wetvol = dryvol + wtrvol;
-      wetrad = cbrt(wetvol / (4.0 / 3.0 * K::pi));
-    }
-    dgn_awet[m] = dgn_a[m] * (wetrad / dryrad);
-    qaerwat[m] = 1.0e3 * naer * wtrvol;
-    wetdens[m] = (wetvol > 1.0e-30) ? (drymass + 1.0e3 * wtrvol) / wetvol : K::wu_dens(w0);
-  }
+  const double rh = water_uptake_rh(qv, temp, pmid, cldn);
+  double sp[7];
+  mode_species<0>(ai, sp);
+  water_uptake_mode<0>(C, sp, rh, dgn_a[0], dgn_awet[0], qaerwat[0], wetdens[0]);
+  mode_species<1>(ai, sp);
+  water_uptake_mode<1>(C, sp, rh, dgn_a[1], dgn_awet[1], qaerwat[1], wetdens[1]);
+  mode_species<2>(ai, sp);
+  water_uptake_mode<2>(C, sp, rh, dgn_a[2], dgn_awet[2], qaerwat[2], wetdens[2]);
+  mode_species<3>(ai, sp);
+  water_uptake_mode<3>(C, sp, rh, dgn_a[3], dgn_awet[3], qaerwat[3], wetdens[3]);
 }
 
 // ============================================================== amicphys
@@ -635,37 +656,53 @@ struct Sub {
   double aer[NAER][NMODE];
 };
 
-// gasaerexch.hpp:255-353: uptake rate per unit number of each mode for a
-// gas with the given diffusivity and mean free path (accommodation 0.65)
-__device__ __forceinline__ void uptake_rates(const StepConsts &C, double gasdiffus,
-                                             double freepath, const double (&dgn_awet)[NMODE],
-                                             double (&uptk)[NMODE]) {
+// gasaerexch.hpp:255-353: uptake rate per unit number of mode n for a gas
+// with the given diffusivity and mean free path (accommodation 0.65)
+__device__ __forceinline__ double uptake_rate_mode(const StepConsts &C, int n, double gasdiffus,
+                                                   double freepath, double dgn_awet) {
   const double tworootpi = 2 * sqrt(K::pi);
   const double root2 = sqrt(2.0);
   const double xg = 7.071067690849304E-01;
   const double wg = 8.862269520759583E-01;
   const double a283 = 0.65 * 0.283, a75 = 0.65 * 0.75;
+  const double lnsg = C.log_sig[n];
+  const double lndpgn = log(dgn_awet);
+  const double kn = 2.0 * freepath / dgn_awet;
+  const double tmpa =
+      1.0 / (1.0 + kn) - (2.0 * kn + 1.0 + a283) / (kn * (kn + 1.0 + a283) + a75);
+  double beta = 1.0 - kn * tmpa;
+  beta = dmax(1.0, dmin(2.0, beta));
+  const double constant = tworootpi * exp(beta * lndpgn + 0.5 * pow(beta * lnsg, 2.0));
+  double sum = 0.0;
 #pragma unroll
-  for (int n = 0; n < NMODE; ++n) {
-    const double lnsg = C.log_sig[n];
-    const double lndpgn = log(dgn_awet[n]);
-    const double kn = 2.0 * freepath / dgn_awet[n];
-    const double tmpa =
-        1.0 / (1.0 + kn) - (2.0 * kn + 1.0 + a283) / (kn * (kn + 1.0 + a283) + a75);
-    double beta = 1.0 - kn * tmpa;
-    beta = dmax(1.0, dmin(2.0, beta));
-    const double constant = tworootpi * exp(beta * lndpgn + 0.5 * pow(beta * lnsg, 2.0));
-    double sum = 0.0;
-#pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const double lndp = lndpgn + beta * lnsg * lnsg + root2 * lnsg * (q == 0 ? xg : -xg);
-      const double dp = exp(lndp);
-      const double knq = 2.0 * freepath / dp;
-      const double hh = (a75 * (1.0 + knq)) / (knq * (knq + 1.0 + a283) + a75);
-      sum += wg * dp * hh / pow(dp, beta);
-    }
-    uptk[n] = constant * gasdiffus * sum;
+  for (int q = 0; q < 2; ++q) {
+    const double lndp = lndpgn + beta * lnsg * lnsg + root2 * lnsg * (q == 0 ? xg : -xg);
+    const double dp = exp(lndp);
+    const double knq = 2.0 * freepath / dp;
+    const double hh = (a75 * (1.0 + knq)) / (knq * (knq + 1.0 + a283) + a75);
+    sum += wg * dp * hh / pow(dp, beta);
   }
+  return constant * gasdiffus * sum;
+}
+
+__device__ __forceinline__ void uptake_rates(const StepConsts &C, double gasdiffus,
+                                             double freepath, const double (&dgn_awet)[NMODE],
+                                             double (&uptk)[NMODE]) {
+#pragma unroll
+  for (int n = 0; n < NMODE; ++n)
+    uptk[n] = uptake_rate_mode(C, n, gasdiffus, freepath, dgn_awet[n]);
+}
+
+// H2SO4 gas diffusivity and mean free path (gasaerexch.hpp:223-253,
+// 402-417)
+__device__ __forceinline__ void h2so4_diffusivity(double temp, double pmid, double &gas_diffus,
+                                                  double &freepath) {
+  const double p_in_atm = pmid / 1.013e5;
+  const double dgas = (1.0e-3 * pow(temp, 1.75) * sqrt(1. / 9.807840000000000E+01 + 0.035)) /
+                      (p_in_atm * pow((pow(4.288000000000000E+01, 1.0 / 3.0) + 2.7189), 2.0));
+  gas_diffus = dgas * 1.0e-4;
+  const double speed = 145.5 * sqrt(temp / 9.807840000000000E+01);
+  freepath = 3.0 * gas_diffus / speed;
 }
 
 // SOA gas-particle exchange: mam_soaexch_1subarea (gasaerexch_soaexch.hpp:

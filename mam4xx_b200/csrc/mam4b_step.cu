@@ -46,6 +46,7 @@ struct StepArgs {
   int *task;         // [ncell]: cell of each queue slot
   int *order;        // [ncell]: slots in solver order, long loops from the
                      // front, short ones from the back
+  double *aux;       // [AUX_FIELDS][ncell], indexed by cell (size/mode kernels)
   unsigned *counters;
 };
 
@@ -58,6 +59,10 @@ struct StepArgs {
 // cells from the hand-off and the loop result. Otherwise full_kernel runs
 // each cell start to end in one thread.
 enum { SOA_G = 0, SOA_A = 1, SOA_OPOA = 5, SOA_UPTK = 9, SOA_G0 = 13, SOA_FIELDS = 14 };
+// per-cell values from size_kernel and mode_kernel for the pre kernel:
+// relative humidity for water uptake, H2SO4 diffusivity and mean free path,
+// per-particle H2SO4 uptake rate of each mode
+enum { AUX_RH = 0, AUX_GDIFF = 1, AUX_FPATH = 2, AUX_RATE = 3, AUX_FIELDS = 7 };
 // queue counters: queued slots, slots handed to the solver, long and short
 // loops in the order list
 enum { CNT_QUEUED = 0, CNT_TAKEN = 1, CNT_LONG = 2, CNT_SHORT = 3, CNT_WORDS = 4 };
@@ -109,14 +114,14 @@ struct ClearMid {
 };
 
 // Clear subarea, mam_amicphys_1subarea (mam4_amicphys.hpp:1127-1697), part 1:
-// optaa-2 production split, H2SO4 diffusivity and uptake rates. Returns the
-// SOAG uptake rates for the SOA loop.
+// optaa-2 production split and H2SO4 uptake rates from the per-particle
+// rates `rate` (uptake_rates). Returns the SOAG uptake rates for the SOA
+// loop.
 template <bool DIAG>
 __device__ __forceinline__ void clear_prefix(const StepArgs &a, double deltat, double temp,
-                                             double pmid, const double (&dgn_awet)[NMODE],
+                                             double pmid, const double (&rate)[NMODE],
                                              const double (&qgas1)[2], Sub &s, ClearMid &cm,
                                              double (&uptk0)[NMODE]) {
-  const StepConsts &C = c_k;
   const double aircon = pmid / (8314.46759100000 * temp);
   cm.netprod1 = 0.0;
   if (a.do_cond && a.optaa == 2) {
@@ -136,17 +141,9 @@ __device__ __forceinline__ void clear_prefix(const StepArgs &a, double deltat, d
       for (int m = 0; m < NMODE; ++m)
         cm.sv_all[x][m] = s.aer[x][m];
   }
-  // H2SO4 gas diffusivity / mean free path (gasaerexch.hpp:223-253, 402-417)
-  const double p_in_atm = pmid / 1.013e5;
-  const double dgas = (1.0e-3 * pow(temp, 1.75) * sqrt(1. / 9.807840000000000E+01 + 0.035)) /
-                      (p_in_atm * pow((pow(4.288000000000000E+01, 1.0 / 3.0) + 2.7189), 2.0));
-  const double gas_diffus = dgas * 1.0e-4;
-  const double speed = 145.5 * sqrt(temp / 9.807840000000000E+01);
-  const double freepath = 3.0 * gas_diffus / speed;
-  uptake_rates(C, gas_diffus, freepath, dgn_awet, cm.uptk1);
 #pragma unroll
   for (int n = 0; n < NMODE; ++n) {
-    cm.uptk1[n] = cm.uptk1[n] * (s.num[n] * aircon);
+    cm.uptk1[n] = rate[n] * (s.num[n] * aircon);
     uptk0[n] = cm.uptk1[n] * 0.81;
   }
 }
@@ -334,8 +331,13 @@ __device__ __forceinline__ int clear_subarea(const StepArgs &a, double deltat, d
                                              const double (&qgas1)[2], Sub &s, Diag *dg,
                                              double afrac) {
   ClearMid cm;
-  double uptk0[NMODE];
-  clear_prefix<DIAG>(a, deltat, temp, pmid, dgn_awet, qgas1, s, cm, uptk0);
+  double uptk0[NMODE], rate[NMODE] = {0, 0, 0, 0};
+  if (a.do_cond) {
+    double gas_diffus, freepath;
+    h2so4_diffusivity(temp, pmid, gas_diffus, freepath);
+    uptake_rates(c_k, gas_diffus, freepath, dgn_awet, rate);
+  }
+  clear_prefix<DIAG>(a, deltat, temp, pmid, rate, qgas1, s, cm, uptk0);
   int niter = 0;
   if (a.do_cond)
     niter = soa_exchange((double)(int)(deltat / 1), temp, pmid, s, uptk0);
@@ -396,7 +398,9 @@ struct Front {
 // size outputs and prepares the amicphys inputs: the part of
 // modal_aero_amicphys_intr (mam4_amicphys.hpp:2120-2260) before the
 // subarea loop, with q_pregaschem = q_precldchem = qq and
-// qqcw_precldchem = qqcw.
+// qqcw_precldchem = qqcw. Without WU the wet sizes are read back from the
+// outputs, written by size_kernel and mode_kernel.
+template <bool WU>
 __device__ __forceinline__ void cell_front(const StepArgs &a, const long long c, Front &f) {
   const StepConsts &C = c_k;
   f.temp = __ldg(a.in[MAM4B_IN_T] + c);
@@ -423,14 +427,23 @@ __device__ __forceinline__ void cell_front(const StepArgs &a, const long long c,
   }
   double pt_i[NPOP], pt_c[NPOP];
   calcsize(C, f.ai, f.ac, dt, f.dgn_a, pt_i, pt_c);
-  double qaerwat[NMODE], wetdens_wu[NMODE];
-  water_uptake(C, f.ai, f.qv, f.temp, f.pmid, f.cld, f.dgn_a, f.dgn_awet, qaerwat, wetdens_wu);
+  double wetdens_wu[NMODE];
+  if (WU) {
+    double qaerwat[NMODE];
+    water_uptake(C, f.ai, f.qv, f.temp, f.pmid, f.cld, f.dgn_a, f.dgn_awet, qaerwat, wetdens_wu);
 #pragma unroll
-  for (int m = 0; m < NMODE; ++m) {
-    a.out[MAM4B_OUT_DGN_A + m][c] = f.dgn_a[m];
-    a.out[MAM4B_OUT_DGN_AWET + m][c] = f.dgn_awet[m];
-    a.out[MAM4B_OUT_WETDENS + m][c] = wetdens_wu[m];
-    a.out[MAM4B_OUT_QAERWAT + m][c] = qaerwat[m];
+    for (int m = 0; m < NMODE; ++m) {
+      a.out[MAM4B_OUT_DGN_A + m][c] = f.dgn_a[m];
+      a.out[MAM4B_OUT_DGN_AWET + m][c] = f.dgn_awet[m];
+      a.out[MAM4B_OUT_WETDENS + m][c] = wetdens_wu[m];
+      a.out[MAM4B_OUT_QAERWAT + m][c] = qaerwat[m];
+    }
+  } else {
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      f.dgn_awet[m] = a.out[MAM4B_OUT_DGN_AWET + m][c];
+      wetdens_wu[m] = a.out[MAM4B_OUT_WETDENS + m][c];
+    }
   }
   // calcsize tendencies applied for one step, then amicphys units
 #pragma unroll
@@ -637,7 +650,7 @@ template <bool DIAG>
 __device__ __forceinline__ void cell_step(const StepArgs &a, const long long c) {
   const StepConsts &C = c_k;
   Front f;
-  cell_front(a, c, f);
+  cell_front<true>(a, c, f);
   const double dt = a.dt;
   Diag dgv;
   Diag *dg = DIAG ? &dgv : nullptr;
@@ -751,7 +764,7 @@ __device__ __forceinline__ void cell_step(const StepArgs &a, const long long c) 
 __device__ __forceinline__ void cell_pre(const StepArgs &a, const long long c) {
   const StepConsts &C = c_k;
   Front f;
-  cell_front(a, c, f);
+  cell_front<false>(a, c, f);
   const double dt = a.dt;
   const double fsoag = C.fcvt_soag;
   if (f.cld > 0.999) {
@@ -777,8 +790,11 @@ __device__ __forceinline__ void cell_pre(const StepArgs &a, const long long c) {
   }
   const double qgas1[2] = {f.g_soag * fsoag, f.g_h2so4 * 1.0};
   ClearMid cm;
-  double uptk0[NMODE];
-  clear_prefix<false>(a, dt, f.temp, f.pmid, f.dgn_awet, qgas1, s, cm, uptk0);
+  double uptk0[NMODE], rate[NMODE];
+#pragma unroll
+  for (int k = 0; k < NMODE; ++k)
+    rate[k] = a.aux[(AUX_RATE + k) * (size_t)a.ncell + c];
+  clear_prefix<false>(a, dt, f.temp, f.pmid, rate, qgas1, s, cm, uptk0);
 
   // queue the cell: solver state and hand-off at the start of the SOA loop
   SoaState st;
@@ -944,6 +960,71 @@ __global__ void __launch_bounds__(128) full_kernel(const __grid_constant__ StepA
     cell_step<DIAG>(a, c);
 }
 
+// Stage 1 of the pipelined step, one thread per cell: calcsize for the dry
+// diameters (an output), the relative humidity of water uptake and the
+// H2SO4 diffusivity and mean free path.
+__global__ void __launch_bounds__(128) size_kernel(const __grid_constant__ StepArgs a) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncell)
+    return;
+  const StepConsts &C = c_k;
+  double ai[NPOP], ac[NPOP];
+#pragma unroll
+  for (int p = 0; p < NPOP; ++p) {
+    ai[p] = __ldg(a.in[MAM4B_IN_AER_I + p] + c);
+    ac[p] = __ldg(a.in[MAM4B_IN_AER_C + p] + c);
+  }
+  double dgn_a[NMODE], pt_i[NPOP], pt_c[NPOP];
+  calcsize(C, ai, ac, a.dt, dgn_a, pt_i, pt_c);
+#pragma unroll
+  for (int m = 0; m < NMODE; ++m)
+    a.out[MAM4B_OUT_DGN_A + m][c] = dgn_a[m];
+  const double temp = __ldg(a.in[MAM4B_IN_T] + c);
+  const double pmid = __ldg(a.in[MAM4B_IN_P] + c);
+  const size_t n = (size_t)a.ncell;
+  a.aux[AUX_RH * n + c] =
+      water_uptake_rh(__ldg(a.in[MAM4B_IN_QV] + c), temp, pmid, __ldg(a.in[MAM4B_IN_CLD] + c));
+  double gd, fp;
+  h2so4_diffusivity(temp, pmid, gd, fp);
+  a.aux[AUX_GDIFF * n + c] = gd;
+  a.aux[AUX_FPATH * n + c] = fp;
+}
+
+// Stage 2, one thread per (cell, mode): water uptake of the mode (Kohler
+// equilibrium, wet size, water, wet density; outputs) and its per-particle
+// H2SO4 uptake rate. The modes are independent here, and a thread holds
+// one mode's state only, so many more warps are resident than in a
+// whole-cell thread.
+template <int M>
+__device__ __forceinline__ void mode_work(const StepArgs &a, const long long c) {
+  const StepConsts &C = c_k;
+  const size_t n = (size_t)a.ncell;
+  double sp[7];
+#pragma unroll
+  for (int s = 0; s < 7; ++s)
+    sp[s] = (s < K::nspec(M)) ? __ldg(a.in[MAM4B_IN_AER_I + K::spec0(M) + (s < K::nspec(M) ? s : 0)] + c) : 0.0;
+  const double dgn_a = a.out[MAM4B_OUT_DGN_A + M][c];
+  double dgn_awet, qaerwat, wetdens;
+  water_uptake_mode<M>(C, sp, a.aux[AUX_RH * n + c], dgn_a, dgn_awet, qaerwat, wetdens);
+  a.out[MAM4B_OUT_DGN_AWET + M][c] = dgn_awet;
+  a.out[MAM4B_OUT_WETDENS + M][c] = wetdens;
+  a.out[MAM4B_OUT_QAERWAT + M][c] = qaerwat;
+  a.aux[(AUX_RATE + M) * n + c] =
+      uptake_rate_mode(C, M, a.aux[AUX_GDIFF * n + c], a.aux[AUX_FPATH * n + c], dgn_awet);
+}
+
+__global__ void __launch_bounds__(128) mode_kernel(const __grid_constant__ StepArgs a) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncell)
+    return;
+  switch (blockIdx.y) {
+  case 0: mode_work<0>(a, c); break;
+  case 1: mode_work<1>(a, c); break;
+  case 2: mode_work<2>(a, c); break;
+  default: mode_work<3>(a, c); break;
+  }
+}
+
 __global__ void __launch_bounds__(128) pre_kernel(const __grid_constant__ StepArgs a) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c < a.ncell)
@@ -1084,8 +1165,9 @@ __global__ void init_consts_kernel(StepConsts *out) { *out = make_consts(); }
 // ============================================ scratch of the no-alloc step
 // mam4b_step_slab_noalloc keeps the pipeline's working memory in this one
 // array instead of context allocations: SOA loop state [SOA_FIELDS][ncell],
-// hand-off [H_FIELDS][ncell], queue and solver order ([ncell] ints each), and
-// a 256-byte tail with the queue counters and a spare flag word. Host code must not pass the
+// hand-off [H_FIELDS][ncell], queue and solver order ([ncell] ints each),
+// per-cell values of the size and mode kernels [AUX_FIELDS][ncell], and a
+// 256-byte tail with the queue counters and a spare flag word. Host code must not pass the
 // name g_noalloc_scratch to a kernel (on the host it is a stand-in, not a
 // device address); it uses the address from cudaGetSymbolAddress.
 constexpr size_t kNoAllocCells = MAM4B_NOALLOC_MAX_CELLS;
@@ -1093,7 +1175,8 @@ constexpr size_t kNoAllocSoa = 0;
 constexpr size_t kNoAllocHand = kNoAllocSoa + (size_t)SOA_FIELDS * kNoAllocCells;
 constexpr size_t kNoAllocTask = kNoAllocHand + (size_t)H_FIELDS * kNoAllocCells;
 constexpr size_t kNoAllocOrder = kNoAllocTask + kNoAllocCells / 2;
-constexpr size_t kNoAllocTail = kNoAllocOrder + kNoAllocCells / 2;
+constexpr size_t kNoAllocAux = kNoAllocOrder + kNoAllocCells / 2;
+constexpr size_t kNoAllocTail = kNoAllocAux + (size_t)AUX_FIELDS * kNoAllocCells;
 constexpr size_t kNoAllocDoubles = kNoAllocTail + 32;
 static_assert(kNoAllocCells % 64 == 0, "scratch regions stay 256-byte aligned");
 static_assert(sizeof(StepConsts) <= (size_t)SOA_FIELDS * kNoAllocCells * sizeof(double),
@@ -1128,6 +1211,7 @@ struct mam4b_ctx {
   double *d_soa;
   double *d_hand;
   int *d_task, *d_order;
+  double *d_aux;
   unsigned *d_counters;  // CNT_WORDS per chunk of the host path
   size_t cap_cells;
   int soa_grid;  // persistent solver blocks (SMs x resident blocks)
@@ -1196,6 +1280,8 @@ cudaError_t ensure_solver_scratch(mam4b_ctx *ctx, size_t ncell) {
   cudaFree(ctx->d_hand);
   cudaFree(ctx->d_task);
   cudaFree(ctx->d_order);
+  cudaFree(ctx->d_aux);
+  ctx->d_aux = nullptr;
   ctx->d_soa = nullptr;
   ctx->d_hand = nullptr;
   ctx->d_task = nullptr;
@@ -1208,6 +1294,8 @@ cudaError_t ensure_solver_scratch(mam4b_ctx *ctx, size_t ncell) {
     e = cudaMalloc(&ctx->d_task, ncell * sizeof(int));
   if (e == cudaSuccess)
     e = cudaMalloc(&ctx->d_order, ncell * sizeof(int));
+  if (e == cudaSuccess)
+    e = cudaMalloc(&ctx->d_aux, (size_t)AUX_FIELDS * ncell * sizeof(double));
   if (e == cudaSuccess)
     ctx->cap_cells = ncell;
   return e;
@@ -1233,6 +1321,7 @@ void set_step_scratch(const mam4b_ctx *ctx, StepArgs &a, size_t c0, int chunk) {
   a.hand = ctx->d_hand + (size_t)H_FIELDS * c0;
   a.task = ctx->d_task + c0;
   a.order = ctx->d_order + c0;
+  a.aux = ctx->d_aux + (size_t)AUX_FIELDS * c0;
   a.counters = ctx->d_counters + (size_t)CNT_WORDS * chunk;
 }
 
@@ -1251,12 +1340,14 @@ cudaError_t launch_pipeline(mam4b_ctx *ctx, const StepArgs &a, cudaStream_t s) {
       ctx->launches += 1;
     return e;
   }
+  size_kernel<<<grid, block, 0, s>>>(a);
+  mode_kernel<<<dim3(grid, NMODE), block, 0, s>>>(a);
   pre_kernel<<<grid, block, 0, s>>>(a);
   soa_kernel<<<ctx->soa_grid, kSoaBlock, 0, s>>>(a);
   post_kernel<<<grid, block, 0, s>>>(a);
   e = cudaGetLastError();
   if (e == cudaSuccess)
-    ctx->launches += 3;
+    ctx->launches += 5;
   return e;
 }
 
@@ -1393,6 +1484,7 @@ mam4b_status mam4b_destroy(mam4b_ctx *ctx) {
   cudaFree(ctx->d_hand);
   cudaFree(ctx->d_task);
   cudaFree(ctx->d_order);
+  cudaFree(ctx->d_aux);
   cudaFree(ctx->d_counters);
   if (ctx->host_streams) {
     for (int k = 0; k < kHostStreams; ++k) {
@@ -1616,6 +1708,7 @@ mam4b_status mam4b_step_slab_noalloc(const mam4b_config *cfg, const double *in_s
   a.hand = nd.scratch + kNoAllocHand;
   a.task = reinterpret_cast<int *>(nd.scratch + kNoAllocTask);
   a.order = reinterpret_cast<int *>(nd.scratch + kNoAllocOrder);
+  a.aux = nd.scratch + kNoAllocAux;
   a.ncell = ncell;
   a.nlev = nlev;
   a.dt = dt;
@@ -1636,6 +1729,8 @@ mam4b_status mam4b_step_slab_noalloc(const mam4b_config *cfg, const double *in_s
     // no SOA loop to pipeline (and no scratch used)
     full_kernel<false><<<grid, block, 0, s>>>(a);
   } else {
+    size_kernel<<<grid, block, 0, s>>>(a);
+    mode_kernel<<<dim3(grid, NMODE), block, 0, s>>>(a);
     pre_kernel<<<grid, block, 0, s>>>(a);
     soa_kernel<<<nd.soa_grid, kSoaBlock, 0, s>>>(a);
     post_kernel<<<grid, block, 0, s>>>(a);
