@@ -208,7 +208,7 @@ mam4b_status mam4b_step_host(mam4b_ctx *ctx, const double *in_slab,
  * The same step as mam4b_step_slab (FP64, no diagnostics, same results),
  * with the working memory of the SOA condensation solver in one fixed
  * device array inside the library instead of context-owned allocations:
- * MAM4B_NOALLOC_MAX_CELLS cells at most, about 15 MB, held on every GPU
+ * MAM4B_NOALLOC_MAX_CELLS cells at most, about 16 MB, held on every GPU
  * that loads the library until the process exits. No context is needed.
  *
  *   cfg      process switches (NULL = mam4b_default_config)

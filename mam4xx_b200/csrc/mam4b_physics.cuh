@@ -1236,12 +1236,41 @@ __device__ __forceinline__ double qnum_intra_inter(double bijdtqnumj, double bii
   return qnumi_bgn * e / (1.0 + (biidt * qnumi_bgn / bijdtqnumj) * (1.0 - e));
 }
 
-// mam_coag_1subarea (coagulation.hpp:1038-1119); coag_in receives the
-// mass moved into the primary-carbon mode (AeroId order)
-__device__ __forceinline__ void coagulation(const StepConsts &C, const CoagTables &T,
-                                            double deltat, double temp, double pmid,
-                                            double aircon, const double (&dgn_awet)[NMODE],
-                                            const double (&wetdens)[NMODE], Sub &s,
+// Coagulation coefficients of the three mode pairs (aitken->accumulation,
+// pcarbon->accumulation, aitken->pcarbon) in the order mam_coag_1subarea
+// uses them (coagulation.hpp:1060-1085), times the air molar concentration:
+// cc[0..2] bij0, cc[3..5] bij3, cc[6..8] bii0, cc[9..11] bjj0.
+MAM4B_HD constexpr int coag_src(int p) { return p == 1 ? 3 : 1; }
+MAM4B_HD constexpr int coag_dst(int p) { return p == 2 ? 3 : 0; }
+__device__ __forceinline__ void coag_pair_coefs(const StepConsts &C, const CoagTables &T, int p,
+                                                double temp, double pmid, double aircon,
+                                                double dgn_src, double dgn_dst, double dens_src,
+                                                double dens_dst, double &bij0, double &bij3,
+                                                double &bii0, double &bjj0) {
+  const int sm = coag_src(p), dm = coag_dst(p);
+  coag_coefs(T, temp, pmid, dgn_src, dgn_dst, K::sig(sm), K::sig(dm), C.log_sig[sm],
+             C.log_sig[dm], dens_src, dens_dst, bij0, bij3, bii0, bjj0);
+  bij0 *= aircon;
+  bij3 *= aircon;
+  bii0 *= aircon;
+  bjj0 *= aircon;
+}
+
+__device__ __forceinline__ void coag_all_coefs(const StepConsts &C, const CoagTables &T,
+                                               double temp, double pmid, double aircon,
+                                               const double (&dgn_awet)[NMODE],
+                                               const double (&wetdens)[NMODE], double (&cc)[12]) {
+#pragma unroll
+  for (int p = 0; p < 3; ++p)
+    coag_pair_coefs(C, T, p, temp, pmid, aircon, dgn_awet[coag_src(p)], dgn_awet[coag_dst(p)],
+                    wetdens[coag_src(p)], wetdens[coag_dst(p)], cc[p], cc[3 + p], cc[6 + p],
+                    cc[9 + p]);
+}
+
+// mam_coag_1subarea (coagulation.hpp:1038-1119) with the coefficients cc of
+// coag_all_coefs; coag_in receives the mass moved into the primary-carbon
+// mode (AeroId order)
+__device__ __forceinline__ void coagulation(double deltat, const double (&cc)[12], Sub &s,
                                             double (&coag_in)[NAER]) {
   double bgn[NAER][NMODE], nbgn[NMODE];
 #pragma unroll
@@ -1256,18 +1285,8 @@ __device__ __forceinline__ void coagulation(const StepConsts &C, const CoagTable
     s.num[m] = dmax(0.0, s.num[m]);
     nbgn[m] = s.num[m];
   }
-  constexpr int srcm[3] = {1, 3, 1}, dstm[3] = {0, 0, 3};
-  double bij0[3], bij3[3], bii0[3], bjj0[3];
-#pragma unroll
-  for (int p = 0; p < 3; ++p) {
-    coag_coefs(T, temp, pmid, dgn_awet[srcm[p]], dgn_awet[dstm[p]], K::sig(srcm[p]),
-               K::sig(dstm[p]), C.log_sig[srcm[p]], C.log_sig[dstm[p]], wetdens[srcm[p]],
-               wetdens[dstm[p]], bij0[p], bij3[p], bii0[p], bjj0[p]);
-    bij0[p] *= aircon;
-    bij3[p] *= aircon;
-    bii0[p] *= aircon;
-    bjj0[p] *= aircon;
-  }
+  const double bij0[3] = {cc[0], cc[1], cc[2]}, bij3[3] = {cc[3], cc[4], cc[5]};
+  const double bii0[3] = {cc[6], cc[7], cc[8]}, bjj0[3] = {cc[9], cc[10], cc[11]};
   // mam_coag_num_update (:982-1027): accumulation, then pcarbon, then aitken
   double tavg[NMODE];
   s.num[0] = nbgn[0] / (1.0 + bjj0[0] * deltat * nbgn[0]);

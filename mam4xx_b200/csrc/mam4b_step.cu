@@ -62,7 +62,8 @@ enum { SOA_G = 0, SOA_A = 1, SOA_OPOA = 5, SOA_UPTK = 9, SOA_G0 = 13, SOA_FIELDS
 // per-cell values from size_kernel and mode_kernel for the pre kernel:
 // relative humidity for water uptake, H2SO4 diffusivity and mean free path,
 // per-particle H2SO4 uptake rate of each mode
-enum { AUX_RH = 0, AUX_GDIFF = 1, AUX_FPATH = 2, AUX_RATE = 3, AUX_FIELDS = 7 };
+// and the 12 coagulation coefficients (coag_all_coefs order)
+enum { AUX_RH = 0, AUX_GDIFF = 1, AUX_FPATH = 2, AUX_RATE = 3, AUX_COAG = 7, AUX_FIELDS = 19 };
 // queue counters: queued slots, slots handed to the solver, long and short
 // loops in the order list
 enum { CNT_QUEUED = 0, CNT_TAKEN = 1, CNT_LONG = 2, CNT_SHORT = 3, CNT_WORDS = 4 };
@@ -93,13 +94,11 @@ enum {
   H_SV_SO4 = 31,   // aitken SO4 and SOA before condensation
   H_SV_SOA = 32,
   H_DGN_PC = 33,   // dry diameter of the primary-carbon mode
-  H_AWET = 34,     // 4 wet diameters
-  H_WETD = 38,     // 4 wet densities (>= 1000)
-  H_RELHUM = 42,   // relative humidity of the clear subarea
-  H_OC = 43,       // 25 outgoing cloud-borne grid means
-  H_CI = 68,       // 25 interstitial contributions of the cloudy subarea
-  H_CG = 93,       // 2 gas contributions of the cloudy subarea (SOAG, H2SO4)
-  H_FIELDS = 95
+  H_RELHUM = 34,   // relative humidity of the clear subarea
+  H_OC = 35,       // 25 outgoing cloud-borne grid means
+  H_CI = 60,       // 25 interstitial contributions of the cloudy subarea
+  H_CG = 85,       // 2 gas contributions of the cloudy subarea (SOAG, H2SO4)
+  H_FIELDS = 87
 };
 
 // State of the clear subarea between the start of condensation and the SOA
@@ -150,14 +149,17 @@ __device__ __forceinline__ void clear_prefix(const StepArgs &a, double deltat, d
 
 // Part 2, after the SOA loop: H2SO4 update, renaming, nucleation,
 // coagulation, aging. With DIAG the per-process increments are added to dg
-// scaled by afrac/(fcvt*deltat).
-template <bool DIAG>
+// scaled by afrac/(fcvt*deltat). With PRECOAG, cc_pre (stride cc_stride)
+// holds the 12 coagulation coefficients of the cell (coag_all_coefs) and
+// dgn_awet/wetdens are not read.
+template <bool DIAG, bool PRECOAG>
 __device__ __forceinline__ void clear_suffix(const StepArgs &a, double deltat, double temp,
                                              double pmid, double zmid, double pblh,
                                              double relhum, double dgn_a_pc,
                                              const double (&dgn_awet)[NMODE],
                                              const double (&wetdens)[NMODE], const ClearMid &cm,
-                                             Sub &s, Diag *dg, double afrac) {
+                                             Sub &s, Diag *dg, double afrac,
+                                             const double *cc_pre, size_t cc_stride) {
   const StepConsts &C = c_k;
   const double aircon = pmid / (8314.46759100000 * temp);
   const double dtsub = (double)(int)(deltat / 1);
@@ -261,8 +263,17 @@ __device__ __forceinline__ void clear_suffix(const StepArgs &a, double deltat, d
           asv[x][m] = s.aer[x][m];
       }
     }
-    const CoagTables T = {kCoagBm0ij, kCoagBm3i, kCoagBm0};
-    coagulation(C, T, dtsub, temp, pmid, aircon, dgn_awet, wetdens, s, coag_in);
+    double cc[12];
+    if (PRECOAG) {
+      // coefficients from pair_kernel
+#pragma unroll
+      for (int k = 0; k < 12; ++k)
+        cc[k] = cc_pre[k * cc_stride];
+    } else {
+      const CoagTables T = {kCoagBm0ij, kCoagBm3i, kCoagBm0};
+      coag_all_coefs(C, T, temp, pmid, aircon, dgn_awet, wetdens, cc);
+    }
+    coagulation(dtsub, cc, s, coag_in);
     if (DIAG) {
 #pragma unroll
       for (int m = 0; m < NMODE; ++m) {
@@ -341,8 +352,8 @@ __device__ __forceinline__ int clear_subarea(const StepArgs &a, double deltat, d
   int niter = 0;
   if (a.do_cond)
     niter = soa_exchange((double)(int)(deltat / 1), temp, pmid, s, uptk0);
-  clear_suffix<DIAG>(a, deltat, temp, pmid, zmid, pblh, relhum, dgn_a[3], dgn_awet, wetdens, cm, s,
-                     dg, afrac);
+  clear_suffix<DIAG, false>(a, deltat, temp, pmid, zmid, pblh, relhum, dgn_a[3], dgn_awet, wetdens, cm, s,
+                     dg, afrac, nullptr, 0);
   return niter;
 }
 
@@ -842,11 +853,8 @@ __device__ __forceinline__ void cell_pre(const StepArgs &a, const long long c) {
   for (int p = 0; p < NPOP; ++p)
     h[(H_POP + p) * n] = pop[p];
 #pragma unroll
-  for (int k = 0; k < NMODE; ++k) {
+  for (int k = 0; k < NMODE; ++k)
     h[(H_UPTK + k) * n] = cm.uptk1[k];
-    h[(H_AWET + k) * n] = f.dgn_awet[k];
-    h[(H_WETD + k) * n] = f.wetdens[k];
-  }
   h[H_NETPROD * n] = cm.netprod1;
   h[H_SV_SO4 * n] = cm.sv_so4_ait;
   h[H_SV_SOA * n] = cm.sv_soa_ait;
@@ -896,15 +904,14 @@ __device__ __forceinline__ void cell_post(const StepArgs &a, unsigned slot) {
   cm.netprod1 = h[H_NETPROD * n];
   cm.sv_so4_ait = h[H_SV_SO4 * n];
   cm.sv_soa_ait = h[H_SV_SOA * n];
-  double dgn_awet[NMODE], wetdens[NMODE];
+  // wet sizes enter the suffix only through the coagulation coefficients,
+  // which pair_kernel computed
+  const double unused[NMODE] = {0, 0, 0, 0};
 #pragma unroll
-  for (int k = 0; k < NMODE; ++k) {
+  for (int k = 0; k < NMODE; ++k)
     cm.uptk1[k] = h[(H_UPTK + k) * n];
-    dgn_awet[k] = h[(H_AWET + k) * n];
-    wetdens[k] = h[(H_WETD + k) * n];
-  }
-  clear_suffix<false>(a, dt, temp, pmid, zm, pblh, h[H_RELHUM * n], h[H_DGN_PC * n], dgn_awet,
-                      wetdens, cm, s, nullptr, 0.0);
+  clear_suffix<false, true>(a, dt, temp, pmid, zm, pblh, h[H_RELHUM * n], h[H_DGN_PC * n], unused,
+                            unused, cm, s, nullptr, 0.0, a.aux + AUX_COAG * n + c, n);
   // recombination (form_gcm_of_gases_and_aerosols_from_subareas)
   const double fsoag = C.fcvt_soag;
   double o_h2so4, o_soag, oi[NPOP], oc[NPOP];
@@ -1023,6 +1030,34 @@ __global__ void __launch_bounds__(128) mode_kernel(const __grid_constant__ StepA
   case 2: mode_work<2>(a, c); break;
   default: mode_work<3>(a, c); break;
   }
+}
+
+// Stage 3, one thread per (cell, mode pair): the Brownian coagulation
+// coefficients of the pair (getcoags, coagulation.hpp:651-817) from the wet
+// sizes and densities of stage 2; they do not depend on what condensation
+// changes, so the post kernel only applies them.
+__global__ void __launch_bounds__(128) pair_kernel(const __grid_constant__ StepArgs a) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncell)
+    return;
+  const StepConsts &C = c_k;
+  const int p = blockIdx.y;
+  const int sm = coag_src(p), dm = coag_dst(p);
+  const double temp = __ldg(a.in[MAM4B_IN_T] + c);
+  const double pmid = __ldg(a.in[MAM4B_IN_P] + c);
+  const double aircon = pmid / (8314.46759100000 * temp);
+  const double dens_s = dmax(1000.0, a.out[MAM4B_OUT_WETDENS + sm][c]);
+  const double dens_d = dmax(1000.0, a.out[MAM4B_OUT_WETDENS + dm][c]);
+  const CoagTables T = {kCoagBm0ij, kCoagBm3i, kCoagBm0};
+  double bij0, bij3, bii0, bjj0;
+  coag_pair_coefs(C, T, p, temp, pmid, aircon, a.out[MAM4B_OUT_DGN_AWET + sm][c],
+                  a.out[MAM4B_OUT_DGN_AWET + dm][c], dens_s, dens_d, bij0, bij3, bii0, bjj0);
+  const size_t n = (size_t)a.ncell;
+  double *cc = a.aux + AUX_COAG * n + c;
+  cc[p * n] = bij0;
+  cc[(3 + p) * n] = bij3;
+  cc[(6 + p) * n] = bii0;
+  cc[(9 + p) * n] = bjj0;
 }
 
 __global__ void __launch_bounds__(128) pre_kernel(const __grid_constant__ StepArgs a) {
@@ -1342,12 +1377,13 @@ cudaError_t launch_pipeline(mam4b_ctx *ctx, const StepArgs &a, cudaStream_t s) {
   }
   size_kernel<<<grid, block, 0, s>>>(a);
   mode_kernel<<<dim3(grid, NMODE), block, 0, s>>>(a);
+  pair_kernel<<<dim3(grid, 3), block, 0, s>>>(a);
   pre_kernel<<<grid, block, 0, s>>>(a);
   soa_kernel<<<ctx->soa_grid, kSoaBlock, 0, s>>>(a);
   post_kernel<<<grid, block, 0, s>>>(a);
   e = cudaGetLastError();
   if (e == cudaSuccess)
-    ctx->launches += 5;
+    ctx->launches += 6;
   return e;
 }
 
@@ -1731,6 +1767,7 @@ mam4b_status mam4b_step_slab_noalloc(const mam4b_config *cfg, const double *in_s
   } else {
     size_kernel<<<grid, block, 0, s>>>(a);
     mode_kernel<<<dim3(grid, NMODE), block, 0, s>>>(a);
+    pair_kernel<<<dim3(grid, 3), block, 0, s>>>(a);
     pre_kernel<<<grid, block, 0, s>>>(a);
     soa_kernel<<<nd.soa_grid, kSoaBlock, 0, s>>>(a);
     post_kernel<<<grid, block, 0, s>>>(a);
