@@ -5,13 +5,17 @@ GPU (4,718,592 cells), FP64, seeded synthetic inputs (mam4xx_b200.workloads
 'c4': H2SO4 1e-15..1e-8 mol/mol, cloud fraction 60% clear / 40% U(0.2, 1)).
 One step = calcsize + water uptake + amicphys over every cell, dt = 1800 s.
 
-  value  cells/s with inputs resident in HBM (one kernel launch per step),
-         whole job = all ranks' cells / max-over-ranks time
+  value  cells/s with inputs resident in HBM (one step = the six-kernel
+         pipeline behind mam4b_step_slab), whole job = all ranks' cells /
+         max-over-ranks time
   e2e    cells/s through the C ABI host entry (mam4b_step_host): pinned host
          slabs copied in, step, results copied out, every step
   roofline  algorithmic HBM bytes (57 input + 68 output doubles per cell plus
-         the per-column boundary-layer height) / measured kernel time, against
-         the measured copy bandwidth of MEASURED_PEAKS.json
+         the per-column boundary-layer height) / measured step time (the
+         unit is one step, i.e. one pass of the six launches), against the
+         measured copy bandwidth of MEASURED_PEAKS.json; traffic = DRAM bytes
+         of the six launches from the committed ncu summary, per cell, times
+         the cells
   cpu_baseline  the mam4xx reference headers compiled for the host
          (oracle/_ref, OpenMP) on a bounded sample of the same cells
 
@@ -58,7 +62,7 @@ def _peaks():
 
 def _traffic_per_launch(ncell):
     """DRAM bytes per launch from the committed ncu summary, scaled by cells."""
-    p = os.path.join(ROOT, "profiles", "step_kernel_c4_ncu.md")
+    p = os.path.join(ROOT, "profiles", "step_pipeline_c4_ncu.md")
     if not os.path.exists(p):
         return None
     txt = open(p).read()
@@ -173,7 +177,7 @@ def run_reference_arm(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=25)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--ncol", type=int, default=NCOL_PER_GPU, help="columns per GPU")
@@ -224,6 +228,7 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     sampler.start()
+    time.sleep(0.5)  # nvidia-smi's first sample lands inside the timed region
     launches0 = ctx.launch_count()
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
