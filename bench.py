@@ -41,7 +41,7 @@ NCOL_PER_GPU = 65536
 NLEV = 72
 WORKLOAD = "c4"
 BYTES_PER_CELL = (57 + 68) * 8  # + 8 bytes of boundary-layer height per column
-METRIC = "cells/s per amicphys step"
+METRIC = "cells/s per amicphys step, FP64 vs mixed @ stated err; adjoint/forward time"
 
 
 def _dist():
@@ -183,6 +183,7 @@ def main():
     ap.add_argument("--ncol", type=int, default=NCOL_PER_GPU, help="columns per GPU")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision legs")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -211,9 +212,9 @@ def main():
     ctx = native.Context()
     stream = torch.cuda.current_stream(dev)
 
-    def step():
+    def step(precision=native.FP64):
         ctx.step_slab(x.data_ptr(), pb.data_ptr(), out.data_ptr(), n, ncol, NLEV, dt,
-                      stream=stream.cuda_stream)
+                      precision=precision, stream=stream.cuda_stream)
 
     for _ in range(args.warmup):
         step()
@@ -284,6 +285,43 @@ def main():
                "steps": ke, "entry": "mam4b_step_host"}
         ectx.close()
 
+    # mixed-precision forms: same workload, same timing, errors against the
+    # FP64 results of this run on a sample of the columns
+    precisions = None
+    if not args.no_mixed:
+        precisions = {}
+        n_s = min(n, 8192 * NLEV)
+        ref_s = out[:, :n_s].cpu().numpy()
+        from mam4xx_b200.precision import error_report
+        for name, prec in (("mixed", native.MIXED), ("mixed_fast", native.MIXED_FAST)):
+            for _ in range(args.warmup):
+                step(prec)
+            if ws > 1:
+                dist.barrier()
+            torch.cuda.synchronize()
+            m0 = torch.cuda.Event(enable_timing=True)
+            m1 = torch.cuda.Event(enable_timing=True)
+            m0.record(stream)
+            for _ in range(args.steps):
+                step(prec)
+            m1.record(stream)
+            torch.cuda.synchronize()
+            m_ms = m0.elapsed_time(m1)
+            if ws > 1:
+                tt = torch.tensor([m_ms], device=dev)
+                dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+                m_ms = float(tt.item())
+            r = error_report(out[:, :n_s].cpu().numpy(), ref_s, x_host[:, :n_s], dt, tol=1e-5)
+            precisions[name] = {
+                "value": ws * n * args.steps / (m_ms * 1e-3), "unit": "cells/s",
+                "ms_per_step": m_ms / args.steps, "speedup_vs_fp64": total_ms / m_ms,
+                "err_vs_fp64": {"sample_cells": n_s, "max": r["max"], "median": r["median"],
+                                "cells_within_1e-5": r["cells_within_tol"],
+                                "cell_err_quantiles": r["cell_err_quantiles"],
+                                "per_output_max": r["per_output_max"],
+                                "per_output_median": r["per_output_median"]}}
+        step(native.FP64)
+
     peak, peak_kind = _peaks()
     alg_bytes = n * BYTES_PER_CELL + ncol * 8
     achieved = alg_bytes / (kernel_ms * 1e-3) / 1e9
@@ -303,6 +341,7 @@ def main():
                      "peak_source": "%s copy bandwidth" % peak_kind,
                      "kernel_ms": kernel_ms, "algorithmic_bytes_per_launch": alg_bytes},
         "e2e": e2e,
+        "precisions": precisions,
         "gpu_launches": int(launches),
         "clocks": clocks,
         "device_flags": flags,

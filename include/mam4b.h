@@ -126,11 +126,20 @@ typedef enum mam4b_status {
 #define MAM4B_FLAG_NONFINITE_OUTPUT 0x4u
 #define MAM4B_FLAGS_ERROR_MASK (MAM4B_FLAG_NONFINITE_INPUT | MAM4B_FLAG_NONFINITE_OUTPUT)
 
-/* Arithmetic of the step. */
+/* Arithmetic of the step. The mixed forms run the bulk in FP32 (water
+ * uptake and Kohler equilibrium, the H2SO4 uptake coefficients, the
+ * coagulation coefficients) and keep FP64 in calcsize, the H2SO4 implicit
+ * exponential update, the renaming transfer fractions, the nucleation rate
+ * fits (their polynomials cancel to a few digits in FP32), aging and every
+ * state update and sum that carries species mass. MAM4B_MIXED keeps the
+ * SOA sub-stepping in FP64 too; MAM4B_MIXED_FAST runs it in FP32, which is
+ * faster but leaves the results of many cells 1e-4..1e-2 away from FP64
+ * (the loop amplifies rounding near equilibrium). Per-process diagnostics
+ * are FP64 only. */
 typedef enum mam4b_precision {
-  MAM4B_FP64 = 0,  /* plain double precision throughout                  */
-  MAM4B_MIXED = 1  /* FP32 bulk; FP64 in the condensation update, the
-                      renaming transfer fractions and conservation sums  */
+  MAM4B_FP64 = 0,       /* plain double precision throughout              */
+  MAM4B_MIXED = 1,      /* FP32 bulk, FP64 condensation                   */
+  MAM4B_MIXED_FAST = 2  /* FP32 bulk and FP32 SOA sub-stepping            */
 } mam4b_precision;
 
 /*

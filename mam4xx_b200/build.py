@@ -39,7 +39,8 @@ def _newer(target, deps):
 
 
 def build_product(force=False):
-    srcs = [os.path.join(CSRC, f) for f in ("mam4b_step.cu", "mam4b_physics.cuh", "coag_tables.inc")]
+    srcs = [os.path.join(CSRC, f) for f in os.listdir(CSRC)
+            if f.endswith((".cu", ".cuh", ".inc")) and not f.startswith("_")]
     srcs.append(os.path.join(ROOT, "include", "mam4b.h"))
     if not force and _newer(LIB, srcs):
         return LIB

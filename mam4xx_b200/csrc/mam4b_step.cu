@@ -15,9 +15,11 @@
 #include <atomic>
 #include <mutex>
 #include <new>
+#include <type_traits>
 
 #include "../../include/mam4b.h"
 #include "mam4b_physics.cuh"
+#include "mam4b_physics_mixed.cuh"
 
 namespace mam4b {
 
@@ -1002,10 +1004,26 @@ __global__ void __launch_bounds__(128) size_kernel(const __grid_constant__ StepA
 // H2SO4 uptake rate. The modes are independent here, and a thread holds
 // one mode's state only, so many more warps are resident than in a
 // whole-cell thread.
-template <int M>
+// With MIXED the mode's arithmetic is single precision (mam4b::f32).
+template <int M, bool MIXED>
 __device__ __forceinline__ void mode_work(const StepArgs &a, const long long c) {
   const StepConsts &C = c_k;
   const size_t n = (size_t)a.ncell;
+  if constexpr (MIXED) {
+    float sp[7];
+#pragma unroll
+    for (int s = 0; s < 7; ++s)
+      sp[s] = (s < K::nspec(M)) ? (float)__ldg(a.in[MAM4B_IN_AER_I + K::spec0(M) + (s < K::nspec(M) ? s : 0)] + c) : 0.0f;
+    float dgn_awet, qaerwat, wetdens;
+    f32::water_uptake_mode<M>(C, sp, a.aux[AUX_RH * n + c],
+                              (float)a.out[MAM4B_OUT_DGN_A + M][c], dgn_awet, qaerwat, wetdens);
+    a.out[MAM4B_OUT_DGN_AWET + M][c] = dgn_awet;
+    a.out[MAM4B_OUT_WETDENS + M][c] = wetdens;
+    a.out[MAM4B_OUT_QAERWAT + M][c] = qaerwat;
+    a.aux[(AUX_RATE + M) * n + c] = f32::uptake_rate_mode(
+        C, M, (float)a.aux[AUX_GDIFF * n + c], (float)a.aux[AUX_FPATH * n + c], dgn_awet);
+    return;
+  }
   double sp[7];
 #pragma unroll
   for (int s = 0; s < 7; ++s)
@@ -1020,15 +1038,16 @@ __device__ __forceinline__ void mode_work(const StepArgs &a, const long long c) 
       uptake_rate_mode(C, M, a.aux[AUX_GDIFF * n + c], a.aux[AUX_FPATH * n + c], dgn_awet);
 }
 
+template <bool MIXED>
 __global__ void __launch_bounds__(128) mode_kernel(const __grid_constant__ StepArgs a) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= a.ncell)
     return;
   switch (blockIdx.y) {
-  case 0: mode_work<0>(a, c); break;
-  case 1: mode_work<1>(a, c); break;
-  case 2: mode_work<2>(a, c); break;
-  default: mode_work<3>(a, c); break;
+  case 0: mode_work<0, MIXED>(a, c); break;
+  case 1: mode_work<1, MIXED>(a, c); break;
+  case 2: mode_work<2, MIXED>(a, c); break;
+  default: mode_work<3, MIXED>(a, c); break;
   }
 }
 
@@ -1036,6 +1055,7 @@ __global__ void __launch_bounds__(128) mode_kernel(const __grid_constant__ StepA
 // coefficients of the pair (getcoags, coagulation.hpp:651-817) from the wet
 // sizes and densities of stage 2; they do not depend on what condensation
 // changes, so the post kernel only applies them.
+template <bool MIXED>
 __global__ void __launch_bounds__(128) pair_kernel(const __grid_constant__ StepArgs a) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= a.ncell)
@@ -1050,8 +1070,20 @@ __global__ void __launch_bounds__(128) pair_kernel(const __grid_constant__ StepA
   const double dens_d = dmax(1000.0, a.out[MAM4B_OUT_WETDENS + dm][c]);
   const CoagTables T = {kCoagBm0ij, kCoagBm3i, kCoagBm0};
   double bij0, bij3, bii0, bjj0;
-  coag_pair_coefs(C, T, p, temp, pmid, aircon, a.out[MAM4B_OUT_DGN_AWET + sm][c],
-                  a.out[MAM4B_OUT_DGN_AWET + dm][c], dens_s, dens_d, bij0, bij3, bii0, bjj0);
+  if constexpr (MIXED) {
+    float f0, f3, fi, fj;
+    f32::coag_pair_coefs(C, T, p, (float)temp, (float)pmid, (float)aircon,
+                         (float)a.out[MAM4B_OUT_DGN_AWET + sm][c],
+                         (float)a.out[MAM4B_OUT_DGN_AWET + dm][c], (float)dens_s, (float)dens_d,
+                         f0, f3, fi, fj);
+    bij0 = f0;
+    bij3 = f3;
+    bii0 = fi;
+    bjj0 = fj;
+  } else {
+    coag_pair_coefs(C, T, p, temp, pmid, aircon, a.out[MAM4B_OUT_DGN_AWET + sm][c],
+                    a.out[MAM4B_OUT_DGN_AWET + dm][c], dens_s, dens_d, bij0, bij3, bii0, bjj0);
+  }
   const size_t n = (size_t)a.ncell;
   double *cc = a.aux + AUX_COAG * n + c;
   cc[p * n] = bij0;
@@ -1079,13 +1111,16 @@ __global__ void __launch_bounds__(128) post_kernel(const __grid_constant__ StepA
 // long loops first, so that the last ones handed out are short. The loop
 // is bound by FP64 division latency: 4 blocks of 256 per SM (64 registers)
 // hide more of it than the unconstrained 93-register build.
+// With MIXED the loop runs in single precision (f32::soa_step).
 constexpr int kSoaBlock = 256;
+template <bool MIXED>
 __global__ void __launch_bounds__(kSoaBlock, 4) soa_kernel(const __grid_constant__ StepArgs a) {
+  using State = typename std::conditional<MIXED, f32::SoaStateF, SoaState>::type;
   const unsigned ntask = a.counters[CNT_QUEUED];
   const unsigned nlong = a.counters[CNT_LONG];
   const int lane = threadIdx.x & 31;
   const size_t n = (size_t)a.ncell;
-  SoaState st;
+  State st;
   unsigned slot = 0;
   bool active = false, want = true;
   while (true) {
@@ -1305,7 +1340,7 @@ cudaError_t ensure_solver_scratch(mam4b_ctx *ctx, size_t ncell) {
     if (e == cudaSuccess)
       e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e == cudaSuccess)
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, soa_kernel, kSoaBlock, 0);
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, soa_kernel<false>, kSoaBlock, 0);
     if (e == cudaSuccess)
       ctx->soa_grid = sms * (per_sm > 0 ? per_sm : 1);
   }
@@ -1360,8 +1395,9 @@ void set_step_scratch(const mam4b_ctx *ctx, StepArgs &a, size_t c0, int chunk) {
   a.counters = ctx->d_counters + (size_t)CNT_WORDS * chunk;
 }
 
-// Clears the counters and queues the three pipeline kernels on s.
-cudaError_t launch_pipeline(mam4b_ctx *ctx, const StepArgs &a, cudaStream_t s) {
+// Clears the counters and queues the pipeline kernels on s in the
+// arithmetic of `precision` (mam4b_precision).
+cudaError_t launch_pipeline(mam4b_ctx *ctx, const StepArgs &a, cudaStream_t s, int precision) {
   cudaError_t e = cudaMemsetAsync(a.counters, 0, CNT_WORDS * sizeof(unsigned), s);
   if (e != cudaSuccess)
     return e;
@@ -1376,10 +1412,20 @@ cudaError_t launch_pipeline(mam4b_ctx *ctx, const StepArgs &a, cudaStream_t s) {
     return e;
   }
   size_kernel<<<grid, block, 0, s>>>(a);
-  mode_kernel<<<dim3(grid, NMODE), block, 0, s>>>(a);
-  pair_kernel<<<dim3(grid, 3), block, 0, s>>>(a);
-  pre_kernel<<<grid, block, 0, s>>>(a);
-  soa_kernel<<<ctx->soa_grid, kSoaBlock, 0, s>>>(a);
+  if (precision != MAM4B_FP64) {
+    mode_kernel<true><<<dim3(grid, NMODE), block, 0, s>>>(a);
+    pair_kernel<true><<<dim3(grid, 3), block, 0, s>>>(a);
+    pre_kernel<<<grid, block, 0, s>>>(a);
+    if (precision == MAM4B_MIXED_FAST)
+      soa_kernel<true><<<ctx->soa_grid, kSoaBlock, 0, s>>>(a);
+    else
+      soa_kernel<false><<<ctx->soa_grid, kSoaBlock, 0, s>>>(a);
+  } else {
+    mode_kernel<false><<<dim3(grid, NMODE), block, 0, s>>>(a);
+    pair_kernel<false><<<dim3(grid, 3), block, 0, s>>>(a);
+    pre_kernel<<<grid, block, 0, s>>>(a);
+    soa_kernel<false><<<ctx->soa_grid, kSoaBlock, 0, s>>>(a);
+  }
   post_kernel<<<grid, block, 0, s>>>(a);
   e = cudaGetLastError();
   if (e == cudaSuccess)
@@ -1450,7 +1496,7 @@ cudaError_t noalloc_setup(int dev) {
   int sms = 0, per_sm = 0;
   e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (e == cudaSuccess)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, soa_kernel, kSoaBlock, 0);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, soa_kernel<false>, kSoaBlock, 0);
   if (e != cudaSuccess)
     return e;
   g_noalloc[dev].scratch = static_cast<double *>(p);
@@ -1537,8 +1583,8 @@ mam4b_status mam4b_step(mam4b_ctx *ctx, const mam4b_state_view *in, const mam4b_
                         int ncol, int nlev, double dt, int precision, void *stream) {
   if (!ctx || !in || !out || ncol < 0 || nlev <= 0 || !(dt > 0.0) || !isfinite(dt))
     return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_step", cudaSuccess);
-  if (precision != MAM4B_FP64)
-    return set_err(ctx, MAM4B_ERR_NOT_SUPPORTED, "mam4b_step: precision", cudaSuccess);
+  if (precision != MAM4B_FP64 && precision != MAM4B_MIXED && precision != MAM4B_MIXED_FAST)
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_step: precision", cudaSuccess);
   StepArgs a;
   memset(&a, 0, sizeof(a));
   bool diag = false;
@@ -1569,6 +1615,9 @@ mam4b_status mam4b_step(mam4b_ctx *ctx, const mam4b_state_view *in, const mam4b_
   if (a.ncell > 0x7fffffffLL)
     return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_step: too many cells", cudaSuccess);
   cudaError_t e;
+  if (diag && precision != MAM4B_FP64)
+    return set_err(ctx, MAM4B_ERR_NOT_SUPPORTED,
+                   "mam4b_step: process diagnostics are FP64 only", cudaSuccess);
   if (diag) {
     // per-process diagnostics: one thread per cell, start to end
     full_kernel<true><<<(unsigned)grid, block, 0, s>>>(a);
@@ -1582,7 +1631,7 @@ mam4b_status mam4b_step(mam4b_ctx *ctx, const mam4b_state_view *in, const mam4b_
   if (e != cudaSuccess)
     return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_step scratch", e);
   set_step_scratch(ctx, a, 0, 0);
-  e = launch_pipeline(ctx, a, s);
+  e = launch_pipeline(ctx, a, s, precision);
   if (e != cudaSuccess)
     return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_step launch", e);
   return MAM4B_OK;
@@ -1624,8 +1673,8 @@ mam4b_status mam4b_step_host(mam4b_ctx *ctx, const double *in_slab, const double
   if (!ctx || !in_slab || !pblh || !out_slab || ncol < 0 || nlev <= 0 ||
       ld < (size_t)ncol * (size_t)nlev || !(dt > 0.0) || !isfinite(dt))
     return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_step_host", cudaSuccess);
-  if (precision != MAM4B_FP64)
-    return set_err(ctx, MAM4B_ERR_NOT_SUPPORTED, "mam4b_step_host: precision", cudaSuccess);
+  if (precision != MAM4B_FP64 && precision != MAM4B_MIXED && precision != MAM4B_MIXED_FAST)
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_step_host: precision", cudaSuccess);
   const size_t n = (size_t)ncol * (size_t)nlev;
   if (n > 0x7fffffffULL)
     return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_step_host: too many cells", cudaSuccess);
@@ -1678,7 +1727,7 @@ mam4b_status mam4b_step_host(mam4b_ctx *ctx, const double *in_slab, const double
       a.out[f] = ctx->d_out + (size_t)f * n + c0;
     set_step_config(ctx, a, (long long)nc, nlev, dt);
     set_step_scratch(ctx, a, c0, i);
-    e = launch_pipeline(ctx, a, s);
+    e = launch_pipeline(ctx, a, s, precision);
     if (e == cudaSuccess)
       e = cudaMemcpy2DAsync(out_slab + c0, hp, ctx->d_out + c0, dp, nc * sizeof(double),
                             MAM4B_NOUT, cudaMemcpyDeviceToHost, s);
@@ -1766,10 +1815,10 @@ mam4b_status mam4b_step_slab_noalloc(const mam4b_config *cfg, const double *in_s
     full_kernel<false><<<grid, block, 0, s>>>(a);
   } else {
     size_kernel<<<grid, block, 0, s>>>(a);
-    mode_kernel<<<dim3(grid, NMODE), block, 0, s>>>(a);
-    pair_kernel<<<dim3(grid, 3), block, 0, s>>>(a);
+    mode_kernel<false><<<dim3(grid, NMODE), block, 0, s>>>(a);
+    pair_kernel<false><<<dim3(grid, 3), block, 0, s>>>(a);
     pre_kernel<<<grid, block, 0, s>>>(a);
-    soa_kernel<<<nd.soa_grid, kSoaBlock, 0, s>>>(a);
+    soa_kernel<false><<<nd.soa_grid, kSoaBlock, 0, s>>>(a);
     post_kernel<<<grid, block, 0, s>>>(a);
   }
   e = cudaGetLastError();

@@ -12,7 +12,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "libmam4b.so")
 
 NIN, NOUT, NDIAG, NPOP = 57, 68, 155, 25
-FP64, MIXED = 0, 1
+FP64, MIXED, MIXED_FAST = 0, 1, 2
 STATUS = {0: "ok", 1: "invalid argument", 2: "cuda error", 3: "not supported",
           4: "device flags", 5: "too many cells for the no-alloc scratch"}
 NOALLOC_MAX_CELLS = 16384  # MAM4B_NOALLOC_MAX_CELLS
