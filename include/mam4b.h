@@ -242,6 +242,25 @@ mam4b_status mam4b_step_slab_noalloc(const mam4b_config *cfg, const double *in_s
                                      int ncol, int nlev, double dt, uint32_t *flags,
                                      void *stream);
 
+/*
+ * Reverse-mode adjoint of the FP64 step (no counterpart in the reference,
+ * which has no derivatives): for every cell, in_bar = (d out / d in)^T
+ * out_bar, where out are the MAM4B_NOUT outputs of mam4b_step_slab at the
+ * state in_slab and out_bar their cotangents (MAM4B_NOUT fields of ld
+ * doubles). in_bar receives MAM4B_NIN fields of ld doubles: the gradients
+ * with respect to temperature, water vapour, H2SO4, SOAG and the 50 aerosol
+ * populations; the pressure, height and cloud-fraction rows are written as
+ * zero (these are held fixed), and the boundary-layer height has no
+ * cotangent. The derivative is that of the branch the forward takes at the
+ * given state (max/min clips, process thresholds and the SOA sub-step count
+ * are not differentiated across). The SOA sub-step states are recomputed
+ * from checkpoints kept every 4 sub-steps. Uses the context's config;
+ * asynchronous on `stream`. Device pointers.
+ */
+mam4b_status mam4b_adjoint_slab(mam4b_ctx *ctx, const double *in_slab, const double *pblh,
+                                const double *out_bar, double *in_bar, size_t ld, int ncol,
+                                int nlev, double dt, void *stream);
+
 /* Synchronises the context's last stream, stores in *flags the OR of the
  * MAM4B_FLAG_* bits raised since the previous call (then clears them), and
  * returns MAM4B_ERR_DEVICE_FLAGS if any bit of MAM4B_FLAGS_ERROR_MASK is

@@ -30,6 +30,12 @@ constexpr int NQTEND = 4;
 // coarse, primary carbon, and the tables of the step, as constexpr accessors
 // that fold to immediates once the per-mode loops are unrolled.
 #define MAM4B_HD __host__ __device__ __forceinline__
+// read-only table load: through the non-coherent cache on the device
+#ifdef __CUDA_ARCH__
+#define MAM4B_LDG(p) __ldg(p)
+#else
+#define MAM4B_LDG(p) (*(p))
+#endif
 namespace K {
 constexpr double pi = 3.14159265358979323846264;
 constexpr double pi_sixth = 3.14159265358979323846264 / 6;
@@ -163,13 +169,13 @@ struct CoagTables {
 
 MAM4B_HD double dmax(double a, double b) { return (a < b) ? b : a; }
 MAM4B_HD double dmin(double a, double b) { return (b < a) ? b : a; }
-__device__ __forceinline__ double sq(double x) { return x * x; }
-__device__ __forceinline__ double cube(double x) { return x * x * x; }
-__device__ __forceinline__ double bound(double lo, double hi, double x) { return dmax(lo, dmin(hi, x)); }
-__device__ __forceinline__ double safe_denominator(double x) {
+MAM4B_HD double sq(double x) { return x * x; }
+MAM4B_HD double cube(double x) { return x * x * x; }
+MAM4B_HD double bound(double lo, double hi, double x) { return dmax(lo, dmin(hi, x)); }
+MAM4B_HD double safe_denominator(double x) {
   return x / (x * x + K::eps * K::eps);
 }
-__device__ __forceinline__ double diam_from_vol(double v, double log_sig) {
+MAM4B_HD double diam_from_vol(double v, double log_sig) {
   // conversions.hpp:299-304
   return cbrt(v / K::pi_sixth) * exp(-1.5 * sq(log_sig));
 }
@@ -178,7 +184,7 @@ __device__ __forceinline__ double diam_from_vol(double v, double log_sig) {
 // modal_aero_calcsize.hpp:750-932 with calcsize.hpp:56-310, 314-376, 481-515.
 // ai/ac: 25 populations (mmr). Writes dgn_i and the calcsize tendencies of
 // the populations (pt_i, pt_c, zero where calcsize leaves them).
-__device__ __forceinline__ void adjust_num_sizes(double drv_i, double drv_c, double init_i,
+MAM4B_HD void adjust_num_sizes(double drv_i, double drv_c, double init_i,
                                                  double init_c, double dt, double v2nmin,
                                                  double v2nmax, double adj_inv, double &num_i,
                                                  double &num_c, double &dqdt, double &dqqcwdt) {
@@ -239,7 +245,7 @@ __device__ __forceinline__ void adjust_num_sizes(double drv_i, double drv_c, dou
   dqqcwdt = (num_c - init_c) * dtinv;
 }
 
-__device__ __forceinline__ void diameter_from_num(double drv, double num, double v2nmin,
+MAM4B_HD void diameter_from_num(double drv, double num, double v2nmin,
                                                   double v2nmax, double dgnmin, double dgnmax,
                                                   double log_sig, double &dgn) {
   // calcsize.hpp:56-78 (leaves dgn untouched when drv <= 0)
@@ -253,7 +259,7 @@ __device__ __forceinline__ void diameter_from_num(double drv, double num, double
     dgn = diam_from_vol(1.0 / (num / drv), log_sig);
 }
 
-__device__ __forceinline__ double size_after_transfer(double drv, double num, double v2n_hi,
+MAM4B_HD double size_after_transfer(double drv, double num, double v2n_hi,
                                                       double v2n_lo, double dgn_hi,
                                                       double dgn_lo, double dgn_nom,
                                                       double log_sig) {
@@ -268,7 +274,7 @@ __device__ __forceinline__ double size_after_transfer(double drv, double num, do
   return dgn_nom;
 }
 
-__device__ __forceinline__ void calcsize(const StepConsts &C, const double (&ai)[NPOP],
+MAM4B_HD void calcsize(const StepConsts &C, const double (&ai)[NPOP],
                                          const double (&ac)[NPOP], double dt,
                                          double (&dgn_i)[NMODE], double (&pt_i)[NPOP],
                                          double (&pt_c)[NPOP]) {
@@ -440,15 +446,15 @@ __device__ __forceinline__ void calcsize(const StepConsts &C, const double (&ai)
 struct cplx {
   double re, im;
 };
-__device__ __forceinline__ cplx cmk(double r, double i) { return cplx{r, i}; }
-__device__ __forceinline__ cplx cadd(cplx a, cplx b) { return cmk(a.re + b.re, a.im + b.im); }
-__device__ __forceinline__ cplx csub(cplx a, cplx b) { return cmk(a.re - b.re, a.im - b.im); }
-__device__ __forceinline__ cplx cneg(cplx a) { return cmk(-a.re, -a.im); }
-__device__ __forceinline__ cplx cmul(cplx a, cplx b) {
+MAM4B_HD cplx cmk(double r, double i) { return cplx{r, i}; }
+MAM4B_HD cplx cadd(cplx a, cplx b) { return cmk(a.re + b.re, a.im + b.im); }
+MAM4B_HD cplx csub(cplx a, cplx b) { return cmk(a.re - b.re, a.im - b.im); }
+MAM4B_HD cplx cneg(cplx a) { return cmk(-a.re, -a.im); }
+MAM4B_HD cplx cmul(cplx a, cplx b) {
   return cmk(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re);
 }
-__device__ __forceinline__ cplx cscale(double s, cplx a) { return cmk(s * a.re, s * a.im); }
-__device__ __forceinline__ cplx cdiv(cplx x, cplx y) {
+MAM4B_HD cplx cscale(double s, cplx a) { return cmk(s * a.re, s * a.im); }
+MAM4B_HD cplx cdiv(cplx x, cplx y) {
   const double s = fabs(y.re) + fabs(y.im);
   if (s == 0.0)
     return cmk(x.re / s, x.im / s);
@@ -458,7 +464,7 @@ __device__ __forceinline__ cplx cdiv(cplx x, cplx y) {
   const cplx r = cmul(xs, ycs);
   return cmk(r.re / yabs2, r.im / yabs2);
 }
-__device__ __forceinline__ cplx csqrt_k(cplx x) {
+MAM4B_HD cplx csqrt_k(cplx x) {
   const double r = x.re, i = x.im;
   if (r == 0.0) {
     const double t = sqrt(fabs(i) / 2);
@@ -468,7 +474,7 @@ __device__ __forceinline__ cplx csqrt_k(cplx x) {
   const double u = t / 2;
   return r > 0.0 ? cmk(u, i / t) : cmk(fabs(i) / t, i < 0.0 ? -u : u);
 }
-__device__ __forceinline__ cplx cpow_k(cplx x, double y) {
+MAM4B_HD cplx cpow_k(cplx x, double y) {
   const double r = hypot(x.re, x.im);
   const double th = atan2(x.im, x.re);
   const double rho = pow(r, y), ang = y * th;
@@ -477,7 +483,7 @@ __device__ __forceinline__ cplx cpow_k(cplx x, double y) {
 
 // Smallest real root >= rdry of x^4 + p3 x^3 + p1 x + p0 (p2 = 0),
 // makoh_quartic + find_real_solution (water_uptake.hpp:101-171).
-__device__ __forceinline__ double kohler_quartic_root(double rdry, double p3, double p1,
+MAM4B_HD double kohler_quartic_root(double rdry, double p3, double p1,
                                                       double p0) {
   const double p2 = 0.0;
   const double qq = -p2 * p2 / 36.0 + (p3 * p1 - 4.0 * p0) / 12.0;
@@ -524,7 +530,7 @@ __device__ __forceinline__ double kohler_quartic_root(double rdry, double p3, do
 }
 
 // modal_aero_kohler (water_uptake.hpp:180-230); rdry in m, returns m
-__device__ __forceinline__ double kohler(const StepConsts &C, double rdry_in, double hygro,
+MAM4B_HD double kohler(const StepConsts &C, double rdry_in, double hygro,
                                          double rh) {
   const double eps = 1e-4;
   const double aa = C.kohler_aa;
@@ -546,7 +552,7 @@ __device__ __forceinline__ double kohler(const StepConsts &C, double rdry_in, do
   return rwet * 1.e-6;
 }
 
-__device__ __forceinline__ double qsat_water(double t, double p) {
+MAM4B_HD double qsat_water(double t, double p) {
   // GoffGratch_svp_water + wv_sat_svp_to_qsat (wv_sat_methods.hpp:14-46, 94-115)
   const double tboil = 373.16, ten = 10, one = 1;
   const double es = pow(ten, -7.90298 * (tboil / t - one) + 5.02808 * log10(tboil / t) -
@@ -564,7 +570,7 @@ __device__ __forceinline__ double qsat_water(double t, double p) {
 // modal_aero_water_uptake_dr with wet density (water_uptake.hpp:362-480);
 // uses the state before the calcsize update, like the reference driver.
 // Relative humidity of the clear part of the cell:
-__device__ __forceinline__ double water_uptake_rh(double qv, double temp, double pmid,
+MAM4B_HD double water_uptake_rh(double qv, double temp, double pmid,
                                                   double cldn) {
   const double qs = qsat_water(temp, pmid);
   const double rh_max = 0.98;
@@ -577,7 +583,7 @@ __device__ __forceinline__ double water_uptake_rh(double qv, double temp, double
 
 // One mode: sp holds its species masses in mode order (sp[0..nspec(m)-1]).
 template <int M>
-__device__ __forceinline__ void water_uptake_mode(const StepConsts &C, const double (&sp)[7],
+MAM4B_HD void water_uptake_mode(const StepConsts &C, const double (&sp)[7],
                                                   double rh, double dgn_a, double &dgn_awet,
                                                   double &qaerwat, double &wetdens) {
   double hygro = 0.0, dryvolmr = 0.0, maer = 0.0;
@@ -623,13 +629,13 @@ __device__ __forceinline__ void water_uptake_mode(const StepConsts &C, const dou
 }
 
 template <int M>
-__device__ __forceinline__ void mode_species(const double (&ai)[NPOP], double (&sp)[7]) {
+MAM4B_HD void mode_species(const double (&ai)[NPOP], double (&sp)[7]) {
 #pragma unroll
   for (int s = 0; s < 7; ++s)
     sp[s] = (s < K::nspec(M)) ? ai[K::spec0(M) + (s < K::nspec(M) ? s : 0)] : 0.0;
 }
 
-__device__ __forceinline__ void water_uptake(const StepConsts &C, const double (&ai)[NPOP],
+MAM4B_HD void water_uptake(const StepConsts &C, const double (&ai)[NPOP],
                                              double qv, double temp, double pmid, double cldn,
                                              const double (&dgn_a)[NMODE],
                                              double (&dgn_awet)[NMODE],
@@ -656,9 +662,68 @@ struct Sub {
   double aer[NAER][NMODE];
 };
 
+// State of the clear subarea between the start of condensation and the SOA
+// loop (everything the rest of mam_amicphys_1subarea needs from before it).
+struct ClearMid {
+  double netprod1;
+  double uptk1[NMODE];
+  double sv_so4_ait, sv_soa_ait;
+  // DIAG only: values before condensation
+  double gas_sv[2];
+  double sv_all[NAER][NMODE];
+};
+
+// population slot <-> Sub (mass slots in fcvt units, numbers as is)
+MAM4B_HD void sub_to_pop(const Sub &s, double (&p)[NPOP]) {
+#pragma unroll
+  for (int m = 0; m < NMODE; ++m) {
+    p[K::numslot(m)] = s.num[m];
+#pragma unroll
+    for (int x = 0; x < NAER; ++x)
+      if (K::aer_slot(x, m) >= 0)
+        p[K::aer_slot(x, m)] = s.aer[x][m];
+  }
+}
+MAM4B_HD void pop_to_sub(const double (&p)[NPOP], Sub &s) {
+#pragma unroll
+  for (int m = 0; m < NMODE; ++m) {
+    s.num[m] = p[K::numslot(m)];
+#pragma unroll
+    for (int x = 0; x < NAER; ++x)
+      s.aer[x][m] = (K::aer_slot(x, m) >= 0) ? p[K::aer_slot(x, m)] : 0.0;
+  }
+}
+
+// Sub-area fields of a Sub from populations with per-mode factors
+// (number, mass), as the subarea set-up does (mam4_amicphys.hpp:460-560).
+MAM4B_HD void load_sub(Sub &s, const double (&q)[NPOP],
+                                         const double (&fac_num)[NMODE],
+                                         const double (&fac_mass)[NMODE]) {
+#pragma unroll
+  for (int m = 0; m < NMODE; ++m) {
+    s.num[m] = (q[K::numslot(m)] * fac_num[m]) * 1;
+#pragma unroll
+    for (int x = 0; x < NAER; ++x) {
+      const int slot = K::aer_slot(x, m);
+      s.aer[x][m] = (slot >= 0) ? (q[slot] * fac_mass[m]) * K::fcvt_aer(x) : 0.0;
+    }
+  }
+}
+MAM4B_HD void load_sub_plain(Sub &s, const double (&q)[NPOP]) {
+#pragma unroll
+  for (int m = 0; m < NMODE; ++m) {
+    s.num[m] = q[K::numslot(m)] * 1;
+#pragma unroll
+    for (int x = 0; x < NAER; ++x) {
+      const int slot = K::aer_slot(x, m);
+      s.aer[x][m] = (slot >= 0) ? q[slot] * K::fcvt_aer(x) : 0.0;
+    }
+  }
+}
+
 // gasaerexch.hpp:255-353: uptake rate per unit number of mode n for a gas
 // with the given diffusivity and mean free path (accommodation 0.65)
-__device__ __forceinline__ double uptake_rate_mode(const StepConsts &C, int n, double gasdiffus,
+MAM4B_HD double uptake_rate_mode(const StepConsts &C, int n, double gasdiffus,
                                                    double freepath, double dgn_awet) {
   const double tworootpi = 2 * sqrt(K::pi);
   const double root2 = sqrt(2.0);
@@ -685,7 +750,7 @@ __device__ __forceinline__ double uptake_rate_mode(const StepConsts &C, int n, d
   return constant * gasdiffus * sum;
 }
 
-__device__ __forceinline__ void uptake_rates(const StepConsts &C, double gasdiffus,
+MAM4B_HD void uptake_rates(const StepConsts &C, double gasdiffus,
                                              double freepath, const double (&dgn_awet)[NMODE],
                                              double (&uptk)[NMODE]) {
 #pragma unroll
@@ -695,7 +760,7 @@ __device__ __forceinline__ void uptake_rates(const StepConsts &C, double gasdiff
 
 // H2SO4 gas diffusivity and mean free path (gasaerexch.hpp:223-253,
 // 402-417)
-__device__ __forceinline__ void h2so4_diffusivity(double temp, double pmid, double &gas_diffus,
+MAM4B_HD void h2so4_diffusivity(double temp, double pmid, double &gas_diffus,
                                                   double &freepath) {
   const double p_in_atm = pmid / 1.013e5;
   const double dgas = (1.0e-3 * pow(temp, 1.75) * sqrt(1. / 9.807840000000000E+01 + 0.035)) /
@@ -720,7 +785,7 @@ struct SoaState {
   int niter;
 };
 
-__device__ __forceinline__ void soa_init(SoaState &st, double dtfull, double temp, double pmid,
+MAM4B_HD void soa_init(SoaState &st, double dtfull, double temp, double pmid,
                                          const Sub &s, const double (&uptk)[NMODE]) {
   const double p0_soa = 1.0e-10 * exp(-(156.0e3 / 8.3144) * ((1.0 / temp) - (1.0 / 298.0)));
   st.g0 = 1.01325e5 * p0_soa / pmid;
@@ -739,7 +804,7 @@ __device__ __forceinline__ void soa_init(SoaState &st, double dtfull, double tem
 
 // sum(uptake * |phi|) of the loop's first pass (the first sub-step is
 // 0.05 / this): a cheap predictor of how many passes the loop will take.
-__device__ __forceinline__ double soa_first_rate(const SoaState &st) {
+MAM4B_HD double soa_first_rate(const SoaState &st) {
   const double g = dmax(st.g, 0.0);
   double r = 0.0;
 #pragma unroll
@@ -754,7 +819,7 @@ __device__ __forceinline__ double soa_first_rate(const SoaState &st) {
 }
 
 // One pass of the reference's while loop; false once the loop has ended.
-__device__ __forceinline__ bool soa_step(SoaState &st) {
+MAM4B_HD bool soa_step(SoaState &st) {
   if (!(st.tcur < st.dtfull - 1.0e-3))
     return false;
   st.niter++;
@@ -833,7 +898,7 @@ __device__ __forceinline__ bool soa_step(SoaState &st) {
 
 // Inline form: runs the whole loop for one subarea; returns the sub-step
 // count (1001 when the cap was reached).
-__device__ __forceinline__ int soa_exchange(double dtfull, double temp, double pmid, Sub &s,
+MAM4B_HD int soa_exchange(double dtfull, double temp, double pmid, Sub &s,
                                             const double (&uptk)[NMODE]) {
   SoaState st;
   soa_init(st, dtfull, temp, pmid, s, uptk);
@@ -847,7 +912,7 @@ __device__ __forceinline__ int soa_exchange(double dtfull, double temp, double p
 }
 
 // H2SO4 quasi-analytic update (gasaerexch.hpp:486-537)
-__device__ __forceinline__ void h2so4_update(double dt, double netprod, Sub &s,
+MAM4B_HD void h2so4_update(double dt, double netprod, Sub &s,
                                              const double (&uptk)[NMODE], double &qavg) {
   const double q1 = s.gas[1];
   double tmpa = 0.0;
@@ -884,7 +949,7 @@ __device__ __forceinline__ void h2so4_update(double dt, double netprod, Sub &s,
 // the pair constants of find_renaming_pairs :393-476). grow_i/grow_c are
 // the growth increments of the aitken species (AeroId order).
 template <bool CLOUDY>
-__device__ __forceinline__ void rename_subarea(const StepConsts &C, Sub &si, Sub &sc,
+MAM4B_HD void rename_subarea(const StepConsts &C, Sub &si, Sub &sc,
                                                const double (&grow_i)[NAER],
                                                const double (&grow_c)[NAER]) {
   const int src = 1, dst = 0;
@@ -972,12 +1037,12 @@ __device__ __forceinline__ void rename_subarea(const StepConsts &C, Sub &si, Sub
 
 // ------------------------------------------------------------ nucleation
 // Vehkamaki et al. (2002) fits (vehkamaki2002.hpp:54-190)
-__device__ __forceinline__ double veh02_x_crit(double lna, double t, double lrh) {
+MAM4B_HD double veh02_x_crit(double lna, double t, double lrh) {
   return 0.740997 - 0.00266379 * t - 0.00349998 * lna + 0.0000504022 * t * lna +
          0.00201048 * lrh - 0.000183289 * t * lrh + 0.00157407 * sq(lrh) -
          0.0000179059 * t * sq(lrh) + 0.000184403 * cube(lrh) - 1.50345e-6 * t * cube(lrh);
 }
-__device__ __forceinline__ double veh02_log_rate(double lna, double t, double lrh, double x) {
+MAM4B_HD double veh02_log_rate(double lna, double t, double lrh, double x) {
   const double a = 0.14309 + 2.21956 * t - 0.0273911 * sq(t) + 0.0000722811 * cube(t) + 5.91822 / x;
   const double b = 0.117489 + 0.462532 * t - 0.0118059 * sq(t) + 0.0000404196 * cube(t) + 15.7963 / x;
   const double c = -0.215554 - 0.0810269 * t + 0.00143581 * sq(t) - 4.7758e-6 * cube(t) - 2.91297 / x;
@@ -991,7 +1056,7 @@ __device__ __forceinline__ double veh02_log_rate(double lna, double t, double lr
   return a + b * lrh + c * sq(lrh) + d * cube(lrh) + e * lna + f * lrh * lna + g * sq(lrh) * lna +
          h * sq(lna) + i * lrh * sq(lna) + j * cube(lna);
 }
-__device__ __forceinline__ double veh02_ntot(double lna, double t, double lrh, double x) {
+MAM4B_HD double veh02_ntot(double lna, double t, double lrh, double x) {
   const double A = -0.00295413 - 0.0976834 * t + 0.00102485 * sq(t) - 2.18646e-6 * cube(t) - 0.101717 / x;
   const double B = -0.00205064 - 0.00758504 * t + 0.000192654 * sq(t) - 6.7043e-7 * cube(t) - 0.255774 / x;
   const double Cc = +0.00322308 + 0.000852637 * t - 0.0000154757 * sq(t) + 5.66661e-8 * cube(t) + 0.0338444 / x;
@@ -1010,7 +1075,7 @@ __device__ __forceinline__ double veh02_ntot(double lna, double t, double lrh, d
 // mer07_veh02_nuc_mosaic_1box (nucleation.hpp:347-860) for method 11, one
 // size bin, no NH3. Quirk kept: a critical cluster that falls between the
 // bin bounds produces nothing (nucleation.hpp:620-631).
-__device__ __forceinline__ void nucleation(const StepConsts &C, double deltat, double temp,
+MAM4B_HD void nucleation(const StepConsts &C, double deltat, double temp,
                                            double pmid, double zmid, double pblh, double relhum,
                                            double uptkrate_h2so4, double qgas_avg1, Sub &s) {
   const double qh2so4_cur = s.gas[1];
@@ -1146,7 +1211,7 @@ __device__ __forceinline__ void nucleation(const StepConsts &C, double deltat, d
 
 // ----------------------------------------------------------- coagulation
 // getcoags_wrapper_f + getcoags (coagulation.hpp:651-817) for one mode pair
-__device__ __forceinline__ void coag_coefs(const CoagTables &T, double airtemp, double airprs,
+MAM4B_HD void coag_coefs(const CoagTables &T, double airtemp, double airprs,
                                            double dgatk, double dgacc, double sgatk,
                                            double sgacc, double xxlsgat, double xxlsgac,
                                            double pdensat, double pdensac, double &bij0,
@@ -1194,8 +1259,8 @@ __device__ __forceinline__ void coag_coefs(const CoagTables &T, double airtemp, 
   // the reference passes (n1, n2n, n2a) into bm*_data(n1, n2a, n2n)
   // (coagulation.hpp:309, 558), i.e. it reads table[n1][n2n][n2a]
   const int tix = n1 * 100 + n2n * 10 + n2a;
-  const double bm0ij = __ldg(T.bm0ij + tix);
-  const double bm3i = __ldg(T.bm3i + tix);
+  const double bm0ij = MAM4B_LDG(T.bm0ij + tix);
+  const double bm3i = MAM4B_LDG(T.bm3i + tix);
   const double coagnc0 = knc * (2.0 + a * (kngat * (esat04 + r2 * esat16 * esac04) +
                                            kngac * (esac04 + ri2 * esac16 * esat04)) +
                                 (r2 + ri2) * esat04 * esac04);
@@ -1215,10 +1280,10 @@ __device__ __forceinline__ void coag_coefs(const CoagTables &T, double airtemp, 
                           2.0 * ri1 * esat64 * esac01);
   const double qv12 = coagnc3 * coagfm3 / (coagnc3 + coagfm3);
   const double cnc11 = knc * (1.0 + esat08 + a * kngat * (esat20 + esat04));
-  const double cfm11 = kfmat * sqdgat * __ldg(T.bm0 + n2n) * (esat01 + esat25 + 2.0 * esat05);
+  const double cfm11 = kfmat * sqdgat * MAM4B_LDG(T.bm0 + n2n) * (esat01 + esat25 + 2.0 * esat05);
   const double qn11 = cfm11 * cnc11 / (cfm11 + cnc11);
   const double cnc22 = knc * (1.0 + esac08 + a * kngac * (esac20 + esac04));
-  const double cfm22 = kfmac * sqdgac * __ldg(T.bm0 + n2a) * (esac01 + esac25 + 2.0 * esac05);
+  const double cfm22 = kfmac * sqdgac * MAM4B_LDG(T.bm0 + n2a) * (esac01 + esac25 + 2.0 * esac05);
   const double qn22 = cfm22 * cnc22 / (cfm22 + cnc22);
   bii0 = dmax(0.0, qn11);
   bjj0 = dmax(0.0, qn22);
@@ -1227,7 +1292,7 @@ __device__ __forceinline__ void coag_coefs(const CoagTables &T, double airtemp, 
   bij3 = dmax(0.0, qv12 / dumatk3);
 }
 
-__device__ __forceinline__ double qnum_intra_inter(double bijdtqnumj, double biidt,
+MAM4B_HD double qnum_intra_inter(double bijdtqnumj, double biidt,
                                                    double qnumi_bgn) {
   // coagulation.hpp:938-952
   if (bijdtqnumj < 1.0e-5)
@@ -1242,7 +1307,7 @@ __device__ __forceinline__ double qnum_intra_inter(double bijdtqnumj, double bii
 // cc[0..2] bij0, cc[3..5] bij3, cc[6..8] bii0, cc[9..11] bjj0.
 MAM4B_HD constexpr int coag_src(int p) { return p == 1 ? 3 : 1; }
 MAM4B_HD constexpr int coag_dst(int p) { return p == 2 ? 3 : 0; }
-__device__ __forceinline__ void coag_pair_coefs(const StepConsts &C, const CoagTables &T, int p,
+MAM4B_HD void coag_pair_coefs(const StepConsts &C, const CoagTables &T, int p,
                                                 double temp, double pmid, double aircon,
                                                 double dgn_src, double dgn_dst, double dens_src,
                                                 double dens_dst, double &bij0, double &bij3,
@@ -1256,7 +1321,7 @@ __device__ __forceinline__ void coag_pair_coefs(const StepConsts &C, const CoagT
   bjj0 *= aircon;
 }
 
-__device__ __forceinline__ void coag_all_coefs(const StepConsts &C, const CoagTables &T,
+MAM4B_HD void coag_all_coefs(const StepConsts &C, const CoagTables &T,
                                                double temp, double pmid, double aircon,
                                                const double (&dgn_awet)[NMODE],
                                                const double (&wetdens)[NMODE], double (&cc)[12]) {
@@ -1270,7 +1335,7 @@ __device__ __forceinline__ void coag_all_coefs(const StepConsts &C, const CoagTa
 // mam_coag_1subarea (coagulation.hpp:1038-1119) with the coefficients cc of
 // coag_all_coefs; coag_in receives the mass moved into the primary-carbon
 // mode (AeroId order)
-__device__ __forceinline__ void coagulation(double deltat, const double (&cc)[12], Sub &s,
+MAM4B_HD void coagulation(double deltat, const double (&cc)[12], Sub &s,
                                             double (&coag_in)[NAER]) {
   double bgn[NAER][NMODE], nbgn[NMODE];
 #pragma unroll
@@ -1335,7 +1400,7 @@ __device__ __forceinline__ void coagulation(double deltat, const double (&cc)[12
 
 // ------------------------------------------------------------------ aging
 // mam_pcarbon_aging_1subarea (aging.hpp:70-361)
-__device__ __forceinline__ void aging(const StepConsts &C, unsigned nmono, double dgn_a_pc, Sub &s,
+MAM4B_HD void aging(const StepConsts &C, unsigned nmono, double dgn_a_pc, Sub &s,
                                       double (&dnum_cond)[NMODE], double (&dnum_coag)[NMODE],
                                       double (&daer_cond)[NAER][NMODE],
                                       double (&daer_coag)[NAER][NMODE],

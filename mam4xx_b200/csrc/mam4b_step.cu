@@ -20,6 +20,7 @@
 #include "../../include/mam4b.h"
 #include "mam4b_physics.cuh"
 #include "mam4b_physics_mixed.cuh"
+#include "mam4b_adjoint.cuh"
 
 namespace mam4b {
 
@@ -101,17 +102,6 @@ enum {
   H_CI = 60,       // 25 interstitial contributions of the cloudy subarea
   H_CG = 85,       // 2 gas contributions of the cloudy subarea (SOAG, H2SO4)
   H_FIELDS = 87
-};
-
-// State of the clear subarea between the start of condensation and the SOA
-// loop (everything the rest of mam_amicphys_1subarea needs from before it).
-struct ClearMid {
-  double netprod1;
-  double uptk1[NMODE];
-  double sv_so4_ait, sv_soa_ait;
-  // DIAG only: values before condensation
-  double gas_sv[2];
-  double sv_all[NAER][NMODE];
 };
 
 // Clear subarea, mam_amicphys_1subarea (mam4_amicphys.hpp:1127-1697), part 1:
@@ -359,27 +349,6 @@ __device__ __forceinline__ int clear_subarea(const StepArgs &a, double deltat, d
   return niter;
 }
 
-// population slot <-> Sub (mass slots in fcvt units, numbers as is)
-__device__ __forceinline__ void sub_to_pop(const Sub &s, double (&p)[NPOP]) {
-#pragma unroll
-  for (int m = 0; m < NMODE; ++m) {
-    p[K::numslot(m)] = s.num[m];
-#pragma unroll
-    for (int x = 0; x < NAER; ++x)
-      if (K::aer_slot(x, m) >= 0)
-        p[K::aer_slot(x, m)] = s.aer[x][m];
-  }
-}
-__device__ __forceinline__ void pop_to_sub(const double (&p)[NPOP], Sub &s) {
-#pragma unroll
-  for (int m = 0; m < NMODE; ++m) {
-    s.num[m] = p[K::numslot(m)];
-#pragma unroll
-    for (int x = 0; x < NAER; ++x)
-      s.aer[x][m] = (K::aer_slot(x, m) >= 0) ? p[K::aer_slot(x, m)] : 0.0;
-  }
-}
-
 __device__ __forceinline__ void store_outputs(const StepArgs &a, long long c, double o_h2so4,
                                               double o_soag, const double (&oi)[NPOP],
                                               const double (&oc)[NPOP], double h2so4, double soag,
@@ -475,33 +444,6 @@ __device__ __forceinline__ void cell_front(const StepArgs &a, const long long c,
   const double ev_sat = 1.00071 * exp(4.5e-8 * f.pmid) * ew;
   const double qv_sat = epsqs * ev_sat / (f.pmid - (1 - epsqs) * ev_sat);
   f.relhumgcm = dmax(0.0, dmin(1.0, f.qv / qv_sat));
-}
-
-// Sub-area fields of a Sub from populations with per-mode factors
-// (number, mass), as the subarea set-up does (mam4_amicphys.hpp:460-560).
-__device__ __forceinline__ void load_sub(Sub &s, const double (&q)[NPOP],
-                                         const double (&fac_num)[NMODE],
-                                         const double (&fac_mass)[NMODE]) {
-#pragma unroll
-  for (int m = 0; m < NMODE; ++m) {
-    s.num[m] = (q[K::numslot(m)] * fac_num[m]) * 1;
-#pragma unroll
-    for (int x = 0; x < NAER; ++x) {
-      const int slot = K::aer_slot(x, m);
-      s.aer[x][m] = (slot >= 0) ? (q[slot] * fac_mass[m]) * K::fcvt_aer(x) : 0.0;
-    }
-  }
-}
-__device__ __forceinline__ void load_sub_plain(Sub &s, const double (&q)[NPOP]) {
-#pragma unroll
-  for (int m = 0; m < NMODE; ++m) {
-    s.num[m] = q[K::numslot(m)] * 1;
-#pragma unroll
-    for (int x = 0; x < NAER; ++x) {
-      const int slot = K::aer_slot(x, m);
-      s.aer[x][m] = (slot >= 0) ? q[slot] * K::fcvt_aer(x) : 0.0;
-    }
-  }
 }
 
 // Renaming of a cloudy (sub)area, interstitial si and cloud-borne sc,
@@ -1168,6 +1110,49 @@ __global__ void __launch_bounds__(kSoaBlock, 4) soa_kernel(const __grid_constant
   }
 }
 
+// ============================================================ adjoint
+// Reverse-mode adjoint of the FP64 step: in_bar = (d out / d in)^T out_bar
+// per cell. Persistent threads; each runs one cell's forward sweep (state
+// at process boundaries in local memory, the SOA loop's state every
+// adj::kSoaCheck passes in its own slice of `ck`, laid out
+// [checkpoint][component][thread] so a warp's accesses are coalesced) and
+// then its reverse sweep.
+struct AdjArgs {
+  const double *in;    // [MAM4B_NIN][ld]
+  const double *pblh;  // [ncol]
+  const double *ybar;  // [MAM4B_NOUT][ld]
+  double *xbar;        // [MAM4B_NIN][ld]
+  size_t ld;
+  long long ncell;
+  int nlev;
+  double dt;
+  adj::AdjCfg cfg;
+  double *ck;          // [6 * kSoaCkMax][nthreads]
+};
+
+__global__ void __launch_bounds__(128) adjoint_kernel(const __grid_constant__ AdjArgs a) {
+  const size_t nthreads = (size_t)gridDim.x * blockDim.x;
+  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const CoagTables T = {kCoagBm0ij, kCoagBm3i, kCoagBm0};
+  double *ck = a.ck + tid;
+  for (long long c = (long long)tid; c < a.ncell; c += (long long)nthreads) {
+    double x[MAM4B_NIN], yb[MAM4B_NOUT], y[MAM4B_NOUT], xb[MAM4B_NIN];
+#pragma unroll
+    for (int f = 0; f < MAM4B_NIN; ++f)
+      x[f] = __ldg(a.in + (size_t)f * a.ld + c);
+#pragma unroll
+    for (int f = 0; f < MAM4B_NOUT; ++f)
+      yb[f] = __ldg(a.ybar + (size_t)f * a.ld + c);
+    const double pblh = __ldg(a.pblh + c / a.nlev);
+    adj::CellTape tp;
+    adj::cell_forward(c_k, T, a.cfg, x, pblh, a.dt, tp, ck, nthreads, y);
+    adj::cell_reverse(c_k, T, a.cfg, x, pblh, a.dt, tp, ck, nthreads, yb, xb);
+#pragma unroll
+    for (int f = 0; f < MAM4B_NIN; ++f)
+      a.xbar[(size_t)f * a.ld + c] = xb[f];
+  }
+}
+
 // ====================================================== derived constants
 // Evaluated once per device by a one-thread kernel, with the same
 // expressions the reference evaluates inline (and the same math library the
@@ -1285,6 +1270,9 @@ struct mam4b_ctx {
   unsigned *d_counters;  // CNT_WORDS per chunk of the host path
   size_t cap_cells;
   int soa_grid;  // persistent solver blocks (SMs x resident blocks)
+  // adjoint: SOA checkpoints of the persistent threads (allocated on first use)
+  double *d_ck;
+  int adj_grid;
   // host path: copy/compute streams and their events (created on first use)
   cudaStream_t hs[kHostStreams];
   cudaEvent_t ev_start, ev_done[kHostStreams];
@@ -1568,6 +1556,7 @@ mam4b_status mam4b_destroy(mam4b_ctx *ctx) {
   cudaFree(ctx->d_order);
   cudaFree(ctx->d_aux);
   cudaFree(ctx->d_counters);
+  cudaFree(ctx->d_ck);
   if (ctx->host_streams) {
     for (int k = 0; k < kHostStreams; ++k) {
       cudaStreamDestroy(ctx->hs[k]);
@@ -1823,6 +1812,54 @@ mam4b_status mam4b_step_slab_noalloc(const mam4b_config *cfg, const double *in_s
   }
   e = cudaGetLastError();
   return e == cudaSuccess ? MAM4B_OK : MAM4B_ERR_CUDA;
+}
+
+mam4b_status mam4b_adjoint_slab(mam4b_ctx *ctx, const double *in_slab, const double *pblh,
+                                const double *out_bar, double *in_bar, size_t ld, int ncol,
+                                int nlev, double dt, void *stream) {
+  if (!ctx || !in_slab || !pblh || !out_bar || !in_bar || ncol < 0 || nlev <= 0 ||
+      ld < (size_t)ncol * (size_t)nlev || !(dt > 0.0) || !isfinite(dt))
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_adjoint_slab", cudaSuccess);
+  cudaStream_t s = (cudaStream_t)stream;
+  ctx->last_stream = s;
+  const long long ncell = (long long)ncol * nlev;
+  if (ncell == 0)
+    return MAM4B_OK;
+  cudaError_t e = cudaSuccess;
+  if (!ctx->d_ck) {
+    int dev = 0, sms = 0, per_sm = 0;
+    e = cudaGetDevice(&dev);
+    if (e == cudaSuccess)
+      e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_kernel, 128, 0);
+    if (e == cudaSuccess) {
+      ctx->adj_grid = sms * (per_sm > 0 ? per_sm : 1);
+      e = cudaMalloc(&ctx->d_ck, (size_t)6 * adj::kSoaCkMax * ctx->adj_grid * 128 * sizeof(double));
+    }
+    if (e != cudaSuccess) {
+      ctx->d_ck = nullptr;
+      return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_adjoint_slab scratch", e);
+    }
+  }
+  AdjArgs a;
+  a.in = in_slab;
+  a.pblh = pblh;
+  a.ybar = out_bar;
+  a.xbar = in_bar;
+  a.ld = ld;
+  a.ncell = ncell;
+  a.nlev = nlev;
+  a.dt = dt;
+  a.cfg = adj::AdjCfg{ctx->cfg.do_cond, ctx->cfg.do_rename, ctx->cfg.do_newnuc, ctx->cfg.do_coag,
+                      ctx->cfg.gaexch_h2so4_uptake_optaa, ctx->cfg.n_so4_monolayers_pcage};
+  a.ck = ctx->d_ck;
+  adjoint_kernel<<<ctx->adj_grid, 128, 0, s>>>(a);
+  e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_adjoint_slab launch", e);
+  ctx->launches += 1;
+  return MAM4B_OK;
 }
 
 mam4b_status mam4b_last_status(mam4b_ctx *ctx, uint32_t *flags) {

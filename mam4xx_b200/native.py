@@ -67,6 +67,8 @@ def lib():
         L.mam4b_last_error.argtypes = [P, ctypes.c_char_p, S]
         L.mam4b_step_slab_noalloc.argtypes = [ctypes.POINTER(Config), P, P, P, S, I, I, D, P, P]
         L.mam4b_step_slab_noalloc.restype = I
+        L.mam4b_adjoint_slab.argtypes = [P, P, P, P, P, S, I, I, D, P]
+        L.mam4b_adjoint_slab.restype = I
         L.mam4b_launch_count.argtypes = [P]
         L.mam4b_launch_count.restype = ctypes.c_uint64
         _lib = L
@@ -75,7 +77,8 @@ def lib():
 
 EXPORTED = ["mam4b_abi_version", "mam4b_default_config", "mam4b_create", "mam4b_destroy",
             "mam4b_step", "mam4b_step_slab", "mam4b_step_host", "mam4b_last_status",
-            "mam4b_last_error", "mam4b_launch_count", "mam4b_step_slab_noalloc"]
+            "mam4b_last_error", "mam4b_launch_count", "mam4b_step_slab_noalloc",
+            "mam4b_adjoint_slab"]
 
 
 def default_config(**overrides):
@@ -146,6 +149,14 @@ class Context:
                                        int(nlev), float(dt), int(precision),
                                        ctypes.c_void_p(stream))
         self._check(st, "mam4b_step_host")
+
+    def adjoint_slab(self, in_ptr, pblh_ptr, out_bar_ptr, in_bar_ptr, ld, ncol, nlev, dt,
+                     stream=0):
+        """in_bar = (d out / d in)^T out_bar (mam4b_adjoint_slab)."""
+        st = self._lib.mam4b_adjoint_slab(self._h, in_ptr, pblh_ptr, out_bar_ptr, in_bar_ptr,
+                                          int(ld), int(ncol), int(nlev), float(dt),
+                                          ctypes.c_void_p(stream))
+        self._check(st, "mam4b_adjoint_slab")
 
     def last_status(self):
         f = ctypes.c_uint32(0)
