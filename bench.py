@@ -141,6 +141,108 @@ def cpu_baseline(x, pblh_cell, dt, target_s=12.0):
             "sample": "first %d cells of the %s workload (%.1f s, OpenMP over cells)" % (n, WORKLOAD, el)}
 
 
+def adjoint_leg(native, torch, dev, stream, args, ws):
+    """Adjoint configuration: 16,384 columns x 72 levels (c5). Forward and
+    adjoint (mam4b_adjoint_slab) timed with CUDA events on the same inputs;
+    the cotangent is that of accumulation-mode number and SO4 mass after the
+    step (both phases), column-integrated with weights pdel/g. A central
+    finite-difference check (relative step 1e-6) of that gradient on 64
+    cells reports the agreement in units of relative sensitivity."""
+    from mam4xx_b200.workloads import make_workload
+    wa = make_workload("c5", seed=20261203 + 4 + 1000 * int(os.environ.get("RANK", "0")))
+    xa = torch.from_numpy(wa["in_slab"]).to(dev)
+    pba = torch.from_numpy(wa["pblh"]).to(dev)
+    na = xa.shape[1]
+    p = wa["in_slab"][1].reshape(wa["ncol"], wa["nlev"])
+    edges = np.concatenate([p[:, :1] * 0.5, 0.5 * (p[:, 1:] + p[:, :-1]), p[:, -1:] * 1.01], axis=1)
+    wts = (np.abs(np.diff(edges, axis=1)) / 9.80616).reshape(-1)
+    jstate = [2 + 7, 2 + 0, 27 + 7, 27 + 0]
+    ybar_h = np.zeros((native.NOUT, na))
+    for k in jstate:
+        ybar_h[k] = wts * wa["dt"]
+    ybar = torch.from_numpy(ybar_h).to(dev)
+    outa = torch.empty((native.NOUT, na), dtype=torch.float64, device=dev)
+    xbar = torch.empty((native.NIN, na), dtype=torch.float64, device=dev)
+    actx = native.Context()
+
+    def fwd():
+        actx.step_slab(xa.data_ptr(), pba.data_ptr(), outa.data_ptr(), na, wa["ncol"], wa["nlev"],
+                       wa["dt"], stream=stream.cuda_stream)
+
+    def adj():
+        actx.adjoint_slab(xa.data_ptr(), pba.data_ptr(), ybar.data_ptr(), xbar.data_ptr(), na,
+                          wa["ncol"], wa["nlev"], wa["dt"], stream=stream.cuda_stream)
+
+    times = {}
+    ka = max(2, min(args.steps, 5))
+    for name, f in (("forward", fwd), ("adjoint", adj)):
+        for _ in range(args.warmup):
+            f()
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(ka):
+            f()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times[name] = e0.elapsed_time(e1) / ka
+    # finite-difference check on 64 cells (first 8 columns x 8 levels)
+    g = xbar.cpu().numpy()
+    x_h = wa["in_slab"]
+    fwd()
+    torch.cuda.synchronize()
+    out_h = outa.cpu().numpy()
+    # 64 cells: 8 levels spread through each of the first 8 columns
+    sub = np.concatenate([c * wa["nlev"] + np.arange(0, wa["nlev"], wa["nlev"] // 8)[:8]
+                          for c in range(8)])
+    ncs = 8
+    xs = x_h[:, :ncs * wa["nlev"]]
+    j0 = wts[:ncs * wa["nlev"]] * sum(xs[5 + k] + out_h[k, :ncs * wa["nlev"]] * wa["dt"] for k in jstate)
+    gs = g[:, :ncs * wa["nlev"]].copy()
+    for k in jstate:
+        gs[5 + k] += wts[:ncs * wa["nlev"]]
+    tx = torch.empty((native.NIN, ncs * wa["nlev"]), dtype=torch.float64, device=dev)
+    to = torch.empty((native.NOUT, ncs * wa["nlev"]), dtype=torch.float64, device=dev)
+    tp = pba[:ncs].contiguous()
+    fctx = native.Context()
+
+    def jcells(xv):
+        tx.copy_(torch.from_numpy(xv))
+        fctx.step_slab(tx.data_ptr(), tp.data_ptr(), to.data_ptr(), xv.shape[1], ncs, wa["nlev"],
+                       wa["dt"], stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        o = to.cpu().numpy()
+        return wts[:ncs * wa["nlev"]] * sum(xv[5 + k] + o[k] * wa["dt"] for k in jstate)
+
+    errs = []
+    for f in [0, 3, 5, 6] + list(range(7, 57)):
+        h = 1e-6 * np.abs(xs[f])
+        xp = xs.copy()
+        xm = xs.copy()
+        xp[f] += h
+        xm[f] -= h
+        fd = (jcells(xp) - jcells(xm)) / np.where(h > 0, 2 * h, 1.0)
+        for c in sub:
+            if xs[f, c] != 0.0:
+                errs.append(abs(gs[f, c] - fd[c]) * abs(xs[f, c]) / abs(j0[c]))
+    errs = np.array(errs)
+    fctx.close()
+    actx.close()
+    return {"workload": "c5: 16384 columns x 72 levels, FP64, dt=1800 s",
+            "objective": "accumulation-mode number + SO4 (interstitial + cloud-borne) after the step, "
+                         "weights pdel/g; gradient w.r.t. T, qv, H2SO4, SOAG, 50 populations",
+            "forward_ms": times["forward"], "adjoint_ms": times["adjoint"],
+            "adjoint_over_forward": times["adjoint"] / times["forward"],
+            "fd_check": {"cells": 64, "entries": int(errs.size), "rel_step": 1e-6,
+                         "units": "|g - fd| |x| / |J_cell|",
+                         "median": float(np.median(errs)), "max": float(errs.max()),
+                         "within_1e-6": float((errs <= 1e-6).mean())}}
+
+
 def run_reference_arm(args):
     ws, rank, _ = _dist()
     if rank != 0:
@@ -184,6 +286,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision legs")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint leg")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -322,6 +425,10 @@ def main():
                                 "per_output_median": r["per_output_median"]}}
         step(native.FP64)
 
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = adjoint_leg(native, torch, dev, stream, args, ws)
+
     peak, peak_kind = _peaks()
     alg_bytes = n * BYTES_PER_CELL + ncol * 8
     achieved = alg_bytes / (kernel_ms * 1e-3) / 1e9
@@ -342,6 +449,7 @@ def main():
                      "kernel_ms": kernel_ms, "algorithmic_bytes_per_launch": alg_bytes},
         "e2e": e2e,
         "precisions": precisions,
+        "adjoint": adjoint,
         "gpu_launches": int(launches),
         "clocks": clocks,
         "device_flags": flags,
