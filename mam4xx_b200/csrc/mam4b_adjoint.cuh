@@ -1949,23 +1949,6 @@ MAM4B_HD void part_factors_rev(double fcldy, double q_i, double q_c, double fcb,
   q_cb += i0b * (1.0 - 1.0 / fcldy);
 }
 
-// state of the forward sweep a cell's reverse needs (about 3 KB)
-struct CellTape {
-  int cat;  // 0 clear, 1 cloudy, 2 partly cloudy
-  double dgn_a[NMODE], dgn_awet[NMODE], wetdens_wu[NMODE], wetdens[NMODE], rh_wu;
-  double qi[NPOP], qc[NPOP], g_h2so4, g_soag, relhumgcm;
-  // partly cloudy
-  double fn_c[NMODE], fn_y[NMODE], fm_c[NMODE], fm_y[NMODE], gcl[2], gcy[2], rhc;
-  bool gcy_clip[2];
-  Sub cy_si, cy_sc;  // cloudy subarea before renaming
-  // clear subarea
-  Sub s_entry, s_pre_soa, s_soa, s_h2so4, s_ren, s_nuc, s_coag;
-  double qgas1[2], rh_sub, gd, fp, rate[NMODE], cc[12], qavg, grow[NAER];
-  ClearMid cm;
-  SoaState soa0;
-  int niter;
-};
-
 // SOA loop with checkpoints of (g, a[4], tcur) every kSoaCheck passes
 constexpr int kSoaCheck = 4;
 constexpr int kSoaCkMax = 1001 / kSoaCheck + 2;
@@ -2013,264 +1996,6 @@ MAM4B_HD void soa_loop_rev(const SoaState &init, int passes, const double *ck, s
   }
 }
 
-// forward sweep of one cell (the arithmetic of cell_step<false>); y gets
-// the 68 outputs
-MAM4B_HD void cell_forward(const StepConsts &C, const CoagTables &T, const AdjCfg &cf,
-                           const double (&x)[MAM4B_NIN], double pblh, double dt, CellTape &tp,
-                           double *ck, size_t cks, double (&y)[MAM4B_NOUT]) {
-  const double temp = x[MAM4B_IN_T], pmid = x[MAM4B_IN_P], zm = x[MAM4B_IN_ZM];
-  const double qv = x[MAM4B_IN_QV], cld = x[MAM4B_IN_CLD];
-  double ai[NPOP], ac[NPOP];
-#pragma unroll
-  for (int p = 0; p < NPOP; ++p) {
-    ai[p] = x[MAM4B_IN_AER_I + p];
-    ac[p] = x[MAM4B_IN_AER_C + p];
-  }
-  double pt_i[NPOP], pt_c[NPOP], qaerwat[NMODE];
-  calcsize(C, ai, ac, dt, tp.dgn_a, pt_i, pt_c);
-  water_uptake(C, ai, qv, temp, pmid, cld, tp.dgn_a, tp.dgn_awet, qaerwat, tp.wetdens_wu);
-  tp.rh_wu = water_uptake_rh(qv, temp, pmid, cld);
-#pragma unroll
-  for (int m = 0; m < NMODE; ++m) {
-    y[MAM4B_OUT_DGN_A + m] = tp.dgn_a[m];
-    y[MAM4B_OUT_DGN_AWET + m] = tp.dgn_awet[m];
-    y[MAM4B_OUT_WETDENS + m] = tp.wetdens_wu[m];
-    y[MAM4B_OUT_QAERWAT + m] = qaerwat[m];
-    tp.wetdens[m] = dmax(1000.0, tp.wetdens_wu[m]);
-  }
-#pragma unroll
-  for (int p = 0; p < NPOP; ++p) {
-    tp.qi[p] = dmax(0.0, dmax(0.0, ai[p] + pt_i[p] * dt) * C.to_vmr[2 + p]);
-    tp.qc[p] = dmax(0.0, dmax(0.0, ac[p] + pt_c[p] * dt) * C.to_vmr[2 + p]);
-  }
-  tp.g_h2so4 = dmax(0.0, x[MAM4B_IN_H2SO4] * C.to_vmr[0]);
-  tp.g_soag = dmax(0.0, x[MAM4B_IN_SOAG] * C.to_vmr[1]);
-  {
-    const double epsqs = 0.018016 / 0.028966;
-    const double tc = temp - 273.15;
-    const double ew = 610.94 * ::exp(17.625 * tc / (234.04 + tc));
-    const double ev_sat = 1.00071 * ::exp(4.5e-8 * pmid) * ew;
-    const double qv_sat = epsqs * ev_sat / (pmid - (1 - epsqs) * ev_sat);
-    tp.relhumgcm = dmax(0.0, dmin(1.0, qv / qv_sat));
-  }
-  const double fsoag = C.fcvt_soag;
-  const bool map_gas = cf.do_cond || cf.do_newnuc;
-  double o_h2so4, o_soag, oi[NPOP], oc[NPOP];
-  tp.niter = 0;
-  if (cld > 0.999) {
-    tp.cat = 1;
-    Sub si, sc;
-    load_sub_plain(si, tp.qi);
-    load_sub_plain(sc, tp.qc);
-    si.gas[0] = si.gas[1] = sc.gas[0] = sc.gas[1] = 0.0;
-    tp.cy_si = si;
-    tp.cy_sc = sc;
-    if (cf.do_rename) {
-      const double z7[NAER] = {0, 0, 0, 0, 0, 0, 0};
-      rename_subarea<true>(C, si, sc, z7, z7);
-    }
-    o_soag = dmax(0.0, 0.0 + tp.g_soag * 1.0);
-    o_h2so4 = dmax(0.0, 0.0 + tp.g_h2so4 * 1.0);
-#pragma unroll
-    for (int m = 0; m < NMODE; ++m) {
-      oi[K::numslot(m)] = dmax(0.0, 0.0 + (si.num[m] / 1.0) * 1.0);
-      oc[K::numslot(m)] = 0.0 + (sc.num[m] / 1.0) * 1.0;
-#pragma unroll
-      for (int xx = 0; xx < NAER; ++xx) {
-        const int sl = K::aer_slot(xx, m);
-        if (sl >= 0) {
-          oi[sl] = dmax(0.0, 0.0 + (si.aer[xx][m] / K::fcvt_aer(xx)) * 1.0);
-          oc[sl] = 0.0 + (sc.aer[xx][m] / K::fcvt_aer(xx)) * 1.0;
-        }
-      }
-    }
-  } else {
-    const bool partly = !(cld < 1.0e-5);
-    tp.cat = partly ? 2 : 0;
-    const double fcldy = cld, fclea = 1.0 - fcldy;
-    double ci[NPOP], cg[2];
-    Sub s;
-    if (!partly) {
-      load_sub_plain(s, tp.qi);
-      s.gas[0] = tp.g_soag * fsoag;
-      s.gas[1] = tp.g_h2so4 * 1.0;
-      tp.rh_sub = tp.relhumgcm;
-#pragma unroll
-      for (int p = 0; p < NPOP; ++p)
-        oc[p] = tp.qc[p];
-    } else {
-#pragma unroll
-      for (int m = 0; m < NMODE; ++m) {
-        part_factors(fcldy, tp.qi[K::numslot(m)], tp.qc[K::numslot(m)], tp.fn_c[m], tp.fn_y[m]);
-        double si_ = 0.0, sc_ = 0.0;
-#pragma unroll
-        for (int k = 0; k < K::nspec(m); ++k) {
-          si_ = si_ + tp.qi[K::spec0(m) + k];
-          sc_ = sc_ + tp.qc[K::spec0(m) + k];
-        }
-        part_factors(fcldy, si_, sc_, tp.fm_c[m], tp.fm_y[m]);
-      }
-      tp.gcl[0] = tp.g_soag;
-      tp.gcl[1] = tp.g_h2so4;
-#pragma unroll
-      for (int g = 0; g < 2; ++g) {
-        tp.gcy[g] = (tp.gcl[g] - fclea * tp.gcl[g]) / fcldy;
-        tp.gcy_clip[g] = tp.gcy[g] < 0;
-        if (tp.gcy_clip[g]) {
-          tp.gcy[g] = 0;
-          tp.gcl[g] = tp.gcl[g] / fclea;
-        }
-      }
-      tp.rhc = bound(0.0, 1.0, (tp.relhumgcm - fcldy) / fclea);
-      Sub si, sc;
-      load_sub(si, tp.qi, tp.fn_y, tp.fm_y);
-#pragma unroll
-      for (int m = 0; m < NMODE; ++m) {
-        sc.num[m] = (tp.qc[K::numslot(m)] / fcldy) * 1;
-#pragma unroll
-        for (int xx = 0; xx < NAER; ++xx) {
-          const int sl = K::aer_slot(xx, m);
-          sc.aer[xx][m] = (sl >= 0) ? (tp.qc[sl] / fcldy) * K::fcvt_aer(xx) : 0.0;
-        }
-      }
-      si.gas[0] = si.gas[1] = sc.gas[0] = sc.gas[1] = 0.0;
-      tp.cy_si = si;
-      tp.cy_sc = sc;
-      if (cf.do_rename) {
-        const double z7[NAER] = {0, 0, 0, 0, 0, 0, 0};
-        rename_subarea<true>(C, si, sc, z7, z7);
-      }
-      cg[0] = tp.gcy[0] * fcldy;
-      cg[1] = tp.gcy[1] * fcldy;
-#pragma unroll
-      for (int m = 0; m < NMODE; ++m) {
-        ci[K::numslot(m)] = (si.num[m] / 1.0) * fcldy;
-        oc[K::numslot(m)] = (0.0 + 0.0 * fclea) + (sc.num[m] / 1.0) * fcldy;
-#pragma unroll
-        for (int xx = 0; xx < NAER; ++xx) {
-          const int sl = K::aer_slot(xx, m);
-          if (sl >= 0) {
-            ci[sl] = (si.aer[xx][m] / K::fcvt_aer(xx)) * fcldy;
-            oc[sl] = (0.0 + 0.0 * fclea) + (sc.aer[xx][m] / K::fcvt_aer(xx)) * fcldy;
-          }
-        }
-      }
-      load_sub(s, tp.qi, tp.fn_c, tp.fm_c);
-      s.gas[0] = tp.gcl[0] * fsoag;
-      s.gas[1] = tp.gcl[1] * 1.0;
-      tp.rh_sub = tp.rhc;
-    }
-    // ---- clear subarea
-    tp.qgas1[0] = tp.g_soag * fsoag;
-    tp.qgas1[1] = tp.g_h2so4 * 1.0;
-    tp.s_entry = s;
-    const double aircon = pmid / (8314.46759100000 * temp);
-    // prefix
-    ClearMid &cm = tp.cm;
-    cm.netprod1 = 0.0;
-    if (cf.do_cond && cf.optaa == 2) {
-      cm.netprod1 = (s.gas[1] - tp.qgas1[1]) / dt;
-      s.gas[1] = (cm.netprod1 >= 0) ? tp.qgas1[1] : 0;
-    }
-    double uptk0[NMODE] = {0, 0, 0, 0};
-    h2so4_diffusivity(temp, pmid, tp.gd, tp.fp);
-#pragma unroll
-    for (int n = 0; n < NMODE; ++n)
-      tp.rate[n] = uptake_rate_mode(C, n, tp.gd, tp.fp, tp.dgn_awet[n]);
-    if (cf.do_cond) {
-      cm.sv_so4_ait = s.aer[1][1];
-      cm.sv_soa_ait = s.aer[0][1];
-#pragma unroll
-      for (int n = 0; n < NMODE; ++n) {
-        cm.uptk1[n] = tp.rate[n] * (s.num[n] * aircon);
-        uptk0[n] = cm.uptk1[n] * 0.81;
-      }
-    } else {
-#pragma unroll
-      for (int n = 0; n < NMODE; ++n)
-        cm.uptk1[n] = 0.0;
-    }
-    tp.s_pre_soa = s;
-    const double dtsub = (double)(int)(dt / 1);
-    if (cf.do_cond) {
-      soa_init(tp.soa0, dtsub, temp, pmid, s, uptk0);
-      SoaState st = tp.soa0;
-      tp.niter = soa_forward_ck(st, ck, cks);
-      s.gas[0] = st.g;
-#pragma unroll
-      for (int n = 0; n < NMODE; ++n)
-        s.aer[0][n] = st.a[n];
-    }
-    tp.s_soa = s;
-    // suffix
-    double qgas_avg1 = s.gas[1];
-    double uptkrate_h2so4 = 0.0;
-#pragma unroll
-    for (int k2 = 0; k2 < NAER; ++k2)
-      tp.grow[k2] = 0.0;
-    if (cf.do_cond) {
-#pragma unroll
-      for (int n = 0; n < NMODE; ++n)
-        uptkrate_h2so4 += cm.uptk1[n];
-      h2so4_update(dtsub, cm.netprod1, s, cm.uptk1, qgas_avg1);
-      tp.grow[1] = s.aer[1][1] - cm.sv_so4_ait;
-      tp.grow[0] = s.aer[0][1] - cm.sv_soa_ait;
-    }
-    tp.qavg = qgas_avg1;
-    tp.s_h2so4 = s;
-    if (cf.do_rename) {
-      const double z7[NAER] = {0, 0, 0, 0, 0, 0, 0};
-      rename_subarea<false>(C, s, s, tp.grow, z7);
-    }
-    tp.s_ren = s;
-    if (cf.do_newnuc)
-      nucleation(C, dtsub, temp, pmid, zm, pblh, tp.rh_sub, uptkrate_h2so4, qgas_avg1, s);
-    tp.s_nuc = s;
-    double coag_in[NAER] = {0, 0, 0, 0, 0, 0, 0};
-    if (cf.do_coag) {
-      coag_all_coefs(C, T, temp, pmid, aircon, tp.dgn_awet, tp.wetdens, tp.cc);
-      coagulation(dtsub, tp.cc, s, coag_in);
-    }
-    tp.s_coag = s;
-    {
-      double dn_c[NMODE] = {0, 0, 0, 0}, dn_g[NMODE] = {0, 0, 0, 0};
-      double dc[NAER][NMODE], dq[NAER][NMODE];
-#pragma unroll
-      for (int a = 0; a < NAER; ++a)
-#pragma unroll
-        for (int m = 0; m < NMODE; ++m) {
-          dc[a][m] = 0.0;
-          dq[a][m] = 0.0;
-        }
-      aging(C, cf.nmono, tp.dgn_a[3], s, dn_c, dn_g, dc, dq, coag_in);
-    }
-    // recombination
-    const double w = partly ? fclea : 1.0 - 0.0;
-    const double gs0 = map_gas ? s.gas[0] / fsoag : (partly ? tp.gcl[0] : tp.g_soag);
-    const double gs1 = map_gas ? s.gas[1] / 1.0 : (partly ? tp.gcl[1] : tp.g_h2so4);
-    o_soag = dmax(0.0, (0.0 + gs0 * w) + (partly ? cg[0] : 0.0));
-    o_h2so4 = dmax(0.0, (0.0 + gs1 * w) + (partly ? cg[1] : 0.0));
-#pragma unroll
-    for (int m = 0; m < NMODE; ++m) {
-      oi[K::numslot(m)] = dmax(0.0, (0.0 + (s.num[m] / 1.0) * w) + (partly ? ci[K::numslot(m)] : 0.0));
-#pragma unroll
-      for (int xx = 0; xx < NAER; ++xx) {
-        const int sl = K::aer_slot(xx, m);
-        if (sl >= 0)
-          oi[sl] = dmax(0.0, (0.0 + (s.aer[xx][m] / K::fcvt_aer(xx)) * w) + (partly ? ci[sl] : 0.0));
-      }
-    }
-  }
-  y[MAM4B_OUT_TEND + 0] = (o_h2so4 * C.to_mmr[0] - x[MAM4B_IN_H2SO4]) / dt;
-  y[MAM4B_OUT_TEND + 1] = (o_soag * C.to_mmr[1] - x[MAM4B_IN_SOAG]) / dt;
-#pragma unroll
-  for (int p = 0; p < NPOP; ++p) {
-    y[MAM4B_OUT_TEND + 2 + p] = (oi[p] * C.to_mmr[2 + p] - ai[p]) / dt;
-    y[MAM4B_OUT_TEND + 27 + p] = (oc[p] * C.to_mmr[2 + p] - ac[p]) / dt;
-  }
-}
-
-
 MAM4B_HD void sub_zero(Sub &b) {
   b.gas[0] = b.gas[1] = 0.0;
 #pragma unroll
@@ -2313,14 +2038,428 @@ MAM4B_HD void load_sub_plain_rev(const Sub &sb, double (&qb)[NPOP]) {
   }
 }
 
-// Reverse sweep of one cell: xb gets (d y / d x)^T yb for the
-// differentiated inputs (T, qv, H2SO4, SOAG, 50 populations); the entries of
-// pressure, height and cloud fraction are set to zero.
-MAM4B_HD void cell_reverse(const StepConsts &C, const CoagTables &T, const AdjCfg &cf,
-                           const double (&x)[MAM4B_NIN], double pblh, double dt,
-                           const CellTape &tp, const double *ck, size_t cks,
-                           const double (&yb)[MAM4B_NOUT], double (&xb)[MAM4B_NIN]) {
-  const double temp = x[MAM4B_IN_T], pmid = x[MAM4B_IN_P], zm = x[MAM4B_IN_ZM];
+
+// ---- front: calcsize, water uptake, subareas, clear-subarea prefix
+// State of the forward sweep up to the SOA loop of the clear subarea (the
+// whole cell for a cloudy one).
+struct FrontTape {
+  int cat;  // 0 clear, 1 cloudy, 2 partly cloudy
+  double dgn_a[NMODE], dgn_awet[NMODE], wetdens_wu[NMODE], wetdens[NMODE], rh_wu;
+  double qi[NPOP], qc[NPOP], g_h2so4, g_soag, relhumgcm;
+  double fn_c[NMODE], fn_y[NMODE], fm_c[NMODE], fm_y[NMODE], gcl[2], gcy[2], rhc;
+  bool gcy_clip[2];
+  Sub cy_si, cy_sc;     // cloudy (sub)area before renaming
+  Sub s_entry;          // clear subarea at entry
+  Sub s_pre_soa;        // clear subarea at the SOA loop
+  double qgas1[2], rh_sub, gd, fp, rate[NMODE];
+  ClearMid cm;
+  SoaState soa0;
+  double ci[NPOP], cg[2], oc[NPOP];  // cloudy-subarea contributions, cloud-borne means
+};
+
+// Forward sweep to the SOA loop (cell_step<false> arithmetic). Writes the
+// 16 size outputs into y, and for a cloudy cell all 68.
+MAM4B_HD void front_forward(const StepConsts &C, const AdjCfg &cf, const double (&x)[MAM4B_NIN],
+                            double dt, FrontTape &ft, double (&y)[MAM4B_NOUT]) {
+  const double temp = x[MAM4B_IN_T], pmid = x[MAM4B_IN_P];
+  const double qv = x[MAM4B_IN_QV], cld = x[MAM4B_IN_CLD];
+  double ai[NPOP], ac[NPOP];
+#pragma unroll
+  for (int p = 0; p < NPOP; ++p) {
+    ai[p] = x[MAM4B_IN_AER_I + p];
+    ac[p] = x[MAM4B_IN_AER_C + p];
+  }
+  double pt_i[NPOP], pt_c[NPOP], qaerwat[NMODE];
+  calcsize(C, ai, ac, dt, ft.dgn_a, pt_i, pt_c);
+  water_uptake(C, ai, qv, temp, pmid, cld, ft.dgn_a, ft.dgn_awet, qaerwat, ft.wetdens_wu);
+  ft.rh_wu = water_uptake_rh(qv, temp, pmid, cld);
+#pragma unroll
+  for (int m = 0; m < NMODE; ++m) {
+    y[MAM4B_OUT_DGN_A + m] = ft.dgn_a[m];
+    y[MAM4B_OUT_DGN_AWET + m] = ft.dgn_awet[m];
+    y[MAM4B_OUT_WETDENS + m] = ft.wetdens_wu[m];
+    y[MAM4B_OUT_QAERWAT + m] = qaerwat[m];
+    ft.wetdens[m] = dmax(1000.0, ft.wetdens_wu[m]);
+  }
+#pragma unroll
+  for (int p = 0; p < NPOP; ++p) {
+    ft.qi[p] = dmax(0.0, dmax(0.0, ai[p] + pt_i[p] * dt) * C.to_vmr[2 + p]);
+    ft.qc[p] = dmax(0.0, dmax(0.0, ac[p] + pt_c[p] * dt) * C.to_vmr[2 + p]);
+  }
+  ft.g_h2so4 = dmax(0.0, x[MAM4B_IN_H2SO4] * C.to_vmr[0]);
+  ft.g_soag = dmax(0.0, x[MAM4B_IN_SOAG] * C.to_vmr[1]);
+  {
+    const double epsqs = 0.018016 / 0.028966;
+    const double tc = temp - 273.15;
+    const double ew = 610.94 * ::exp(17.625 * tc / (234.04 + tc));
+    const double ev_sat = 1.00071 * ::exp(4.5e-8 * pmid) * ew;
+    const double qv_sat = epsqs * ev_sat / (pmid - (1 - epsqs) * ev_sat);
+    ft.relhumgcm = dmax(0.0, dmin(1.0, qv / qv_sat));
+  }
+  const double fsoag = C.fcvt_soag;
+  if (cld > 0.999) {
+    ft.cat = 1;
+    Sub si, sc;
+    load_sub_plain(si, ft.qi);
+    load_sub_plain(sc, ft.qc);
+    si.gas[0] = si.gas[1] = sc.gas[0] = sc.gas[1] = 0.0;
+    ft.cy_si = si;
+    ft.cy_sc = sc;
+    if (cf.do_rename) {
+      const double z7[NAER] = {0, 0, 0, 0, 0, 0, 0};
+      rename_subarea<true>(C, si, sc, z7, z7);
+    }
+    const double o_soag = dmax(0.0, 0.0 + ft.g_soag * 1.0);
+    const double o_h2so4 = dmax(0.0, 0.0 + ft.g_h2so4 * 1.0);
+    double oi[NPOP];
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      oi[K::numslot(m)] = dmax(0.0, 0.0 + (si.num[m] / 1.0) * 1.0);
+      ft.oc[K::numslot(m)] = 0.0 + (sc.num[m] / 1.0) * 1.0;
+#pragma unroll
+      for (int xx = 0; xx < NAER; ++xx) {
+        const int sl = K::aer_slot(xx, m);
+        if (sl >= 0) {
+          oi[sl] = dmax(0.0, 0.0 + (si.aer[xx][m] / K::fcvt_aer(xx)) * 1.0);
+          ft.oc[sl] = 0.0 + (sc.aer[xx][m] / K::fcvt_aer(xx)) * 1.0;
+        }
+      }
+    }
+    y[MAM4B_OUT_TEND + 0] = (o_h2so4 * C.to_mmr[0] - x[MAM4B_IN_H2SO4]) / dt;
+    y[MAM4B_OUT_TEND + 1] = (o_soag * C.to_mmr[1] - x[MAM4B_IN_SOAG]) / dt;
+#pragma unroll
+    for (int p = 0; p < NPOP; ++p) {
+      y[MAM4B_OUT_TEND + 2 + p] = (oi[p] * C.to_mmr[2 + p] - ai[p]) / dt;
+      y[MAM4B_OUT_TEND + 27 + p] = (ft.oc[p] * C.to_mmr[2 + p] - ac[p]) / dt;
+    }
+    return;
+  }
+  const bool partly = !(cld < 1.0e-5);
+  ft.cat = partly ? 2 : 0;
+  const double fcldy = cld, fclea = 1.0 - fcldy;
+  Sub s;
+  if (!partly) {
+    load_sub_plain(s, ft.qi);
+    s.gas[0] = ft.g_soag * fsoag;
+    s.gas[1] = ft.g_h2so4 * 1.0;
+    ft.rh_sub = ft.relhumgcm;
+#pragma unroll
+    for (int p = 0; p < NPOP; ++p) {
+      ft.oc[p] = ft.qc[p];
+      ft.ci[p] = 0.0;
+    }
+    ft.cg[0] = ft.cg[1] = 0.0;
+  } else {
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      part_factors(fcldy, ft.qi[K::numslot(m)], ft.qc[K::numslot(m)], ft.fn_c[m], ft.fn_y[m]);
+      double si_ = 0.0, sc_ = 0.0;
+#pragma unroll
+      for (int k = 0; k < K::nspec(m); ++k) {
+        si_ = si_ + ft.qi[K::spec0(m) + k];
+        sc_ = sc_ + ft.qc[K::spec0(m) + k];
+      }
+      part_factors(fcldy, si_, sc_, ft.fm_c[m], ft.fm_y[m]);
+    }
+    ft.gcl[0] = ft.g_soag;
+    ft.gcl[1] = ft.g_h2so4;
+#pragma unroll
+    for (int g = 0; g < 2; ++g) {
+      ft.gcy[g] = (ft.gcl[g] - fclea * ft.gcl[g]) / fcldy;
+      ft.gcy_clip[g] = ft.gcy[g] < 0;
+      if (ft.gcy_clip[g]) {
+        ft.gcy[g] = 0;
+        ft.gcl[g] = ft.gcl[g] / fclea;
+      }
+    }
+    ft.rhc = bound(0.0, 1.0, (ft.relhumgcm - fcldy) / fclea);
+    Sub si, sc;
+    load_sub(si, ft.qi, ft.fn_y, ft.fm_y);
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      sc.num[m] = (ft.qc[K::numslot(m)] / fcldy) * 1;
+#pragma unroll
+      for (int xx = 0; xx < NAER; ++xx) {
+        const int sl = K::aer_slot(xx, m);
+        sc.aer[xx][m] = (sl >= 0) ? (ft.qc[sl] / fcldy) * K::fcvt_aer(xx) : 0.0;
+      }
+    }
+    si.gas[0] = si.gas[1] = sc.gas[0] = sc.gas[1] = 0.0;
+    ft.cy_si = si;
+    ft.cy_sc = sc;
+    if (cf.do_rename) {
+      const double z7[NAER] = {0, 0, 0, 0, 0, 0, 0};
+      rename_subarea<true>(C, si, sc, z7, z7);
+    }
+    ft.cg[0] = ft.gcy[0] * fcldy;
+    ft.cg[1] = ft.gcy[1] * fcldy;
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      ft.ci[K::numslot(m)] = (si.num[m] / 1.0) * fcldy;
+      ft.oc[K::numslot(m)] = (0.0 + 0.0 * fclea) + (sc.num[m] / 1.0) * fcldy;
+#pragma unroll
+      for (int xx = 0; xx < NAER; ++xx) {
+        const int sl = K::aer_slot(xx, m);
+        if (sl >= 0) {
+          ft.ci[sl] = (si.aer[xx][m] / K::fcvt_aer(xx)) * fcldy;
+          ft.oc[sl] = (0.0 + 0.0 * fclea) + (sc.aer[xx][m] / K::fcvt_aer(xx)) * fcldy;
+        }
+      }
+    }
+    load_sub(s, ft.qi, ft.fn_c, ft.fm_c);
+    s.gas[0] = ft.gcl[0] * fsoag;
+    s.gas[1] = ft.gcl[1] * 1.0;
+    ft.rh_sub = ft.rhc;
+  }
+  ft.qgas1[0] = ft.g_soag * fsoag;
+  ft.qgas1[1] = ft.g_h2so4 * 1.0;
+  ft.s_entry = s;
+  const double aircon = pmid / (8314.46759100000 * temp);
+  ClearMid &cm = ft.cm;
+  cm.netprod1 = 0.0;
+  if (cf.do_cond && cf.optaa == 2) {
+    cm.netprod1 = (s.gas[1] - ft.qgas1[1]) / dt;
+    s.gas[1] = (cm.netprod1 >= 0) ? ft.qgas1[1] : 0;
+  }
+  double uptk0[NMODE] = {0, 0, 0, 0};
+  h2so4_diffusivity(temp, pmid, ft.gd, ft.fp);
+#pragma unroll
+  for (int n = 0; n < NMODE; ++n)
+    ft.rate[n] = uptake_rate_mode(C, n, ft.gd, ft.fp, ft.dgn_awet[n]);
+  cm.sv_so4_ait = s.aer[1][1];
+  cm.sv_soa_ait = s.aer[0][1];
+#pragma unroll
+  for (int n = 0; n < NMODE; ++n) {
+    cm.uptk1[n] = cf.do_cond ? ft.rate[n] * (s.num[n] * aircon) : 0.0;
+    uptk0[n] = cm.uptk1[n] * 0.81;
+  }
+  ft.s_pre_soa = s;
+  soa_init(ft.soa0, (double)(int)(dt / 1), temp, pmid, s, uptk0);
+}
+
+// ---- suffix: H2SO4 update, renaming, nucleation, coagulation, aging and
+// the recombination with the cloudy subarea, from the state after the SOA
+// loop (s_soa) to the 52 tendencies
+struct SuffixIn {
+  Sub s_soa;
+  ClearMid cm;  // netprod1, uptk1, sv_so4_ait, sv_soa_ait
+  double dgn_pc, rh_sub, cc[12];
+  bool partly;
+  double fclea, ci[NPOP], cg[2];
+};
+
+struct SuffixStates {
+  Sub s_h2so4, s_ren, s_nuc, s_coag, s_fin;
+  double qavg, grow[NAER], uptkrate;
+};
+
+MAM4B_HD void suffix_states(const StepConsts &C, const AdjCfg &cf, double temp, double pmid,
+                            double zm, double pblh, double dt, const SuffixIn &in,
+                            SuffixStates &st) {
+  const double dtsub = (double)(int)(dt / 1);
+  Sub s = in.s_soa;
+  double qgas_avg1 = s.gas[1];
+  st.uptkrate = 0.0;
+#pragma unroll
+  for (int k = 0; k < NAER; ++k)
+    st.grow[k] = 0.0;
+  if (cf.do_cond) {
+#pragma unroll
+    for (int n = 0; n < NMODE; ++n)
+      st.uptkrate += in.cm.uptk1[n];
+    h2so4_update(dtsub, in.cm.netprod1, s, in.cm.uptk1, qgas_avg1);
+    st.grow[1] = s.aer[1][1] - in.cm.sv_so4_ait;
+    st.grow[0] = s.aer[0][1] - in.cm.sv_soa_ait;
+  }
+  st.qavg = qgas_avg1;
+  st.s_h2so4 = s;
+  if (cf.do_rename) {
+    const double z7[NAER] = {0, 0, 0, 0, 0, 0, 0};
+    rename_subarea<false>(C, s, s, st.grow, z7);
+  }
+  st.s_ren = s;
+  if (cf.do_newnuc)
+    nucleation(C, dtsub, temp, pmid, zm, pblh, in.rh_sub, st.uptkrate, qgas_avg1, s);
+  st.s_nuc = s;
+  double coag_in[NAER] = {0, 0, 0, 0, 0, 0, 0};
+  if (cf.do_coag)
+    coagulation(dtsub, in.cc, s, coag_in);
+  st.s_coag = s;
+  double dn_c[NMODE] = {0, 0, 0, 0}, dn_g[NMODE] = {0, 0, 0, 0};
+  double dc[NAER][NMODE], dq[NAER][NMODE];
+#pragma unroll
+  for (int a = 0; a < NAER; ++a)
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      dc[a][m] = 0.0;
+      dq[a][m] = 0.0;
+    }
+  aging(C, cf.nmono, in.dgn_pc, s, dn_c, dn_g, dc, dq, coag_in);
+  st.s_fin = s;
+}
+
+// the 52 tendencies of a cell with a clear subarea (condensation on, so the
+// gases always come from the subarea states)
+MAM4B_HD void suffix_outputs(const StepConsts &C, const SuffixIn &in, const SuffixStates &st,
+                             const double (&x)[MAM4B_NIN], const double (&oc)[NPOP], double dt,
+                             double (&y)[MAM4B_NOUT]) {
+  const double fsoag = C.fcvt_soag;
+  const Sub &s = st.s_fin;
+  const double w = in.partly ? in.fclea : 1.0 - 0.0;
+  const double o_soag = dmax(0.0, (0.0 + (s.gas[0] / fsoag) * w) + (in.partly ? in.cg[0] : 0.0));
+  const double o_h2so4 = dmax(0.0, (0.0 + (s.gas[1] / 1.0) * w) + (in.partly ? in.cg[1] : 0.0));
+  y[MAM4B_OUT_TEND + 0] = (o_h2so4 * C.to_mmr[0] - x[MAM4B_IN_H2SO4]) / dt;
+  y[MAM4B_OUT_TEND + 1] = (o_soag * C.to_mmr[1] - x[MAM4B_IN_SOAG]) / dt;
+#pragma unroll
+  for (int m = 0; m < NMODE; ++m) {
+    const int ns = K::numslot(m);
+    const double oin = dmax(0.0, (0.0 + (s.num[m] / 1.0) * w) + (in.partly ? in.ci[ns] : 0.0));
+    y[MAM4B_OUT_TEND + 2 + ns] = (oin * C.to_mmr[2 + ns] - x[MAM4B_IN_AER_I + ns]) / dt;
+#pragma unroll
+    for (int xx = 0; xx < NAER; ++xx) {
+      const int sl = K::aer_slot(xx, m);
+      if (sl >= 0) {
+        const double o = dmax(0.0, (0.0 + (s.aer[xx][m] / K::fcvt_aer(xx)) * w) +
+                                       (in.partly ? in.ci[sl] : 0.0));
+        y[MAM4B_OUT_TEND + 2 + sl] = (o * C.to_mmr[2 + sl] - x[MAM4B_IN_AER_I + sl]) / dt;
+      }
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < NPOP; ++p)
+    y[MAM4B_OUT_TEND + 27 + p] = (oc[p] * C.to_mmr[2 + p] - x[MAM4B_IN_AER_C + p]) / dt;
+}
+
+struct SuffixBar {
+  Sub sb;  // cotangent of the subarea state after the SOA loop
+  double netprodb, uptk1b[NMODE], sv_so4b, sv_soab, dgn_pcb, rh_subb, tb;
+  double ccb[12], cib[NPOP], cgb[2];
+};
+
+// Reverse of recombination and suffix; yb: cotangents of the 52
+// tendencies (the interstitial and gas rows are used here).
+MAM4B_HD void suffix_rev(const StepConsts &C, const AdjCfg &cf, double temp, double pmid, double zm,
+                         double pblh, double dt, const SuffixIn &in, const SuffixStates &st,
+                         const double (&ybt)[MAM4B_NUM_PROG], SuffixBar &out) {
+  const double fsoag = C.fcvt_soag;
+  const double dtsub = (double)(int)(dt / 1);
+  const double z7[NAER] = {0, 0, 0, 0, 0, 0, 0};
+  Sub &sb = out.sb;
+  sub_zero(sb);
+  out.netprodb = out.sv_so4b = out.sv_soab = out.dgn_pcb = out.rh_subb = out.tb = 0.0;
+#pragma unroll
+  for (int n = 0; n < NMODE; ++n)
+    out.uptk1b[n] = 0.0;
+#pragma unroll
+  for (int k = 0; k < 12; ++k)
+    out.ccb[k] = 0.0;
+#pragma unroll
+  for (int p = 0; p < NPOP; ++p)
+    out.cib[p] = 0.0;
+  out.cgb[0] = out.cgb[1] = 0.0;
+  // recombination
+  const Sub &s = st.s_fin;
+  const double w = in.partly ? in.fclea : 1.0 - 0.0;
+  {
+    const double o_soagb = ybt[1] * C.to_mmr[1] / dt;
+    const double o_h2so4b = ybt[0] * C.to_mmr[0] / dt;
+    const double b0 = maxc_rev(0.0, (0.0 + (s.gas[0] / fsoag) * w) + (in.partly ? in.cg[0] : 0.0), o_soagb);
+    const double b1 = maxc_rev(0.0, (0.0 + (s.gas[1] / 1.0) * w) + (in.partly ? in.cg[1] : 0.0), o_h2so4b);
+    if (in.partly) {
+      out.cgb[0] += b0;
+      out.cgb[1] += b1;
+    }
+    sb.gas[0] += b0 * w / fsoag;
+    sb.gas[1] += b1 * w;
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      const int ns = K::numslot(m);
+      const double oib = ybt[2 + ns] * C.to_mmr[2 + ns] / dt;
+      const double bn = maxc_rev(0.0, (0.0 + (s.num[m] / 1.0) * w) + (in.partly ? in.ci[ns] : 0.0), oib);
+      sb.num[m] += bn * w;
+      if (in.partly)
+        out.cib[ns] += bn;
+#pragma unroll
+      for (int xx = 0; xx < NAER; ++xx) {
+        const int sl = K::aer_slot(xx, m);
+        if (sl >= 0) {
+          const double ob = ybt[2 + sl] * C.to_mmr[2 + sl] / dt;
+          const double ba = maxc_rev(0.0, (0.0 + (s.aer[xx][m] / K::fcvt_aer(xx)) * w) +
+                                              (in.partly ? in.ci[sl] : 0.0), ob);
+          sb.aer[xx][m] += ba * w / K::fcvt_aer(xx);
+          if (in.partly)
+            out.cib[sl] += ba;
+        }
+      }
+    }
+  }
+  aging_rev(C, cf.nmono, in.dgn_pc, st.s_coag, sb, out.dgn_pcb);
+  if (cf.do_coag) {
+    const double cinb[NAER] = {0, 0, 0, 0, 0, 0, 0};
+    coagulation_rev(dtsub, in.cc, st.s_nuc, sb, out.ccb, cinb);
+  }
+  double uptkrateb = 0.0, qavgb = 0.0;
+  if (cf.do_newnuc)
+    nucleation_rev(C, dtsub, temp, pmid, zm, pblh, in.rh_sub, st.uptkrate, st.qavg,
+                   st.s_ren.gas[1], st.s_ren.num[1], st.s_ren.aer[1][1], sb.gas[1], sb.num[1],
+                   sb.aer[1][1], out.tb, out.rh_subb, uptkrateb, qavgb);
+  double growb[NAER] = {0, 0, 0, 0, 0, 0, 0};
+  if (cf.do_rename) {
+    Sub dummy;
+    sub_zero(dummy);
+    double gcb2[NAER] = {0, 0, 0, 0, 0, 0, 0};
+    rename_subarea_rev<false>(C, st.s_h2so4, st.s_h2so4, st.grow, z7, sb, dummy, growb, gcb2);
+  }
+  if (cf.do_cond) {
+    sb.aer[1][1] += growb[1];
+    out.sv_so4b -= growb[1];
+    sb.aer[0][1] += growb[0];
+    out.sv_soab -= growb[0];
+#pragma unroll
+    for (int n = 0; n < NMODE; ++n)
+      out.uptk1b[n] += uptkrateb;
+    double a1b[NMODE];
+#pragma unroll
+    for (int n = 0; n < NMODE; ++n)
+      a1b[n] = sb.aer[1][n];
+    double q1b = 0.0;
+    h2so4_update_rev(dtsub, in.cm.netprod1, in.s_soa.gas[1], in.cm.uptk1, sb.gas[1], qavgb, a1b,
+                     q1b, out.netprodb, out.uptk1b);
+    sb.gas[1] = q1b;
+#pragma unroll
+    for (int n = 0; n < NMODE; ++n)
+      sb.aer[1][n] = a1b[n];
+  } else {
+    sb.gas[1] += qavgb;
+  }
+}
+
+// coagulation coefficients reverse: ccb to T, the wet diameters and the
+// wet densities (dmax(1000, .) applied)
+MAM4B_HD void coef_rev(const StepConsts &C, const CoagTables &T, double temp, double pmid,
+                       const double (&dgn_awet)[NMODE], const double (&wetdens)[NMODE],
+                       const double (&ccb)[12], double &tb, double (&dgn_awetb)[NMODE],
+                       double (&wetdensb)[NMODE]) {
+#pragma unroll
+  for (int p = 0; p < 3; ++p) {
+    const int sm = coag_src(p), dm = coag_dst(p);
+    const double cb4[4] = {ccb[p], ccb[3 + p], ccb[6 + p], ccb[9 + p]};
+    coag_pair_coefs_rev(C, T, p, temp, pmid, dgn_awet[sm], dgn_awet[dm], wetdens[sm], wetdens[dm],
+                        cb4, tb, dgn_awetb[sm], dgn_awetb[dm], wetdensb[sm], wetdensb[dm]);
+  }
+}
+
+// ---- reverse of the front: the clear-subarea prefix (from the suffix's
+// cotangents and the SOA loop's initial-state cotangents lb), the subarea
+// set-up, the cloudy (sub)area, water uptake and calcsize, into xb.
+// Extra cotangents of the front values: dgn_awetb, wetdensb (coagulation
+// coefficients), tb_extra (T).
+MAM4B_HD void front_rev(const StepConsts &C, const AdjCfg &cf, const double (&x)[MAM4B_NIN],
+                        double dt, const FrontTape &ft, const SuffixBar *sbar, const SoaBar *lb,
+                        const double (&yb)[MAM4B_NOUT], const double (&dgn_awetb_in)[NMODE],
+                        const double (&wetdensb_in)[NMODE], double tb_extra,
+                        double (&xb)[MAM4B_NIN]) {
+  const double temp = x[MAM4B_IN_T], pmid = x[MAM4B_IN_P];
   const double qv = x[MAM4B_IN_QV], cld = x[MAM4B_IN_CLD];
   double ai[NPOP], ac[NPOP];
 #pragma unroll
@@ -2331,36 +2470,31 @@ MAM4B_HD void cell_reverse(const StepConsts &C, const CoagTables &T, const AdjCf
 #pragma unroll
   for (int f = 0; f < MAM4B_NIN; ++f)
     xb[f] = 0.0;
-  double aib[NPOP], acb[NPOP], qib[NPOP], qcb[NPOP], oib[NPOP], ocb[NPOP];
+  double aib[NPOP], acb[NPOP], qib[NPOP], qcb[NPOP], ocb[NPOP];
 #pragma unroll
   for (int p = 0; p < NPOP; ++p) {
-    oib[p] = yb[MAM4B_OUT_TEND + 2 + p] * C.to_mmr[2 + p] / dt;
     ocb[p] = yb[MAM4B_OUT_TEND + 27 + p] * C.to_mmr[2 + p] / dt;
     aib[p] = -yb[MAM4B_OUT_TEND + 2 + p] / dt;
     acb[p] = -yb[MAM4B_OUT_TEND + 27 + p] / dt;
     qib[p] = 0.0;
     qcb[p] = 0.0;
   }
-  const double o_h2so4b = yb[MAM4B_OUT_TEND + 0] * C.to_mmr[0] / dt;
-  const double o_soagb = yb[MAM4B_OUT_TEND + 1] * C.to_mmr[1] / dt;
   xb[MAM4B_IN_H2SO4] -= yb[MAM4B_OUT_TEND + 0] / dt;
   xb[MAM4B_IN_SOAG] -= yb[MAM4B_OUT_TEND + 1] / dt;
   double dgn_ab[NMODE], dgn_awetb[NMODE], wetdens_wub[NMODE], qaerwatb[NMODE], wetdensb[NMODE];
 #pragma unroll
   for (int m = 0; m < NMODE; ++m) {
     dgn_ab[m] = yb[MAM4B_OUT_DGN_A + m];
-    dgn_awetb[m] = yb[MAM4B_OUT_DGN_AWET + m];
+    dgn_awetb[m] = yb[MAM4B_OUT_DGN_AWET + m] + dgn_awetb_in[m];
     wetdens_wub[m] = yb[MAM4B_OUT_WETDENS + m];
     qaerwatb[m] = yb[MAM4B_OUT_QAERWAT + m];
-    wetdensb[m] = 0.0;
+    wetdensb[m] = wetdensb_in[m];
   }
-  double g_h2so4b = 0.0, g_soagb = 0.0, relhumb = 0.0, tb = 0.0, qvb = 0.0;
+  double g_h2so4b = 0.0, g_soagb = 0.0, relhumb = 0.0, tb = tb_extra, qvb = 0.0;
   const double fsoag = C.fcvt_soag;
-  const bool map_gas = cf.do_cond || cf.do_newnuc;
   const double z7[NAER] = {0, 0, 0, 0, 0, 0, 0};
-  if (tp.cat == 1) {
-    // cloudy cell: renaming only
-    Sub si = tp.cy_si, sc = tp.cy_sc;
+  if (ft.cat == 1) {
+    Sub si = ft.cy_si, sc = ft.cy_sc;
     if (cf.do_rename)
       rename_subarea<true>(C, si, sc, z7, z7);
     Sub sib, scb;
@@ -2368,262 +2502,114 @@ MAM4B_HD void cell_reverse(const StepConsts &C, const CoagTables &T, const AdjCf
     sub_zero(scb);
 #pragma unroll
     for (int m = 0; m < NMODE; ++m) {
-      sib.num[m] += maxc_rev(0.0, 0.0 + si.num[m], oib[K::numslot(m)]);
-      scb.num[m] += ocb[K::numslot(m)];
+      const int ns = K::numslot(m);
+      sib.num[m] += maxc_rev(0.0, 0.0 + si.num[m], yb[MAM4B_OUT_TEND + 2 + ns] * C.to_mmr[2 + ns] / dt);
+      scb.num[m] += ocb[ns];
 #pragma unroll
       for (int xx = 0; xx < NAER; ++xx) {
         const int sl = K::aer_slot(xx, m);
         if (sl >= 0) {
-          sib.aer[xx][m] += maxc_rev(0.0, 0.0 + si.aer[xx][m] / K::fcvt_aer(xx), oib[sl]) / K::fcvt_aer(xx);
+          const double oib = yb[MAM4B_OUT_TEND + 2 + sl] * C.to_mmr[2 + sl] / dt;
+          sib.aer[xx][m] += maxc_rev(0.0, 0.0 + si.aer[xx][m] / K::fcvt_aer(xx), oib) / K::fcvt_aer(xx);
           scb.aer[xx][m] += ocb[sl] / K::fcvt_aer(xx);
         }
       }
     }
-    g_soagb += maxc_rev(0.0, 0.0 + tp.g_soag, o_soagb);
-    g_h2so4b += maxc_rev(0.0, 0.0 + tp.g_h2so4, o_h2so4b);
+    g_soagb += maxc_rev(0.0, 0.0 + ft.g_soag, yb[MAM4B_OUT_TEND + 1] * C.to_mmr[1] / dt);
+    g_h2so4b += maxc_rev(0.0, 0.0 + ft.g_h2so4, yb[MAM4B_OUT_TEND + 0] * C.to_mmr[0] / dt);
     if (cf.do_rename) {
       double gb1[NAER] = {0, 0, 0, 0, 0, 0, 0}, gb2[NAER] = {0, 0, 0, 0, 0, 0, 0};
-      rename_subarea_rev<true>(C, tp.cy_si, tp.cy_sc, z7, z7, sib, scb, gb1, gb2);
+      rename_subarea_rev<true>(C, ft.cy_si, ft.cy_sc, z7, z7, sib, scb, gb1, gb2);
     }
     load_sub_plain_rev(sib, qib);
     load_sub_plain_rev(scb, qcb);
   } else {
-    const bool partly = tp.cat == 2;
+    const bool partly = ft.cat == 2;
     const double fcldy = cld, fclea = 1.0 - fcldy;
-    const double w = partly ? fclea : 1.0 - 0.0;
     const double aircon = pmid / (8314.46759100000 * temp);
-    const double dtsub = (double)(int)(dt / 1);
-    // final clear-subarea state (after aging)
-    Sub s = tp.s_coag;
-    {
-      double dn_c[NMODE] = {0, 0, 0, 0}, dn_g[NMODE] = {0, 0, 0, 0};
-      double dc[NAER][NMODE], dq[NAER][NMODE], ci0[NAER] = {0, 0, 0, 0, 0, 0, 0};
-#pragma unroll
-      for (int a = 0; a < NAER; ++a)
-#pragma unroll
-        for (int m = 0; m < NMODE; ++m) {
-          dc[a][m] = 0.0;
-          dq[a][m] = 0.0;
-        }
-      aging(C, cf.nmono, tp.dgn_a[3], s, dn_c, dn_g, dc, dq, ci0);
-    }
-    // cloudy subarea contributions (partly cloudy)
-    Sub csi, csc;
-    double ci[NPOP], cg[2];
-    if (partly) {
-      csi = tp.cy_si;
-      csc = tp.cy_sc;
-      if (cf.do_rename)
-        rename_subarea<true>(C, csi, csc, z7, z7);
-      cg[0] = tp.gcy[0] * fcldy;
-      cg[1] = tp.gcy[1] * fcldy;
-#pragma unroll
-      for (int m = 0; m < NMODE; ++m) {
-        ci[K::numslot(m)] = (csi.num[m] / 1.0) * fcldy;
-#pragma unroll
-        for (int xx = 0; xx < NAER; ++xx) {
-          const int sl = K::aer_slot(xx, m);
-          if (sl >= 0)
-            ci[sl] = (csi.aer[xx][m] / K::fcvt_aer(xx)) * fcldy;
-        }
-      }
-    } else {
-      cg[0] = cg[1] = 0.0;
-#pragma unroll
-      for (int p = 0; p < NPOP; ++p)
-        ci[p] = 0.0;
-    }
-    // ---- recombination reverse
-    Sub sb;
-    sub_zero(sb);
-    double cib[NPOP], cgb[2] = {0, 0}, gclb[2] = {0, 0};
-#pragma unroll
-    for (int p = 0; p < NPOP; ++p)
-      cib[p] = 0.0;
-    {
-      const double gs0 = map_gas ? s.gas[0] / fsoag : (partly ? tp.gcl[0] : tp.g_soag);
-      const double gs1 = map_gas ? s.gas[1] / 1.0 : (partly ? tp.gcl[1] : tp.g_h2so4);
-      const double b0 = maxc_rev(0.0, (0.0 + gs0 * w) + cg[0], o_soagb);
-      const double b1 = maxc_rev(0.0, (0.0 + gs1 * w) + cg[1], o_h2so4b);
-      cgb[0] += b0;
-      cgb[1] += b1;
-      if (map_gas) {
-        sb.gas[0] += b0 * w / fsoag;
-        sb.gas[1] += b1 * w;
-      } else if (partly) {
-        gclb[0] += b0 * w;
-        gclb[1] += b1 * w;
-      } else {
-        g_soagb += b0 * w;
-        g_h2so4b += b1 * w;
-      }
-#pragma unroll
-      for (int m = 0; m < NMODE; ++m) {
-        const int ns = K::numslot(m);
-        const double bn = maxc_rev(0.0, (0.0 + (s.num[m] / 1.0) * w) + ci[ns], oib[ns]);
-        sb.num[m] += bn * w;
-        cib[ns] += bn;
-#pragma unroll
-        for (int xx = 0; xx < NAER; ++xx) {
-          const int sl = K::aer_slot(xx, m);
-          if (sl >= 0) {
-            const double ba = maxc_rev(0.0, (0.0 + (s.aer[xx][m] / K::fcvt_aer(xx)) * w) + ci[sl], oib[sl]);
-            sb.aer[xx][m] += ba * w / K::fcvt_aer(xx);
-            cib[sl] += ba;
-          }
-        }
-      }
-    }
-    // ---- clear-subarea suffix reverse
-    aging_rev(C, cf.nmono, tp.dgn_a[3], tp.s_coag, sb, dgn_ab[3]);
-    if (cf.do_coag) {
-      double ccb[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-      const double cinb[NAER] = {0, 0, 0, 0, 0, 0, 0};
-      coagulation_rev(dtsub, tp.cc, tp.s_nuc, sb, ccb, cinb);
-#pragma unroll
-      for (int p = 0; p < 3; ++p) {
-        const int sm = coag_src(p), dm = coag_dst(p);
-        const double cb4[4] = {ccb[p], ccb[3 + p], ccb[6 + p], ccb[9 + p]};
-        coag_pair_coefs_rev(C, T, p, temp, pmid, tp.dgn_awet[sm], tp.dgn_awet[dm], tp.wetdens[sm],
-                            tp.wetdens[dm], cb4, tb, dgn_awetb[sm], dgn_awetb[dm], wetdensb[sm],
-                            wetdensb[dm]);
-      }
-    }
-    double uptkrateb = 0.0, qavgb = 0.0, rh_subb = 0.0;
-    double uptkrate = 0.0;
-#pragma unroll
-    for (int n = 0; n < NMODE; ++n)
-      uptkrate += tp.cm.uptk1[n];
-    if (!cf.do_cond)
-      uptkrate = 0.0;
-    if (cf.do_newnuc)
-      nucleation_rev(C, dtsub, temp, pmid, zm, pblh, tp.rh_sub, uptkrate, tp.qavg, tp.s_ren.gas[1],
-                     tp.s_ren.num[1], tp.s_ren.aer[1][1], sb.gas[1], sb.num[1], sb.aer[1][1], tb,
-                     rh_subb, uptkrateb, qavgb);
-    double growb[NAER] = {0, 0, 0, 0, 0, 0, 0};
-    if (cf.do_rename) {
-      Sub dummy;
-      sub_zero(dummy);
-      double gcb2[NAER] = {0, 0, 0, 0, 0, 0, 0};
-      rename_subarea_rev<false>(C, tp.s_h2so4, tp.s_h2so4, tp.grow, z7, sb, dummy, growb, gcb2);
-    }
-    double uptk1b[NMODE] = {0, 0, 0, 0}, netprodb = 0.0, sv_so4b = 0.0, sv_soab = 0.0;
+    Sub sb = sbar->sb;  // state after the SOA loop == before it, except SOA
+    // SOA loop initial state and parameters
     if (cf.do_cond) {
-      // grow[1] = s.aer[1][1] - sv_so4; grow[0] = s.aer[0][1] - sv_soa
-      sb.aer[1][1] += growb[1];
-      sv_so4b -= growb[1];
-      sb.aer[0][1] += growb[0];
-      sv_soab -= growb[0];
-#pragma unroll
-      for (int n = 0; n < NMODE; ++n)
-        uptk1b[n] += uptkrateb;
-      double a1b[NMODE];
-#pragma unroll
-      for (int n = 0; n < NMODE; ++n)
-        a1b[n] = sb.aer[1][n];
-      double q1b = 0.0;
-      h2so4_update_rev(dtsub, tp.cm.netprod1, tp.s_soa.gas[1], tp.cm.uptk1, sb.gas[1], qavgb, a1b,
-                       q1b, netprodb, uptk1b);
-      sb.gas[1] = q1b;
-#pragma unroll
-      for (int n = 0; n < NMODE; ++n)
-        sb.aer[1][n] = a1b[n];
-      // SOA loop
-      SoaBar b;
-      b.g = sb.gas[0];
-      b.tcur = 0.0;
-      b.g0 = 0.0;
-#pragma unroll
-      for (int n = 0; n < NMODE; ++n) {
-        b.a[n] = sb.aer[0][n];
-        b.opoa[n] = 0.0;
-        b.uptk[n] = 0.0;
-      }
-      soa_loop_rev(tp.soa0, tp.niter, ck, cks, b);
-      sb.gas[0] = b.g;
+      sb.gas[0] = lb->g;
       constexpr double opoa_frac[NMODE] = {0.1, 0.1, 0.1, 0.0};
 #pragma unroll
-      for (int n = 0; n < NMODE; ++n) {
-        sb.aer[0][n] = b.a[n];
-        sb.aer[2][n] += maxxc_rev(tp.s_pre_soa.aer[2][n], 0.0, b.opoa[n] * opoa_frac[n]);
-        uptk1b[n] += b.uptk[n] * 0.81;  // uptk0 = uptk1 * 0.81
-      }
-      tb += b.g0 * soa_g0_dT(temp, pmid);
-      // sv = state at the prefix
-      sb.aer[1][1] += sv_so4b;
-      sb.aer[0][1] += sv_soab;
-      // uptk1 = rate * (num * aircon)
-      double aircb = 0.0;
-      double rateb[NMODE];
+      for (int n = 0; n < NMODE; ++n)
+        sb.aer[0][n] = lb->a[n];
+#pragma unroll
+      for (int n = 0; n < NMODE; ++n)
+        sb.aer[2][n] += maxxc_rev(ft.s_pre_soa.aer[2][n], 0.0, lb->opoa[n] * opoa_frac[n]);
+      tb += lb->g0 * soa_g0_dT(temp, pmid);
+    }
+    double uptk1b[NMODE];
+#pragma unroll
+    for (int n = 0; n < NMODE; ++n)
+      uptk1b[n] = sbar->uptk1b[n] + (cf.do_cond ? lb->uptk[n] * 0.81 : 0.0);
+    tb += sbar->tb;
+    dgn_ab[3] += sbar->dgn_pcb;
+    // sv = state at the prefix
+    sb.aer[1][1] += sbar->sv_so4b;
+    sb.aer[0][1] += sbar->sv_soab;
+    if (cf.do_cond) {
+      double aircb = 0.0, rateb[NMODE];
 #pragma unroll
       for (int n = 0; n < NMODE; ++n) {
-        rateb[n] = uptk1b[n] * (tp.s_pre_soa.num[n] * aircon);
-        sb.num[n] += uptk1b[n] * tp.rate[n] * aircon;
-        aircb += uptk1b[n] * tp.rate[n] * tp.s_pre_soa.num[n];
+        rateb[n] = uptk1b[n] * (ft.s_pre_soa.num[n] * aircon);
+        sb.num[n] += uptk1b[n] * ft.rate[n] * aircon;
+        aircb += uptk1b[n] * ft.rate[n] * ft.s_pre_soa.num[n];
       }
       tb -= aircb * aircon / temp;
       double gdb = 0.0, fpb = 0.0;
 #pragma unroll
       for (int n = 0; n < NMODE; ++n)
-        uptake_rate_mode_rev(C, n, tp.gd, tp.fp, tp.dgn_awet[n], rateb[n], gdb, fpb, dgn_awetb[n]);
+        uptake_rate_mode_rev(C, n, ft.gd, ft.fp, ft.dgn_awet[n], rateb[n], gdb, fpb, dgn_awetb[n]);
       h2so4_diffusivity_rev(temp, pmid, gdb, fpb, tb);
-    } else {
-      // qavg = s.gas[1] at the suffix entry
-      sb.gas[1] += qavgb;
     }
     // optaa-2 production split
     double qgas1b[2] = {0, 0};
     if (cf.do_cond && cf.optaa == 2) {
-      const double np = tp.cm.netprod1;
-      double npb = netprodb;
-      if (np >= 0)
+      if (ft.cm.netprod1 >= 0)
         qgas1b[1] += sb.gas[1];
-      // netprod1 = (s.gas[1] - qgas1[1]) / dt, s.gas[1] is then replaced
-      sb.gas[1] = npb / dt;
-      qgas1b[1] -= npb / dt;
+      sb.gas[1] = sbar->netprodb / dt;
+      qgas1b[1] -= sbar->netprodb / dt;
     }
     g_soagb += qgas1b[0] * fsoag;
     g_h2so4b += qgas1b[1];
-    // entry of the clear subarea
     if (!partly) {
       load_sub_plain_rev(sb, qib);
       g_soagb += sb.gas[0] * fsoag;
       g_h2so4b += sb.gas[1];
-      relhumb += rh_subb;
+      relhumb += sbar->rh_subb;
 #pragma unroll
       for (int p = 0; p < NPOP; ++p)
         qcb[p] += ocb[p];
     } else {
       double fn_cb[NMODE] = {0, 0, 0, 0}, fm_cb[NMODE] = {0, 0, 0, 0};
       double fn_yb[NMODE] = {0, 0, 0, 0}, fm_yb[NMODE] = {0, 0, 0, 0};
-      load_sub_rev(sb, tp.qi, tp.fn_c, tp.fm_c, qib, fn_cb, fm_cb);
-      gclb[0] += sb.gas[0] * fsoag;
-      gclb[1] += sb.gas[1];
-      // rhc = bound(0, 1, (relhumgcm - fcldy) / fclea)
-      relhumb += boundc_rev(0.0, 1.0, (tp.relhumgcm - fcldy) / fclea, rh_subb) / fclea;
-      // cloudy subarea
+      load_sub_rev(sb, ft.qi, ft.fn_c, ft.fm_c, qib, fn_cb, fm_cb);
+      double gclb[2] = {sb.gas[0] * fsoag, sb.gas[1]};
+      relhumb += boundc_rev(0.0, 1.0, (ft.relhumgcm - fcldy) / fclea, sbar->rh_subb) / fclea;
       Sub sib, scb;
       sub_zero(sib);
       sub_zero(scb);
 #pragma unroll
       for (int m = 0; m < NMODE; ++m) {
-        sib.num[m] += cib[K::numslot(m)] * fcldy;
+        sib.num[m] += sbar->cib[K::numslot(m)] * fcldy;
         scb.num[m] += ocb[K::numslot(m)] * fcldy;
 #pragma unroll
         for (int xx = 0; xx < NAER; ++xx) {
           const int sl = K::aer_slot(xx, m);
           if (sl >= 0) {
-            sib.aer[xx][m] += cib[sl] * fcldy / K::fcvt_aer(xx);
+            sib.aer[xx][m] += sbar->cib[sl] * fcldy / K::fcvt_aer(xx);
             scb.aer[xx][m] += ocb[sl] * fcldy / K::fcvt_aer(xx);
           }
         }
       }
-      double gcyb[2] = {cgb[0] * fcldy, cgb[1] * fcldy};
+      const double gcyb[2] = {sbar->cgb[0] * fcldy, sbar->cgb[1] * fcldy};
       if (cf.do_rename) {
         double gb1[NAER] = {0, 0, 0, 0, 0, 0, 0}, gb2[NAER] = {0, 0, 0, 0, 0, 0, 0};
-        rename_subarea_rev<true>(C, tp.cy_si, tp.cy_sc, z7, z7, sib, scb, gb1, gb2);
+        rename_subarea_rev<true>(C, ft.cy_si, ft.cy_sc, z7, z7, sib, scb, gb1, gb2);
       }
-      load_sub_rev(sib, tp.qi, tp.fn_y, tp.fm_y, qib, fn_yb, fm_yb);
+      load_sub_rev(sib, ft.qi, ft.fn_y, ft.fm_y, qib, fn_yb, fm_yb);
 #pragma unroll
       for (int m = 0; m < NMODE; ++m) {
         qcb[K::numslot(m)] += scb.num[m] / fcldy;
@@ -2634,29 +2620,21 @@ MAM4B_HD void cell_reverse(const StepConsts &C, const CoagTables &T, const AdjCf
             qcb[sl] += scb.aer[xx][m] * K::fcvt_aer(xx) / fcldy;
         }
       }
-      // gases
-      const double g0[2] = {tp.g_soag, tp.g_h2so4};
       double g0b[2];
 #pragma unroll
-      for (int g = 0; g < 2; ++g) {
-        if (tp.gcy_clip[g])
-          g0b[g] = gclb[g] / fclea;
-        else
-          g0b[g] = gclb[g] + gcyb[g] * (1.0 - fclea) / fcldy;
-      }
-      (void)g0;
+      for (int g = 0; g < 2; ++g)
+        g0b[g] = ft.gcy_clip[g] ? gclb[g] / fclea : gclb[g] + gcyb[g] * (1.0 - fclea) / fcldy;
       g_soagb += g0b[0];
       g_h2so4b += g0b[1];
-      // partition factors
 #pragma unroll
       for (int m = 0; m < NMODE; ++m) {
-        part_factors_rev(fcldy, tp.qi[K::numslot(m)], tp.qc[K::numslot(m)], fn_cb[m], fn_yb[m],
+        part_factors_rev(fcldy, ft.qi[K::numslot(m)], ft.qc[K::numslot(m)], fn_cb[m], fn_yb[m],
                          qib[K::numslot(m)], qcb[K::numslot(m)]);
         double si_ = 0.0, sc_ = 0.0;
 #pragma unroll
         for (int k = 0; k < K::nspec(m); ++k) {
-          si_ = si_ + tp.qi[K::spec0(m) + k];
-          sc_ = sc_ + tp.qc[K::spec0(m) + k];
+          si_ = si_ + ft.qi[K::spec0(m) + k];
+          sc_ = sc_ + ft.qc[K::spec0(m) + k];
         }
         double sib_ = 0.0, scb_ = 0.0;
         part_factors_rev(fcldy, si_, sc_, fm_cb[m], fm_yb[m], sib_, scb_);
@@ -2668,14 +2646,13 @@ MAM4B_HD void cell_reverse(const StepConsts &C, const CoagTables &T, const AdjCf
       }
     }
   }
-  // ---- front reverse
+  // front
   xb[MAM4B_IN_H2SO4] += maxc_rev(0.0, x[MAM4B_IN_H2SO4] * C.to_vmr[0], g_h2so4b) * C.to_vmr[0];
   xb[MAM4B_IN_SOAG] += maxc_rev(0.0, x[MAM4B_IN_SOAG] * C.to_vmr[1], g_soagb) * C.to_vmr[1];
   relhum_gcm_rev(qv, temp, pmid, relhumb, qvb, tb);
 #pragma unroll
   for (int m = 0; m < NMODE; ++m)
-    wetdens_wub[m] += maxc_rev(1000.0, tp.wetdens_wu[m], wetdensb[m]);
-  // q = dmax(0, dmax(0, a + pt dt) * to_vmr)
+    wetdens_wub[m] += maxc_rev(1000.0, ft.wetdens_wu[m], wetdensb[m]);
   double pt_ib[NPOP], pt_cb[NPOP];
   {
     double dgn_tmp[NMODE], pt_i[NPOP], pt_c[NPOP];
@@ -2692,17 +2669,15 @@ MAM4B_HD void cell_reverse(const StepConsts &C, const CoagTables &T, const AdjCf
       pt_cb[p] = ubc * dt;
     }
   }
-  // water uptake per mode, then its humidity
   double rh_wub = 0.0;
   {
-    double spb[7];
-    double sp[7];
+    double spb[7], sp[7];
 #define MAM4B_WU_REV(M)                                                                      \
   {                                                                                          \
     mode_species<M>(ai, sp);                                                                 \
     for (int k = 0; k < 7; ++k)                                                              \
       spb[k] = 0.0;                                                                          \
-    water_uptake_mode_rev<M>(C, sp, tp.rh_wu, tp.dgn_a[M], dgn_awetb[M], qaerwatb[M],        \
+    water_uptake_mode_rev<M>(C, sp, ft.rh_wu, ft.dgn_a[M], dgn_awetb[M], qaerwatb[M],        \
                              wetdens_wub[M], spb, rh_wub, dgn_ab[M]);                        \
     for (int k = 0; k < K::nspec(M); ++k)                                                    \
       aib[K::spec0(M) + k] += spb[k];                                                        \
@@ -2722,6 +2697,90 @@ MAM4B_HD void cell_reverse(const StepConsts &C, const CoagTables &T, const AdjCf
     xb[MAM4B_IN_AER_I + p] += aib[p];
     xb[MAM4B_IN_AER_C + p] += acb[p];
   }
+}
+
+// suffix inputs of a cell from its front tape and the SOA loop result
+MAM4B_HD void suffix_in_from_front(const FrontTape &ft, const SoaState &soa_end, double cld,
+                                   const double (&cc)[12], SuffixIn &in) {
+  in.s_soa = ft.s_pre_soa;
+  in.s_soa.gas[0] = soa_end.g;
+#pragma unroll
+  for (int n = 0; n < NMODE; ++n)
+    in.s_soa.aer[0][n] = soa_end.a[n];
+  in.cm = ft.cm;
+  in.dgn_pc = ft.dgn_a[3];
+  in.rh_sub = ft.rh_sub;
+#pragma unroll
+  for (int k = 0; k < 12; ++k)
+    in.cc[k] = cc[k];
+  in.partly = ft.cat == 2;
+  in.fclea = 1.0 - cld;
+#pragma unroll
+  for (int p = 0; p < NPOP; ++p)
+    in.ci[p] = ft.ci[p];
+  in.cg[0] = ft.cg[0];
+  in.cg[1] = ft.cg[1];
+}
+
+// ---- whole cell in one thread (forward then reverse); the SOA
+// checkpoints go to ck (stride cks). y gets the 68 outputs.
+MAM4B_HD void cell_adjoint(const StepConsts &C, const CoagTables &T, const AdjCfg &cf,
+                           const double (&x)[MAM4B_NIN], double pblh, double dt, double *ck,
+                           size_t cks, const double (&yb)[MAM4B_NOUT], double (&y)[MAM4B_NOUT],
+                           double (&xb)[MAM4B_NIN], int &niter) {
+  FrontTape ft;
+  front_forward(C, cf, x, dt, ft, y);
+  const double zero4[NMODE] = {0, 0, 0, 0};
+  niter = 0;
+  if (ft.cat == 1) {
+    front_rev(C, cf, x, dt, ft, nullptr, nullptr, yb, zero4, zero4, 0.0, xb);
+    return;
+  }
+  const double temp = x[MAM4B_IN_T], pmid = x[MAM4B_IN_P], zm = x[MAM4B_IN_ZM];
+  SoaState se = ft.soa0;
+  if (cf.do_cond)
+    niter = soa_forward_ck(se, ck, cks);
+  double cc[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  if (cf.do_coag) {
+    const double aircon = pmid / (8314.46759100000 * temp);
+    coag_all_coefs(C, T, temp, pmid, aircon, ft.dgn_awet, ft.wetdens, cc);
+  }
+  SuffixIn in;
+  if (cf.do_cond) {
+    suffix_in_from_front(ft, se, x[MAM4B_IN_CLD], cc, in);
+  } else {
+    SoaState none = ft.soa0;
+    none.g = ft.s_pre_soa.gas[0];
+#pragma unroll
+    for (int n = 0; n < NMODE; ++n)
+      none.a[n] = ft.s_pre_soa.aer[0][n];
+    suffix_in_from_front(ft, none, x[MAM4B_IN_CLD], cc, in);
+  }
+  SuffixStates st;
+  suffix_states(C, cf, temp, pmid, zm, pblh, dt, in, st);
+  suffix_outputs(C, in, st, x, ft.oc, dt, y);
+  double ybt[MAM4B_NUM_PROG];
+#pragma unroll
+  for (int k = 0; k < MAM4B_NUM_PROG; ++k)
+    ybt[k] = yb[MAM4B_OUT_TEND + k];
+  SuffixBar sbar;
+  suffix_rev(C, cf, temp, pmid, zm, pblh, dt, in, st, ybt, sbar);
+  double dgn_awetb[NMODE] = {0, 0, 0, 0}, wetdensb[NMODE] = {0, 0, 0, 0}, tb = 0.0;
+  if (cf.do_coag)
+    coef_rev(C, T, temp, pmid, ft.dgn_awet, ft.wetdens, sbar.ccb, tb, dgn_awetb, wetdensb);
+  SoaBar lb;
+  lb.g = sbar.sb.gas[0];
+  lb.tcur = 0.0;
+  lb.g0 = 0.0;
+#pragma unroll
+  for (int n = 0; n < NMODE; ++n) {
+    lb.a[n] = sbar.sb.aer[0][n];
+    lb.opoa[n] = 0.0;
+    lb.uptk[n] = 0.0;
+  }
+  if (cf.do_cond)
+    soa_loop_rev(ft.soa0, niter, ck, cks, lb);
+  front_rev(C, cf, x, dt, ft, &sbar, &lb, yb, dgn_awetb, wetdensb, tb, xb);
 }
 
 }  // namespace adj

@@ -69,7 +69,8 @@ enum { SOA_G = 0, SOA_A = 1, SOA_OPOA = 5, SOA_UPTK = 9, SOA_G0 = 13, SOA_FIELDS
 enum { AUX_RH = 0, AUX_GDIFF = 1, AUX_FPATH = 2, AUX_RATE = 3, AUX_COAG = 7, AUX_FIELDS = 19 };
 // queue counters: queued slots, slots handed to the solver, long and short
 // loops in the order list
-enum { CNT_QUEUED = 0, CNT_TAKEN = 1, CNT_LONG = 2, CNT_SHORT = 3, CNT_WORDS = 4 };
+enum { CNT_QUEUED = 0, CNT_TAKEN = 1, CNT_LONG = 2, CNT_SHORT = 3, CNT_TAKEN_ADJ = 4,
+       CNT_WORDS = 8 };
 // A loop is started early when its first sub-step is shorter than
 // dt / kLongLoopSteps, i.e. when it is expected to take at least about that
 // many sub-steps (the SOA loop's step is 0.05 / sum(uptake * |phi|)).
@@ -101,7 +102,8 @@ enum {
   H_OC = 35,       // 25 outgoing cloud-borne grid means
   H_CI = 60,       // 25 interstitial contributions of the cloudy subarea
   H_CG = 85,       // 2 gas contributions of the cloudy subarea (SOAG, H2SO4)
-  H_FIELDS = 87
+  H_SOAG0 = 87,    // SOA gas at the start of the loop (read by the adjoint)
+  H_FIELDS = 88
 };
 
 // Clear subarea, mam_amicphys_1subarea (mam4_amicphys.hpp:1127-1697), part 1:
@@ -804,6 +806,7 @@ __device__ __forceinline__ void cell_pre(const StepArgs &a, const long long c) {
   h[H_SV_SOA * n] = cm.sv_soa_ait;
   h[H_DGN_PC * n] = f.dgn_a[3];
   h[H_RELHUM * n] = rh;
+  h[H_SOAG0 * n] = s.gas[0];
 #pragma unroll
   for (int p = 0; p < NPOP; ++p)
     h[(H_OC + p) * n] = oc[p];
@@ -1144,13 +1147,283 @@ __global__ void __launch_bounds__(128) adjoint_kernel(const __grid_constant__ Ad
     for (int f = 0; f < MAM4B_NOUT; ++f)
       yb[f] = __ldg(a.ybar + (size_t)f * a.ld + c);
     const double pblh = __ldg(a.pblh + c / a.nlev);
-    adj::CellTape tp;
-    adj::cell_forward(c_k, T, a.cfg, x, pblh, a.dt, tp, ck, nthreads, y);
-    adj::cell_reverse(c_k, T, a.cfg, x, pblh, a.dt, tp, ck, nthreads, yb, xb);
+    int niter;
+    adj::cell_adjoint(c_k, T, a.cfg, x, pblh, a.dt, ck, nthreads, yb, y, xb, niter);
 #pragma unroll
     for (int f = 0; f < MAM4B_NIN; ++f)
       a.xbar[(size_t)f * a.ld + c] = xb[f];
   }
+}
+
+// ---- pipelined adjoint (condensation on): after the forward pipeline,
+// adj_post_kernel reverses each queued cell's suffix (H2SO4 update,
+// renaming, nucleation, coagulation, aging, recombination) from the
+// hand-off, adj_soa_kernel reverses the SOA loops with the same work
+// stealing as the forward solver, and adj_pre_kernel recomputes each cell's
+// front and reverses it. Cotangents pass through cell-indexed scratch.
+enum {
+  AB_SB = 0,        // 29: subarea state after the loop: num[4], aer[1..6][4], gas[1]
+  AB_NETPROD = 29,
+  AB_UPTK1 = 30,    // 4
+  AB_SV_SO4 = 34,
+  AB_SV_SOA = 35,
+  AB_DGN_PC = 36,
+  AB_RH_SUB = 37,
+  AB_T = 38,
+  AB_DGN_AWET = 39,  // 4
+  AB_WETDENS = 43,   // 4
+  AB_CI = 47,        // 25
+  AB_CG = 72,        // 2
+  AB_FIELDS = 74
+};
+enum { LB_G = 0, LB_A = 1, LB_OPOA = 5, LB_UPTK = 9, LB_G0 = 13, LB_FIELDS = 14 };
+
+struct AdjPipeArgs {
+  StepArgs s;           // the forward pipeline's arguments and scratch
+  const double *ybar;   // [MAM4B_NOUT][ld]
+  double *xbar;         // [MAM4B_NIN][ld]
+  size_t ld;
+  double *abar;         // [AB_FIELDS][ncell]
+  double *lbar;         // [LB_FIELDS][ncell]
+  double *ck;           // SOA checkpoints [6 kSoaCkMax][nthreads of adj_soa_kernel]
+  adj::AdjCfg cfg;
+};
+
+// sb slot j (0..28) <-> Sub components other than the SOA ones
+MAM4B_HD double &sb_ref(Sub &b, int j) {
+  if (j < 4)
+    return b.num[j];
+  if (j < 28)
+    return b.aer[1 + (j - 4) / 4][(j - 4) % 4];
+  return b.gas[1];
+}
+
+__global__ void __launch_bounds__(128) adj_post_kernel(const __grid_constant__ AdjPipeArgs p) {
+  const StepArgs &a = p.s;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)a.counters[CNT_QUEUED])
+    return;
+  const StepConsts &C = c_k;
+  const CoagTables T = {kCoagBm0ij, kCoagBm3i, kCoagBm0};
+  const size_t n = (size_t)a.ncell;
+  const long long c = a.task[i];
+  const double temp = __ldg(a.in[MAM4B_IN_T] + c);
+  const double pmid = __ldg(a.in[MAM4B_IN_P] + c);
+  const double zm = __ldg(a.in[MAM4B_IN_ZM] + c);
+  const double cld = __ldg(a.in[MAM4B_IN_CLD] + c);
+  const double pblh = __ldg(a.pblh + c / a.nlev);
+  const double *h = a.hand + i;
+  double *q = a.soa + i;
+  adj::SuffixIn in;
+  {
+    double pop[NPOP];
+#pragma unroll
+    for (int k = 0; k < NPOP; ++k)
+      pop[k] = h[(H_POP + k) * n];
+    pop_to_sub(pop, in.s_soa);
+  }
+  in.s_soa.gas[0] = q[SOA_G * n];
+  in.s_soa.gas[1] = h[H_GAS1 * n];
+#pragma unroll
+  for (int k = 0; k < NMODE; ++k)
+    in.s_soa.aer[0][k] = q[(SOA_A + k) * n];
+  in.cm.netprod1 = h[H_NETPROD * n];
+  in.cm.sv_so4_ait = h[H_SV_SO4 * n];
+  in.cm.sv_soa_ait = h[H_SV_SOA * n];
+#pragma unroll
+  for (int k = 0; k < NMODE; ++k)
+    in.cm.uptk1[k] = h[(H_UPTK + k) * n];
+  in.dgn_pc = h[H_DGN_PC * n];
+  in.rh_sub = h[H_RELHUM * n];
+#pragma unroll
+  for (int k = 0; k < 12; ++k)
+    in.cc[k] = a.aux[(AUX_COAG + k) * n + c];
+  in.partly = !(cld < 1.0e-5);
+  in.fclea = 1.0 - cld;
+#pragma unroll
+  for (int k = 0; k < NPOP; ++k)
+    in.ci[k] = in.partly ? h[(H_CI + k) * n] : 0.0;
+  in.cg[0] = in.partly ? h[H_CG * n] : 0.0;
+  in.cg[1] = in.partly ? h[(H_CG + 1) * n] : 0.0;
+  adj::SuffixStates st;
+  adj::suffix_states(C, p.cfg, temp, pmid, zm, pblh, a.dt, in, st);
+  double ybt[MAM4B_NUM_PROG];
+#pragma unroll
+  for (int k = 0; k < MAM4B_NUM_PROG; ++k)
+    ybt[k] = __ldg(p.ybar + (size_t)(MAM4B_OUT_TEND + k) * p.ld + c);
+  adj::SuffixBar sb;
+  adj::suffix_rev(C, p.cfg, temp, pmid, zm, pblh, a.dt, in, st, ybt, sb);
+  double dgn_awet[NMODE], wetdens[NMODE], dgn_awetb[NMODE] = {0, 0, 0, 0},
+                                           wetdensb[NMODE] = {0, 0, 0, 0};
+#pragma unroll
+  for (int m = 0; m < NMODE; ++m) {
+    dgn_awet[m] = a.out[MAM4B_OUT_DGN_AWET + m][c];
+    wetdens[m] = dmax(1000.0, a.out[MAM4B_OUT_WETDENS + m][c]);
+  }
+  double tb = sb.tb;
+  if (p.cfg.do_coag)
+    adj::coef_rev(C, T, temp, pmid, dgn_awet, wetdens, sb.ccb, tb, dgn_awetb, wetdensb);
+  // loop-end cotangents for the solver's reverse (slot-indexed)
+  q[SOA_G * n] = sb.sb.gas[0];
+#pragma unroll
+  for (int k = 0; k < NMODE; ++k)
+    q[(SOA_A + k) * n] = sb.sb.aer[0][k];
+  double *ab = p.abar + c;
+#pragma unroll
+  for (int j = 0; j < 29; ++j)
+    ab[(AB_SB + j) * n] = sb_ref(sb.sb, j);
+  ab[AB_NETPROD * n] = sb.netprodb;
+#pragma unroll
+  for (int k = 0; k < NMODE; ++k) {
+    ab[(AB_UPTK1 + k) * n] = sb.uptk1b[k];
+    ab[(AB_DGN_AWET + k) * n] = dgn_awetb[k];
+    ab[(AB_WETDENS + k) * n] = wetdensb[k];
+  }
+  ab[AB_SV_SO4 * n] = sb.sv_so4b;
+  ab[AB_SV_SOA * n] = sb.sv_soab;
+  ab[AB_DGN_PC * n] = sb.dgn_pcb;
+  ab[AB_RH_SUB * n] = sb.rh_subb;
+  ab[AB_T * n] = tb;
+#pragma unroll
+  for (int k = 0; k < NPOP; ++k)
+    ab[(AB_CI + k) * n] = sb.cib[k];
+  ab[AB_CG * n] = sb.cgb[0];
+  ab[(AB_CG + 1) * n] = sb.cgb[1];
+}
+
+// Reverse of the SOA loops, one loop per lane with work stealing (long
+// loops first, as in the forward solver): forward from the loop's start
+// with checkpoints, then reverse from the loop-end cotangents.
+__global__ void __launch_bounds__(kSoaBlock, 2) adj_soa_kernel(const __grid_constant__ AdjPipeArgs p) {
+  const StepArgs &a = p.s;
+  const unsigned ntask = a.counters[CNT_QUEUED];
+  const unsigned nlong = a.counters[CNT_LONG];
+  const int lane = threadIdx.x & 31;
+  const size_t n = (size_t)a.ncell;
+  const size_t nthreads = (size_t)gridDim.x * blockDim.x;
+  double *ck = p.ck + (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  while (true) {
+    unsigned base = 0;
+    if (lane == 0)
+      base = atomicAdd(&a.counters[CNT_TAKEN_ADJ], 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= ntask)
+      break;
+    const unsigned t = base + lane;
+    if (t < ntask) {
+      const unsigned slot = (unsigned)(t < nlong ? a.order[t] : a.order[a.ncell - 1 - (t - nlong)]);
+      const double *h = a.hand + slot;
+      const double *q = a.soa + slot;
+      SoaState st;
+      st.g = h[H_SOAG0 * n];
+      {
+        double pop[NPOP];
+#pragma unroll
+        for (int k = 0; k < NPOP; ++k)
+          pop[k] = h[(H_POP + k) * n];
+        Sub s0;
+        pop_to_sub(pop, s0);
+#pragma unroll
+        for (int k = 0; k < NMODE; ++k)
+          st.a[k] = s0.aer[0][k];
+      }
+#pragma unroll
+      for (int k = 0; k < NMODE; ++k) {
+        st.opoa[k] = q[(SOA_OPOA + k) * n];
+        st.uptk[k] = q[(SOA_UPTK + k) * n];
+      }
+      st.g0 = q[SOA_G0 * n];
+      st.tcur = 0.0;
+      st.dtfull = (double)(int)(a.dt / 1);
+      st.niter = 0;
+      const SoaState init = st;
+      const int passes = adj::soa_forward_ck(st, ck, nthreads);
+      adj::SoaBar b;
+      b.g = q[SOA_G * n];
+#pragma unroll
+      for (int k = 0; k < NMODE; ++k) {
+        b.a[k] = q[(SOA_A + k) * n];
+        b.opoa[k] = 0.0;
+        b.uptk[k] = 0.0;
+      }
+      b.tcur = 0.0;
+      b.g0 = 0.0;
+      adj::soa_loop_rev(init, passes, ck, nthreads, b);
+      const long long c = a.task[slot];
+      double *lb = p.lbar + c;
+      lb[LB_G * n] = b.g;
+#pragma unroll
+      for (int k = 0; k < NMODE; ++k) {
+        lb[(LB_A + k) * n] = b.a[k];
+        lb[(LB_OPOA + k) * n] = b.opoa[k];
+        lb[(LB_UPTK + k) * n] = b.uptk[k];
+      }
+      lb[LB_G0 * n] = b.g0;
+    }
+  }
+}
+
+// Reverse of each cell's front (and of cloudy cells entirely).
+__global__ void __launch_bounds__(128) adj_pre_kernel(const __grid_constant__ AdjPipeArgs p) {
+  const StepArgs &a = p.s;
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncell)
+    return;
+  const size_t n = (size_t)a.ncell;
+  double x[MAM4B_NIN], yb[MAM4B_NOUT], y[MAM4B_NOUT], xb[MAM4B_NIN];
+#pragma unroll
+  for (int f = 0; f < MAM4B_NIN; ++f)
+    x[f] = __ldg(a.in[f] + c);
+#pragma unroll
+  for (int f = 0; f < MAM4B_NOUT; ++f)
+    yb[f] = __ldg(p.ybar + (size_t)f * p.ld + c);
+  adj::FrontTape ft;
+  adj::front_forward(c_k, p.cfg, x, a.dt, ft, y);
+  const double zero4[NMODE] = {0, 0, 0, 0};
+  if (ft.cat == 1) {
+    adj::front_rev(c_k, p.cfg, x, a.dt, ft, nullptr, nullptr, yb, zero4, zero4, 0.0, xb);
+  } else {
+    const double *ab = p.abar + c;
+    const double *lbp = p.lbar + c;
+    adj::SuffixBar sb;
+    adj::sub_zero(sb.sb);
+#pragma unroll
+    for (int j = 0; j < 29; ++j)
+      sb_ref(sb.sb, j) = ab[(AB_SB + j) * n];
+    sb.netprodb = ab[AB_NETPROD * n];
+    double dgn_awetb[NMODE], wetdensb[NMODE];
+#pragma unroll
+    for (int k = 0; k < NMODE; ++k) {
+      sb.uptk1b[k] = ab[(AB_UPTK1 + k) * n];
+      dgn_awetb[k] = ab[(AB_DGN_AWET + k) * n];
+      wetdensb[k] = ab[(AB_WETDENS + k) * n];
+    }
+    sb.sv_so4b = ab[AB_SV_SO4 * n];
+    sb.sv_soab = ab[AB_SV_SOA * n];
+    sb.dgn_pcb = ab[AB_DGN_PC * n];
+    sb.rh_subb = ab[AB_RH_SUB * n];
+    sb.tb = 0.0;
+#pragma unroll
+    for (int k = 0; k < NPOP; ++k)
+      sb.cib[k] = ab[(AB_CI + k) * n];
+    sb.cgb[0] = ab[AB_CG * n];
+    sb.cgb[1] = ab[(AB_CG + 1) * n];
+    adj::SoaBar lb;
+    lb.g = lbp[LB_G * n];
+#pragma unroll
+    for (int k = 0; k < NMODE; ++k) {
+      lb.a[k] = lbp[(LB_A + k) * n];
+      lb.opoa[k] = lbp[(LB_OPOA + k) * n];
+      lb.uptk[k] = lbp[(LB_UPTK + k) * n];
+    }
+    lb.g0 = lbp[LB_G0 * n];
+    lb.tcur = 0.0;
+    adj::front_rev(c_k, p.cfg, x, a.dt, ft, &sb, &lb, yb, dgn_awetb, wetdensb,
+                   ab[AB_T * n], xb);
+  }
+#pragma unroll
+  for (int f = 0; f < MAM4B_NIN; ++f)
+    p.xbar[(size_t)f * p.ld + c] = xb[f];
 }
 
 // ====================================================== derived constants
@@ -1270,9 +1543,13 @@ struct mam4b_ctx {
   unsigned *d_counters;  // CNT_WORDS per chunk of the host path
   size_t cap_cells;
   int soa_grid;  // persistent solver blocks (SMs x resident blocks)
-  // adjoint: SOA checkpoints of the persistent threads (allocated on first use)
+  // adjoint: SOA checkpoints of the persistent threads (allocated on first
+  // use) and the cotangent scratch of the pipelined adjoint (grown)
   double *d_ck;
   int adj_grid;
+  double *d_ck2, *d_abar, *d_lbar;
+  int adj_soa_grid;
+  size_t cap_adj;
   // host path: copy/compute streams and their events (created on first use)
   cudaStream_t hs[kHostStreams];
   cudaEvent_t ev_start, ev_done[kHostStreams];
@@ -1557,6 +1834,9 @@ mam4b_status mam4b_destroy(mam4b_ctx *ctx) {
   cudaFree(ctx->d_aux);
   cudaFree(ctx->d_counters);
   cudaFree(ctx->d_ck);
+  cudaFree(ctx->d_ck2);
+  cudaFree(ctx->d_abar);
+  cudaFree(ctx->d_lbar);
   if (ctx->host_streams) {
     for (int k = 0; k < kHostStreams; ++k) {
       cudaStreamDestroy(ctx->hs[k]);
@@ -1814,51 +2094,125 @@ mam4b_status mam4b_step_slab_noalloc(const mam4b_config *cfg, const double *in_s
   return e == cudaSuccess ? MAM4B_OK : MAM4B_ERR_CUDA;
 }
 
+// Reverse-mode adjoint (include/mam4b.h). With condensation on: the
+// forward pipeline into the context's output scratch, then the three
+// reverse kernels; otherwise one thread per cell (adjoint_kernel).
 mam4b_status mam4b_adjoint_slab(mam4b_ctx *ctx, const double *in_slab, const double *pblh,
                                 const double *out_bar, double *in_bar, size_t ld, int ncol,
                                 int nlev, double dt, void *stream) {
   if (!ctx || !in_slab || !pblh || !out_bar || !in_bar || ncol < 0 || nlev <= 0 ||
       ld < (size_t)ncol * (size_t)nlev || !(dt > 0.0) || !isfinite(dt))
     return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_adjoint_slab", cudaSuccess);
+  if (!ctx->cfg.do_cond && !ctx->cfg.do_newnuc)
+    return set_err(ctx, MAM4B_ERR_NOT_SUPPORTED,
+                   "mam4b_adjoint_slab: needs condensation or nucleation on", cudaSuccess);
   cudaStream_t s = (cudaStream_t)stream;
   ctx->last_stream = s;
   const long long ncell = (long long)ncol * nlev;
   if (ncell == 0)
     return MAM4B_OK;
+  if (ncell > 0x7fffffffLL)
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_adjoint_slab: too many cells", cudaSuccess);
+  const adj::AdjCfg cfg = {ctx->cfg.do_cond, ctx->cfg.do_rename, ctx->cfg.do_newnuc,
+                           ctx->cfg.do_coag, ctx->cfg.gaexch_h2so4_uptake_optaa,
+                           ctx->cfg.n_so4_monolayers_pcage};
   cudaError_t e = cudaSuccess;
-  if (!ctx->d_ck) {
+  if (!ctx->cfg.do_cond) {
+    if (!ctx->d_ck) {
+      int dev = 0, sms = 0, per_sm = 0;
+      e = cudaGetDevice(&dev);
+      if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_kernel, 128, 0);
+      if (e == cudaSuccess) {
+        ctx->adj_grid = sms * (per_sm > 0 ? per_sm : 1);
+        e = cudaMalloc(&ctx->d_ck, (size_t)6 * adj::kSoaCkMax * ctx->adj_grid * 128 * sizeof(double));
+      }
+      if (e != cudaSuccess) {
+        ctx->d_ck = nullptr;
+        return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_adjoint_slab scratch", e);
+      }
+    }
+    AdjArgs a;
+    a.in = in_slab;
+    a.pblh = pblh;
+    a.ybar = out_bar;
+    a.xbar = in_bar;
+    a.ld = ld;
+    a.ncell = ncell;
+    a.nlev = nlev;
+    a.dt = dt;
+    a.cfg = cfg;
+    a.ck = ctx->d_ck;
+    adjoint_kernel<<<ctx->adj_grid, 128, 0, s>>>(a);
+    e = cudaGetLastError();
+    if (e != cudaSuccess)
+      return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_adjoint_slab launch", e);
+    ctx->launches += 1;
+    return MAM4B_OK;
+  }
+  // pipelined adjoint
+  const size_t n = (size_t)ncell;
+  e = grow(&ctx->d_out, &ctx->cap_out, (size_t)MAM4B_NOUT * n);
+  if (e == cudaSuccess)
+    e = ensure_solver_scratch(ctx, n);
+  if (e == cudaSuccess && ctx->cap_adj < n) {
+    cudaFree(ctx->d_abar);
+    cudaFree(ctx->d_lbar);
+    ctx->d_abar = ctx->d_lbar = nullptr;
+    ctx->cap_adj = 0;
+    e = cudaMalloc(&ctx->d_abar, (size_t)AB_FIELDS * n * sizeof(double));
+    if (e == cudaSuccess)
+      e = cudaMalloc(&ctx->d_lbar, (size_t)LB_FIELDS * n * sizeof(double));
+    if (e == cudaSuccess)
+      ctx->cap_adj = n;
+  }
+  if (e == cudaSuccess && !ctx->d_ck2) {
     int dev = 0, sms = 0, per_sm = 0;
     e = cudaGetDevice(&dev);
     if (e == cudaSuccess)
       e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e == cudaSuccess)
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_kernel, 128, 0);
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adj_soa_kernel, kSoaBlock, 0);
     if (e == cudaSuccess) {
-      ctx->adj_grid = sms * (per_sm > 0 ? per_sm : 1);
-      e = cudaMalloc(&ctx->d_ck, (size_t)6 * adj::kSoaCkMax * ctx->adj_grid * 128 * sizeof(double));
-    }
-    if (e != cudaSuccess) {
-      ctx->d_ck = nullptr;
-      return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_adjoint_slab scratch", e);
+      ctx->adj_soa_grid = sms * (per_sm > 0 ? per_sm : 1);
+      e = cudaMalloc(&ctx->d_ck2,
+                     (size_t)6 * adj::kSoaCkMax * ctx->adj_soa_grid * kSoaBlock * sizeof(double));
+      if (e != cudaSuccess)
+        ctx->d_ck2 = nullptr;
     }
   }
-  AdjArgs a;
-  a.in = in_slab;
-  a.pblh = pblh;
-  a.ybar = out_bar;
-  a.xbar = in_bar;
-  a.ld = ld;
-  a.ncell = ncell;
-  a.nlev = nlev;
-  a.dt = dt;
-  a.cfg = adj::AdjCfg{ctx->cfg.do_cond, ctx->cfg.do_rename, ctx->cfg.do_newnuc, ctx->cfg.do_coag,
-                      ctx->cfg.gaexch_h2so4_uptake_optaa, ctx->cfg.n_so4_monolayers_pcage};
-  a.ck = ctx->d_ck;
-  adjoint_kernel<<<ctx->adj_grid, 128, 0, s>>>(a);
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_adjoint_slab scratch", e);
+  AdjPipeArgs p;
+  memset(&p, 0, sizeof(p));
+  for (int f = 0; f < MAM4B_NIN; ++f)
+    p.s.in[f] = in_slab + (size_t)f * ld;
+  p.s.pblh = pblh;
+  for (int f = 0; f < MAM4B_NOUT; ++f)
+    p.s.out[f] = ctx->d_out + (size_t)f * n;
+  set_step_config(ctx, p.s, ncell, nlev, dt);
+  set_step_scratch(ctx, p.s, 0, 0);
+  p.ybar = out_bar;
+  p.xbar = in_bar;
+  p.ld = ld;
+  p.abar = ctx->d_abar;
+  p.lbar = ctx->d_lbar;
+  p.ck = ctx->d_ck2;
+  p.cfg = cfg;
+  e = launch_pipeline(ctx, p.s, s, MAM4B_FP64);
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_adjoint_slab forward", e);
+  const int block = 128;
+  const unsigned grid = (unsigned)((ncell + block - 1) / block);
+  adj_post_kernel<<<grid, block, 0, s>>>(p);
+  adj_soa_kernel<<<ctx->adj_soa_grid, kSoaBlock, 0, s>>>(p);
+  adj_pre_kernel<<<grid, block, 0, s>>>(p);
   e = cudaGetLastError();
   if (e != cudaSuccess)
     return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_adjoint_slab launch", e);
-  ctx->launches += 1;
+  ctx->launches += 3;
   return MAM4B_OK;
 }
 
