@@ -1971,29 +1971,36 @@ MAM4B_HD int soa_forward_ck(SoaState &st, double *ck, size_t cks) {
   return k;  // passes taken (the reference's niter, minus the failed test)
 }
 
+// one block of the loop's reverse: passes [base, base + kSoaCheck) from the
+// checkpoint at base (tmpl supplies the loop parameters opoa, uptk, g0,
+// dtfull, which the passes do not change)
+MAM4B_HD void soa_block_rev(const SoaState &tmpl, int base, int passes, const double *ck,
+                            size_t cks, SoaBar &b) {
+  SoaState blk[kSoaCheck];
+  const double *e = ck + (size_t)6 * (base / kSoaCheck) * cks;
+  SoaState st = tmpl;
+  st.g = e[0];
+#pragma unroll
+  for (int n = 0; n < NMODE; ++n)
+    st.a[n] = e[(1 + n) * cks];
+  st.tcur = e[5 * cks];
+  st.niter = base;
+  const int cnt = (passes - base < kSoaCheck) ? passes - base : kSoaCheck;
+  for (int i = 0; i < cnt; ++i) {
+    blk[i] = st;
+    soa_step(st);
+  }
+  for (int i = cnt - 1; i >= 0; --i)
+    soa_step_rev(blk[i], b);
+}
+
 // reverse of the loop: b holds the cotangents of the final (g, a, tcur) on
 // entry, of the initial state on return (parameters accumulated)
 MAM4B_HD void soa_loop_rev(const SoaState &init, int passes, const double *ck, size_t cks,
                           SoaBar &b) {
-  SoaState blk[kSoaCheck];
   for (int base = ((passes - 1) / kSoaCheck) * kSoaCheck; base >= 0 && passes > 0;
-       base -= kSoaCheck) {
-    const double *e = ck + (size_t)6 * (base / kSoaCheck) * cks;
-    SoaState st = init;
-    st.g = e[0];
-#pragma unroll
-    for (int n = 0; n < NMODE; ++n)
-      st.a[n] = e[(1 + n) * cks];
-    st.tcur = e[5 * cks];
-    st.niter = base;
-    const int cnt = (passes - base < kSoaCheck) ? passes - base : kSoaCheck;
-    for (int i = 0; i < cnt; ++i) {
-      blk[i] = st;
-      soa_step(st);
-    }
-    for (int i = cnt - 1; i >= 0; --i)
-      soa_step_rev(blk[i], b);
-  }
+       base -= kSoaCheck)
+    soa_block_rev(init, base, passes, ck, cks, b);
 }
 
 MAM4B_HD void sub_zero(Sub &b) {
