@@ -2066,8 +2066,18 @@ struct FrontTape {
 
 // Forward sweep to the SOA loop (cell_step<false> arithmetic). Writes the
 // 16 size outputs into y, and for a cloudy cell all 68.
+// Front values that the forward pipeline has computed already (water
+// uptake of each mode, H2SO4 diffusivity, mean free path and per-particle
+// uptake rates): with KNOWN, front_forward takes them from kn instead of
+// recomputing them.
+struct FrontKnown {
+  double dgn_awet[NMODE], wetdens_wu[NMODE], qaerwat[NMODE], rh_wu, gd, fp, rate[NMODE];
+};
+
+template <bool KNOWN>
 MAM4B_HD void front_forward(const StepConsts &C, const AdjCfg &cf, const double (&x)[MAM4B_NIN],
-                            double dt, FrontTape &ft, double (&y)[MAM4B_NOUT]) {
+                            double dt, FrontTape &ft, double (&y)[MAM4B_NOUT],
+                            const FrontKnown *kn = nullptr) {
   const double temp = x[MAM4B_IN_T], pmid = x[MAM4B_IN_P];
   const double qv = x[MAM4B_IN_QV], cld = x[MAM4B_IN_CLD];
   double ai[NPOP], ac[NPOP];
@@ -2078,8 +2088,18 @@ MAM4B_HD void front_forward(const StepConsts &C, const AdjCfg &cf, const double 
   }
   double pt_i[NPOP], pt_c[NPOP], qaerwat[NMODE];
   calcsize(C, ai, ac, dt, ft.dgn_a, pt_i, pt_c);
-  water_uptake(C, ai, qv, temp, pmid, cld, ft.dgn_a, ft.dgn_awet, qaerwat, ft.wetdens_wu);
-  ft.rh_wu = water_uptake_rh(qv, temp, pmid, cld);
+  if constexpr (KNOWN) {
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      ft.dgn_awet[m] = kn->dgn_awet[m];
+      ft.wetdens_wu[m] = kn->wetdens_wu[m];
+      qaerwat[m] = kn->qaerwat[m];
+    }
+    ft.rh_wu = kn->rh_wu;
+  } else {
+    water_uptake(C, ai, qv, temp, pmid, cld, ft.dgn_a, ft.dgn_awet, qaerwat, ft.wetdens_wu);
+    ft.rh_wu = water_uptake_rh(qv, temp, pmid, cld);
+  }
 #pragma unroll
   for (int m = 0; m < NMODE; ++m) {
     y[MAM4B_OUT_DGN_A + m] = ft.dgn_a[m];
@@ -2229,10 +2249,18 @@ MAM4B_HD void front_forward(const StepConsts &C, const AdjCfg &cf, const double 
     s.gas[1] = (cm.netprod1 >= 0) ? ft.qgas1[1] : 0;
   }
   double uptk0[NMODE] = {0, 0, 0, 0};
-  h2so4_diffusivity(temp, pmid, ft.gd, ft.fp);
+  if constexpr (KNOWN) {
+    ft.gd = kn->gd;
+    ft.fp = kn->fp;
 #pragma unroll
-  for (int n = 0; n < NMODE; ++n)
-    ft.rate[n] = uptake_rate_mode(C, n, ft.gd, ft.fp, ft.dgn_awet[n]);
+    for (int n = 0; n < NMODE; ++n)
+      ft.rate[n] = kn->rate[n];
+  } else {
+    h2so4_diffusivity(temp, pmid, ft.gd, ft.fp);
+#pragma unroll
+    for (int n = 0; n < NMODE; ++n)
+      ft.rate[n] = uptake_rate_mode(C, n, ft.gd, ft.fp, ft.dgn_awet[n]);
+  }
   cm.sv_so4_ait = s.aer[1][1];
   cm.sv_soa_ait = s.aer[0][1];
 #pragma unroll
@@ -2456,16 +2484,29 @@ MAM4B_HD void coef_rev(const StepConsts &C, const CoagTables &T, double temp, do
   }
 }
 
-// ---- reverse of the front: the clear-subarea prefix (from the suffix's
-// cotangents and the SOA loop's initial-state cotangents lb), the subarea
-// set-up, the cloudy (sub)area, water uptake and calcsize, into xb.
+// ---- reverse of the front, in three parts:
+// front_rev_head: the clear-subarea prefix (from the suffix's cotangents
+//   and the SOA loop's initial-state cotangents lb), the subarea set-up,
+//   the cloudy (sub)area and the clipping after calcsize; xb receives the
+//   partial cotangents of the inputs, tl those of the water uptake's
+//   outputs and of calcsize's (diameters, tendencies);
+// front_rev_mode<M>: water uptake of mode M (adds to xb's species rows of
+//   the mode and to tl.dgn_ab[M]; returns the cotangent of the RH);
+// front_rev_tail: RH of water uptake and calcsize, into xb.
 // Extra cotangents of the front values: dgn_awetb, wetdensb (coagulation
 // coefficients), tb_extra (T).
-MAM4B_HD void front_rev(const StepConsts &C, const AdjCfg &cf, const double (&x)[MAM4B_NIN],
-                        double dt, const FrontTape &ft, const SuffixBar *sbar, const SoaBar *lb,
-                        const double (&yb)[MAM4B_NOUT], const double (&dgn_awetb_in)[NMODE],
-                        const double (&wetdensb_in)[NMODE], double tb_extra,
-                        double (&xb)[MAM4B_NIN]) {
+struct FrontTail {
+  double pt_ib[NPOP], pt_cb[NPOP];  // calcsize tendencies
+  double dgn_ab[NMODE];             // dry diameters
+  double dgn_awetb[NMODE], qaerwatb[NMODE], wetdens_wub[NMODE];  // water-uptake outputs
+};
+
+MAM4B_HD void front_rev_head(const StepConsts &C, const AdjCfg &cf, const double (&x)[MAM4B_NIN],
+                             double dt, const FrontTape &ft, const SuffixBar *sbar,
+                             const SoaBar *lb, const double (&yb)[MAM4B_NOUT],
+                             const double (&dgn_awetb_in)[NMODE],
+                             const double (&wetdensb_in)[NMODE], double tb_extra,
+                             double (&xb)[MAM4B_NIN], FrontTail &tl) {
   const double temp = x[MAM4B_IN_T], pmid = x[MAM4B_IN_P];
   const double qv = x[MAM4B_IN_QV], cld = x[MAM4B_IN_CLD];
   double ai[NPOP], ac[NPOP];
@@ -2660,7 +2701,6 @@ MAM4B_HD void front_rev(const StepConsts &C, const AdjCfg &cf, const double (&x)
 #pragma unroll
   for (int m = 0; m < NMODE; ++m)
     wetdens_wub[m] += maxc_rev(1000.0, ft.wetdens_wu[m], wetdensb[m]);
-  double pt_ib[NPOP], pt_cb[NPOP];
   {
     double dgn_tmp[NMODE], pt_i[NPOP], pt_c[NPOP];
     calcsize(C, ai, ac, dt, dgn_tmp, pt_i, pt_c);
@@ -2672,37 +2712,93 @@ MAM4B_HD void front_rev(const StepConsts &C, const AdjCfg &cf, const double (&x)
       const double ubc = maxc_rev(0.0, uc, maxc_rev(0.0, vc, qcb[p]) * C.to_vmr[2 + p]);
       aib[p] += ubi;
       acb[p] += ubc;
-      pt_ib[p] = ubi * dt;
-      pt_cb[p] = ubc * dt;
+      tl.pt_ib[p] = ubi * dt;
+      tl.pt_cb[p] = ubc * dt;
     }
   }
-  double rh_wub = 0.0;
-  {
-    double spb[7], sp[7];
-#define MAM4B_WU_REV(M)                                                                      \
-  {                                                                                          \
-    mode_species<M>(ai, sp);                                                                 \
-    for (int k = 0; k < 7; ++k)                                                              \
-      spb[k] = 0.0;                                                                          \
-    water_uptake_mode_rev<M>(C, sp, ft.rh_wu, ft.dgn_a[M], dgn_awetb[M], qaerwatb[M],        \
-                             wetdens_wub[M], spb, rh_wub, dgn_ab[M]);                        \
-    for (int k = 0; k < K::nspec(M); ++k)                                                    \
-      aib[K::spec0(M) + k] += spb[k];                                                        \
+#pragma unroll
+  for (int m = 0; m < NMODE; ++m) {
+    tl.dgn_ab[m] = dgn_ab[m];
+    tl.dgn_awetb[m] = dgn_awetb[m];
+    tl.qaerwatb[m] = qaerwatb[m];
+    tl.wetdens_wub[m] = wetdens_wub[m];
   }
-    MAM4B_WU_REV(0)
-    MAM4B_WU_REV(1)
-    MAM4B_WU_REV(2)
-    MAM4B_WU_REV(3)
-#undef MAM4B_WU_REV
-  }
-  water_uptake_rh_rev(qv, temp, pmid, cld, rh_wub, qvb, tb);
-  calcsize_rev(C, ai, ac, dt, dgn_ab, pt_ib, pt_cb, aib, acb);
   xb[MAM4B_IN_T] += tb;
   xb[MAM4B_IN_QV] += qvb;
 #pragma unroll
   for (int p = 0; p < NPOP; ++p) {
     xb[MAM4B_IN_AER_I + p] += aib[p];
     xb[MAM4B_IN_AER_C + p] += acb[p];
+  }
+}
+
+// water uptake of mode M: sp the mode's species (mode_species<M>), rh_wu
+// and dgn_a the forward's values; spb receives the species' cotangents
+template <int M>
+MAM4B_HD double front_rev_mode(const StepConsts &C, const double (&sp)[7], double rh_wu,
+                               double dgn_a, double dgn_awetb, double qaerwatb,
+                               double wetdens_wub, double (&spb)[7], double &dgn_ab) {
+#pragma unroll
+  for (int k = 0; k < 7; ++k)
+    spb[k] = 0.0;
+  double rh_wub = 0.0;
+  water_uptake_mode_rev<M>(C, sp, rh_wu, dgn_a, dgn_awetb, qaerwatb, wetdens_wub, spb, rh_wub,
+                           dgn_ab);
+  return rh_wub;
+}
+
+// rh_wub: the sum of the modes' RH cotangents; aib, acb, tb, qvb hold the
+// partial cotangents of the populations, T and qv (the species complete
+// with the water uptake's) and receive the rest
+MAM4B_HD void front_rev_tail(const StepConsts &C, const double (&ai)[NPOP],
+                             const double (&ac)[NPOP], double qv, double temp, double pmid,
+                             double cld, double dt, const FrontTail &tl, double rh_wub,
+                             double (&aib)[NPOP], double (&acb)[NPOP], double &tb, double &qvb) {
+  water_uptake_rh_rev(qv, temp, pmid, cld, rh_wub, qvb, tb);
+  calcsize_rev(C, ai, ac, dt, tl.dgn_ab, tl.pt_ib, tl.pt_cb, aib, acb);
+}
+
+// the whole reverse of the front in one thread
+MAM4B_HD void front_rev(const StepConsts &C, const AdjCfg &cf, const double (&x)[MAM4B_NIN],
+                        double dt, const FrontTape &ft, const SuffixBar *sbar, const SoaBar *lb,
+                        const double (&yb)[MAM4B_NOUT], const double (&dgn_awetb_in)[NMODE],
+                        const double (&wetdensb_in)[NMODE], double tb_extra,
+                        double (&xb)[MAM4B_NIN]) {
+  FrontTail tl;
+  front_rev_head(C, cf, x, dt, ft, sbar, lb, yb, dgn_awetb_in, wetdensb_in, tb_extra, xb, tl);
+  double ai[NPOP];
+#pragma unroll
+  for (int p = 0; p < NPOP; ++p)
+    ai[p] = x[MAM4B_IN_AER_I + p];
+  double rh_wub = 0.0;
+  double sp[7], spb[7];
+#define MAM4B_WU_REV(M)                                                                     \
+  {                                                                                         \
+    mode_species<M>(ai, sp);                                                                \
+    const double r = front_rev_mode<M>(C, sp, ft.rh_wu, ft.dgn_a[M], tl.dgn_awetb[M],       \
+                                       tl.qaerwatb[M], tl.wetdens_wub[M], spb, tl.dgn_ab[M]); \
+    rh_wub += r;                                                                            \
+    for (int k = 0; k < K::nspec(M); ++k)                                                   \
+      xb[MAM4B_IN_AER_I + K::spec0(M) + k] += spb[k];                                       \
+  }
+  MAM4B_WU_REV(0)
+  MAM4B_WU_REV(1)
+  MAM4B_WU_REV(2)
+  MAM4B_WU_REV(3)
+#undef MAM4B_WU_REV
+  double ac[NPOP], aib[NPOP], acb[NPOP];
+#pragma unroll
+  for (int p = 0; p < NPOP; ++p) {
+    ac[p] = x[MAM4B_IN_AER_C + p];
+    aib[p] = xb[MAM4B_IN_AER_I + p];
+    acb[p] = xb[MAM4B_IN_AER_C + p];
+  }
+  front_rev_tail(C, ai, ac, x[MAM4B_IN_QV], x[MAM4B_IN_T], x[MAM4B_IN_P], x[MAM4B_IN_CLD], dt, tl,
+                 rh_wub, aib, acb, xb[MAM4B_IN_T], xb[MAM4B_IN_QV]);
+#pragma unroll
+  for (int p = 0; p < NPOP; ++p) {
+    xb[MAM4B_IN_AER_I + p] = aib[p];
+    xb[MAM4B_IN_AER_C + p] = acb[p];
   }
 }
 
@@ -2736,7 +2832,7 @@ MAM4B_HD void cell_adjoint(const StepConsts &C, const CoagTables &T, const AdjCf
                            size_t cks, const double (&yb)[MAM4B_NOUT], double (&y)[MAM4B_NOUT],
                            double (&xb)[MAM4B_NIN], int &niter) {
   FrontTape ft;
-  front_forward(C, cf, x, dt, ft, y);
+  front_forward<false>(C, cf, x, dt, ft, y);
   const double zero4[NMODE] = {0, 0, 0, 0};
   niter = 0;
   if (ft.cat == 1) {

@@ -1447,7 +1447,16 @@ __global__ void __launch_bounds__(kSoaBlock, 2) adj_soa_kernel(const __grid_cons
   }
 }
 
-// Reverse of each cell's front (and of cloudy cells entirely).
+// Reverse of each cell's front (and of cloudy cells entirely), up to the
+// water uptake: the front's forward sweep takes water uptake, diffusivity
+// and uptake rates from the forward pipeline (out rows, aux), the
+// reverse leaves the partial input cotangents in xbar and the cotangents
+// of the water uptake's and calcsize's outputs in abar (FT_* fields, over
+// the suffix cotangents it has read).
+enum { FT_PT_IB = 0, FT_PT_CB = 25, FT_DGN_AB = 50, FT_DGN_AWETB = 54, FT_QAERWATB = 58,
+       FT_WETDENS_WUB = 62, FT_RHB = 66, FT_FIELDS = 70 };
+static_assert(FT_FIELDS <= AB_FIELDS, "front hand-off must fit in abar");
+
 __global__ void __launch_bounds__(128) adj_pre_kernel(const __grid_constant__ AdjPipeArgs p) {
   const StepArgs &a = p.s;
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1461,11 +1470,23 @@ __global__ void __launch_bounds__(128) adj_pre_kernel(const __grid_constant__ Ad
 #pragma unroll
   for (int f = 0; f < MAM4B_NOUT; ++f)
     yb[f] = __ldg(p.ybar + (size_t)f * p.ld + c);
+  adj::FrontKnown kn;
+#pragma unroll
+  for (int m = 0; m < NMODE; ++m) {
+    kn.dgn_awet[m] = a.out[MAM4B_OUT_DGN_AWET + m][c];
+    kn.wetdens_wu[m] = a.out[MAM4B_OUT_WETDENS + m][c];
+    kn.qaerwat[m] = a.out[MAM4B_OUT_QAERWAT + m][c];
+    kn.rate[m] = a.aux[(AUX_RATE + m) * n + c];
+  }
+  kn.rh_wu = a.aux[AUX_RH * n + c];
+  kn.gd = a.aux[AUX_GDIFF * n + c];
+  kn.fp = a.aux[AUX_FPATH * n + c];
   adj::FrontTape ft;
-  adj::front_forward(c_k, p.cfg, x, a.dt, ft, y);
+  adj::front_forward<true>(c_k, p.cfg, x, a.dt, ft, y, &kn);
   const double zero4[NMODE] = {0, 0, 0, 0};
+  adj::FrontTail tl;
   if (ft.cat == 1) {
-    adj::front_rev(c_k, p.cfg, x, a.dt, ft, nullptr, nullptr, yb, zero4, zero4, 0.0, xb);
+    adj::front_rev_head(c_k, p.cfg, x, a.dt, ft, nullptr, nullptr, yb, zero4, zero4, 0.0, xb, tl);
   } else {
     const double *ab = p.abar + c;
     const double *lbp = p.lbar + c;
@@ -1502,12 +1523,103 @@ __global__ void __launch_bounds__(128) adj_pre_kernel(const __grid_constant__ Ad
     }
     lb.g0 = lbp[LB_G0 * n];
     lb.tcur = 0.0;
-    adj::front_rev(c_k, p.cfg, x, a.dt, ft, &sb, &lb, yb, dgn_awetb, wetdensb,
-                   ab[AB_T * n], xb);
+    adj::front_rev_head(c_k, p.cfg, x, a.dt, ft, &sb, &lb, yb, dgn_awetb, wetdensb,
+                        ab[AB_T * n], xb, tl);
   }
 #pragma unroll
   for (int f = 0; f < MAM4B_NIN; ++f)
     p.xbar[(size_t)f * p.ld + c] = xb[f];
+  double *ft_out = p.abar + c;
+#pragma unroll
+  for (int k = 0; k < NPOP; ++k) {
+    ft_out[(FT_PT_IB + k) * n] = tl.pt_ib[k];
+    ft_out[(FT_PT_CB + k) * n] = tl.pt_cb[k];
+  }
+#pragma unroll
+  for (int m = 0; m < NMODE; ++m) {
+    ft_out[(FT_DGN_AB + m) * n] = tl.dgn_ab[m];
+    ft_out[(FT_DGN_AWETB + m) * n] = tl.dgn_awetb[m];
+    ft_out[(FT_QAERWATB + m) * n] = tl.qaerwatb[m];
+    ft_out[(FT_WETDENS_WUB + m) * n] = tl.wetdens_wub[m];
+  }
+}
+
+// Reverse of the water uptake, one thread per (cell, mode) as in the
+// forward's mode_kernel: adds the species' cotangents to xbar, updates the
+// mode's dry-diameter cotangent and leaves the RH cotangent in abar.
+template <int M>
+__device__ __forceinline__ void adj_mode_work(const AdjPipeArgs &p, long long c) {
+  const StepArgs &a = p.s;
+  const size_t n = (size_t)a.ncell;
+  double sp[7], spb[7];
+#pragma unroll
+  for (int s = 0; s < 7; ++s)
+    sp[s] = (s < K::nspec(M)) ? __ldg(a.in[MAM4B_IN_AER_I + K::spec0(M) + (s < K::nspec(M) ? s : 0)] + c) : 0.0;
+  double *ft = p.abar + c;
+  double dgn_ab = ft[(FT_DGN_AB + M) * n];
+  const double r = adj::front_rev_mode<M>(
+      c_k, sp, a.aux[AUX_RH * n + c], a.out[MAM4B_OUT_DGN_A + M][c], ft[(FT_DGN_AWETB + M) * n],
+      ft[(FT_QAERWATB + M) * n], ft[(FT_WETDENS_WUB + M) * n], spb, dgn_ab);
+  ft[(FT_DGN_AB + M) * n] = dgn_ab;
+  ft[(FT_RHB + M) * n] = r;
+#pragma unroll
+  for (int s = 0; s < K::nspec(M); ++s)
+    p.xbar[(size_t)(MAM4B_IN_AER_I + K::spec0(M) + s) * p.ld + c] += spb[s];
+}
+
+__global__ void __launch_bounds__(128) adj_mode_kernel(const __grid_constant__ AdjPipeArgs p) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= p.s.ncell)
+    return;
+  switch (blockIdx.y) {
+  case 0: adj_mode_work<0>(p, c); break;
+  case 1: adj_mode_work<1>(p, c); break;
+  case 2: adj_mode_work<2>(p, c); break;
+  default: adj_mode_work<3>(p, c); break;
+  }
+}
+
+// Last part of the reverse, per cell: RH of water uptake and calcsize.
+__global__ void __launch_bounds__(128) adj_fin_kernel(const __grid_constant__ AdjPipeArgs p) {
+  const StepArgs &a = p.s;
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncell)
+    return;
+  const size_t n = (size_t)a.ncell;
+  double ai[NPOP], ac[NPOP], aib[NPOP], acb[NPOP];
+  double *xbc = p.xbar + c;
+#pragma unroll
+  for (int k = 0; k < NPOP; ++k) {
+    ai[k] = __ldg(a.in[MAM4B_IN_AER_I + k] + c);
+    ac[k] = __ldg(a.in[MAM4B_IN_AER_C + k] + c);
+    aib[k] = xbc[(size_t)(MAM4B_IN_AER_I + k) * p.ld];
+    acb[k] = xbc[(size_t)(MAM4B_IN_AER_C + k) * p.ld];
+  }
+  double tb = xbc[(size_t)MAM4B_IN_T * p.ld], qvb = xbc[(size_t)MAM4B_IN_QV * p.ld];
+  const double *ft = p.abar + c;
+  adj::FrontTail tl;
+#pragma unroll
+  for (int k = 0; k < NPOP; ++k) {
+    tl.pt_ib[k] = ft[(FT_PT_IB + k) * n];
+    tl.pt_cb[k] = ft[(FT_PT_CB + k) * n];
+  }
+#pragma unroll
+  for (int m = 0; m < NMODE; ++m)
+    tl.dgn_ab[m] = ft[(FT_DGN_AB + m) * n];
+  double rh_wub = 0.0;
+#pragma unroll
+  for (int m = 0; m < NMODE; ++m)
+    rh_wub += ft[(FT_RHB + m) * n];
+  adj::front_rev_tail(c_k, ai, ac, __ldg(a.in[MAM4B_IN_QV] + c), __ldg(a.in[MAM4B_IN_T] + c),
+                      __ldg(a.in[MAM4B_IN_P] + c), __ldg(a.in[MAM4B_IN_CLD] + c), a.dt, tl, rh_wub,
+                      aib, acb, tb, qvb);
+  xbc[(size_t)MAM4B_IN_T * p.ld] = tb;
+  xbc[(size_t)MAM4B_IN_QV * p.ld] = qvb;
+#pragma unroll
+  for (int k = 0; k < NPOP; ++k) {
+    xbc[(size_t)(MAM4B_IN_AER_I + k) * p.ld] = aib[k];
+    xbc[(size_t)(MAM4B_IN_AER_C + k) * p.ld] = acb[k];
+  }
 }
 
 // ====================================================== derived constants
@@ -2311,10 +2423,12 @@ mam4b_status mam4b_adjoint_slab(mam4b_ctx *ctx, const double *in_slab, const dou
   adj_sort_kernel<<<sort_grid, 256, 0, s>>>(p);
   adj_soa_kernel<<<ctx->adj_soa_grid, kSoaBlock, 0, s>>>(p);
   adj_pre_kernel<<<grid, block, 0, s>>>(p);
+  adj_mode_kernel<<<dim3(grid, NMODE), block, 0, s>>>(p);
+  adj_fin_kernel<<<grid, block, 0, s>>>(p);
   e = cudaGetLastError();
   if (e != cudaSuccess)
     return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_adjoint_slab launch", e);
-  ctx->launches += 6;
+  ctx->launches += 8;
   return MAM4B_OK;
 }
 
