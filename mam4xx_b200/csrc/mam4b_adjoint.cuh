@@ -1360,7 +1360,13 @@ MAM4B_HD void soa_step_rev(const SoaState &st, SoaBar &b) {
   }
   const double q = (tot - ta) / (1.0 + tbs);
   const double gn = dmax(0.0, q);
-  // ---- reverse
+  // ---- reverse (reciprocals taken once: the cotangents need not round as
+  // the forward does)
+  double rden[NMODE];
+#pragma unroll
+  for (int n = 0; n < NMODE; ++n)
+    rden[n] = skip[n] ? 0.0 : 1.0 / den[n];
+  const double r1 = 1.0 / (1.0 + tbs);
   double gnb = b.g, ab_[NMODE], betab[NMODE], denb[NMODE], sat2b[NMODE], satb[NMODE], gsb[NMODE];
   double gb = 0.0, totb = 0.0, tab = 0.0, tbb = 0.0, dtcurb = 0.0, tcurb = 0.0;
 #pragma unroll
@@ -1381,32 +1387,33 @@ MAM4B_HD void soa_step_rev(const SoaState &st, SoaBar &b) {
   for (int n = 0; n < NMODE; ++n) {
     if (skip[n])
       continue;  // a'[n] = 0
-    const double an = (a[n] + beta[n] * gn) / den[n];
-    const double numb = b.a[n] / den[n];
-    denb[n] -= b.a[n] * an / den[n];
+    const double an = (a[n] + beta[n] * gn) * rden[n];
+    const double numb = b.a[n] * rden[n];
+    denb[n] -= numb * an;
     ab_[n] += numb;
     betab[n] += numb * gn;
     gnb += numb * beta[n];
   }
   const double qb = maxc_rev(0.0, q, gnb);
-  totb += qb / (1.0 + tbs);
-  tab -= qb / (1.0 + tbs);
-  tbb -= qb * q / (1.0 + tbs);
+  const double qr = qb * r1;
+  totb += qr;
+  tab -= qr;
+  tbb -= qr * q;
 #pragma unroll
   for (int n = 0; n < NMODE; ++n) {
     if (skip[n])
       continue;
-    ab_[n] += tab / den[n];
-    betab[n] += tbb / den[n];
-    denb[n] -= (tab * a[n] + tbb * beta[n]) / (den[n] * den[n]);
+    ab_[n] += tab * rden[n];
+    betab[n] += tbb * rden[n];
+    denb[n] -= (tab * a[n] + tbb * beta[n]) * (rden[n] * rden[n]);
     betab[n] += denb[n] * sat2[n];
     sat2b[n] += denb[n] * beta[n];
     if (del[n] > 0.0) {
       const double a_tmp = a[n] + beta[n] * del[n];
       const double aoa2 = st.opoa[n] + a_tmp;
-      const double M2 = dmax(aoa2, 1.0e-20);
-      b.g0 += sat2b[n] / M2;
-      const double M2b = -sat2b[n] * sat2[n] / M2;
+      const double rM2 = 1.0 / dmax(aoa2, 1.0e-20);
+      b.g0 += sat2b[n] * rM2;
+      const double M2b = -sat2b[n] * sat2[n] * rM2;
       const double aoa2b = maxxc_rev(aoa2, 1.0e-20, M2b);
       b.opoa[n] += aoa2b;
       ab_[n] += aoa2b;
@@ -1433,9 +1440,10 @@ MAM4B_HD void soa_step_rev(const SoaState &st, SoaBar &b) {
       continue;
     b.uptk[n] += tmpbb * fabs(phi[n]);
     const double phib = tmpbb * st.uptk[n] * (phi[n] < 0.0 ? -1.0 : 1.0);
-    gb += phib / M1[n];
-    gsb[n] -= phib / M1[n];
-    const double M1b = -phib * phi[n] / M1[n];
+    const double rM1 = 1.0 / M1[n];
+    gb += phib * rM1;
+    gsb[n] -= phib * rM1;
+    const double M1b = -phib * phi[n] * rM1;
     // M1 = dmax(g, m2), m2 = dmax(gs, 1e-20)
     const double m2 = dmax(gs[n], 1.0e-20);
     if (g < m2) {
@@ -1447,9 +1455,9 @@ MAM4B_HD void soa_step_rev(const SoaState &st, SoaBar &b) {
     satb[n] += gsb[n] * a[n];
     ab_[n] += gsb[n] * sat[n];
     // sat = g0 / dmax(aoa, 1e-20)
-    const double M = dmax(aoa[n], 1.0e-20);
-    b.g0 += satb[n] / M;
-    const double Mb = -satb[n] * sat[n] / M;
+    const double rM = 1.0 / dmax(aoa[n], 1.0e-20);
+    b.g0 += satb[n] * rM;
+    const double Mb = -satb[n] * sat[n] * rM;
     const double aoab = maxxc_rev(aoa[n], 1.0e-20, Mb);
     b.opoa[n] += aoab;
     ab_[n] += aoab;
