@@ -10,6 +10,9 @@ One step = calcsize + water uptake + amicphys over every cell, dt = 1800 s.
          max-over-ranks time
   e2e    cells/s through the C ABI host entry (mam4b_step_host): pinned host
          slabs copied in, step, results copied out, every step
+  roofline_fp64  algorithmic flops per cell (baseline/flops_per_cell.json,
+         counted on the CPU restatement) x cells / step time, against the
+         FP64 FMA peak measured in the same run (libmam4b_peaks.so)
   roofline  algorithmic HBM bytes (57 input + 68 output doubles per cell plus
          the per-column boundary-layer height) / measured step time (the
          unit is one step, i.e. one pass of the six launches), against the
@@ -58,6 +61,32 @@ def _peaks():
             d = json.load(f)
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def _flops_per_cell(workload):
+    """Algorithmic flops per cell (+ - * /; libm calls apart) of the
+    workload, counted on the CPU restatement by oracle/count_flops.py."""
+    p = os.path.join(ROOT, "baseline", "flops_per_cell.json")
+    if not os.path.exists(p):
+        return None, None
+    with open(p) as f:
+        d = json.load(f)["configs"][workload]
+    return float(d["flops_per_cell"]), float(d["special_per_cell"])
+
+
+def _fp_peaks():
+    """FP64 and FP32 vector FMA peaks (GFLOP/s), measured now on this device
+    by libmam4b_peaks.so (8 independent FMA chains per thread)."""
+    import ctypes
+    lib = ctypes.CDLL(os.path.join(ROOT, "mam4xx_b200", "libmam4b_peaks.so"))
+    lib.mam4b_peak_gflops.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    res = {}
+    for name, fp64 in (("fp64", 1), ("fp32", 0)):
+        g, ms = ctypes.c_double(), ctypes.c_double()
+        if lib.mam4b_peak_gflops(fp64, ctypes.byref(g), ctypes.byref(ms)) != 0:
+            raise RuntimeError("peak measurement failed")
+        res[name] = g.value
+    return res
 
 
 def _traffic_per_launch(ncell):
@@ -430,6 +459,18 @@ def main():
         adjoint = adjoint_leg(native, torch, dev, stream, args, ws)
 
     peak, peak_kind = _peaks()
+    fpeaks = _fp_peaks()
+    flops_cell, special_cell = _flops_per_cell(WORKLOAD)
+    roof64 = None
+    if flops_cell is not None:
+        g = flops_cell * n / (kernel_ms * 1e-3) / 1e9
+        roof64 = {"bound": "fp64", "achieved": g, "peak": fpeaks["fp64"], "unit": "GFLOP/s",
+                  "frac": g / fpeaks["fp64"],
+                  "flops_per_cell": flops_cell, "libm_calls_per_cell": special_cell,
+                  "peak_source": "measured now: FP64 FMA chains (libmam4b_peaks.so)",
+                  "fp32_peak": fpeaks["fp32"],
+                  "flops_source": "baseline/flops_per_cell.json (operation-counting build of "
+                                  "the CPU restatement; + - * / one flop each, libm calls apart)"}
     alg_bytes = n * BYTES_PER_CELL + ncol * 8
     achieved = alg_bytes / (kernel_ms * 1e-3) / 1e9
     traffic = _traffic_per_launch(n)
@@ -447,6 +488,7 @@ def main():
                      "frac": achieved / peak, "traffic": traffic,
                      "peak_source": "%s copy bandwidth" % peak_kind,
                      "kernel_ms": kernel_ms, "algorithmic_bytes_per_launch": alg_bytes},
+        "roofline_fp64": roof64,
         "e2e": e2e,
         "precisions": precisions,
         "adjoint": adjoint,

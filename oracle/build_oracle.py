@@ -6,6 +6,9 @@
   oracle/libmam4oracle_gpu.so the same source compiled for the GPU with nvcc
                              (CUDA libm, no FMA contraction): the libm-matched
                              diagnostic oracle
+  oracle/libmam4oracle_count.so the restatement compiled as C++ with an
+                             operation-counting real type (oracle/opcount.cpp):
+                             the algorithmic flop count of the step
   oracle/_ref/libmam4ref.so  g++, the mam4xx reference headers included
                              read-only from <ref>/src and compiled unchanged
                              against the host shim in oracle/shim; built only
@@ -27,6 +30,7 @@ PORT_SO = os.path.join(HERE, "libmam4oracle.so")
 ULP_SO = os.path.join(HERE, "libmam4oracle_ulp.so")
 REF_SO = os.path.join(HERE, "_ref", "libmam4ref.so")
 GPU_SO = os.path.join(HERE, "libmam4oracle_gpu.so")
+COUNT_SO = os.path.join(HERE, "libmam4oracle_count.so")
 DEFAULT_REF = "/root/reference"
 
 COMMON = ["-O3", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off"]
@@ -60,6 +64,10 @@ def build(ref=None, force=False):
         _run([os.environ.get("NVCC", "nvcc"), "-x", "cu", "-gencode", "arch=compute_100a,code=sm_100a",
               "-O3", "-std=c++17", "--fmad=false", "-Xcompiler", "-fPIC", "-shared",
               os.path.join(HERE, "mam4_oracle_gpu.cu"), "-o", GPU_SO])
+    if force or _stale(COUNT_SO, deps + [os.path.join(HERE, "opcount.cpp")]):
+        # single-threaded: the tally is one global
+        _run(["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-ffp-contract=off",
+              os.path.join(HERE, "opcount.cpp"), "-o", COUNT_SO, "-lm"])
     ref = ref or DEFAULT_REF
     src = os.path.join(ref, "src")
     if os.path.isdir(os.path.join(src, "mam4xx")):

@@ -105,7 +105,11 @@ void mam4orc_set_ulp_noise(unsigned long long seed) { g_noise_seed = seed; }
 #define NOISE_SEED_CELL(c) ((void)0)
 #endif
 
+#ifndef ORACLE_REAL
 typedef double real;
+#else
+typedef ORACLE_REAL real;
+#endif
 
 #define NMODE 4
 #define NAER 7
@@ -2122,24 +2126,27 @@ ORC_FN int step_cell(const calcsize_data *cd, const double *in, size_t ld, size_
                                   wetdens, diag ? dg : NULL);
   if (out) {
 #define OUT(f) out[(size_t)(f) * ldo + c]
-    OUT(MAM4B_OUT_TEND + 0) = (qq[2] * to_mmr(2) - IN(MAM4B_IN_H2SO4)) / dt;
-    OUT(MAM4B_OUT_TEND + 1) = (qq[5] * to_mmr(5) - IN(MAM4B_IN_SOAG)) / dt;
+    /* (double) casts: no-ops here, conversions in the op-counting build */
+    OUT(MAM4B_OUT_TEND + 0) = (double)((qq[2] * to_mmr(2) - IN(MAM4B_IN_H2SO4)) / dt);
+    OUT(MAM4B_OUT_TEND + 1) = (double)((qq[5] * to_mmr(5) - IN(MAM4B_IN_SOAG)) / dt);
     for (int p = 0; p < MAM4B_NUM_POPS; ++p) {
       const int i31 = 6 + p;
-      OUT(MAM4B_OUT_TEND + 2 + p) = (qq[i31] * to_mmr(i31) - IN(MAM4B_IN_AER_I + p)) / dt;
-      OUT(MAM4B_OUT_TEND + 27 + p) = (qqcw31[i31] * to_mmr(i31) - IN(MAM4B_IN_AER_C + p)) / dt;
+      OUT(MAM4B_OUT_TEND + 2 + p) =
+          (double)((qq[i31] * to_mmr(i31) - IN(MAM4B_IN_AER_I + p)) / dt);
+      OUT(MAM4B_OUT_TEND + 27 + p) =
+          (double)((qqcw31[i31] * to_mmr(i31) - IN(MAM4B_IN_AER_C + p)) / dt);
     }
     for (int m = 0; m < NMODE; ++m) {
-      OUT(MAM4B_OUT_DGN_A + m) = dgncur_a[m];
-      OUT(MAM4B_OUT_DGN_AWET + m) = dgncur_awet[m];
-      OUT(MAM4B_OUT_WETDENS + m) = wetdens[m];
-      OUT(MAM4B_OUT_QAERWAT + m) = qaerwat[m];
+      OUT(MAM4B_OUT_DGN_A + m) = (double)dgncur_a[m];
+      OUT(MAM4B_OUT_DGN_AWET + m) = (double)dgncur_awet[m];
+      OUT(MAM4B_OUT_WETDENS + m) = (double)wetdens[m];
+      OUT(MAM4B_OUT_QAERWAT + m) = (double)qaerwat[m];
     }
 #undef OUT
   }
   if (diag)
     for (int k = 0; k < 5 * PCNST; ++k)
-      diag[(size_t)k * ldd + c] = dg[k];
+      diag[(size_t)k * ldd + c] = (double)dg[k];
 #undef IN
   return niter;
 }
@@ -2176,6 +2183,9 @@ void mam4orc_soa_niter(int ncell, const double *in, size_t ld_in, const double *
     niter[c] = step_cell(cdata(), in, ld_in, (size_t)c, pblh_cell[c], NULL, 0, NULL, 0, dt, cfg);
 }
 
+/* stage-level entries: plain-double builds only (the op-counting build of
+ * oracle/opcount.cpp counts the whole step) */
+#ifndef ORACLE_REAL
 void mam4orc_calcsize(int ncell, const double *state_q, const double *qqcw, double dt,
                       double *dgncur_a, double *dgncur_c, double *ptend, double *dqqcwdt) {
   for (int c = 0; c < ncell; ++c) {
@@ -2224,4 +2234,5 @@ void mam4orc_aging(unsigned n_so4_monolayers_pcage, const double *dgn_a, double 
                          (real(*)[NMODE])qaer_cur, (real(*)[NMODE])qaer_del_cond,
                          (real(*)[NMODE])qaer_del_coag, qaer_del_coag_in);
 }
+#endif /* !ORACLE_REAL */
 #endif /* !ORACLE_GPU */

@@ -19,6 +19,7 @@ REF_SO = os.path.join(HERE, "_ref", "libmam4ref.so")
 PORT_SO = os.path.join(HERE, "libmam4oracle.so")
 ULP_SO = os.path.join(HERE, "libmam4oracle_ulp.so")
 GPU_SO = os.path.join(HERE, "libmam4oracle_gpu.so")
+COUNT_SO = os.path.join(HERE, "libmam4oracle_count.so")
 
 NIN, NOUT, NDIAG = 57, 68, 155
 
@@ -278,3 +279,40 @@ def parity(candidate, ref_out, in_slab, pblh_cell, dt, cfg=None, tol=TOL):
         raise AssertionError("parity: %s; worst output %d cell %d (%r vs %r); %s"
                              % (", ".join(problems), f, c, candidate[f, c], ref_out[f, c], summary))
     return summary
+
+
+class CountOracle:
+    """The restatement built with an operation-counting real type
+    (oracle/opcount.cpp): same outputs as PortOracle, plus the tally of
+    + - * /, libm calls, min/max and compares of the cells stepped."""
+
+    FIELDS = ("add", "mul", "div", "special", "minmax", "cmp")
+
+    def __init__(self):
+        if not os.path.exists(COUNT_SO):
+            raise FileNotFoundError(COUNT_SO)
+        self.lib = ctypes.CDLL(COUNT_SO)
+        self.lib.mam4orc_step.argtypes = [_I, _P, _S, _P, _P, _S, _P, _S, _D, _P, _I]
+        self.lib.mam4orc_step.restype = _I
+        self.lib.mam4cnt_tally.argtypes = [_P]
+        self.lib.mam4cnt_tally.restype = None
+        self.tally()
+
+    def tally(self):
+        t = np.zeros(6, dtype=np.uint64)
+        self.lib.mam4cnt_tally(t.ctypes.data)
+        return dict(zip(self.FIELDS, (int(v) for v in t)))
+
+    def step(self, in_slab, pblh_cell, dt, cfg=None):
+        """Steps the cells; returns (outputs, tally of this call)."""
+        cfg = cfg or default_config()
+        x = np.ascontiguousarray(in_slab, dtype=np.float64)
+        pb = np.ascontiguousarray(pblh_cell, dtype=np.float64)
+        n = x.shape[1]
+        out = np.zeros((NOUT, n))
+        self.tally()
+        st = self.lib.mam4orc_step(n, x.ctypes.data, n, pb.ctypes.data, out.ctypes.data, n, None,
+                                   0, dt, ctypes.byref(cfg), 1)
+        if st != 0:
+            raise RuntimeError("oracle step failed: %d" % st)
+        return out, self.tally()

@@ -165,3 +165,25 @@ def test_oracle_conservation_internal_units(port_oracle):
     soa_before = fam(x[5:57], "SOA") + x[6] * MW_DRY_AIR / ADV_MASS[5] * (12.011 / 150)
     soa_after = fam(after, "SOA") + after[1] * MW_DRY_AIR / ADV_MASS[5] * (12.011 / 150)
     np.testing.assert_allclose(soa_after, soa_before, rtol=1e-12)
+
+
+def test_counting_build_matches_and_counts():
+    """The operation-counting build computes the plain build's outputs bit
+    for bit, and the committed flop counts are those of the restatement
+    (a fresh count on a smaller sample lands within the sampling spread)."""
+    import json
+    import os
+    from oracle.pyoracle import CountOracle, PortOracle
+    w = make_workload("c4", ncol=8, seed=17)
+    pb = pblh_per_cell(w)
+    out, t = CountOracle().step(w["in_slab"], pb, w["dt"])
+    np.testing.assert_array_equal(out, PortOracle().step(w["in_slab"], pb, w["dt"]))
+    n = w["in_slab"].shape[1]
+    assert t["div"] > 0 and t["special"] > 100 * n
+    path = os.path.join(os.path.dirname(os.path.dirname(__file__)), "baseline",
+                        "flops_per_cell.json")
+    committed = json.load(open(path))["configs"]
+    from oracle.count_flops import count
+    fresh = count(cells=2304)
+    for name, v in fresh.items():
+        assert abs(v["flops_per_cell"] / committed[name]["flops_per_cell"] - 1) < 0.15, name
