@@ -178,7 +178,8 @@ def adjoint_leg(native, torch, dev, stream, args, ws):
     finite-difference check (relative step 1e-6) of that gradient on 64
     cells reports the agreement in units of relative sensitivity."""
     from mam4xx_b200.workloads import make_workload
-    wa = make_workload("c5", seed=20261203 + 4 + 1000 * int(os.environ.get("RANK", "0")))
+    wa = make_workload("c5", ncol=args.adjoint_ncol,
+                       seed=20261203 + 4 + 1000 * int(os.environ.get("RANK", "0")))
     xa = torch.from_numpy(wa["in_slab"]).to(dev)
     pba = torch.from_numpy(wa["pblh"]).to(dev)
     na = xa.shape[1]
@@ -316,6 +317,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision legs")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint leg")
+    ap.add_argument("--adjoint-ncol", type=int, default=16384,
+                    help="columns of the adjoint leg (16,384 is its configuration; smaller "
+                         "only for profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
