@@ -1713,11 +1713,16 @@ static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 using namespace mam4b;
 
 // Host-buffer path: columns are processed in chunks of about kHostChunkCells
-// cells, round-robin over kHostStreams streams, so that the host->device
-// copy of one chunk, the kernels of another and the device->host copy of a
-// third run at the same time.
-constexpr int kHostStreams = 3;
-constexpr long long kHostChunkCells = 1LL << 19;
+// cells on one stream per stage: all host->device copies back to back on
+// the copy-in stream, each chunk's kernels on one of kComputeStreams
+// streams once its inputs have arrived, each chunk's device->host copy on
+// the copy-out stream once its kernels are done. Both copy engines stay
+// busy from the first chunk to the last (the copies, not the kernels,
+// bound this path); the chunks' kernels overlap, which hides the tail of
+// each chunk's SOA solver (its longest loop).
+constexpr int kComputeStreams = 4;
+constexpr int kHostStreams = 2 + kComputeStreams;  // in, compute..., out
+constexpr long long kHostChunkCells = 1LL << 18;
 constexpr int kMaxChunks = 64;
 
 struct mam4b_ctx {
@@ -1751,6 +1756,7 @@ struct mam4b_ctx {
   // host path: copy/compute streams and their events (created on first use)
   cudaStream_t hs[kHostStreams];
   cudaEvent_t ev_start, ev_done[kHostStreams];
+  cudaEvent_t ev_in[kMaxChunks], ev_comp[kMaxChunks];  // per chunk: inputs in, kernels done
   bool host_streams;
 };
 
@@ -1899,22 +1905,40 @@ cudaError_t launch_pipeline(mam4b_ctx *ctx, const StepArgs &a, cudaStream_t s, i
 cudaError_t ensure_host_streams(mam4b_ctx *ctx) {
   if (ctx->host_streams)
     return cudaSuccess;
-  cudaError_t e = cudaEventCreateWithFlags(&ctx->ev_start, cudaEventDisableTiming);
-  int k = 0;
-  for (; k < kHostStreams && e == cudaSuccess; ++k) {
-    e = cudaStreamCreateWithFlags(&ctx->hs[k], cudaStreamNonBlocking);
-    if (e == cudaSuccess) {
-      e = cudaEventCreateWithFlags(&ctx->ev_done[k], cudaEventDisableTiming);
-      if (e != cudaSuccess)
-        cudaStreamDestroy(ctx->hs[k]);
-    }
+  // created in order; on failure everything created so far is released
+  int ns = 0, ne = 0;
+  cudaEvent_t *evs[1 + kHostStreams + 2 * kMaxChunks];
+  evs[ne] = &ctx->ev_start;
+  cudaError_t e = cudaEventCreateWithFlags(evs[ne], cudaEventDisableTiming);
+  if (e == cudaSuccess)
+    ++ne;
+  for (; ns < kHostStreams && e == cudaSuccess; ++ns) {
+    e = cudaStreamCreateWithFlags(&ctx->hs[ns], cudaStreamNonBlocking);
+    if (e != cudaSuccess)
+      break;
+  }
+  for (int k = 0; k < kHostStreams && e == cudaSuccess; ++k) {
+    evs[ne] = &ctx->ev_done[k];
+    e = cudaEventCreateWithFlags(evs[ne], cudaEventDisableTiming);
+    if (e == cudaSuccess)
+      ++ne;
+  }
+  for (int i = 0; i < kMaxChunks && e == cudaSuccess; ++i) {
+    evs[ne] = &ctx->ev_in[i];
+    e = cudaEventCreateWithFlags(evs[ne], cudaEventDisableTiming);
+    if (e != cudaSuccess)
+      break;
+    ++ne;
+    evs[ne] = &ctx->ev_comp[i];
+    e = cudaEventCreateWithFlags(evs[ne], cudaEventDisableTiming);
+    if (e == cudaSuccess)
+      ++ne;
   }
   if (e != cudaSuccess) {
-    for (int j = 0; j < k - 1; ++j) {
+    for (int j = 0; j < ns; ++j)
       cudaStreamDestroy(ctx->hs[j]);
-      cudaEventDestroy(ctx->ev_done[j]);
-    }
-    cudaEventDestroy(ctx->ev_start);
+    for (int j = 0; j < ne; ++j)
+      cudaEventDestroy(*evs[j]);
     return e;
   }
   ctx->host_streams = true;
@@ -2042,6 +2066,10 @@ mam4b_status mam4b_destroy(mam4b_ctx *ctx) {
       cudaStreamDestroy(ctx->hs[k]);
       cudaEventDestroy(ctx->ev_done[k]);
     }
+    for (int i = 0; i < kMaxChunks; ++i) {
+      cudaEventDestroy(ctx->ev_in[i]);
+      cudaEventDestroy(ctx->ev_comp[i]);
+    }
     cudaEventDestroy(ctx->ev_start);
   }
   delete ctx;
@@ -2162,29 +2190,43 @@ mam4b_status mam4b_step_host(mam4b_ctx *ctx, const double *in_slab, const double
     e = ensure_host_streams(ctx);
   if (e != cudaSuccess)
     return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_step_host scratch", e);
-  // chunks of whole columns
+  // chunks of whole columns: the first ones a quarter and a half of the
+  // steady size, so that the copy-out engine starts early; at most
+  // kMaxChunks (the steady size grows for very large batches)
   int chunk_cols = (int)(kHostChunkCells / nlev);
   if (chunk_cols < 1)
     chunk_cols = 1;
-  if ((ncol + chunk_cols - 1) / chunk_cols > kMaxChunks)
-    chunk_cols = (ncol + kMaxChunks - 1) / kMaxChunks;
-  const int nchunk = (ncol + chunk_cols - 1) / chunk_cols;
+  if ((ncol + chunk_cols - 1) / chunk_cols > kMaxChunks - 2)
+    chunk_cols = (ncol + kMaxChunks - 3) / (kMaxChunks - 2);
+  int chunk_start[kMaxChunks + 1];
+  int nchunk = 0;
+  for (int col = 0; col < ncol; ++nchunk) {
+    chunk_start[nchunk] = col;
+    const int want = nchunk == 0 ? (chunk_cols + 3) / 4 : nchunk == 1 ? (chunk_cols + 1) / 2 : chunk_cols;
+    col += want < ncol - col ? want : ncol - col;
+  }
+  chunk_start[nchunk] = ncol;
   // the internal streams start after the work already queued on us
   e = cudaEventRecord(ctx->ev_start, us);
   for (int k = 0; k < kHostStreams && e == cudaSuccess; ++k)
     e = cudaStreamWaitEvent(ctx->hs[k], ctx->ev_start, 0);
   const size_t dp = n * sizeof(double), hp = ld * sizeof(double);
+  cudaStream_t s_in = ctx->hs[0], s_out = ctx->hs[kHostStreams - 1];
   for (int i = 0; i < nchunk && e == cudaSuccess; ++i) {
-    cudaStream_t s = ctx->hs[i % kHostStreams];
-    const int col0 = i * chunk_cols;
-    const int ncc = (col0 + chunk_cols <= ncol) ? chunk_cols : ncol - col0;
+    cudaStream_t s = ctx->hs[1 + i % kComputeStreams];
+    const int col0 = chunk_start[i];
+    const int ncc = chunk_start[i + 1] - col0;
     const size_t c0 = (size_t)col0 * nlev, nc = (size_t)ncc * nlev;
     // field f of the chunk: nc doubles at f*ld + c0 on the host, f*n + c0 on the device
     e = cudaMemcpy2DAsync(ctx->d_in + c0, dp, in_slab + c0, hp, nc * sizeof(double), MAM4B_NIN,
-                          cudaMemcpyHostToDevice, s);
+                          cudaMemcpyHostToDevice, s_in);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(ctx->d_pblh + col0, pblh + col0, (size_t)ncc * sizeof(double),
-                          cudaMemcpyHostToDevice, s);
+                          cudaMemcpyHostToDevice, s_in);
+    if (e == cudaSuccess)
+      e = cudaEventRecord(ctx->ev_in[i], s_in);
+    if (e == cudaSuccess)
+      e = cudaStreamWaitEvent(s, ctx->ev_in[i], 0);
     if (e != cudaSuccess)
       break;
     StepArgs a;
@@ -2198,8 +2240,12 @@ mam4b_status mam4b_step_host(mam4b_ctx *ctx, const double *in_slab, const double
     set_step_scratch(ctx, a, c0, i);
     e = launch_pipeline(ctx, a, s, precision);
     if (e == cudaSuccess)
+      e = cudaEventRecord(ctx->ev_comp[i], s);
+    if (e == cudaSuccess)
+      e = cudaStreamWaitEvent(s_out, ctx->ev_comp[i], 0);
+    if (e == cudaSuccess)
       e = cudaMemcpy2DAsync(out_slab + c0, hp, ctx->d_out + c0, dp, nc * sizeof(double),
-                            MAM4B_NOUT, cudaMemcpyDeviceToHost, s);
+                            MAM4B_NOUT, cudaMemcpyDeviceToHost, s_out);
   }
   // us waits for every internal stream, then the call returns
   for (int k = 0; k < kHostStreams; ++k) {

@@ -179,8 +179,9 @@ def test_host_entry_matches_device_entry(cuda_device):
 
 
 def test_host_entry_chunked_pipeline(cuda_device):
-    """The host entry streams columns in chunks of ~2^19 cells over several
-    streams: 16,000 x 72 cells make 3 chunks, the last one ragged. A padded
+    """The host entry streams columns in chunks of up to ~2^18 cells over
+    copy-in, compute and copy-out streams: 16,000 x 72 cells make 6 chunks,
+    the first two smaller, the last one ragged. A padded
     host leading dimension and a second, smaller call on the same context
     (chunk scratch reused) must give the device entry's results bit for bit."""
     ctx = native.Context()
