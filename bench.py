@@ -22,6 +22,11 @@ One step = calcsize + water uptake + amicphys over every cell, dt = 1800 s.
   cpu_baseline  the mam4xx reference headers compiled for the host
          (oracle/_ref, OpenMP) on a bounded sample of the same cells
 
+  processes  the per-process entries (mam4b_calcsize_process,
+         mam4b_coagulation_process) on the same columns: cells/s, the HBM
+         roofline of their algorithmic bytes, and the reference's own
+         process classes on the host as their CPU baseline
+
 --impl reference times that CPU implementation alone, as the reference arm.
 Multi-GPU: one process per GPU (torchrun); each rank owns its own 65,536
 columns, no data exchange (cells are independent); timing is max over ranks.
@@ -168,6 +173,104 @@ def cpu_baseline(x, pblh_cell, dt, target_s=12.0):
     el = time.perf_counter() - t
     return {"value": n / el, "unit": "cells/s", "cores": cores, "kind": kind,
             "sample": "first %d cells of the %s workload (%.1f s, OpenMP over cells)" % (n, WORKLOAD, el)}
+
+
+# algorithmic bytes per cell of the per-process entries (FP64): CalcSize
+# reads 50 state fields and 20 tendencies it adds to (4 numbers, 16 common
+# species) and writes 24 tendencies and 8 diameters; Coagulation reads T,
+# p, 8 wet sizes, 32 interstitial states and their 32 tendencies and writes
+# both back
+PROCESS_BYTES_PER_CELL = {"calcsize": (50 + 20 + 24 + 8) * 8, "coagulation": (42 + 32 + 64) * 8}
+
+
+def processes_leg(native, torch, dev, stream, args, ws, hbm_peak):
+    """Per-process entries (mam4b_calcsize_process, mam4b_coagulation_process)
+    on the forward workload's columns, inputs resident, CUDA events; the
+    reference's own process classes (oracle/_ref, OpenMP over columns) timed
+    on 256 of those columns for the CPU baseline."""
+    from mam4xx_b200.workloads import make_process_inputs
+    ncol = args.ncol
+    d = make_process_inputs(WORKLOAD, ncol=ncol, seed=20261203 + 3 + 1000 * int(os.environ.get("RANK", "0")))
+    n = d["prog"].shape[1]
+    prog = torch.from_numpy(d["prog"]).to(dev)
+    prog_a0 = torch.from_numpy(d["prog_aero"]).to(dev)
+    prog_a = prog_a0.clone()
+    tend0 = torch.from_numpy(d["tend0"]).to(dev)
+    tend = tend0.clone()
+    dgn = torch.empty((8, n), dtype=torch.float64, device=dev)
+    t = torch.from_numpy(d["temp"]).to(dev)
+    p = torch.from_numpy(d["pmid"]).to(dev)
+    wet = torch.from_numpy(d["wet"]).to(dev)
+    ctx = native.Context()
+    pf = native.ProgFields.from_slab(prog.data_ptr(), n)
+    pa = native.ProgFields.from_slab(prog_a.data_ptr(), n)
+    tf = native.ProgFields.from_slab(tend.data_ptr(), n)
+    di = [dgn[m].data_ptr() for m in range(4)]
+    dc = [dgn[4 + m].data_ptr() for m in range(4)]
+    wd = [wet[m].data_ptr() for m in range(4)]
+    wg = [wet[4 + m].data_ptr() for m in range(4)]
+
+    def calcsize():
+        ctx.calcsize_process(pf, tf, di, dc, ncol, NLEV, d["dt"], stream=stream.cuda_stream)
+
+    def coag():
+        ctx.coagulation_process(t.data_ptr(), p.data_ptr(), wd, wg, pa, tf, ncol, NLEV, d["dt"],
+                                stream=stream.cuda_stream)
+
+    res = {}
+    for name, f in (("calcsize", calcsize), ("coagulation", coag)):
+        for _ in range(args.warmup):
+            f()
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        k = max(3, args.steps)
+        e0.record(stream)
+        for _ in range(k):
+            f()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / k
+        if ws > 1:
+            tt = torch.tensor([ms], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms = float(tt.item())
+        gbs = PROCESS_BYTES_PER_CELL[name] * n / (ms * 1e-3) / 1e9
+        res[name] = {"value": ws * n / (ms * 1e-3), "unit": "cells/s", "ms_per_call": ms,
+                     "cells_per_gpu": n,
+                     "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm_peak,
+                                  "unit": "GB/s", "frac": gbs / hbm_peak,
+                                  "algorithmic_bytes_per_cell": PROCESS_BYTES_PER_CELL[name]}}
+    # (the timed calls above keep adding to the same tendencies and, for
+    # coagulation, keep coagulating the same state: fine for timing)
+    if not args.no_cpu_baseline and int(os.environ.get("RANK", "0")) == 0:
+        try:
+            from oracle.pyoracle import ReferenceOracle
+            r = ReferenceOracle()
+            nc = min(ncol, 256)
+            m = nc * NLEV
+            sl = slice(0, m)
+            r.calcsize_process(nc, NLEV, d["prog"][:, sl], d["tend0"][:, sl], d["dt"])
+            t0 = time.perf_counter()
+            r.calcsize_process(nc, NLEV, d["prog"][:, sl], d["tend0"][:, sl], d["dt"])
+            t1 = time.perf_counter()
+            r.coag_process(nc, NLEV, d["temp"][sl], d["pmid"][sl], d["wet"][:, sl],
+                           d["prog_aero"][:, sl], d["tend0"][:, sl], d["dt"])
+            t2 = time.perf_counter()
+            import multiprocessing
+            for name, el in (("calcsize", t1 - t0), ("coagulation", t2 - t1)):
+                res[name]["cpu_baseline"] = {
+                    "value": m / el, "unit": "cells/s", "kind": "reference",
+                    "cores": multiprocessing.cpu_count(),
+                    "sample": "%d columns x %d levels, the reference's process class "
+                              "(OpenMP over columns)" % (nc, NLEV)}
+        except Exception as e:  # reported, never silently replaced
+            res["cpu_baseline_error"] = str(e)
+    ctx.close()
+    return res
 
 
 def adjoint_leg(native, torch, dev, stream, args, ws):
@@ -317,6 +420,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision legs")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint leg")
+    ap.add_argument("--no-processes", action="store_true",
+                    help="skip the per-process entries (CalcSize, Coagulation) leg")
     ap.add_argument("--adjoint-ncol", type=int, default=16384,
                     help="columns of the adjoint leg (16,384 is its configuration; smaller "
                          "only for profiling)")
@@ -463,6 +568,9 @@ def main():
         adjoint = adjoint_leg(native, torch, dev, stream, args, ws)
 
     peak, peak_kind = _peaks()
+    processes = None
+    if not args.no_processes:
+        processes = processes_leg(native, torch, dev, stream, args, ws, peak)
     fpeaks = _fp_peaks()
     flops_cell, special_cell = _flops_per_cell(WORKLOAD)
     roof64 = None
@@ -496,6 +604,7 @@ def main():
         "e2e": e2e,
         "precisions": precisions,
         "adjoint": adjoint,
+        "processes": processes,
         "gpu_launches": int(launches),
         "clocks": clocks,
         "device_flags": flags,

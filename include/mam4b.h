@@ -253,13 +253,79 @@ mam4b_status mam4b_step_slab_noalloc(const mam4b_config *cfg, const double *in_s
  * zero (these are held fixed), and the boundary-layer height has no
  * cotangent. The derivative is that of the branch the forward takes at the
  * given state (max/min clips, process thresholds and the SOA sub-step count
- * are not differentiated across). The SOA sub-step states are recomputed
+ * are not differentiated across). With condensation on, the SOA loop's
+ * state is stored before every sub-step; without it, states are recomputed
  * from checkpoints kept every 4 sub-steps. Uses the context's config;
  * asynchronous on `stream`. Device pointers.
  */
 mam4b_status mam4b_adjoint_slab(mam4b_ctx *ctx, const double *in_slab, const double *pblh,
                                 const double *out_bar, double *in_bar, size_t ld, int ncol,
                                 int nlev, double dt, void *stream);
+
+/*
+ * Per-process entries: the batched form of two mam4xx AeroProcess
+ * implementations, for host models that call the processes one at a time
+ * instead of the whole step. Their state is Prognostics-style: one device
+ * array per (mode, index), one entry per cell (cell = col*nlev + lev, the
+ * ColumnViews of mam4::Prognostics, src/mam4xx/aero_config.hpp:74-124,
+ * laid end to end). Mass mixing ratios in kg/kg, numbers in #/kg,
+ * tendencies per second. The second index of q_aero_* follows each
+ * reference process (they differ): see the entries.
+ */
+typedef struct mam4b_prog_fields {
+  double *n_mode_i[MAM4B_NUM_MODES];
+  double *n_mode_c[MAM4B_NUM_MODES];
+  double *q_aero_i[MAM4B_NUM_MODES][MAM4B_NUM_AERO];
+  double *q_aero_c[MAM4B_NUM_MODES][MAM4B_NUM_AERO];
+} mam4b_prog_fields;
+
+/* CalcSize::Config (src/mam4xx/calcsize.hpp:835-842); both default to 1. */
+typedef struct mam4b_calcsize_config {
+  int do_aitacc_transfer; /* aitken <-> accumulation exchange             */
+  int do_adjust;          /* number adjustment toward the size bounds     */
+} mam4b_calcsize_config;
+
+/*
+ * CalcSize::compute_tendencies (src/mam4xx/calcsize.hpp:963-1220) over a
+ * batch of columns. Reads progs->n_mode_{i,c}[m] and
+ * progs->q_aero_{i,c}[m][s] for the species s of mode m in the mode's own
+ * order (aero_modes.hpp:214-243: accumulation SO4 POM SOA BC DST NaCl MOM,
+ * aitken SO4 SOA NaCl MOM, coarse DST NaCl SO4 BC POM SOA MOM, primary
+ * carbon POM BC MOM). Writes dgncur_i[m], dgncur_c[m] (dry geometric-mean
+ * diameters [m], 4 device arrays each). Tendencies as the reference: the
+ * number tendencies of the modes it adjusts are overwritten; the aitken <->
+ * accumulation transfers are added to the number and common-species
+ * tendencies already in tends; other tendency arrays are not touched (only
+ * the fields read or written must be non-null). cfg NULL = defaults.
+ * Asynchronous on `stream`.
+ */
+mam4b_status mam4b_calcsize_process(mam4b_ctx *ctx, const mam4b_calcsize_config *cfg,
+                                    const mam4b_prog_fields *progs,
+                                    const mam4b_prog_fields *tends,
+                                    double *const dgncur_i[MAM4B_NUM_MODES],
+                                    double *const dgncur_c[MAM4B_NUM_MODES], int ncol,
+                                    int nlev, double dt, void *stream);
+
+/*
+ * Coagulation::compute_tendencies (src/mam4xx/coagulation.hpp:1198-1209,
+ * coagulation_rates_1box :1121-1183) over a batch of columns: Brownian
+ * coagulation of the aitken, accumulation and primary-carbon interstitial
+ * modes over dt. Reads temperature [K], pressure [Pa], the wet density
+ * [kg/m3] and wet diameter [m] of the 4 modes, progs->n_mode_i[m] and
+ * progs->q_aero_i[m][a] for all 7 AeroIds a of every mode (SOA SO4 POM BC
+ * NaCl DST MOM, mam4::AeroId order, as that routine indexes them: all 28
+ * arrays non-null). As the reference: tends->n_mode_i / q_aero_i +=
+ * (after - before) / dt, and progs->n_mode_i / q_aero_i are overwritten
+ * with the state after coagulation. Cloud-borne fields are not used.
+ * Asynchronous on `stream`.
+ */
+mam4b_status mam4b_coagulation_process(mam4b_ctx *ctx, const double *temperature,
+                                       const double *pressure,
+                                       const double *const wet_density[MAM4B_NUM_MODES],
+                                       const double *const wet_diameter_i[MAM4B_NUM_MODES],
+                                       const mam4b_prog_fields *progs,
+                                       const mam4b_prog_fields *tends, int ncol, int nlev,
+                                       double dt, void *stream);
 
 /* Synchronises the context's last stream, stores in *flags the OR of the
  * MAM4B_FLAG_* bits raised since the previous call (then clears them), and

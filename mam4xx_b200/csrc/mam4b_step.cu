@@ -22,6 +22,7 @@
 #include "mam4b_physics.cuh"
 #include "mam4b_physics_mixed.cuh"
 #include "mam4b_adjoint.cuh"
+#include "mam4b_process.cuh"
 
 namespace mam4b {
 
@@ -1707,6 +1708,20 @@ static_assert(sizeof(StepConsts) <= (size_t)SOA_FIELDS * kNoAllocCells * sizeof(
               "constants staging fits in the SOA region");
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 
+// ---- per-process entries (CalcSize, Coagulation): one thread per cell
+__global__ void __launch_bounds__(128) calcsize_process_kernel(const __grid_constant__ CalcSizeArgs a) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < a.ncell)
+    calcsize_process_cell(c_k, a, c);
+}
+
+__global__ void __launch_bounds__(128) coag_process_kernel(const __grid_constant__ CoagProcessArgs a) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const CoagTables T = {kCoagBm0ij, kCoagBm3i, kCoagBm0};
+  if (c < a.ncell)
+    coag_process_cell(c_k, T, a, c);
+}
+
 }  // namespace mam4b
 
 // =============================================================== C ABI
@@ -2475,6 +2490,121 @@ mam4b_status mam4b_adjoint_slab(mam4b_ctx *ctx, const double *in_slab, const dou
   if (e != cudaSuccess)
     return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_adjoint_slab launch", e);
   ctx->launches += 8;
+  return MAM4B_OK;
+}
+
+static bool copy_prog_fields(const mam4b_prog_fields *f, ProgFields &o) {
+  if (!f)
+    return false;
+  for (int m = 0; m < NMODE; ++m) {
+    o.n_i[m] = f->n_mode_i[m];
+    o.n_c[m] = f->n_mode_c[m];
+    for (int x = 0; x < NAER; ++x) {
+      o.q_i[m][x] = f->q_aero_i[m][x];
+      o.q_c[m][x] = f->q_aero_c[m][x];
+    }
+  }
+  return true;
+}
+
+// CalcSize::compute_tendencies (calcsize.hpp:963-1220), batched
+mam4b_status mam4b_calcsize_process(mam4b_ctx *ctx, const mam4b_calcsize_config *cfg,
+                                    const mam4b_prog_fields *progs,
+                                    const mam4b_prog_fields *tends,
+                                    double *const dgncur_i[MAM4B_NUM_MODES],
+                                    double *const dgncur_c[MAM4B_NUM_MODES], int ncol,
+                                    int nlev, double dt, void *stream) {
+  const char *what = "mam4b_calcsize_process";
+  if (!ctx || ncol < 0 || nlev <= 0 || !(dt > 0.0) || !isfinite(dt) || !dgncur_i || !dgncur_c)
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, what, cudaSuccess);
+  CalcSizeArgs a;
+  memset(&a, 0, sizeof(a));
+  if (!copy_prog_fields(progs, a.progs) || !copy_prog_fields(tends, a.tends))
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, what, cudaSuccess);
+  a.do_aitacc_transfer = cfg ? (cfg->do_aitacc_transfer != 0) : 1;
+  a.do_adjust = cfg ? (cfg->do_adjust != 0) : 1;
+  // every field the process reads or writes must be given
+  for (int m = 0; m < NMODE; ++m) {
+    if (!dgncur_i[m] || !dgncur_c[m] || !a.progs.n_i[m] || !a.progs.n_c[m])
+      return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_calcsize_process: null field",
+                     cudaSuccess);
+    a.dgn_i[m] = dgncur_i[m];
+    a.dgn_c[m] = dgncur_c[m];
+    const bool tn = a.do_adjust && !(a.do_aitacc_transfer && m <= 1);
+    const bool tx = a.do_aitacc_transfer && m <= 1;
+    if ((tn || tx) && (!a.tends.n_i[m] || !a.tends.n_c[m]))
+      return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_calcsize_process: null tendency",
+                     cudaSuccess);
+    for (int s = 0; s < K::nspec(m); ++s) {
+      if (!a.progs.q_i[m][s] || !a.progs.q_c[m][s])
+        return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_calcsize_process: null field",
+                       cudaSuccess);
+    }
+  }
+  if (a.do_aitacc_transfer) {
+    const int acc_s[4] = {0, 2, 5, 6}, ait_s[4] = {0, 1, 2, 3};
+    for (int k = 0; k < 4; ++k)
+      if (!a.tends.q_i[0][acc_s[k]] || !a.tends.q_c[0][acc_s[k]] || !a.tends.q_i[1][ait_s[k]] ||
+          !a.tends.q_c[1][ait_s[k]])
+        return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT,
+                       "mam4b_calcsize_process: null tendency", cudaSuccess);
+  }
+  a.ncell = (long long)ncol * nlev;
+  a.dt = dt;
+  cudaStream_t s = (cudaStream_t)stream;
+  ctx->last_stream = s;
+  if (a.ncell == 0)
+    return MAM4B_OK;
+  const int block = 128;
+  calcsize_process_kernel<<<(unsigned)((a.ncell + block - 1) / block), block, 0, s>>>(a);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, what, e);
+  ctx->launches += 1;
+  return MAM4B_OK;
+}
+
+// Coagulation::compute_tendencies (coagulation.hpp:1198-1209), batched
+mam4b_status mam4b_coagulation_process(mam4b_ctx *ctx, const double *temperature,
+                                       const double *pressure,
+                                       const double *const wet_density[MAM4B_NUM_MODES],
+                                       const double *const wet_diameter_i[MAM4B_NUM_MODES],
+                                       const mam4b_prog_fields *progs,
+                                       const mam4b_prog_fields *tends, int ncol, int nlev,
+                                       double dt, void *stream) {
+  const char *what = "mam4b_coagulation_process";
+  if (!ctx || ncol < 0 || nlev <= 0 || !(dt > 0.0) || !isfinite(dt) || !temperature ||
+      !pressure || !wet_density || !wet_diameter_i)
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, what, cudaSuccess);
+  CoagProcessArgs a;
+  memset(&a, 0, sizeof(a));
+  if (!copy_prog_fields(progs, a.progs) || !copy_prog_fields(tends, a.tends))
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, what, cudaSuccess);
+  a.temp = temperature;
+  a.pmid = pressure;
+  for (int m = 0; m < NMODE; ++m) {
+    if (!wet_density[m] || !wet_diameter_i[m] || !a.progs.n_i[m] || !a.tends.n_i[m])
+      return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_coagulation_process: null field",
+                     cudaSuccess);
+    a.wet_density[m] = wet_density[m];
+    a.dgn_awet[m] = wet_diameter_i[m];
+    for (int x = 0; x < NAER; ++x)
+      if (!a.progs.q_i[m][x] || !a.tends.q_i[m][x])
+        return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT,
+                       "mam4b_coagulation_process: null field", cudaSuccess);
+  }
+  a.ncell = (long long)ncol * nlev;
+  a.dt = dt;
+  cudaStream_t s = (cudaStream_t)stream;
+  ctx->last_stream = s;
+  if (a.ncell == 0)
+    return MAM4B_OK;
+  const int block = 128;
+  coag_process_kernel<<<(unsigned)((a.ncell + block - 1) / block), block, 0, s>>>(a);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, what, e);
+  ctx->launches += 1;
   return MAM4B_OK;
 }
 

@@ -39,6 +39,36 @@ class TendView(ctypes.Structure):
     _fields_ = [("field", ctypes.c_void_p * NOUT), ("diag", ctypes.c_void_p * NDIAG)]
 
 
+NUM_MODES, NUM_AERO = 4, 7
+PROG_FIELDS = 64  # n_mode_i[4], n_mode_c[4], q_aero_i[4][7], q_aero_c[4][7]
+
+
+class ProgFields(ctypes.Structure):
+    """mam4b_prog_fields: Prognostics-style device arrays per (mode, index)."""
+    _fields_ = [("n_mode_i", ctypes.c_void_p * NUM_MODES),
+                ("n_mode_c", ctypes.c_void_p * NUM_MODES),
+                ("q_aero_i", (ctypes.c_void_p * NUM_AERO) * NUM_MODES),
+                ("q_aero_c", (ctypes.c_void_p * NUM_AERO) * NUM_MODES)]
+
+    @classmethod
+    def from_slab(cls, base, n):
+        """The 64 fields of one slab of doubles, field f at base + 8 f n:
+        n_mode_i[4], n_mode_c[4], q_aero_i[4][7], q_aero_c[4][7]."""
+        f = cls()
+        for m in range(NUM_MODES):
+            f.n_mode_i[m] = base + 8 * m * n
+            f.n_mode_c[m] = base + 8 * (4 + m) * n
+            for a in range(NUM_AERO):
+                f.q_aero_i[m][a] = base + 8 * (8 + 7 * m + a) * n
+                f.q_aero_c[m][a] = base + 8 * (36 + 7 * m + a) * n
+        return f
+
+
+class CalcSizeConfig(ctypes.Structure):
+    """mam4b_calcsize_config: CalcSize::Config (src/mam4xx/calcsize.hpp:835-842)."""
+    _fields_ = [("do_aitacc_transfer", ctypes.c_int), ("do_adjust", ctypes.c_int)]
+
+
 _lib = None
 
 
@@ -69,6 +99,14 @@ def lib():
         L.mam4b_step_slab_noalloc.restype = I
         L.mam4b_adjoint_slab.argtypes = [P, P, P, P, P, S, I, I, D, P]
         L.mam4b_adjoint_slab.restype = I
+        PF = ctypes.POINTER(ProgFields)
+        P4 = ctypes.c_void_p * NUM_MODES
+        L.mam4b_calcsize_process.argtypes = [P, ctypes.POINTER(CalcSizeConfig), PF, PF,
+                                             ctypes.POINTER(P4), ctypes.POINTER(P4), I, I, D, P]
+        L.mam4b_calcsize_process.restype = I
+        L.mam4b_coagulation_process.argtypes = [P, P, P, ctypes.POINTER(P4), ctypes.POINTER(P4),
+                                                PF, PF, I, I, D, P]
+        L.mam4b_coagulation_process.restype = I
         L.mam4b_launch_count.argtypes = [P]
         L.mam4b_launch_count.restype = ctypes.c_uint64
         _lib = L
@@ -78,7 +116,7 @@ def lib():
 EXPORTED = ["mam4b_abi_version", "mam4b_default_config", "mam4b_create", "mam4b_destroy",
             "mam4b_step", "mam4b_step_slab", "mam4b_step_host", "mam4b_last_status",
             "mam4b_last_error", "mam4b_launch_count", "mam4b_step_slab_noalloc",
-            "mam4b_adjoint_slab"]
+            "mam4b_adjoint_slab", "mam4b_calcsize_process", "mam4b_coagulation_process"]
 
 
 def default_config(**overrides):
@@ -157,6 +195,32 @@ class Context:
                                           int(ld), int(ncol), int(nlev), float(dt),
                                           ctypes.c_void_p(stream))
         self._check(st, "mam4b_adjoint_slab")
+
+    def calcsize_process(self, progs, tends, dgncur_i, dgncur_c, ncol, nlev, dt,
+                         do_aitacc_transfer=True, do_adjust=True, stream=0):
+        """CalcSize::compute_tendencies over ncol x nlev cells
+        (mam4b_calcsize_process). progs, tends: ProgFields; dgncur_i,
+        dgncur_c: 4 device pointers each."""
+        cfg = CalcSizeConfig(int(do_aitacc_transfer), int(do_adjust))
+        di = (ctypes.c_void_p * NUM_MODES)(*dgncur_i)
+        dc = (ctypes.c_void_p * NUM_MODES)(*dgncur_c)
+        st = self._lib.mam4b_calcsize_process(self._h, ctypes.byref(cfg), ctypes.byref(progs),
+                                              ctypes.byref(tends), ctypes.byref(di),
+                                              ctypes.byref(dc), int(ncol), int(nlev), float(dt),
+                                              ctypes.c_void_p(stream))
+        self._check(st, "mam4b_calcsize_process")
+
+    def coagulation_process(self, temperature, pressure, wet_density, wet_diameter_i, progs,
+                            tends, ncol, nlev, dt, stream=0):
+        """Coagulation::compute_tendencies over ncol x nlev cells
+        (mam4b_coagulation_process); progs are updated in place."""
+        wd = (ctypes.c_void_p * NUM_MODES)(*wet_density)
+        wg = (ctypes.c_void_p * NUM_MODES)(*wet_diameter_i)
+        st = self._lib.mam4b_coagulation_process(self._h, temperature, pressure, ctypes.byref(wd),
+                                                 ctypes.byref(wg), ctypes.byref(progs),
+                                                 ctypes.byref(tends), int(ncol), int(nlev),
+                                                 float(dt), ctypes.c_void_p(stream))
+        self._check(st, "mam4b_coagulation_process")
 
     def last_status(self):
         f = ctypes.c_uint32(0)

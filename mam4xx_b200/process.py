@@ -87,6 +87,7 @@ Tendencies = Prognostics
 class Diagnostics:
     """Outputs of the step from mam4::Diagnostics: dry and wet geometric-mean
     diameters and wet density of the interstitial modes, the aerosol water,
+    the cloud-borne dry diameters (written by CalcSizeProcess),
     and optionally the amicphys process tendencies
     (gas_aero_exchange_{condensation, renaming, nucleation, coagulation,
     renaming_cloud_borne}, each a list of 31 tracer tensors)."""
@@ -95,8 +96,10 @@ class Diagnostics:
                  "renaming_cloud_borne")
 
     def __init__(self, dry_geometric_mean_diameter_i, wet_geometric_mean_diameter_i,
-                 wet_density, aerosol_water, gas_aero_exchange=None):
+                 wet_density, aerosol_water, gas_aero_exchange=None,
+                 dry_geometric_mean_diameter_c=None):
         self.dry_geometric_mean_diameter_i = dry_geometric_mean_diameter_i
+        self.dry_geometric_mean_diameter_c = dry_geometric_mean_diameter_c
         self.wet_geometric_mean_diameter_i = wet_geometric_mean_diameter_i
         self.wet_density = wet_density
         self.aerosol_water = aerosol_water
@@ -109,7 +112,7 @@ class Diagnostics:
         if with_process_tendencies:
             gae = {p: [e() for _ in range(31)] for p in cls.PROCESSES}
         return cls([e() for _ in range(4)], [e() for _ in range(4)], [e() for _ in range(4)],
-                   [e() for _ in range(4)], gae)
+                   [e() for _ in range(4)], gae, [e() for _ in range(4)])
 
 
 def _ptr(t, shape, what):
@@ -250,3 +253,106 @@ def outputs_from_slab(out_slab, ncol, nlev, diag_slab=None):
     diags = Diagnostics([v(52 + m) for m in range(4)], [v(56 + m) for m in range(4)],
                         [v(60 + m) for m in range(4)], [v(64 + m) for m in range(4)], gae)
     return tends, diags
+
+
+def _prog_fields(p, shp, what, nspec_only):
+    """ProgFields of a Prognostics container of (ncol, nlev) tensors; index
+    lists shorter than 7 leave the remaining (mode, index) pairs null."""
+    f = native.ProgFields()
+    for m in range(NUM_MODES):
+        f.n_mode_i[m] = _ptr(p.n_mode_i[m], shp, "%s n_mode_i[%d]" % (what, m))
+        f.n_mode_c[m] = _ptr(p.n_mode_c[m], shp, "%s n_mode_c[%d]" % (what, m))
+        for k, t in enumerate(p.q_aero_i[m]):
+            if t is not None:
+                f.q_aero_i[m][k] = _ptr(t, shp, "%s q_aero_i[%d][%d]" % (what, m, k))
+        for k, t in enumerate(p.q_aero_c[m]):
+            if t is not None:
+                f.q_aero_c[m][k] = _ptr(t, shp, "%s q_aero_c[%d][%d]" % (what, m, k))
+    return f
+
+
+class CalcSizeProcess:
+    """mam4::CalcSize behind the AeroProcess contract, batched over columns
+    (mam4b_calcsize_process; src/mam4xx/calcsize.hpp:835-1220). Prognostics
+    and Tendencies index q_aero_*[mode] by the species' position within the
+    mode, as CalcSize does. Writes the dry diameters of both phases into
+    diagnostics.dry_geometric_mean_diameter_i / _c."""
+
+    class Config:
+        def __init__(self, do_aitacc_transfer=True, do_adjust=True):
+            self.do_aitacc_transfer = do_aitacc_transfer
+            self.do_adjust = do_adjust
+
+    def __init__(self, aero_config=None, process_config=None):
+        self.init(aero_config or AeroConfig(), process_config)
+
+    @staticmethod
+    def name():
+        return "MAM4 CalcSize on B200"
+
+    def init(self, aero_config, process_config=None):
+        self.aero_config = aero_config
+        self.process_config = process_config or CalcSizeProcess.Config()
+        self._ctx = native.Context()
+
+    def validate(self, atmosphere, prognostics):
+        return True  # calcsize.hpp: no validity checks
+
+    def compute_tendencies(self, t, dt, atmosphere, surface, prognostics, diagnostics,
+                           tendencies, stream=None):
+        ncol, nlev = atmosphere.shape
+        shp = (ncol, nlev)
+        pf = _prog_fields(prognostics, shp, "prognostics", True)
+        tf = _prog_fields(tendencies, shp, "tendencies", True)
+        di = [_ptr(diagnostics.dry_geometric_mean_diameter_i[m], shp, "dgncur_i") for m in range(4)]
+        dc = [_ptr(diagnostics.dry_geometric_mean_diameter_c[m], shp, "dgncur_c") for m in range(4)]
+        s = stream if stream is not None else torch.cuda.current_stream()
+        c = self.process_config
+        self._ctx.calcsize_process(pf, tf, di, dc, ncol, nlev, dt,
+                                   do_aitacc_transfer=c.do_aitacc_transfer,
+                                   do_adjust=c.do_adjust, stream=s.cuda_stream)
+
+
+class CoagulationProcess:
+    """mam4::Coagulation behind the AeroProcess contract, batched over
+    columns (mam4b_coagulation_process; src/mam4xx/coagulation.hpp:
+    1121-1209). As that routine, q_aero_i[mode] is indexed by mam4::AeroId
+    (SOA SO4 POM BC NaCl DST MOM) and needs all 7 entries for every mode;
+    reads diagnostics.wet_density and wet_geometric_mean_diameter_i, adds
+    to the interstitial tendencies and overwrites the interstitial
+    prognostics with the coagulated state."""
+
+    class Config:
+        pass
+
+    def __init__(self, aero_config=None, process_config=None):
+        self.init(aero_config or AeroConfig(), process_config)
+
+    @staticmethod
+    def name():
+        return "MAM4 Coagulation on B200"
+
+    def init(self, aero_config, process_config=None):
+        self.aero_config = aero_config
+        self.process_config = process_config or CoagulationProcess.Config()
+        self._ctx = native.Context()
+
+    def validate(self, atmosphere, prognostics):
+        return True  # coagulation.hpp:47-52 returns true
+
+    def compute_tendencies(self, t, dt, atmosphere, surface, prognostics, diagnostics,
+                           tendencies, stream=None):
+        ncol, nlev = atmosphere.shape
+        shp = (ncol, nlev)
+        for m in range(NUM_MODES):
+            if len(prognostics.q_aero_i[m]) != NUM_AERO or len(tendencies.q_aero_i[m]) != NUM_AERO:
+                raise ValueError("Coagulation needs q_aero_i[mode] for all %d AeroIds" % NUM_AERO)
+        pf = _prog_fields(prognostics, shp, "prognostics", False)
+        tf = _prog_fields(tendencies, shp, "tendencies", False)
+        wd = [_ptr(diagnostics.wet_density[m], shp, "wet_density") for m in range(4)]
+        wg = [_ptr(diagnostics.wet_geometric_mean_diameter_i[m], shp, "wet diameter")
+              for m in range(4)]
+        s = stream if stream is not None else torch.cuda.current_stream()
+        self._ctx.coagulation_process(_ptr(atmosphere.temperature, shp, "temperature"),
+                                      _ptr(atmosphere.pressure, shp, "pressure"), wd, wg, pf, tf,
+                                      ncol, nlev, dt, stream=s.cuda_stream)

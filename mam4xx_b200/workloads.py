@@ -175,3 +175,47 @@ def make_workload(name="c1", ncol=None, nlev=None, seed=None):
 
 def pblh_per_cell(w):
     return np.repeat(w["pblh"], w["nlev"])
+
+
+# ------------------------------------------------------ per-process inputs
+AERO_IDS = ("SOA", "SO4", "POM", "BC", "NaCl", "DST", "MOM")  # mam4::AeroId order
+
+
+def prog_slab(in_slab, by_aero_id=False):
+    """The 64 Prognostics-style fields (n_mode_i[4], n_mode_c[4],
+    q_aero_i[4][7], q_aero_c[4][7]) of a step input slab. The second index
+    of q_aero_* is the species' position within its mode (CalcSize's
+    indexing), or its mam4::AeroId with by_aero_id (Coagulation's), where
+    the (mode, AeroId) pairs that are not species of the mode are zero."""
+    n = in_slab.shape[1]
+    out = np.zeros((64, n))
+    for slot, (m, sp) in enumerate(POPULATIONS):
+        for phase, base in ((0, IN_AER_I), (1, IN_AER_C)):
+            row = in_slab[base + slot]
+            if sp == "num":
+                out[4 * phase + m] = row
+            else:
+                k = AERO_IDS.index(sp) if by_aero_id else MODE_SPECIES_SLOTS[m].index(slot)
+                out[8 + 28 * phase + 7 * m + k] = row
+    return out
+
+
+def make_process_inputs(name="c2", ncol=None, nlev=None, seed=None):
+    """Inputs of the per-process entries from a workload configuration:
+    the step's populations as Prognostics fields (both index conventions),
+    T and p, wet diameters of each mode drawn around its nominal size
+    (0.5..4 x, log-uniform) and wet densities U(1000, 2000) kg/m3, and
+    non-zero starting tendencies (the processes add to them)."""
+    w = make_workload(name, ncol=ncol, nlev=nlev, seed=seed)
+    x = w["in_slab"]
+    n = x.shape[1]
+    rng = np.random.default_rng(77 + (seed or 0))
+    wet = np.zeros((8, n))
+    for m in range(4):
+        wet[m] = rng.uniform(1000.0, 2000.0, n)
+        wet[4 + m] = _DGN_NOM[m] * _logu(rng, 0.5, 4.0, n)
+    prog = prog_slab(x)
+    tend0 = rng.standard_normal((64, n)) * (np.abs(prog) / 86400.0 + 1e-30)
+    return {"ncol": w["ncol"], "nlev": w["nlev"], "dt": w["dt"], "temp": x[0].copy(),
+            "pmid": x[1].copy(), "wet": wet, "prog": prog, "prog_aero": prog_slab(x, True),
+            "tend0": tend0}

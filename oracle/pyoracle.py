@@ -143,6 +143,38 @@ class ReferenceOracle(_Oracle):
     prefix = "mam4ref"
     path = REF_SO
 
+    def calcsize_process(self, ncol, nlev, prog, tend, dt, do_aitacc_transfer=True,
+                         do_adjust=True):
+        """mam4::CalcSize::compute_tendencies column by column. prog, tend:
+        (64, ncell) field-major (n_mode_i[4], n_mode_c[4], q_aero_i[4][7],
+        q_aero_c[4][7]); returns (tend after, dgn (8, ncell): interstitial
+        then cloud-borne dry diameters)."""
+        prog = np.array(prog, dtype=np.float64, order="C")
+        tend = np.array(tend, dtype=np.float64, order="C")
+        dgn = np.zeros((8, prog.shape[1]))
+        f = self.lib.mam4ref_calcsize_process
+        f.argtypes = [_I, _I, _I, _I, _D, _P, _P, _P]
+        f.restype = None
+        f(ncol, nlev, int(do_aitacc_transfer), int(do_adjust), dt, prog.ctypes.data,
+          tend.ctypes.data, dgn.ctypes.data)
+        return tend, dgn
+
+    def coag_process(self, ncol, nlev, temp, pmid, wet, prog, tend, dt):
+        """mam4::Coagulation::compute_tendencies column by column. wet: (8,
+        ncell) wet density [4] then wet diameter [4]; returns (prog after,
+        tend after)."""
+        prog = np.array(prog, dtype=np.float64, order="C")
+        tend = np.array(tend, dtype=np.float64, order="C")
+        wet = np.ascontiguousarray(wet, dtype=np.float64)
+        t = np.ascontiguousarray(temp, dtype=np.float64)
+        p = np.ascontiguousarray(pmid, dtype=np.float64)
+        f = self.lib.mam4ref_coag_process
+        f.argtypes = [_I, _I, _D, _P, _P, _P, _P, _P]
+        f.restype = None
+        f(ncol, nlev, dt, t.ctypes.data, p.ctypes.data, wet.ctypes.data, prog.ctypes.data,
+          tend.ctypes.data)
+        return prog, tend
+
 
 class PortOracle(_Oracle):
     prefix = "mam4orc"

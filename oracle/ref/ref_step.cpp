@@ -25,6 +25,8 @@
 //      q_pregaschem = q_precldchem = qq and qqcw_precldchem = qqcw;
 //   7. vmr -> mmr and tendency = (after - before)/dt.
 
+#include <mam4xx/calcsize.hpp>
+#include <mam4xx/coagulation.hpp>
 #include <mam4xx/mam4_amicphys.hpp>
 #include <mam4xx/modal_aero_calcsize.hpp>
 #include <mam4xx/water_uptake.hpp>
@@ -32,6 +34,7 @@
 #include "../oracle_api.h"
 
 #include <cstring>
+#include <vector>
 #include <omp.h>
 
 namespace {
@@ -286,6 +289,96 @@ void mam4ref_aging(unsigned n_so4_monolayers_pcage, const double *dgn_a,
       reinterpret_cast<Real(*)[4]>(qaer_del_cond),
       reinterpret_cast<Real(*)[4]>(qaer_del_coag),
       reinterpret_cast<Real(*)[1]>(qaer_del_coag_in));
+}
+
+// Per-process entries: the reference's CalcSize and Coagulation process
+// classes run column by column (OpenMP over columns) on Prognostics / Diagnostics / Tendencies
+// whose ColumnViews point into the caller's field-major arrays
+// (cell = col * nlev + lev):
+//   prog, tend  64 fields: n_mode_i[4], n_mode_c[4], q_aero_i[4][7],
+//               q_aero_c[4][7] (tend is read and written)
+//   dgn         8 fields: dry diameters interstitial [4], cloud-borne [4]
+namespace {
+constexpr int kProgFields = 64;
+
+void bind_prog(mam4::Prognostics &p, double *base, size_t n, size_t c0, int nlev) {
+  for (int m = 0; m < 4; ++m) {
+    p.n_mode_i[m] = mam4::ColumnView(base + (size_t)m * n + c0, nlev);
+    p.n_mode_c[m] = mam4::ColumnView(base + (size_t)(4 + m) * n + c0, nlev);
+    for (int a = 0; a < 7; ++a) {
+      p.q_aero_i[m][a] = mam4::ColumnView(base + (size_t)(8 + 7 * m + a) * n + c0, nlev);
+      p.q_aero_c[m][a] = mam4::ColumnView(base + (size_t)(36 + 7 * m + a) * n + c0, nlev);
+    }
+  }
+}
+
+mam4::Atmosphere column_atmosphere(int nlev, const double *temp, const double *pmid,
+                                   std::vector<double> &zeros) {
+  zeros.assign((size_t)nlev + 1, 0.0);
+  mam4::ConstColumnView z(zeros.data(), nlev);
+  mam4::ConstColumnView t = temp ? mam4::ConstColumnView(temp, nlev) : z;
+  mam4::ConstColumnView p = pmid ? mam4::ConstColumnView(pmid, nlev) : z;
+  mam4::ConstColumnView zi(zeros.data(), nlev + 1);
+  return mam4::Atmosphere(nlev, t, p, z, z, z, z, z, z, z, zi, z, z, 1000.0);
+}
+} // namespace
+
+void mam4ref_calcsize_process(int ncol, int nlev, int do_aitacc_transfer, int do_adjust,
+                              double dt, double *prog, double *tend, double *dgn) {
+  const size_t n = (size_t)ncol * nlev;
+  mam4::AeroConfig aero_config;
+  mam4::CalcSize::Config cfg;
+  cfg.do_aitacc_transfer = do_aitacc_transfer != 0;
+  cfg.do_adjust = do_adjust != 0;
+  mam4::CalcSize process;
+  process.init(aero_config, cfg);
+  const mam4::Surface sfc{};
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int col = 0; col < ncol; ++col) {
+    std::vector<double> zeros;
+    const size_t c0 = (size_t)col * nlev;
+    mam4::Prognostics progs(nlev);
+    mam4::Tendencies tends(nlev);
+    mam4::Diagnostics diags(nlev);
+    bind_prog(progs, prog, n, c0, nlev);
+    bind_prog(tends, tend, n, c0, nlev);
+    for (int m = 0; m < 4; ++m) {
+      diags.dry_geometric_mean_diameter_i[m] = mam4::ColumnView(dgn + (size_t)m * n + c0, nlev);
+      diags.dry_geometric_mean_diameter_c[m] =
+          mam4::ColumnView(dgn + (size_t)(4 + m) * n + c0, nlev);
+    }
+    const mam4::Atmosphere atm = column_atmosphere(nlev, nullptr, nullptr, zeros);
+    mam4::ThreadTeam team;
+    process.compute_tendencies(aero_config, team, 0.0, dt, atm, sfc, progs, diags, tends);
+  }
+}
+
+// wet: 8 fields, wet density [4] then wet diameter [4]
+void mam4ref_coag_process(int ncol, int nlev, double dt, const double *temp,
+                          const double *pmid, double *wet, double *prog, double *tend) {
+  const size_t n = (size_t)ncol * nlev;
+  mam4::AeroConfig aero_config;
+  mam4::Coagulation process;
+  process.init(aero_config);
+  const mam4::Surface sfc{};
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int col = 0; col < ncol; ++col) {
+    std::vector<double> zeros;
+    const size_t c0 = (size_t)col * nlev;
+    mam4::Prognostics progs(nlev);
+    mam4::Tendencies tends(nlev);
+    mam4::Diagnostics diags(nlev);
+    bind_prog(progs, prog, n, c0, nlev);
+    bind_prog(tends, tend, n, c0, nlev);
+    for (int m = 0; m < 4; ++m) {
+      diags.wet_density[m] = mam4::ColumnView(wet + (size_t)m * n + c0, nlev);
+      diags.wet_geometric_mean_diameter_i[m] =
+          mam4::ColumnView(wet + (size_t)(4 + m) * n + c0, nlev);
+    }
+    const mam4::Atmosphere atm = column_atmosphere(nlev, temp + c0, pmid + c0, zeros);
+    mam4::ThreadTeam team;
+    process.compute_tendencies(aero_config, team, 0.0, dt, atm, sfc, progs, diags, tends);
+  }
 }
 
 long mam4ref_assert_failures(void) { return mam4shim::assert_failures(); }

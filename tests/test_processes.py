@@ -1,0 +1,70 @@
+"""Per-process entries on the CPU side: the reference's own CalcSize and
+Coagulation process classes (compiled unchanged into oracle/_ref) behave as
+the reference documents, and the C ABI rejects bad arguments before any
+CUDA call."""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from mam4xx_b200 import native
+from mam4xx_b200.workloads import AERO_IDS, make_process_inputs, prog_slab, make_workload
+
+
+def test_prog_slab_layouts():
+    w = make_workload("c2", ncol=2, seed=4)
+    p = prog_slab(w["in_slab"])
+    q = prog_slab(w["in_slab"], by_aero_id=True)
+    # numbers are the same; accumulation SO4 is species 0 of the mode, AeroId 1
+    np.testing.assert_array_equal(p[:8], q[:8])
+    np.testing.assert_array_equal(p[8 + 0], q[8 + AERO_IDS.index("SO4")])
+    # primary carbon has POM, BC, MOM only
+    assert (q[8 + 21 + AERO_IDS.index("SO4")] == 0).all()
+    assert (p[8 + 21 + 3:8 + 28] == 0).all()
+
+
+def test_reference_calcsize_process_touches_what_it_documents(ref_oracle):
+    d = make_process_inputs("c2", ncol=16, seed=11)
+    tend, dgn = ref_oracle.calcsize_process(d["ncol"], d["nlev"], d["prog"], d["tend0"], d["dt"])
+    assert np.isfinite(tend).all() and (dgn > 0).all()
+    changed = set(np.nonzero(np.abs(tend - d["tend0"]).max(axis=1))[0])
+    # numbers of all modes (adjusted or exchanged), and the species the
+    # aitken and accumulation modes share, both phases
+    common = {8 + s for s in (0, 2, 5, 6)} | {15 + s for s in range(4)}
+    common |= {c + 28 for c in common}
+    assert changed <= set(range(8)) | common
+    # without adjustment the exchange conserves aitken + accumulation number
+    t2, _ = ref_oracle.calcsize_process(d["ncol"], d["nlev"], d["prog"], d["tend0"], d["dt"],
+                                        do_adjust=False)
+    ch = t2 - d["tend0"]
+    assert np.abs(ch[0] + ch[1]).max() <= 1e-12 * np.abs(ch[0]).max()
+    # no exchange and no adjustment: nothing changes, diameters still written
+    t3, dg3 = ref_oracle.calcsize_process(d["ncol"], d["nlev"], d["prog"], d["tend0"], d["dt"],
+                                          do_aitacc_transfer=False, do_adjust=False)
+    np.testing.assert_array_equal(t3, d["tend0"])
+    assert (dg3 > 0).all()
+
+
+def test_reference_coag_process_conserves_species_mass(ref_oracle):
+    d = make_process_inputs("c2", ncol=16, seed=12)
+    prog, tend = ref_oracle.coag_process(d["ncol"], d["nlev"], d["temp"], d["pmid"], d["wet"],
+                                         d["prog_aero"], d["tend0"], d["dt"])
+    for a in range(7):
+        before = sum(d["prog_aero"][8 + 7 * m + a] for m in range(4))
+        after = sum(prog[8 + 7 * m + a] for m in range(4))
+        assert np.abs(after - before).max() <= 1e-14 * np.abs(before).max() + 1e-300
+    assert (prog[:4] <= d["prog_aero"][:4] * (1 + 1e-15)).all()  # coagulation removes number
+    np.testing.assert_allclose((tend - d["tend0"])[:36] * d["dt"], (prog - d["prog_aero"])[:36],
+                               rtol=1e-9, atol=1e-12 * np.abs(d["prog_aero"]).max())
+
+
+def test_process_entries_reject_bad_arguments_without_a_device():
+    L = native.lib()
+    pf = native.ProgFields()
+    four = (ctypes.c_void_p * 4)()
+    assert L.mam4b_calcsize_process(None, None, ctypes.byref(pf), ctypes.byref(pf),
+                                    ctypes.byref(four), ctypes.byref(four), 1, 1, 1.0, None) == 1
+    assert L.mam4b_coagulation_process(None, None, None, ctypes.byref(four), ctypes.byref(four),
+                                       ctypes.byref(pf), ctypes.byref(pf), 1, 1, 1.0,
+                                       None) == 1
