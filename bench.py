@@ -273,6 +273,54 @@ def processes_leg(native, torch, dev, stream, args, ws, hbm_peak):
     return res
 
 
+def tracers_leg(native, torch, dev, stream, args, ws, x, pb, ncol, dt, step_ms):
+    """The step through mam4b_step_tracers on TracersView-layout arrays
+    (state_q tracer order, 40 tracers, tracer stride = cells) built from
+    the forward workload's inputs: same kernels, read and written in place."""
+    n = x.shape[1]
+    q = torch.zeros((40, n), dtype=torch.float64, device=dev)
+    qc = torch.zeros((40, n), dtype=torch.float64, device=dev)
+    q[0] = x[3]
+    q[11] = x[5]
+    q[14] = x[6]
+    q[15:40] = x[7:32]
+    qc[15:40] = x[32:57]
+    pt_q = torch.zeros_like(q)
+    pt_c = torch.zeros_like(q)
+    mode = torch.empty((16, n), dtype=torch.float64, device=dev)
+    ctx = native.Context()
+
+    def f():
+        ctx.step_tracers(q.data_ptr(), qc.data_ptr(), n, x[0].data_ptr(), x[1].data_ptr(),
+                         x[2].data_ptr(), x[4].data_ptr(), pb.data_ptr(), pt_q.data_ptr(),
+                         pt_c.data_ptr(), mode.data_ptr(), n, ncol, NLEV, dt,
+                         stream=stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        f()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    k = max(2, min(args.steps, 5))
+    e0.record(stream)
+    for _ in range(k):
+        f()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / k
+    if ws > 1:
+        tt = torch.tensor([ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    ctx.close()
+    return {"value": ws * n / (ms * 1e-3), "unit": "cells/s", "ms_per_step": ms,
+            "vs_step_slab": step_ms / ms,
+            "layout": "mam4::TracersView (tracer, column, level), E3SM state_q order"}
+
+
 def adjoint_leg(native, torch, dev, stream, args, ws):
     """Adjoint configuration: 16,384 columns x 72 levels (c5). Forward and
     adjoint (mam4b_adjoint_slab) timed with CUDA events on the same inputs;
@@ -571,6 +619,8 @@ def main():
     processes = None
     if not args.no_processes:
         processes = processes_leg(native, torch, dev, stream, args, ws, peak)
+        processes["tracers"] = tracers_leg(native, torch, dev, stream, args, ws, x, pb, ncol,
+                                           dt, ms_per_step)
     fpeaks = _fp_peaks()
     flops_cell, special_cell = _flops_per_cell(WORKLOAD)
     roof64 = None

@@ -263,6 +263,39 @@ mam4b_status mam4b_adjoint_slab(mam4b_ctx *ctx, const double *in_slab, const dou
                                 int nlev, double dt, void *stream);
 
 /*
+ * Step on tracer arrays (E3SM state_q tracer order, the layout of
+ * mam4::TracersView, src/mam4xx/mam4_types.hpp:46-50: tracer, column,
+ * level). For hosts that keep their aerosol state as tracer arrays rather
+ * than per-species views: the step reads and writes them in place through
+ * its field table, with no repacking pass (the mmr -> vmr conversion of
+ * utils.hpp:112-360 / conversions.hpp:56-75 is done inside the kernels).
+ *
+ *   q, qqcw        interstitial and cloud-borne tracers [kg/kg, #/kg]:
+ *                  tracer t of cell c at q[t*tracer_stride + c], c = col*nlev
+ *                  + lev; the order of extract_stateq_from_prognostics
+ *                  (utils.hpp:205-259): 0 qv, 1 qc, 2 qi, 3 nc, 4 ni, 9..14
+ *                  O3 H2O2 H2SO4 SO2 DMS SOAG, 15..39 the 25 aerosol
+ *                  populations of the input table above. Read: q rows 0, 11,
+ *                  14, 15..39 and qqcw rows 15..39.
+ *   temperature, pressure, height, cloud_fraction  one value per cell
+ *   pblh           one value per column
+ *   ptend_q, ptend_qqcw  tendencies in the same tracer layout and stride:
+ *                  rows 11, 14, 15..39 of ptend_q and 15..39 of ptend_qqcw
+ *                  are written, every other row is left as it is.
+ *   mode_out       16 rows of mode_stride doubles: dry diameter, wet
+ *                  diameter, wet density, aerosol water of the 4 modes.
+ * Same kernels and results as mam4b_step. Asynchronous on `stream`.
+ */
+#define MAM4B_TRACER_COUNT 40
+mam4b_status mam4b_step_tracers(mam4b_ctx *ctx, const double *q, const double *qqcw,
+                                size_t tracer_stride, const double *temperature,
+                                const double *pressure, const double *height,
+                                const double *cloud_fraction, const double *pblh,
+                                double *ptend_q, double *ptend_qqcw, double *mode_out,
+                                size_t mode_stride, int ncol, int nlev, double dt,
+                                int precision, void *stream);
+
+/*
  * Per-process entries: the batched form of two mam4xx AeroProcess
  * implementations, for host models that call the processes one at a time
  * instead of the whole step. Their state is Prognostics-style: one device

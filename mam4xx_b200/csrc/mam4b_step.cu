@@ -2493,6 +2493,46 @@ mam4b_status mam4b_adjoint_slab(mam4b_ctx *ctx, const double *in_slab, const dou
   return MAM4B_OK;
 }
 
+// The step on mam4::TracersView-layout arrays (state_q tracer order,
+// utils.hpp:205-259): a field table into the caller's rows, then the step.
+mam4b_status mam4b_step_tracers(mam4b_ctx *ctx, const double *q, const double *qqcw,
+                                size_t tracer_stride, const double *temperature,
+                                const double *pressure, const double *height,
+                                const double *cloud_fraction, const double *pblh,
+                                double *ptend_q, double *ptend_qqcw, double *mode_out,
+                                size_t mode_stride, int ncol, int nlev, double dt,
+                                int precision, void *stream) {
+  const size_t n = (size_t)(ncol > 0 ? ncol : 0) * (size_t)(nlev > 0 ? nlev : 0);
+  if (!ctx || !q || !qqcw || !temperature || !pressure || !height || !cloud_fraction || !pblh ||
+      !ptend_q || !ptend_qqcw || !mode_out || ncol < 0 || nlev <= 0 || tracer_stride < n ||
+      mode_stride < n)
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_step_tracers", cudaSuccess);
+  constexpr int kQv = 0, kH2so4 = 11, kSoag = 14, kAero = 15;
+  mam4b_state_view iv;
+  mam4b_tend_view ov;
+  memset(&iv, 0, sizeof(iv));
+  memset(&ov, 0, sizeof(ov));
+  iv.field[MAM4B_IN_T] = temperature;
+  iv.field[MAM4B_IN_P] = pressure;
+  iv.field[MAM4B_IN_ZM] = height;
+  iv.field[MAM4B_IN_QV] = q + (size_t)kQv * tracer_stride;
+  iv.field[MAM4B_IN_CLD] = cloud_fraction;
+  iv.field[MAM4B_IN_H2SO4] = q + (size_t)kH2so4 * tracer_stride;
+  iv.field[MAM4B_IN_SOAG] = q + (size_t)kSoag * tracer_stride;
+  ov.field[MAM4B_OUT_TEND + 0] = ptend_q + (size_t)kH2so4 * tracer_stride;
+  ov.field[MAM4B_OUT_TEND + 1] = ptend_q + (size_t)kSoag * tracer_stride;
+  for (int p = 0; p < MAM4B_NUM_POPS; ++p) {
+    iv.field[MAM4B_IN_AER_I + p] = q + (size_t)(kAero + p) * tracer_stride;
+    iv.field[MAM4B_IN_AER_C + p] = qqcw + (size_t)(kAero + p) * tracer_stride;
+    ov.field[MAM4B_OUT_TEND + 2 + p] = ptend_q + (size_t)(kAero + p) * tracer_stride;
+    ov.field[MAM4B_OUT_TEND + 27 + p] = ptend_qqcw + (size_t)(kAero + p) * tracer_stride;
+  }
+  for (int k = 0; k < 16; ++k)
+    ov.field[MAM4B_OUT_DGN_A + k] = mode_out + (size_t)k * mode_stride;
+  iv.pblh = pblh;
+  return mam4b_step(ctx, &iv, &ov, ncol, nlev, dt, precision, stream);
+}
+
 static bool copy_prog_fields(const mam4b_prog_fields *f, ProgFields &o) {
   if (!f)
     return false;

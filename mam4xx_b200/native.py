@@ -99,6 +99,8 @@ def lib():
         L.mam4b_step_slab_noalloc.restype = I
         L.mam4b_adjoint_slab.argtypes = [P, P, P, P, P, S, I, I, D, P]
         L.mam4b_adjoint_slab.restype = I
+        L.mam4b_step_tracers.argtypes = [P, P, P, S, P, P, P, P, P, P, P, P, S, I, I, D, I, P]
+        L.mam4b_step_tracers.restype = I
         PF = ctypes.POINTER(ProgFields)
         P4 = ctypes.c_void_p * NUM_MODES
         L.mam4b_calcsize_process.argtypes = [P, ctypes.POINTER(CalcSizeConfig), PF, PF,
@@ -116,7 +118,8 @@ def lib():
 EXPORTED = ["mam4b_abi_version", "mam4b_default_config", "mam4b_create", "mam4b_destroy",
             "mam4b_step", "mam4b_step_slab", "mam4b_step_host", "mam4b_last_status",
             "mam4b_last_error", "mam4b_launch_count", "mam4b_step_slab_noalloc",
-            "mam4b_adjoint_slab", "mam4b_calcsize_process", "mam4b_coagulation_process"]
+            "mam4b_adjoint_slab", "mam4b_calcsize_process", "mam4b_coagulation_process",
+            "mam4b_step_tracers"]
 
 
 def default_config(**overrides):
@@ -195,6 +198,18 @@ class Context:
                                           int(ld), int(ncol), int(nlev), float(dt),
                                           ctypes.c_void_p(stream))
         self._check(st, "mam4b_adjoint_slab")
+
+    def step_tracers(self, q, qqcw, tracer_stride, temperature, pressure, height,
+                     cloud_fraction, pblh, ptend_q, ptend_qqcw, mode_out, mode_stride, ncol,
+                     nlev, dt, precision=FP64, stream=0):
+        """The step on tracer-layout arrays (mam4b_step_tracers); device
+        pointers."""
+        st = self._lib.mam4b_step_tracers(self._h, q, qqcw, int(tracer_stride), temperature,
+                                          pressure, height, cloud_fraction, pblh, ptend_q,
+                                          ptend_qqcw, mode_out, int(mode_stride), int(ncol),
+                                          int(nlev), float(dt), int(precision),
+                                          ctypes.c_void_p(stream))
+        self._check(st, "mam4b_step_tracers")
 
     def calcsize_process(self, progs, tends, dgncur_i, dgncur_c, ncol, nlev, dt,
                          do_aitacc_transfer=True, do_adjust=True, stream=0):
