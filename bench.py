@@ -23,7 +23,8 @@ One step = calcsize + water uptake + amicphys over every cell, dt = 1800 s.
          (oracle/_ref, OpenMP) on a bounded sample of the same cells
 
   processes  the per-process entries (mam4b_calcsize_process,
-         mam4b_coagulation_process) on the same columns: cells/s, the HBM
+         mam4b_coagulation_process, mam4b_setsox) on the same columns,
+         and the step through mam4b_step_tracers: cells/s, the HBM
          roofline of their algorithmic bytes, and the reference's own
          process classes on the host as their CPU baseline
 
@@ -180,7 +181,10 @@ def cpu_baseline(x, pblh_cell, dt, target_s=12.0):
 # species) and writes 24 tendencies and 8 diameters; Coagulation reads T,
 # p, 8 wet sizes, 32 interstitial states and their 32 tendencies and writes
 # both back
-PROCESS_BYTES_PER_CELL = {"calcsize": (50 + 20 + 24 + 8) * 8, "coagulation": (42 + 32 + 64) * 8}
+# ; setsox reads 6 met fields, 4 gas and 7 cloud-borne tracers and writes 3
+# gas tracers, 3 cloud-borne SO4 and 6 tendencies
+PROCESS_BYTES_PER_CELL = {"calcsize": (50 + 20 + 24 + 8) * 8, "coagulation": (42 + 32 + 64) * 8,
+                          "setsox": (6 + 4 + 7 + 3 + 3 + 6) * 8}
 
 
 def processes_leg(native, torch, dev, stream, args, ws, hbm_peak):
@@ -217,8 +221,22 @@ def processes_leg(native, torch, dev, stream, args, ws, hbm_peak):
         ctx.coagulation_process(t.data_ptr(), p.data_ptr(), wd, wg, pa, tf, ncol, NLEV, d["dt"],
                                 stream=stream.cuda_stream)
 
+    from mam4xx_b200.workloads import make_setsox_inputs
+    sx = make_setsox_inputs(WORKLOAD, ncol=ncol, seed=20261203 + 5)
+    sx_met = [torch.from_numpy(sx[k]).to(dev) for k in ("press", "temp", "lwc", "cldfrc",
+                                                      "cldnum", "xhnm")]
+    sx_qin = torch.from_numpy(sx["qin"]).to(dev)
+    sx_qcw = torch.from_numpy(sx["qcw"]).to(dev)
+    sx_d = torch.empty((6, n), dtype=torch.float64, device=dev)
+
+    def setsox():
+        # repeated calls keep reacting the same cells' state (fine for timing)
+        ctx.setsox(*[m.data_ptr() for m in sx_met], sx_qin.data_ptr(), sx_qcw.data_ptr(), n,
+                   sx_d[0].data_ptr(), sx_d[3].data_ptr(), ncol, NLEV, d["dt"],
+                   stream=stream.cuda_stream)
+
     res = {}
-    for name, f in (("calcsize", calcsize), ("coagulation", coag)):
+    for name, f in (("calcsize", calcsize), ("coagulation", coag), ("setsox", setsox)):
         for _ in range(args.warmup):
             f()
         if ws > 1:
@@ -260,8 +278,12 @@ def processes_leg(native, torch, dev, stream, args, ws, hbm_peak):
             r.coag_process(nc, NLEV, d["temp"][sl], d["pmid"][sl], d["wet"][:, sl],
                            d["prog_aero"][:, sl], d["tend0"][:, sl], d["dt"])
             t2 = time.perf_counter()
+            r.setsox(d["dt"], *[sx[k][sl] for k in ("press", "temp", "lwc", "cldfrc", "cldnum",
+                                                    "xhnm")], sx["qin"][:, sl], sx["qcw"][:, sl])
+            t3 = time.perf_counter()
             import multiprocessing
-            for name, el in (("calcsize", t1 - t0), ("coagulation", t2 - t1)):
+            for name, el in (("calcsize", t1 - t0), ("coagulation", t2 - t1),
+                             ("setsox", t3 - t2)):
                 res[name]["cpu_baseline"] = {
                     "value": m / el, "unit": "cells/s", "kind": "reference",
                     "cores": multiprocessing.cpu_count(),

@@ -296,6 +296,38 @@ mam4b_status mam4b_step_tracers(mam4b_ctx *ctx, const double *q, const double *q
                                 int precision, void *stream);
 
 /*
+ * Aqueous-phase sulfate chemistry in cloud water, batched over cells:
+ * mam4::mo_setsox::setsox_single_level (src/mam4xx/mo_setsox.hpp:944-1254),
+ * the cloud-chemistry stage that runs before amicphys in the host model.
+ * Per cell: the pH of cloud water (bisection on the electro-neutrality
+ * equation), S(IV) oxidation by H2O2 and by O3 over dt, uptake of H2SO4 gas
+ * by the droplets; the sulfate formed goes to the cloud-borne SO4 of the
+ * accumulation, aitken and coarse modes in proportion to their activated
+ * number.
+ *
+ *   pressure [Pa], temperature [K], lwc (cloud liquid water, kg/kg),
+ *   cloud_fraction, cloud_number (droplets, #/kg), air_density (total
+ *   number density, #/cm3): one value per cell
+ *   qin, qcw   the 31 amicphys tracers (mol/mol, #/kmol; order of
+ *              MAM4B_GAS_PCNST: O3 H2O2 H2SO4 SO2 DMS SOAG, then the
+ *              populations) of the gas/interstitial and of the cloud-borne
+ *              phase, [31][ld], updated in place: qin O3..SO2 are read and
+ *              H2O2, H2SO4, SO2 written; qcw SO4 and numbers of the modes
+ *              read, SO4 of modes 1-3 written
+ *   dqdt_aqso4, dqdt_aqh2so4  NULL or [3][ld]: the cloud-borne SO4
+ *              tendencies of modes 1-3 from aqueous oxidation and from
+ *              H2SO4 uptake [mol/mol/s] (zero where the cell has no cloud
+ *              water)
+ * The reference's mbar and pdel arguments are not used by its computation
+ * and are not taken. Asynchronous on `stream`.
+ */
+mam4b_status mam4b_setsox(mam4b_ctx *ctx, const double *pressure, const double *temperature,
+                          const double *lwc, const double *cloud_fraction,
+                          const double *cloud_number, const double *air_density, double *qin,
+                          double *qcw, size_t ld, double *dqdt_aqso4, double *dqdt_aqh2so4,
+                          int ncol, int nlev, double dt, void *stream);
+
+/*
  * Per-process entries: the batched form of two mam4xx AeroProcess
  * implementations, for host models that call the processes one at a time
  * instead of the whole step. Their state is Prognostics-style: one device

@@ -23,6 +23,7 @@
 #include "mam4b_physics_mixed.cuh"
 #include "mam4b_adjoint.cuh"
 #include "mam4b_process.cuh"
+#include "mam4b_setsox.cuh"
 
 namespace mam4b {
 
@@ -1046,7 +1047,9 @@ __global__ void __launch_bounds__(128) pre_kernel(const __grid_constant__ StepAr
     cell_pre(a, c);
 }
 
-__global__ void __launch_bounds__(128) post_kernel(const __grid_constant__ StepArgs a) {
+// 4 blocks of 128 per SM (128 registers, a few hundred bytes spilled to
+// L1): 2 % faster than the unconstrained 231-register build.
+__global__ void __launch_bounds__(128, 4) post_kernel(const __grid_constant__ StepArgs a) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < (long long)a.counters[CNT_QUEUED])
     cell_post(a, (unsigned)i);
@@ -1720,6 +1723,45 @@ __global__ void __launch_bounds__(128) coag_process_kernel(const __grid_constant
   const CoagTables T = {kCoagBm0ij, kCoagBm3i, kCoagBm0};
   if (c < a.ncell)
     coag_process_cell(c_k, T, a, c);
+}
+
+// ---- aqueous sulfate chemistry (setsox), one thread per cell
+struct SetsoxArgs {
+  const double *press, *temp, *lwc, *cldfrc, *cldnum, *xhnm;
+  double *qin, *qcw;  // [31][ld]
+  double *dso4, *dh2so4;  // [3][ld] or null
+  size_t ld;
+  long long ncell;
+  double dt;
+};
+
+__global__ void __launch_bounds__(128) setsox_kernel(const __grid_constant__ SetsoxArgs a) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncell)
+    return;
+  constexpr int kIn[4] = {0, 1, 2, 3};
+  constexpr int kCw[7] = {6, 13, 14, 18, 21, 26, 30};
+  double qin[31], qcw[31];
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    qin[kIn[k]] = a.qin[(size_t)kIn[k] * a.ld + c];
+#pragma unroll
+  for (int k = 0; k < 7; ++k)
+    qcw[kCw[k]] = a.qcw[(size_t)kCw[k] * a.ld + c];
+  double dso4[3], dh2so4[3];
+  sox::setsox_cell(a.dt, a.press[c], a.temp[c], a.lwc[c], a.cldfrc[c], a.cldnum[c], a.xhnm[c],
+                   qin, qcw, dso4, dh2so4);
+#pragma unroll
+  for (int k = 1; k < 4; ++k)
+    a.qin[(size_t)k * a.ld + c] = qin[k];
+#pragma unroll
+  for (int m = 0; m < 3; ++m) {
+    a.qcw[(size_t)sox::so4_cw(m) * a.ld + c] = qcw[sox::so4_cw(m)];
+    if (a.dso4)
+      a.dso4[(size_t)m * a.ld + c] = dso4[m];
+    if (a.dh2so4)
+      a.dh2so4[(size_t)m * a.ld + c] = dh2so4[m];
+  }
 }
 
 }  // namespace mam4b
@@ -2531,6 +2573,45 @@ mam4b_status mam4b_step_tracers(mam4b_ctx *ctx, const double *q, const double *q
     ov.field[MAM4B_OUT_DGN_A + k] = mode_out + (size_t)k * mode_stride;
   iv.pblh = pblh;
   return mam4b_step(ctx, &iv, &ov, ncol, nlev, dt, precision, stream);
+}
+
+// mo_setsox::setsox_single_level (mo_setsox.hpp:944-1254), batched
+mam4b_status mam4b_setsox(mam4b_ctx *ctx, const double *pressure, const double *temperature,
+                          const double *lwc, const double *cloud_fraction,
+                          const double *cloud_number, const double *air_density, double *qin,
+                          double *qcw, size_t ld, double *dqdt_aqso4, double *dqdt_aqh2so4,
+                          int ncol, int nlev, double dt, void *stream) {
+  const char *what = "mam4b_setsox";
+  const size_t n = (size_t)(ncol > 0 ? ncol : 0) * (size_t)(nlev > 0 ? nlev : 0);
+  if (!ctx || !pressure || !temperature || !lwc || !cloud_fraction || !cloud_number ||
+      !air_density || !qin || !qcw || ncol < 0 || nlev <= 0 || ld < n || !(dt > 0.0) ||
+      !isfinite(dt))
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, what, cudaSuccess);
+  SetsoxArgs a;
+  a.press = pressure;
+  a.temp = temperature;
+  a.lwc = lwc;
+  a.cldfrc = cloud_fraction;
+  a.cldnum = cloud_number;
+  a.xhnm = air_density;
+  a.qin = qin;
+  a.qcw = qcw;
+  a.dso4 = dqdt_aqso4;
+  a.dh2so4 = dqdt_aqh2so4;
+  a.ld = ld;
+  a.ncell = (long long)n;
+  a.dt = dt;
+  cudaStream_t s = (cudaStream_t)stream;
+  ctx->last_stream = s;
+  if (n == 0)
+    return MAM4B_OK;
+  const int block = 128;
+  setsox_kernel<<<(unsigned)((n + block - 1) / block), block, 0, s>>>(a);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, what, e);
+  ctx->launches += 1;
+  return MAM4B_OK;
 }
 
 static bool copy_prog_fields(const mam4b_prog_fields *f, ProgFields &o) {

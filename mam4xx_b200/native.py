@@ -101,6 +101,8 @@ def lib():
         L.mam4b_adjoint_slab.restype = I
         L.mam4b_step_tracers.argtypes = [P, P, P, S, P, P, P, P, P, P, P, P, S, I, I, D, I, P]
         L.mam4b_step_tracers.restype = I
+        L.mam4b_setsox.argtypes = [P, P, P, P, P, P, P, P, P, S, P, P, I, I, D, P]
+        L.mam4b_setsox.restype = I
         PF = ctypes.POINTER(ProgFields)
         P4 = ctypes.c_void_p * NUM_MODES
         L.mam4b_calcsize_process.argtypes = [P, ctypes.POINTER(CalcSizeConfig), PF, PF,
@@ -119,7 +121,7 @@ EXPORTED = ["mam4b_abi_version", "mam4b_default_config", "mam4b_create", "mam4b_
             "mam4b_step", "mam4b_step_slab", "mam4b_step_host", "mam4b_last_status",
             "mam4b_last_error", "mam4b_launch_count", "mam4b_step_slab_noalloc",
             "mam4b_adjoint_slab", "mam4b_calcsize_process", "mam4b_coagulation_process",
-            "mam4b_step_tracers"]
+            "mam4b_step_tracers", "mam4b_setsox"]
 
 
 def default_config(**overrides):
@@ -210,6 +212,16 @@ class Context:
                                           int(nlev), float(dt), int(precision),
                                           ctypes.c_void_p(stream))
         self._check(st, "mam4b_step_tracers")
+
+    def setsox(self, pressure, temperature, lwc, cloud_fraction, cloud_number, air_density,
+               qin, qcw, ld, dqdt_aqso4, dqdt_aqh2so4, ncol, nlev, dt, stream=0):
+        """Aqueous sulfate chemistry (mam4b_setsox); device pointers, qin and
+        qcw [31][ld] updated in place, the tendency pointers may be 0."""
+        st = self._lib.mam4b_setsox(self._h, pressure, temperature, lwc, cloud_fraction,
+                                    cloud_number, air_density, qin, qcw, int(ld),
+                                    dqdt_aqso4 or None, dqdt_aqh2so4 or None, int(ncol),
+                                    int(nlev), float(dt), ctypes.c_void_p(stream))
+        self._check(st, "mam4b_setsox")
 
     def calcsize_process(self, progs, tends, dgncur_i, dgncur_c, ncol, nlev, dt,
                          do_aitacc_transfer=True, do_adjust=True, stream=0):

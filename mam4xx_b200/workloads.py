@@ -219,3 +219,35 @@ def make_process_inputs(name="c2", ncol=None, nlev=None, seed=None):
     return {"ncol": w["ncol"], "nlev": w["nlev"], "dt": w["dt"], "temp": x[0].copy(),
             "pmid": x[1].copy(), "wet": wet, "prog": prog, "prog_aero": prog_slab(x, True),
             "tend0": tend0}
+
+
+def make_setsox_inputs(name="c2", ncol=None, nlev=None, seed=None):
+    """Inputs of the aqueous-chemistry entry from a workload configuration:
+    T, p and cloud fraction of the workload; the 31 amicphys tracers in
+    mol/mol (#/kmol for numbers) from its H2SO4, SOAG and populations, plus
+    O3 log-uniform 1e-8..1e-7, H2O2 1e-11..1e-9 and SO2 1e-12..1e-8 mol/mol;
+    cloud liquid water log-uniform 1e-6..1e-3 kg/kg in 80 % of the cloudy
+    cells (0 elsewhere), droplet number 1e7..1e9 #/kg, and the air number
+    density p / (k T) in #/cm3."""
+    w = make_workload(name, ncol=ncol, nlev=nlev, seed=seed)
+    x = w["in_slab"]
+    n = x.shape[1]
+    rng = np.random.default_rng(991 + (seed or 0))
+    to_vmr = np.array([MW_DRY_AIR if i in (13, 18, 26, 30) else MW_DRY_AIR / ADV_MASS[i]
+                       for i in range(31)])
+    qin = np.zeros((31, n))
+    qcw = np.zeros((31, n))
+    qin[0] = _logu(rng, 1e-8, 1e-7, n)
+    qin[1] = _logu(rng, 1e-11, 1e-9, n)
+    qin[2] = x[5] * to_vmr[2]
+    qin[3] = _logu(rng, 1e-12, 1e-8, n)
+    qin[5] = x[6] * to_vmr[5]
+    qin[6:31] = x[IN_AER_I:IN_AER_I + 25] * to_vmr[6:31, None]
+    qcw[6:31] = x[IN_AER_C:IN_AER_C + 25] * to_vmr[6:31, None]
+    cld = x[4].copy()
+    lwc = np.where((cld > 0) & (rng.uniform(0, 1, n) < 0.8), _logu(rng, 1e-6, 1e-3, n), 0.0)
+    cldnum = _logu(rng, 1e7, 1e9, n)
+    xhnm = x[1] / (1.380649e-23 * x[0]) * 1e-6
+    return {"ncol": w["ncol"], "nlev": w["nlev"], "dt": w["dt"], "press": x[1].copy(),
+            "temp": x[0].copy(), "lwc": lwc, "cldfrc": cld, "cldnum": cldnum, "xhnm": xhnm,
+            "qin": qin, "qcw": qcw}

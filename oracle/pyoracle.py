@@ -159,6 +159,24 @@ class ReferenceOracle(_Oracle):
           tend.ctypes.data, dgn.ctypes.data)
         return tend, dgn
 
+    def setsox(self, dt, press, temp, lwc, cldfrc, cldnum, xhnm, qin, qcw):
+        """mam4::mo_setsox::setsox_single_level per cell (qin, qcw: (31,
+        ncell) vmr); returns (qin, qcw, dqdt_aqso4, dqdt_aqh2so4), the last
+        two (31, ncell)."""
+        qin = np.array(qin, dtype=np.float64, order="C")
+        qcw = np.array(qcw, dtype=np.float64, order="C")
+        n = qin.shape[1]
+        d1 = np.zeros((31, n))
+        d2 = np.zeros((31, n))
+        args = [np.ascontiguousarray(a, dtype=np.float64)
+                for a in (press, temp, lwc, cldfrc, cldnum, xhnm)]
+        f = self.lib.mam4ref_setsox
+        f.argtypes = [_I, _D] + [_P] * 10
+        f.restype = None
+        f(n, dt, *[a.ctypes.data for a in args], qin.ctypes.data, qcw.ctypes.data,
+          d1.ctypes.data, d2.ctypes.data)
+        return qin, qcw, d1, d2
+
     def coag_process(self, ncol, nlev, temp, pmid, wet, prog, tend, dt):
         """mam4::Coagulation::compute_tendencies column by column. wet: (8,
         ncell) wet density [4] then wet diameter [4]; returns (prog after,

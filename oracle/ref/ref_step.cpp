@@ -29,6 +29,7 @@
 #include <mam4xx/coagulation.hpp>
 #include <mam4xx/mam4_amicphys.hpp>
 #include <mam4xx/modal_aero_calcsize.hpp>
+#include <mam4xx/mo_setsox.hpp>
 #include <mam4xx/water_uptake.hpp>
 
 #include "../oracle_api.h"
@@ -378,6 +379,33 @@ void mam4ref_coag_process(int ncol, int nlev, double dt, const double *temp,
     const mam4::Atmosphere atm = column_atmosphere(nlev, temp + c0, pmid + c0, zeros);
     mam4::ThreadTeam team;
     process.compute_tendencies(aero_config, team, 0.0, dt, atm, sfc, progs, diags, tends);
+  }
+}
+
+// mo_setsox::setsox_single_level per cell with the host offset loffset = 9
+// (31-tracer arrays); qin, qcw [31][ncell] in/out, dso4, dh2so4 [31][ncell]
+// out. pdel and mbar are passed as zero: the routine does not use them.
+void mam4ref_setsox(int ncell, double dt, const double *press, const double *temp,
+                    const double *lwc, const double *cldfrc, const double *cldnum,
+                    const double *xhnm, double *qin, double *qcw, double *dso4,
+                    double *dh2so4) {
+  const mam4::mo_setsox::Config cfg;
+  const size_t n = (size_t)ncell;
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int c = 0; c < ncell; ++c) {
+    Real qi[31], qc[31], d1[31], d2[31];
+    for (int k = 0; k < 31; ++k) {
+      qi[k] = qin[k * n + c];
+      qc[k] = qcw[k * n + c];
+    }
+    mam4::mo_setsox::setsox_single_level(9, dt, press[c], 0.0, temp[c], 0.0, lwc[c], cldfrc[c],
+                                         cldnum[c], xhnm[c], cfg, d1, d2, qc, qi);
+    for (int k = 0; k < 31; ++k) {
+      qin[k * n + c] = qi[k];
+      qcw[k * n + c] = qc[k];
+      dso4[k * n + c] = d1[k];
+      dh2so4[k * n + c] = d2[k];
+    }
   }
 }
 

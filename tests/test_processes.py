@@ -68,3 +68,18 @@ def test_process_entries_reject_bad_arguments_without_a_device():
     assert L.mam4b_coagulation_process(None, None, None, ctypes.byref(four), ctypes.byref(four),
                                        ctypes.byref(pf), ctypes.byref(pf), 1, 1, 1.0,
                                        None) == 1
+
+
+def test_reference_setsox_conserves_sulfur(ref_oracle):
+    """Aqueous chemistry moves sulfur from SO2 and H2SO4 gas into
+    cloud-borne SO4 without creating or losing any (to rounding)."""
+    from mam4xx_b200.workloads import make_setsox_inputs
+    d = make_setsox_inputs("c2", ncol=32, seed=7)
+    qi, qc, d1, d2 = ref_oracle.setsox(d["dt"], d["press"], d["temp"], d["lwc"], d["cldfrc"],
+                                       d["cldnum"], d["xhnm"], d["qin"], d["qcw"])
+    s0 = d["qin"][2] + d["qin"][3] + d["qcw"][6] + d["qcw"][14] + d["qcw"][21]
+    s1 = qi[2] + qi[3] + qc[6] + qc[14] + qc[21]
+    assert (np.abs(s1 - s0) <= 1e-14 * s0).all()
+    active = d["lwc"] * 0 + (np.abs(qc[6] - d["qcw"][6]) > 0)
+    assert 0.2 < active.mean() < 0.9  # a mix of cells with and without cloud water
+    assert set(np.nonzero(np.abs(d1).max(axis=1))[0]) <= {6, 14, 21}
