@@ -23,7 +23,8 @@ One step = calcsize + water uptake + amicphys over every cell, dt = 1800 s.
          (oracle/_ref, OpenMP) on a bounded sample of the same cells
 
   processes  the per-process entries (mam4b_calcsize_process,
-         mam4b_coagulation_process, mam4b_setsox) on the same columns,
+         mam4b_coagulation_process, mam4b_setsox, mam4b_activate) on the
+         same columns,
          and the step through mam4b_step_tracers: cells/s, the HBM
          roofline of their algorithmic bytes, and the reference's own
          process classes on the host as their CPU baseline
@@ -184,7 +185,8 @@ def cpu_baseline(x, pblh_cell, dt, target_s=12.0):
 # ; setsox reads 6 met fields, 4 gas and 7 cloud-borne tracers and writes 3
 # gas tracers, 3 cloud-borne SO4 and 6 tendencies
 PROCESS_BYTES_PER_CELL = {"calcsize": (50 + 20 + 24 + 8) * 8, "coagulation": (42 + 32 + 64) * 8,
-                          "setsox": (6 + 4 + 7 + 3 + 3 + 6) * 8}
+                          "setsox": (6 + 4 + 7 + 3 + 3 + 6) * 8,
+                          "activation": (28 + 17) * 8}
 
 
 def processes_leg(native, torch, dev, stream, args, ws, hbm_peak):
@@ -235,8 +237,20 @@ def processes_leg(native, torch, dev, stream, args, ws, hbm_peak):
                    sx_d[0].data_ptr(), sx_d[3].data_ptr(), ncol, NLEV, d["dt"],
                    stream=stream.cuda_stream)
 
+    from mam4xx_b200.workloads import make_activation_inputs
+    ac = make_activation_inputs(WORKLOAD, ncol=ncol, seed=20261203 + 6)
+    ac_x = torch.from_numpy(ac["in_slab"]).to(dev)
+    ac_rho = torch.from_numpy(ac["rho"]).to(dev)
+    ac_w = torch.from_numpy(ac["w"]).to(dev)
+    ac_out = torch.empty((17, n), dtype=torch.float64, device=dev)
+
+    def activation():
+        ctx.activate(ac_x.data_ptr(), n, ac_rho.data_ptr(), ac_w.data_ptr(), ac_out.data_ptr(),
+                     ncol, NLEV, stream=stream.cuda_stream)
+
     res = {}
-    for name, f in (("calcsize", calcsize), ("coagulation", coag), ("setsox", setsox)):
+    for name, f in (("calcsize", calcsize), ("coagulation", coag), ("setsox", setsox),
+                    ("activation", activation)):
         for _ in range(args.warmup):
             f()
         if ws > 1:
@@ -281,9 +295,11 @@ def processes_leg(native, torch, dev, stream, args, ws, hbm_peak):
             r.setsox(d["dt"], *[sx[k][sl] for k in ("press", "temp", "lwc", "cldfrc", "cldnum",
                                                     "xhnm")], sx["qin"][:, sl], sx["qcw"][:, sl])
             t3 = time.perf_counter()
+            r.activate(ac["in_slab"][:, sl], ac["rho"][sl], ac["w"][sl])
+            t4 = time.perf_counter()
             import multiprocessing
             for name, el in (("calcsize", t1 - t0), ("coagulation", t2 - t1),
-                             ("setsox", t3 - t2)):
+                             ("setsox", t3 - t2), ("activation", t4 - t3)):
                 res[name]["cpu_baseline"] = {
                     "value": m / el, "unit": "cells/s", "kind": "reference",
                     "cores": multiprocessing.cpu_count(),

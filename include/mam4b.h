@@ -296,6 +296,29 @@ mam4b_status mam4b_step_tracers(mam4b_ctx *ctx, const double *q, const double *q
                                 int precision, void *stream);
 
 /*
+ * Aerosol activation, batched over cells: the per-cell part of mam4xx's
+ * droplet nucleation, get_activate_frac (src/mam4xx/ndrop.hpp:699-765):
+ * number, volume and hygroscopicity of the 4 interstitial modes (loadaer),
+ * then the Abdul-Razzak & Ghan activated fractions for the updraft
+ * (activate_modal with maxsat, maximum updraft 10 m/s). A consumer of the
+ * aerosol state the step produces.
+ *
+ *   in_slab     the step's input layout (MAM4B_NIN fields of ld doubles);
+ *               reads temperature and the 25 interstitial populations
+ *   air_density [kg/m3] and updraft (subgrid vertical velocity, m/s), one
+ *               per cell; the aerosol is loaded at the same level
+ *   out         17 fields of ld doubles: activated number fraction of the 4
+ *               modes, activated mass fraction, their fluxes (fraction x
+ *               updraft, m/s), and the flux at full activation; all zero
+ *               where there is no accumulation-mode aerosol or no updraft
+ * Mode number bounds of loadaer: the modes' nominal volume-to-number
+ * ratios at their maximum and minimum diameters. Asynchronous on `stream`.
+ */
+mam4b_status mam4b_activate(mam4b_ctx *ctx, const double *in_slab, size_t ld,
+                            const double *air_density, const double *updraft, double *out,
+                            int ncol, int nlev, void *stream);
+
+/*
  * Aqueous-phase sulfate chemistry in cloud water, batched over cells:
  * mam4::mo_setsox::setsox_single_level (src/mam4xx/mo_setsox.hpp:944-1254),
  * the cloud-chemistry stage that runs before amicphys in the host model.

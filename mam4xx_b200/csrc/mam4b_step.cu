@@ -24,6 +24,7 @@
 #include "mam4b_adjoint.cuh"
 #include "mam4b_process.cuh"
 #include "mam4b_setsox.cuh"
+#include "mam4b_activation.cuh"
 
 namespace mam4b {
 
@@ -1764,6 +1765,29 @@ __global__ void __launch_bounds__(128) setsox_kernel(const __grid_constant__ Set
   }
 }
 
+// ---- aerosol activation (ndrop get_activate_frac), one thread per cell
+struct ActivateArgs {
+  const double *temp, *aer[NPOP], *rho, *w;
+  double *out;  // [17][ld]
+  size_t ld;
+  long long ncell;
+};
+
+__global__ void __launch_bounds__(128) activate_kernel(const __grid_constant__ ActivateArgs a) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncell)
+    return;
+  double ai[NPOP], out[17];
+#pragma unroll
+  for (int p = 0; p < NPOP; ++p)
+    ai[p] = __ldg(a.aer[p] + c);
+  const double rho = __ldg(a.rho + c);
+  act::activate_cell(c_k, ai, rho, rho, __ldg(a.w + c), __ldg(a.temp + c), out);
+#pragma unroll
+  for (int k = 0; k < 17; ++k)
+    a.out[(size_t)k * a.ld + c] = out[k];
+}
+
 }  // namespace mam4b
 
 // =============================================================== C ABI
@@ -2573,6 +2597,36 @@ mam4b_status mam4b_step_tracers(mam4b_ctx *ctx, const double *q, const double *q
     ov.field[MAM4B_OUT_DGN_A + k] = mode_out + (size_t)k * mode_stride;
   iv.pblh = pblh;
   return mam4b_step(ctx, &iv, &ov, ncol, nlev, dt, precision, stream);
+}
+
+// ndrop get_activate_frac (ndrop.hpp:699-765), batched
+mam4b_status mam4b_activate(mam4b_ctx *ctx, const double *in_slab, size_t ld,
+                            const double *air_density, const double *updraft, double *out,
+                            int ncol, int nlev, void *stream) {
+  const char *what = "mam4b_activate";
+  const size_t n = (size_t)(ncol > 0 ? ncol : 0) * (size_t)(nlev > 0 ? nlev : 0);
+  if (!ctx || !in_slab || !air_density || !updraft || !out || ncol < 0 || nlev <= 0 || ld < n)
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, what, cudaSuccess);
+  ActivateArgs a;
+  a.temp = in_slab + (size_t)MAM4B_IN_T * ld;
+  for (int p = 0; p < NPOP; ++p)
+    a.aer[p] = in_slab + (size_t)(MAM4B_IN_AER_I + p) * ld;
+  a.rho = air_density;
+  a.w = updraft;
+  a.out = out;
+  a.ld = ld;
+  a.ncell = (long long)n;
+  cudaStream_t s = (cudaStream_t)stream;
+  ctx->last_stream = s;
+  if (n == 0)
+    return MAM4B_OK;
+  const int block = 128;
+  activate_kernel<<<(unsigned)((n + block - 1) / block), block, 0, s>>>(a);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, what, e);
+  ctx->launches += 1;
+  return MAM4B_OK;
 }
 
 // mo_setsox::setsox_single_level (mo_setsox.hpp:944-1254), batched

@@ -101,6 +101,8 @@ def lib():
         L.mam4b_adjoint_slab.restype = I
         L.mam4b_step_tracers.argtypes = [P, P, P, S, P, P, P, P, P, P, P, P, S, I, I, D, I, P]
         L.mam4b_step_tracers.restype = I
+        L.mam4b_activate.argtypes = [P, P, S, P, P, P, I, I, P]
+        L.mam4b_activate.restype = I
         L.mam4b_setsox.argtypes = [P, P, P, P, P, P, P, P, P, S, P, P, I, I, D, P]
         L.mam4b_setsox.restype = I
         PF = ctypes.POINTER(ProgFields)
@@ -121,7 +123,7 @@ EXPORTED = ["mam4b_abi_version", "mam4b_default_config", "mam4b_create", "mam4b_
             "mam4b_step", "mam4b_step_slab", "mam4b_step_host", "mam4b_last_status",
             "mam4b_last_error", "mam4b_launch_count", "mam4b_step_slab_noalloc",
             "mam4b_adjoint_slab", "mam4b_calcsize_process", "mam4b_coagulation_process",
-            "mam4b_step_tracers", "mam4b_setsox"]
+            "mam4b_step_tracers", "mam4b_setsox", "mam4b_activate"]
 
 
 def default_config(**overrides):
@@ -212,6 +214,13 @@ class Context:
                                           int(nlev), float(dt), int(precision),
                                           ctypes.c_void_p(stream))
         self._check(st, "mam4b_step_tracers")
+
+    def activate(self, in_ptr, ld, air_density, updraft, out, ncol, nlev, stream=0):
+        """Aerosol activation fractions (mam4b_activate); device pointers,
+        out [17][ld]."""
+        st = self._lib.mam4b_activate(self._h, in_ptr, int(ld), air_density, updraft, out,
+                                      int(ncol), int(nlev), ctypes.c_void_p(stream))
+        self._check(st, "mam4b_activate")
 
     def setsox(self, pressure, temperature, lwc, cloud_fraction, cloud_number, air_density,
                qin, qcw, ld, dqdt_aqso4, dqdt_aqh2so4, ncol, nlev, dt, stream=0):

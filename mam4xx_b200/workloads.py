@@ -251,3 +251,19 @@ def make_setsox_inputs(name="c2", ncol=None, nlev=None, seed=None):
     return {"ncol": w["ncol"], "nlev": w["nlev"], "dt": w["dt"], "press": x[1].copy(),
             "temp": x[0].copy(), "lwc": lwc, "cldfrc": cld, "cldnum": cldnum, "xhnm": xhnm,
             "qin": qin, "qcw": qcw}
+
+
+def make_activation_inputs(name="c2", ncol=None, nlev=None, seed=None):
+    """Inputs of the activation entry: a workload's input slab, the air
+    density p / (R_air T) and an updraft log-uniform 0.01..3 m/s, zero or
+    negative in 10 % of the cells (no activation there)."""
+    w = make_workload(name, ncol=ncol, nlev=nlev, seed=seed)
+    x = w["in_slab"]
+    n = x.shape[1]
+    rng = np.random.default_rng(313 + (seed or 0))
+    r_air = 6.022214076e23 * 1.380649e-23 / 0.028966
+    rho = x[1] / (r_air * x[0])
+    wup = _logu(rng, 0.01, 3.0, n)
+    cut = rng.uniform(0, 1, n)
+    wup = np.where(cut < 0.05, 0.0, np.where(cut < 0.1, -wup, wup))
+    return {"ncol": w["ncol"], "nlev": w["nlev"], "in_slab": x, "rho": rho, "w": wup}

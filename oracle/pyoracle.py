@@ -159,6 +159,29 @@ class ReferenceOracle(_Oracle):
           tend.ctypes.data, dgn.ctypes.data)
         return tend, dgn
 
+    def maxsat(self, zeta, eta, smc):
+        """ndrop::maxsat for 4 modes."""
+        f = self.lib.mam4ref_maxsat
+        f.argtypes = [_D, _P, _P]
+        f.restype = _D
+        e = np.ascontiguousarray(eta, dtype=np.float64)
+        s = np.ascontiguousarray(smc, dtype=np.float64)
+        return f(zeta, e.ctypes.data, s.ctypes.data)
+
+    def activate(self, in_slab, rho, w):
+        """ndrop::get_activate_frac per cell; in_slab (NIN, ncell); returns
+        (17, ncell): fn[4], fm[4], fluxn[4], fluxm[4], flux_fullact."""
+        x = np.ascontiguousarray(in_slab, dtype=np.float64)
+        n = x.shape[1]
+        out = np.zeros((17, n))
+        r = np.ascontiguousarray(rho, dtype=np.float64)
+        ww = np.ascontiguousarray(w, dtype=np.float64)
+        f = self.lib.mam4ref_activate
+        f.argtypes = [_I, _P, _P, _P, _P]
+        f.restype = None
+        f(n, x.ctypes.data, r.ctypes.data, ww.ctypes.data, out.ctypes.data)
+        return out
+
     def setsox(self, dt, press, temp, lwc, cldfrc, cldnum, xhnm, qin, qcw):
         """mam4::mo_setsox::setsox_single_level per cell (qin, qcw: (31,
         ncell) vmr); returns (qin, qcw, dqdt_aqso4, dqdt_aqh2so4), the last

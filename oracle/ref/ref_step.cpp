@@ -30,6 +30,7 @@
 #include <mam4xx/mam4_amicphys.hpp>
 #include <mam4xx/modal_aero_calcsize.hpp>
 #include <mam4xx/mo_setsox.hpp>
+#include <mam4xx/ndrop.hpp>
 #include <mam4xx/water_uptake.hpp>
 
 #include "../oracle_api.h"
@@ -407,6 +408,52 @@ void mam4ref_setsox(int ncell, double dt, const double *press, const double *tem
       dh2so4[k * n + c] = d2[k];
     }
   }
+}
+
+// ndrop::get_activate_frac per cell on the interstitial populations of a
+// step input slab (field-major, ld = ncell), with the E3SM parameters of
+// get_e3sm_parameters and the constants of ndrop_init; the mode number
+// bounds are ndrop_init's volume-to-number ratios (at the maximum and the
+// minimum diameter). out [17][ncell]: fn[4], fm[4], fluxn[4], fluxm[4],
+// flux_fullact (zero where activate_modal returns early).
+void mam4ref_activate(int ncell, const double *in, const double *rho, const double *w,
+                      double *out) {
+  using namespace mam4::ndrop;
+  int nspec_amode[4], lspectype[maxd_aspectype][4], lmassptr[maxd_aspectype][4], numptr[4];
+  Real specdens[maxd_aspectype], spechygro[maxd_aspectype];
+  int mam_idx[4][nspec_max], mam_cnst_idx[4][nspec_max];
+  get_e3sm_parameters(nspec_amode, lspectype, lmassptr, numptr, specdens, spechygro, mam_idx,
+                      mam_cnst_idx);
+  Real exp45logsig[4], alogsig[4], aten, v2n_min[4], v2n_max[4];
+  ndrop_init(exp45logsig, alogsig, aten, v2n_min, v2n_max);
+  const size_t n = (size_t)ncell;
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int c = 0; c < ncell; ++c) {
+    Real state_q[mam4::aero_model::pcnst] = {};
+    for (int p = 0; p < 25; ++p)
+      state_q[15 + p] = in[(size_t)(MAM4B_IN_AER_I + p) * n + c];
+    Real fn[4] = {}, fm[4] = {}, fluxn[4] = {}, fluxm[4] = {}, flux_fullact = 0;
+    get_activate_frac(state_q, rho[c], rho[c], w[c], in[(size_t)MAM4B_IN_T * n + c], lspectype,
+                      specdens, spechygro, lmassptr, v2n_min, v2n_max, numptr, nspec_amode,
+                      exp45logsig, alogsig, aten, fn, fm, fluxn, fluxm, flux_fullact);
+    for (int m = 0; m < 4; ++m) {
+      out[(size_t)m * n + c] = fn[m];
+      out[(size_t)(4 + m) * n + c] = fm[m];
+      out[(size_t)(8 + m) * n + c] = fluxn[m];
+      out[(size_t)(12 + m) * n + c] = fluxm[m];
+    }
+    out[(size_t)16 * n + c] = flux_fullact;
+  }
+}
+
+double mam4ref_maxsat(double zeta, const double *eta, const double *smc) {
+  Real e[4], sm[4], smax = 0;
+  for (int m = 0; m < 4; ++m) {
+    e[m] = eta[m];
+    sm[m] = smc[m];
+  }
+  mam4::ndrop::maxsat(zeta, e, 4, sm, smax);
+  return smax;
 }
 
 long mam4ref_assert_failures(void) { return mam4shim::assert_failures(); }

@@ -83,3 +83,24 @@ def test_reference_setsox_conserves_sulfur(ref_oracle):
     active = d["lwc"] * 0 + (np.abs(qc[6] - d["qcw"][6]) > 0)
     assert 0.2 < active.mean() < 0.9  # a mix of cells with and without cloud water
     assert set(np.nonzero(np.abs(d1).max(axis=1))[0]) <= {6, 14, 21}
+
+
+def test_reference_maxsat_known_answers(ref_oracle):
+    """The maximum-supersaturation values of the reference's own unit test
+    (src/tests/mam4_ndrop_unit_tests.cpp:210-257)."""
+    assert ref_oracle.maxsat(0.0, [0.0] * 4, [1.0] * 4) == pytest.approx(1e-20, rel=1e-15)
+    assert ref_oracle.maxsat(0.0, [0.0] * 4, [0.0] * 4) == pytest.approx(1e-10, rel=1e-15)
+    assert ref_oracle.maxsat(0.0, [1.0] * 4, [1.0] * 4) == pytest.approx(0.4698982924029698,
+                                                                         rel=1e-14)
+
+
+def test_reference_activation_fractions(ref_oracle):
+    from mam4xx_b200.workloads import make_activation_inputs
+    d = make_activation_inputs("c2", ncol=16, seed=3)
+    out = ref_oracle.activate(d["in_slab"], d["rho"], d["w"])
+    fn, fm = out[0:4], out[4:8]
+    assert ((fn >= 0) & (fn <= 1) & (fm >= 0) & (fm <= 1)).all()
+    assert (fm >= fn - 1e-12).all()  # larger particles activate first
+    no_up = d["w"] <= 0
+    assert no_up.any() and (out[:, no_up] == 0).all()
+    np.testing.assert_array_equal(out[16, ~no_up], d["w"][~no_up])
