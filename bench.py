@@ -23,8 +23,8 @@ One step = calcsize + water uptake + amicphys over every cell, dt = 1800 s.
          (oracle/_ref, OpenMP) on a bounded sample of the same cells
 
   processes  the per-process entries (mam4b_calcsize_process,
-         mam4b_coagulation_process, mam4b_setsox, mam4b_activate) on the
-         same columns,
+         mam4b_coagulation_process, mam4b_setsox, mam4b_activate,
+         mam4b_optics_lw with seeded stand-in tables) on the same columns,
          and the step through mam4b_step_tracers: cells/s, the HBM
          roofline of their algorithmic bytes, and the reference's own
          process classes on the host as their CPU baseline
@@ -186,7 +186,7 @@ def cpu_baseline(x, pblh_cell, dt, target_s=12.0):
 # gas tracers, 3 cloud-borne SO4 and 6 tendencies
 PROCESS_BYTES_PER_CELL = {"calcsize": (50 + 20 + 24 + 8) * 8, "coagulation": (42 + 32 + 64) * 8,
                           "setsox": (6 + 4 + 7 + 3 + 3 + 6) * 8,
-                          "activation": (28 + 17) * 8}
+                          "activation": (28 + 17) * 8, "optics_lw": (55 + 16) * 8}
 
 
 def processes_leg(native, torch, dev, stream, args, ws, hbm_peak):
@@ -248,9 +248,21 @@ def processes_leg(native, torch, dev, stream, args, ws, hbm_peak):
         ctx.activate(ac_x.data_ptr(), n, ac_rho.data_ptr(), ac_w.data_ptr(), ac_out.data_ptr(),
                      ncol, NLEV, stream=stream.cuda_stream)
 
+    from mam4xx_b200.workloads import make_optics_lw_tables, make_workload
+    ow = make_workload(WORKLOAD, ncol=ncol, seed=20261203 + 7)
+    ox = torch.from_numpy(ow["in_slab"]).to(dev)
+    opd = torch.from_numpy(np.random.default_rng(8).uniform(100.0, 3000.0, n)).to(dev)
+    otau = torch.empty((16, n), dtype=torch.float64, device=dev)
+    otables = make_optics_lw_tables(seed=1)
+    ctx.optics_lw_set_tables(otables)
+
+    def optics_lw():
+        ctx.optics_lw(ox.data_ptr(), n, opd.data_ptr(), otau.data_ptr(), ncol, NLEV, d["dt"],
+                      stream=stream.cuda_stream)
+
     res = {}
     for name, f in (("calcsize", calcsize), ("coagulation", coag), ("setsox", setsox),
-                    ("activation", activation)):
+                    ("activation", activation), ("optics_lw", optics_lw)):
         for _ in range(args.warmup):
             f()
         if ws > 1:
@@ -297,9 +309,12 @@ def processes_leg(native, torch, dev, stream, args, ws, hbm_peak):
             t3 = time.perf_counter()
             r.activate(ac["in_slab"][:, sl], ac["rho"][sl], ac["w"][sl])
             t4 = time.perf_counter()
+            r.optics_lw(ow["in_slab"][:, sl], opd.cpu().numpy()[sl], d["dt"], otables)
+            t5 = time.perf_counter()
             import multiprocessing
             for name, el in (("calcsize", t1 - t0), ("coagulation", t2 - t1),
-                             ("setsox", t3 - t2), ("activation", t4 - t3)):
+                             ("setsox", t3 - t2), ("activation", t4 - t3),
+                             ("optics_lw", t5 - t4)):
                 res[name]["cpu_baseline"] = {
                     "value": m / el, "unit": "cells/s", "kind": "reference",
                     "cores": multiprocessing.cpu_count(),

@@ -296,6 +296,47 @@ mam4b_status mam4b_step_tracers(mam4b_ctx *ctx, const double *q, const double *q
                                 int precision, void *stream);
 
 /*
+ * Longwave aerosol optics, batched over cells:
+ * mam4::modal_aero_opt::modal_aero_lw_k (src/mam4xx/modal_aero_opt.hpp:
+ * 879-989). Per cell: dry and wet mode diameters and aerosol water
+ * (calcsize and water uptake, as in the step), then for every mode and
+ * longwave band the volume-mixed complex refractive index of species and
+ * water, bilinear interpolation of the Chebyshev coefficients of specific
+ * absorption in the mode's refractive-index table, and the layer's
+ * absorption optical depth tauxar = max(0, absorption) x wet volume x
+ * rho_water x pdeldry / g, summed over modes.
+ *
+ * The tables (in the host model read from its optics files) are set once
+ * per context with mam4b_optics_lw_set_tables (host arrays, copied):
+ *   specrefindex    [16 bands][MAM4B_OPTICS_NTYPES species types] complex,
+ *                   as (real, imaginary) pairs: the refractive index of
+ *                   each species type of get_e3sm_parameters (ndrop.hpp:
+ *                   44-114), mapped to the modes by species type
+ *   water_refindex  [16] complex, (real, imaginary) pairs
+ *   refrtab, refitab  [4 modes][16][7] and [4][16][10]: the real and
+ *                   imaginary refractive-index grids of each table
+ *   absp            [4][16][5 coefficients][7][10]: Chebyshev coefficients
+ *                   of specific absorption
+ * mam4b_optics_lw reads the step's input layout (MAM4B_NIN fields of ld
+ * doubles; qv, T, p, cloud fraction and both aerosol phases), pdeldry (dry
+ * pressure thickness, Pa, one per cell) and writes tauxar, 16 fields of ld
+ * doubles. Asynchronous on `stream`.
+ */
+#define MAM4B_OPTICS_NTYPES 14
+#define MAM4B_OPTICS_LW_BANDS 16
+typedef struct mam4b_optics_lw_tables {
+  const double *specrefindex;
+  const double *water_refindex;
+  const double *refrtab;
+  const double *refitab;
+  const double *absp;
+} mam4b_optics_lw_tables;
+mam4b_status mam4b_optics_lw_set_tables(mam4b_ctx *ctx, const mam4b_optics_lw_tables *tables);
+mam4b_status mam4b_optics_lw(mam4b_ctx *ctx, const double *in_slab, size_t ld,
+                             const double *pdeldry, double *tauxar, int ncol, int nlev,
+                             double dt, void *stream);
+
+/*
  * Aerosol activation, batched over cells: the per-cell part of mam4xx's
  * droplet nucleation, get_activate_frac (src/mam4xx/ndrop.hpp:699-765):
  * number, volume and hygroscopicity of the 4 interstitial modes (loadaer),

@@ -10,6 +10,7 @@
 
 #include <math.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -25,6 +26,7 @@
 #include "mam4b_process.cuh"
 #include "mam4b_setsox.cuh"
 #include "mam4b_activation.cuh"
+#include "mam4b_optics.cuh"
 
 namespace mam4b {
 
@@ -1788,6 +1790,35 @@ __global__ void __launch_bounds__(128) activate_kernel(const __grid_constant__ A
     a.out[(size_t)k * a.ld + c] = out[k];
 }
 
+// ---- longwave aerosol optics (modal_aero_lw_k), one thread per cell
+struct OpticsLwArgs {
+  const double *in[MAM4B_NIN];
+  const double *pdeldry;
+  const double *tables;
+  double *tau;  // [16][ld]
+  size_t ld;
+  long long ncell;
+  double dt;
+};
+
+__global__ void __launch_bounds__(128) optics_lw_kernel(const __grid_constant__ OpticsLwArgs a) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncell)
+    return;
+  double ai[NPOP], ac[NPOP], tau[opt::kLwBands];
+#pragma unroll
+  for (int p = 0; p < NPOP; ++p) {
+    ai[p] = __ldg(a.in[MAM4B_IN_AER_I + p] + c);
+    ac[p] = __ldg(a.in[MAM4B_IN_AER_C + p] + c);
+  }
+  opt::lw_cell(c_k, a.tables, ai, ac, __ldg(a.in[MAM4B_IN_QV] + c), __ldg(a.in[MAM4B_IN_T] + c),
+               __ldg(a.in[MAM4B_IN_P] + c), __ldg(a.in[MAM4B_IN_CLD] + c), __ldg(a.pdeldry + c),
+               a.dt, tau);
+#pragma unroll
+  for (int b = 0; b < opt::kLwBands; ++b)
+    a.tau[(size_t)b * a.ld + c] = tau[b];
+}
+
 }  // namespace mam4b
 
 // =============================================================== C ABI
@@ -1831,6 +1862,7 @@ struct mam4b_ctx {
   int adj_grid;
   double *d_ck2, *d_abar, *d_lbar;
   int *d_npass;         // [cap_adj]: passes of each SOA loop
+  double *d_optics_lw;  // longwave optics tables (opt::kTableDoubles), set by the host
   unsigned *d_bins;     // [2 kPassBins]: loops per pass count, start offsets
   int adj_soa_grid;
   size_t cap_adj;
@@ -2142,6 +2174,7 @@ mam4b_status mam4b_destroy(mam4b_ctx *ctx) {
   cudaFree(ctx->d_lbar);
   cudaFree(ctx->d_npass);
   cudaFree(ctx->d_bins);
+  cudaFree(ctx->d_optics_lw);
   if (ctx->host_streams) {
     for (int k = 0; k < kHostStreams; ++k) {
       cudaStreamDestroy(ctx->hs[k]);
@@ -2597,6 +2630,81 @@ mam4b_status mam4b_step_tracers(mam4b_ctx *ctx, const double *q, const double *q
     ov.field[MAM4B_OUT_DGN_A + k] = mode_out + (size_t)k * mode_stride;
   iv.pblh = pblh;
   return mam4b_step(ctx, &iv, &ov, ncol, nlev, dt, precision, stream);
+}
+
+// longwave optics tables: the reference's per-type species refractive
+// indices mapped to modes by species type (set_device_specrefindex,
+// modal_aero_opt.hpp:142-190), water, grids and absorption tables
+mam4b_status mam4b_optics_lw_set_tables(mam4b_ctx *ctx, const mam4b_optics_lw_tables *t) {
+  const char *what = "mam4b_optics_lw_set_tables";
+  if (!ctx || !t || !t->specrefindex || !t->water_refindex || !t->refrtab || !t->refitab ||
+      !t->absp)
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, what, cudaSuccess);
+  double *h = (double *)malloc(sizeof(double) * opt::kTableDoubles);
+  if (!h)
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_optics_lw_set_tables: host memory",
+                   cudaSuccess);
+  memset(h, 0, sizeof(double) * opt::kTableDoubles);
+  for (int m = 0; m < NMODE; ++m)
+    for (int s = 0; s < K::nspec(m); ++s)
+      for (int b = 0; b < opt::kLwBands; ++b) {
+        const int type = act::spectype(m, s) - 1;
+        const size_t src = 2 * ((size_t)b * MAM4B_OPTICS_NTYPES + type);
+        h[opt::kSpecRe + (m * 7 + s) * opt::kLwBands + b] = t->specrefindex[src];
+        h[opt::kSpecIm + (m * 7 + s) * opt::kLwBands + b] = t->specrefindex[src + 1];
+      }
+  for (int b = 0; b < opt::kLwBands; ++b) {
+    h[opt::kWaterRe + b] = t->water_refindex[2 * b];
+    h[opt::kWaterIm + b] = t->water_refindex[2 * b + 1];
+  }
+  memcpy(h + opt::kRefr, t->refrtab, sizeof(double) * 4 * opt::kLwBands * opt::kPrefr);
+  memcpy(h + opt::kRefi, t->refitab, sizeof(double) * 4 * opt::kLwBands * opt::kPrefi);
+  memcpy(h + opt::kAbsp, t->absp,
+         sizeof(double) * 4 * opt::kLwBands * opt::kNcoef * opt::kPrefr * opt::kPrefi);
+  cudaError_t e = cudaSuccess;
+  if (!ctx->d_optics_lw)
+    e = cudaMalloc(&ctx->d_optics_lw, sizeof(double) * opt::kTableDoubles);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(ctx->d_optics_lw, h, sizeof(double) * opt::kTableDoubles,
+                   cudaMemcpyHostToDevice);
+  free(h);
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, what, e);
+  return MAM4B_OK;
+}
+
+// modal_aero_opt::modal_aero_lw_k (modal_aero_opt.hpp:879-989), batched
+mam4b_status mam4b_optics_lw(mam4b_ctx *ctx, const double *in_slab, size_t ld,
+                             const double *pdeldry, double *tauxar, int ncol, int nlev,
+                             double dt, void *stream) {
+  const char *what = "mam4b_optics_lw";
+  const size_t n = (size_t)(ncol > 0 ? ncol : 0) * (size_t)(nlev > 0 ? nlev : 0);
+  if (!ctx || !in_slab || !pdeldry || !tauxar || ncol < 0 || nlev <= 0 || ld < n ||
+      !(dt > 0.0) || !isfinite(dt))
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, what, cudaSuccess);
+  if (!ctx->d_optics_lw)
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_optics_lw: tables not set",
+                   cudaSuccess);
+  OpticsLwArgs a;
+  for (int f = 0; f < MAM4B_NIN; ++f)
+    a.in[f] = in_slab + (size_t)f * ld;
+  a.pdeldry = pdeldry;
+  a.tables = ctx->d_optics_lw;
+  a.tau = tauxar;
+  a.ld = ld;
+  a.ncell = (long long)n;
+  a.dt = dt;
+  cudaStream_t s = (cudaStream_t)stream;
+  ctx->last_stream = s;
+  if (n == 0)
+    return MAM4B_OK;
+  const int block = 128;
+  optics_lw_kernel<<<(unsigned)((n + block - 1) / block), block, 0, s>>>(a);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, what, e);
+  ctx->launches += 1;
+  return MAM4B_OK;
 }
 
 // ndrop get_activate_frac (ndrop.hpp:699-765), batched

@@ -64,6 +64,13 @@ class ProgFields(ctypes.Structure):
         return f
 
 
+class OpticsLwTables(ctypes.Structure):
+    """mam4b_optics_lw_tables (host pointers)."""
+    _fields_ = [("specrefindex", ctypes.c_void_p), ("water_refindex", ctypes.c_void_p),
+                ("refrtab", ctypes.c_void_p), ("refitab", ctypes.c_void_p),
+                ("absp", ctypes.c_void_p)]
+
+
 class CalcSizeConfig(ctypes.Structure):
     """mam4b_calcsize_config: CalcSize::Config (src/mam4xx/calcsize.hpp:835-842)."""
     _fields_ = [("do_aitacc_transfer", ctypes.c_int), ("do_adjust", ctypes.c_int)]
@@ -101,6 +108,10 @@ def lib():
         L.mam4b_adjoint_slab.restype = I
         L.mam4b_step_tracers.argtypes = [P, P, P, S, P, P, P, P, P, P, P, P, S, I, I, D, I, P]
         L.mam4b_step_tracers.restype = I
+        L.mam4b_optics_lw_set_tables.argtypes = [P, ctypes.POINTER(OpticsLwTables)]
+        L.mam4b_optics_lw_set_tables.restype = I
+        L.mam4b_optics_lw.argtypes = [P, P, S, P, P, I, I, D, P]
+        L.mam4b_optics_lw.restype = I
         L.mam4b_activate.argtypes = [P, P, S, P, P, P, I, I, P]
         L.mam4b_activate.restype = I
         L.mam4b_setsox.argtypes = [P, P, P, P, P, P, P, P, P, S, P, P, I, I, D, P]
@@ -123,7 +134,8 @@ EXPORTED = ["mam4b_abi_version", "mam4b_default_config", "mam4b_create", "mam4b_
             "mam4b_step", "mam4b_step_slab", "mam4b_step_host", "mam4b_last_status",
             "mam4b_last_error", "mam4b_launch_count", "mam4b_step_slab_noalloc",
             "mam4b_adjoint_slab", "mam4b_calcsize_process", "mam4b_coagulation_process",
-            "mam4b_step_tracers", "mam4b_setsox", "mam4b_activate"]
+            "mam4b_step_tracers", "mam4b_setsox", "mam4b_activate",
+            "mam4b_optics_lw_set_tables", "mam4b_optics_lw"]
 
 
 def default_config(**overrides):
@@ -214,6 +226,23 @@ class Context:
                                           int(nlev), float(dt), int(precision),
                                           ctypes.c_void_p(stream))
         self._check(st, "mam4b_step_tracers")
+
+    def optics_lw_set_tables(self, tables):
+        """Copies the longwave optics tables (dict of numpy arrays, see
+        workloads.make_optics_lw_tables) into the context."""
+        import numpy as np
+        arrs = {k: np.ascontiguousarray(v, dtype=np.float64) for k, v in tables.items()}
+        t = OpticsLwTables(*[arrs[k].ctypes.data for k in ("specrefindex", "water_refindex",
+                                                           "refrtab", "refitab", "absp")])
+        st = self._lib.mam4b_optics_lw_set_tables(self._h, ctypes.byref(t))
+        self._check(st, "mam4b_optics_lw_set_tables")
+
+    def optics_lw(self, in_ptr, ld, pdeldry, tauxar, ncol, nlev, dt, stream=0):
+        """Longwave absorption optical depth (mam4b_optics_lw); device
+        pointers, tauxar [16][ld]."""
+        st = self._lib.mam4b_optics_lw(self._h, in_ptr, int(ld), pdeldry, tauxar, int(ncol),
+                                       int(nlev), float(dt), ctypes.c_void_p(stream))
+        self._check(st, "mam4b_optics_lw")
 
     def activate(self, in_ptr, ld, air_density, updraft, out, ncol, nlev, stream=0):
         """Aerosol activation fractions (mam4b_activate); device pointers,

@@ -267,3 +267,27 @@ def make_activation_inputs(name="c2", ncol=None, nlev=None, seed=None):
     cut = rng.uniform(0, 1, n)
     wup = np.where(cut < 0.05, 0.0, np.where(cut < 0.1, -wup, wup))
     return {"ncol": w["ncol"], "nlev": w["nlev"], "in_slab": x, "rho": rho, "w": wup}
+
+
+def make_optics_lw_tables(seed=0):
+    """Seeded stand-ins for the longwave optics tables the host model reads
+    from its optics files (same shapes and value ranges, not the data):
+    species-type refractive indices (real 1.4..1.9, imaginary 1e-4..0.5),
+    water (1.2..1.4, 1e-3..0.5), per-(mode, band) refractive-index grids
+    (7 real values over 1.2..2.0, 10 imaginary values over 1e-4..1) and
+    Chebyshev absorption coefficients (5 per grid point)."""
+    rng = np.random.default_rng(4242 + seed)
+    nb, nt = 16, 14
+    spec = np.empty((nb, nt, 2))
+    spec[..., 0] = rng.uniform(1.4, 1.9, (nb, nt))
+    spec[..., 1] = _logu(rng, 1e-4, 0.5, nb * nt).reshape(nb, nt)
+    water = np.empty((nb, 2))
+    water[:, 0] = rng.uniform(1.2, 1.4, nb)
+    water[:, 1] = _logu(rng, 1e-3, 0.5, nb)
+    refr = np.sort(rng.uniform(1.2, 2.0, (4, nb, 7)), axis=2)
+    refr[..., 0], refr[..., -1] = 1.2, 2.0
+    refi = np.sort(_logu(rng, 1e-4, 1.0, 4 * nb * 10).reshape(4, nb, 10), axis=2)
+    absp = rng.normal(0.0, 300.0, (4, nb, 5, 7, 10))
+    absp[:, :, 0] = rng.uniform(500.0, 2000.0, (4, nb, 7, 10))
+    return {"specrefindex": np.ascontiguousarray(spec), "water_refindex": water,
+            "refrtab": refr, "refitab": refi, "absp": absp}

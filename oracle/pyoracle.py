@@ -159,6 +159,20 @@ class ReferenceOracle(_Oracle):
           tend.ctypes.data, dgn.ctypes.data)
         return tend, dgn
 
+    def optics_lw(self, in_slab, pdeldry, dt, tables):
+        """modal_aero_opt::modal_aero_lw_k per cell; returns tau (16, ncell)."""
+        x = np.ascontiguousarray(in_slab, dtype=np.float64)
+        n = x.shape[1]
+        tau = np.zeros((16, n))
+        pd = np.ascontiguousarray(pdeldry, dtype=np.float64)
+        t = [np.ascontiguousarray(tables[k], dtype=np.float64)
+             for k in ("specrefindex", "water_refindex", "refrtab", "refitab", "absp")]
+        f = self.lib.mam4ref_optics_lw
+        f.argtypes = [_I, _P, _P, _D] + [_P] * 6
+        f.restype = None
+        f(n, x.ctypes.data, pd.ctypes.data, dt, *[a.ctypes.data for a in t], tau.ctypes.data)
+        return tau
+
     def maxsat(self, zeta, eta, smc):
         """ndrop::maxsat for 4 modes."""
         f = self.lib.mam4ref_maxsat

@@ -31,6 +31,7 @@
 #include <mam4xx/modal_aero_calcsize.hpp>
 #include <mam4xx/mo_setsox.hpp>
 #include <mam4xx/ndrop.hpp>
+#include <mam4xx/modal_aero_opt.hpp>
 #include <mam4xx/water_uptake.hpp>
 
 #include "../oracle_api.h"
@@ -443,6 +444,57 @@ void mam4ref_activate(int ncell, const double *in, const double *rho, const doub
       out[(size_t)(12 + m) * n + c] = fluxm[m];
     }
     out[(size_t)16 * n + c] = flux_fullact;
+  }
+}
+
+// modal_aero_opt::modal_aero_lw_k per cell on a step input slab
+// (field-major, ld = ncell) with the given tables (layouts of
+// mam4b_optics_lw_tables); tau [16][ncell].
+void mam4ref_optics_lw(int ncell, const double *in, const double *pdeldry, double dt,
+                       const double *specref, const double *water, const double *refr,
+                       const double *refi, const double *absp, double *tau) {
+  using namespace mam4::modal_aero_opt;
+  AerosolOpticsDeviceData d;
+  set_aerosol_optics_data_for_modal_aero_lw_views(d);
+  set_complex_views_modal_aero(d);
+  ComplexView2D::host_mirror_type host("specrefndx", nlwbands, mam4::ndrop::maxd_aspectype);
+  for (int b = 0; b < nlwbands; ++b)
+    for (int t = 0; t < mam4::ndrop::maxd_aspectype; ++t)
+      host(b, t) = Kokkos::complex<Real>(specref[2 * (b * 14 + t)], specref[2 * (b * 14 + t) + 1]);
+  set_device_specrefindex(d.specrefindex_lw, "long_wave", host);
+  for (int b = 0; b < nlwbands; ++b)
+    d.crefwlw(b) = Kokkos::complex<Real>(water[2 * b], water[2 * b + 1]);
+  for (int m = 0; m < 4; ++m)
+    for (int b = 0; b < nlwbands; ++b) {
+      for (int i = 0; i < prefr; ++i)
+        d.refrtablw[m][b](i) = refr[(m * nlwbands + b) * prefr + i];
+      for (int j = 0; j < prefi; ++j)
+        d.refitablw[m][b](j) = refi[(m * nlwbands + b) * prefi + j];
+      for (int c = 0; c < ncoef; ++c)
+        for (int i = 0; i < prefr; ++i)
+          for (int j = 0; j < prefi; ++j)
+            d.absplw[m][b](c, i, j) =
+                absp[(((m * nlwbands + b) * ncoef + c) * prefr + i) * prefi + j];
+    }
+  const CalcsizeData &cd = calcsize_data();
+  const size_t n = (size_t)ncell;
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int c = 0; c < ncell; ++c) {
+    auto IN = [&](int f) { return in[(size_t)f * n + c]; };
+    Real state_q[40] = {}, qqcw[40] = {};
+    state_q[0] = IN(MAM4B_IN_QV);
+    state_q[11] = IN(MAM4B_IN_H2SO4);
+    state_q[14] = IN(MAM4B_IN_SOAG);
+    for (int p = 0; p < MAM4B_NUM_POPS; ++p) {
+      state_q[15 + p] = IN(MAM4B_IN_AER_I + p);
+      qqcw[15 + p] = IN(MAM4B_IN_AER_C + p);
+    }
+    Real cld = IN(MAM4B_IN_CLD);
+    Real t[nlwbands] = {};
+    modal_aero_lw_k(pdeldry[c], IN(MAM4B_IN_P), IN(MAM4B_IN_T), cld, state_q, qqcw, dt, d, cd,
+                    t);
+    for (int b = 0; b < nlwbands; ++b)
+      tau[(size_t)b * n + c] = t[b];
   }
 }
 

@@ -323,6 +323,7 @@ public:
   using reference_type = value_type &;
   using data_type = DataType;
   using HostMirror = View<std::remove_const_t<DataType>>;
+  using host_mirror_type = HostMirror;
   using non_const_type = View<std::remove_const_t<DataType>>;
   using const_type = View<const DataType>;
   using memory_space = HostSpace;

@@ -104,3 +104,17 @@ def test_reference_activation_fractions(ref_oracle):
     no_up = d["w"] <= 0
     assert no_up.any() and (out[:, no_up] == 0).all()
     np.testing.assert_array_equal(out[16, ~no_up], d["w"][~no_up])
+
+
+def test_reference_optics_lw_scales_with_layer_mass(ref_oracle):
+    """Longwave absorption optical depth: finite, non-negative, and
+    proportional to the layer's dry mass (pdeldry / g)."""
+    from mam4xx_b200.workloads import make_optics_lw_tables
+    w = make_workload("c2", ncol=8, seed=6)
+    tb = make_optics_lw_tables()
+    n = w["in_slab"].shape[1]
+    pdel = np.full(n, 1000.0)
+    t1 = ref_oracle.optics_lw(w["in_slab"], pdel, w["dt"], tb)
+    t2 = ref_oracle.optics_lw(w["in_slab"], 2 * pdel, w["dt"], tb)
+    assert np.isfinite(t1).all() and (t1 >= 0).all() and (t1 > 0).mean() > 0.9
+    np.testing.assert_allclose(t2, 2 * t1, rtol=1e-14)
