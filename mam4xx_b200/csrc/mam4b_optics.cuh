@@ -47,87 +47,79 @@ MAM4B_HD void table_factors(int n, double ref, const double *tab, int &ix, doubl
   }
 }
 
-// One cell. ai, ac: 25 interstitial / cloud-borne populations; tables:
-// device table (layout above); tau: absorption optical depth per band.
-MAM4B_HD void lw_cell(const StepConsts &C, const double *tables, const double (&ai)[NPOP],
-                      const double (&ac)[NPOP], double qv, double temp, double pmid, double cld,
-                      double pdeldry, double dt, double (&tau)[kLwBands]) {
-  double dgn_a[NMODE], pt_i[NPOP], pt_c[NPOP], dgn_w[NMODE], qaerwat[NMODE], wetdens[NMODE];
-  calcsize(C, ai, ac, dt, dgn_a, pt_i, pt_c);
-  water_uptake(C, ai, qv, temp, pmid, cld, dgn_a, dgn_w, qaerwat, wetdens);
-  const double rga = 1.0 / 9.80616;
-  const double mass = pdeldry * rga;
-#pragma unroll
-  for (int b = 0; b < kLwBands; ++b)
-    tau[b] = 0.0;
+// Chebyshev polynomials at the surface-mode radius of a mode with wet
+// diameter dgn_w (modal_size_parameters, method 2)
+MAM4B_HD void mode_cheb(int m, double dgn_w, double (&cheb)[kNcoef]) {
   const double xrmin = log(0.01e-6), xrmax = log(25.e-6);
-  for (int m = 0; m < NMODE; ++m) {
-    // modal_size_parameters (method 2)
-    const double alnsg = log(K::sig(m));
-    const double logradsurf = log(0.5 * dgn_w[m]) + 2.0 * alnsg * alnsg;
-    double xrad = bound(xrmin, xrmax, logradsurf);
-    xrad = (2.0 * xrad - xrmax - xrmin) / (xrmax - xrmin);
-    double cheb[kNcoef];
-    cheb[0] = 1.0;
-    cheb[1] = xrad;
+  const double alnsg = log(K::sig(m));
+  const double logradsurf = log(0.5 * dgn_w) + 2.0 * alnsg * alnsg;
+  double xrad = bound(xrmin, xrmax, logradsurf);
+  xrad = (2.0 * xrad - xrmax - xrmin) / (xrmax - xrmin);
+  cheb[0] = 1.0;
+  cheb[1] = xrad;
 #pragma unroll
-    for (int nc = 2; nc < kNcoef; ++nc)
-      cheb[nc] = 2.0 * xrad * cheb[nc - 1] - cheb[nc - 2];
-    double specvol[7];
-    const int nspec = K::nspec(m);
-    for (int s = 0; s < nspec; ++s)
-      specvol[s] = ai[K::spec0(m) + s] / act::type_dens(act::spectype(m, s));
-    for (int b = 0; b < kLwBands; ++b) {
-      // calc_refin_complex (longwave)
-      double dryvol = 0.0, cre = 0.0, cim = 0.0;
-      for (int s = 0; s < nspec; ++s) {
-        dryvol += specvol[s];
-        cre += specvol[s] * MAM4B_LDG(tables + kSpecRe + (m * 7 + s) * kLwBands + b);
-        cim += specvol[s] * MAM4B_LDG(tables + kSpecIm + (m * 7 + s) * kLwBands + b);
-      }
-      double watervol = qaerwat[m] / 1.0e3;
-      double wetvol = watervol + dryvol;
-      if (watervol < 0.0) {
-        watervol = 0.0;
-        wetvol = dryvol;
-      }
-      cre += watervol * MAM4B_LDG(tables + kWaterRe + b);
-      cim += watervol * MAM4B_LDG(tables + kWaterIm + b);
-      if (wetvol > 1.e-40) {
-        cre /= wetvol;
-        cim /= wetvol;
-      }
-      const double refr = cre, refi = fabs(cim);
-      // binterp over the refractive-index table
-      const double *rt = tables + kRefr + (m * kLwBands + b) * kPrefr;
-      const double *it = tables + kRefi + (m * kLwBands + b) * kPrefi;
-      int itab, jtab;
-      double ttab, utab;
-      table_factors(kPrefr, refr, rt, itab, ttab);
-      table_factors(kPrefi, refi, it, jtab, utab);
-      const double tu = ttab * utab;
-      const double tuc = ttab - tu;
-      const double tcuc = 1.0 - tuc - utab;
-      const double tcu = utab - tu;
-      const int jp1 = (jtab + 1 < kPrefi - 1) ? jtab + 1 : kPrefi - 1;
-      const int ip1 = (itab + 1 < kPrefr - 1) ? itab + 1 : kPrefr - 1;
-      const double *tb = tables + kAbsp + (m * kLwBands + b) * kNcoef * kPrefr * kPrefi;
-      double pabs = 0.0;
-#pragma unroll
-      for (int c = 0; c < kNcoef; ++c) {
-        const double *tc = tb + c * kPrefr * kPrefi;
-        const double coef = tcuc * MAM4B_LDG(tc + itab * kPrefi + jtab) +
-                            tuc * MAM4B_LDG(tc + ip1 * kPrefi + jtab) +
-                            tu * MAM4B_LDG(tc + ip1 * kPrefi + jp1) +
-                            tcu * MAM4B_LDG(tc + itab * kPrefi + jp1);
-        // calc_parameterized
-        pabs = (c == 0) ? 0.5 * coef : pabs + cheb[c] * coef;
-      }
-      pabs *= wetvol * 1.0e3;
-      pabs = dmax(0.0, pabs);
-      tau[b] += pabs * mass;
-    }
+  for (int nc = 2; nc < kNcoef; ++nc)
+    cheb[nc] = 2.0 * xrad * cheb[nc - 1] - cheb[nc - 2];
+}
+
+// Absorption optical depth of mode m in band b for one cell: specvol the
+// mode's species volumes, qaerwat the mode's water, cheb its Chebyshev
+// polynomials, mass the layer's dry mass per area (calc_refin_complex,
+// binterp, calc_parameterized and the product of modal_aero_lw_k)
+// species volumes of mode m (specmmr / specdens, no clipping)
+MAM4B_HD void mode_specvol(int m, const double (&ai)[NPOP], double (&specvol)[7]) {
+  for (int s = 0; s < K::nspec(m); ++s)
+    specvol[s] = ai[K::spec0(m) + s] / act::type_dens(act::spectype(m, s));
+}
+
+MAM4B_HD double mode_band_tau(const double *tables, int m, int b, const double (&specvol)[7],
+                              double qaerwat, const double (&cheb)[kNcoef], double mass) {
+  const int nspec = K::nspec(m);
+  double dryvol = 0.0, cre = 0.0, cim = 0.0;
+  for (int s = 0; s < nspec; ++s) {
+    dryvol += specvol[s];
+    cre += specvol[s] * MAM4B_LDG(tables + kSpecRe + (m * 7 + s) * kLwBands + b);
+    cim += specvol[s] * MAM4B_LDG(tables + kSpecIm + (m * 7 + s) * kLwBands + b);
   }
+  double watervol = qaerwat / 1.0e3;
+  double wetvol = watervol + dryvol;
+  if (watervol < 0.0) {
+    watervol = 0.0;
+    wetvol = dryvol;
+  }
+  cre += watervol * MAM4B_LDG(tables + kWaterRe + b);
+  cim += watervol * MAM4B_LDG(tables + kWaterIm + b);
+  if (wetvol > 1.e-40) {
+    cre /= wetvol;
+    cim /= wetvol;
+  }
+  const double refr = cre, refi = fabs(cim);
+  const double *rt = tables + kRefr + (m * kLwBands + b) * kPrefr;
+  const double *it = tables + kRefi + (m * kLwBands + b) * kPrefi;
+  int itab, jtab;
+  double ttab, utab;
+  table_factors(kPrefr, refr, rt, itab, ttab);
+  table_factors(kPrefi, refi, it, jtab, utab);
+  const double tu = ttab * utab;
+  const double tuc = ttab - tu;
+  const double tcuc = 1.0 - tuc - utab;
+  const double tcu = utab - tu;
+  const int jp1 = (jtab + 1 < kPrefi - 1) ? jtab + 1 : kPrefi - 1;
+  const int ip1 = (itab + 1 < kPrefr - 1) ? itab + 1 : kPrefr - 1;
+  const double *tb = tables + kAbsp + (m * kLwBands + b) * kNcoef * kPrefr * kPrefi;
+  double pabs = 0.0;
+#pragma unroll
+  for (int c = 0; c < kNcoef; ++c) {
+    const double *tc = tb + c * kPrefr * kPrefi;
+    const double coef = tcuc * MAM4B_LDG(tc + itab * kPrefi + jtab) +
+                        tuc * MAM4B_LDG(tc + ip1 * kPrefi + jtab) +
+                        tu * MAM4B_LDG(tc + ip1 * kPrefi + jp1) +
+                        tcu * MAM4B_LDG(tc + itab * kPrefi + jp1);
+    pabs = (c == 0) ? 0.5 * coef : pabs + cheb[c] * coef;
+  }
+  pabs *= wetvol * 1.0e3;
+  pabs = dmax(0.0, pabs);
+  return pabs * mass;
 }
 
 }  // namespace opt

@@ -1790,33 +1790,97 @@ __global__ void __launch_bounds__(128) activate_kernel(const __grid_constant__ A
     a.out[(size_t)k * a.ld + c] = out[k];
 }
 
-// ---- longwave aerosol optics (modal_aero_lw_k), one thread per cell
+// ---- longwave aerosol optics (modal_aero_lw_k) in three launches, as the
+// step is split: mode sizes per cell (calcsize, RH), water uptake and the
+// Chebyshev polynomials per (cell, mode), then the optical depth per
+// (cell, band) summed over the modes in order (one band per block row,
+// so a warp's table reads share a band). Scratch rows (per cell):
+// dry diameter [4], RH, aerosol water [4], Chebyshev polynomials [4][5].
+enum { OS_DGN = 0, OS_RH = 4, OS_QW = 5, OS_CHEB = 9, OS_FIELDS = 29 };
 struct OpticsLwArgs {
   const double *in[MAM4B_NIN];
   const double *pdeldry;
   const double *tables;
   double *tau;  // [16][ld]
+  double *scr;  // [OS_FIELDS][ncell]
   size_t ld;
   long long ncell;
   double dt;
 };
 
-__global__ void __launch_bounds__(128) optics_lw_kernel(const __grid_constant__ OpticsLwArgs a) {
+__global__ void __launch_bounds__(128) optics_size_kernel(const __grid_constant__ OpticsLwArgs a) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= a.ncell)
     return;
-  double ai[NPOP], ac[NPOP], tau[opt::kLwBands];
+  double ai[NPOP], ac[NPOP], dgn_a[NMODE], pt_i[NPOP], pt_c[NPOP];
 #pragma unroll
   for (int p = 0; p < NPOP; ++p) {
     ai[p] = __ldg(a.in[MAM4B_IN_AER_I + p] + c);
     ac[p] = __ldg(a.in[MAM4B_IN_AER_C + p] + c);
   }
-  opt::lw_cell(c_k, a.tables, ai, ac, __ldg(a.in[MAM4B_IN_QV] + c), __ldg(a.in[MAM4B_IN_T] + c),
-               __ldg(a.in[MAM4B_IN_P] + c), __ldg(a.in[MAM4B_IN_CLD] + c), __ldg(a.pdeldry + c),
-               a.dt, tau);
+  calcsize(c_k, ai, ac, a.dt, dgn_a, pt_i, pt_c);
+  const size_t n = (size_t)a.ncell;
 #pragma unroll
-  for (int b = 0; b < opt::kLwBands; ++b)
-    a.tau[(size_t)b * a.ld + c] = tau[b];
+  for (int m = 0; m < NMODE; ++m)
+    a.scr[(OS_DGN + m) * n + c] = dgn_a[m];
+  a.scr[OS_RH * n + c] = water_uptake_rh(__ldg(a.in[MAM4B_IN_QV] + c), __ldg(a.in[MAM4B_IN_T] + c),
+                                         __ldg(a.in[MAM4B_IN_P] + c), __ldg(a.in[MAM4B_IN_CLD] + c));
+}
+
+template <int M>
+__device__ __forceinline__ void optics_mode_work(const OpticsLwArgs &a, long long c) {
+  const size_t n = (size_t)a.ncell;
+  double sp[7];
+#pragma unroll
+  for (int s = 0; s < 7; ++s)
+    sp[s] = (s < K::nspec(M)) ? __ldg(a.in[MAM4B_IN_AER_I + K::spec0(M) + (s < K::nspec(M) ? s : 0)] + c) : 0.0;
+  double dgn_w, qw, wd;
+  water_uptake_mode<M>(c_k, sp, a.scr[OS_RH * n + c], a.scr[(OS_DGN + M) * n + c], dgn_w, qw,
+                       wd);
+  double cheb[opt::kNcoef];
+  opt::mode_cheb(M, dgn_w, cheb);
+  a.scr[(OS_QW + M) * n + c] = qw;
+#pragma unroll
+  for (int k = 0; k < opt::kNcoef; ++k)
+    a.scr[(OS_CHEB + opt::kNcoef * M + k) * n + c] = cheb[k];
+}
+
+__global__ void __launch_bounds__(128) optics_mode_kernel(const __grid_constant__ OpticsLwArgs a) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncell)
+    return;
+  switch (blockIdx.y) {
+  case 0: optics_mode_work<0>(a, c); break;
+  case 1: optics_mode_work<1>(a, c); break;
+  case 2: optics_mode_work<2>(a, c); break;
+  default: optics_mode_work<3>(a, c); break;
+  }
+}
+
+__global__ void __launch_bounds__(128) optics_band_kernel(const __grid_constant__ OpticsLwArgs a) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncell)
+    return;
+  const int b = blockIdx.y;
+  const size_t n = (size_t)a.ncell;
+  double ai[NPOP];
+#pragma unroll
+  for (int p = 0; p < NPOP; ++p)
+    ai[p] = (K::numslot(0) == p || K::numslot(1) == p || K::numslot(2) == p || K::numslot(3) == p)
+                ? 0.0
+                : __ldg(a.in[MAM4B_IN_AER_I + p] + c);
+  const double mass = __ldg(a.pdeldry + c) * (1.0 / 9.80616);
+  double tau = 0.0;
+#pragma unroll
+  for (int m = 0; m < NMODE; ++m) {
+    double cheb[opt::kNcoef], specvol[7];
+#pragma unroll
+    for (int k = 0; k < opt::kNcoef; ++k)
+      cheb[k] = a.scr[(OS_CHEB + opt::kNcoef * m + k) * n + c];
+    opt::mode_specvol(m, ai, specvol);
+    tau += opt::mode_band_tau(a.tables, m, b, specvol, a.scr[(OS_QW + m) * n + c], cheb, mass);
+  }
+  a.tau[(size_t)b * a.ld + c] = tau;
 }
 
 }  // namespace mam4b
@@ -1863,6 +1927,8 @@ struct mam4b_ctx {
   double *d_ck2, *d_abar, *d_lbar;
   int *d_npass;         // [cap_adj]: passes of each SOA loop
   double *d_optics_lw;  // longwave optics tables (opt::kTableDoubles), set by the host
+  double *d_optics_scr; // longwave optics per-cell sizes (OS_FIELDS per cell), grown
+  size_t cap_optics_scr;
   unsigned *d_bins;     // [2 kPassBins]: loops per pass count, start offsets
   int adj_soa_grid;
   size_t cap_adj;
@@ -2175,6 +2241,7 @@ mam4b_status mam4b_destroy(mam4b_ctx *ctx) {
   cudaFree(ctx->d_npass);
   cudaFree(ctx->d_bins);
   cudaFree(ctx->d_optics_lw);
+  cudaFree(ctx->d_optics_scr);
   if (ctx->host_streams) {
     for (int k = 0; k < kHostStreams; ++k) {
       cudaStreamDestroy(ctx->hs[k]);
@@ -2698,12 +2765,19 @@ mam4b_status mam4b_optics_lw(mam4b_ctx *ctx, const double *in_slab, size_t ld,
   ctx->last_stream = s;
   if (n == 0)
     return MAM4B_OK;
+  cudaError_t e = grow(&ctx->d_optics_scr, &ctx->cap_optics_scr, (size_t)OS_FIELDS * n);
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_optics_lw scratch", e);
+  a.scr = ctx->d_optics_scr;
   const int block = 128;
-  optics_lw_kernel<<<(unsigned)((n + block - 1) / block), block, 0, s>>>(a);
-  const cudaError_t e = cudaGetLastError();
+  const unsigned grid = (unsigned)((n + block - 1) / block);
+  optics_size_kernel<<<grid, block, 0, s>>>(a);
+  optics_mode_kernel<<<dim3(grid, NMODE), block, 0, s>>>(a);
+  optics_band_kernel<<<dim3(grid, opt::kLwBands), block, 0, s>>>(a);
+  e = cudaGetLastError();
   if (e != cudaSuccess)
     return set_err(ctx, MAM4B_ERR_CUDA, what, e);
-  ctx->launches += 1;
+  ctx->launches += 3;
   return MAM4B_OK;
 }
 
