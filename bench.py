@@ -24,7 +24,8 @@ One step = calcsize + water uptake + amicphys over every cell, dt = 1800 s.
 
   processes  the per-process entries (mam4b_calcsize_process,
          mam4b_coagulation_process, mam4b_setsox, mam4b_activate,
-         mam4b_optics_lw with seeded stand-in tables) on the same columns,
+         mam4b_optics_lw, mam4b_optics_sw with seeded stand-in tables) on
+         the same columns,
          and the step through mam4b_step_tracers: cells/s, the HBM
          roofline of their algorithmic bytes, and the reference's own
          process classes on the host as their CPU baseline
@@ -186,7 +187,8 @@ def cpu_baseline(x, pblh_cell, dt, target_s=12.0):
 # gas tracers, 3 cloud-borne SO4 and 6 tendencies
 PROCESS_BYTES_PER_CELL = {"calcsize": (50 + 20 + 24 + 8) * 8, "coagulation": (42 + 32 + 64) * 8,
                           "setsox": (6 + 4 + 7 + 3 + 3 + 6) * 8,
-                          "activation": (28 + 17) * 8, "optics_lw": (55 + 16) * 8}
+                          "activation": (28 + 17) * 8, "optics_lw": (55 + 16) * 8,
+                          "optics_sw": (55 + 56) * 8}
 
 
 def processes_leg(native, torch, dev, stream, args, ws, hbm_peak):
@@ -260,9 +262,20 @@ def processes_leg(native, torch, dev, stream, args, ws, hbm_peak):
         ctx.optics_lw(ox.data_ptr(), n, opd.data_ptr(), otau.data_ptr(), ncol, NLEV, d["dt"],
                       stream=stream.cuda_stream)
 
+    from mam4xx_b200.workloads import make_optics_sw_tables
+    sw_tables = make_optics_sw_tables(seed=2)
+    ctx.optics_sw_set_tables(sw_tables)
+    sw_out = torch.empty((4, 14, n), dtype=torch.float64, device=dev)
+    sw_aod = torch.empty((ncol,), dtype=torch.float64, device=dev)
+
+    def optics_sw():
+        ctx.optics_sw(ox.data_ptr(), n, opd.data_ptr(), sw_out.data_ptr(), sw_aod.data_ptr(),
+                      ncol, NLEV, d["dt"], stream=stream.cuda_stream)
+
     res = {}
     for name, f in (("calcsize", calcsize), ("coagulation", coag), ("setsox", setsox),
-                    ("activation", activation), ("optics_lw", optics_lw)):
+                    ("activation", activation), ("optics_lw", optics_lw),
+                    ("optics_sw", optics_sw)):
         for _ in range(args.warmup):
             f()
         if ws > 1:
@@ -311,10 +324,12 @@ def processes_leg(native, torch, dev, stream, args, ws, hbm_peak):
             t4 = time.perf_counter()
             r.optics_lw(ow["in_slab"][:, sl], opd.cpu().numpy()[sl], d["dt"], otables)
             t5 = time.perf_counter()
+            r.optics_sw(nc, NLEV, ow["in_slab"][:, sl], opd.cpu().numpy()[sl], d["dt"], sw_tables)
+            t6 = time.perf_counter()
             import multiprocessing
             for name, el in (("calcsize", t1 - t0), ("coagulation", t2 - t1),
                              ("setsox", t3 - t2), ("activation", t4 - t3),
-                             ("optics_lw", t5 - t4)):
+                             ("optics_lw", t5 - t4), ("optics_sw", t6 - t5)):
                 res[name]["cpu_baseline"] = {
                     "value": m / el, "unit": "cells/s", "kind": "reference",
                     "cores": multiprocessing.cpu_count(),

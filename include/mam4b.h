@@ -337,6 +337,40 @@ mam4b_status mam4b_optics_lw(mam4b_ctx *ctx, const double *in_slab, size_t ld,
                              double dt, void *stream);
 
 /*
+ * Shortwave aerosol optics, batched over cells: mam4::modal_aero_opt::
+ * modal_aero_sw (src/mam4xx/modal_aero_opt.hpp:536-878). Per cell, mode
+ * and shortwave band (14): the mode sizes as for the longwave, the
+ * volume-mixed refractive index, the Chebyshev coefficients of specific
+ * extinction, absorption and asymmetry interpolated in the mode's tables,
+ * extinction exp(Chebyshev) (geometric optics above 25 um surface radius),
+ * the single-scattering albedo and the layer products; summed over the
+ * modes per band. Tables per context (host arrays, copied):
+ *   specrefindex [14 bands][MAM4B_OPTICS_NTYPES] and water_refindex [14],
+ *   complex as (real, imaginary) pairs; refrtab [4][14][7], refitab
+ *   [4][14][10]; extp, absp, asmp [4][14][5][7][10]
+ * out: 4 x 14 fields of ld doubles, tauxar[band] (optical depth), then
+ * wa (x single-scattering albedo), ga (x asymmetry), fa (x asymmetry^2).
+ * aodvis: NULL or one value per column, the visible-band (index 9) optical
+ * depth summed over levels and modes. The reference's extra layer above
+ * the model top (constant values) is not produced. Asynchronous on
+ * `stream`.
+ */
+#define MAM4B_OPTICS_SW_BANDS 14
+typedef struct mam4b_optics_sw_tables {
+  const double *specrefindex;
+  const double *water_refindex;
+  const double *refrtab;
+  const double *refitab;
+  const double *extp;
+  const double *absp;
+  const double *asmp;
+} mam4b_optics_sw_tables;
+mam4b_status mam4b_optics_sw_set_tables(mam4b_ctx *ctx, const mam4b_optics_sw_tables *tables);
+mam4b_status mam4b_optics_sw(mam4b_ctx *ctx, const double *in_slab, size_t ld,
+                             const double *pdeldry, double *out, double *aodvis, int ncol,
+                             int nlev, double dt, void *stream);
+
+/*
  * Aerosol activation, batched over cells: the per-cell part of mam4xx's
  * droplet nucleation, get_activate_frac (src/mam4xx/ndrop.hpp:699-765):
  * number, volume and hygroscopicity of the 4 interstitial modes (loadaer),

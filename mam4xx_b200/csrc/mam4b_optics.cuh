@@ -124,3 +124,134 @@ MAM4B_HD double mode_band_tau(const double *tables, int m, int b, const double (
 
 }  // namespace opt
 }  // namespace mam4b
+
+namespace mam4b {
+namespace opt {
+
+// ---------------------------------------------------------------- shortwave
+// modal_aero_sw_wo_diagnostics_k (modal_aero_opt.hpp:536-747) and the mode
+// sums of modal_aero_sw (:749-878). Device table layout (doubles):
+constexpr int kSwBands = 14;
+constexpr int kSwSpecRe = 0;                                     // [4][7][14]
+constexpr int kSwSpecIm = kSwSpecRe + 4 * 7 * kSwBands;          // [4][7][14]
+constexpr int kSwWaterRe = kSwSpecIm + 4 * 7 * kSwBands;         // [14]
+constexpr int kSwWaterIm = kSwWaterRe + kSwBands;                // [14]
+constexpr int kSwRefr = kSwWaterIm + kSwBands;                   // [4][14][7]
+constexpr int kSwRefi = kSwRefr + 4 * kSwBands * kPrefr;         // [4][14][10]
+constexpr int kSwTab = kNcoef * kPrefr * kPrefi;                 // one coefficient table
+constexpr int kSwExt = kSwRefi + 4 * kSwBands * kPrefi;          // [4][14][5][7][10]
+constexpr int kSwAbs = kSwExt + 4 * kSwBands * kSwTab;
+constexpr int kSwAsm = kSwAbs + 4 * kSwBands * kSwTab;
+constexpr int kSwTableDoubles = kSwAsm + 4 * kSwBands * kSwTab;
+constexpr int kSwDiagBand = 9;  // visible band of the optical-depth diagnostic
+
+// surface-mode radius, its log (method 1: log of the radius) and the
+// Chebyshev polynomials (modal_size_parameters)
+MAM4B_HD void mode_cheb_sw(int m, double dgn_w, double &radsurf, double &logradsurf,
+                           double (&cheb)[kNcoef]) {
+  const double xrmin = log(0.01e-6), xrmax = log(25.e-6);
+  const double alnsg = log(K::sig(m));
+  const double explnsigma = exp(2.0 * alnsg * alnsg);
+  radsurf = 0.5 * dgn_w * explnsigma;
+  logradsurf = log(radsurf);
+  double xrad = bound(xrmin, xrmax, logradsurf);
+  xrad = (2.0 * xrad - xrmax - xrmin) / (xrmax - xrmin);
+  cheb[0] = 1.0;
+  cheb[1] = xrad;
+#pragma unroll
+  for (int nc = 2; nc < kNcoef; ++nc)
+    cheb[nc] = 2.0 * xrad * cheb[nc - 1] - cheb[nc - 2];
+}
+
+// bilinear weights of the three coefficient tables of (m, b)
+MAM4B_HD void sw_coefs(const double *tables, int m, int b, double refr, double refi,
+                       double (&cext)[kNcoef], double (&cabs)[kNcoef],
+                       double (&casm)[kNcoef]) {
+  const double *rt = tables + kSwRefr + (m * kSwBands + b) * kPrefr;
+  const double *it = tables + kSwRefi + (m * kSwBands + b) * kPrefi;
+  int itab, jtab;
+  double ttab, utab;
+  table_factors(kPrefr, refr, rt, itab, ttab);
+  table_factors(kPrefi, refi, it, jtab, utab);
+  const double tu = ttab * utab;
+  const double tuc = ttab - tu;
+  const double tcuc = 1.0 - tuc - utab;
+  const double tcu = utab - tu;
+  const int jp1 = (jtab + 1 < kPrefi - 1) ? jtab + 1 : kPrefi - 1;
+  const int ip1 = (itab + 1 < kPrefr - 1) ? itab + 1 : kPrefr - 1;
+  const size_t off = (size_t)(m * kSwBands + b) * kSwTab;
+#pragma unroll
+  for (int c = 0; c < kNcoef; ++c) {
+    const size_t o = off + (size_t)c * kPrefr * kPrefi;
+    const double *e = tables + kSwExt + o, *a = tables + kSwAbs + o, *s = tables + kSwAsm + o;
+    cext[c] = tcuc * MAM4B_LDG(e + itab * kPrefi + jtab) + tuc * MAM4B_LDG(e + ip1 * kPrefi + jtab) +
+              tu * MAM4B_LDG(e + ip1 * kPrefi + jp1) + tcu * MAM4B_LDG(e + itab * kPrefi + jp1);
+    cabs[c] = tcuc * MAM4B_LDG(a + itab * kPrefi + jtab) + tuc * MAM4B_LDG(a + ip1 * kPrefi + jtab) +
+              tu * MAM4B_LDG(a + ip1 * kPrefi + jp1) + tcu * MAM4B_LDG(a + itab * kPrefi + jp1);
+    casm[c] = tcuc * MAM4B_LDG(s + itab * kPrefi + jtab) + tuc * MAM4B_LDG(s + ip1 * kPrefi + jtab) +
+              tu * MAM4B_LDG(s + ip1 * kPrefi + jp1) + tcu * MAM4B_LDG(s + itab * kPrefi + jp1);
+  }
+}
+
+MAM4B_HD double cheb_eval(const double (&coef)[kNcoef], const double (&cheb)[kNcoef]) {
+  double p = 0.5 * coef[0];
+#pragma unroll
+  for (int nc = 1; nc < kNcoef; ++nc)
+    p += cheb[nc] * coef[nc];
+  return p;
+}
+
+// optical depth, single-scattering and asymmetry products of mode m in
+// band b for one cell: out = {tauxar, wa, ga, fa}
+MAM4B_HD void mode_band_sw(const double *tables, int m, int b, const double (&specvol)[7],
+                           double qaerwat, const double (&cheb)[kNcoef], double radsurf,
+                           double logradsurf, double mass, double (&out)[4]) {
+  const int nspec = K::nspec(m);
+  double dryvol = 0.0;
+  for (int s = 0; s < nspec; ++s)
+    dryvol += specvol[s];
+  if (dryvol < 0.0 && dryvol > -1.e-16) {
+    out[0] = out[1] = out[2] = out[3] = 0.0;
+    return;
+  }
+  // calc_refin_complex (shortwave)
+  double dv = 0.0, cre = 0.0, cim = 0.0;
+  for (int s = 0; s < nspec; ++s) {
+    dv += specvol[s];
+    cre += specvol[s] * MAM4B_LDG(tables + kSwSpecRe + (m * 7 + s) * kSwBands + b);
+    cim += specvol[s] * MAM4B_LDG(tables + kSwSpecIm + (m * 7 + s) * kSwBands + b);
+  }
+  double watervol = qaerwat / 1.0e3;
+  double wetvol = watervol + dv;
+  if (watervol < 0.0) {
+    watervol = 0.0;
+    wetvol = dv;
+  }
+  cre += watervol * MAM4B_LDG(tables + kSwWaterRe + b);
+  cim += watervol * MAM4B_LDG(tables + kSwWaterIm + b);
+  const double den = dmax(wetvol, 1.e-40);
+  cre /= den;
+  cim /= den;
+  double cext[kNcoef], cabs[kNcoef], casm[kNcoef];
+  sw_coefs(tables, m, b, cre, fabs(cim), cext, cabs, casm);
+  double pext = cheb_eval(cext, cheb);
+  double pabs = cheb_eval(cabs, cheb);
+  const double pasm = cheb_eval(casm, cheb);
+  const double xrmax = log(25.e-6);
+  if (logradsurf <= xrmax)
+    pext = exp(pext);
+  else
+    pext = 1.5 / (radsurf * 1.0e3);
+  pext *= wetvol * 1.0e3;
+  pabs *= wetvol * 1.0e3;
+  pabs = bound(0.0, pext, pabs);
+  const double palb = 1.0 - pabs / dmax(pext, 1.e-40);
+  const double dopaer = pext * mass;
+  out[0] = dopaer;
+  out[1] = dopaer * palb;
+  out[2] = dopaer * palb * pasm;
+  out[3] = dopaer * palb * pasm * pasm;
+}
+
+}  // namespace opt
+}  // namespace mam4b

@@ -1883,6 +1883,105 @@ __global__ void __launch_bounds__(128) optics_band_kernel(const __grid_constant_
   a.tau[(size_t)b * a.ld + c] = tau;
 }
 
+// ---- shortwave aerosol optics (modal_aero_sw): optics_size_kernel, then
+// per (cell, mode) water uptake and the method-1 size parameters, per
+// (cell, band) the four mode-summed products, and per column the visible
+// optical depth. Scratch rows beyond the longwave ones: Chebyshev
+// polynomials [4][5], surface radius [4], its log [4], visible-band
+// optical depth of each mode [4].
+enum { SS_CHEB = 9, SS_RAD = 29, SS_LOGRAD = 33, SS_AOD = 37, SS_FIELDS = 41 };
+struct OpticsSwArgs {
+  OpticsLwArgs base;  // inputs, tables, scratch, ld, ncell, dt (base.tau unused)
+  double *out;        // [4][14][ld]: tauxar, wa, ga, fa
+  double *aodvis;     // [ncol] or null
+  int ncol, nlev;
+};
+
+template <int M>
+__device__ __forceinline__ void optics_sw_mode_work(const OpticsSwArgs &w, long long c) {
+  const OpticsLwArgs &a = w.base;
+  const size_t n = (size_t)a.ncell;
+  double sp[7];
+#pragma unroll
+  for (int s = 0; s < 7; ++s)
+    sp[s] = (s < K::nspec(M)) ? __ldg(a.in[MAM4B_IN_AER_I + K::spec0(M) + (s < K::nspec(M) ? s : 0)] + c) : 0.0;
+  double dgn_w, qw, wd;
+  water_uptake_mode<M>(c_k, sp, a.scr[OS_RH * n + c], a.scr[(OS_DGN + M) * n + c], dgn_w, qw,
+                       wd);
+  double cheb[opt::kNcoef], rad, lrad;
+  opt::mode_cheb_sw(M, dgn_w, rad, lrad, cheb);
+  a.scr[(OS_QW + M) * n + c] = qw;
+#pragma unroll
+  for (int k = 0; k < opt::kNcoef; ++k)
+    a.scr[(SS_CHEB + opt::kNcoef * M + k) * n + c] = cheb[k];
+  a.scr[(SS_RAD + M) * n + c] = rad;
+  a.scr[(SS_LOGRAD + M) * n + c] = lrad;
+}
+
+__global__ void __launch_bounds__(128) optics_sw_mode_kernel(const __grid_constant__ OpticsSwArgs w) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= w.base.ncell)
+    return;
+  switch (blockIdx.y) {
+  case 0: optics_sw_mode_work<0>(w, c); break;
+  case 1: optics_sw_mode_work<1>(w, c); break;
+  case 2: optics_sw_mode_work<2>(w, c); break;
+  default: optics_sw_mode_work<3>(w, c); break;
+  }
+}
+
+__global__ void __launch_bounds__(128) optics_sw_band_kernel(const __grid_constant__ OpticsSwArgs w) {
+  const OpticsLwArgs &a = w.base;
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncell)
+    return;
+  const int b = blockIdx.y;
+  const size_t n = (size_t)a.ncell;
+  double ai[NPOP];
+#pragma unroll
+  for (int p = 0; p < NPOP; ++p)
+    ai[p] = (K::numslot(0) == p || K::numslot(1) == p || K::numslot(2) == p || K::numslot(3) == p)
+                ? 0.0
+                : __ldg(a.in[MAM4B_IN_AER_I + p] + c);
+  const double mass = __ldg(a.pdeldry + c) * (1.0 / 9.80616);
+  double sum[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+  for (int m = 0; m < NMODE; ++m) {
+    double cheb[opt::kNcoef], specvol[7], o[4];
+#pragma unroll
+    for (int k = 0; k < opt::kNcoef; ++k)
+      cheb[k] = a.scr[(SS_CHEB + opt::kNcoef * m + k) * n + c];
+    opt::mode_specvol(m, ai, specvol);
+    opt::mode_band_sw(a.tables, m, b, specvol, a.scr[(OS_QW + m) * n + c], cheb,
+                      a.scr[(SS_RAD + m) * n + c], a.scr[(SS_LOGRAD + m) * n + c], mass, o);
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      sum[q] += o[q];
+    if (b == opt::kSwDiagBand)
+      a.scr[(SS_AOD + m) * n + c] = o[0];
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+    w.out[((size_t)q * opt::kSwBands + b) * a.ld + c] = sum[q];
+}
+
+// visible optical depth of each column: its levels' mode optical depths
+// summed level by level, mode by mode (the reduction of modal_aero_sw)
+__global__ void __launch_bounds__(128) optics_sw_aod_kernel(const __grid_constant__ OpticsSwArgs w) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= w.ncol)
+    return;
+  const size_t n = (size_t)w.base.ncell;
+  double s = 0.0;
+  for (int k = 0; k < w.nlev; ++k) {
+    const size_t c = (size_t)col * w.nlev + k;
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m)
+      s += w.base.scr[(SS_AOD + m) * n + c];
+  }
+  w.aodvis[col] = s;
+}
+
 }  // namespace mam4b
 
 // =============================================================== C ABI
@@ -1927,7 +2026,8 @@ struct mam4b_ctx {
   double *d_ck2, *d_abar, *d_lbar;
   int *d_npass;         // [cap_adj]: passes of each SOA loop
   double *d_optics_lw;  // longwave optics tables (opt::kTableDoubles), set by the host
-  double *d_optics_scr; // longwave optics per-cell sizes (OS_FIELDS per cell), grown
+  double *d_optics_sw;  // shortwave optics tables (opt::kSwTableDoubles), set by the host
+  double *d_optics_scr; // optics per-cell sizes (SS_FIELDS per cell), grown
   size_t cap_optics_scr;
   unsigned *d_bins;     // [2 kPassBins]: loops per pass count, start offsets
   int adj_soa_grid;
@@ -2242,6 +2342,7 @@ mam4b_status mam4b_destroy(mam4b_ctx *ctx) {
   cudaFree(ctx->d_bins);
   cudaFree(ctx->d_optics_lw);
   cudaFree(ctx->d_optics_scr);
+  cudaFree(ctx->d_optics_sw);
   if (ctx->host_streams) {
     for (int k = 0; k < kHostStreams; ++k) {
       cudaStreamDestroy(ctx->hs[k]);
@@ -2737,6 +2838,96 @@ mam4b_status mam4b_optics_lw_set_tables(mam4b_ctx *ctx, const mam4b_optics_lw_ta
   free(h);
   if (e != cudaSuccess)
     return set_err(ctx, MAM4B_ERR_CUDA, what, e);
+  return MAM4B_OK;
+}
+
+// shortwave optics tables (layouts of mam4b_optics_sw_tables)
+mam4b_status mam4b_optics_sw_set_tables(mam4b_ctx *ctx, const mam4b_optics_sw_tables *t) {
+  const char *what = "mam4b_optics_sw_set_tables";
+  if (!ctx || !t || !t->specrefindex || !t->water_refindex || !t->refrtab || !t->refitab ||
+      !t->extp || !t->absp || !t->asmp)
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, what, cudaSuccess);
+  double *h = (double *)malloc(sizeof(double) * opt::kSwTableDoubles);
+  if (!h)
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_optics_sw_set_tables: host memory",
+                   cudaSuccess);
+  memset(h, 0, sizeof(double) * opt::kSwTableDoubles);
+  for (int m = 0; m < NMODE; ++m)
+    for (int s = 0; s < K::nspec(m); ++s)
+      for (int b = 0; b < opt::kSwBands; ++b) {
+        const int type = act::spectype(m, s) - 1;
+        const size_t src = 2 * ((size_t)b * MAM4B_OPTICS_NTYPES + type);
+        h[opt::kSwSpecRe + (m * 7 + s) * opt::kSwBands + b] = t->specrefindex[src];
+        h[opt::kSwSpecIm + (m * 7 + s) * opt::kSwBands + b] = t->specrefindex[src + 1];
+      }
+  for (int b = 0; b < opt::kSwBands; ++b) {
+    h[opt::kSwWaterRe + b] = t->water_refindex[2 * b];
+    h[opt::kSwWaterIm + b] = t->water_refindex[2 * b + 1];
+  }
+  memcpy(h + opt::kSwRefr, t->refrtab, sizeof(double) * 4 * opt::kSwBands * opt::kPrefr);
+  memcpy(h + opt::kSwRefi, t->refitab, sizeof(double) * 4 * opt::kSwBands * opt::kPrefi);
+  memcpy(h + opt::kSwExt, t->extp, sizeof(double) * 4 * opt::kSwBands * opt::kSwTab);
+  memcpy(h + opt::kSwAbs, t->absp, sizeof(double) * 4 * opt::kSwBands * opt::kSwTab);
+  memcpy(h + opt::kSwAsm, t->asmp, sizeof(double) * 4 * opt::kSwBands * opt::kSwTab);
+  cudaError_t e = cudaSuccess;
+  if (!ctx->d_optics_sw)
+    e = cudaMalloc(&ctx->d_optics_sw, sizeof(double) * opt::kSwTableDoubles);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(ctx->d_optics_sw, h, sizeof(double) * opt::kSwTableDoubles,
+                   cudaMemcpyHostToDevice);
+  free(h);
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, what, e);
+  return MAM4B_OK;
+}
+
+// modal_aero_opt::modal_aero_sw (modal_aero_opt.hpp:536-878), batched
+mam4b_status mam4b_optics_sw(mam4b_ctx *ctx, const double *in_slab, size_t ld,
+                             const double *pdeldry, double *out, double *aodvis, int ncol,
+                             int nlev, double dt, void *stream) {
+  const char *what = "mam4b_optics_sw";
+  const size_t n = (size_t)(ncol > 0 ? ncol : 0) * (size_t)(nlev > 0 ? nlev : 0);
+  if (!ctx || !in_slab || !pdeldry || !out || ncol < 0 || nlev <= 0 || ld < n || !(dt > 0.0) ||
+      !isfinite(dt))
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, what, cudaSuccess);
+  if (!ctx->d_optics_sw)
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_optics_sw: tables not set",
+                   cudaSuccess);
+  OpticsSwArgs w;
+  memset(&w, 0, sizeof(w));
+  for (int f = 0; f < MAM4B_NIN; ++f)
+    w.base.in[f] = in_slab + (size_t)f * ld;
+  w.base.pdeldry = pdeldry;
+  w.base.tables = ctx->d_optics_sw;
+  w.base.ld = ld;
+  w.base.ncell = (long long)n;
+  w.base.dt = dt;
+  w.out = out;
+  w.aodvis = aodvis;
+  w.ncol = ncol;
+  w.nlev = nlev;
+  cudaStream_t s = (cudaStream_t)stream;
+  ctx->last_stream = s;
+  if (n == 0)
+    return MAM4B_OK;
+  cudaError_t e = grow(&ctx->d_optics_scr, &ctx->cap_optics_scr, (size_t)SS_FIELDS * n);
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_optics_sw scratch", e);
+  w.base.scr = ctx->d_optics_scr;
+  const int block = 128;
+  const unsigned grid = (unsigned)((n + block - 1) / block);
+  optics_size_kernel<<<grid, block, 0, s>>>(w.base);
+  optics_sw_mode_kernel<<<dim3(grid, NMODE), block, 0, s>>>(w);
+  optics_sw_band_kernel<<<dim3(grid, opt::kSwBands), block, 0, s>>>(w);
+  int launches = 3;
+  if (aodvis) {
+    optics_sw_aod_kernel<<<(unsigned)((ncol + block - 1) / block), block, 0, s>>>(w);
+    ++launches;
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, what, e);
+  ctx->launches += launches;
   return MAM4B_OK;
 }
 

@@ -71,6 +71,12 @@ class OpticsLwTables(ctypes.Structure):
                 ("absp", ctypes.c_void_p)]
 
 
+class OpticsSwTables(ctypes.Structure):
+    """mam4b_optics_sw_tables (host pointers)."""
+    _fields_ = [(k, ctypes.c_void_p) for k in ("specrefindex", "water_refindex", "refrtab",
+                                               "refitab", "extp", "absp", "asmp")]
+
+
 class CalcSizeConfig(ctypes.Structure):
     """mam4b_calcsize_config: CalcSize::Config (src/mam4xx/calcsize.hpp:835-842)."""
     _fields_ = [("do_aitacc_transfer", ctypes.c_int), ("do_adjust", ctypes.c_int)]
@@ -112,6 +118,10 @@ def lib():
         L.mam4b_optics_lw_set_tables.restype = I
         L.mam4b_optics_lw.argtypes = [P, P, S, P, P, I, I, D, P]
         L.mam4b_optics_lw.restype = I
+        L.mam4b_optics_sw_set_tables.argtypes = [P, ctypes.POINTER(OpticsSwTables)]
+        L.mam4b_optics_sw_set_tables.restype = I
+        L.mam4b_optics_sw.argtypes = [P, P, S, P, P, P, I, I, D, P]
+        L.mam4b_optics_sw.restype = I
         L.mam4b_activate.argtypes = [P, P, S, P, P, P, I, I, P]
         L.mam4b_activate.restype = I
         L.mam4b_setsox.argtypes = [P, P, P, P, P, P, P, P, P, S, P, P, I, I, D, P]
@@ -135,7 +145,8 @@ EXPORTED = ["mam4b_abi_version", "mam4b_default_config", "mam4b_create", "mam4b_
             "mam4b_last_error", "mam4b_launch_count", "mam4b_step_slab_noalloc",
             "mam4b_adjoint_slab", "mam4b_calcsize_process", "mam4b_coagulation_process",
             "mam4b_step_tracers", "mam4b_setsox", "mam4b_activate",
-            "mam4b_optics_lw_set_tables", "mam4b_optics_lw"]
+            "mam4b_optics_lw_set_tables", "mam4b_optics_lw", "mam4b_optics_sw_set_tables",
+            "mam4b_optics_sw"]
 
 
 def default_config(**overrides):
@@ -243,6 +254,24 @@ class Context:
         st = self._lib.mam4b_optics_lw(self._h, in_ptr, int(ld), pdeldry, tauxar, int(ncol),
                                        int(nlev), float(dt), ctypes.c_void_p(stream))
         self._check(st, "mam4b_optics_lw")
+
+    def optics_sw_set_tables(self, tables):
+        """Copies the shortwave optics tables (dict of numpy arrays, see
+        workloads.make_optics_sw_tables) into the context."""
+        import numpy as np
+        keys = ("specrefindex", "water_refindex", "refrtab", "refitab", "extp", "absp", "asmp")
+        arrs = {k: np.ascontiguousarray(tables[k], dtype=np.float64) for k in keys}
+        t = OpticsSwTables(*[arrs[k].ctypes.data for k in keys])
+        st = self._lib.mam4b_optics_sw_set_tables(self._h, ctypes.byref(t))
+        self._check(st, "mam4b_optics_sw_set_tables")
+
+    def optics_sw(self, in_ptr, ld, pdeldry, out, aodvis, ncol, nlev, dt, stream=0):
+        """Shortwave optics (mam4b_optics_sw); device pointers, out [4][14][ld],
+        aodvis [ncol] or 0."""
+        st = self._lib.mam4b_optics_sw(self._h, in_ptr, int(ld), pdeldry, out, aodvis or None,
+                                       int(ncol), int(nlev), float(dt),
+                                       ctypes.c_void_p(stream))
+        self._check(st, "mam4b_optics_sw")
 
     def activate(self, in_ptr, ld, air_density, updraft, out, ncol, nlev, stream=0):
         """Aerosol activation fractions (mam4b_activate); device pointers,

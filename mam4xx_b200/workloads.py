@@ -291,3 +291,30 @@ def make_optics_lw_tables(seed=0):
     absp[:, :, 0] = rng.uniform(500.0, 2000.0, (4, nb, 7, 10))
     return {"specrefindex": np.ascontiguousarray(spec), "water_refindex": water,
             "refrtab": refr, "refitab": refi, "absp": absp}
+
+
+def make_optics_sw_tables(seed=0):
+    """Seeded stand-ins for the shortwave optics tables (shapes and value
+    ranges of the host model's files, not their data): refractive indices
+    (real 1.3..1.8, imaginary 1e-8..0.1), water (1.33, 1e-9..1e-6), grids
+    as for the longwave, and Chebyshev coefficients of log specific
+    extinction (first one 2..10), absorption and asymmetry."""
+    rng = np.random.default_rng(5151 + seed)
+    nb, nt = 14, 14
+    spec = np.empty((nb, nt, 2))
+    spec[..., 0] = rng.uniform(1.3, 1.8, (nb, nt))
+    spec[..., 1] = _logu(rng, 1e-8, 0.1, nb * nt).reshape(nb, nt)
+    water = np.empty((nb, 2))
+    water[:, 0] = 1.33
+    water[:, 1] = _logu(rng, 1e-9, 1e-6, nb)
+    refr = np.sort(rng.uniform(1.2, 2.0, (4, nb, 7)), axis=2)
+    refr[..., 0], refr[..., -1] = 1.2, 2.0
+    refi = np.sort(_logu(rng, 1e-9, 1.0, 4 * nb * 10).reshape(4, nb, 10), axis=2)
+    extp = rng.normal(0.0, 0.5, (4, nb, 5, 7, 10))
+    extp[:, :, 0] = rng.uniform(2.0, 10.0, (4, nb, 7, 10))
+    absp = rng.normal(0.0, 50.0, (4, nb, 5, 7, 10))
+    absp[:, :, 0] = rng.uniform(10.0, 500.0, (4, nb, 7, 10))
+    asmp = rng.normal(0.0, 0.1, (4, nb, 5, 7, 10))
+    asmp[:, :, 0] = rng.uniform(0.8, 1.6, (4, nb, 7, 10))
+    return {"specrefindex": np.ascontiguousarray(spec), "water_refindex": water,
+            "refrtab": refr, "refitab": refi, "extp": extp, "absp": absp, "asmp": asmp}

@@ -173,6 +173,24 @@ class ReferenceOracle(_Oracle):
         f(n, x.ctypes.data, pd.ctypes.data, dt, *[a.ctypes.data for a in t], tau.ctypes.data)
         return tau
 
+    def optics_sw(self, ncol, nlev, in_slab, pdeldry, dt, tables):
+        """modal_aero_sw per cell with its mode and column sums; returns
+        (out (4, 14, ncell): tauxar, wa, ga, fa; aod (ncol,))."""
+        x = np.ascontiguousarray(in_slab, dtype=np.float64)
+        n = x.shape[1]
+        out = np.zeros((4, 14, n))
+        aod = np.zeros(ncol)
+        pd = np.ascontiguousarray(pdeldry, dtype=np.float64)
+        t = [np.ascontiguousarray(tables[k], dtype=np.float64)
+             for k in ("specrefindex", "water_refindex", "refrtab", "refitab", "extp", "absp",
+                       "asmp")]
+        f = self.lib.mam4ref_optics_sw
+        f.argtypes = [_I, _I, _P, _P, _D] + [_P] * 9
+        f.restype = None
+        f(ncol, nlev, x.ctypes.data, pd.ctypes.data, dt, *[a.ctypes.data for a in t],
+          out.ctypes.data, aod.ctypes.data)
+        return out, aod
+
     def maxsat(self, zeta, eta, smc):
         """ndrop::maxsat for 4 modes."""
         f = self.lib.mam4ref_maxsat

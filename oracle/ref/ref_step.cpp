@@ -498,6 +498,80 @@ void mam4ref_optics_lw(int ncell, const double *in, const double *pdeldry, doubl
   }
 }
 
+// modal_aero_opt::modal_aero_sw_wo_diagnostics_k per cell, then the mode
+// sums and the visible-band column sum of modal_aero_sw (same order:
+// modes 0..3; levels top down, modes within each level). out [4][14][ncell]
+// (tauxar, wa, ga, fa); aod [ncol].
+void mam4ref_optics_sw(int ncol, int nlev, const double *in, const double *pdeldry, double dt,
+                       const double *specref, const double *water, const double *refr,
+                       const double *refi, const double *extp, const double *absp,
+                       const double *asmp, double *out, double *aod) {
+  using namespace mam4::modal_aero_opt;
+  AerosolOpticsDeviceData d;
+  set_aerosol_optics_data_for_modal_aero_sw_views(d);
+  set_complex_views_modal_aero(d);
+  ComplexView2D::host_mirror_type host("specrefndx", nswbands, mam4::ndrop::maxd_aspectype);
+  for (int b = 0; b < nswbands; ++b)
+    for (int t = 0; t < mam4::ndrop::maxd_aspectype; ++t)
+      host(b, t) = Kokkos::complex<Real>(specref[2 * (b * 14 + t)], specref[2 * (b * 14 + t) + 1]);
+  set_device_specrefindex(d.specrefindex_sw, "short_wave", host);
+  for (int b = 0; b < nswbands; ++b)
+    d.crefwsw(b) = Kokkos::complex<Real>(water[2 * b], water[2 * b + 1]);
+  for (int m = 0; m < 4; ++m)
+    for (int b = 0; b < nswbands; ++b) {
+      for (int i = 0; i < prefr; ++i)
+        d.refrtabsw[m][b](i) = refr[(m * nswbands + b) * prefr + i];
+      for (int j = 0; j < prefi; ++j)
+        d.refitabsw[m][b](j) = refi[(m * nswbands + b) * prefi + j];
+      for (int c = 0; c < ncoef; ++c)
+        for (int i = 0; i < prefr; ++i)
+          for (int j = 0; j < prefi; ++j) {
+            const size_t k = (((size_t)(m * nswbands + b) * ncoef + c) * prefr + i) * prefi + j;
+            d.extpsw[m][b](c, i, j) = extp[k];
+            d.abspsw[m][b](c, i, j) = absp[k];
+            d.asmpsw[m][b](c, i, j) = asmp[k];
+          }
+    }
+  const CalcsizeData &cd = calcsize_data();
+  const size_t n = (size_t)ncol * nlev;
+  std::vector<double> vis(n * 4);
+#pragma omp parallel for schedule(dynamic, 64)
+  for (long long cc = 0; cc < (long long)n; ++cc) {
+    const size_t c = (size_t)cc;
+    auto IN = [&](int f) { return in[(size_t)f * n + c]; };
+    Real state_q[40] = {}, qqcw[40] = {};
+    state_q[0] = IN(MAM4B_IN_QV);
+    state_q[11] = IN(MAM4B_IN_H2SO4);
+    state_q[14] = IN(MAM4B_IN_SOAG);
+    for (int p = 0; p < MAM4B_NUM_POPS; ++p) {
+      state_q[15 + p] = IN(MAM4B_IN_AER_I + p);
+      qqcw[15 + p] = IN(MAM4B_IN_AER_C + p);
+    }
+    Real cld = IN(MAM4B_IN_CLD);
+    View2D t("t", 4, nswbands), wa("wa", 4, nswbands), ga("ga", 4, nswbands),
+        fa("fa", 4, nswbands);
+    modal_aero_sw_wo_diagnostics_k(pdeldry[c], IN(MAM4B_IN_P), IN(MAM4B_IN_T), cld, state_q,
+                                   qqcw, dt, d, cd, t, wa, ga, fa);
+    const View2D *q4[4] = {&t, &wa, &ga, &fa};
+    for (int q = 0; q < 4; ++q)
+      for (int b = 0; b < nswbands; ++b) {
+        Real sum = 0;
+        for (int m = 0; m < 4; ++m)
+          sum += (*q4[q])(m, b);
+        out[((size_t)q * nswbands + b) * n + c] = sum;
+      }
+    for (int m = 0; m < 4; ++m)
+      vis[c * 4 + m] = t(m, idx_sw_diag);
+  }
+  for (int col = 0; col < ncol; ++col) {
+    Real s = 0;
+    for (int k = 0; k < nlev; ++k)
+      for (int m = 0; m < 4; ++m)
+        s += vis[((size_t)col * nlev + k) * 4 + m];
+    aod[col] = s;
+  }
+}
+
 double mam4ref_maxsat(double zeta, const double *eta, const double *smc) {
   Real e[4], sm[4], smax = 0;
   for (int m = 0; m < 4; ++m) {

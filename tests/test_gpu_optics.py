@@ -1,6 +1,8 @@
-"""Longwave aerosol optics on the GPU (mam4b_optics_lw) against the
-reference's own modal_aero_opt::modal_aero_lw_k compiled unchanged for the
-host (oracle/_ref), both given the same seeded stand-in tables (the host
+"""Aerosol optics on the GPU (mam4b_optics_lw, mam4b_optics_sw) against
+the reference's own modal_aero_opt::modal_aero_lw_k and
+modal_aero_sw_wo_diagnostics_k (with modal_aero_sw's mode and column sums)
+compiled unchanged for the host (oracle/_ref), both given the same seeded
+stand-in tables (the host
 model's optics files are not in the repository). The mode sizes come from
 calcsize and the water-uptake quartic, whose math-library sensitivity the
 step's parity tests measure; the bar here is 1e-10 relative (floor 1e-30)
@@ -42,3 +44,32 @@ def test_optics_lw_needs_tables(cuda_device):
     t = torch.zeros((native.NIN, 4), dtype=torch.float64, device="cuda")
     with pytest.raises(native.MicrophysicsError, match="tables not set"):
         ctx.optics_lw(t.data_ptr(), 4, t.data_ptr(), t.data_ptr(), 1, 4, 1800.0)
+
+
+@pytest.mark.parametrize("name,ncol", [("c2", 128), ("c4", 128)])
+def test_optics_sw_matches_reference(cuda_device, ref_oracle, name, ncol):
+    from mam4xx_b200.workloads import make_optics_sw_tables
+    w = make_workload(name, ncol=ncol, seed=41)
+    tb = make_optics_sw_tables(seed=2)
+    x = w["in_slab"]
+    n = x.shape[1]
+    pdel = np.random.default_rng(4).uniform(100.0, 3000.0, n)
+    ctx = native.Context()
+    ctx.optics_sw_set_tables(tb)
+    xd = torch.from_numpy(x).cuda()
+    pd = torch.from_numpy(pdel).cuda()
+    out = torch.full((4, 14, n), float("nan"), dtype=torch.float64, device="cuda")
+    aod = torch.full((w["ncol"],), float("nan"), dtype=torch.float64, device="cuda")
+    ctx.optics_sw(xd.data_ptr(), n, pd.data_ptr(), out.data_ptr(), aod.data_ptr(), w["ncol"],
+                  w["nlev"], w["dt"])
+    torch.cuda.synchronize()
+    g, ga = out.cpu().numpy(), aod.cpu().numpy()
+    r, ra = ref_oracle.optics_sw(w["ncol"], w["nlev"], x, pdel, w["dt"], tb)
+    assert np.isfinite(g).all() and np.isfinite(ga).all()
+    # wa, ga, fa are the optical depth times the albedo 1 - absorption /
+    # extinction and the asymmetry, which cancel when absorption nears
+    # extinction: their error is measured against the band's optical depth
+    scale = np.maximum(np.abs(r), np.abs(r[0])[None])
+    err = np.abs(g - r) / np.maximum(scale, 1e-30)
+    assert err.max() <= 1e-10, (err.max(), np.quantile(err, 0.99))
+    np.testing.assert_allclose(ga, ra, rtol=1e-10)
