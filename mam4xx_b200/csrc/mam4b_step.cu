@@ -1210,7 +1210,7 @@ MAM4B_HD double &sb_ref(Sub &b, int j) {
   return b.gas[1];
 }
 
-__global__ void __launch_bounds__(128) adj_post_kernel(const __grid_constant__ AdjPipeArgs p) {
+__global__ void __launch_bounds__(128, 4) adj_post_kernel(const __grid_constant__ AdjPipeArgs p) {
   const StepArgs &a = p.s;
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (long long)a.counters[CNT_QUEUED])
@@ -1454,6 +1454,10 @@ __global__ void __launch_bounds__(kSoaBlock, 2) adj_soa_kernel(const __grid_cons
   }
 }
 
+// The whole-cell reverse kernels (adj_post, adj_pre, adj_fin) run 4 blocks
+// of 128 per SM (128 registers, their tapes in L1-cached local memory):
+// 2.8 ms faster in total than unconstrained at 255 registers.
+//
 // Reverse of each cell's front (and of cloudy cells entirely), up to the
 // water uptake: the front's forward sweep takes water uptake, diffusivity
 // and uptake rates from the forward pipeline (out rows, aux), the
@@ -1464,7 +1468,7 @@ enum { FT_PT_IB = 0, FT_PT_CB = 25, FT_DGN_AB = 50, FT_DGN_AWETB = 54, FT_QAERWA
        FT_WETDENS_WUB = 62, FT_RHB = 66, FT_FIELDS = 70 };
 static_assert(FT_FIELDS <= AB_FIELDS, "front hand-off must fit in abar");
 
-__global__ void __launch_bounds__(128) adj_pre_kernel(const __grid_constant__ AdjPipeArgs p) {
+__global__ void __launch_bounds__(128, 4) adj_pre_kernel(const __grid_constant__ AdjPipeArgs p) {
   const StepArgs &a = p.s;
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= a.ncell)
@@ -1587,7 +1591,7 @@ __global__ void __launch_bounds__(128) adj_mode_kernel(const __grid_constant__ A
 }
 
 // Last part of the reverse, per cell: RH of water uptake and calcsize.
-__global__ void __launch_bounds__(128) adj_fin_kernel(const __grid_constant__ AdjPipeArgs p) {
+__global__ void __launch_bounds__(128, 4) adj_fin_kernel(const __grid_constant__ AdjPipeArgs p) {
   const StepArgs &a = p.s;
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= a.ncell)
