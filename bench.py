@@ -187,6 +187,8 @@ def cpu_baseline(x, pblh_cell, dt, target_s=12.0):
 # gas tracers, 3 cloud-borne SO4 and 6 tendencies
 PROCESS_BYTES_PER_CELL = {"calcsize": (50 + 20 + 24 + 8) * 8, "coagulation": (42 + 32 + 64) * 8,
                           "setsox": (6 + 4 + 7 + 3 + 3 + 6) * 8,
+                          "gas_chemistry": (2 + 9 + 8 + 30 + 30 + 30) * 8,
+                          "step_chem": (57 + 55 + 68 + 4) * 8,
                           "activation": (28 + 17) * 8, "optics_lw": (55 + 16) * 8,
                           "optics_sw": (55 + 56) * 8}
 
@@ -239,6 +241,29 @@ def processes_leg(native, torch, dev, stream, args, ws, hbm_peak):
                    sx_d[0].data_ptr(), sx_d[3].data_ptr(), ncol, NLEV, d["dt"],
                    stream=stream.cuda_stream)
 
+    from mam4xx_b200.workloads import make_gas_chemistry_inputs
+    gc = make_gas_chemistry_inputs(WORKLOAD, ncol=ncol, seed=20261203 + 9)
+    gc_dev = {k: torch.from_numpy(np.ascontiguousarray(gc[k])).to(dev)
+              for k in ("temp", "photo", "extfrc", "inv", "het", "qq")}
+
+    def gas_chemistry():
+        # repeated calls keep reacting the same cells' state (fine for timing)
+        ctx.gas_chemistry(*[gc_dev[k].data_ptr() for k in ("temp", "photo", "extfrc", "inv",
+                                                            "het", "qq")],
+                          n, ncol, NLEV, gc["dt"], stream=stream.cuda_stream)
+
+    from mam4xx_b200.workloads import make_chem_step_inputs
+    cw = make_chem_step_inputs(WORKLOAD, ncol=ncol, seed=20261203 + 10)
+    cw_x = torch.from_numpy(cw["in_slab"]).to(dev)
+    cw_pb = torch.from_numpy(cw["pblh"]).to(dev)
+    cw_ch = torch.from_numpy(cw["chem_in"]).to(dev)
+    cw_out = torch.empty((native.NOUT, n), dtype=torch.float64, device=dev)
+    cw_cout = torch.empty((native.CHEM_NOUT, n), dtype=torch.float64, device=dev)
+
+    def step_chem():
+        ctx.step_chem_slab(cw_x.data_ptr(), cw_pb.data_ptr(), cw_ch.data_ptr(), cw_out.data_ptr(),
+                           cw_cout.data_ptr(), n, ncol, NLEV, cw["dt"], stream=stream.cuda_stream)
+
     from mam4xx_b200.workloads import make_activation_inputs
     ac = make_activation_inputs(WORKLOAD, ncol=ncol, seed=20261203 + 6)
     ac_x = torch.from_numpy(ac["in_slab"]).to(dev)
@@ -274,8 +299,9 @@ def processes_leg(native, torch, dev, stream, args, ws, hbm_peak):
 
     res = {}
     for name, f in (("calcsize", calcsize), ("coagulation", coag), ("setsox", setsox),
-                    ("activation", activation), ("optics_lw", optics_lw),
-                    ("optics_sw", optics_sw)):
+                    ("gas_chemistry", gas_chemistry), ("step_chem", step_chem),
+                    ("activation", activation),
+                    ("optics_lw", optics_lw), ("optics_sw", optics_sw)):
         for _ in range(args.warmup):
             f()
         if ws > 1:
@@ -326,10 +352,17 @@ def processes_leg(native, torch, dev, stream, args, ws, hbm_peak):
             t5 = time.perf_counter()
             r.optics_sw(nc, NLEV, ow["in_slab"][:, sl], opd.cpu().numpy()[sl], d["dt"], sw_tables)
             t6 = time.perf_counter()
+            r.gas_chemistry(gc["dt"], *[gc[k][..., sl] for k in ("temp", "photo", "extfrc", "inv",
+                                                                  "het", "qq")])
+            t7 = time.perf_counter()
+            from mam4xx_b200.workloads import pblh_per_cell
+            r.step_chem(cw["in_slab"][:, sl], pblh_per_cell(cw)[sl], cw["chem_in"][:, sl], cw["dt"])
+            t8 = time.perf_counter()
             import multiprocessing
             for name, el in (("calcsize", t1 - t0), ("coagulation", t2 - t1),
                              ("setsox", t3 - t2), ("activation", t4 - t3),
-                             ("optics_lw", t5 - t4), ("optics_sw", t6 - t5)):
+                             ("optics_lw", t5 - t4), ("optics_sw", t6 - t5),
+                             ("gas_chemistry", t7 - t6), ("step_chem", t8 - t7)):
                 res[name]["cpu_baseline"] = {
                     "value": m / el, "unit": "cells/s", "kind": "reference",
                     "cores": multiprocessing.cpu_count(),

@@ -426,6 +426,72 @@ mam4b_status mam4b_setsox(mam4b_ctx *ctx, const double *pressure, const double *
                           int ncol, int nlev, double dt, void *stream);
 
 /*
+ * Gas-phase chemistry, batched over cells:
+ * mam4::microphysics::gas_phase_chemistry (src/mam4xx/gas_phase_chemistry.hpp:
+ * 40-117), the chemistry stage that runs before cloud chemistry and
+ * amicphys in the host model, for the mechanism of
+ * src/mam4xx/gas_chem_mechanism.hpp: reaction rates (setrxt, usrrxt,
+ * adjrxt), then imp_sol's implicit Euler step with Newton-Raphson iteration
+ * and step control (src/mam4xx/gas_chem.hpp:262-426).
+ *
+ *   temperature [K], photo_rates (the one photolysis rate, of H2O2, 1/s):
+ *              one value per cell
+ *   extfrc     [MAM4B_GAS_EXTCNT][ld] external forcing [molecules/cm3/s]
+ *   invariants [MAM4B_GAS_NFS][ld] invariant densities [molecules/cm3]
+ *              (0 total air, 1 N2, 2 O2, 3 H2O, 4 OH, 5 NO3, 6 HO2, 7 O3:
+ *              mo_setinv::setinv_single_level)
+ *   het_rates  [MAM4B_GAS_PCNST][ld] wet-removal rates [1/s] (row 0 unused)
+ *   qq         [MAM4B_GAS_PCNST][ld] the 31 tracers [mol/mol, #/kmol],
+ *              updated in place (tracer 0, O3, is neither read nor written)
+ * Asynchronous on `stream`.
+ */
+#define MAM4B_GAS_EXTCNT 9
+#define MAM4B_GAS_NFS 8
+mam4b_status mam4b_gas_chemistry(mam4b_ctx *ctx, const double *temperature,
+                                 const double *photo_rates, const double *extfrc,
+                                 const double *invariants, const double *het_rates, double *qq,
+                                 size_t ld, int ncol, int nlev, double dt, void *stream);
+
+/*
+ * The step with the chemistry that precedes amicphys in the host model,
+ * fused per cell: calcsize, water uptake and the calcsize update as in
+ * mam4b_step; then gas-phase chemistry (gas_phase_chemistry, as
+ * mam4b_gas_chemistry) and aqueous chemistry (setsox_single_level, as
+ * mam4b_setsox) on the cell's 31 tracers; then modal_aero_amicphys_intr
+ * (src/mam4xx/mam4_amicphys.hpp:2120) with the states the chemistry leaves:
+ * q_pregaschem before gas chemistry, q_precldchem and qqcw_precldchem before
+ * aqueous chemistry, qq and qqcw after it. With distinct states the
+ * H2SO4 production of the other processes (gaexch_h2so4_uptake_optaa = 2)
+ * feeds condensation, and cloud-chemistry growth feeds renaming.
+ *
+ *   in_slab, pblh, out_slab  the step's layouts (MAM4B_NIN / MAM4B_NOUT
+ *              fields of ld doubles); out_slab's tendencies are relative to
+ *              the inputs, so they include the chemistry
+ *   chem_in    MAM4B_CHEM_NIN fields of ld doubles (below); the total air
+ *              density of aqueous chemistry is the invariant density 0
+ *   chem_out   MAM4B_CHEM_NOUT fields of ld doubles: tendencies [kg/kg/s]
+ *              of O3 (zero: neither chemistry changes it), H2O2, SO2, DMS
+ * FP64, one thread per cell. Asynchronous on `stream`.
+ */
+enum {
+  MAM4B_CHEM_IN_O3 = 0,      /* O3, H2O2, SO2, DMS mass mixing ratios [kg/kg] */
+  MAM4B_CHEM_IN_H2O2 = 1,
+  MAM4B_CHEM_IN_SO2 = 2,
+  MAM4B_CHEM_IN_DMS = 3,
+  MAM4B_CHEM_IN_PHOTO = 4,   /* H2O2 photolysis rate [1/s] */
+  MAM4B_CHEM_IN_EXTFRC = 5,  /* MAM4B_GAS_EXTCNT external forcings [molecules/cm3/s] */
+  MAM4B_CHEM_IN_INV = 14,    /* MAM4B_GAS_NFS invariant densities [molecules/cm3] */
+  MAM4B_CHEM_IN_HET = 22,    /* MAM4B_GAS_PCNST wet-removal rates [1/s] (first unused) */
+  MAM4B_CHEM_IN_LWC = 53,    /* cloud liquid water [kg/kg] */
+  MAM4B_CHEM_IN_CLDNUM = 54, /* cloud droplet number [#/kg] */
+  MAM4B_CHEM_NIN = 55
+};
+enum { MAM4B_CHEM_OUT_TEND = 0, MAM4B_CHEM_NOUT = 4 };
+mam4b_status mam4b_step_chem_slab(mam4b_ctx *ctx, const double *in_slab, const double *pblh,
+                                  const double *chem_in, double *out_slab, double *chem_out,
+                                  size_t ld, int ncol, int nlev, double dt, void *stream);
+
+/*
  * Per-process entries: the batched form of two mam4xx AeroProcess
  * implementations, for host models that call the processes one at a time
  * instead of the whole step. Their state is Prognostics-style: one device

@@ -25,6 +25,7 @@
 #include "mam4b_adjoint.cuh"
 #include "mam4b_process.cuh"
 #include "mam4b_setsox.cuh"
+#include "mam4b_gaschem.cuh"
 #include "mam4b_activation.cuh"
 #include "mam4b_optics.cuh"
 
@@ -719,21 +720,261 @@ __device__ __forceinline__ void cell_step(const StepArgs &a, const long long c) 
   }
 }
 
+// ---- the step with the chemistry that precedes amicphys, one thread per
+// cell: calcsize and water uptake, the calcsize update, then gas-phase
+// chemistry (gas_phase_chemistry.hpp:40) and aqueous chemistry
+// (mo_setsox.hpp:944) on the cell's 31 tracers, then amicphys with the three
+// states the chemistry leaves: before gas chemistry (q_pregaschem), before
+// cloud chemistry (q_precldchem, qqcw_precldchem) and after it (qq, qqcw).
+struct ChemArgs {
+  const double *in;  // [MAM4B_CHEM_NIN][ld]
+  double *out;       // [MAM4B_CHEM_NOUT][ld]
+  size_t ld;
+};
+
+// amicphys-unit states before the chemistry, clipped at zero as amicphys
+// clips its inputs (mam4_amicphys.hpp:2258-2267)
+struct ChemPre {
+  double g1[2];               // SOAG, H2SO4 before gas chemistry
+  double g2[2];               // SOAG, H2SO4 before cloud chemistry
+  double qi2[NPOP], qc2[NPOP];  // populations before cloud chemistry
+};
+
+// Renaming in a cloudy (sub)area whose populations grew by cloud chemistry:
+// the growth increments of the aitken mode are the change from the
+// before-cloud-chemistry state (mam4_amicphys.hpp:1440-1455; no
+// condensation in a cloudy subarea).
+__device__ __forceinline__ void cloudy_rename_grown(const StepArgs &a, Sub &si, Sub &sc,
+                                                    const Sub &si2, const Sub &sc2) {
+  const StepConsts &C = c_k;
+  si.gas[0] = si.gas[1] = sc.gas[0] = sc.gas[1] = 0.0;
+  if (!a.do_rename)
+    return;
+  double gi[NAER], gc[NAER];
+#pragma unroll
+  for (int x = 0; x < NAER; ++x) {
+    gi[x] = (si.aer[x][1] - si2.aer[x][1]) / 1 + 0.0;
+    gc[x] = (sc.aer[x][1] - sc2.aer[x][1]) / 1;
+  }
+  rename_subarea<true>(C, si, sc, gi, gc);
+}
+
+// Cloudy grid cell (cloud fraction > 0.999) after chemistry.
+__device__ __forceinline__ void cloudy_cell_chem(const StepArgs &a, const Front &f,
+                                                 const ChemPre &cp, double &o_h2so4,
+                                                 double &o_soag, double (&oi)[NPOP],
+                                                 double (&oc)[NPOP]) {
+  Sub si, sc;
+  load_sub_plain(si, f.qi);
+  load_sub_plain(sc, f.qc);
+  {
+    Sub si2, sc2;
+    load_sub_plain(si2, cp.qi2);
+    load_sub_plain(sc2, cp.qc2);
+    cloudy_rename_grown(a, si, sc, si2, sc2);
+  }
+  const double w = 1.0;
+  o_soag = dmax(0.0, 0.0 + f.g_soag * w);
+  o_h2so4 = dmax(0.0, 0.0 + f.g_h2so4 * w);
+#pragma unroll
+  for (int m = 0; m < NMODE; ++m) {
+    oi[K::numslot(m)] = dmax(0.0, 0.0 + (si.num[m] / 1.0) * w);
+    oc[K::numslot(m)] = 0.0 + (sc.num[m] / 1.0) * w;
+#pragma unroll
+    for (int x = 0; x < NAER; ++x) {
+      const int slot = K::aer_slot(x, m);
+      if (slot >= 0) {
+        oi[slot] = dmax(0.0, 0.0 + (si.aer[x][m] / K::fcvt_aer(x)) * w);
+        oc[slot] = 0.0 + (sc.aer[x][m] / K::fcvt_aer(x)) * w;
+      }
+    }
+  }
+}
+
+// Partly cloudy grid cell after chemistry (set_subarea_gases_and_aerosols,
+// mam4_amicphys.hpp:679-911): the interstitial partition factors come from
+// the before-cloud-chemistry state and split both it and the current one;
+// gases keep their before-cloud-chemistry value in the clear subarea and
+// the cloudy subarea takes the remainder of the current grid mean
+// (compute_qsub_from_gcm_and_qsub_of_other_subarea, :367-408).
+__device__ __forceinline__ void partly_cloudy_setup_chem(const StepArgs &a, const Front &f,
+                                                         const ChemPre &cp, Sub &s,
+                                                         double (&gcl)[2], double &rhc,
+                                                         double (&ci)[NPOP], double (&cg)[2],
+                                                         double (&oc)[NPOP]) {
+  const StepConsts &C = c_k;
+  const double fcldy = f.cld, fclea = 1.0 - fcldy;
+  double fn_c[NMODE], fn_y[NMODE], fm_c[NMODE], fm_y[NMODE];
+  auto part = [&](double q_i, double q_c, double &fc, double &fy) {
+    const double cldbrn_cldy = q_c / fcldy;
+    const double intrst_cldy = dmax(0.0, ((q_i + q_c) - cldbrn_cldy));
+    const double intrst_clea = (q_i - fcldy * intrst_cldy) / fclea;
+    double r = dmax(1.e-35, intrst_clea * fclea) / dmax(1.e-35, q_i);
+    r = dmax(0.0, dmin(1.0, r));
+    fc = r / fclea;
+    fy = (1 - r) / fcldy;
+  };
+#pragma unroll
+  for (int m = 0; m < NMODE; ++m) {
+    part(cp.qi2[K::numslot(m)], cp.qc2[K::numslot(m)], fn_c[m], fn_y[m]);
+    double si_ = 0.0, sc_ = 0.0;
+#pragma unroll
+    for (int k = 0; k < K::nspec(m); ++k) {
+      si_ = si_ + cp.qi2[K::spec0(m) + k];
+      sc_ = sc_ + cp.qc2[K::spec0(m) + k];
+    }
+    part(si_, sc_, fm_c[m], fm_y[m]);
+  }
+  const double g3[2] = {f.g_soag, f.g_h2so4};
+  double gcy[2];
+#pragma unroll
+  for (int g = 0; g < 2; ++g) {
+    gcl[g] = cp.g2[g];
+    gcy[g] = (g3[g] - fclea * gcl[g]) / fcldy;
+    if (gcy[g] < 0) {
+      gcy[g] = 0;
+      gcl[g] = g3[g] / fclea;
+    }
+  }
+  rhc = bound(0.0, 1.0, (f.relhumgcm - fcldy) / fclea);
+  {
+    Sub si, sc, si2, sc2;
+    load_sub(si, f.qi, fn_y, fm_y);
+    load_sub(si2, cp.qi2, fn_y, fm_y);
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      sc.num[m] = (f.qc[K::numslot(m)] / fcldy) * 1;
+      sc2.num[m] = (cp.qc2[K::numslot(m)] / fcldy) * 1;
+#pragma unroll
+      for (int x = 0; x < NAER; ++x) {
+        const int slot = K::aer_slot(x, m);
+        sc.aer[x][m] = (slot >= 0) ? (f.qc[slot] / fcldy) * K::fcvt_aer(x) : 0.0;
+        sc2.aer[x][m] = (slot >= 0) ? (cp.qc2[slot] / fcldy) * K::fcvt_aer(x) : 0.0;
+      }
+    }
+    cloudy_rename_grown(a, si, sc, si2, sc2);
+    cg[0] = gcy[0] * fcldy;
+    cg[1] = gcy[1] * fcldy;
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      ci[K::numslot(m)] = (si.num[m] / 1.0) * fcldy;
+      oc[K::numslot(m)] = (0.0 + 0.0 * fclea) + (sc.num[m] / 1.0) * fcldy;
+#pragma unroll
+      for (int x = 0; x < NAER; ++x) {
+        const int slot = K::aer_slot(x, m);
+        if (slot >= 0) {
+          ci[slot] = (si.aer[x][m] / K::fcvt_aer(x)) * fcldy;
+          oc[slot] = (0.0 + 0.0 * fclea) + (sc.aer[x][m] / K::fcvt_aer(x)) * fcldy;
+        }
+      }
+    }
+  }
+  load_sub(s, f.qi, fn_c, fm_c);
+  s.gas[0] = gcl[0] * C.fcvt_soag;
+  s.gas[1] = gcl[1] * 1.0;
+}
+
+// amicphys tracer index of the gas-chemistry gases O3, H2O2, SO2, DMS
+__device__ __forceinline__ constexpr int chem_gas_i31(int g) { return g < 2 ? g : g + 1; }
+
+// The chemistry of a cell between its front (calcsize, water uptake, the
+// calcsize update) and amicphys: gas-phase chemistry, then aqueous
+// chemistry, on the cell's 31 tracers in vmr; cp receives the states before
+// each, f the state after both (clipped, as amicphys reads it), and the
+// four chemistry gases' tendencies are written.
+__device__ __forceinline__ void run_chemistry(const StepArgs &a, const ChemArgs &ch,
+                                              const long long c, Front &f, ChemPre &cp) {
+  const StepConsts &C = c_k;
+  const double dt = a.dt;
+  auto CIN = [&](int k) { return __ldg(ch.in + (size_t)k * ch.ld + c); };
+  double qq[31], qqcw[31];
+  double gas_in[4];
+#pragma unroll
+  for (int g = 0; g < 4; ++g) {
+    const int i = chem_gas_i31(g);
+    gas_in[g] = CIN(MAM4B_CHEM_IN_O3 + g);
+    qq[i] = gas_in[g] * (K::mw_dry_air / K::adv_mass(i));
+    qqcw[i] = 0.0;
+  }
+  qq[2] = f.h2so4 * C.to_vmr[0];
+  qq[5] = f.soag * C.to_vmr[1];
+  qqcw[2] = qqcw[5] = 0.0;
+#pragma unroll
+  for (int p = 0; p < NPOP; ++p) {
+    qq[6 + p] = f.qi[p];
+    qqcw[6 + p] = f.qc[p];
+  }
+  cp.g1[0] = dmax(0.0, qq[5]);
+  cp.g1[1] = dmax(0.0, qq[2]);
+  {  // gas-phase chemistry
+    double ext[gch::kExt], inv[gch::kInv];
+#pragma unroll
+    for (int e = 0; e < gch::kExt; ++e)
+      ext[e] = CIN(MAM4B_CHEM_IN_EXTFRC + e);
+#pragma unroll
+    for (int i = 0; i < gch::kInv; ++i)
+      inv[i] = CIN(MAM4B_CHEM_IN_INV + i);
+    const double *het_c = ch.in + (size_t)MAM4B_CHEM_IN_HET * ch.ld + c;
+    const size_t ld = ch.ld;
+    auto het = [het_c, ld](int t) { return __ldg(het_c + (size_t)t * ld); };
+    gch::gas_chemistry_cell(f.temp, dt, CIN(MAM4B_CHEM_IN_PHOTO), ext, inv, het, qq);
+  }
+  cp.g2[0] = dmax(0.0, qq[5]);
+  cp.g2[1] = dmax(0.0, qq[2]);
+#pragma unroll
+  for (int p = 0; p < NPOP; ++p) {
+    cp.qi2[p] = dmax(0.0, qq[6 + p]);
+    cp.qc2[p] = dmax(0.0, qqcw[6 + p]);
+  }
+  {  // cloud chemistry; the total air density is the invariant density of air
+    double dso4[3], dh2so4[3];
+    sox::setsox_cell(dt, f.pmid, f.temp, CIN(MAM4B_CHEM_IN_LWC), f.cld,
+                     CIN(MAM4B_CHEM_IN_CLDNUM), CIN(MAM4B_CHEM_IN_INV + 0), qq, qqcw, dso4,
+                     dh2so4);
+  }
+  f.g_soag = dmax(0.0, qq[5]);
+  f.g_h2so4 = dmax(0.0, qq[2]);
+#pragma unroll
+  for (int p = 0; p < NPOP; ++p) {
+    f.qi[p] = dmax(0.0, qq[6 + p]);
+    f.qc[p] = dmax(0.0, qqcw[6 + p]);
+  }
+  // the gases amicphys does not map keep the chemistry's result
+#pragma unroll
+  for (int g = 0; g < 4; ++g) {
+    const int i = chem_gas_i31(g);
+    ch.out[(size_t)(MAM4B_CHEM_OUT_TEND + g) * ch.ld + c] =
+        (qq[i] * (K::adv_mass(i) / K::mw_dry_air) - gas_in[g]) / dt;
+  }
+}
+
 // First half of the pipelined step (condensation on, no diagnostics): the
 // cell's front; cloudy cells finish here; every other cell sets up its
 // clear subarea (and, when partly cloudy, runs the cloudy one), runs the
 // clear subarea up to the SOA loop and hands the state at that point to the
 // solver and the post kernel. The clear-subarea part runs converged for
 // clear and partly cloudy cells alike.
-__device__ __forceinline__ void cell_pre(const StepArgs &a, const long long c) {
+// With CHEM the cell's chemistry runs between its front and amicphys
+// (run_chemistry), and the subarea set-up takes the pre-chemistry states;
+// the post kernel needs nothing else, as everything it reads of the cell's
+// state comes through the hand-off.
+template <bool CHEM>
+__device__ __forceinline__ void cell_pre(const StepArgs &a, const ChemArgs &ch,
+                                         const long long c) {
   const StepConsts &C = c_k;
   Front f;
   cell_front<false>(a, c, f);
+  ChemPre cp;
+  if constexpr (CHEM)
+    run_chemistry(a, ch, c, f, cp);
   const double dt = a.dt;
   const double fsoag = C.fcvt_soag;
   if (f.cld > 0.999) {
     double o_h2so4, o_soag, oi[NPOP], oc[NPOP];
-    cloudy_cell<false>(a, f, o_h2so4, o_soag, oi, oc, nullptr);
+    if constexpr (CHEM)
+      cloudy_cell_chem(a, f, cp, o_h2so4, o_soag, oi, oc);
+    else
+      cloudy_cell<false>(a, f, o_h2so4, o_soag, oi, oc, nullptr);
     store_outputs(a, c, o_h2so4, o_soag, oi, oc, f.h2so4, f.soag, f.ai, f.ac);
     return;
   }
@@ -750,9 +991,16 @@ __device__ __forceinline__ void cell_pre(const StepArgs &a, const long long c) {
       oc[p] = f.qc[p];
   } else {
     double gcl[2];
-    partly_cloudy_setup<false>(a, f, s, gcl, rh, ci, cg, oc, nullptr);
+    if constexpr (CHEM)
+      partly_cloudy_setup_chem(a, f, cp, s, gcl, rh, ci, cg, oc);
+    else
+      partly_cloudy_setup<false>(a, f, s, gcl, rh, ci, cg, oc, nullptr);
   }
-  const double qgas1[2] = {f.g_soag * fsoag, f.g_h2so4 * 1.0};
+  double qgas1[2] = {f.g_soag * fsoag, f.g_h2so4 * 1.0};
+  if constexpr (CHEM) {
+    qgas1[0] = cp.g1[0] * fsoag;
+    qgas1[1] = cp.g1[1] * 1.0;
+  }
   ClearMid cm;
   double uptk0[NMODE], rate[NMODE];
 #pragma unroll
@@ -921,6 +1169,80 @@ __global__ void __launch_bounds__(128) full_kernel(const __grid_constant__ StepA
     cell_step<DIAG>(a, c);
 }
 
+// The step with chemistry start to end in one thread (process switches
+// without condensation: no SOA loop to pipeline).
+__device__ __forceinline__ void cell_step_chem(const StepArgs &a, const ChemArgs &ch,
+                                               const long long c) {
+  const StepConsts &C = c_k;
+  Front f;
+  cell_front<true>(a, c, f);
+  const double dt = a.dt;
+  ChemPre cp;
+  run_chemistry(a, ch, c, f, cp);
+  double o_h2so4, o_soag, oi[NPOP], oc[NPOP];
+  const double fsoag = C.fcvt_soag;
+  const bool map_gas = a.do_cond || a.do_newnuc;
+  const double qgas1[2] = {cp.g1[0] * fsoag, cp.g1[1] * 1.0};
+  if (f.cld > 0.999) {
+    cloudy_cell_chem(a, f, cp, o_h2so4, o_soag, oi, oc);
+  } else if (f.cld < 1.0e-5) {
+    Sub s;
+    load_sub_plain(s, f.qi);
+    s.gas[0] = f.g_soag * fsoag;
+    s.gas[1] = f.g_h2so4 * 1.0;
+    const int niter = clear_subarea<false>(a, dt, f.temp, f.pmid, f.zm, f.pblh, f.relhumgcm,
+                                           f.dgn_a, f.dgn_awet, f.wetdens, qgas1, s, nullptr,
+                                           1.0);
+    if (niter > 1000)
+      atomicOr(a.flags, MAM4B_FLAG_SOA_NITER_LIMIT);
+    const double w = 1.0 - 0.0;
+    o_soag = dmax(0.0, 0.0 + (map_gas ? s.gas[0] / fsoag : f.g_soag) * w);
+    o_h2so4 = dmax(0.0, 0.0 + (map_gas ? s.gas[1] / 1.0 : f.g_h2so4) * w);
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      oi[K::numslot(m)] = dmax(0.0, 0.0 + (s.num[m] / 1.0) * w);
+#pragma unroll
+      for (int x = 0; x < NAER; ++x) {
+        const int slot = K::aer_slot(x, m);
+        if (slot >= 0)
+          oi[slot] = dmax(0.0, 0.0 + (s.aer[x][m] / K::fcvt_aer(x)) * w);
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < NPOP; ++p)
+      oc[p] = f.qc[p];
+  } else {
+    const double fclea = 1.0 - f.cld;
+    Sub s;
+    double gcl[2], rhc, ci[NPOP], cg[2];
+    partly_cloudy_setup_chem(a, f, cp, s, gcl, rhc, ci, cg, oc);
+    const int niter = clear_subarea<false>(a, dt, f.temp, f.pmid, f.zm, f.pblh, rhc, f.dgn_a,
+                                           f.dgn_awet, f.wetdens, qgas1, s, nullptr, fclea);
+    if (niter > 1000)
+      atomicOr(a.flags, MAM4B_FLAG_SOA_NITER_LIMIT);
+    o_soag = dmax(0.0, (0.0 + (map_gas ? s.gas[0] / fsoag : gcl[0]) * fclea) + cg[0]);
+    o_h2so4 = dmax(0.0, (0.0 + (map_gas ? s.gas[1] / 1.0 : gcl[1]) * fclea) + cg[1]);
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      oi[K::numslot(m)] = dmax(0.0, (0.0 + (s.num[m] / 1.0) * fclea) + ci[K::numslot(m)]);
+#pragma unroll
+      for (int x = 0; x < NAER; ++x) {
+        const int slot = K::aer_slot(x, m);
+        if (slot >= 0)
+          oi[slot] = dmax(0.0, (0.0 + (s.aer[x][m] / K::fcvt_aer(x)) * fclea) + ci[slot]);
+      }
+    }
+  }
+  store_outputs(a, c, o_h2so4, o_soag, oi, oc, f.h2so4, f.soag, f.ai, f.ac);
+}
+
+__global__ void __launch_bounds__(128) chem_step_kernel(const __grid_constant__ StepArgs a,
+                                                        const __grid_constant__ ChemArgs ch) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < a.ncell)
+    cell_step_chem(a, ch, c);
+}
+
 // Stage 1 of the pipelined step, one thread per cell: calcsize for the dry
 // diameters (an output), the relative humidity of water uptake and the
 // H2SO4 diffusivity and mean free path.
@@ -1046,8 +1368,17 @@ __global__ void __launch_bounds__(128) pair_kernel(const __grid_constant__ StepA
 
 __global__ void __launch_bounds__(128) pre_kernel(const __grid_constant__ StepArgs a) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const ChemArgs none = {nullptr, nullptr, 0};
   if (c < a.ncell)
-    cell_pre(a, c);
+    cell_pre<false>(a, none, c);
+}
+
+// The pre stage of the step with chemistry (mam4b_step_chem_slab).
+__global__ void __launch_bounds__(128) pre_chem_kernel(const __grid_constant__ StepArgs a,
+                                                       const __grid_constant__ ChemArgs ch) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < a.ncell)
+    cell_pre<true>(a, ch, c);
 }
 
 // 4 blocks of 128 per SM (128 registers, a few hundred bytes spilled to
@@ -1771,6 +2102,44 @@ __global__ void __launch_bounds__(128) setsox_kernel(const __grid_constant__ Set
   }
 }
 
+// ---- gas-phase chemistry (gas_phase_chemistry), one thread per cell
+struct GasChemArgs {
+  const double *temp, *photo;
+  const double *extfrc, *inv, *het;  // [9][ld], [8][ld], [31][ld]
+  double *qq;                        // [31][ld]
+  size_t ld;
+  long long ncell;
+  double dt;
+};
+
+// 4 blocks of 128 per SM (128 registers, the solver's spills in L1): 2.0 ms
+// on 65,536 x 72 cells against 3.0 ms unconstrained at 247 registers.
+__global__ void __launch_bounds__(128, 4) gaschem_kernel(const __grid_constant__ GasChemArgs a) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncell)
+    return;
+  double ext[gch::kExt], inv[gch::kInv], qq[gch::kTracers];
+#pragma unroll
+  for (int e = 0; e < gch::kExt; ++e)
+    ext[e] = __ldg(a.extfrc + (size_t)e * a.ld + c);
+#pragma unroll
+  for (int i = 0; i < gch::kInv; ++i)
+    inv[i] = __ldg(a.inv + (size_t)i * a.ld + c);
+#pragma unroll
+  for (int k = 1; k < gch::kTracers; ++k)
+    qq[k] = a.qq[(size_t)k * a.ld + c];
+  qq[0] = 0.0;  // O3 is neither read nor changed
+  // removal rates are read where used (each Newton iteration): after the
+  // first read they come from L1, and the solver's registers stay free
+  const double *het_c = a.het + c;
+  const size_t ld = a.ld;
+  auto het = [het_c, ld](int t) { return __ldg(het_c + (size_t)t * ld); };
+  gch::gas_chemistry_cell(__ldg(a.temp + c), a.dt, __ldg(a.photo + c), ext, inv, het, qq);
+#pragma unroll
+  for (int k = 1; k < gch::kTracers; ++k)
+    a.qq[(size_t)k * a.ld + c] = qq[k];
+}
+
 // ---- aerosol activation (ndrop get_activate_frac), one thread per cell
 struct ActivateArgs {
   const double *temp, *aer[NPOP], *rho, *w;
@@ -2149,7 +2518,9 @@ void set_step_scratch(const mam4b_ctx *ctx, StepArgs &a, size_t c0, int chunk) {
 
 // Clears the counters and queues the pipeline kernels on s in the
 // arithmetic of `precision` (mam4b_precision).
-cudaError_t launch_pipeline(mam4b_ctx *ctx, const StepArgs &a, cudaStream_t s, int precision) {
+// With ch (FP64 only) the cells' chemistry runs in the pre stage.
+cudaError_t launch_pipeline(mam4b_ctx *ctx, const StepArgs &a, cudaStream_t s, int precision,
+                            const ChemArgs *ch = nullptr) {
   cudaError_t e = cudaMemsetAsync(a.counters, 0, CNT_WORDS * sizeof(unsigned), s);
   if (e != cudaSuccess)
     return e;
@@ -2157,7 +2528,10 @@ cudaError_t launch_pipeline(mam4b_ctx *ctx, const StepArgs &a, cudaStream_t s, i
   const unsigned grid = (unsigned)((a.ncell + block - 1) / block);
   if (!a.do_cond) {
     // no SOA loop to pipeline
-    full_kernel<false><<<grid, block, 0, s>>>(a);
+    if (ch)
+      chem_step_kernel<<<grid, block, 0, s>>>(a, *ch);
+    else
+      full_kernel<false><<<grid, block, 0, s>>>(a);
     e = cudaGetLastError();
     if (e == cudaSuccess)
       ctx->launches += 1;
@@ -2175,7 +2549,10 @@ cudaError_t launch_pipeline(mam4b_ctx *ctx, const StepArgs &a, cudaStream_t s, i
   } else {
     mode_kernel<false><<<dim3(grid, NMODE), block, 0, s>>>(a);
     pair_kernel<false><<<dim3(grid, 3), block, 0, s>>>(a);
-    pre_kernel<<<grid, block, 0, s>>>(a);
+    if (ch)
+      pre_chem_kernel<<<grid, block, 0, s>>>(a, *ch);
+    else
+      pre_kernel<<<grid, block, 0, s>>>(a);
     soa_kernel<false><<<ctx->soa_grid, kSoaBlock, 0, s>>>(a);
   }
   post_kernel<<<grid, block, 0, s>>>(a);
@@ -2436,6 +2813,44 @@ mam4b_status mam4b_step_slab(mam4b_ctx *ctx, const double *in_slab, const double
   for (int f = 0; f < MAM4B_NOUT; ++f)
     ov.field[f] = out_slab + (size_t)f * ld;
   return mam4b_step(ctx, &iv, &ov, ncol, nlev, dt, precision, stream);
+}
+
+// The step with gas-phase and aqueous chemistry ahead of amicphys (FP64):
+// the forward pipeline with the chemistry in its pre stage; slabs of ld
+// doubles per field.
+mam4b_status mam4b_step_chem_slab(mam4b_ctx *ctx, const double *in_slab, const double *pblh,
+                                  const double *chem_in, double *out_slab, double *chem_out,
+                                  size_t ld, int ncol, int nlev, double dt, void *stream) {
+  const char *what = "mam4b_step_chem_slab";
+  if (!ctx || !in_slab || !pblh || !chem_in || !out_slab || !chem_out || ncol < 0 ||
+      nlev <= 0 || ld < (size_t)ncol * (size_t)nlev || !(dt > 0.0) || !isfinite(dt))
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, what, cudaSuccess);
+  StepArgs a;
+  memset(&a, 0, sizeof(a));
+  for (int f = 0; f < MAM4B_NIN; ++f)
+    a.in[f] = in_slab + (size_t)f * ld;
+  a.pblh = pblh;
+  for (int f = 0; f < MAM4B_NOUT; ++f)
+    a.out[f] = out_slab + (size_t)f * ld;
+  set_step_config(ctx, a, (long long)ncol * nlev, nlev, dt);
+  ChemArgs ch;
+  ch.in = chem_in;
+  ch.out = chem_out;
+  ch.ld = ld;
+  cudaStream_t s = (cudaStream_t)stream;
+  ctx->last_stream = s;
+  if (a.ncell == 0)
+    return MAM4B_OK;
+  if (a.ncell > 0x7fffffffLL)
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, what, cudaSuccess);
+  cudaError_t e = ensure_solver_scratch(ctx, (size_t)a.ncell);
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, what, e);
+  set_step_scratch(ctx, a, 0, 0);
+  e = launch_pipeline(ctx, a, s, MAM4B_FP64, &ch);
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, what, e);
+  return MAM4B_OK;
 }
 
 static cudaError_t grow(double **p, size_t *cap, size_t need) {
@@ -3038,6 +3453,39 @@ mam4b_status mam4b_setsox(mam4b_ctx *ctx, const double *pressure, const double *
     return MAM4B_OK;
   const int block = 128;
   setsox_kernel<<<(unsigned)((n + block - 1) / block), block, 0, s>>>(a);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, what, e);
+  ctx->launches += 1;
+  return MAM4B_OK;
+}
+
+// gas_phase_chemistry (gas_phase_chemistry.hpp:40-117), batched
+mam4b_status mam4b_gas_chemistry(mam4b_ctx *ctx, const double *temperature,
+                                 const double *photo_rates, const double *extfrc,
+                                 const double *invariants, const double *het_rates, double *qq,
+                                 size_t ld, int ncol, int nlev, double dt, void *stream) {
+  const char *what = "mam4b_gas_chemistry";
+  const size_t n = (size_t)(ncol > 0 ? ncol : 0) * (size_t)(nlev > 0 ? nlev : 0);
+  if (!ctx || !temperature || !photo_rates || !extfrc || !invariants || !het_rates || !qq ||
+      ncol < 0 || nlev <= 0 || ld < n || !(dt > 0.0) || !isfinite(dt))
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, what, cudaSuccess);
+  GasChemArgs a;
+  a.temp = temperature;
+  a.photo = photo_rates;
+  a.extfrc = extfrc;
+  a.inv = invariants;
+  a.het = het_rates;
+  a.qq = qq;
+  a.ld = ld;
+  a.ncell = (long long)n;
+  a.dt = dt;
+  cudaStream_t s = (cudaStream_t)stream;
+  ctx->last_stream = s;
+  if (n == 0)
+    return MAM4B_OK;
+  const int block = 128;
+  gaschem_kernel<<<(unsigned)((n + block - 1) / block), block, 0, s>>>(a);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess)
     return set_err(ctx, MAM4B_ERR_CUDA, what, e);

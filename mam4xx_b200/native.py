@@ -12,6 +12,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "libmam4b.so")
 
 NIN, NOUT, NDIAG, NPOP = 57, 68, 155, 25
+CHEM_NIN, CHEM_NOUT = 55, 4  # mam4b_step_chem_slab: MAM4B_CHEM_NIN, MAM4B_CHEM_NOUT
 FP64, MIXED, MIXED_FAST = 0, 1, 2
 STATUS = {0: "ok", 1: "invalid argument", 2: "cuda error", 3: "not supported",
           4: "device flags", 5: "too many cells for the no-alloc scratch"}
@@ -126,6 +127,10 @@ def lib():
         L.mam4b_activate.restype = I
         L.mam4b_setsox.argtypes = [P, P, P, P, P, P, P, P, P, S, P, P, I, I, D, P]
         L.mam4b_setsox.restype = I
+        L.mam4b_gas_chemistry.argtypes = [P, P, P, P, P, P, P, S, I, I, D, P]
+        L.mam4b_gas_chemistry.restype = I
+        L.mam4b_step_chem_slab.argtypes = [P, P, P, P, P, P, S, I, I, D, P]
+        L.mam4b_step_chem_slab.restype = I
         PF = ctypes.POINTER(ProgFields)
         P4 = ctypes.c_void_p * NUM_MODES
         L.mam4b_calcsize_process.argtypes = [P, ctypes.POINTER(CalcSizeConfig), PF, PF,
@@ -144,7 +149,8 @@ EXPORTED = ["mam4b_abi_version", "mam4b_default_config", "mam4b_create", "mam4b_
             "mam4b_step", "mam4b_step_slab", "mam4b_step_host", "mam4b_last_status",
             "mam4b_last_error", "mam4b_launch_count", "mam4b_step_slab_noalloc",
             "mam4b_adjoint_slab", "mam4b_calcsize_process", "mam4b_coagulation_process",
-            "mam4b_step_tracers", "mam4b_setsox", "mam4b_activate",
+            "mam4b_step_tracers", "mam4b_setsox", "mam4b_gas_chemistry", "mam4b_step_chem_slab",
+            "mam4b_activate",
             "mam4b_optics_lw_set_tables", "mam4b_optics_lw", "mam4b_optics_sw_set_tables",
             "mam4b_optics_sw"]
 
@@ -289,6 +295,24 @@ class Context:
                                     dqdt_aqso4 or None, dqdt_aqh2so4 or None, int(ncol),
                                     int(nlev), float(dt), ctypes.c_void_p(stream))
         self._check(st, "mam4b_setsox")
+
+    def step_chem_slab(self, in_ptr, pblh_ptr, chem_in_ptr, out_ptr, chem_out_ptr, ld, ncol,
+                       nlev, dt, stream=0):
+        """The step with gas-phase and aqueous chemistry ahead of amicphys
+        (mam4b_step_chem_slab); device slabs of ld doubles per field."""
+        st = self._lib.mam4b_step_chem_slab(self._h, in_ptr, pblh_ptr, chem_in_ptr, out_ptr,
+                                            chem_out_ptr, int(ld), int(ncol), int(nlev),
+                                            float(dt), ctypes.c_void_p(stream))
+        self._check(st, "mam4b_step_chem_slab")
+
+    def gas_chemistry(self, temperature, photo_rates, extfrc, invariants, het_rates, qq, ld,
+                      ncol, nlev, dt, stream=0):
+        """Gas-phase chemistry (mam4b_gas_chemistry); device pointers, qq
+        [31][ld] updated in place."""
+        st = self._lib.mam4b_gas_chemistry(self._h, temperature, photo_rates, extfrc, invariants,
+                                           het_rates, qq, int(ld), int(ncol), int(nlev), float(dt),
+                                           ctypes.c_void_p(stream))
+        self._check(st, "mam4b_gas_chemistry")
 
     def calcsize_process(self, progs, tends, dgncur_i, dgncur_c, ncol, nlev, dt,
                          do_aitacc_transfer=True, do_adjust=True, stream=0):

@@ -221,15 +221,15 @@ def make_process_inputs(name="c2", ncol=None, nlev=None, seed=None):
             "tend0": tend0}
 
 
-def make_setsox_inputs(name="c2", ncol=None, nlev=None, seed=None):
+def make_setsox_inputs(name="c2", ncol=None, nlev=None, seed=None, w=None):
     """Inputs of the aqueous-chemistry entry from a workload configuration:
     T, p and cloud fraction of the workload; the 31 amicphys tracers in
     mol/mol (#/kmol for numbers) from its H2SO4, SOAG and populations, plus
     O3 log-uniform 1e-8..1e-7, H2O2 1e-11..1e-9 and SO2 1e-12..1e-8 mol/mol;
     cloud liquid water log-uniform 1e-6..1e-3 kg/kg in 80 % of the cloudy
     cells (0 elsewhere), droplet number 1e7..1e9 #/kg, and the air number
-    density p / (k T) in #/cm3."""
-    w = make_workload(name, ncol=ncol, nlev=nlev, seed=seed)
+    density p / (k T) in #/cm3. w: the workload, if already made."""
+    w = w or make_workload(name, ncol=ncol, nlev=nlev, seed=seed)
     x = w["in_slab"]
     n = x.shape[1]
     rng = np.random.default_rng(991 + (seed or 0))
@@ -251,6 +251,96 @@ def make_setsox_inputs(name="c2", ncol=None, nlev=None, seed=None):
     return {"ncol": w["ncol"], "nlev": w["nlev"], "dt": w["dt"], "press": x[1].copy(),
             "temp": x[0].copy(), "lwc": lwc, "cldfrc": cld, "cldnum": cldnum, "xhnm": xhnm,
             "qin": qin, "qcw": qcw}
+
+
+def make_gas_chemistry_inputs(name="c2", ncol=None, nlev=None, seed=None, negative_frac=0.0,
+                              w=None):
+    """Inputs of the gas-phase chemistry entry from a workload configuration:
+    its temperature; invariant densities as mo_setinv sets them (total air
+    10 p / (k_cgs T), N2 0.79 and O2 0.21 of it, H2O from the workload's qv,
+    (clipped at zero), OH, NO3, HO2 and O3 from offline mixing ratios log-uniform 1e-15..1e-12,
+    1e-14..1e-10, 1e-13..1e-10 and 1e-8..1e-6); the H2O2 photolysis rate
+    log-uniform 1e-7..1e-5 /s, zero (night) in 30 % of the cells; external
+    forcing log-uniform 1e-3..1e2 molecules/cm3/s, zero in half the entries;
+    wet-removal rates log-uniform 1e-8..1e-3 /s, zero in half the entries;
+    the 31 tracers from the workload's H2SO4, SOAG and populations (mol/mol,
+    #/kmol) plus O3 1e-8..1e-6, H2O2 1e-12..1e-9, SO2 1e-12..1e-8 and DMS
+    1e-12..1e-9 mol/mol. With negative_frac > 0 that fraction of the cells
+    gets one tracer slightly negative (-1e-20), which the Newton iteration
+    never meets (clipping), so those cells take the step-cutting path.
+    w: the workload, if already made."""
+    w = w or make_workload(name, ncol=ncol, nlev=nlev, seed=seed)
+    x = w["in_slab"]
+    n = x.shape[1]
+    rng = np.random.default_rng(2718 + (seed or 0))
+    to_vmr = np.array([MW_DRY_AIR if i in (13, 18, 26, 30) else MW_DRY_AIR / ADV_MASS[i]
+                       for i in range(31)])
+    temp = x[0].copy()
+    m = 10.0 * x[1] / (0.13806500000000001e-15 * temp)
+    # water vapour as a mixing ratio, clipped at zero: the workload's qv is
+    # drawn through the Magnus saturation formula, which goes negative where
+    # the saturation pressure exceeds the pressure (hot cells near the top)
+    h2ovmr = np.maximum(x[3], 0.0) * (MW_DRY_AIR / 18.015)
+    inv = np.zeros((8, n))
+    inv[0] = m
+    inv[1] = 0.79 * m
+    inv[2] = 0.21 * m
+    inv[3] = h2ovmr * m
+    inv[4] = _logu(rng, 1e-15, 1e-12, n) * m
+    inv[5] = _logu(rng, 1e-14, 1e-10, n) * m
+    inv[6] = _logu(rng, 1e-13, 1e-10, n) * m
+    inv[7] = _logu(rng, 1e-8, 1e-6, n) * m
+    photo = np.where(rng.uniform(0, 1, n) < 0.3, 0.0, _logu(rng, 1e-7, 1e-5, n))
+    extfrc = np.where(rng.uniform(0, 1, (9, n)) < 0.5, 0.0,
+                      _logu(rng, 1e-3, 1e2, 9 * n).reshape(9, n))
+    het = np.where(rng.uniform(0, 1, (31, n)) < 0.5, 0.0,
+                   _logu(rng, 1e-8, 1e-3, 31 * n).reshape(31, n))
+    qq = np.zeros((31, n))
+    qq[0] = _logu(rng, 1e-8, 1e-6, n)
+    qq[1] = _logu(rng, 1e-12, 1e-9, n)
+    qq[2] = x[5] * to_vmr[2]
+    qq[3] = _logu(rng, 1e-12, 1e-8, n)
+    qq[4] = _logu(rng, 1e-12, 1e-9, n)
+    qq[5] = x[6] * to_vmr[5]
+    qq[6:31] = x[IN_AER_I:IN_AER_I + 25] * to_vmr[6:31, None]
+    if negative_frac > 0:
+        pick = np.nonzero(rng.uniform(0, 1, n) < negative_frac)[0]
+        qq[rng.integers(1, 31, pick.size), pick] = -1e-20
+    return {"ncol": w["ncol"], "nlev": w["nlev"], "dt": w["dt"], "temp": temp, "photo": photo,
+            "extfrc": extfrc, "inv": inv, "het": het, "qq": qq}
+
+
+CHEM_NIN, CHEM_NOUT = 55, 4
+CHEM_IN_PHOTO, CHEM_IN_EXTFRC, CHEM_IN_INV, CHEM_IN_HET, CHEM_IN_LWC, CHEM_IN_CLDNUM = (
+    4, 5, 14, 22, 53, 54)
+
+
+def make_chem_step_inputs(name="c2", ncol=None, nlev=None, seed=None, inert=False):
+    """Inputs of the step with chemistry: the workload (make_workload) and
+    its chemistry slab (CHEM_NIN fields): O3, H2O2, SO2, DMS as mass mixing
+    ratios and the gas-phase chemistry inputs of make_gas_chemistry_inputs,
+    cloud water and droplet number of make_setsox_inputs, for the same
+    cells. inert=True zeroes every rate, forcing and the cloud water, so
+    that neither chemistry changes anything."""
+    w = make_workload(name, ncol=ncol, nlev=nlev, seed=seed)
+    g = make_gas_chemistry_inputs(name, seed=seed, w=w)
+    sx = make_setsox_inputs(name, seed=seed, w=w)
+    n = w["in_slab"].shape[1]
+    ch = np.zeros((CHEM_NIN, n))
+    for k, i31 in enumerate((0, 1, 3, 4)):
+        ch[k] = g["qq"][i31] * (ADV_MASS[i31] / MW_DRY_AIR)
+    if not inert:
+        ch[CHEM_IN_PHOTO] = g["photo"]
+        ch[CHEM_IN_EXTFRC:CHEM_IN_EXTFRC + 9] = g["extfrc"]
+        ch[CHEM_IN_HET:CHEM_IN_HET + 31] = g["het"]
+        ch[CHEM_IN_LWC] = sx["lwc"]
+    ch[CHEM_IN_INV:CHEM_IN_INV + 8] = g["inv"]
+    if inert:
+        ch[CHEM_IN_INV + 4:CHEM_IN_INV + 7] = 0.0  # no OH, NO3, HO2: no reactions
+    ch[CHEM_IN_CLDNUM] = sx["cldnum"]
+    w = dict(w)
+    w["chem_in"] = ch
+    return w
 
 
 def make_activation_inputs(name="c2", ncol=None, nlev=None, seed=None):

@@ -22,6 +22,7 @@ GPU_SO = os.path.join(HERE, "libmam4oracle_gpu.so")
 COUNT_SO = os.path.join(HERE, "libmam4oracle_count.so")
 
 NIN, NOUT, NDIAG = 57, 68, 155
+CHEM_NIN, CHEM_NOUT = 55, 4  # step-with-chemistry extra inputs and outputs
 
 
 class Config(ctypes.Structure):
@@ -231,6 +232,40 @@ class ReferenceOracle(_Oracle):
         f(n, dt, *[a.ctypes.data for a in args], qin.ctypes.data, qcw.ctypes.data,
           d1.ctypes.data, d2.ctypes.data)
         return qin, qcw, d1, d2
+
+    def step_chem(self, in_slab, pblh_cell, chem_in, dt, cfg=None, nthreads=0):
+        """The step with gas-phase and aqueous chemistry ahead of amicphys
+        (the reference's functions composed per cell); chem_in
+        (MAM4B_CHEM_NIN, ncell). Returns (out, chem_out)."""
+        x = np.ascontiguousarray(in_slab, dtype=np.float64)
+        ch = np.ascontiguousarray(chem_in, dtype=np.float64)
+        n = x.shape[1]
+        assert ch.shape == (CHEM_NIN, n)
+        pb = np.ascontiguousarray(pblh_cell, dtype=np.float64)
+        out = np.zeros((NOUT, n))
+        cout = np.zeros((CHEM_NOUT, n))
+        cfg = cfg or default_config()
+        f = self.lib.mam4ref_step_chem
+        f.argtypes = [_I, _P, _P, _P, _P, _P, _D, ctypes.POINTER(Config), _I]
+        f.restype = _I
+        rc = f(n, _ptr(x), _ptr(pb), _ptr(ch), _ptr(out), _ptr(cout), dt, ctypes.byref(cfg),
+               nthreads)
+        if rc != 0:
+            raise RuntimeError("reference step_chem failed: %d" % rc)
+        return out, cout
+
+    def gas_chemistry(self, dt, temp, photo, extfrc, inv, het, qq):
+        """mam4::microphysics::gas_phase_chemistry per cell (extfrc (9,
+        ncell), inv (8, ncell), het and qq (31, ncell)); returns qq after."""
+        qq = np.array(qq, dtype=np.float64, order="C")
+        n = qq.shape[1]
+        args = [np.ascontiguousarray(a, dtype=np.float64)
+                for a in (temp, photo, extfrc, inv, het)]
+        f = self.lib.mam4ref_gas_chemistry
+        f.argtypes = [_I, _D] + [_P] * 6
+        f.restype = None
+        f(n, dt, *[a.ctypes.data for a in args], qq.ctypes.data)
+        return qq
 
     def coag_process(self, ncol, nlev, temp, pmid, wet, prog, tend, dt):
         """mam4::Coagulation::compute_tendencies column by column. wet: (8,

@@ -27,6 +27,7 @@
 
 #include <mam4xx/calcsize.hpp>
 #include <mam4xx/coagulation.hpp>
+#include <mam4xx/gas_phase_chemistry.hpp>
 #include <mam4xx/mam4_amicphys.hpp>
 #include <mam4xx/modal_aero_calcsize.hpp>
 #include <mam4xx/mo_setsox.hpp>
@@ -197,6 +198,98 @@ void step_cell(const double *in, size_t ld, size_t c, double pblh, double *out,
   }
 }
 
+// The step with chemistry ahead of amicphys (the GPU's mam4b_step_chem_slab):
+// steps 1-4 of step_cell; the 31 tracers in vmr with O3, H2O2, SO2, DMS from
+// chem_in; microphysics::gas_phase_chemistry; mo_setsox::setsox_single_level
+// (loffset 9, the total air density = invariant 0); modal_aero_amicphys_intr
+// with q_pregaschem = before gas chemistry, q_precldchem / qqcw_precldchem =
+// before aqueous chemistry; vmr -> mmr and tendencies as step_cell, plus the
+// four chemistry gases' tendencies in chem_out.
+void step_chem_cell(const double *in, size_t ld, size_t c, double pblh,
+                    const double *chem, double *out, double *chem_out, double dt,
+                    const mam4b_config &cfg) {
+  using namespace mam4::gas_chemistry;
+  auto IN = [&](int f) { return in[(size_t)f * ld + c]; };
+  auto CH = [&](int f) { return chem[(size_t)f * ld + c]; };
+  Real state_q[40] = {}, qqcw[40] = {};
+  state_q[0] = IN(MAM4B_IN_QV);
+  state_q[11] = IN(MAM4B_IN_H2SO4);
+  state_q[14] = IN(MAM4B_IN_SOAG);
+  const int gas_slot[4] = {9, 10, 12, 13}; // O3, H2O2, SO2, DMS in state_q
+  for (int g = 0; g < 4; ++g)
+    state_q[gas_slot[g]] = CH(MAM4B_CHEM_IN_O3 + g);
+  for (int p = 0; p < MAM4B_NUM_POPS; ++p) {
+    state_q[15 + p] = IN(MAM4B_IN_AER_I + p);
+    qqcw[15 + p] = IN(MAM4B_IN_AER_C + p);
+  }
+  const Real temp = IN(MAM4B_IN_T), pmid = IN(MAM4B_IN_P);
+  const Real cld = IN(MAM4B_IN_CLD);
+
+  Real dgncur_a[4], dgncur_c[4], ptend[40], dqqcwdt[40];
+  calcsize_cell(state_q, qqcw, dt, dgncur_a, dgncur_c, ptend, dqqcwdt);
+  Real dgncur_awet[4], qaerwat[4], wetdens[4];
+  water_uptake_cell(state_q, temp, pmid, cld, dgncur_a, dgncur_awet, qaerwat, wetdens);
+  for (int i = 15; i < 40; ++i) {
+    state_q[i] = mam4::max(0.0, state_q[i] + ptend[i] * dt);
+    qqcw[i] = mam4::max(0.0, qqcw[i] + dqqcwdt[i] * dt);
+  }
+  Real qq[31], qqcw31[31];
+  for (int i = 0; i < 31; ++i) {
+    qq[i] = state_q[9 + i] * to_vmr_factor(i);
+    qqcw31[i] = qqcw[9 + i] * to_vmr_factor(i);
+  }
+  Real q_pregaschem[31];
+  std::memcpy(q_pregaschem, qq, sizeof(qq));
+
+  Real ph[mam4::mo_photo::phtcnt], ex[extcnt], iv[nfs], ht[gas_pcnst];
+  ph[0] = CH(MAM4B_CHEM_IN_PHOTO);
+  for (int k = 0; k < extcnt; ++k)
+    ex[k] = CH(MAM4B_CHEM_IN_EXTFRC + k);
+  for (int k = 0; k < nfs; ++k)
+    iv[k] = CH(MAM4B_CHEM_IN_INV + k);
+  for (int k = 0; k < gas_pcnst; ++k)
+    ht[k] = CH(MAM4B_CHEM_IN_HET + k);
+  mam4::microphysics::gas_phase_chemistry(temp, dt, ph, ex, iv, ht, qq);
+
+  Real q_precldchem[31], qqcw_precldchem[31];
+  std::memcpy(q_precldchem, qq, sizeof(qq));
+  std::memcpy(qqcw_precldchem, qqcw31, sizeof(qqcw31));
+  {
+    const mam4::mo_setsox::Config scfg;
+    Real d1[31], d2[31];
+    mam4::mo_setsox::setsox_single_level(9, dt, pmid, 0.0, temp, 0.0, CH(MAM4B_CHEM_IN_LWC), cld,
+                                         CH(MAM4B_CHEM_IN_CLDNUM), iv[0], scfg, d1, d2, qqcw31,
+                                         qq);
+  }
+  {
+    using View2D = mam4::microphysics::View2D;
+    View2D d[5];
+    mam4::microphysics::modal_aero_amicphys_intr(
+        amicphys_config(cfg), dt, cfg.n_so4_monolayers_pcage, temp, pmid, 0.0,
+        IN(MAM4B_IN_ZM), pblh, IN(MAM4B_IN_QV), cld, qq, qqcw31, 0, d[0], d[1], d[2], d[3],
+        d[4], q_pregaschem, q_precldchem, qqcw_precldchem, dgncur_a, dgncur_awet, wetdens);
+  }
+  auto OUT = [&](int f) -> double & { return out[(size_t)f * ld + c]; };
+  OUT(MAM4B_OUT_TEND + 0) = (qq[2] * to_mmr_factor(2) - IN(MAM4B_IN_H2SO4)) / dt;
+  OUT(MAM4B_OUT_TEND + 1) = (qq[5] * to_mmr_factor(5) - IN(MAM4B_IN_SOAG)) / dt;
+  for (int p = 0; p < MAM4B_NUM_POPS; ++p) {
+    const int i31 = 6 + p;
+    OUT(MAM4B_OUT_TEND + 2 + p) = (qq[i31] * to_mmr_factor(i31) - IN(MAM4B_IN_AER_I + p)) / dt;
+    OUT(MAM4B_OUT_TEND + 27 + p) =
+        (qqcw31[i31] * to_mmr_factor(i31) - IN(MAM4B_IN_AER_C + p)) / dt;
+  }
+  for (int m = 0; m < 4; ++m) {
+    OUT(MAM4B_OUT_DGN_A + m) = dgncur_a[m];
+    OUT(MAM4B_OUT_DGN_AWET + m) = dgncur_awet[m];
+    OUT(MAM4B_OUT_WETDENS + m) = wetdens[m];
+    OUT(MAM4B_OUT_QAERWAT + m) = qaerwat[m];
+  }
+  const int gas_i31[4] = {0, 1, 3, 4};
+  for (int g = 0; g < 4; ++g)
+    chem_out[(size_t)(MAM4B_CHEM_OUT_TEND + g) * ld + c] =
+        (qq[gas_i31[g]] * to_mmr_factor(gas_i31[g]) - CH(MAM4B_CHEM_IN_O3 + g)) / dt;
+}
+
 } // namespace
 
 extern "C" {
@@ -213,6 +306,19 @@ int mam4ref_step(int ncell, const double *in, size_t ld_in,
   for (int c = 0; c < ncell; ++c)
     step_cell(in, ld_in, (size_t)c, pblh_cell[c], out, ld_out, diag, ld_diag,
               dt, *cfg);
+  return MAM4B_OK;
+}
+
+int mam4ref_step_chem(int ncell, const double *in, const double *pblh_cell,
+                      const double *chem_in, double *out, double *chem_out, double dt,
+                      const mam4b_config *cfg, int nthreads) {
+  if (ncell < 0 || !in || !pblh_cell || !chem_in || !out || !chem_out || !cfg || dt <= 0)
+    return MAM4B_ERR_INVALID_ARGUMENT;
+  (void)calcsize_data();
+  const int nt = nthreads > 0 ? nthreads : omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nt)
+  for (int c = 0; c < ncell; ++c)
+    step_chem_cell(in, (size_t)ncell, (size_t)c, pblh_cell[c], chem_in, out, chem_out, dt, *cfg);
   return MAM4B_OK;
 }
 
@@ -408,6 +514,31 @@ void mam4ref_setsox(int ncell, double dt, const double *press, const double *tem
       dso4[k * n + c] = d1[k];
       dh2so4[k * n + c] = d2[k];
     }
+  }
+}
+
+// microphysics::gas_phase_chemistry per cell: photo [ncell], extfrc
+// [9][ncell], inv [8][ncell], het [31][ncell]; qq [31][ncell] in/out.
+void mam4ref_gas_chemistry(int ncell, double dt, const double *temp, const double *photo,
+                           const double *extfrc, const double *inv, const double *het,
+                           double *qq) {
+  using namespace mam4::gas_chemistry;
+  const size_t n = (size_t)ncell;
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int c = 0; c < ncell; ++c) {
+    Real ph[mam4::mo_photo::phtcnt], ex[extcnt], iv[nfs], ht[gas_pcnst], q[gas_pcnst];
+    ph[0] = photo[c];
+    for (int k = 0; k < extcnt; ++k)
+      ex[k] = extfrc[k * n + c];
+    for (int k = 0; k < nfs; ++k)
+      iv[k] = inv[k * n + c];
+    for (int k = 0; k < gas_pcnst; ++k) {
+      ht[k] = het[k * n + c];
+      q[k] = qq[k * n + c];
+    }
+    mam4::microphysics::gas_phase_chemistry(temp[c], dt, ph, ex, iv, ht, q);
+    for (int k = 0; k < gas_pcnst; ++k)
+      qq[k * n + c] = q[k];
   }
 }
 

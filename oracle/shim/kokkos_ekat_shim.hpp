@@ -618,6 +618,13 @@ void parallel_reduce(const IndexRange<I> &r, const F &f, Max<T> red) {
     f(i, acc);
   red.ref = acc;
 }
+// Serial inclusive scan: one pass with final = true, double accumulator
+// (the only value type the headers scan).
+template <class I, class F> void parallel_scan(const IndexRange<I> &r, const F &f) {
+  double acc = 0.0;
+  for (I i = r.b; i < r.e; ++i)
+    f(i, acc, true);
+}
 template <class M, class F> void single(const M &, const F &f) { f(); }
 struct PerTeamT {};
 struct PerThreadT {};
