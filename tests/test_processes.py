@@ -4,6 +4,7 @@ the reference documents, and the C ABI rejects bad arguments before any
 CUDA call."""
 
 import ctypes
+import os
 
 import numpy as np
 import pytest
@@ -146,3 +147,49 @@ def test_gas_chemistry_rejects_bad_arguments_without_a_device():
     L = native.lib()
     assert L.mam4b_gas_chemistry(None, None, None, None, None, None, None, 1, 1, 1, 1.0,
                                  None) == 1
+
+
+_GASCHEM_HOST = r'''
+#include "mam4b_gaschem.cuh"
+extern "C" void run(int n, double dt, const double *temp, const double *photo, const double *ext,
+                    const double *inv, const double *het, double *qq) {
+  for (int c = 0; c < n; ++c) {
+    double e[9], iv[8], q[31];
+    for (int k = 0; k < 9; ++k) e[k] = ext[k * n + c];
+    for (int k = 0; k < 8; ++k) iv[k] = inv[k * n + c];
+    for (int k = 0; k < 31; ++k) q[k] = qq[k * n + c];
+    auto h = [&](int t) { return het[t * n + c]; };
+    mam4b::gch::gas_chemistry_cell(temp[c], dt, photo[c], e, iv, h, q);
+    for (int k = 0; k < 31; ++k) qq[k * n + c] = q[k];
+  }
+}
+'''
+
+
+def test_gas_chemistry_restatement_bitwise_on_host(ref_oracle, tmp_path):
+    """The kernel's gas-chemistry header compiled for the host (no FMA
+    contraction, glibc) equals the reference's gas_phase_chemistry bit for
+    bit, the step-cutting path of negative tracers included."""
+    import shutil
+    import subprocess
+    from mam4xx_b200.workloads import make_gas_chemistry_inputs
+    nvcc = shutil.which("nvcc")
+    if not nvcc:
+        pytest.skip("nvcc not found")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "gaschem_host.cu"
+    src.write_text(_GASCHEM_HOST)
+    so = tmp_path / "gaschem_host.so"
+    subprocess.run([nvcc, "-std=c++17", "--expt-relaxed-constexpr", "-I",
+                    os.path.join(root, "mam4xx_b200", "csrc"), "-Xcompiler",
+                    "-fPIC,-ffp-contract=off", "-shared", str(src), "-o", str(so)], check=True)
+    L = ctypes.CDLL(str(so))
+    for neg in (0.0, 0.05):
+        d = make_gas_chemistry_inputs("c4", ncol=32, seed=3, negative_frac=neg)
+        r = ref_oracle.gas_chemistry(d["dt"], d["temp"], d["photo"], d["extfrc"], d["inv"],
+                                     d["het"], d["qq"])
+        q = np.array(d["qq"], order="C")
+        args = [np.ascontiguousarray(d[k]) for k in ("temp", "photo", "extfrc", "inv", "het")]
+        L.run(ctypes.c_int(q.shape[1]), ctypes.c_double(d["dt"]),
+              *[ctypes.c_void_p(a.ctypes.data) for a in args], ctypes.c_void_p(q.ctypes.data))
+        np.testing.assert_array_equal(q, r)
