@@ -189,6 +189,8 @@ PROCESS_BYTES_PER_CELL = {"calcsize": (50 + 20 + 24 + 8) * 8, "coagulation": (42
                           "setsox": (6 + 4 + 7 + 3 + 3 + 6) * 8,
                           "gas_chemistry": (2 + 9 + 8 + 30 + 30 + 30) * 8,
                           "step_chem": (57 + 55 + 68 + 4) * 8,
+                          "aero_rad_props_sw": (55 + 1 + 42 + 2 + 56) * 8,
+                          "aero_rad_props_lw": (55 + 1 + 16 + 2 + 16) * 8,
                           "activation": (28 + 17) * 8, "optics_lw": (55 + 16) * 8,
                           "optics_sw": (55 + 56) * 8}
 
@@ -297,11 +299,28 @@ def processes_leg(native, torch, dev, stream, args, ws, hbm_peak):
         ctx.optics_sw(ox.data_ptr(), n, opd.data_ptr(), sw_out.data_ptr(), sw_aod.data_ptr(),
                       ncol, NLEV, d["dt"], stream=stream.cuda_stream)
 
+    from mam4xx_b200.workloads import make_rad_props_inputs
+    rw = make_rad_props_inputs(WORKLOAD, ncol=ncol, seed=20261203 + 11)
+    rd = {k: torch.from_numpy(np.ascontiguousarray(rw[k])).to(dev)
+          for k in ("in_slab", "pdeldry", "pint", "zi", "ext_sw", "ssa_sw", "af_sw", "ext_lw")}
+
+    def rad_sw():
+        ctx.aero_rad_props_sw(rd["in_slab"].data_ptr(), n, rd["pdeldry"].data_ptr(),
+                              rd["pint"].data_ptr(), rd["zi"].data_ptr(), rd["ext_sw"].data_ptr(),
+                              rd["ssa_sw"].data_ptr(), rd["af_sw"].data_ptr(), sw_out.data_ptr(),
+                              sw_aod.data_ptr(), 0, ncol, NLEV, d["dt"], stream=stream.cuda_stream)
+
+    def rad_lw():
+        ctx.aero_rad_props_lw(rd["in_slab"].data_ptr(), n, rd["pdeldry"].data_ptr(),
+                              rd["pint"].data_ptr(), rd["zi"].data_ptr(), rd["ext_lw"].data_ptr(),
+                              otau.data_ptr(), 0, ncol, NLEV, d["dt"], stream=stream.cuda_stream)
+
     res = {}
     for name, f in (("calcsize", calcsize), ("coagulation", coag), ("setsox", setsox),
                     ("gas_chemistry", gas_chemistry), ("step_chem", step_chem),
                     ("activation", activation),
-                    ("optics_lw", optics_lw), ("optics_sw", optics_sw)):
+                    ("optics_lw", optics_lw), ("optics_sw", optics_sw),
+                    ("aero_rad_props_sw", rad_sw), ("aero_rad_props_lw", rad_lw)):
         for _ in range(args.warmup):
             f()
         if ws > 1:

@@ -394,6 +394,40 @@ mam4b_status mam4b_activate(mam4b_ctx *ctx, const double *in_slab, size_t ld,
                             int ncol, int nlev, void *stream);
 
 /*
+ * The radiation-facing aerosol optics of the host model, batched over
+ * columns: aero_rad_props_sw and aero_rad_props_lw
+ * (src/mam4xx/aero_rad_props.hpp:250-338, 339-410). The modal optics of
+ * mam4b_optics_sw / mam4b_optics_lw (same arguments, same tables), then the
+ * WMO lapse-rate tropopause of each column (tropopause_twmo,
+ * src/mam4xx/tropopause.hpp:75-193) and the volcanic (CMIP6) stratospheric
+ * aerosol over them: averaged half and half at the tropopause level,
+ * replacing the modal values above it.
+ *
+ *   pint, zi   interface pressure [Pa] and height above the surface [m],
+ *              nlev + 1 per column (top first): element col*(nlev+1) + k
+ *   ext_sw, ssa_sw, af_sw  [MAM4B_OPTICS_SW_BANDS][ld]: volcanic extinction
+ *              [1/m], single-scattering albedo and asymmetry per cell
+ *   ext_lw     [MAM4B_OPTICS_LW_BANDS][ld]: volcanic extinction [1/m]
+ *   out, odap  as mam4b_optics_sw's out and mam4b_optics_lw's tauxar
+ *   aodvis     NULL or per column: the visible optical depth of the modal
+ *              aerosol (before the volcanic values, as in the reference)
+ *   trop_level NULL or [ncol] ints (out): the tropopause level of each
+ *              column, 0 where none is found (the reference's value then)
+ * The tropopause search needs nlev >= 2; the reference fixes nlev at its
+ * build's level count. Asynchronous on `stream`.
+ */
+mam4b_status mam4b_aero_rad_props_sw(mam4b_ctx *ctx, const double *in_slab, size_t ld,
+                                     const double *pdeldry, const double *pint, const double *zi,
+                                     const double *ext_sw, const double *ssa_sw,
+                                     const double *af_sw, double *out, double *aodvis,
+                                     int *trop_level, int ncol, int nlev, double dt,
+                                     void *stream);
+mam4b_status mam4b_aero_rad_props_lw(mam4b_ctx *ctx, const double *in_slab, size_t ld,
+                                     const double *pdeldry, const double *pint, const double *zi,
+                                     const double *ext_lw, double *odap, int *trop_level,
+                                     int ncol, int nlev, double dt, void *stream);
+
+/*
  * Aqueous-phase sulfate chemistry in cloud water, batched over cells:
  * mam4::mo_setsox::setsox_single_level (src/mam4xx/mo_setsox.hpp:944-1254),
  * the cloud-chemistry stage that runs before amicphys in the host model.

@@ -255,3 +255,94 @@ MAM4B_HD void mode_band_sw(const double *tables, int m, int b, const double (&sp
 
 }  // namespace opt
 }  // namespace mam4b
+
+// ---- radiation-facing optics: the tropopause and the volcanic (CMIP6)
+// stratospheric aerosol, aero_rad_props (src/mam4xx/aero_rad_props.hpp).
+namespace mam4b {
+namespace rad {
+
+// R/cp of dry air and -g/R_dry (tropopause.hpp:17-30, mam4_constants.hpp)
+constexpr double kRgas = 6.022214076e23 * 1.380649e-23;
+constexpr double kKap = ((kRgas * 1e3) / (0.028966 * 1e3)) / 1.00464e3;
+constexpr double kFaktor = -9.80616 / (kRgas / 0.028966);
+constexpr double kKa1 = kKap - 1.0;
+
+// lapse rate and mean temperature between two levels in p^kappa
+// (get_dtdz, tropopause.hpp:32-49)
+MAM4B_HD void lapse_rate(double pm, double pmk, double p_up, double p_down, double t_up,
+                         double t_down, double &dtdz, double &tm) {
+  const double a1 = (t_up - t_down) / (pow(p_up, kKap) - pow(p_down, kKap));
+  const double b1 = t_down - a1 * pow(p_down, kKap);
+  tm = a1 * pmk + b1;
+  const double dtdp = a1 * kKap * (pow(pm, kKa1));
+  dtdz = kFaktor * dtdp * pm / tm;
+}
+
+// WMO lapse-rate tropopause of a column (twmo, Reichler et al. 2003;
+// tropopause.hpp:75-171): scanning up from the surface, the first level
+// where the lapse rate falls below 2 K/km, between 75 and 450 hPa, and
+// stays below it on average over the 2 km above. Returns its pressure, or
+// -99 when there is none. temp(k), pmid(k): level k of the column, k = 0
+// at the top.
+template <class ColT, class ColP>
+MAM4B_HD double twmo_pressure(const ColT &temp, const ColP &pmid, int nlev) {
+  const double gam = -0.002, plimu = 45000, pliml = 7500, deltaz = 2000.0;
+  double pmk = 0.5 * (pow(pmid(nlev - 2), kKap) + pow(pmid(nlev - 1), kKap));
+  double pm = pow(pmk, (1.0 / kKap));
+  double dtdz, tm;
+  lapse_rate(pm, pmk, pmid(nlev - 2), pmid(nlev - 1), temp(nlev - 2), temp(nlev - 1), dtdz, tm);
+  for (int k = nlev - 2; k >= 1; --k) {
+    const double pmk0 = pmk, dtdz0 = dtdz;
+    pmk = 0.5 * (pow(pmid(k - 1), kKap) + pow(pmid(k), kKap));
+    pm = pow(pmk, (1.0 / kKap));
+    lapse_rate(pm, pmk, pmid(k - 1), pmid(k), temp(k - 1), temp(k), dtdz, tm);
+    if (dtdz <= gam || pm > plimu)
+      continue;
+    double ptph;
+    if (dtdz0 < gam) {
+      const double ag = (dtdz - dtdz0) / (pmk - pmk0);
+      const double bg = dtdz0 - (ag * pmk0);
+      ptph = exp(log((gam - bg) / ag) / kKap);
+    } else {
+      ptph = pm;
+    }
+    if (ptph < pliml || ptph > plimu)
+      continue;
+    const double p2km = ptph + deltaz * (pm / tm) * kFaktor;
+    double asum = 0.0;
+    int icount = 0;
+    for (int j = k; j >= 1; --j) {
+      const double pmk2 = 0.5 * (pow(pmid(j - 1), kKap) + pow(pmid(j), kKap));
+      const double pm2 = pow(pmk2, 1.0 / kKap);
+      if (pm2 > ptph)
+        continue;
+      if (pm2 < p2km)
+        return ptph;  // the layer above stays stable: tropopause found
+      double dtdz2 = 0.0, tm2 = 0.0;
+      lapse_rate(pm2, pmk2, pmid(j - 1), pmid(j), temp(j - 1), temp(j), dtdz2, tm2);
+      asum += dtdz2;
+      icount++;
+      const double aquer = asum / double(icount);
+      if (aquer <= gam)
+        break;  // not stable enough above: try the next level up
+    }
+  }
+  return -99.0;
+}
+
+// tropopause_twmo (tropopause.hpp:173-193): the level k in [2, nlev-1],
+// scanning up, whose upper interface pressure pint(k) lies at or below the
+// tropopause pressure; 0 when there is no tropopause or no such level.
+template <class ColT, class ColP, class ColI>
+MAM4B_HD int tropopause_level(const ColT &temp, const ColP &pmid, const ColI &pint, int nlev) {
+  const double tp = twmo_pressure(temp, pmid, nlev);
+  if (tp > 0) {
+    for (int k = nlev - 1; k > 1; --k)
+      if (tp >= pint(k))
+        return k;
+  }
+  return 0;
+}
+
+}  // namespace rad
+}  // namespace mam4b

@@ -2355,6 +2355,79 @@ __global__ void __launch_bounds__(128) optics_sw_aod_kernel(const __grid_constan
   w.aodvis[col] = s;
 }
 
+// ---- aero_rad_props: tropopause per column, then the volcanic (CMIP6)
+// extinction over the modal optics at and above it
+struct RadArgs {
+  const double *temp, *pmid;     // step input fields (cell = col * nlev + k)
+  const double *pint, *zi;       // [col * (nlev + 1) + k]: interface pressure, height
+  const double *ext, *ssa, *af;  // [band][ld]: extinction [1/m], albedo, asymmetry
+  double *out;                   // shortwave [4][14][ld], longwave [16][ld]
+  int *trop;                     // [ncol]
+  size_t ld;
+  int ncol, nlev;
+};
+
+// one thread per column (the search reads the column bottom up)
+__global__ void __launch_bounds__(128) tropopause_kernel(const __grid_constant__ RadArgs r) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= r.ncol)
+    return;
+  const size_t c0 = (size_t)col * r.nlev, i0 = (size_t)col * (r.nlev + 1);
+  auto T = [&](int k) { return __ldg(r.temp + c0 + k); };
+  auto P = [&](int k) { return __ldg(r.pmid + c0 + k); };
+  auto PI = [&](int k) { return __ldg(r.pint + i0 + k); };
+  r.trop[col] = rad::tropopause_level(T, P, PI, r.nlev);
+}
+
+// volcanic_cmip_sw (aero_rad_props.hpp:38-119): at the tropopause level the
+// four layer products are averaged with the volcanic ones, above it they
+// are replaced (the file's values hold all stratospheric aerosol there)
+__global__ void __launch_bounds__(128) volcanic_sw_kernel(const __grid_constant__ RadArgs r) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= (long long)r.ncol * r.nlev)
+    return;
+  const int col = (int)(c / r.nlev), k = (int)(c % r.nlev);
+  const int lev = __ldg(r.trop + col);
+  if (k > lev)
+    return;
+  const size_t i0 = (size_t)col * (r.nlev + 1);
+  const double thk = __ldg(r.zi + i0 + k) - __ldg(r.zi + i0 + k + 1);
+  const size_t ld = r.ld, nb = opt::kSwBands;
+  for (int b = 0; b < opt::kSwBands; ++b) {
+    const double ext = thk * __ldg(r.ext + b * ld + c);
+    const double asym = __ldg(r.af + b * ld + c);
+    const double ext_ssa = ext * __ldg(r.ssa + b * ld + c);
+    const double ext_ssa_asym = ext_ssa * asym;
+    const double v[4] = {ext, ext_ssa, ext_ssa_asym, ext_ssa_asym * asym};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      double *o = r.out + (q * nb + b) * ld + c;
+      *o = k == lev ? 0.5 * (*o + v[q]) : v[q];
+    }
+  }
+}
+
+// compute_odap_volcanic_at_troplayer_lw / _above_troplayer_lw
+// (aero_rad_props.hpp:121-208): the absorption optical depth, averaged at
+// the tropopause level, replaced above it
+__global__ void __launch_bounds__(128) volcanic_lw_kernel(const __grid_constant__ RadArgs r) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= (long long)r.ncol * r.nlev)
+    return;
+  const int col = (int)(c / r.nlev), k = (int)(c % r.nlev);
+  const int lev = __ldg(r.trop + col);
+  if (k > lev)
+    return;
+  const size_t i0 = (size_t)col * (r.nlev + 1);
+  const double thk = __ldg(r.zi + i0 + k) - __ldg(r.zi + i0 + k + 1);
+  const size_t ld = r.ld;
+  for (int b = 0; b < opt::kLwBands; ++b) {
+    double *o = r.out + b * ld + c;
+    const double v = thk * __ldg(r.ext + b * ld + c);
+    *o = k == lev ? 0.5 * (*o + v) : v;
+  }
+}
+
 }  // namespace mam4b
 
 // =============================================================== C ABI
@@ -2402,6 +2475,8 @@ struct mam4b_ctx {
   double *d_optics_sw;  // shortwave optics tables (opt::kSwTableDoubles), set by the host
   double *d_optics_scr; // optics per-cell sizes (SS_FIELDS per cell), grown
   size_t cap_optics_scr;
+  int *d_trop;          // [cap_trop]: tropopause level per column (aero_rad_props)
+  size_t cap_trop;
   unsigned *d_bins;     // [2 kPassBins]: loops per pass count, start offsets
   int adj_soa_grid;
   size_t cap_adj;
@@ -2724,6 +2799,7 @@ mam4b_status mam4b_destroy(mam4b_ctx *ctx) {
   cudaFree(ctx->d_optics_lw);
   cudaFree(ctx->d_optics_scr);
   cudaFree(ctx->d_optics_sw);
+  cudaFree(ctx->d_trop);
   if (ctx->host_streams) {
     for (int k = 0; k < kHostStreams; ++k) {
       cudaStreamDestroy(ctx->hs[k]);
@@ -3388,6 +3464,105 @@ mam4b_status mam4b_optics_lw(mam4b_ctx *ctx, const double *in_slab, size_t ld,
   if (e != cudaSuccess)
     return set_err(ctx, MAM4B_ERR_CUDA, what, e);
   ctx->launches += 3;
+  return MAM4B_OK;
+}
+
+// Tropopause levels of the columns into trop (caller's array, or the
+// context's when NULL); r gets the layout fields.
+static mam4b_status rad_props_tropopause(mam4b_ctx *ctx, const char *what, RadArgs &r,
+                                         const double *in_slab, const double *pint,
+                                         const double *zi, int *trop_level, cudaStream_t s) {
+  r.temp = in_slab + (size_t)MAM4B_IN_T * r.ld;
+  r.pmid = in_slab + (size_t)MAM4B_IN_P * r.ld;
+  r.pint = pint;
+  r.zi = zi;
+  r.trop = trop_level;
+  if (!r.trop) {
+    if (ctx->cap_trop < (size_t)r.ncol) {
+      cudaFree(ctx->d_trop);
+      ctx->d_trop = nullptr;
+      ctx->cap_trop = 0;
+      const cudaError_t e = cudaMalloc(&ctx->d_trop, (size_t)r.ncol * sizeof(int));
+      if (e != cudaSuccess)
+        return set_err(ctx, MAM4B_ERR_CUDA, what, e);
+      ctx->cap_trop = (size_t)r.ncol;
+    }
+    r.trop = ctx->d_trop;
+  }
+  const int block = 128;
+  tropopause_kernel<<<(unsigned)((r.ncol + block - 1) / block), block, 0, s>>>(r);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, what, e);
+  ctx->launches += 1;
+  return MAM4B_OK;
+}
+
+// aero_rad_props_sw (aero_rad_props.hpp:250-338), batched
+mam4b_status mam4b_aero_rad_props_sw(mam4b_ctx *ctx, const double *in_slab, size_t ld,
+                                     const double *pdeldry, const double *pint, const double *zi,
+                                     const double *ext_sw, const double *ssa_sw,
+                                     const double *af_sw, double *out, double *aodvis,
+                                     int *trop_level, int ncol, int nlev, double dt,
+                                     void *stream) {
+  const char *what = "mam4b_aero_rad_props_sw";
+  if (!ctx || !pint || !zi || !ext_sw || !ssa_sw || !af_sw || nlev < 2)
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, what, cudaSuccess);
+  mam4b_status st = mam4b_optics_sw(ctx, in_slab, ld, pdeldry, out, aodvis, ncol, nlev, dt, stream);
+  if (st != MAM4B_OK || ncol == 0)
+    return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  RadArgs r;
+  memset(&r, 0, sizeof(r));
+  r.ld = ld;
+  r.ncol = ncol;
+  r.nlev = nlev;
+  r.ext = ext_sw;
+  r.ssa = ssa_sw;
+  r.af = af_sw;
+  r.out = out;
+  st = rad_props_tropopause(ctx, what, r, in_slab, pint, zi, trop_level, s);
+  if (st != MAM4B_OK)
+    return st;
+  const int block = 128;
+  const size_t n = (size_t)ncol * nlev;
+  volcanic_sw_kernel<<<(unsigned)((n + block - 1) / block), block, 0, s>>>(r);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, what, e);
+  ctx->launches += 1;
+  return MAM4B_OK;
+}
+
+// aero_rad_props_lw (aero_rad_props.hpp:339-410), batched
+mam4b_status mam4b_aero_rad_props_lw(mam4b_ctx *ctx, const double *in_slab, size_t ld,
+                                     const double *pdeldry, const double *pint, const double *zi,
+                                     const double *ext_lw, double *odap, int *trop_level,
+                                     int ncol, int nlev, double dt, void *stream) {
+  const char *what = "mam4b_aero_rad_props_lw";
+  if (!ctx || !pint || !zi || !ext_lw || nlev < 2)
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, what, cudaSuccess);
+  mam4b_status st = mam4b_optics_lw(ctx, in_slab, ld, pdeldry, odap, ncol, nlev, dt, stream);
+  if (st != MAM4B_OK || ncol == 0)
+    return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  RadArgs r;
+  memset(&r, 0, sizeof(r));
+  r.ld = ld;
+  r.ncol = ncol;
+  r.nlev = nlev;
+  r.ext = ext_lw;
+  r.out = odap;
+  st = rad_props_tropopause(ctx, what, r, in_slab, pint, zi, trop_level, s);
+  if (st != MAM4B_OK)
+    return st;
+  const int block = 128;
+  const size_t n = (size_t)ncol * nlev;
+  volcanic_lw_kernel<<<(unsigned)((n + block - 1) / block), block, 0, s>>>(r);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, what, e);
+  ctx->launches += 1;
   return MAM4B_OK;
 }
 

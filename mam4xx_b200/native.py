@@ -131,6 +131,10 @@ def lib():
         L.mam4b_gas_chemistry.restype = I
         L.mam4b_step_chem_slab.argtypes = [P, P, P, P, P, P, S, I, I, D, P]
         L.mam4b_step_chem_slab.restype = I
+        L.mam4b_aero_rad_props_sw.argtypes = [P, P, S, P, P, P, P, P, P, P, P, P, I, I, D, P]
+        L.mam4b_aero_rad_props_sw.restype = I
+        L.mam4b_aero_rad_props_lw.argtypes = [P, P, S, P, P, P, P, P, P, I, I, D, P]
+        L.mam4b_aero_rad_props_lw.restype = I
         PF = ctypes.POINTER(ProgFields)
         P4 = ctypes.c_void_p * NUM_MODES
         L.mam4b_calcsize_process.argtypes = [P, ctypes.POINTER(CalcSizeConfig), PF, PF,
@@ -152,7 +156,7 @@ EXPORTED = ["mam4b_abi_version", "mam4b_default_config", "mam4b_create", "mam4b_
             "mam4b_step_tracers", "mam4b_setsox", "mam4b_gas_chemistry", "mam4b_step_chem_slab",
             "mam4b_activate",
             "mam4b_optics_lw_set_tables", "mam4b_optics_lw", "mam4b_optics_sw_set_tables",
-            "mam4b_optics_sw"]
+            "mam4b_optics_sw", "mam4b_aero_rad_props_sw", "mam4b_aero_rad_props_lw"]
 
 
 def default_config(**overrides):
@@ -304,6 +308,25 @@ class Context:
                                             chem_out_ptr, int(ld), int(ncol), int(nlev),
                                             float(dt), ctypes.c_void_p(stream))
         self._check(st, "mam4b_step_chem_slab")
+
+    def aero_rad_props_sw(self, in_ptr, ld, pdeldry, pint, zi, ext_sw, ssa_sw, af_sw, out,
+                          aodvis, trop_level, ncol, nlev, dt, stream=0):
+        """aero_rad_props_sw (mam4b_aero_rad_props_sw): shortwave optics
+        with the volcanic aerosol over the tropopause; aodvis and
+        trop_level may be 0."""
+        st = self._lib.mam4b_aero_rad_props_sw(self._h, in_ptr, int(ld), pdeldry, pint, zi,
+                                               ext_sw, ssa_sw, af_sw, out, aodvis or None,
+                                               trop_level or None, int(ncol), int(nlev),
+                                               float(dt), ctypes.c_void_p(stream))
+        self._check(st, "mam4b_aero_rad_props_sw")
+
+    def aero_rad_props_lw(self, in_ptr, ld, pdeldry, pint, zi, ext_lw, odap, trop_level, ncol,
+                          nlev, dt, stream=0):
+        """aero_rad_props_lw (mam4b_aero_rad_props_lw); trop_level may be 0."""
+        st = self._lib.mam4b_aero_rad_props_lw(self._h, in_ptr, int(ld), pdeldry, pint, zi,
+                                               ext_lw, odap, trop_level or None, int(ncol),
+                                               int(nlev), float(dt), ctypes.c_void_p(stream))
+        self._check(st, "mam4b_aero_rad_props_lw")
 
     def gas_chemistry(self, temperature, photo_rates, extfrc, invariants, het_rates, qq, ld,
                       ncol, nlev, dt, stream=0):

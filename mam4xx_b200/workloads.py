@@ -343,6 +343,59 @@ def make_chem_step_inputs(name="c2", ncol=None, nlev=None, seed=None, inert=Fals
     return w
 
 
+def make_rad_props_inputs(name="c2", ncol=None, nlev=None, seed=None, no_tropopause_frac=0.1):
+    """Inputs of the radiation-facing optics entries (aero_rad_props): the
+    workload's aerosol with an atmosphere that has a tropopause. Per column:
+    surface temperature U(280, 305) K falling 6.5 K/km up to a tropopause at
+    U(9, 17) km and rising 1.5 K/km above it, with 0.2 K of noise per level;
+    a fraction no_tropopause_frac of the columns falls 8 K/km up to 60 hPa
+    and is isothermal above (no tropopause: the reference's level 0). Heights are hypsometric on
+    the workload's pressure levels; interfaces at the geometric means of
+    adjacent levels, 101325 Pa at the surface; water vapour redrawn at
+    relative humidity U(0.05, 0.99). Volcanic inputs per cell: shortwave
+    extinction log-uniform 1e-8..1e-5 /m, albedo U(0.9, 1), asymmetry
+    U(0.6, 0.8); longwave extinction 1e-9..1e-6 /m."""
+    w = dict(make_workload(name, ncol=ncol, nlev=nlev, seed=seed))
+    ncol, nlev = w["ncol"], w["nlev"]
+    x = w["in_slab"].copy()
+    n = ncol * nlev
+    rng = np.random.default_rng(4711 + (seed or 0))
+    plev = x[1][:nlev].copy()
+    pint = np.empty(nlev + 1)
+    pint[1:nlev] = np.sqrt(plev[:-1] * plev[1:])
+    pint[0] = plev[0] * np.sqrt(plev[0] / plev[1])
+    pint[nlev] = 101325.0
+    rd_over_g = 287.04 / 9.80616
+    z_approx = 7500.0 * np.log(101325.0 / plev)  # first guess of the heights
+    t0 = rng.uniform(280.0, 305.0, ncol)[:, None]
+    zt = rng.uniform(9000.0, 17000.0, ncol)[:, None]
+    none = (rng.uniform(0, 1, ncol) < no_tropopause_frac)[:, None]
+    tt = t0 - 6.5e-3 * zt
+    temp = np.where(z_approx[None, :] <= zt, t0 - 6.5e-3 * z_approx[None, :],
+                    tt + 1.5e-3 * (z_approx[None, :] - zt))
+    # no tropopause: unstable up to 60 hPa, isothermal above (stable only
+    # above the search's 75 hPa limit)
+    z60 = 7500.0 * np.log(101325.0 / 6000.0)
+    temp = np.where(none, t0 - 8.0e-3 * np.minimum(z_approx[None, :], z60), temp)
+    temp = temp + rng.normal(0.0, 0.2, (ncol, nlev))
+    zi = np.zeros((ncol, nlev + 1))
+    for k in range(nlev - 1, -1, -1):
+        zi[:, k] = zi[:, k + 1] + rd_over_g * temp[:, k] * np.log(pint[k + 1] / pint[k])
+    zm = 0.5 * (zi[:, :-1] + zi[:, 1:])
+    x[0] = temp.reshape(-1)
+    x[2] = zm.reshape(-1)
+    x[3] = rng.uniform(0.05, 0.99, n) * np.maximum(magnus_qv_sat(x[0], x[1]), 0.0)
+    w["in_slab"] = x
+    w["pint"] = np.tile(pint, ncol)
+    w["zi"] = zi.reshape(-1)
+    w["pdeldry"] = np.tile(np.diff(pint), ncol)
+    w["ext_sw"] = _logu(rng, 1e-8, 1e-5, 14 * n).reshape(14, n)
+    w["ssa_sw"] = rng.uniform(0.9, 1.0, (14, n))
+    w["af_sw"] = rng.uniform(0.6, 0.8, (14, n))
+    w["ext_lw"] = _logu(rng, 1e-9, 1e-6, 16 * n).reshape(16, n)
+    return w
+
+
 def make_activation_inputs(name="c2", ncol=None, nlev=None, seed=None):
     """Inputs of the activation entry: a workload's input slab, the air
     density p / (R_air T) and an updraft log-uniform 0.01..3 m/s, zero or

@@ -192,6 +192,24 @@ class ReferenceOracle(_Oracle):
           out.ctypes.data, aod.ctypes.data)
         return out, aod
 
+    def rad_props_volcanic(self, sw, ncol, nlev, in_slab, pint, zi, ext, ssa, af, modal):
+        """The reference's tropopause_or_quit and volcanic updates of
+        aero_rad_props_sw (sw=True) / aero_rad_props_lw on modal optics
+        results; returns (updated copy, tropopause level per column)."""
+        x = np.ascontiguousarray(in_slab, dtype=np.float64)
+        out = np.array(modal, dtype=np.float64, order="C")
+        trop = np.zeros(ncol, dtype=np.int32)
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (pint, zi, ext)]
+        if sw:
+            arrs += [np.ascontiguousarray(a, dtype=np.float64) for a in (ssa, af)]
+        f = self.lib.mam4ref_rad_props_volcanic
+        f.argtypes = [_I, _I, _I] + [_P] * 8
+        f.restype = None
+        f(int(bool(sw)), ncol, nlev, x.ctypes.data, arrs[0].ctypes.data, arrs[1].ctypes.data,
+          arrs[2].ctypes.data, arrs[3].ctypes.data if sw else None,
+          arrs[4].ctypes.data if sw else None, out.ctypes.data, trop.ctypes.data)
+        return out, trop
+
     def maxsat(self, zeta, eta, smc):
         """ndrop::maxsat for 4 modes."""
         f = self.lib.mam4ref_maxsat

@@ -26,6 +26,7 @@
 //   7. vmr -> mmr and tendency = (after - before)/dt.
 
 #include <mam4xx/calcsize.hpp>
+#include <mam4xx/aero_rad_props.hpp>
 #include <mam4xx/coagulation.hpp>
 #include <mam4xx/gas_phase_chemistry.hpp>
 #include <mam4xx/mam4_amicphys.hpp>
@@ -700,6 +701,63 @@ void mam4ref_optics_sw(int ncol, int nlev, const double *in, const double *pdeld
       for (int m = 0; m < 4; ++m)
         s += vis[((size_t)col * nlev + k) * 4 + m];
     aod[col] = s;
+  }
+}
+
+// The part of aero_rad_props_sw / aero_rad_props_lw after the modal optics:
+// tropopause_or_quit and the volcanic updates, column by column, on the
+// modal results (mam4ref_optics_sw's out [4][14][n] or mam4ref_optics_lw's
+// tau [16][n], updated in place) in the reference's own layouts
+// (tau (band, 0:nlev); odap (band, nlev); sw extinction (band, nlev), sw
+// albedo and asymmetry and lw extinction (nlev, band)). pint, zi: nlev+1
+// per column; ext/ssa/af: [band][n]; trop: [ncol] out.
+void mam4ref_rad_props_volcanic(int sw, int ncol, int nlev, const double *in, const double *pint,
+                                const double *zi, const double *ext, const double *ssa,
+                                const double *af, double *out, int *trop) {
+  namespace arp = mam4::aero_rad_props;
+  using View2D = arp::View2D;
+  const size_t n = (size_t)ncol * nlev;
+  const int nb = sw ? arp::nswbands : arp::nlwbands;
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int col = 0; col < ncol; ++col) {
+    const size_t c0 = (size_t)col * nlev, i0 = (size_t)col * (nlev + 1);
+    mam4::ConstColumnView pmid(in + (size_t)MAM4B_IN_P * n + c0, nlev);
+    mam4::ConstColumnView temp(in + (size_t)MAM4B_IN_T * n + c0, nlev);
+    mam4::ConstColumnView zm(in + (size_t)MAM4B_IN_ZM * n + c0, nlev);
+    mam4::ConstColumnView pi(pint + i0, nlev + 1), z(zi + i0, nlev + 1);
+    const int lev = arp::tropopause_or_quit(pmid, pi, temp, zm, z);
+    trop[col] = lev;
+    mam4::ThreadTeam team;
+    if (sw) {
+      View2D q[4] = {View2D("tau", nb, nlev + 1), View2D("tau_w", nb, nlev + 1),
+                     View2D("tau_w_g", nb, nlev + 1), View2D("tau_w_f", nb, nlev + 1)};
+      View2D e("ext", nb, nlev), a("ssa", nlev, nb), g("af", nlev, nb);
+      for (int b = 0; b < nb; ++b)
+        for (int k = 0; k < nlev; ++k) {
+          e(b, k) = ext[(size_t)b * n + c0 + k];
+          a(k, b) = ssa[(size_t)b * n + c0 + k];
+          g(k, b) = af[(size_t)b * n + c0 + k];
+          for (int j = 0; j < 4; ++j)
+            q[j](b, k + 1) = out[((size_t)j * nb + b) * n + c0 + k];
+        }
+      arp::volcanic_cmip_sw(team, z, lev, e, a, g, q[0], q[1], q[2], q[3]);
+      for (int b = 0; b < nb; ++b)
+        for (int k = 0; k < nlev; ++k)
+          for (int j = 0; j < 4; ++j)
+            out[((size_t)j * nb + b) * n + c0 + k] = q[j](b, k + 1);
+    } else {
+      View2D odap("odap", nb, nlev), e("ext", nlev, nb);
+      for (int b = 0; b < nb; ++b)
+        for (int k = 0; k < nlev; ++k) {
+          odap(b, k) = out[(size_t)b * n + c0 + k];
+          e(k, b) = ext[(size_t)b * n + c0 + k];
+        }
+      arp::compute_odap_volcanic_at_troplayer_lw(team, lev, z, e, odap);
+      arp::compute_odap_volcanic_above_troplayer_lw(team, lev, z, e, odap);
+      for (int b = 0; b < nb; ++b)
+        for (int k = 0; k < nlev; ++k)
+          out[(size_t)b * n + c0 + k] = odap(b, k);
+    }
   }
 }
 

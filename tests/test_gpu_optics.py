@@ -73,3 +73,77 @@ def test_optics_sw_matches_reference(cuda_device, ref_oracle, name, ncol):
     err = np.abs(g - r) / np.maximum(scale, 1e-30)
     assert err.max() <= 1e-10, (err.max(), np.quantile(err, 0.99))
     np.testing.assert_allclose(ga, ra, rtol=1e-10)
+
+
+def _rad_inputs(name, ncol, seed):
+    from mam4xx_b200.workloads import make_rad_props_inputs
+    w = make_rad_props_inputs(name, ncol=ncol, seed=seed)
+    return w, {k: torch.from_numpy(np.ascontiguousarray(w[k])).cuda()
+               for k in ("in_slab", "pdeldry", "pint", "zi", "ext_sw", "ssa_sw", "af_sw",
+                         "ext_lw")}
+
+
+@pytest.mark.parametrize("name,ncol", [("c2", 128), ("c4", 64)])
+def test_aero_rad_props_sw_matches_reference(cuda_device, ref_oracle, name, ncol):
+    """aero_rad_props_sw: the modal optics, the tropopause (bitwise the
+    reference's level on every column, some columns without one) and the
+    volcanic values at and above it."""
+    from mam4xx_b200.workloads import make_optics_sw_tables
+    w, d = _rad_inputs(name, ncol, 43)
+    tb = make_optics_sw_tables(seed=2)
+    n, nc, nl = w["in_slab"].shape[1], w["ncol"], w["nlev"]
+    ctx = native.Context()
+    ctx.optics_sw_set_tables(tb)
+    out = torch.full((4, 14, n), float("nan"), dtype=torch.float64, device="cuda")
+    aod = torch.full((nc,), float("nan"), dtype=torch.float64, device="cuda")
+    trop = torch.full((nc,), -7, dtype=torch.int32, device="cuda")
+    ctx.aero_rad_props_sw(d["in_slab"].data_ptr(), n, d["pdeldry"].data_ptr(),
+                          d["pint"].data_ptr(), d["zi"].data_ptr(), d["ext_sw"].data_ptr(),
+                          d["ssa_sw"].data_ptr(), d["af_sw"].data_ptr(), out.data_ptr(),
+                          aod.data_ptr(), trop.data_ptr(), nc, nl, w["dt"])
+    torch.cuda.synchronize()
+    g, gt = out.cpu().numpy(), trop.cpu().numpy()
+    modal, ra = ref_oracle.optics_sw(nc, nl, w["in_slab"], w["pdeldry"], w["dt"], tb)
+    r, rt = ref_oracle.rad_props_volcanic(True, nc, nl, w["in_slab"], w["pint"], w["zi"],
+                                          w["ext_sw"], w["ssa_sw"], w["af_sw"], modal)
+    np.testing.assert_array_equal(gt, rt)
+    assert (rt == 0).any() and (rt > 20).mean() > 0.5
+    assert np.isfinite(g).all()
+    scale = np.maximum(np.abs(r), np.abs(r[0])[None])
+    err = np.abs(g - r) / np.maximum(scale, 1e-30)
+    assert err.max() <= 1e-10, (err.max(), np.quantile(err, 0.99))
+    np.testing.assert_allclose(aod.cpu().numpy(), ra, rtol=1e-10)
+    # above the tropopause the volcanic values alone (bitwise: same products)
+    k = np.arange(n) % nl
+    above = k < np.repeat(rt, nl)
+    np.testing.assert_array_equal(g[:, :, above], r[:, :, above])
+
+
+def test_aero_rad_props_lw_matches_reference(cuda_device, ref_oracle):
+    w, d = _rad_inputs("c2", 128, 44)
+    tb = make_optics_lw_tables(seed=1)
+    n, nc, nl = w["in_slab"].shape[1], w["ncol"], w["nlev"]
+    ctx = native.Context()
+    ctx.optics_lw_set_tables(tb)
+    odap = torch.full((16, n), float("nan"), dtype=torch.float64, device="cuda")
+    ctx.aero_rad_props_lw(d["in_slab"].data_ptr(), n, d["pdeldry"].data_ptr(),
+                          d["pint"].data_ptr(), d["zi"].data_ptr(), d["ext_lw"].data_ptr(),
+                          odap.data_ptr(), 0, nc, nl, w["dt"])
+    torch.cuda.synchronize()
+    g = odap.cpu().numpy()
+    modal = ref_oracle.optics_lw(w["in_slab"], w["pdeldry"], w["dt"], tb)
+    r, rt = ref_oracle.rad_props_volcanic(False, nc, nl, w["in_slab"], w["pint"], w["zi"],
+                                          w["ext_lw"], None, None, modal)
+    assert np.isfinite(g).all()
+    err = np.abs(g - r) / np.maximum(np.abs(r), 1e-30)
+    assert err.max() <= 1e-10, (err.max(), np.quantile(err, 0.99))
+
+
+def test_aero_rad_props_reject_bad_arguments(cuda_device):
+    ctx = native.Context()
+    t = torch.zeros((native.NIN, 4), dtype=torch.float64, device="cuda")
+    p = t.data_ptr()
+    with pytest.raises(native.MicrophysicsError):
+        ctx.aero_rad_props_lw(p, 4, p, 0, p, p, p, 0, 1, 4, 1800.0)  # no interface pressure
+    with pytest.raises(native.MicrophysicsError):
+        ctx.aero_rad_props_sw(p, 4, p, p, p, p, p, p, p, 0, 0, 1, 1, 1800.0)  # nlev < 2

@@ -193,3 +193,47 @@ def test_gas_chemistry_restatement_bitwise_on_host(ref_oracle, tmp_path):
         L.run(ctypes.c_int(q.shape[1]), ctypes.c_double(d["dt"]),
               *[ctypes.c_void_p(a.ctypes.data) for a in args], ctypes.c_void_p(q.ctypes.data))
         np.testing.assert_array_equal(q, r)
+
+
+_TROP_HOST = r'''
+#include "mam4b_optics.cuh"
+extern "C" void run(int ncol, int nlev, const double *temp, const double *pmid,
+                    const double *pint, int *out) {
+  for (int c = 0; c < ncol; ++c) {
+    auto T = [&](int k) { return temp[(size_t)c * nlev + k]; };
+    auto P = [&](int k) { return pmid[(size_t)c * nlev + k]; };
+    auto PI = [&](int k) { return pint[(size_t)c * (nlev + 1) + k]; };
+    out[c] = mam4b::rad::tropopause_level(T, P, PI, nlev);
+  }
+}
+'''
+
+
+def test_tropopause_restatement_equals_reference_on_host(ref_oracle, tmp_path):
+    """The kernel's WMO tropopause search compiled for the host finds the
+    reference's level (tropopause_twmo) on every column, including the
+    columns without a tropopause (level 0)."""
+    import shutil
+    import subprocess
+    from mam4xx_b200.workloads import make_rad_props_inputs
+    nvcc = shutil.which("nvcc")
+    if not nvcc:
+        pytest.skip("nvcc not found")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "trop_host.cu"
+    src.write_text(_TROP_HOST)
+    so = tmp_path / "trop_host.so"
+    subprocess.run([nvcc, "-std=c++17", "--expt-relaxed-constexpr", "-I",
+                    os.path.join(root, "mam4xx_b200", "csrc"), "-Xcompiler",
+                    "-fPIC,-ffp-contract=off", "-shared", str(src), "-o", str(so)], check=True)
+    L = ctypes.CDLL(str(so))
+    w = make_rad_props_inputs("c2", ncol=200, seed=5, no_tropopause_frac=0.2)
+    nc, nl = w["ncol"], w["nlev"]
+    x = w["in_slab"]
+    _, rt = ref_oracle.rad_props_volcanic(False, nc, nl, x, w["pint"], w["zi"], w["ext_lw"],
+                                          None, None, np.zeros((16, nc * nl)))
+    t, p, pi = (np.ascontiguousarray(a) for a in (x[0], x[1], w["pint"]))
+    got = np.zeros(nc, dtype=np.int32)
+    L.run(nc, nl, *[ctypes.c_void_p(a.ctypes.data) for a in (t, p, pi, got)])
+    np.testing.assert_array_equal(got, rt)
+    assert (rt == 0).sum() >= 10 and (rt > 20).sum() >= 100
