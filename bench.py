@@ -191,6 +191,7 @@ PROCESS_BYTES_PER_CELL = {"calcsize": (50 + 20 + 24 + 8) * 8, "coagulation": (42
                           "step_chem": (57 + 55 + 68 + 4) * 8,
                           "aero_rad_props_sw": (55 + 1 + 42 + 2 + 56) * 8,
                           "aero_rad_props_lw": (55 + 1 + 16 + 2 + 16) * 8,
+                          "dropmixnuc": (54 + 4 + 2 + 66) * 8,
                           "activation": (28 + 17) * 8, "optics_lw": (55 + 16) * 8,
                           "optics_sw": (55 + 56) * 8}
 
@@ -315,12 +316,24 @@ def processes_leg(native, torch, dev, stream, args, ws, hbm_peak):
                               rd["pint"].data_ptr(), rd["zi"].data_ptr(), rd["ext_lw"].data_ptr(),
                               otau.data_ptr(), 0, ncol, NLEV, d["dt"], stream=stream.cuda_stream)
 
+    from mam4xx_b200.workloads import make_dropmix_inputs
+    dw = make_dropmix_inputs(WORKLOAD, ncol=ncol, seed=20261203 + 12)
+    dd = {k: torch.from_numpy(np.ascontiguousarray(dw[k])).to(dev)
+          for k in ("in_slab", "mix", "pint", "kvh")}
+    d_out = torch.empty((66, n), dtype=torch.float64, device=dev)
+
+    def dropmix():
+        ctx.dropmixnuc(dd["in_slab"].data_ptr(), n, dd["mix"].data_ptr(), dd["pint"].data_ptr(),
+                       dd["kvh"].data_ptr(), d_out.data_ptr(), ncol, NLEV, 6, dw["dt"],
+                       stream=stream.cuda_stream)
+
     res = {}
     for name, f in (("calcsize", calcsize), ("coagulation", coag), ("setsox", setsox),
                     ("gas_chemistry", gas_chemistry), ("step_chem", step_chem),
                     ("activation", activation),
                     ("optics_lw", optics_lw), ("optics_sw", optics_sw),
-                    ("aero_rad_props_sw", rad_sw), ("aero_rad_props_lw", rad_lw)):
+                    ("aero_rad_props_sw", rad_sw), ("aero_rad_props_lw", rad_lw),
+                    ("dropmixnuc", dropmix)):
         for _ in range(args.warmup):
             f()
         if ws > 1:
@@ -377,11 +390,15 @@ def processes_leg(native, torch, dev, stream, args, ws, hbm_peak):
             from mam4xx_b200.workloads import pblh_per_cell
             r.step_chem(cw["in_slab"][:, sl], pblh_per_cell(cw)[sl], cw["chem_in"][:, sl], cw["dt"])
             t8 = time.perf_counter()
+            r.dropmixnuc(nc, NLEV, 6, True, dw["dt"], dw["in_slab"][:, sl], dw["mix"][:, sl],
+                         dw["pint"][:nc * (NLEV + 1)], dw["kvh"][:nc * (NLEV + 1)])
+            t9 = time.perf_counter()
             import multiprocessing
             for name, el in (("calcsize", t1 - t0), ("coagulation", t2 - t1),
                              ("setsox", t3 - t2), ("activation", t4 - t3),
                              ("optics_lw", t5 - t4), ("optics_sw", t6 - t5),
-                             ("gas_chemistry", t7 - t6), ("step_chem", t8 - t7)):
+                             ("gas_chemistry", t7 - t6), ("step_chem", t8 - t7),
+                             ("dropmixnuc", t9 - t8)):
                 res[name]["cpu_baseline"] = {
                     "value": m / el, "unit": "cells/s", "kind": "reference",
                     "cores": multiprocessing.cpu_count(),

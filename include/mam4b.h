@@ -399,7 +399,7 @@ mam4b_status mam4b_activate(mam4b_ctx *ctx, const double *in_slab, size_t ld,
  * (src/mam4xx/aero_rad_props.hpp:250-338, 339-410). The modal optics of
  * mam4b_optics_sw / mam4b_optics_lw (same arguments, same tables), then the
  * WMO lapse-rate tropopause of each column (tropopause_twmo,
- * src/mam4xx/tropopause.hpp:75-193) and the volcanic (CMIP6) stratospheric
+ * src/mam4xx/tropopause.hpp:81-233) and the volcanic (CMIP6) stratospheric
  * aerosol over them: averaged half and half at the tropopause level,
  * replacing the modal values above it.
  *
@@ -426,6 +426,57 @@ mam4b_status mam4b_aero_rad_props_lw(mam4b_ctx *ctx, const double *in_slab, size
                                      const double *pdeldry, const double *pint, const double *zi,
                                      const double *ext_lw, double *odap, int *trop_level,
                                      int ncol, int nlev, double dt, void *stream);
+
+/*
+ * Droplet activation and vertical mixing, batched over columns:
+ * mam4::ndrop::dropmixnuc (src/mam4xx/ndrop.hpp:1393-1714). Per level,
+ * from top_lev down: release of aerosol where the cloud shrank and
+ * activation where it grew (update_from_newcld), activation at cloud base
+ * from the level below (update_from_cldn_profile); then explicit,
+ * sub-stepped vertical mixing of droplets and of interstitial and
+ * cloud-borne aerosol (update_from_explmix); then tendencies and CCN.
+ *
+ *   in_slab    the step's input layout: temperature, pressure, height,
+ *              cloud fraction (the new one), the 25 interstitial
+ *              populations (state_q) and the 25 cloud-borne ones (qqcw)
+ *   mix_in     MAM4B_DROPMIX_NIN fields of ld doubles (below)
+ *   pint, kvh  interface pressure [Pa] and vertical diffusivity [m2/s],
+ *              nlev + 1 per column (top first): element col*(nlev+1) + k
+ *   out        MAM4B_DROPMIX_NOUT fields of ld doubles (below); above
+ *              top_lev the droplet number is the input one, wtke is set,
+ *              and every other field is zero (the cloud-borne aerosol is
+ *              removed there, as the reference does)
+ *   top_lev    first level treated, 1 <= top_lev <= nlev - 2 (the
+ *              reference reads one level above it)
+ *   vertical_mix  enable_aero_vertical_mix
+ * factnum starts at zero; rpdel is 1 / pdel. One block of 128 threads per
+ * column; about 1 KB of shared memory per level (at most ~200 levels).
+ * Asynchronous on `stream`.
+ */
+enum {
+  MAM4B_DROPMIX_IN_PDEL = 0,    /* layer pressure thickness [Pa] */
+  MAM4B_DROPMIX_IN_CLDO = 1,    /* cloud fraction of the previous step */
+  MAM4B_DROPMIX_IN_NCLDWTR = 2, /* cloud droplet number [#/kg] */
+  MAM4B_DROPMIX_IN_WSUB = 3,    /* subgrid vertical velocity [m/s] */
+  MAM4B_DROPMIX_NIN = 4
+};
+enum {
+  MAM4B_DROPMIX_OUT_QCLD = 0,     /* droplet number after mixing [#/kg] */
+  MAM4B_DROPMIX_OUT_TENDND = 1,   /* droplet number tendency [#/kg/s] */
+  MAM4B_DROPMIX_OUT_NSOURCE = 2,  /* droplet number source [#/kg/s] */
+  MAM4B_DROPMIX_OUT_NDROPMIX = 3, /* droplet number mixing [#/kg/s] */
+  MAM4B_DROPMIX_OUT_NDROPCOL = 4, /* column droplet number of the level [#/m2] */
+  MAM4B_DROPMIX_OUT_WTKE = 5,     /* turbulent vertical velocity [m/s] */
+  MAM4B_DROPMIX_OUT_FACTNUM = 6,  /* 4 activated number fractions */
+  MAM4B_DROPMIX_OUT_CCN = 10,     /* CCN at 0.02..1 % supersaturation [#/cm3], 6 */
+  MAM4B_DROPMIX_OUT_PTEND = 16,   /* 25 interstitial tendencies [kg/kg/s, #/kg/s] */
+  MAM4B_DROPMIX_OUT_QQCW = 41,    /* 25 cloud-borne populations after */
+  MAM4B_DROPMIX_NOUT = 66
+};
+mam4b_status mam4b_dropmixnuc(mam4b_ctx *ctx, const double *in_slab, size_t ld,
+                              const double *mix_in, const double *pint, const double *kvh,
+                              double *out, int ncol, int nlev, int top_lev, int vertical_mix,
+                              double dt, void *stream);
 
 /*
  * Aqueous-phase sulfate chemistry in cloud water, batched over cells:
@@ -466,7 +517,7 @@ mam4b_status mam4b_setsox(mam4b_ctx *ctx, const double *pressure, const double *
  * amicphys in the host model, for the mechanism of
  * src/mam4xx/gas_chem_mechanism.hpp: reaction rates (setrxt, usrrxt,
  * adjrxt), then imp_sol's implicit Euler step with Newton-Raphson iteration
- * and step control (src/mam4xx/gas_chem.hpp:262-426).
+ * and step control (src/mam4xx/gas_chem.hpp:234-424).
  *
  *   temperature [K], photo_rates (the one photolysis rate, of H2O2, 1/s):
  *              one value per cell

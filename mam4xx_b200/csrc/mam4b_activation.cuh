@@ -114,8 +114,9 @@ MAM4B_HD double max_supersat(double zeta, const double (&eta)[NMODE],
 // [kg/m3] at the level the aerosol is loaded from and at the cell, updraft
 // w [m/s], temperature. out: fn[4], fm[4], fluxn[4], fluxm[4],
 // flux_fullact (all zero when there is no accumulation-mode aerosol or no
-// updraft, the cases where activate_modal returns without writing).
-MAM4B_HD void activate_cell(const StepConsts &C, const double (&ai)[NPOP], double rho_load,
+// updraft, the cases where activate_modal returns without writing; the
+// return value is false then).
+MAM4B_HD bool activate_cell(const StepConsts &C, const double (&ai)[NPOP], double rho_load,
                             double rho, double w, double tair, double (&out)[17]) {
 #pragma unroll
   for (int k = 0; k < 17; ++k)
@@ -144,7 +145,7 @@ MAM4B_HD void activate_cell(const StepConsts &C, const double (&ai)[NPOP], doubl
   }
   // activate_modal with wmaxf = 10
   if (na[0] < 1.0e-20 || w <= 0.0)
-    return;
+    return false;
   const double wmaxf = 10.0;
   const double sq2 = sqrt(2.0);
   const double twothird = 2.0 / 3.0;
@@ -193,6 +194,7 @@ MAM4B_HD void activate_cell(const StepConsts &C, const double (&ai)[NPOP], doubl
     out[12 + m] = out[4 + m] * w;
   }
   out[16] = w;
+  return true;
 }
 
 }  // namespace act

@@ -2,8 +2,8 @@
 // mam4::microphysics::gas_phase_chemistry (src/mam4xx/gas_phase_chemistry.hpp:
 // 40-117) for the mechanism of src/mam4xx/gas_chem_mechanism.hpp (31 tracers,
 // 7 reactions, 30 implicit species): reaction rates, then the fully implicit
-// Euler step of imp_sol (src/mam4xx/gas_chem.hpp:262-426) with its
-// Newton-Raphson iteration (:77-260) and time-step control.
+// Euler step of imp_sol (src/mam4xx/gas_chem.hpp:234-424) with its
+// Newton-Raphson iteration (:73-231) and time-step control.
 //
 // The mechanism is linear in the tracers and nearly diagonal: implicit
 // species k is tracer k+1, and only two off-diagonal couplings exist, SO2 ->
@@ -32,14 +32,14 @@ constexpr double kRelErr = 1.0e-3;
 constexpr double kSmallForcing = 1.0e-40;
 
 // external forcing feeding implicit species k (-1: none), indprd class 4
-// (gas_chem_mechanism.hpp:102-142); species 0 (H2O2) gains r1 instead
+// (gas_chem_mechanism.hpp:101-140); species 0 (H2O2) gains r1 instead
 MAM4B_HD constexpr int ext_of_species(int k) {
   return k == 2 ? 0 : k == 4 ? 8 : k == 5 ? 1 : k == 12 ? 5 : k == 13 ? 2 : k == 17 ? 6
        : k == 26 ? 3 : k == 27 ? 4 : k == 29 ? 7 : -1;
 }
 
 // Reaction rates of the 7 reactions (setrxt, usrrxt, adjrxt;
-// gas_chem_mechanism.hpp:41-81, gas_chem.hpp:20-66): temperature and
+// gas_chem_mechanism.hpp:41-71, gas_chem.hpp:21-63): temperature and
 // invariant densities inv [molecules/cm3] (0 total, 3 H2O, 4 OH, 5 NO3,
 // 6 HO2), photolysis rate of H2O2 in r[0].
 MAM4B_HD void reaction_rates(double temp, double photo, const double (&inv)[kInv],

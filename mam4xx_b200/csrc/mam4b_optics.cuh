@@ -268,7 +268,7 @@ constexpr double kFaktor = -9.80616 / (kRgas / 0.028966);
 constexpr double kKa1 = kKap - 1.0;
 
 // lapse rate and mean temperature between two levels in p^kappa
-// (get_dtdz, tropopause.hpp:32-49)
+// (get_dtdz, tropopause.hpp:34-55)
 MAM4B_HD void lapse_rate(double pm, double pmk, double p_up, double p_down, double t_up,
                          double t_down, double &dtdz, double &tm) {
   const double a1 = (t_up - t_down) / (pow(p_up, kKap) - pow(p_down, kKap));
@@ -279,7 +279,7 @@ MAM4B_HD void lapse_rate(double pm, double pmk, double p_up, double p_down, doub
 }
 
 // WMO lapse-rate tropopause of a column (twmo, Reichler et al. 2003;
-// tropopause.hpp:75-171): scanning up from the surface, the first level
+// tropopause.hpp:81-204): scanning up from the surface, the first level
 // where the lapse rate falls below 2 K/km, between 75 and 450 hPa, and
 // stays below it on average over the 2 km above. Returns its pressure, or
 // -99 when there is none. temp(k), pmid(k): level k of the column, k = 0
@@ -330,7 +330,7 @@ MAM4B_HD double twmo_pressure(const ColT &temp, const ColP &pmid, int nlev) {
   return -99.0;
 }
 
-// tropopause_twmo (tropopause.hpp:173-193): the level k in [2, nlev-1],
+// tropopause_twmo (tropopause.hpp:210-233): the level k in [2, nlev-1],
 // scanning up, whose upper interface pressure pint(k) lies at or below the
 // tropopause pressure; 0 when there is no tropopause or no such level.
 template <class ColT, class ColP, class ColI>

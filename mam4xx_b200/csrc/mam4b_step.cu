@@ -27,6 +27,7 @@
 #include "mam4b_setsox.cuh"
 #include "mam4b_gaschem.cuh"
 #include "mam4b_activation.cuh"
+#include "mam4b_dropmix.cuh"
 #include "mam4b_optics.cuh"
 
 namespace mam4b {
@@ -2428,6 +2429,340 @@ __global__ void __launch_bounds__(128) volcanic_lw_kernel(const __grid_constant_
   }
 }
 
+// ---- droplet activation and vertical mixing (ndrop dropmixnuc), one
+// block per column; the levels are spread over the block's threads and
+// every phase that reads a neighbouring level is separated by a barrier.
+struct DropmixArgs {
+  const double *in[MAM4B_NIN];  // step input fields: T, p, z, cloud fraction, populations
+  const double *mix;            // [MAM4B_DROPMIX_NIN][ld]
+  const double *pint, *kvh;     // [col * (nlev + 1) + k]
+  double *out;                  // [MAM4B_DROPMIX_NOUT][ld]
+  unsigned *flags;
+  size_t ld;
+  int ncol, nlev, top_lev, vertical_mix;
+  double dt;
+};
+
+// shared-memory layout of one column (doubles)
+enum { DM_CS = 0, DM_DZ, DM_ZN, DM_ZS, DM_EDDY, DM_CSBOT, DM_CSBOT_CSCEN, DM_WTKE, DM_QCLD,
+       DM_QNCLD, DM_NSOURCE, DM_EKP, DM_EKM, DM_OVP, DM_OVM, DM_LEVEL_FIELDS };
+constexpr int kDmMaxSub = 100000;  // bound on the mixing sub-steps
+
+__global__ void __launch_bounds__(128) dropmix_kernel(const __grid_constant__ DropmixArgs a) {
+  extern __shared__ double sm[];
+  const StepConsts &C = c_k;
+  const int col = blockIdx.x, nlev = a.nlev, top = a.top_lev;
+  const size_t c0 = (size_t)col * nlev, i0 = (size_t)col * (nlev + 1), ld = a.ld;
+  double *lev = sm;                                       // [DM_LEVEL_FIELDS][nlev]
+  double *nact = sm + (size_t)DM_LEVEL_FIELDS * nlev;     // [nlev][NMODE]
+  double *mact = nact + (size_t)NMODE * nlev;             // [nlev][NMODE]
+  double *fnum = mact + (size_t)NMODE * nlev;             // [nlev][NMODE]
+  double *raer = fnum + (size_t)NMODE * nlev;             // [2][nlev][NPOP]
+  double *rcw = raer + (size_t)2 * NPOP * nlev;           // [2][nlev][NPOP]
+  auto L = [&](int f, int k) -> double & { return lev[(size_t)f * nlev + k]; };
+  auto R = [&](int b, int k, int p) -> double & { return raer[((size_t)b * nlev + k) * NPOP + p]; };
+  auto W = [&](int b, int k, int p) -> double & { return rcw[((size_t)b * nlev + k) * NPOP + p]; };
+  auto IN = [&](int f, int k) { return __ldg(a.in[f] + c0 + k); };
+  auto MIX = [&](int f, int k) { return __ldg(a.mix + (size_t)f * ld + c0 + k); };
+  auto load_ai = [&](int k, double (&ai)[NPOP]) {
+#pragma unroll
+    for (int p = 0; p < NPOP; ++p)
+      ai[p] = IN(MAM4B_IN_AER_I + p, k);
+  };
+  const double dt = a.dt, dtinv = 1.0 / dt;
+  const double gravity = act::kGravity, rair = act::kRAir;
+
+  // per-level quantities (dropmixnuc :1440-1490)
+  for (int k = threadIdx.x; k < nlev; k += blockDim.x) {
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      nact[k * NMODE + m] = 0.0;
+      mact[k * NMODE + m] = 0.0;
+      fnum[k * NMODE + m] = 0.0;  // factnum starts at zero
+    }
+    const double cs = IN(MAM4B_IN_P, k) / (rair * IN(MAM4B_IN_T, k));
+    const double rpdel = 1.0 / MIX(MAM4B_DROPMIX_IN_PDEL, k);
+    L(DM_CS, k) = cs;
+    L(DM_DZ, k) = 1.0 / (cs * gravity * rpdel);
+    L(DM_ZN, k) = gravity * rpdel;
+    L(DM_WTKE, k) = dmax(MIX(MAM4B_DROPMIX_IN_WSUB, k), 0.1);
+    L(DM_QCLD, k) = MIX(MAM4B_DROPMIX_IN_NCLDWTR, k);
+    L(DM_NSOURCE, k) = 0.0;
+    // levels above top_lev keep zero, as the reference's work arrays
+    L(DM_ZS, k) = 0.0;
+    L(DM_EDDY, k) = 0.0;
+    L(DM_CSBOT, k) = 0.0;
+    L(DM_CSBOT_CSCEN, k) = 0.0;
+    for (int p = 0; p < NPOP; ++p) {
+      R(0, k, p) = IN(MAM4B_IN_AER_I + p, k);
+      W(0, k, p) = IN(MAM4B_IN_AER_C + p, k);
+      R(1, k, p) = 0.0;
+      W(1, k, p) = 0.0;
+    }
+  }
+  __syncthreads();
+  for (int k = top + threadIdx.x; k < nlev; k += blockDim.x) {
+    if (k < nlev - 1) {
+      L(DM_ZS, k) = 1.0 / (IN(MAM4B_IN_ZM, k) - IN(MAM4B_IN_ZM, k + 1));
+      L(DM_EDDY, k) = bound(0.01, 100.0, __ldg(a.kvh + i0 + k + 1));
+      L(DM_CSBOT, k) =
+          2.0 * __ldg(a.pint + i0 + k + 1) / (rair * (IN(MAM4B_IN_T, k) + IN(MAM4B_IN_T, k + 1)));
+      L(DM_CSBOT_CSCEN, k) = L(DM_CSBOT, k) / L(DM_CS, k);
+    } else {
+      L(DM_ZS, k) = 1.0 / (IN(MAM4B_IN_ZM, k - 1) - IN(MAM4B_IN_ZM, k));
+      L(DM_EDDY, k) = 0.0;
+      L(DM_CSBOT, k) = IN(MAM4B_IN_P, k) / (rair * IN(MAM4B_IN_T, k));
+      L(DM_CSBOT_CSCEN, k) = 1.0;
+    }
+  }
+  __syncthreads();
+
+  // new cloud (update_from_newcld): shrinking cloud releases, growing cloud
+  // activates the level's own aerosol
+  for (int k = top + threadIdx.x; k < nlev; k += blockDim.x) {
+    const double cldn = IN(MAM4B_IN_CLD, k), cldo = MIX(MAM4B_DROPMIX_IN_CLDO, k);
+    const double delt_cld = cldn - cldo;
+    double &qcld = L(DM_QCLD, k), &nsource = L(DM_NSOURCE, k);
+    if (cldn < cldo) {
+      nsource += qcld * (cldn - cldo) / cldo * dtinv;
+      qcld *= (1.0 + (cldn - cldo) / cldo);
+      const double frac = (cldn - cldo) / cldo;
+#pragma unroll
+      for (int m = 0; m < NMODE; ++m)
+        for (int l = 0; l <= K::nspec(m); ++l) {
+          const int p = dmx::pop_of(m, l);
+          const double dact = W(0, k, p) * frac;
+          W(0, k, p) += dact;
+          R(0, k, p) -= dact;
+        }
+    }
+    if (cldn - cldo > 0.01) {
+      double ai[NPOP], o[17];
+      load_ai(k, ai);
+      const double cs = L(DM_CS, k);
+      if (act::activate_cell(C, ai, cs, cs, L(DM_WTKE, k), IN(MAM4B_IN_T, k), o)) {
+#pragma unroll
+        for (int m = 0; m < NMODE; ++m)
+          fnum[k * NMODE + m] = o[m];
+      } else {
+#pragma unroll
+        for (int m = 0; m < NMODE; ++m)
+          o[4 + m] = 0.0;  // fm stays zero, factnum as it was
+      }
+#pragma unroll
+      for (int m = 0; m < NMODE; ++m) {
+        const int pn = K::numslot(m);
+        const double dact = delt_cld * fnum[k * NMODE + m] * ai[pn];
+        qcld += dact;
+        nsource += dact * dtinv;
+        W(0, k, pn) += dact;
+        R(0, k, pn) -= dact;
+        const double fm_delt = delt_cld * o[4 + m];
+        for (int l = 1; l <= K::nspec(m); ++l) {
+          const int p = dmx::pop_of(m, l);
+          const double d = fm_delt * ai[p];
+          W(0, k, p) += d;
+          R(0, k, p) -= d;
+        }
+      }
+    }
+  }
+  __syncthreads();
+
+  // cloud-base activation (update_from_cldn_profile). A level reads the
+  // number of the level below it before that level clears its cloud, as
+  // in the reference's ascending order: reads and activation first, the
+  // clearing after a barrier.
+  for (int k = top + threadIdx.x; k < nlev - 1; k += blockDim.x) {
+    const double cldn = IN(MAM4B_IN_CLD, k), cldn1 = IN(MAM4B_IN_CLD, k + 1);
+    if (cldn > 0.01 && cldn - cldn1 > 0.01) {
+      L(DM_EDDY, k) = L(DM_WTKE, k) / L(DM_ZS, k);
+      double ai[NPOP], o[17];
+      load_ai(k + 1, ai);
+      const double cs = L(DM_CS, k);
+      if (act::activate_cell(C, ai, L(DM_CS, k + 1), cs, L(DM_WTKE, k), IN(MAM4B_IN_T, k), o)) {
+#pragma unroll
+        for (int m = 0; m < NMODE; ++m)
+          fnum[k * NMODE + m] = o[m];
+      } else {
+#pragma unroll
+        for (int m = 0; m < 8; ++m)
+          o[8 + m] = 0.0;
+      }
+      const double delz_cld = cldn - cldn1;
+      double fluxntot = 0.0;
+      const double crdz = L(DM_CSBOT_CSCEN, k) / L(DM_DZ, k);
+#pragma unroll
+      for (int m = 0; m < NMODE; ++m) {
+        nact[k * NMODE + m] += o[8 + m] * crdz * delz_cld;
+        mact[k * NMODE + m] += o[12 + m] * crdz * delz_cld;
+        fluxntot += o[8 + m] * delz_cld * R(0, k + 1, K::numslot(m)) * cs;
+      }
+      L(DM_NSOURCE, k) += fluxntot / (cs * L(DM_DZ, k));
+    }
+  }
+  __syncthreads();
+  for (int k = top + threadIdx.x; k < nlev - 1; k += blockDim.x) {
+    if (!(IN(MAM4B_IN_CLD, k) > 0.01)) {
+      L(DM_NSOURCE, k) -= L(DM_QCLD, k) * dtinv;
+      L(DM_QCLD, k) = 0.0;
+      for (int p = 0; p < NPOP; ++p) {
+        R(0, k, p) += W(0, k, p);
+        W(0, k, p) = 0.0;
+      }
+    }
+  }
+  __syncthreads();
+
+  // mixing set-up (update_from_explmix :1192-1225); the time-step bound is
+  // a minimum over levels, the same in any order
+  double dtmin = 1.79769313486231570e+308;
+  for (int k = top + threadIdx.x; k < nlev; k += blockDim.x) {
+    const int kp1 = k + 1 < nlev ? k + 1 : nlev - 1, km1 = k - 1 > top ? k - 1 : top;
+    const double cld = IN(MAM4B_IN_CLD, k), cldp = IN(MAM4B_IN_CLD, kp1), cldm = IN(MAM4B_IN_CLD, km1);
+    L(DM_OVP, k) = cldp > 1e-10 ? dmin(cld / cldp, 1.0) : 1.0;
+    L(DM_OVM, k) = cldm > 1e-10 ? dmin(cld / cldm, 1.0) : 1.0;
+    const double ekp = L(DM_ZN, k) * L(DM_EDDY, k) * L(DM_CSBOT, k) * L(DM_ZS, k);
+    // top_lev >= 1: level k - 1 exists (above top_lev its terms are zero)
+    const double ekm = L(DM_ZN, k) * L(DM_EDDY, k - 1) * L(DM_CSBOT, k - 1) * L(DM_ZS, km1);
+    L(DM_EKP, k) = ekp;
+    L(DM_EKM, k) = ekm;
+    const double tinv = ekp + ekm;
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      nact[k * NMODE + m] = dmin(nact[k * NMODE + m], ekp);
+      mact[k * NMODE + m] = dmin(mact[k * NMODE + m], ekp);
+    }
+    if (tinv > 1e-6)
+      dtmin = dmin(dtmin, 1.0 / tinv);
+  }
+  // block-wide minimum through shared memory (the level fields' DM_QNCLD
+  // row is free until the sub-steps)
+  __shared__ double red[32];
+  for (int o = 16; o > 0; o >>= 1)
+    dtmin = dmin(dtmin, __shfl_down_sync(0xffffffffu, dtmin, o));
+  if ((threadIdx.x & 31) == 0)
+    red[threadIdx.x >> 5] = dtmin;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double v = red[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+      v = dmin(v, red[w]);
+    red[0] = v;
+  }
+  __syncthreads();
+  dtmin = red[0];
+  double dtmix = 0.9 * dtmin;
+  const double nsub_d = dt / dtmix + 1;
+  int nsubmix = nsub_d < (double)kDmMaxSub ? (int)nsub_d : kDmMaxSub;
+  if (!(nsub_d < (double)kDmMaxSub) && threadIdx.x == 0)
+    atomicOr(a.flags, MAM4B_FLAG_NONFINITE_OUTPUT);
+  dtmix = dt / nsubmix;
+
+  int nsav = 0, nnew = 1;
+  for (int isub = 0; isub < nsubmix; ++isub) {
+    if (isub > 0) {
+      const int t = nsav;
+      nsav = nnew;
+      nnew = t;
+    }
+    for (int k = top + threadIdx.x; k < nlev; k += blockDim.x)
+      L(DM_QNCLD, k) = L(DM_QCLD, k);
+    __syncthreads();
+    for (int k = top + threadIdx.x; k < nlev; k += blockDim.x) {
+      const int kp1 = k + 1 < nlev ? k + 1 : nlev - 1, km1 = k - 1 > top ? k - 1 : top;
+      const double ekp = L(DM_EKP, k), ekm = L(DM_EKM, k), ovp = L(DM_OVP, k), ovm = L(DM_OVM, k);
+      double srcn = 0.0;
+#pragma unroll
+      for (int m = 0; m < NMODE; ++m) {
+        const int pn = K::numslot(m);
+        srcn += nact[k * NMODE + m] * R(nsav, kp1, pn);
+        if (k == nlev - 1) {
+          const double tmpa = R(nsav, k, pn) * nact[k * NMODE + m] + W(nsav, k, pn) * nact[k * NMODE + m];
+          srcn += dmax(0.0, tmpa);
+        }
+      }
+      if (a.vertical_mix)
+        L(DM_QCLD, k) = dmx::explmix(L(DM_QNCLD, km1), L(DM_QNCLD, k), L(DM_QNCLD, kp1), srcn, ekp,
+                                     ekm, ovp, ovm, dtmix);
+#pragma unroll
+      for (int m = 0; m < NMODE; ++m)
+        for (int l = 0; l <= K::nspec(m); ++l) {
+          const int p = dmx::pop_of(m, l);
+          double source;
+          if (k < nlev - 1) {
+            const double act = l ? mact[k * NMODE + m] : nact[k * NMODE + m];
+            source = act * R(nsav, kp1, p);
+          } else {
+            const double tmpa = R(nsav, k, p) * nact[k * NMODE + m] + W(nsav, k, p) * nact[k * NMODE + m];
+            source = dmax(0.0, tmpa);
+          }
+          W(nnew, k, p) = dmx::explmix(W(nsav, km1, p), W(nsav, k, p), W(nsav, kp1, p), source,
+                                       ekp, ekm, ovp, ovm, dtmix);
+          if (a.vertical_mix)
+            R(nnew, k, p) = dmx::explmix_act(R(nsav, km1, p), R(nsav, k, p), R(nsav, kp1, p),
+                                             source, ekp, ekm, ovp, ovm, dtmix, W(nsav, km1, p),
+                                             W(nsav, kp1, p));
+        }
+    }
+    __syncthreads();
+  }
+
+  // clear-sky levels give their cloud-borne aerosol back; outputs
+  for (int k = threadIdx.x; k < nlev; k += blockDim.x) {
+    const size_t c = c0 + k;
+    double *o = a.out + c;
+    o[(size_t)MAM4B_DROPMIX_OUT_WTKE * ld] = L(DM_WTKE, k);
+    if (k < top) {
+      o[(size_t)MAM4B_DROPMIX_OUT_QCLD * ld] = L(DM_QCLD, k);
+      for (int f = MAM4B_DROPMIX_OUT_TENDND; f < MAM4B_DROPMIX_NOUT; ++f)
+        if (f != MAM4B_DROPMIX_OUT_WTKE)
+          o[(size_t)f * ld] = 0.0;
+      continue;
+    }
+    const double ncldwtr = MIX(MAM4B_DROPMIX_IN_NCLDWTR, k);
+    if (IN(MAM4B_IN_CLD, k) == 0.0) {
+      L(DM_QCLD, k) = 0.0;
+      for (int p = 0; p < NPOP; ++p) {
+        R(nnew, k, p) += W(nnew, k, p);
+        W(nnew, k, p) = 0.0;
+      }
+    }
+    const double qcld = L(DM_QCLD, k);
+    o[(size_t)MAM4B_DROPMIX_OUT_QCLD * ld] = qcld;
+    o[(size_t)MAM4B_DROPMIX_OUT_NDROPMIX * ld] = (qcld - ncldwtr) * dtinv - L(DM_NSOURCE, k);
+    o[(size_t)MAM4B_DROPMIX_OUT_TENDND * ld] = (dmax(qcld, 1.e-6) - ncldwtr) * dtinv;
+    o[(size_t)MAM4B_DROPMIX_OUT_NDROPCOL * ld] = ncldwtr * MIX(MAM4B_DROPMIX_IN_PDEL, k) / gravity;
+    o[(size_t)MAM4B_DROPMIX_OUT_NSOURCE * ld] = L(DM_NSOURCE, k);
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m)
+      o[(size_t)(MAM4B_DROPMIX_OUT_FACTNUM + m) * ld] = fnum[k * NMODE + m];
+    double ai[NPOP], qcb_shift[NMODE][7], qcb_num[NMODE];
+    load_ai(k, ai);
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+#pragma unroll
+      for (int s = 0; s < 7; ++s)
+        qcb_shift[m][s] = 0.0;
+      for (int l = 0; l <= K::nspec(m); ++l) {
+        const int p = dmx::pop_of(m, l);
+        const double q = dmax(W(nnew, k, p), 0.0);
+        o[(size_t)(MAM4B_DROPMIX_OUT_QQCW + p) * ld] = q;
+        o[(size_t)(MAM4B_DROPMIX_OUT_PTEND + p) * ld] = (R(nnew, k, p) - ai[p]) * dtinv;
+        if (l == 0)
+          qcb_num[m] = q;
+        else if (l < K::nspec(m))
+          qcb_shift[m][l] = q;  // species l - 1's mass, read as species l
+      }
+    }
+    double ccn[dmx::kPsat];
+    dmx::ccn_cell(C, ai, qcb_shift, qcb_num, IN(MAM4B_IN_T, k), L(DM_CS, k), ccn);
+#pragma unroll
+    for (int l = 0; l < dmx::kPsat; ++l)
+      o[(size_t)(MAM4B_DROPMIX_OUT_CCN + l) * ld] = ccn[l];
+  }
+}
+
 }  // namespace mam4b
 
 // =============================================================== C ABI
@@ -3560,6 +3895,51 @@ mam4b_status mam4b_aero_rad_props_lw(mam4b_ctx *ctx, const double *in_slab, size
   const size_t n = (size_t)ncol * nlev;
   volcanic_lw_kernel<<<(unsigned)((n + block - 1) / block), block, 0, s>>>(r);
   const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, what, e);
+  ctx->launches += 1;
+  return MAM4B_OK;
+}
+
+// ndrop::dropmixnuc (ndrop.hpp:1393-1714), one block per column
+mam4b_status mam4b_dropmixnuc(mam4b_ctx *ctx, const double *in_slab, size_t ld,
+                              const double *mix_in, const double *pint, const double *kvh,
+                              double *out, int ncol, int nlev, int top_lev, int vertical_mix,
+                              double dt, void *stream) {
+  const char *what = "mam4b_dropmixnuc";
+  const size_t n = (size_t)(ncol > 0 ? ncol : 0) * (size_t)(nlev > 0 ? nlev : 0);
+  if (!ctx || !in_slab || !mix_in || !pint || !kvh || !out || ncol < 0 || nlev < 2 || ld < n ||
+      top_lev < 1 || top_lev > nlev - 2 || !(dt > 0.0) || !isfinite(dt))
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, what, cudaSuccess);
+  const size_t smem = (size_t)nlev * (DM_LEVEL_FIELDS + 3 * NMODE + 4 * NPOP) * sizeof(double);
+  if (smem > 200 * 1024)
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_dropmixnuc: too many levels",
+                   cudaSuccess);
+  DropmixArgs a;
+  memset(&a, 0, sizeof(a));
+  for (int f = 0; f < MAM4B_NIN; ++f)
+    a.in[f] = in_slab + (size_t)f * ld;
+  a.mix = mix_in;
+  a.pint = pint;
+  a.kvh = kvh;
+  a.out = out;
+  a.flags = ctx->d_flags;
+  a.ld = ld;
+  a.ncol = ncol;
+  a.nlev = nlev;
+  a.top_lev = top_lev;
+  a.vertical_mix = vertical_mix ? 1 : 0;
+  a.dt = dt;
+  cudaStream_t s = (cudaStream_t)stream;
+  ctx->last_stream = s;
+  if (n == 0)
+    return MAM4B_OK;
+  cudaError_t e = cudaFuncSetAttribute(dropmix_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, what, e);
+  dropmix_kernel<<<(unsigned)ncol, 128, smem, s>>>(a);
+  e = cudaGetLastError();
   if (e != cudaSuccess)
     return set_err(ctx, MAM4B_ERR_CUDA, what, e);
   ctx->launches += 1;

@@ -135,6 +135,8 @@ def lib():
         L.mam4b_aero_rad_props_sw.restype = I
         L.mam4b_aero_rad_props_lw.argtypes = [P, P, S, P, P, P, P, P, P, I, I, D, P]
         L.mam4b_aero_rad_props_lw.restype = I
+        L.mam4b_dropmixnuc.argtypes = [P, P, S, P, P, P, P, I, I, I, I, D, P]
+        L.mam4b_dropmixnuc.restype = I
         PF = ctypes.POINTER(ProgFields)
         P4 = ctypes.c_void_p * NUM_MODES
         L.mam4b_calcsize_process.argtypes = [P, ctypes.POINTER(CalcSizeConfig), PF, PF,
@@ -156,7 +158,8 @@ EXPORTED = ["mam4b_abi_version", "mam4b_default_config", "mam4b_create", "mam4b_
             "mam4b_step_tracers", "mam4b_setsox", "mam4b_gas_chemistry", "mam4b_step_chem_slab",
             "mam4b_activate",
             "mam4b_optics_lw_set_tables", "mam4b_optics_lw", "mam4b_optics_sw_set_tables",
-            "mam4b_optics_sw", "mam4b_aero_rad_props_sw", "mam4b_aero_rad_props_lw"]
+            "mam4b_optics_sw", "mam4b_aero_rad_props_sw", "mam4b_aero_rad_props_lw",
+            "mam4b_dropmixnuc"]
 
 
 def default_config(**overrides):
@@ -327,6 +330,15 @@ class Context:
                                                ext_lw, odap, trop_level or None, int(ncol),
                                                int(nlev), float(dt), ctypes.c_void_p(stream))
         self._check(st, "mam4b_aero_rad_props_lw")
+
+    def dropmixnuc(self, in_ptr, ld, mix_in, pint, kvh, out, ncol, nlev, top_lev, dt,
+                   vertical_mix=True, stream=0):
+        """ndrop::dropmixnuc over ncol columns (mam4b_dropmixnuc)."""
+        st = self._lib.mam4b_dropmixnuc(self._h, in_ptr, int(ld), mix_in, pint, kvh, out,
+                                        int(ncol), int(nlev), int(top_lev),
+                                        int(bool(vertical_mix)), float(dt),
+                                        ctypes.c_void_p(stream))
+        self._check(st, "mam4b_dropmixnuc")
 
     def gas_chemistry(self, temperature, photo_rates, extfrc, invariants, het_rates, qq, ld,
                       ncol, nlev, dt, stream=0):

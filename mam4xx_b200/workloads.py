@@ -396,6 +396,33 @@ def make_rad_props_inputs(name="c2", ncol=None, nlev=None, seed=None, no_tropopa
     return w
 
 
+DROPMIX_NIN, DROPMIX_NOUT = 4, 66
+
+
+def make_dropmix_inputs(name="c2", ncol=None, nlev=None, seed=None):
+    """Inputs of the droplet activation and mixing entry (dropmixnuc): the
+    atmosphere and aerosol of make_rad_props_inputs (hypsometric heights,
+    interfaces) with the workload's cloud fraction as the new one; the
+    previous cloud fraction differs from it by U(-0.3, 0.3) in 70 % of the
+    cells (clipped to [0, 1]); droplet number log-uniform 1e6..1e9 #/kg
+    where there was cloud; subgrid updraft U(0.02, 2) m/s; vertical
+    diffusivity log-uniform 1e-3..200 m2/s at the interfaces."""
+    w = dict(make_rad_props_inputs(name, ncol=ncol, nlev=nlev, seed=seed))
+    n = w["in_slab"].shape[1]
+    rng = np.random.default_rng(8191 + (seed or 0))
+    cldn = w["in_slab"][4]
+    cldo = np.where(rng.uniform(0, 1, n) < 0.7,
+                    np.clip(cldn + rng.uniform(-0.3, 0.3, n), 0.0, 1.0), cldn)
+    mix = np.zeros((DROPMIX_NIN, n))
+    mix[0] = w["pdeldry"]
+    mix[1] = cldo
+    mix[2] = np.where(cldo > 0, _logu(rng, 1e6, 1e9, n), 0.0)
+    mix[3] = rng.uniform(0.02, 2.0, n)
+    w["mix"] = mix
+    w["kvh"] = _logu(rng, 1e-3, 200.0, w["ncol"] * (w["nlev"] + 1))
+    return w
+
+
 def make_activation_inputs(name="c2", ncol=None, nlev=None, seed=None):
     """Inputs of the activation entry: a workload's input slab, the air
     density p / (R_air T) and an updraft log-uniform 0.01..3 m/s, zero or

@@ -210,6 +210,19 @@ class ReferenceOracle(_Oracle):
           arrs[4].ctypes.data if sw else None, out.ctypes.data, trop.ctypes.data)
         return out, trop
 
+    def dropmixnuc(self, ncol, nlev, top_lev, vertical_mix, dt, in_slab, mix, pint, kvh):
+        """ndrop::dropmixnuc column by column; returns out (66, ncell) in
+        the layout of MAM4B_DROPMIX_OUT_*."""
+        x = np.ascontiguousarray(in_slab, dtype=np.float64)
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (mix, pint, kvh)]
+        out = np.zeros((66, x.shape[1]))
+        f = self.lib.mam4ref_dropmixnuc
+        f.argtypes = [_I, _I, _I, _I, _D] + [_P] * 5
+        f.restype = None
+        f(ncol, nlev, top_lev, int(bool(vertical_mix)), dt, x.ctypes.data,
+          *[a.ctypes.data for a in arrs], out.ctypes.data)
+        return out
+
     def maxsat(self, zeta, eta, smc):
         """ndrop::maxsat for 4 modes."""
         f = self.lib.mam4ref_maxsat

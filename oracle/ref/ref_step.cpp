@@ -761,6 +761,95 @@ void mam4ref_rad_props_volcanic(int sw, int ncol, int nlev, const double *in, co
   }
 }
 
+// ndrop::dropmixnuc column by column (OpenMP over columns) on the step's
+// input layout (in [NIN][n]), mix [4][n] (pdel, cldo, ncldwtr, wsub), pint
+// and kvh (nlev + 1 per column); rpdel = 1 / pdel, factnum and every work
+// array start at zero. out [66][n] in the layout of MAM4B_DROPMIX_OUT_*
+// (populations in the step's order; the reference's qqcw_fld is in its own
+// per-mode number-first order).
+void mam4ref_dropmixnuc(int ncol, int nlev, int top_lev, int vertical_mix, double dt,
+                        const double *in, const double *mix, const double *pint,
+                        const double *kvh, double *out) {
+  namespace nd = mam4::ndrop;
+  using V1 = mam4::ColumnView;
+  using V2 = nd::View2D;
+  using V3 = nd::View3D;
+  constexpr int nm = 4, np = MAM4B_NUM_POPS;
+  const size_t n = (size_t)ncol * nlev;
+  int nspec_amode[nd::maxd_aspectype] = {}, numptr_amode[nm];
+  int lspectype_amode[nd::maxd_aspectype][nm], lmassptr_amode[nd::maxd_aspectype][nm];
+  Real specdens_amode[nd::maxd_aspectype], spechygro[nd::maxd_aspectype];
+  int mam_idx[nm][nd::nspec_max], mam_cnst_idx[nm][nd::nspec_max];
+  nd::get_e3sm_parameters(nspec_amode, lspectype_amode, lmassptr_amode, numptr_amode,
+                          specdens_amode, spechygro, mam_idx, mam_cnst_idx);
+  Real exp45logsig[nm], alogsig[nm], aten, n2v_min[nm], n2v_max[nm];
+  nd::ndrop_init(exp45logsig, alogsig, aten, n2v_min, n2v_max);
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int col = 0; col < ncol; ++col) {
+    const size_t c0 = (size_t)col * nlev, i0 = (size_t)col * (nlev + 1);
+    auto colv = [&](const double *base) { return mam4::ConstColumnView(base + c0, nlev); };
+    std::vector<double> rpdel_v(nlev), wsub_v(nlev), cldo_v(nlev);
+    for (int k = 0; k < nlev; ++k) {
+      rpdel_v[k] = 1.0 / mix[0 * n + c0 + k];
+      cldo_v[k] = mix[1 * n + c0 + k];
+      wsub_v[k] = mix[3 * n + c0 + k];
+    }
+    V2 sq("state_q", nlev, mam4::aero_model::pcnst);
+    V2 qqcw("qqcw", nd::ncnst_tot, nlev);
+    for (int k = 0; k < nlev; ++k)
+      for (int p = 0; p < np; ++p)
+        sq(k, 15 + p) = in[(size_t)(MAM4B_IN_AER_I + p) * n + c0 + k];
+    for (int m = 0; m < nm; ++m)
+      for (int l = 0; l <= nspec_amode[m]; ++l) {
+        const int mm = mam_idx[m][l] - 1, q = mam_cnst_idx[m][l] - 1 - 15;
+        for (int k = 0; k < nlev; ++k)
+          qqcw(mm, k) = in[(size_t)(MAM4B_IN_AER_C + q) * n + c0 + k];
+      }
+    V1 qcld("qcld", nlev), wsub(wsub_v.data(), nlev), cldo(cldo_v.data(), nlev);
+    V2 ptend("ptend", mam4::aero_model::pcnst, nlev), factnum("factnum", nm, nlev);
+    V1 tendnd("tendnd", nlev), ndropcol("ndropcol", nlev), ndropmix("ndropmix", nlev),
+        nsource("nsource", nlev), wtke("wtke", nlev);
+    V2 ccn("ccn", nlev, nd::psat), coltend("coltend", nd::ncnst_tot, nlev),
+        coltend_cw("coltend_cw", nd::ncnst_tot, nlev);
+    V3 raercol_cw("raercol_cw", nlev, 2, nd::ncnst_tot), raercol("raercol", nlev, 2, nd::ncnst_tot);
+    V2 nact("nact", nlev, nm), mact("mact", nlev, nm);
+    V1 w[15];
+    for (auto &v : w)
+      v = V1("work", nlev);
+    mam4::ThreadTeam team;
+    nd::dropmixnuc(team, dt, colv(in + (size_t)MAM4B_IN_T * n), colv(in + (size_t)MAM4B_IN_P * n),
+                   mam4::ConstColumnView(pint + i0, nlev + 1), colv(mix + 0 * n),
+                   mam4::ConstColumnView(rpdel_v.data(), nlev), colv(in + (size_t)MAM4B_IN_ZM * n),
+                   sq, colv(mix + 2 * n), mam4::ConstColumnView(kvh + i0, nlev + 1),
+                   colv(in + (size_t)MAM4B_IN_CLD * n), lspectype_amode, specdens_amode, spechygro,
+                   lmassptr_amode, n2v_min, n2v_max, numptr_amode, nspec_amode, exp45logsig,
+                   alogsig, aten, mam_idx, mam_cnst_idx, vertical_mix != 0, qcld, wsub, cldo, qqcw,
+                   ptend, tendnd, factnum, ndropcol, ndropmix, nsource, wtke, ccn, coltend,
+                   coltend_cw, top_lev, raercol_cw, raercol, nact, mact, w[0], w[1], w[2], w[3],
+                   w[4], w[5], w[6], w[7], w[8], w[9], w[10], w[11], w[12], w[13], w[14]);
+    auto O = [&](int f, int k) -> double & { return out[(size_t)f * n + c0 + k]; };
+    for (int k = 0; k < nlev; ++k) {
+      O(MAM4B_DROPMIX_OUT_QCLD, k) = qcld(k);
+      O(MAM4B_DROPMIX_OUT_TENDND, k) = tendnd(k);
+      O(MAM4B_DROPMIX_OUT_NSOURCE, k) = nsource(k);
+      O(MAM4B_DROPMIX_OUT_NDROPMIX, k) = ndropmix(k);
+      O(MAM4B_DROPMIX_OUT_NDROPCOL, k) = ndropcol(k);
+      O(MAM4B_DROPMIX_OUT_WTKE, k) = wtke(k);
+      for (int m = 0; m < nm; ++m)
+        O(MAM4B_DROPMIX_OUT_FACTNUM + m, k) = factnum(m, k);
+      for (int l = 0; l < nd::psat; ++l)
+        O(MAM4B_DROPMIX_OUT_CCN + l, k) = ccn(k, l);
+      for (int p = 0; p < np; ++p)
+        O(MAM4B_DROPMIX_OUT_PTEND + p, k) = ptend(15 + p, k);
+      for (int m = 0; m < nm; ++m)
+        for (int l = 0; l <= nspec_amode[m]; ++l) {
+          const int mm = mam_idx[m][l] - 1, q = mam_cnst_idx[m][l] - 1 - 15;
+          O(MAM4B_DROPMIX_OUT_QQCW + q, k) = qqcw(mm, k);
+        }
+    }
+  }
+}
+
 double mam4ref_maxsat(double zeta, const double *eta, const double *smc) {
   Real e[4], sm[4], smax = 0;
   for (int m = 0; m < 4; ++m) {

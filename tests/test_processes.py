@@ -237,3 +237,24 @@ def test_tropopause_restatement_equals_reference_on_host(ref_oracle, tmp_path):
     L.run(nc, nl, *[ctypes.c_void_p(a.ctypes.data) for a in (t, p, pi, got)])
     np.testing.assert_array_equal(got, rt)
     assert (rt == 0).sum() >= 10 and (rt > 20).sum() >= 100
+
+
+def test_reference_dropmixnuc_properties(ref_oracle):
+    """The reference's dropmixnuc on the seeded column inputs: finite,
+    non-negative droplet number and cloud-borne aerosol, and above top_lev
+    the droplet number passed through and the cloud-borne aerosol removed."""
+    from mam4xx_b200.workloads import make_dropmix_inputs
+    w = make_dropmix_inputs("c2", ncol=8, seed=2)
+    out = ref_oracle.dropmixnuc(w["ncol"], w["nlev"], 6, True, w["dt"], w["in_slab"], w["mix"],
+                                w["pint"], w["kvh"])
+    assert np.isfinite(out).all()
+    assert (out[0] >= 0).all() and (out[41:66] >= 0).all()
+    above = np.arange(out.shape[1]) % w["nlev"] < 6
+    np.testing.assert_array_equal(out[0, above], w["mix"][2, above])
+    assert (out[41:66, above] == 0).all()
+
+
+def test_dropmixnuc_rejects_bad_arguments_without_a_device():
+    L = native.lib()
+    assert L.mam4b_dropmixnuc(None, None, 0, None, None, None, None, 1, 72, 6, 1, 1.0,
+                              None) == 1
