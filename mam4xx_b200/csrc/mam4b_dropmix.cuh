@@ -22,6 +22,10 @@ constexpr int kPsat = 6;  // supersaturations of the CCN diagnostic
 // population of species l of mode m in the reference's per-mode order:
 // l = 0 the number, l >= 1 species l - 1
 MAM4B_HD constexpr int pop_of(int m, int l) { return l == 0 ? K::numslot(m) : K::spec0(m) + l - 1; }
+// mode of population p (its species, then its number, mode by mode)
+MAM4B_HD constexpr int mode_of(int p) {
+  return p <= K::numslot(0) ? 0 : p <= K::numslot(1) ? 1 : p <= K::numslot(2) ? 2 : 3;
+}
 
 // explmix (ndrop.hpp:1090-1110): droplet number and cloud-borne aerosol
 MAM4B_HD double explmix(double qkm1, double qk, double qkp1, double src, double ekp, double ekm,

@@ -278,24 +278,36 @@ MAM4B_HD void lapse_rate(double pm, double pmk, double p_up, double p_down, doub
   dtdz = kFaktor * dtdp * pm / tm;
 }
 
-// WMO lapse-rate tropopause of a column (twmo, Reichler et al. 2003;
-// tropopause.hpp:81-204): scanning up from the surface, the first level
-// where the lapse rate falls below 2 K/km, between 75 and 450 hPa, and
-// stays below it on average over the 2 km above. Returns its pressure, or
-// -99 when there is none. temp(k), pmid(k): level k of the column, k = 0
-// at the top.
+// The lapse-rate quantities of the layer between levels k - 1 and k
+// (k >= 1): mean p^kappa, mean pressure, dT/dz and mean temperature, as
+// twmo computes them for its scan (tropopause.hpp:114-119, 124-129,
+// 171-188); the same values wherever the scan asks for them.
+struct LapsePair {
+  double pmk, pm, dtdz, tm;
+};
 template <class ColT, class ColP>
-MAM4B_HD double twmo_pressure(const ColT &temp, const ColP &pmid, int nlev) {
+MAM4B_HD LapsePair lapse_pair(const ColT &temp, const ColP &pmid, int k) {
+  LapsePair q;
+  q.pmk = 0.5 * (pow(pmid(k - 1), kKap) + pow(pmid(k), kKap));
+  q.pm = pow(q.pmk, (1.0 / kKap));
+  lapse_rate(q.pm, q.pmk, pmid(k - 1), pmid(k), temp(k - 1), temp(k), q.dtdz, q.tm);
+  return q;
+}
+
+// WMO lapse-rate tropopause of a column (twmo, Reichler et al. 2003;
+// tropopause.hpp:81-204) from its layers' lapse-rate quantities pair(k),
+// k = 1 .. nlev-1: scanning up from the surface, the first layer where the
+// lapse rate falls below 2 K/km, between 75 and 450 hPa, and stays below
+// it on average over the 2 km above. Returns its pressure, or -99 when
+// there is none.
+template <class Pairs>
+MAM4B_HD double twmo_from_pairs(const Pairs &pair, int nlev) {
   const double gam = -0.002, plimu = 45000, pliml = 7500, deltaz = 2000.0;
-  double pmk = 0.5 * (pow(pmid(nlev - 2), kKap) + pow(pmid(nlev - 1), kKap));
-  double pm = pow(pmk, (1.0 / kKap));
-  double dtdz, tm;
-  lapse_rate(pm, pmk, pmid(nlev - 2), pmid(nlev - 1), temp(nlev - 2), temp(nlev - 1), dtdz, tm);
+  LapsePair cur = pair(nlev - 1);
   for (int k = nlev - 2; k >= 1; --k) {
-    const double pmk0 = pmk, dtdz0 = dtdz;
-    pmk = 0.5 * (pow(pmid(k - 1), kKap) + pow(pmid(k), kKap));
-    pm = pow(pmk, (1.0 / kKap));
-    lapse_rate(pm, pmk, pmid(k - 1), pmid(k), temp(k - 1), temp(k), dtdz, tm);
+    const double pmk0 = cur.pmk, dtdz0 = cur.dtdz;
+    cur = pair(k);
+    const double pmk = cur.pmk, pm = cur.pm, dtdz = cur.dtdz, tm = cur.tm;
     if (dtdz <= gam || pm > plimu)
       continue;
     double ptph;
@@ -312,15 +324,12 @@ MAM4B_HD double twmo_pressure(const ColT &temp, const ColP &pmid, int nlev) {
     double asum = 0.0;
     int icount = 0;
     for (int j = k; j >= 1; --j) {
-      const double pmk2 = 0.5 * (pow(pmid(j - 1), kKap) + pow(pmid(j), kKap));
-      const double pm2 = pow(pmk2, 1.0 / kKap);
-      if (pm2 > ptph)
+      const LapsePair up = pair(j);
+      if (up.pm > ptph)
         continue;
-      if (pm2 < p2km)
+      if (up.pm < p2km)
         return ptph;  // the layer above stays stable: tropopause found
-      double dtdz2 = 0.0, tm2 = 0.0;
-      lapse_rate(pm2, pmk2, pmid(j - 1), pmid(j), temp(j - 1), temp(j), dtdz2, tm2);
-      asum += dtdz2;
+      asum += up.dtdz;
       icount++;
       const double aquer = asum / double(icount);
       if (aquer <= gam)
@@ -330,18 +339,25 @@ MAM4B_HD double twmo_pressure(const ColT &temp, const ColP &pmid, int nlev) {
   return -99.0;
 }
 
-// tropopause_twmo (tropopause.hpp:210-233): the level k in [2, nlev-1],
-// scanning up, whose upper interface pressure pint(k) lies at or below the
-// tropopause pressure; 0 when there is no tropopause or no such level.
-template <class ColT, class ColP, class ColI>
-MAM4B_HD int tropopause_level(const ColT &temp, const ColP &pmid, const ColI &pint, int nlev) {
-  const double tp = twmo_pressure(temp, pmid, nlev);
+// tropopause_twmo's level search (tropopause.hpp:222-231) for tropopause
+// pressure tp: the level k in [2, nlev-1], scanning up, whose upper
+// interface pressure pint(k) lies at or below tp; 0 when tp is not
+// positive or no level qualifies.
+template <class ColI>
+MAM4B_HD int tropopause_level_at(double tp, const ColI &pint, int nlev) {
   if (tp > 0) {
     for (int k = nlev - 1; k > 1; --k)
       if (tp >= pint(k))
         return k;
   }
   return 0;
+}
+
+// tropopause_twmo (tropopause.hpp:210-233) of one column, serially.
+template <class ColT, class ColP, class ColI>
+MAM4B_HD int tropopause_level(const ColT &temp, const ColP &pmid, const ColI &pint, int nlev) {
+  auto pair = [&](int k) { return lapse_pair(temp, pmid, k); };
+  return tropopause_level_at(twmo_from_pairs(pair, nlev), pint, nlev);
 }
 
 }  // namespace rad

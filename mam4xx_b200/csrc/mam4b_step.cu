@@ -2368,16 +2368,39 @@ struct RadArgs {
   int ncol, nlev;
 };
 
-// one thread per column (the search reads the column bottom up)
+// one warp per column: the lanes compute every layer's lapse-rate
+// quantities (the pow-heavy part) into shared memory, then one lane runs
+// the scan on them
 __global__ void __launch_bounds__(128) tropopause_kernel(const __grid_constant__ RadArgs r) {
-  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  extern __shared__ double tsm[];  // [warps][4][nlev]
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nlev = r.nlev;
+  const int col = blockIdx.x * (blockDim.x >> 5) + warp;
   if (col >= r.ncol)
-    return;
-  const size_t c0 = (size_t)col * r.nlev, i0 = (size_t)col * (r.nlev + 1);
+    return;  // the whole warp: col is the same on every lane
+  double *s = tsm + (size_t)warp * 4 * nlev;
+  const size_t c0 = (size_t)col * nlev, i0 = (size_t)col * (nlev + 1);
   auto T = [&](int k) { return __ldg(r.temp + c0 + k); };
   auto P = [&](int k) { return __ldg(r.pmid + c0 + k); };
-  auto PI = [&](int k) { return __ldg(r.pint + i0 + k); };
-  r.trop[col] = rad::tropopause_level(T, P, PI, r.nlev);
+  for (int k = 1 + lane; k < nlev; k += 32) {
+    const rad::LapsePair q = rad::lapse_pair(T, P, k);
+    s[k] = q.pmk;
+    s[nlev + k] = q.pm;
+    s[2 * nlev + k] = q.dtdz;
+    s[3 * nlev + k] = q.tm;
+  }
+  __syncwarp();
+  if (lane == 0) {
+    auto pair = [&](int k) {
+      rad::LapsePair q;
+      q.pmk = s[k];
+      q.pm = s[nlev + k];
+      q.dtdz = s[2 * nlev + k];
+      q.tm = s[3 * nlev + k];
+      return q;
+    };
+    auto PI = [&](int k) { return __ldg(r.pint + i0 + k); };
+    r.trop[col] = rad::tropopause_level_at(rad::twmo_from_pairs(pair, nlev), PI, nlev);
+  }
 }
 
 // volcanic_cmip_sw (aero_rad_props.hpp:38-119): at the tropopause level the
@@ -2448,9 +2471,21 @@ enum { DM_CS = 0, DM_DZ, DM_ZN, DM_ZS, DM_EDDY, DM_CSBOT, DM_CSBOT_CSCEN, DM_WTK
        DM_QNCLD, DM_NSOURCE, DM_EKP, DM_EKM, DM_OVP, DM_OVM, DM_LEVEL_FIELDS };
 constexpr int kDmMaxSub = 100000;  // bound on the mixing sub-steps
 
+// The activation and CCN code is called from several phases; kept out of
+// line so that the kernel's code stays small enough for the instruction
+// cache (inlined copies made instruction fetch the first stall).
+__device__ __noinline__ bool dm_activate(const double (&ai)[NPOP], double rho_load, double rho,
+                                         double w, double tair, double (&o)[17]) {
+  return act::activate_cell(c_k, ai, rho_load, rho, w, tair, o);
+}
+__device__ __noinline__ void dm_ccn(const double (&ai)[NPOP], const double (&qcb_shift)[NMODE][7],
+                                    const double (&qcb_num)[NMODE], double tair, double rho,
+                                    double (&ccn)[dmx::kPsat]) {
+  dmx::ccn_cell(c_k, ai, qcb_shift, qcb_num, tair, rho, ccn);
+}
+
 __global__ void __launch_bounds__(128) dropmix_kernel(const __grid_constant__ DropmixArgs a) {
   extern __shared__ double sm[];
-  const StepConsts &C = c_k;
   const int col = blockIdx.x, nlev = a.nlev, top = a.top_lev;
   const size_t c0 = (size_t)col * nlev, i0 = (size_t)col * (nlev + 1), ld = a.ld;
   double *lev = sm;                                       // [DM_LEVEL_FIELDS][nlev]
@@ -2540,7 +2575,7 @@ __global__ void __launch_bounds__(128) dropmix_kernel(const __grid_constant__ Dr
       double ai[NPOP], o[17];
       load_ai(k, ai);
       const double cs = L(DM_CS, k);
-      if (act::activate_cell(C, ai, cs, cs, L(DM_WTKE, k), IN(MAM4B_IN_T, k), o)) {
+      if (dm_activate(ai, cs, cs, L(DM_WTKE, k), IN(MAM4B_IN_T, k), o)) {
 #pragma unroll
         for (int m = 0; m < NMODE; ++m)
           fnum[k * NMODE + m] = o[m];
@@ -2580,7 +2615,7 @@ __global__ void __launch_bounds__(128) dropmix_kernel(const __grid_constant__ Dr
       double ai[NPOP], o[17];
       load_ai(k + 1, ai);
       const double cs = L(DM_CS, k);
-      if (act::activate_cell(C, ai, L(DM_CS, k + 1), cs, L(DM_WTKE, k), IN(MAM4B_IN_T, k), o)) {
+      if (dm_activate(ai, L(DM_CS, k + 1), cs, L(DM_WTKE, k), IN(MAM4B_IN_T, k), o)) {
 #pragma unroll
         for (int m = 0; m < NMODE; ++m)
           fnum[k * NMODE + m] = o[m];
@@ -2636,8 +2671,7 @@ __global__ void __launch_bounds__(128) dropmix_kernel(const __grid_constant__ Dr
     if (tinv > 1e-6)
       dtmin = dmin(dtmin, 1.0 / tinv);
   }
-  // block-wide minimum through shared memory (the level fields' DM_QNCLD
-  // row is free until the sub-steps)
+  // block-wide minimum: warp shuffles, then one value per warp in shared memory
   __shared__ double red[32];
   for (int o = 16; o > 0; o >>= 1)
     dtmin = dmin(dtmin, __shfl_down_sync(0xffffffffu, dtmin, o));
@@ -2659,51 +2693,53 @@ __global__ void __launch_bounds__(128) dropmix_kernel(const __grid_constant__ Dr
     atomicOr(a.flags, MAM4B_FLAG_NONFINITE_OUTPUT);
   dtmix = dt / nsubmix;
 
+  // sub-steps: one work item per (level, population) plus one per level for
+  // the droplet number, spread over the block; populations and droplet
+  // number double-buffered (nsav read, nnew written), one barrier per step
   int nsav = 0, nnew = 1;
+  auto Q = [&](int b, int k) -> double & { return L(b ? DM_QNCLD : DM_QCLD, k); };
+  const int nitem = (nlev - top) * (NPOP + 1);
   for (int isub = 0; isub < nsubmix; ++isub) {
     if (isub > 0) {
       const int t = nsav;
       nsav = nnew;
       nnew = t;
     }
-    for (int k = top + threadIdx.x; k < nlev; k += blockDim.x)
-      L(DM_QNCLD, k) = L(DM_QCLD, k);
-    __syncthreads();
-    for (int k = top + threadIdx.x; k < nlev; k += blockDim.x) {
+    for (int t = threadIdx.x; t < nitem; t += blockDim.x) {
+      const int k = top + t / (NPOP + 1), j = t % (NPOP + 1);
       const int kp1 = k + 1 < nlev ? k + 1 : nlev - 1, km1 = k - 1 > top ? k - 1 : top;
       const double ekp = L(DM_EKP, k), ekm = L(DM_EKM, k), ovp = L(DM_OVP, k), ovm = L(DM_OVM, k);
-      double srcn = 0.0;
+      if (j == NPOP) {
+        double srcn = 0.0;
 #pragma unroll
-      for (int m = 0; m < NMODE; ++m) {
-        const int pn = K::numslot(m);
-        srcn += nact[k * NMODE + m] * R(nsav, kp1, pn);
-        if (k == nlev - 1) {
-          const double tmpa = R(nsav, k, pn) * nact[k * NMODE + m] + W(nsav, k, pn) * nact[k * NMODE + m];
-          srcn += dmax(0.0, tmpa);
-        }
-      }
-      if (a.vertical_mix)
-        L(DM_QCLD, k) = dmx::explmix(L(DM_QNCLD, km1), L(DM_QNCLD, k), L(DM_QNCLD, kp1), srcn, ekp,
-                                     ekm, ovp, ovm, dtmix);
-#pragma unroll
-      for (int m = 0; m < NMODE; ++m)
-        for (int l = 0; l <= K::nspec(m); ++l) {
-          const int p = dmx::pop_of(m, l);
-          double source;
-          if (k < nlev - 1) {
-            const double act = l ? mact[k * NMODE + m] : nact[k * NMODE + m];
-            source = act * R(nsav, kp1, p);
-          } else {
-            const double tmpa = R(nsav, k, p) * nact[k * NMODE + m] + W(nsav, k, p) * nact[k * NMODE + m];
-            source = dmax(0.0, tmpa);
+        for (int m = 0; m < NMODE; ++m) {
+          const int pn = K::numslot(m);
+          srcn += nact[k * NMODE + m] * R(nsav, kp1, pn);
+          if (k == nlev - 1) {
+            const double tmpa = R(nsav, k, pn) * nact[k * NMODE + m] + W(nsav, k, pn) * nact[k * NMODE + m];
+            srcn += dmax(0.0, tmpa);
           }
-          W(nnew, k, p) = dmx::explmix(W(nsav, km1, p), W(nsav, k, p), W(nsav, kp1, p), source,
-                                       ekp, ekm, ovp, ovm, dtmix);
-          if (a.vertical_mix)
-            R(nnew, k, p) = dmx::explmix_act(R(nsav, km1, p), R(nsav, k, p), R(nsav, kp1, p),
-                                             source, ekp, ekm, ovp, ovm, dtmix, W(nsav, km1, p),
-                                             W(nsav, kp1, p));
         }
+        Q(nnew, k) = a.vertical_mix ? dmx::explmix(Q(nsav, km1), Q(nsav, k), Q(nsav, kp1), srcn,
+                                                   ekp, ekm, ovp, ovm, dtmix)
+                                    : Q(nsav, k);
+      } else {
+        const int p = j, m = dmx::mode_of(p);
+        double source;
+        if (k < nlev - 1) {
+          const double act = p == K::numslot(m) ? nact[k * NMODE + m] : mact[k * NMODE + m];
+          source = act * R(nsav, kp1, p);
+        } else {
+          const double tmpa = R(nsav, k, p) * nact[k * NMODE + m] + W(nsav, k, p) * nact[k * NMODE + m];
+          source = dmax(0.0, tmpa);
+        }
+        W(nnew, k, p) = dmx::explmix(W(nsav, km1, p), W(nsav, k, p), W(nsav, kp1, p), source, ekp,
+                                     ekm, ovp, ovm, dtmix);
+        if (a.vertical_mix)
+          R(nnew, k, p) = dmx::explmix_act(R(nsav, km1, p), R(nsav, k, p), R(nsav, kp1, p), source,
+                                           ekp, ekm, ovp, ovm, dtmix, W(nsav, km1, p),
+                                           W(nsav, kp1, p));
+      }
     }
     __syncthreads();
   }
@@ -2722,13 +2758,13 @@ __global__ void __launch_bounds__(128) dropmix_kernel(const __grid_constant__ Dr
     }
     const double ncldwtr = MIX(MAM4B_DROPMIX_IN_NCLDWTR, k);
     if (IN(MAM4B_IN_CLD, k) == 0.0) {
-      L(DM_QCLD, k) = 0.0;
+      Q(nnew, k) = 0.0;
       for (int p = 0; p < NPOP; ++p) {
         R(nnew, k, p) += W(nnew, k, p);
         W(nnew, k, p) = 0.0;
       }
     }
-    const double qcld = L(DM_QCLD, k);
+    const double qcld = Q(nnew, k);
     o[(size_t)MAM4B_DROPMIX_OUT_QCLD * ld] = qcld;
     o[(size_t)MAM4B_DROPMIX_OUT_NDROPMIX * ld] = (qcld - ncldwtr) * dtinv - L(DM_NSOURCE, k);
     o[(size_t)MAM4B_DROPMIX_OUT_TENDND * ld] = (dmax(qcld, 1.e-6) - ncldwtr) * dtinv;
@@ -2756,7 +2792,7 @@ __global__ void __launch_bounds__(128) dropmix_kernel(const __grid_constant__ Dr
       }
     }
     double ccn[dmx::kPsat];
-    dmx::ccn_cell(C, ai, qcb_shift, qcb_num, IN(MAM4B_IN_T, k), L(DM_CS, k), ccn);
+    dm_ccn(ai, qcb_shift, qcb_num, IN(MAM4B_IN_T, k), L(DM_CS, k), ccn);
 #pragma unroll
     for (int l = 0; l < dmx::kPsat; ++l)
       o[(size_t)(MAM4B_DROPMIX_OUT_CCN + l) * ld] = ccn[l];
@@ -3824,8 +3860,11 @@ static mam4b_status rad_props_tropopause(mam4b_ctx *ctx, const char *what, RadAr
     }
     r.trop = ctx->d_trop;
   }
-  const int block = 128;
-  tropopause_kernel<<<(unsigned)((r.ncol + block - 1) / block), block, 0, s>>>(r);
+  const int block = 128, per_block = block / 32;
+  const size_t smem = (size_t)per_block * 4 * r.nlev * sizeof(double);
+  if (smem > 48 * 1024)
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, what, cudaSuccess);
+  tropopause_kernel<<<(unsigned)((r.ncol + per_block - 1) / per_block), block, smem, s>>>(r);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess)
     return set_err(ctx, MAM4B_ERR_CUDA, what, e);
@@ -3938,7 +3977,9 @@ mam4b_status mam4b_dropmixnuc(mam4b_ctx *ctx, const double *in_slab, size_t ld,
                                        (int)smem);
   if (e != cudaSuccess)
     return set_err(ctx, MAM4B_ERR_CUDA, what, e);
-  dropmix_kernel<<<(unsigned)ncol, 128, smem, s>>>(a);
+  // one thread per level (whole warps, at most 128; larger columns loop)
+  const int block = nlev >= 128 ? 128 : ((nlev + 31) / 32) * 32;
+  dropmix_kernel<<<(unsigned)ncol, block, smem, s>>>(a);
   e = cudaGetLastError();
   if (e != cudaSuccess)
     return set_err(ctx, MAM4B_ERR_CUDA, what, e);
