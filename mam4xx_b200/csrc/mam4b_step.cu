@@ -2460,11 +2460,17 @@ struct DropmixArgs {
   const double *mix;            // [MAM4B_DROPMIX_NIN][ld]
   const double *pint, *kvh;     // [col * (nlev + 1) + k]
   double *out;                  // [MAM4B_DROPMIX_NOUT][ld]
+  double *act;                  // [DA_FIELDS][ncol * nlev]: activation results
   unsigned *flags;
   size_t ld;
   int ncol, nlev, top_lev, vertical_mix;
   double dt;
 };
+// activation results of a level, computed ahead by dropmix_act_kernel:
+// growing cloud (computed flag, fn, fm) and cloud base (flag, fn, fluxn,
+// fluxm)
+enum { DA_NEW_OK = 0, DA_NEW_FN = 1, DA_NEW_FM = 5, DA_BASE_OK = 9, DA_BASE_FN = 10,
+       DA_BASE_FLUXN = 14, DA_BASE_FLUXM = 18, DA_FIELDS = 22 };
 
 // shared-memory layout of one column (doubles)
 enum { DM_CS = 0, DM_DZ, DM_ZN, DM_ZS, DM_EDDY, DM_CSBOT, DM_CSBOT_CSCEN, DM_WTKE, DM_QCLD,
@@ -2484,6 +2490,54 @@ __device__ __noinline__ void dm_ccn(const double (&ai)[NPOP], const double (&qcb
   dmx::ccn_cell(c_k, ai, qcb_shift, qcb_num, tair, rho, ccn);
 }
 
+// The activations of every level (they read only the inputs), one thread
+// per cell, ahead of the column kernel: growing cloud activates the
+// level's own aerosol, a cloud base the aerosol of the level below.
+__global__ void __launch_bounds__(128) dropmix_act_kernel(const __grid_constant__ DropmixArgs a) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = (long long)a.ncol * a.nlev;
+  if (c >= n)
+    return;
+  const int k = (int)(c % a.nlev);
+  double *act = a.act + c;
+  act[(size_t)DA_NEW_OK * n] = 0.0;
+  act[(size_t)DA_BASE_OK * n] = 0.0;
+  if (k < a.top_lev)
+    return;
+  const double rair = act::kRAir;
+  auto IN = [&](int f, long long cc) { return __ldg(a.in[f] + cc); };
+  const double temp = IN(MAM4B_IN_T, c), cs = IN(MAM4B_IN_P, c) / (rair * temp);
+  const double wtke = dmax(__ldg(a.mix + (size_t)MAM4B_DROPMIX_IN_WSUB * a.ld + c), 0.1);
+  const double cldn = IN(MAM4B_IN_CLD, c);
+  double ai[NPOP], o[17];
+  if (cldn - __ldg(a.mix + (size_t)MAM4B_DROPMIX_IN_CLDO * a.ld + c) > 0.01) {
+#pragma unroll
+    for (int p = 0; p < NPOP; ++p)
+      ai[p] = IN(MAM4B_IN_AER_I + p, c);
+    const bool ok = dm_activate(ai, cs, cs, wtke, temp, o);
+    act[(size_t)DA_NEW_OK * n] = ok ? 1.0 : 0.0;
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      act[(size_t)(DA_NEW_FN + m) * n] = o[m];
+      act[(size_t)(DA_NEW_FM + m) * n] = o[4 + m];
+    }
+  }
+  if (k < a.nlev - 1 && cldn > 0.01 && cldn - IN(MAM4B_IN_CLD, c + 1) > 0.01) {
+#pragma unroll
+    for (int p = 0; p < NPOP; ++p)
+      ai[p] = IN(MAM4B_IN_AER_I + p, c + 1);
+    const double cs1 = IN(MAM4B_IN_P, c + 1) / (rair * IN(MAM4B_IN_T, c + 1));
+    const bool ok = dm_activate(ai, cs1, cs, wtke, temp, o);
+    act[(size_t)DA_BASE_OK * n] = ok ? 1.0 : 0.0;
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      act[(size_t)(DA_BASE_FN + m) * n] = o[m];
+      act[(size_t)(DA_BASE_FLUXN + m) * n] = o[8 + m];
+      act[(size_t)(DA_BASE_FLUXM + m) * n] = o[12 + m];
+    }
+  }
+}
+
 __global__ void __launch_bounds__(128) dropmix_kernel(const __grid_constant__ DropmixArgs a) {
   extern __shared__ double sm[];
   const int col = blockIdx.x, nlev = a.nlev, top = a.top_lev;
@@ -2499,6 +2553,8 @@ __global__ void __launch_bounds__(128) dropmix_kernel(const __grid_constant__ Dr
   auto W = [&](int b, int k, int p) -> double & { return rcw[((size_t)b * nlev + k) * NPOP + p]; };
   auto IN = [&](int f, int k) { return __ldg(a.in[f] + c0 + k); };
   auto MIX = [&](int f, int k) { return __ldg(a.mix + (size_t)f * ld + c0 + k); };
+  const size_t ncell = (size_t)a.ncol * nlev;
+  auto ACT = [&](int f, int k) { return a.act[(size_t)f * ncell + c0 + k]; };
   auto load_ai = [&](int k, double (&ai)[NPOP]) {
 #pragma unroll
     for (int p = 0; p < NPOP; ++p)
@@ -2572,17 +2628,14 @@ __global__ void __launch_bounds__(128) dropmix_kernel(const __grid_constant__ Dr
         }
     }
     if (cldn - cldo > 0.01) {
-      double ai[NPOP], o[17];
+      double ai[NPOP], fm[NMODE];
       load_ai(k, ai);
-      const double cs = L(DM_CS, k);
-      if (dm_activate(ai, cs, cs, L(DM_WTKE, k), IN(MAM4B_IN_T, k), o)) {
+      const bool ok = ACT(DA_NEW_OK, k) != 0.0;
 #pragma unroll
-        for (int m = 0; m < NMODE; ++m)
-          fnum[k * NMODE + m] = o[m];
-      } else {
-#pragma unroll
-        for (int m = 0; m < NMODE; ++m)
-          o[4 + m] = 0.0;  // fm stays zero, factnum as it was
+      for (int m = 0; m < NMODE; ++m) {
+        if (ok)
+          fnum[k * NMODE + m] = ACT(DA_NEW_FN + m, k);
+        fm[m] = ok ? ACT(DA_NEW_FM + m, k) : 0.0;  // else factnum as it was
       }
 #pragma unroll
       for (int m = 0; m < NMODE; ++m) {
@@ -2592,7 +2645,7 @@ __global__ void __launch_bounds__(128) dropmix_kernel(const __grid_constant__ Dr
         nsource += dact * dtinv;
         W(0, k, pn) += dact;
         R(0, k, pn) -= dact;
-        const double fm_delt = delt_cld * o[4 + m];
+        const double fm_delt = delt_cld * fm[m];
         for (int l = 1; l <= K::nspec(m); ++l) {
           const int p = dmx::pop_of(m, l);
           const double d = fm_delt * ai[p];
@@ -2612,26 +2665,20 @@ __global__ void __launch_bounds__(128) dropmix_kernel(const __grid_constant__ Dr
     const double cldn = IN(MAM4B_IN_CLD, k), cldn1 = IN(MAM4B_IN_CLD, k + 1);
     if (cldn > 0.01 && cldn - cldn1 > 0.01) {
       L(DM_EDDY, k) = L(DM_WTKE, k) / L(DM_ZS, k);
-      double ai[NPOP], o[17];
-      load_ai(k + 1, ai);
       const double cs = L(DM_CS, k);
-      if (dm_activate(ai, L(DM_CS, k + 1), cs, L(DM_WTKE, k), IN(MAM4B_IN_T, k), o)) {
-#pragma unroll
-        for (int m = 0; m < NMODE; ++m)
-          fnum[k * NMODE + m] = o[m];
-      } else {
-#pragma unroll
-        for (int m = 0; m < 8; ++m)
-          o[8 + m] = 0.0;
-      }
+      const bool ok = ACT(DA_BASE_OK, k) != 0.0;
       const double delz_cld = cldn - cldn1;
       double fluxntot = 0.0;
       const double crdz = L(DM_CSBOT_CSCEN, k) / L(DM_DZ, k);
 #pragma unroll
       for (int m = 0; m < NMODE; ++m) {
-        nact[k * NMODE + m] += o[8 + m] * crdz * delz_cld;
-        mact[k * NMODE + m] += o[12 + m] * crdz * delz_cld;
-        fluxntot += o[8 + m] * delz_cld * R(0, k + 1, K::numslot(m)) * cs;
+        if (ok)
+          fnum[k * NMODE + m] = ACT(DA_BASE_FN + m, k);
+        const double fluxn = ok ? ACT(DA_BASE_FLUXN + m, k) : 0.0;
+        const double fluxm = ok ? ACT(DA_BASE_FLUXM + m, k) : 0.0;
+        nact[k * NMODE + m] += fluxn * crdz * delz_cld;
+        mact[k * NMODE + m] += fluxm * crdz * delz_cld;
+        fluxntot += fluxn * delz_cld * R(0, k + 1, K::numslot(m)) * cs;
       }
       L(DM_NSOURCE, k) += fluxntot / (cs * L(DM_DZ, k));
     }
@@ -2848,6 +2895,8 @@ struct mam4b_ctx {
   size_t cap_optics_scr;
   int *d_trop;          // [cap_trop]: tropopause level per column (aero_rad_props)
   size_t cap_trop;
+  double *d_dmx;        // dropmixnuc activation results (DA_FIELDS per cell), grown
+  size_t cap_dmx;
   unsigned *d_bins;     // [2 kPassBins]: loops per pass count, start offsets
   int adj_soa_grid;
   size_t cap_adj;
@@ -3171,6 +3220,7 @@ mam4b_status mam4b_destroy(mam4b_ctx *ctx) {
   cudaFree(ctx->d_optics_scr);
   cudaFree(ctx->d_optics_sw);
   cudaFree(ctx->d_trop);
+  cudaFree(ctx->d_dmx);
   if (ctx->host_streams) {
     for (int k = 0; k < kHostStreams; ++k) {
       cudaStreamDestroy(ctx->hs[k]);
@@ -3973,17 +4023,21 @@ mam4b_status mam4b_dropmixnuc(mam4b_ctx *ctx, const double *in_slab, size_t ld,
   ctx->last_stream = s;
   if (n == 0)
     return MAM4B_OK;
-  cudaError_t e = cudaFuncSetAttribute(dropmix_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
+  cudaError_t e = grow(&ctx->d_dmx, &ctx->cap_dmx, (size_t)DA_FIELDS * n);
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_dropmixnuc scratch", e);
+  a.act = ctx->d_dmx;
+  e = cudaFuncSetAttribute(dropmix_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess)
     return set_err(ctx, MAM4B_ERR_CUDA, what, e);
+  dropmix_act_kernel<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(a);
   // one thread per level (whole warps, at most 128; larger columns loop)
   const int block = nlev >= 128 ? 128 : ((nlev + 31) / 32) * 32;
   dropmix_kernel<<<(unsigned)ncol, block, smem, s>>>(a);
   e = cudaGetLastError();
   if (e != cudaSuccess)
     return set_err(ctx, MAM4B_ERR_CUDA, what, e);
-  ctx->launches += 1;
+  ctx->launches += 2;
   return MAM4B_OK;
 }
 
