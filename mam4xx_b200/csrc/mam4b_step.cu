@@ -2231,12 +2231,16 @@ __global__ void __launch_bounds__(128) optics_mode_kernel(const __grid_constant_
   }
 }
 
+// The band is the grid's fastest index: the blocks of one group of cells
+// run back to back for every band, so each cell's inputs come from DRAM
+// once and from L2 for the other bands.
 __global__ void __launch_bounds__(128) optics_band_kernel(const __grid_constant__ OpticsLwArgs a) {
-  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= a.ncell)
-    return;
-  const int b = blockIdx.y;
+  const int b = blockIdx.x;
   const size_t n = (size_t)a.ncell;
+  for (long long cb = blockIdx.y; cb * blockDim.x < a.ncell; cb += gridDim.y) {
+  const long long c = cb * blockDim.x + threadIdx.x;
+  if (c >= a.ncell)
+    break;
   double ai[NPOP];
 #pragma unroll
   for (int p = 0; p < NPOP; ++p)
@@ -2255,6 +2259,7 @@ __global__ void __launch_bounds__(128) optics_band_kernel(const __grid_constant_
     tau += opt::mode_band_tau(a.tables, m, b, specvol, a.scr[(OS_QW + m) * n + c], cheb, mass);
   }
   a.tau[(size_t)b * a.ld + c] = tau;
+  }
 }
 
 // ---- shortwave aerosol optics (modal_aero_sw): optics_size_kernel, then
@@ -2304,13 +2309,15 @@ __global__ void __launch_bounds__(128) optics_sw_mode_kernel(const __grid_consta
   }
 }
 
+// band-fastest grid, as optics_band_kernel
 __global__ void __launch_bounds__(128) optics_sw_band_kernel(const __grid_constant__ OpticsSwArgs w) {
   const OpticsLwArgs &a = w.base;
-  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= a.ncell)
-    return;
-  const int b = blockIdx.y;
+  const int b = blockIdx.x;
   const size_t n = (size_t)a.ncell;
+  for (long long cb = blockIdx.y; cb * blockDim.x < a.ncell; cb += gridDim.y) {
+  const long long c = cb * blockDim.x + threadIdx.x;
+  if (c >= a.ncell)
+    break;
   double ai[NPOP];
 #pragma unroll
   for (int p = 0; p < NPOP; ++p)
@@ -2337,6 +2344,7 @@ __global__ void __launch_bounds__(128) optics_sw_band_kernel(const __grid_consta
 #pragma unroll
   for (int q = 0; q < 4; ++q)
     w.out[((size_t)q * opt::kSwBands + b) * a.ld + c] = sum[q];
+  }
 }
 
 // visible optical depth of each column: its levels' mode optical depths
@@ -3834,7 +3842,7 @@ mam4b_status mam4b_optics_sw(mam4b_ctx *ctx, const double *in_slab, size_t ld,
   const unsigned grid = (unsigned)((n + block - 1) / block);
   optics_size_kernel<<<grid, block, 0, s>>>(w.base);
   optics_sw_mode_kernel<<<dim3(grid, NMODE), block, 0, s>>>(w);
-  optics_sw_band_kernel<<<dim3(grid, opt::kSwBands), block, 0, s>>>(w);
+  optics_sw_band_kernel<<<dim3(opt::kSwBands, grid < 65535u ? grid : 65535u), block, 0, s>>>(w);
   int launches = 3;
   if (aodvis) {
     optics_sw_aod_kernel<<<(unsigned)((ncol + block - 1) / block), block, 0, s>>>(w);
@@ -3880,7 +3888,7 @@ mam4b_status mam4b_optics_lw(mam4b_ctx *ctx, const double *in_slab, size_t ld,
   const unsigned grid = (unsigned)((n + block - 1) / block);
   optics_size_kernel<<<grid, block, 0, s>>>(a);
   optics_mode_kernel<<<dim3(grid, NMODE), block, 0, s>>>(a);
-  optics_band_kernel<<<dim3(grid, opt::kLwBands), block, 0, s>>>(a);
+  optics_band_kernel<<<dim3(opt::kLwBands, grid < 65535u ? grid : 65535u), block, 0, s>>>(a);
   e = cudaGetLastError();
   if (e != cudaSuccess)
     return set_err(ctx, MAM4B_ERR_CUDA, what, e);
