@@ -258,3 +258,22 @@ def test_dropmixnuc_rejects_bad_arguments_without_a_device():
     L = native.lib()
     assert L.mam4b_dropmixnuc(None, None, 0, None, None, None, None, 1, 72, 6, 1, 1.0,
                               None) == 1
+
+
+def test_reference_chem_step_reduces_to_the_plain_step(ref_oracle):
+    """With every chemistry rate, forcing and the cloud water zero, the
+    reference composition of the step with chemistry (gas chemistry,
+    setsox, amicphys with the three states) equals the plain step bit for
+    bit; with active chemistry the H2SO4 tendency differs."""
+    from mam4xx_b200.workloads import make_chem_step_inputs, pblh_per_cell
+    for inert in (True, False):
+        w = make_chem_step_inputs("c2", ncol=16, inert=inert)
+        out, cout = ref_oracle.step_chem(w["in_slab"], pblh_per_cell(w), w["chem_in"], w["dt"])
+        plain = ref_oracle.step(w["in_slab"], pblh_per_cell(w), w["dt"])
+        assert np.isfinite(out).all() and np.isfinite(cout).all()
+        if inert:
+            np.testing.assert_array_equal(out, plain)
+            # the chemistry gases only pass through the mmr -> vmr -> mmr round trip
+            assert (np.abs(cout) <= 1e-12 * np.abs(w["chem_in"][:4]) / w["dt"]).all()
+        else:
+            assert (np.abs(out[0] - plain[0]) > 1e-6 * np.abs(plain[0])).mean() > 0.1
