@@ -2,12 +2,14 @@
 
 Workload: the uneven-batching configuration, 65,536 columns x 72 levels per
 GPU (4,718,592 cells), FP64, seeded synthetic inputs (mam4xx_b200.workloads
-'c4': H2SO4 1e-15..1e-8 mol/mol, cloud fraction 60% clear / 40% U(0.2, 1)).
-One step = calcsize + water uptake + amicphys over every cell, dt = 1800 s.
+'c4': H2SO4 1e-15..1e-8 mol/mol, cloud fraction 60% clear / 40% U(0.2, 1),
+mode numbers 1e5..1e6 #/kg so that the SOA condensation sub-step count
+ranges over 1..20 per cell). One step = calcsize + water uptake + amicphys
+over every cell, dt = 1800 s.
 
-  value  cells/s with inputs resident in HBM (one step = the six-kernel
-         pipeline behind mam4b_step_slab), whole job = all ranks' cells /
-         max-over-ranks time
+  value  cells/s with inputs resident in HBM (one step = the pipeline
+         behind mam4b_step_slab), whole job = all ranks' cells /
+         max-over-ranks time (mam4xx_b200.distributed.timed_steps)
   e2e    cells/s through the C ABI host entry (mam4b_step_host): pinned host
          slabs copied in, step, results copied out, every step
   roofline_fp64  algorithmic flops per cell (baseline/flops_per_cell.json,
@@ -15,20 +17,25 @@ One step = calcsize + water uptake + amicphys over every cell, dt = 1800 s.
          FP64 FMA peak measured in the same run (libmam4b_peaks.so)
   roofline  algorithmic HBM bytes (57 input + 68 output doubles per cell plus
          the per-column boundary-layer height) / measured step time (the
-         unit is one step, i.e. one pass of the six launches), against the
-         measured copy bandwidth of MEASURED_PEAKS.json; traffic = DRAM bytes
-         of the six launches from the committed ncu summary, per cell, times
-         the cells
+         unit is one step), against the measured copy bandwidth of
+         MEASURED_PEAKS.json; traffic = DRAM bytes per cell of the step's
+         kernels measured by ncu (baseline/dram_traffic.json) times the cells
   cpu_baseline  the mam4xx reference headers compiled for the host
-         (oracle/_ref, OpenMP) on a bounded sample of the same cells
+         (oracle/_ref, the tuned build, OpenMP) on a bounded sample of the
+         same cells; the compiler flags are stated in its "sample"
 
-  processes  the per-process entries (mam4b_calcsize_process,
-         mam4b_coagulation_process, mam4b_setsox, mam4b_activate,
-         mam4b_optics_lw, mam4b_optics_sw with seeded stand-in tables) on
-         the same columns,
-         and the step through mam4b_step_tracers: cells/s, the HBM
-         roofline of their algorithmic bytes, and the reference's own
-         process classes on the host as their CPU baseline
+  precisions  the mixed-precision forms on their configuration c3
+         (65,536 x 72, 30 % of cells near the renaming cut-off): cells/s,
+         speed-up over the FP64 step on the same cells, and every cell's
+         error against the FP64 result
+  adjoint  forward and adjoint time on c5 (16,384 x 72) and a central
+         finite-difference check of the gradient
+  processes  the per-process and downstream entries (CalcSize, Coagulation,
+         setsox, gas chemistry, the step with chemistry, activation, optics,
+         aero_rad_props, dropmixnuc) and the step through
+         mam4b_step_tracers: cells/s, the HBM roofline of their algorithmic
+         bytes, and the reference's own process classes on the host as their
+         CPU baseline
 
 --impl reference times that CPU implementation alone, as the reference arm.
 Multi-GPU: one process per GPU (torchrun); each rank owns its own 65,536
@@ -38,7 +45,6 @@ columns, no data exchange (cells are independent); timing is max over ranks.
 import argparse
 import json
 import os
-import re
 import subprocess
 import sys
 import time
@@ -51,6 +57,7 @@ sys.path.insert(0, ROOT)
 NCOL_PER_GPU = 65536
 NLEV = 72
 WORKLOAD = "c4"
+REF_SAMPLE_NCOL = 1024  # columns of the reference arm's per-step sample
 BYTES_PER_CELL = (57 + 68) * 8  # + 8 bytes of boundary-layer height per column
 METRIC = "cells/s per amicphys step, FP64 vs mixed @ stated err; adjoint/forward time"
 
@@ -97,14 +104,16 @@ def _fp_peaks():
     return res
 
 
-def _traffic_per_launch(ncell):
-    """DRAM bytes per launch from the committed ncu summary, scaled by cells."""
-    p = os.path.join(ROOT, "profiles", "step_pipeline_c4_ncu.md")
+def _traffic_per_launch(workload, ncell):
+    """DRAM bytes (read + write) of one step, from the per-cell traffic of
+    the step's kernels measured by ncu (baseline/dram_traffic.json), scaled
+    by the cells; None where no capture of this workload is recorded."""
+    p = os.path.join(ROOT, "baseline", "dram_traffic.json")
     if not os.path.exists(p):
         return None
-    txt = open(p).read()
-    m = re.search(r"traffic_bytes_per_cell:\s*([0-9.eE+-]+)", txt)
-    return None if not m else float(m.group(1)) * ncell
+    with open(p) as f:
+        d = json.load(f).get("configs", {}).get(workload)
+    return None if not d else float(d["bytes_per_cell"]) * ncell
 
 
 class ClockSampler:
@@ -160,11 +169,11 @@ class ClockSampler:
 
 
 def cpu_baseline(x, pblh_cell, dt, target_s=12.0):
-    """Times the reference headers built for the host (or the restatement
-    where that build is absent) on a bounded sample of the workload."""
+    """Times the reference headers built for the host (the tuned build where
+    the host has AVX2/FMA, else the parity build, else the restatement) on a
+    bounded sample of the workload, OpenMP over cells on every host core."""
     from oracle import pyoracle
-    orc = pyoracle.ReferenceOracle() if pyoracle.reference_available() else pyoracle.PortOracle()
-    kind = "reference" if pyoracle.reference_available() else "port"
+    orc, kind, flags = pyoracle.baseline_oracle()
     cores = os.cpu_count() or 1
     n0 = min(x.shape[1], 8 * 1024)
     t = time.perf_counter()
@@ -175,7 +184,8 @@ def cpu_baseline(x, pblh_cell, dt, target_s=12.0):
     orc.step(x[:, :n], pblh_cell[:n], dt, nthreads=cores)
     el = time.perf_counter() - t
     return {"value": n / el, "unit": "cells/s", "cores": cores, "kind": kind,
-            "sample": "first %d cells of the %s workload (%.1f s, OpenMP over cells)" % (n, WORKLOAD, el)}
+            "sample": "first %d cells of the %s workload (%.1f s, OpenMP over cells); %s"
+                      % (n, WORKLOAD, el, flags)}
 
 
 # algorithmic bytes per cell of the per-process entries (FP64): CalcSize
@@ -364,7 +374,7 @@ def processes_leg(native, torch, dev, stream, args, ws, hbm_peak):
     if not args.no_cpu_baseline and int(os.environ.get("RANK", "0")) == 0:
         try:
             from oracle.pyoracle import ReferenceOracle
-            r = ReferenceOracle()
+            r = ReferenceOracle()  # the process classes exist in the parity build
             nc = min(ncol, 256)
             m = nc * NLEV
             sl = slice(0, m)
@@ -567,11 +577,10 @@ def run_reference_arm(args):
         return 0
     from mam4xx_b200.workloads import make_workload, pblh_per_cell
     from oracle import pyoracle
-    orc = pyoracle.ReferenceOracle() if pyoracle.reference_available() else pyoracle.PortOracle()
-    kind = "reference" if pyoracle.reference_available() else "port"
+    orc, kind, flags = pyoracle.baseline_oracle()
     cores = os.cpu_count() or 1
     # a bounded sample per step: 1024 columns x 72 levels of the same workload
-    w = make_workload(WORKLOAD, ncol=1024)
+    w = make_workload(WORKLOAD, ncol=REF_SAMPLE_NCOL)
     x, pb, dt = w["in_slab"], pblh_per_cell(w), w["dt"]
     n = x.shape[1]
     for _ in range(args.warmup):
@@ -585,13 +594,77 @@ def run_reference_arm(args):
             "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": "%s sample %d columns x %d levels" % (WORKLOAD, 1024, NLEV),
-                       "ncol": 1024, "nlev": NLEV, "dt_s": dt},
+            "config": {"workload": _workload_name(NCOL_PER_GPU),
+                       "sample_per_step": "first %d columns x %d levels" % (REF_SAMPLE_NCOL, NLEV),
+                       "ncol": REF_SAMPLE_NCOL, "nlev": NLEV, "dt_s": dt},
             "cpu_baseline": {"value": v, "unit": "cells/s", "cores": cores, "kind": kind,
-                             "sample": "1024 columns x 72 levels per step, OpenMP over cells"},
+                             "sample": "%d columns x 72 levels of %s per step, OpenMP over cells; %s"
+                                       % (REF_SAMPLE_NCOL, WORKLOAD, flags)},
             "e2e": {"value": v, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def _workload_name(ncol):
+    return ("%s: uneven batching (SOA sub-steps 1..20 per cell), %d columns x %d levels per GPU, "
+            "FP64, dt=1800 s" % (WORKLOAD, ncol, NLEV))
+
+
+def _r(v, digits=4):
+    """Rounds floats (recursively) to `digits` significant digits so the
+    JSON line stays short."""
+    if isinstance(v, float):
+        return float("%.*g" % (digits, v)) if np.isfinite(v) else v
+    if isinstance(v, dict):
+        return {k: _r(x, digits) for k, x in v.items()}
+    if isinstance(v, (list, tuple)):
+        return [_r(x, digits) for x in v]
+    return v
+
+
+def mixed_leg(native, torch, dev, stream, args, ws, rank):
+    """Mixed precision on its configuration c3 (65,536 x 72, 30 % of cells
+    near the renaming cut-off): the FP64 step and both mixed forms timed on
+    the same resident inputs; every cell's error against this run's FP64
+    result (mam4xx_b200.precision.error_report_device)."""
+    from mam4xx_b200.distributed import EventClock, max_over_ranks, timed_steps
+    from mam4xx_b200.precision import error_report_device
+    from mam4xx_b200.workloads import make_workload
+    wm = make_workload("c3", ncol=args.ncol, seed=20261203 + 2 + 1000 * rank)
+    xm = torch.from_numpy(wm["in_slab"]).to(dev)
+    pbm = torch.from_numpy(wm["pblh"]).to(dev)
+    nm = xm.shape[1]
+    ref = torch.empty((native.NOUT, nm), dtype=torch.float64, device=dev)
+    got = torch.empty_like(ref)
+    ctx = native.Context()
+    res = {"workload": "c3: %d columns x %d levels, 30%% of cells near the renaming cut-off"
+                       % (wm["ncol"], NLEV)}
+    times = {}
+    for name, prec, o in (("fp64", native.FP64, ref), ("mixed", native.MIXED, got),
+                          ("mixed_fast", native.MIXED_FAST, got)):
+        def f(prec=prec, o=o):
+            ctx.step_slab(xm.data_ptr(), pbm.data_ptr(), o.data_ptr(), nm, wm["ncol"], NLEV,
+                          wm["dt"], precision=prec, stream=stream.cuda_stream)
+        ms, _, _ = timed_steps(f, args.steps, args.warmup, EventClock(stream),
+                               sync=torch.cuda.synchronize, device=dev)
+        times[name] = ms / args.steps
+        if name == "fp64":
+            res["fp64"] = {"value": ws * nm / (times[name] * 1e-3), "ms_per_step": times[name]}
+            continue
+        r = error_report_device(got, ref, xm, wm["dt"], tol=1e-5)
+        worst = sorted(range(native.NOUT), key=lambda k: -r["per_output_max"][k])[:6]
+        res[name] = {"value": ws * nm / (times[name] * 1e-3), "unit": "cells/s",
+                     "ms_per_step": times[name],
+                     "speedup_vs_fp64": max_over_ranks(times["fp64"] / times[name], dev),
+                     "err_vs_fp64": {"cells": r["cells"], "max": r["max"], "median": r["median"],
+                                     "cells_within_1e-5": r["cells_within_tol"],
+                                     "cells_outside_1e-5": r["cells_outside_tol"],
+                                     "cell_err_quantiles": r["cell_err_quantiles"],
+                                     "worst_outputs": {str(k): r["per_output_max"][k] for k in worst},
+                                     "per_output_max": r["per_output_max"],
+                                     "per_output_median": r["per_output_median"]}}
+    ctx.close()
+    return res
 
 
 def main():
@@ -618,6 +691,7 @@ def main():
     import torch
     import torch.distributed as dist
     from mam4xx_b200 import native
+    from mam4xx_b200.distributed import EventClock, sharded_rate, timed_steps
     from mam4xx_b200.workloads import make_workload, pblh_per_cell
 
     ws, rank, local = _dist()
@@ -628,6 +702,8 @@ def main():
                                 device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
     ncol = args.ncol
+    # weak scaling: rank r owns its own ncol columns (seeded by rank), the
+    # columns [r*ncol, (r+1)*ncol) of the whole job's batch
     w = make_workload(WORKLOAD, ncol=ncol, seed=20261203 + 3 + 1000 * rank)
     x_host = w["in_slab"]
     n = x_host.shape[1]
@@ -647,37 +723,21 @@ def main():
     torch.cuda.synchronize()
     flags = ctx.last_status()
 
-    # device-resident timing: every launch bracketed by events on its stream
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(args.steps)]
+    # device-resident timing: CUDA events on the launching stream, per step
     sampler = ClockSampler(local)
-    if ws > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    sampler.start()
-    time.sleep(0.5)  # nvidia-smi's first sample lands inside the timed region
+
+    def start_sampler():
+        sampler.start()
+        time.sleep(0.5)  # nvidia-smi's first sample lands inside the timed region
+
     launches0 = ctx.launch_count()
-    t_start = torch.cuda.Event(enable_timing=True)
-    t_end = torch.cuda.Event(enable_timing=True)
-    t_start.record(stream)
-    for i in range(args.steps):
-        evs[i][0].record(stream)
-        step()
-        evs[i][1].record(stream)
-    t_end.record(stream)
-    torch.cuda.synchronize()
-    if ws > 1:
-        dist.barrier()
+    ms_max, _, laps = timed_steps(step, args.steps, 0, EventClock(stream),
+                                  sync=torch.cuda.synchronize, device=dev, on_start=start_sampler)
     clocks = sampler.stop()
     launches = ctx.launch_count() - launches0
-    total_ms = t_start.elapsed_time(t_end)
-    kernel_ms = float(np.mean([a.elapsed_time(b) for a, b in evs]))
-    if ws > 1:
-        tt = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
-    ms_per_step = total_ms / args.steps
-    value = ws * n * args.steps / (total_ms * 1e-3)
+    kernel_ms = float(np.mean(laps))
+    ms_per_step = ms_max / args.steps
+    value = sharded_rate(n, args.steps, ms_max, device=dev)
 
     # end-to-end through the host entry of the C ABI
     e2e = None
@@ -686,67 +746,23 @@ def main():
         pbh = torch.from_numpy(w["pblh"]).pin_memory()
         oh = torch.empty((native.NOUT, n), dtype=torch.float64).pin_memory()
         ectx = native.Context()
-        for _ in range(2):
+
+        def host_step():
             ectx.step_host(xin.data_ptr(), pbh.data_ptr(), oh.data_ptr(), n, ncol, NLEV, dt,
                            stream=stream.cuda_stream)
         ke = max(2, min(args.steps, 5))
-        if ws > 1:
-            dist.barrier()
-        a0 = torch.cuda.Event(enable_timing=True)
-        a1 = torch.cuda.Event(enable_timing=True)
-        a0.record(stream)
-        for _ in range(ke):
-            ectx.step_host(xin.data_ptr(), pbh.data_ptr(), oh.data_ptr(), n, ncol, NLEV, dt,
-                           stream=stream.cuda_stream)
-        a1.record(stream)
-        torch.cuda.synchronize()
-        e_ms = a0.elapsed_time(a1)
-        if ws > 1:
-            tt = torch.tensor([e_ms], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            e_ms = float(tt.item())
-        e2e = {"value": ws * n * ke / (e_ms * 1e-3), "unit": "cells/s",
+        e_ms, _, _ = timed_steps(host_step, ke, 2, EventClock(stream),
+                                 sync=torch.cuda.synchronize, device=dev)
+        e2e = {"value": sharded_rate(n, ke, e_ms, device=dev), "unit": "cells/s",
                "h2d_bytes_per_step": int(native.NIN * n * 8 + ncol * 8),
                "d2h_bytes_per_step": int(native.NOUT * n * 8),
-               "steps": ke, "entry": "mam4b_step_host"}
+               "steps": ke, "entry": "mam4b_step_host (pinned host slabs)"}
         ectx.close()
+        del xin, oh
 
-    # mixed-precision forms: same workload, same timing, errors against the
-    # FP64 results of this run on a sample of the columns
     precisions = None
     if not args.no_mixed:
-        precisions = {}
-        n_s = min(n, 8192 * NLEV)
-        ref_s = out[:, :n_s].cpu().numpy()
-        from mam4xx_b200.precision import error_report
-        for name, prec in (("mixed", native.MIXED), ("mixed_fast", native.MIXED_FAST)):
-            for _ in range(args.warmup):
-                step(prec)
-            if ws > 1:
-                dist.barrier()
-            torch.cuda.synchronize()
-            m0 = torch.cuda.Event(enable_timing=True)
-            m1 = torch.cuda.Event(enable_timing=True)
-            m0.record(stream)
-            for _ in range(args.steps):
-                step(prec)
-            m1.record(stream)
-            torch.cuda.synchronize()
-            m_ms = m0.elapsed_time(m1)
-            if ws > 1:
-                tt = torch.tensor([m_ms], device=dev)
-                dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-                m_ms = float(tt.item())
-            r = error_report(out[:, :n_s].cpu().numpy(), ref_s, x_host[:, :n_s], dt, tol=1e-5)
-            precisions[name] = {
-                "value": ws * n * args.steps / (m_ms * 1e-3), "unit": "cells/s",
-                "ms_per_step": m_ms / args.steps, "speedup_vs_fp64": total_ms / m_ms,
-                "err_vs_fp64": {"sample_cells": n_s, "max": r["max"], "median": r["median"],
-                                "cells_within_1e-5": r["cells_within_tol"],
-                                "cell_err_quantiles": r["cell_err_quantiles"],
-                                "per_output_max": r["per_output_max"],
-                                "per_output_median": r["per_output_median"]}}
-        step(native.FP64)
+        precisions = mixed_leg(native, torch, dev, stream, args, ws, rank)
 
     adjoint = None
     if not args.no_adjoint:
@@ -772,35 +788,36 @@ def main():
                                   "the CPU restatement; + - * / one flop each, libm calls apart)"}
     alg_bytes = n * BYTES_PER_CELL + ncol * 8
     achieved = alg_bytes / (kernel_ms * 1e-3) / 1e9
-    traffic = _traffic_per_launch(n)
+    traffic = _traffic_per_launch(WORKLOAD, n)
     line = {
         "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded draws with the configuration's distributions)",
-        "config": {"workload": "%s: uneven batching, %d columns x %d levels per GPU, FP64, dt=1800 s"
-                               % (WORKLOAD, ncol, NLEV),
+        "config": {"workload": _workload_name(ncol),
                    "ncol_per_gpu": ncol, "nlev": NLEV, "cells_per_gpu": n,
                    "parallelism": "column shards, one per GPU" if ws > 1 else "single GPU",
                    "l2": "inputs (%.2f GB) larger than L2, no flush" % (native.NIN * n * 8 / 1e9)},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic,
-                     "peak_source": "%s copy bandwidth" % peak_kind,
-                     "kernel_ms": kernel_ms, "algorithmic_bytes_per_launch": alg_bytes},
-        "roofline_fp64": roof64,
-        "e2e": e2e,
-        "precisions": precisions,
-        "adjoint": adjoint,
-        "processes": processes,
         "gpu_launches": int(launches),
         "clocks": clocks,
         "device_flags": flags,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": "%s copy bandwidth" % peak_kind,
+                     "kernel_ms": kernel_ms, "algorithmic_bytes_per_launch": alg_bytes,
+                     "unit_of_launch": "one step (the pipeline behind mam4b_step_slab)"},
+        "roofline_fp64": roof64,
+        "e2e": e2e,
     }
     if rank == 0 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(x_host, pblh_per_cell(w), dt)
         except Exception as e:  # reported, never silently replaced
             line["cpu_baseline"] = {"error": str(e)}
+    # the long per-entry reports go last, rounded
+    line["processes"] = _r(processes, 3)
+    line["precisions"] = _r(precisions, 3)
+    line["adjoint"] = _r(adjoint, 4)
     if ws > 1:
         dist.barrier()
         dist.destroy_process_group()

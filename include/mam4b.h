@@ -215,8 +215,10 @@ mam4b_status mam4b_step_host(mam4b_ctx *ctx, const double *in_slab,
  * host models that forbid allocation after start-up because cudaMalloc and
  * cudaFree can synchronise the whole device and stall their other streams.
  * The same step as mam4b_step_slab (FP64, no diagnostics, same results),
- * with the working memory of the SOA condensation solver in one fixed
- * device array inside the library instead of context-owned allocations:
+ * with the whole pipeline scratch (the SOA solver's loop state, the
+ * hand-off between the pipeline kernels, the work queue and its counters,
+ * the per-cell auxiliaries) in one fixed device array inside the library
+ * instead of context-owned allocations:
  * MAM4B_NOALLOC_MAX_CELLS cells at most, about 16 MB, held on every GPU
  * that loads the library until the process exits. No context is needed.
  *

@@ -3475,8 +3475,9 @@ mam4b_status mam4b_step_host(mam4b_ctx *ctx, const double *in_slab, const double
 // kernels as mam4b_step, with their scratch in g_noalloc_scratch. Nothing
 // here allocates: set-up uses cudaGetSymbolAddress, a kernel, copies into
 // the constant bank and occupancy queries; each step clears the counters
-// with cudaMemsetAsync and launches three kernels. All calls share the
-// array, so calls that overlap on the GPU race.
+// with cudaMemsetAsync and launches the six pipeline kernels (size, mode,
+// pair, pre, soa, post), or the one full_kernel when condensation is off.
+// All calls share the array, so calls that overlap on the GPU race.
 mam4b_status mam4b_step_slab_noalloc(const mam4b_config *cfg, const double *in_slab,
                                      const double *pblh, double *out_slab, size_t ld, int ncol,
                                      int nlev, double dt, uint32_t *flags, void *stream) {

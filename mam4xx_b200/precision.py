@@ -38,3 +38,48 @@ def error_report(out, ref, in_slab, dt, tol=1e-5):
                                for q in (0.5, 0.9, 0.99, 0.999)},
         "tol": tol,
     }
+
+
+def error_report_device(out, ref, in_slab, dt, tol=1e-5, chunk=1 << 20):
+    """error_report over every cell, computed on the device in chunks of
+    cells (torch tensors (68, n), (68, n), (57, n) float64 on one device).
+    Per-output medians are taken over a seeded sample of 2^20 cells."""
+    import torch
+    n = out.shape[1]
+    per_out_max = torch.zeros(NOUT, dtype=torch.float64, device=out.device)
+    cell_err = torch.empty(n, dtype=torch.float64, device=out.device)
+    for c0 in range(0, n, chunk):
+        c1 = min(n, c0 + chunk)
+        q0 = in_slab[STATE0:STATE0 + 52, c0:c1].abs()
+        q1 = (in_slab[STATE0:STATE0 + 52, c0:c1] + ref[:52, c0:c1] * dt).abs()
+        e_t = (out[:52, c0:c1] - ref[:52, c0:c1]).abs() * dt / torch.clamp(torch.maximum(q0, q1),
+                                                                            min=1e-30)
+        e_d = (out[52:, c0:c1] - ref[52:, c0:c1]).abs() / torch.clamp(ref[52:, c0:c1].abs(),
+                                                                      min=1e-300)
+        e = torch.cat([e_t, e_d], dim=0)
+        e = torch.where(torch.isnan(e), torch.full_like(e, float("inf")), e)
+        per_out_max = torch.maximum(per_out_max, e.max(dim=1).values)
+        cell_err[c0:c1] = e.max(dim=0).values
+    g = torch.Generator(device="cpu").manual_seed(12345)
+    sample = torch.randperm(n, generator=g)[: min(n, 1 << 20)].to(out.device)
+    q0 = in_slab[STATE0:STATE0 + 52][:, sample].abs()
+    q1 = (in_slab[STATE0:STATE0 + 52][:, sample] + ref[:52][:, sample] * dt).abs()
+    e_t = (out[:52][:, sample] - ref[:52][:, sample]).abs() * dt / torch.clamp(
+        torch.maximum(q0, q1), min=1e-30)
+    e_d = (out[52:][:, sample] - ref[52:][:, sample]).abs() / torch.clamp(
+        ref[52:][:, sample].abs(), min=1e-300)
+    es = torch.cat([e_t, e_d], dim=0)
+    qs = (0.5, 0.9, 0.99, 0.999, 0.9999)
+    cq = torch.quantile(cell_err[sample], torch.tensor(qs, dtype=torch.float64,
+                                                       device=out.device))
+    return {
+        "cells": int(n),
+        "max": float(per_out_max.max()),
+        "median": float(es.median()),
+        "per_output_max": [float(v) for v in per_out_max.cpu()],
+        "per_output_median": [float(v) for v in es.median(dim=1).values.cpu()],
+        "cells_within_tol": float((cell_err <= tol).double().mean()),
+        "cells_outside_tol": int((cell_err > tol).sum()),
+        "cell_err_quantiles": {str(q): float(v) for q, v in zip(qs, cq.cpu())},
+        "tol": tol,
+    }

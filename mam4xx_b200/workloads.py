@@ -10,8 +10,17 @@ shapes and value distributions of the step's benchmark configurations:
   c3  65536 x 72, like c2 but 30% of cells get an Aitken number that puts the
       Aitken dry diameter within +-10% of the renaming cut-off diameter
   c4  65536 x 72, H2SO4 log-uniform 1e-15..1e-8 mol/mol, cloud fraction 0 for
-      60% of cells and U(0.2, 1) for 40% (uneven condensation sub-stepping)
+      60% of cells and U(0.2, 1) for 40%, mode numbers log-uniform
+      1e5..1e6 #/kg: the SOA condensation sub-step count then ranges over
+      1..20 per cell (uneven sub-stepping; the histogram measured on the
+      CPU oracle is baseline/soa_passes_c4.json, oracle/soa_pass_histogram.py)
   c5  16384 x 72, like c2 (adjoint configuration)
+  c4_stress  c4 with the common number range 1e5..1e10 #/kg: 1..1000
+      sub-steps per cell (mean about 80, a few cells at the cap of 1000)
+
+The sub-step count of the SOA loop (gasaerexch_soaexch.hpp:170-173) grows
+with the uptake rate times the time step, i.e. with the mode numbers; the
+H2SO4 range does not drive it.
 
 Common distributions (per cell): T ~ U(200, 310) K; RH ~ U(0.05, 0.99)
 converted to a vapour mixing ratio with the Magnus saturation formula used
@@ -71,8 +80,10 @@ CONFIGS = {
     "c2": dict(index=1, ncol=4096, nlev=72, clouds="uniform"),
     "c3": dict(index=2, ncol=65536, nlev=72, clouds="uniform", near_cutoff=0.3),
     "c4": dict(index=3, ncol=65536, nlev=72, clouds="bimodal",
-               h2so4_range=(1e-15, 1e-8)),
+               h2so4_range=(1e-15, 1e-8), number_range=(1e5, 1e6)),
     "c5": dict(index=4, ncol=16384, nlev=72, clouds="uniform"),
+    "c4_stress": dict(index=3, ncol=65536, nlev=72, clouds="bimodal",
+                      h2so4_range=(1e-15, 1e-8)),
 }
 
 DT = 1800.0
@@ -143,10 +154,11 @@ def make_workload(name="c1", ncol=None, nlev=None, seed=None):
     x[IN_H2SO4] = h2so4_vmr * ADV_MASS[2] / MW_DRY_AIR
     x[IN_SOAG] = soag_vmr * ADV_MASS[5] / MW_DRY_AIR
 
+    nlo, nhi = cfg.get("number_range", (1e5, 1e10))
     for base, cloudy in ((IN_AER_I, False), (IN_AER_C, True)):
         for slot, (mode, spec) in enumerate(POPULATIONS):
             if spec == "num":
-                v = _logu(rng, 1e5, 1e10, n)
+                v = _logu(rng, nlo, nhi, n)
             else:
                 v = _logu(rng, 1e-14, 1e-8, n)
             if cloudy and cfg["clouds"] == "none":

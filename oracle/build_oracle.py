@@ -15,10 +15,17 @@
                              when the reference tree exists (no cmake, no
                              Kokkos/EKAT: the shim stands in for the small
                              surface the headers use)
+  oracle/_ref/libmam4ref_tuned.so  the same reference build tuned for speed
+                             (-O3 -march=x86-64-v3: AVX2 and FMA, FP
+                             contraction allowed): the timed CPU baseline;
+                             loaded only on hosts with AVX2 and FMA
 
-Both use -O3 -ffp-contract=off so that every expression rounds in source
-order, and OpenMP for the multi-core CPU baseline. No -march=native: the
-libraries travel to other hosts.
+The parity builds use -O3 -ffp-contract=off so that every expression rounds
+in source order, and OpenMP for the multi-core CPU baseline. No
+-march=native: the libraries travel to other hosts.
+
+The mam4xx tree is taken from build(ref=...), else from the environment
+variable MAM4XX_REFERENCE, else from the default checkout location below.
 """
 
 import os
@@ -29,9 +36,11 @@ ROOT = os.path.dirname(HERE)
 PORT_SO = os.path.join(HERE, "libmam4oracle.so")
 ULP_SO = os.path.join(HERE, "libmam4oracle_ulp.so")
 REF_SO = os.path.join(HERE, "_ref", "libmam4ref.so")
+REF_TUNED_SO = os.path.join(HERE, "_ref", "libmam4ref_tuned.so")
 GPU_SO = os.path.join(HERE, "libmam4oracle_gpu.so")
 COUNT_SO = os.path.join(HERE, "libmam4oracle_count.so")
-DEFAULT_REF = "/root/reference"
+DEFAULT_REF = "/root/reference"  # default checkout of the mam4xx tree
+TUNED = ["-O3", "-march=x86-64-v3", "-ffp-contract=fast", "-fPIC", "-shared", "-fopenmp"]
 
 COMMON = ["-O3", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off"]
 
@@ -68,7 +77,7 @@ def build(ref=None, force=False):
         # single-threaded: the tally is one global
         _run(["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-ffp-contract=off",
               os.path.join(HERE, "opcount.cpp"), "-o", COUNT_SO, "-lm"])
-    ref = ref or DEFAULT_REF
+    ref = ref or os.environ.get("MAM4XX_REFERENCE") or DEFAULT_REF
     src = os.path.join(ref, "src")
     if os.path.isdir(os.path.join(src, "mam4xx")):
         shim = os.path.join(HERE, "shim")
@@ -77,6 +86,9 @@ def build(ref=None, force=False):
             os.makedirs(os.path.dirname(REF_SO), exist_ok=True)
             _run(["g++", "-std=c++17"] + COMMON + ["-I", shim, "-I", src,
                   os.path.join(HERE, "ref", "ref_step.cpp"), "-o", REF_SO])
+        if force or _stale(REF_TUNED_SO, rdeps):
+            _run(["g++", "-std=c++17"] + TUNED + ["-I", shim, "-I", src,
+                  os.path.join(HERE, "ref", "ref_step.cpp"), "-o", REF_TUNED_SO])
     return PORT_SO
 
 

@@ -16,6 +16,10 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_SO = os.path.join(HERE, "_ref", "libmam4ref.so")
+REF_TUNED_SO = os.path.join(HERE, "_ref", "libmam4ref_tuned.so")
+# compiler flags of the two reference builds (oracle/build_oracle.py)
+REF_FLAGS = "g++ -O3 -ffp-contract=off -fopenmp (parity build)"
+REF_TUNED_FLAGS = "g++ -O3 -march=x86-64-v3 -ffp-contract=fast -fopenmp (tuned build)"
 PORT_SO = os.path.join(HERE, "libmam4oracle.so")
 ULP_SO = os.path.join(HERE, "libmam4oracle_ulp.so")
 GPU_SO = os.path.join(HERE, "libmam4oracle_gpu.so")
@@ -313,6 +317,37 @@ class ReferenceOracle(_Oracle):
         f(ncol, nlev, dt, t.ctypes.data, p.ctypes.data, wet.ctypes.data, prog.ctypes.data,
           tend.ctypes.data)
         return prog, tend
+
+
+def _host_has_avx2_fma():
+    try:
+        with open("/proc/cpuinfo") as f:
+            flags = next((ln for ln in f if ln.startswith("flags")), "").split()
+    except OSError:
+        return False
+    return "avx2" in flags and "fma" in flags
+
+
+class TunedReferenceOracle(ReferenceOracle):
+    """The reference build tuned for speed (AVX2/FMA, FP contraction): the
+    timed CPU baseline. Its results differ from the parity build's in the
+    last bits (contracted multiply-adds); it is timed, never compared."""
+    path = REF_TUNED_SO
+    flags = REF_TUNED_FLAGS
+
+
+ReferenceOracle.flags = REF_FLAGS
+
+
+def baseline_oracle():
+    """(oracle, kind, flags) of the CPU baseline: the tuned reference build
+    where it exists and the host has AVX2 and FMA, else the parity build of
+    the reference, else the restatement."""
+    if os.path.exists(REF_TUNED_SO) and _host_has_avx2_fma():
+        return TunedReferenceOracle(), "reference", REF_TUNED_FLAGS
+    if reference_available():
+        return ReferenceOracle(), "reference", REF_FLAGS
+    return PortOracle(), "port", "gcc -O3 -ffp-contract=off -fopenmp (restatement)"
 
 
 class PortOracle(_Oracle):

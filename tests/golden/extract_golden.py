@@ -88,7 +88,9 @@ def extract_coag(ref):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    # the mam4xx tree: first argument, else MAM4XX_REFERENCE, else the default checkout
+    ref = (sys.argv[1] if len(sys.argv) > 1 else
+           os.environ.get("MAM4XX_REFERENCE", "/root/reference"))
     here = os.path.dirname(os.path.abspath(__file__))
     g = extract_gasaerexch(ref)
     assert len(g["in_qgas_cur"]) == 3 and len(g["in_qgas_cur"][0]) == 10

@@ -10,12 +10,17 @@ must equal that entry point's bit for bit (the exact-equality criterion of
 the other bitwise GPU tests), also on the second of two calls in a row,
 when the array still holds the first call's contents.
 
-The file is named to be collected last; the no-alloc call comes first in
-the GPU test so that, run alone in a fresh process, it also covers the
-one-time set-up (constant tables filled without an allocation).
+The file is named to be collected last. After other GPU tests have run in
+the same process, the constant tables are already on the device, so the
+set-up path that fills them through the fixed array without an allocation
+is covered by a fresh child process whose first CUDA work is a no-alloc
+call.
 """
 
 import ctypes
+import os
+import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -81,3 +86,72 @@ def test_noalloc_matches_step_slab_on_two_calls_in_a_row():
         r = ref.cpu().numpy()
         assert np.isfinite(g).all()
         assert np.array_equal(g, r), "no-alloc step differs from mam4b_step_slab"
+
+
+def _compare_with_step_slab(cfg, w, flags):
+    """One no-alloc call and one mam4b_step_slab call with the same config
+    on the same inputs; returns both outputs (host arrays)."""
+    import torch
+    dev = torch.device("cuda:0")
+    x = torch.from_numpy(w["in_slab"]).to(dev)
+    pb = torch.from_numpy(w["pblh"]).to(dev)
+    n = x.shape[1]
+    out = torch.full((native.NOUT, n), float("nan"), dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    st = _call_noalloc(cfg, x.data_ptr(), pb.data_ptr(), out.data_ptr(), n, w["ncol"], w["nlev"],
+                       w["dt"], None if flags is None else flags.data_ptr())
+    assert st == 0, native.STATUS.get(st, st)
+    torch.cuda.synchronize()
+    ctx = native.Context(cfg)
+    ref = torch.full_like(out, float("nan"))
+    ctx.step_slab(x.data_ptr(), pb.data_ptr(), ref.data_ptr(), n, w["ncol"], w["nlev"], w["dt"])
+    torch.cuda.synchronize()
+    ctx.close()
+    return out.cpu().numpy(), ref.cpu().numpy()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["no_flags_word", "no_condensation", "exactly_at_cap"])
+def test_noalloc_edge_cases_match_step_slab(case):
+    """The spare flag word (flags = NULL), the one-kernel path without
+    condensation, and a batch of exactly MAM4B_NOALLOC_MAX_CELLS cells."""
+    cfg = native.default_config()
+    if case == "no_flags_word":
+        w = make_workload("c2", ncol=21, nlev=72, seed=93)
+    elif case == "no_condensation":
+        cfg.do_cond = 0
+        w = make_workload("c4", ncol=40, nlev=72, seed=94)
+    else:
+        cap = native.NOALLOC_MAX_CELLS
+        w = make_workload("c4", ncol=cap // 64, nlev=64, seed=95)
+        assert w["ncol"] * w["nlev"] == cap
+    got, ref = _compare_with_step_slab(cfg, w, None)
+    assert np.isfinite(got).all()
+    assert np.array_equal(got, ref), "no-alloc step differs from mam4b_step_slab (%s)" % case
+
+
+_FRESH = r"""
+import sys
+import numpy as np
+sys.path.insert(0, {root!r})
+sys.path.insert(0, {tests!r})
+import test_zz_no_alloc as t
+from mam4xx_b200 import native
+from mam4xx_b200.workloads import make_workload
+w = make_workload("c2", ncol=9, nlev=72, seed=96)
+got, ref = t._compare_with_step_slab(native.default_config(), w, None)
+assert np.array_equal(got, ref), "differs"
+print("fresh-process no-alloc ok")
+"""
+
+
+@pytest.mark.gpu
+def test_noalloc_first_call_in_a_fresh_process():
+    """A child process whose first CUDA work is the no-alloc call: its
+    set-up stages the constant tables in the fixed array (no allocation);
+    the result must equal mam4b_step_slab's, run afterwards in the child."""
+    here = os.path.dirname(os.path.abspath(__file__))
+    code = _FRESH.format(root=os.path.dirname(here), tests=here)
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "fresh-process no-alloc ok" in r.stdout
