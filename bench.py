@@ -606,8 +606,10 @@ def run_reference_arm(args):
 
 
 def _workload_name(ncol):
-    return ("%s: uneven batching (SOA sub-steps 1..20 per cell), %d columns x %d levels per GPU, "
-            "FP64, dt=1800 s" % (WORKLOAD, ncol, NLEV))
+    what = {"c4": "uneven batching (SOA sub-steps 1..20 per cell)",
+            "c4_stress": "uneven batching stress case (SOA sub-steps 1..1000 per cell)"}
+    return ("%s: %s, %d columns x %d levels per GPU, FP64, dt=1800 s"
+            % (WORKLOAD, what.get(WORKLOAD, "workload configuration"), ncol, NLEV))
 
 
 def _r(v, digits=4):
@@ -668,6 +670,7 @@ def mixed_leg(native, torch, dev, stream, args, ws, rank):
 
 
 def main():
+    global WORKLOAD
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=25)
@@ -680,11 +683,15 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint leg")
     ap.add_argument("--no-processes", action="store_true",
                     help="skip the per-process entries (CalcSize, Coagulation) leg")
+    ap.add_argument("--workload", default=WORKLOAD,
+                    help="workload configuration of the headline step (c4 is the benchmark "
+                         "configuration; c4_stress has 1..1000 SOA sub-steps per cell)")
     ap.add_argument("--adjoint-ncol", type=int, default=16384,
                     help="columns of the adjoint leg (16,384 is its configuration; smaller "
                          "only for profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    WORKLOAD = args.workload
     if args.impl == "reference":
         return run_reference_arm(args)
 
@@ -711,7 +718,11 @@ def main():
     x = torch.from_numpy(x_host).to(dev)
     pb = torch.from_numpy(w["pblh"]).to(dev)
     out = torch.empty((native.NOUT, n), dtype=torch.float64, device=dev)
+    # the context starts with the launch shape chosen by the autotuner for
+    # this device (mam4xx_b200/mam4b_tuning.json, loaded by mam4b_create)
+    # and replays the step as one CUDA graph
     ctx = native.Context()
+    ctx.set_graph_mode(True)
     stream = torch.cuda.current_stream(dev)
 
     def step(precision=native.FP64):
@@ -738,6 +749,26 @@ def main():
     kernel_ms = float(np.mean(laps))
     ms_per_step = ms_max / args.steps
     value = sharded_rate(n, args.steps, ms_max, device=dev)
+
+    # the same step with the built-in launch shape and plain launches
+    tuned_shape = ctx.tuning().as_dict()
+    tfile = os.path.join(ROOT, "mam4xx_b200", "mam4b_tuning.json")
+    dctx = native.Context()
+    dctx.set_tuning(native.default_tuning())
+
+    def default_step():
+        dctx.step_slab(x.data_ptr(), pb.data_ptr(), out.data_ptr(), n, ncol, NLEV, dt,
+                       stream=stream.cuda_stream)
+    d_ms, _, _ = timed_steps(default_step, args.steps, args.warmup, EventClock(stream),
+                             sync=torch.cuda.synchronize, device=dev)
+    dctx.close()
+    tuning = {"shape": tuned_shape,
+              "source": ("mam4xx_b200/mam4b_tuning.json" if tuned_shape
+                         != native.default_tuning().as_dict() else "built-in defaults"),
+              "file_present": os.path.exists(tfile),
+              "graph": True,
+              "tuned_graph_ms_per_step": ms_per_step,
+              "default_plain_ms_per_step": d_ms / args.steps}
 
     # end-to-end through the host entry of the C ABI
     e2e = None
@@ -799,6 +830,7 @@ def main():
                    "parallelism": "column shards, one per GPU" if ws > 1 else "single GPU",
                    "l2": "inputs (%.2f GB) larger than L2, no flush" % (native.NIN * n * 8 / 1e9)},
         "gpu_launches": int(launches),
+        "tuning": tuning,
         "clocks": clocks,
         "device_flags": flags,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

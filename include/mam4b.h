@@ -199,6 +199,76 @@ mam4b_status mam4b_step_slab(mam4b_ctx *ctx, const double *in_slab,
                              void *stream);
 
 /*
+ * Launch shape of the forward step's kernels (no counterpart in the
+ * reference, whose only knob is the Kokkos team size of its column loop,
+ * src/validation/validation.hpp:25-30). The step runs as six kernels: size
+ * (calcsize, one thread per cell), mode (water uptake, one thread per cell
+ * and mode), pair (coagulation coefficients, one thread per cell and mode
+ * pair), pre (each cell up to the SOA condensation loop), soa (the
+ * persistent loop solver) and post (the rest of each cell). Blocks are 64,
+ * 128 or 256 threads (128 or 256 for soa); *_regs selects the compiled
+ * register cap of a kernel (size 255, 128 or 96; pre and post 255, 168 or 128;
+ * soa 64, 96 or 128; block x regs <= 65536); soa_blocks_per_sm sizes the
+ * solver's persistent grid (1..16 blocks per SM); cells_per_thread (1, 2,
+ * 4) is how many cells each thread of size, pre and post steps, i.e.
+ * 32 x cells_per_thread cells per warp. Every shape computes the same
+ * results bit for bit; only the speed differs.
+ */
+typedef struct mam4b_tuning {
+  int size_block, size_regs;
+  int mode_block, pair_block;
+  int pre_block, pre_regs;
+  int post_block, post_regs;
+  int soa_block, soa_regs, soa_blocks_per_sm;
+  int cells_per_thread;
+} mam4b_tuning;
+
+/* The built-in shape (size 128/128, mode 128, pair 128, pre 128/255, post
+ * 128/128, soa 256/64 x 4 per SM, one cell per thread). */
+void mam4b_default_tuning(mam4b_tuning *t);
+
+/* A context starts with the shape in the file named by the environment
+ * variable MAM4B_TUNING_FILE, else in mam4b_tuning.json next to this
+ * library, when that file parses, is valid and was chosen on a device of the
+ * current device's name; else with the defaults. */
+mam4b_status mam4b_get_tuning(const mam4b_ctx *ctx, mam4b_tuning *t);
+/* MAM4B_ERR_INVALID_ARGUMENT for a shape outside the values above. */
+mam4b_status mam4b_set_tuning(mam4b_ctx *ctx, const mam4b_tuning *t);
+
+/* Reads a tuning file: a flat JSON object with the integer fields of
+ * mam4b_tuning under their own names and "device": "<device name>" (copied
+ * to device, which may be NULL). No CUDA call. */
+mam4b_status mam4b_tuning_from_json(const char *path, mam4b_tuning *t, char *device,
+                                    size_t device_len);
+
+/*
+ * Project autotuner: times the candidate shapes of every stage on the given
+ * batch (device slabs as for mam4b_step_slab, `reps` timed repetitions of
+ * each, 1..100), picks the fastest per stage and the fastest
+ * cells_per_thread, and sets the result on ctx when the whole step is
+ * faster with it than with the defaults (else the defaults). best,
+ * default_ms and best_ms (may be NULL) receive the shape and the two
+ * whole-step times [ms]. Synchronous; out_slab is overwritten with the
+ * step's results. Needs condensation on (the pipelined step).
+ */
+mam4b_status mam4b_autotune(mam4b_ctx *ctx, const double *in_slab, const double *pblh,
+                            double *out_slab, size_t ld, int ncol, int nlev, double dt,
+                            int precision, int reps, void *stream, mam4b_tuning *best,
+                            float *default_ms, float *best_ms);
+
+/*
+ * Graph mode (off by default). When on, mam4b_step and mam4b_step_slab
+ * capture the step's kernels (pipelined form: condensation on, no
+ * diagnostics) into a CUDA graph on the first call and replay it with one
+ * graph launch on `stream` while the call's arguments (pointers, sizes,
+ * dt, precision, launch shape) stay the same; a call with other arguments
+ * recaptures the graph and updates it in place. The capture runs on a
+ * private stream of the context. Results are identical to the plain
+ * launches.
+ */
+mam4b_status mam4b_set_graph_mode(mam4b_ctx *ctx, int enable);
+
+/*
  * Host-buffer convenience: copies the host slabs to the device, runs the
  * step and copies the results back, all on `stream`, then synchronises.
  * Scratch device memory is kept in ctx and reused across calls.

@@ -7,6 +7,7 @@
 // Cells are independent: there is no inter-thread communication and no
 // shared memory; the coagulation correction tables are read through L1.
 #include <cuda_runtime.h>
+#include <dlfcn.h>
 
 #include <math.h>
 #include <stdio.h>
@@ -18,6 +19,7 @@
 #include <mutex>
 #include <new>
 #include <type_traits>
+#include <vector>
 
 #include "../../include/mam4b.h"
 #include "mam4b_physics.cuh"
@@ -60,6 +62,7 @@ struct StepArgs {
   double *aux;       // [AUX_FIELDS][ncell], indexed by cell (size/mode kernels)
   unsigned *counters;
   int *npass;        // [ncell] or null: passes of each slot's loop (adjoint only)
+  int mixed;         // the mode/pair stages ran in FP32 (MAM4B_MIXED, _FAST)
 };
 
 // The step runs as a pipeline of three kernels when condensation is on and
@@ -959,7 +962,55 @@ __device__ __forceinline__ void run_chemistry(const StepArgs &a, const ChemArgs 
 // (run_chemistry), and the subarea set-up takes the pre-chemistry states;
 // the post kernel needs nothing else, as everything it reads of the cell's
 // state comes through the hand-off.
-template <bool CHEM>
+// The per-particle H2SO4 uptake rate of mode M of cell c as the FP64 step
+// computes it: FP64 water uptake of the mode from the cell's inputs, the
+// calcsize dry diameter and the relative humidity of the size stage, then
+// uptake_rate_mode. The mixed step (FP32 rates from the mode stage) uses
+// it where a decision of the SOA loop sits at its threshold, so that the
+// decision is the FP64 step's.
+template <int M>
+__device__ double rate_fp64_mode(const StepArgs &a, const long long c) {
+  const StepConsts &C = c_k;
+  const size_t n = (size_t)a.ncell;
+  double sp[7];
+#pragma unroll
+  for (int s = 0; s < 7; ++s)
+    sp[s] = (s < K::nspec(M)) ? __ldg(a.in[MAM4B_IN_AER_I + K::spec0(M) + (s < K::nspec(M) ? s : 0)] + c) : 0.0;
+  double dgn_awet, qaerwat, wetdens;
+  water_uptake_mode<M>(C, sp, a.aux[AUX_RH * n + c], a.out[MAM4B_OUT_DGN_A + M][c], dgn_awet,
+                       qaerwat, wetdens);
+  return uptake_rate_mode(C, M, a.aux[AUX_GDIFF * n + c], a.aux[AUX_FPATH * n + c], dgn_awet);
+}
+__device__ __noinline__ double rate_fp64(const StepArgs &a, const long long c, int m) {
+  switch (m) {
+  case 0: return rate_fp64_mode<0>(a, c);
+  case 1: return rate_fp64_mode<1>(a, c);
+  case 2: return rate_fp64_mode<2>(a, c);
+  default: return rate_fp64_mode<3>(a, c);
+  }
+}
+
+// The SOA loop skips a mode, and zeroes its SOA, when its uptake rate is
+// not above 1e-15 (gasaerexch_soaexch.hpp:189-193). With FP32 rates
+// (relative error well below 1e-5) a rate within 1e-4 of that threshold may
+// fall on the other side of it than the FP64 step's, so such modes take
+// the FP64 rate instead (a few cells in 10^4).
+__device__ __forceinline__ void guard_soa_threshold(const StepArgs &a, const long long c,
+                                                    double temp, double pmid, const Sub &s,
+                                                    double (&rate)[NMODE], ClearMid &cm,
+                                                    double (&uptk0)[NMODE]) {
+  const double aircon = pmid / (8314.46759100000 * temp);
+#pragma unroll
+  for (int k = 0; k < NMODE; ++k) {
+    if (fabs(uptk0[k] - 1.0e-15) <= 1.0e-4 * 1.0e-15) {
+      rate[k] = rate_fp64(a, c, k);
+      cm.uptk1[k] = rate[k] * (s.num[k] * aircon);
+      uptk0[k] = cm.uptk1[k] * 0.81;
+    }
+  }
+}
+
+template <bool CHEM, bool MIXED = false>
 __device__ __forceinline__ void cell_pre(const StepArgs &a, const ChemArgs &ch,
                                          const long long c) {
   const StepConsts &C = c_k;
@@ -1008,6 +1059,10 @@ __device__ __forceinline__ void cell_pre(const StepArgs &a, const ChemArgs &ch,
   for (int k = 0; k < NMODE; ++k)
     rate[k] = a.aux[(AUX_RATE + k) * (size_t)a.ncell + c];
   clear_prefix<false>(a, dt, f.temp, f.pmid, rate, qgas1, s, cm, uptk0);
+  if constexpr (MIXED) {
+    if (a.do_cond)
+      guard_soa_threshold(a, c, f.temp, f.pmid, s, rate, cm, uptk0);
+  }
 
   // queue the cell: solver state and hand-off at the start of the SOA loop
   SoaState st;
@@ -1244,13 +1299,20 @@ __global__ void __launch_bounds__(128) chem_step_kernel(const __grid_constant__ 
     cell_step_chem(a, ch, c);
 }
 
+// Launch shapes of the pipeline kernels. Each whole-cell kernel is compiled
+// once per register cap (__maxnreg__; a lower cap lets more warps reside on
+// an SM, at the price of spills) and takes its block size and the number
+// of cells each thread steps (a grid-stride loop) at launch; the values are
+// chosen per device by mam4b_autotune (include/mam4b.h). The arithmetic is
+// the same in every variant, so their results are bit for bit equal.
+// Register caps compiled:
+//   size_kernel 255, 128, 96; pre_kernel and post_kernel 255, 168, 128;
+//   soa_kernel 64, 96, 128.
+
 // Stage 1 of the pipelined step, one thread per cell: calcsize for the dry
 // diameters (an output), the relative humidity of water uptake and the
 // H2SO4 diffusivity and mean free path.
-__global__ void __launch_bounds__(128) size_kernel(const __grid_constant__ StepArgs a) {
-  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= a.ncell)
-    return;
+__device__ __forceinline__ void size_cell(const StepArgs &a, const long long c) {
   const StepConsts &C = c_k;
   double ai[NPOP], ac[NPOP];
 #pragma unroll
@@ -1272,6 +1334,13 @@ __global__ void __launch_bounds__(128) size_kernel(const __grid_constant__ StepA
   h2so4_diffusivity(temp, pmid, gd, fp);
   a.aux[AUX_GDIFF * n + c] = gd;
   a.aux[AUX_FPATH * n + c] = fp;
+}
+
+template <int R>
+__global__ void __maxnreg__(R) size_kernel(const __grid_constant__ StepArgs a) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < a.ncell; c += stride)
+    size_cell(a, c);
 }
 
 // Stage 2, one thread per (cell, mode): water uptake of the mode (Kohler
@@ -1314,7 +1383,7 @@ __device__ __forceinline__ void mode_work(const StepArgs &a, const long long c) 
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(128) mode_kernel(const __grid_constant__ StepArgs a) {
+__global__ void mode_kernel(const __grid_constant__ StepArgs a) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= a.ncell)
     return;
@@ -1331,7 +1400,7 @@ __global__ void __launch_bounds__(128) mode_kernel(const __grid_constant__ StepA
 // sizes and densities of stage 2; they do not depend on what condensation
 // changes, so the post kernel only applies them.
 template <bool MIXED>
-__global__ void __launch_bounds__(128) pair_kernel(const __grid_constant__ StepArgs a) {
+__global__ void pair_kernel(const __grid_constant__ StepArgs a) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= a.ncell)
     return;
@@ -1345,7 +1414,16 @@ __global__ void __launch_bounds__(128) pair_kernel(const __grid_constant__ StepA
   const double dens_d = dmax(1000.0, a.out[MAM4B_OUT_WETDENS + dm][c]);
   const CoagTables T = {kCoagBm0ij, kCoagBm3i, kCoagBm0};
   double bij0, bij3, bii0, bjj0;
+  // the FP32 coefficients unless the correction-table index (round() of
+  // 2 ln(dg_dst / dg_src) / ln 2, coagulation.hpp:715-717) sits within 1e-3
+  // of a rounding boundary, where FP32 might round the other way
+  bool fp32 = MIXED;
   if constexpr (MIXED) {
+    const double r = a.out[MAM4B_OUT_DGN_AWET + dm][c] / a.out[MAM4B_OUT_DGN_AWET + sm][c];
+    const double xr = log(r) / log(sqrt(2.0));
+    fp32 = fabs(xr - floor(xr) - 0.5) > 1.0e-3;
+  }
+  if (fp32) {
     float f0, f3, fi, fj;
     f32::coag_pair_coefs(C, T, p, (float)temp, (float)pmid, (float)aircon,
                          (float)a.out[MAM4B_OUT_DGN_AWET + sm][c],
@@ -1367,11 +1445,12 @@ __global__ void __launch_bounds__(128) pair_kernel(const __grid_constant__ StepA
   cc[(9 + p) * n] = bjj0;
 }
 
-__global__ void __launch_bounds__(128) pre_kernel(const __grid_constant__ StepArgs a) {
-  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+template <int R, bool MIXED>
+__global__ void __maxnreg__(R) pre_kernel(const __grid_constant__ StepArgs a) {
   const ChemArgs none = {nullptr, nullptr, 0};
-  if (c < a.ncell)
-    cell_pre<false>(a, none, c);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < a.ncell; c += stride)
+    cell_pre<false, MIXED>(a, none, c);
 }
 
 // The pre stage of the step with chemistry (mam4b_step_chem_slab).
@@ -1382,11 +1461,13 @@ __global__ void __launch_bounds__(128) pre_chem_kernel(const __grid_constant__ S
     cell_pre<true>(a, ch, c);
 }
 
-// 4 blocks of 128 per SM (128 registers, a few hundred bytes spilled to
-// L1): 2 % faster than the unconstrained 231-register build.
-__global__ void __launch_bounds__(128, 4) post_kernel(const __grid_constant__ StepArgs a) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < (long long)a.counters[CNT_QUEUED])
+// (the 128-register cap, 4 blocks of 128 per SM with a few hundred bytes
+// spilled to L1, was 2 % faster than the unconstrained 231-register build)
+template <int R>
+__global__ void __maxnreg__(R) post_kernel(const __grid_constant__ StepArgs a) {
+  const long long nq = (long long)a.counters[CNT_QUEUED];
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += stride)
     cell_post(a, (unsigned)i);
 }
 
@@ -1398,9 +1479,11 @@ __global__ void __launch_bounds__(128, 4) post_kernel(const __grid_constant__ St
 // is bound by FP64 division latency: 4 blocks of 256 per SM (64 registers)
 // hide more of it than the unconstrained 93-register build.
 // With MIXED the loop runs in single precision (f32::soa_step).
+// Launched with any block size that is a multiple of 32 and one grid of
+// persistent blocks (SMs x blocks per SM).
 constexpr int kSoaBlock = 256;
-template <bool MIXED>
-__global__ void __launch_bounds__(kSoaBlock, 4) soa_kernel(const __grid_constant__ StepArgs a) {
+template <bool MIXED, int R>
+__global__ void __maxnreg__(R) soa_kernel(const __grid_constant__ StepArgs a) {
   using State = typename std::conditional<MIXED, f32::SoaStateF, SoaState>::type;
   const unsigned ntask = a.counters[CNT_QUEUED];
   const unsigned nlong = a.counters[CNT_LONG];
@@ -2890,7 +2973,17 @@ struct mam4b_ctx {
   double *d_aux;
   unsigned *d_counters;  // CNT_WORDS per chunk of the host path
   size_t cap_cells;
-  int soa_grid;  // persistent solver blocks (SMs x resident blocks)
+  int sms;              // SMs of the device (persistent solver grid = sms x blocks per SM)
+  mam4b_tuning tune;    // launch shape of the forward pipeline
+  // graph mode (mam4b_set_graph_mode): the pipeline of the last call,
+  // captured once and replayed while the call's arguments stay the same
+  bool use_graph;
+  cudaStream_t cap_stream;
+  cudaGraph_t graph;
+  cudaGraphExec_t graph_exec;
+  StepArgs graph_args;
+  int graph_precision;
+  mam4b_tuning graph_tune;
   // adjoint: SOA checkpoints of the persistent threads (allocated on first
   // use) and the cotangent scratch of the pipelined adjoint (grown)
   double *d_ck;
@@ -2958,16 +3051,6 @@ cudaError_t ensure_solver_scratch(mam4b_ctx *ctx, size_t ncell) {
   cudaError_t e = cudaSuccess;
   if (!ctx->d_counters)
     e = cudaMalloc(&ctx->d_counters, (size_t)CNT_WORDS * kMaxChunks * sizeof(unsigned));
-  if (e == cudaSuccess && ctx->soa_grid == 0) {
-    int dev = 0, sms = 0, per_sm = 0;
-    e = cudaGetDevice(&dev);
-    if (e == cudaSuccess)
-      e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (e == cudaSuccess)
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, soa_kernel<false>, kSoaBlock, 0);
-    if (e == cudaSuccess)
-      ctx->soa_grid = sms * (per_sm > 0 ? per_sm : 1);
-  }
   if (e != cudaSuccess || ctx->cap_cells >= ncell)
     return e;
   cudaFree(ctx->d_soa);
@@ -3019,47 +3102,214 @@ void set_step_scratch(const mam4b_ctx *ctx, StepArgs &a, size_t c0, int chunk) {
   a.counters = ctx->d_counters + (size_t)CNT_WORDS * chunk;
 }
 
+// ----------------------------------------------------- launch shapes
+// The forward pipeline's launch shape (mam4b_tuning): block sizes, register
+// caps (compiled variants of the whole-cell kernels) and cells per thread.
+// Every shape runs the same arithmetic, so results are bit for bit equal.
+bool valid_block(int b, int regs) {
+  return (b == 64 || b == 128 || b == 256) && (long long)b * regs <= 65536;
+}
+bool valid_tuning(const mam4b_tuning &t) {
+  return (t.size_regs == 255 || t.size_regs == 128 || t.size_regs == 96) &&
+         valid_block(t.size_block, t.size_regs) &&
+         valid_block(t.mode_block, 64) && valid_block(t.pair_block, 128) &&
+         (t.pre_regs == 255 || t.pre_regs == 168 || t.pre_regs == 128) &&
+         valid_block(t.pre_block, t.pre_regs) &&
+         (t.post_regs == 255 || t.post_regs == 168 || t.post_regs == 128) &&
+         valid_block(t.post_block, t.post_regs) &&
+         (t.soa_regs == 64 || t.soa_regs == 96 || t.soa_regs == 128) &&
+         (t.soa_block == 128 || t.soa_block == 256) &&
+         (long long)t.soa_block * t.soa_regs <= 65536 && t.soa_blocks_per_sm >= 1 &&
+         t.soa_blocks_per_sm <= 16 &&
+         (t.cells_per_thread == 1 || t.cells_per_thread == 2 || t.cells_per_thread == 4);
+}
+
+unsigned grid_for(long long n, int block, int cpt) {
+  const long long per = (long long)block * cpt;
+  const long long g = (n + per - 1) / per;
+  return (unsigned)(g > 0 ? g : 1);
+}
+
+// Stage launchers. Stage order: 0 size, 1 mode, 2 pair, 3 pre, 4 soa, 5 post.
+void launch_size(const mam4b_tuning &t, const StepArgs &a, cudaStream_t s) {
+  const unsigned g = grid_for(a.ncell, t.size_block, t.cells_per_thread);
+  if (t.size_regs == 96)
+    size_kernel<96><<<g, t.size_block, 0, s>>>(a);
+  else if (t.size_regs == 128)
+    size_kernel<128><<<g, t.size_block, 0, s>>>(a);
+  else
+    size_kernel<255><<<g, t.size_block, 0, s>>>(a);
+}
+void launch_mode(const mam4b_tuning &t, const StepArgs &a, cudaStream_t s, bool mixed) {
+  const dim3 g(grid_for(a.ncell, t.mode_block, 1), NMODE);
+  if (mixed)
+    mode_kernel<true><<<g, t.mode_block, 0, s>>>(a);
+  else
+    mode_kernel<false><<<g, t.mode_block, 0, s>>>(a);
+}
+void launch_pair(const mam4b_tuning &t, const StepArgs &a, cudaStream_t s, bool mixed) {
+  const dim3 g(grid_for(a.ncell, t.pair_block, 1), 3);
+  if (mixed)
+    pair_kernel<true><<<g, t.pair_block, 0, s>>>(a);
+  else
+    pair_kernel<false><<<g, t.pair_block, 0, s>>>(a);
+}
+template <bool MIXED>
+void launch_pre_t(const mam4b_tuning &t, const StepArgs &a, cudaStream_t s) {
+  const unsigned g = grid_for(a.ncell, t.pre_block, t.cells_per_thread);
+  if (t.pre_regs == 128)
+    pre_kernel<128, MIXED><<<g, t.pre_block, 0, s>>>(a);
+  else if (t.pre_regs == 168)
+    pre_kernel<168, MIXED><<<g, t.pre_block, 0, s>>>(a);
+  else
+    pre_kernel<255, MIXED><<<g, t.pre_block, 0, s>>>(a);
+}
+void launch_pre(const mam4b_tuning &t, const StepArgs &a, cudaStream_t s, bool mixed = false) {
+  if (mixed)
+    launch_pre_t<true>(t, a, s);
+  else
+    launch_pre_t<false>(t, a, s);
+}
+template <bool MIXED>
+void launch_soa_t(const mam4b_tuning &t, int sms, const StepArgs &a, cudaStream_t s) {
+  const unsigned g = (unsigned)(sms * t.soa_blocks_per_sm);
+  if (t.soa_regs == 128)
+    soa_kernel<MIXED, 128><<<g, t.soa_block, 0, s>>>(a);
+  else if (t.soa_regs == 96)
+    soa_kernel<MIXED, 96><<<g, t.soa_block, 0, s>>>(a);
+  else
+    soa_kernel<MIXED, 64><<<g, t.soa_block, 0, s>>>(a);
+}
+void launch_soa(const mam4b_tuning &t, int sms, const StepArgs &a, cudaStream_t s, bool fast) {
+  if (fast)
+    launch_soa_t<true>(t, sms, a, s);
+  else
+    launch_soa_t<false>(t, sms, a, s);
+}
+void launch_post(const mam4b_tuning &t, const StepArgs &a, cudaStream_t s) {
+  // one thread per queued slot at most; the kernel reads the queue length
+  const unsigned g = grid_for(a.ncell, t.post_block, t.cells_per_thread);
+  if (t.post_regs == 255)
+    post_kernel<255><<<g, t.post_block, 0, s>>>(a);
+  else if (t.post_regs == 168)
+    post_kernel<168><<<g, t.post_block, 0, s>>>(a);
+  else
+    post_kernel<128><<<g, t.post_block, 0, s>>>(a);
+}
+
 // Clears the counters and queues the pipeline kernels on s in the
-// arithmetic of `precision` (mam4b_precision).
-// With ch (FP64 only) the cells' chemistry runs in the pre stage.
-cudaError_t launch_pipeline(mam4b_ctx *ctx, const StepArgs &a, cudaStream_t s, int precision,
-                            const ChemArgs *ch = nullptr) {
+// arithmetic of `precision` (mam4b_precision) with launch shape t on a
+// device of `sms` SMs. With ch (FP64 only) the cells' chemistry runs in
+// the pre stage. With ev (7 events), ev[k] is recorded before stage k and
+// ev[6] after the last: the per-stage times of mam4b_autotune.
+cudaError_t launch_pipeline_t(const mam4b_tuning &t, int sms, const StepArgs &a_in,
+                              cudaStream_t s, int precision, const ChemArgs *ch, cudaEvent_t *ev,
+                              std::atomic<unsigned long long> *launches) {
+  StepArgs a = a_in;
+  a.mixed = precision != MAM4B_FP64;
   cudaError_t e = cudaMemsetAsync(a.counters, 0, CNT_WORDS * sizeof(unsigned), s);
   if (e != cudaSuccess)
     return e;
-  const int block = 128;
-  const unsigned grid = (unsigned)((a.ncell + block - 1) / block);
   if (!a.do_cond) {
     // no SOA loop to pipeline
+    const int block = 128;
+    const unsigned grid = (unsigned)((a.ncell + block - 1) / block);
     if (ch)
       chem_step_kernel<<<grid, block, 0, s>>>(a, *ch);
     else
       full_kernel<false><<<grid, block, 0, s>>>(a);
     e = cudaGetLastError();
-    if (e == cudaSuccess)
-      ctx->launches += 1;
+    if (e == cudaSuccess && launches)
+      *launches += 1;
     return e;
   }
-  size_kernel<<<grid, block, 0, s>>>(a);
-  if (precision != MAM4B_FP64) {
-    mode_kernel<true><<<dim3(grid, NMODE), block, 0, s>>>(a);
-    pair_kernel<true><<<dim3(grid, 3), block, 0, s>>>(a);
-    pre_kernel<<<grid, block, 0, s>>>(a);
-    if (precision == MAM4B_MIXED_FAST)
-      soa_kernel<true><<<ctx->soa_grid, kSoaBlock, 0, s>>>(a);
-    else
-      soa_kernel<false><<<ctx->soa_grid, kSoaBlock, 0, s>>>(a);
+  const bool mixed = precision != MAM4B_FP64;
+  auto mark = [&](int k) {
+    if (ev)
+      cudaEventRecord(ev[k], s);
+  };
+  mark(0);
+  launch_size(t, a, s);
+  mark(1);
+  launch_mode(t, a, s, mixed);
+  mark(2);
+  launch_pair(t, a, s, mixed);
+  mark(3);
+  if (ch) {
+    const int block = 128;
+    pre_chem_kernel<<<(unsigned)((a.ncell + block - 1) / block), block, 0, s>>>(a, *ch);
   } else {
-    mode_kernel<false><<<dim3(grid, NMODE), block, 0, s>>>(a);
-    pair_kernel<false><<<dim3(grid, 3), block, 0, s>>>(a);
-    if (ch)
-      pre_chem_kernel<<<grid, block, 0, s>>>(a, *ch);
-    else
-      pre_kernel<<<grid, block, 0, s>>>(a);
-    soa_kernel<false><<<ctx->soa_grid, kSoaBlock, 0, s>>>(a);
+    launch_pre(t, a, s, mixed);
   }
-  post_kernel<<<grid, block, 0, s>>>(a);
+  mark(4);
+  launch_soa(t, sms, a, s, precision == MAM4B_MIXED_FAST);
+  mark(5);
+  launch_post(t, a, s);
+  mark(6);
   e = cudaGetLastError();
+  if (e == cudaSuccess && launches)
+    *launches += 6;
+  return e;
+}
+
+void drop_graph(mam4b_ctx *ctx) {
+  if (ctx->graph_exec)
+    cudaGraphExecDestroy(ctx->graph_exec);
+  if (ctx->graph)
+    cudaGraphDestroy(ctx->graph);
+  ctx->graph_exec = nullptr;
+  ctx->graph = nullptr;
+}
+
+// The forward pipeline with the context's launch shape. With graph mode on
+// and `graph` set (mam4b_step's device entry), the pipeline is captured on
+// a private stream into a CUDA graph, instantiated once and replayed on s;
+// a call with other arguments (pointers, sizes, precision, launch shape)
+// recaptures and updates the instantiated graph in place, or
+// re-instantiates it when the update is refused.
+cudaError_t launch_pipeline(mam4b_ctx *ctx, const StepArgs &a, cudaStream_t s, int precision,
+                            const ChemArgs *ch = nullptr, bool graph = false) {
+  if (!graph || !ctx->use_graph || ch || !a.do_cond)
+    return launch_pipeline_t(ctx->tune, ctx->sms, a, s, precision, ch, nullptr, &ctx->launches);
+  const bool same = ctx->graph_exec && memcmp(&ctx->graph_args, &a, sizeof(StepArgs)) == 0 &&
+                    ctx->graph_precision == precision &&
+                    memcmp(&ctx->graph_tune, &ctx->tune, sizeof(mam4b_tuning)) == 0;
+  cudaError_t e = cudaSuccess;
+  if (!same) {
+    if (!ctx->cap_stream)
+      e = cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking);
+    cudaGraph_t g = nullptr;
+    if (e == cudaSuccess)
+      e = cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeRelaxed);
+    if (e == cudaSuccess) {
+      const cudaError_t el = launch_pipeline_t(ctx->tune, ctx->sms, a, ctx->cap_stream, precision,
+                                               nullptr, nullptr, nullptr);
+      e = cudaStreamEndCapture(ctx->cap_stream, &g);
+      if (e == cudaSuccess)
+        e = el;
+    }
+    if (e == cudaSuccess && ctx->graph_exec) {
+      cudaGraphExecUpdateResultInfo info;
+      if (cudaGraphExecUpdate(ctx->graph_exec, g, &info) != cudaSuccess) {
+        (void)cudaGetLastError();  // the refusal is not an error of the step
+        cudaGraphExecDestroy(ctx->graph_exec);
+        ctx->graph_exec = nullptr;
+      }
+    }
+    if (e == cudaSuccess && !ctx->graph_exec)
+      e = cudaGraphInstantiate(&ctx->graph_exec, g, 0);
+    if (ctx->graph)
+      cudaGraphDestroy(ctx->graph);
+    ctx->graph = g;
+    if (e != cudaSuccess) {
+      drop_graph(ctx);
+      return e;
+    }
+    ctx->graph_args = a;
+    ctx->graph_precision = precision;
+    ctx->graph_tune = ctx->tune;
+  }
+  e = cudaGraphLaunch(ctx->graph_exec, s);
   if (e == cudaSuccess)
     ctx->launches += 6;
   return e;
@@ -3113,7 +3363,7 @@ cudaError_t ensure_host_streams(mam4b_ctx *ctx) {
 struct NoAllocDevice {
   bool ready;
   double *scratch;  // device address of g_noalloc_scratch on this device
-  int soa_grid;
+  int sms;          // SMs of the device (the solver's persistent grid)
 };
 NoAllocDevice g_noalloc[64];
 
@@ -3143,22 +3393,172 @@ cudaError_t noalloc_setup(int dev) {
       return e;
     g_consts_ready[dev] = true;
   }
-  int sms = 0, per_sm = 0;
+  int sms = 0;
   e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (e == cudaSuccess)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, soa_kernel<false>, kSoaBlock, 0);
   if (e != cudaSuccess)
     return e;
   g_noalloc[dev].scratch = static_cast<double *>(p);
-  g_noalloc[dev].soa_grid = sms * (per_sm > 0 ? per_sm : 1);
+  g_noalloc[dev].sms = sms;
   g_noalloc[dev].ready = true;
   return cudaSuccess;
+}
+// ------------------------------------------------------- tuning files
+// A tuning file is a flat JSON object with the integer fields of
+// mam4b_tuning under their own names and the device name it was chosen on
+// ("device": "NVIDIA B200"), e.g. as written by mam4xx_b200/autotune.py.
+const char *const kTuningKeys[] = {"size_block", "size_regs", "mode_block", "pair_block",
+                                   "pre_block", "pre_regs", "post_block", "post_regs",
+                                   "soa_block", "soa_regs", "soa_blocks_per_sm",
+                                   "cells_per_thread"};
+int *tuning_field(mam4b_tuning &t, int k) {
+  int *f[] = {&t.size_block, &t.size_regs, &t.mode_block, &t.pair_block, &t.pre_block,
+              &t.pre_regs, &t.post_block, &t.post_regs, &t.soa_block, &t.soa_regs,
+              &t.soa_blocks_per_sm, &t.cells_per_thread};
+  return f[k];
+}
+
+// Value text after "key": in json, or nullptr.
+const char *json_value(const char *json, const char *key) {
+  char pat[64];
+  snprintf(pat, sizeof(pat), "\"%s\"", key);
+  const char *p = strstr(json, pat);
+  if (!p)
+    return nullptr;
+  p += strlen(pat);
+  while (*p == ' ' || *p == '\t' || *p == '\n' || *p == '\r')
+    ++p;
+  if (*p != ':')
+    return nullptr;
+  ++p;
+  while (*p == ' ' || *p == '\t' || *p == '\n' || *p == '\r')
+    ++p;
+  return p;
+}
+
+mam4b_status parse_tuning(const char *json, mam4b_tuning *t, char *device, size_t device_len) {
+  mam4b_tuning r;
+  mam4b_default_tuning(&r);
+  for (int k = 0; k < (int)(sizeof(kTuningKeys) / sizeof(kTuningKeys[0])); ++k) {
+    const char *v = json_value(json, kTuningKeys[k]);
+    if (!v)
+      return MAM4B_ERR_INVALID_ARGUMENT;
+    char *end = nullptr;
+    const long x = strtol(v, &end, 10);
+    if (end == v || x < 0 || x > 4096)
+      return MAM4B_ERR_INVALID_ARGUMENT;
+    *tuning_field(r, k) = (int)x;
+  }
+  if (!valid_tuning(r))
+    return MAM4B_ERR_INVALID_ARGUMENT;
+  if (device && device_len) {
+    device[0] = '\0';
+    const char *v = json_value(json, "device");
+    if (v && *v == '"') {
+      const char *q = strchr(v + 1, '"');
+      if (q) {
+        size_t n = (size_t)(q - v - 1);
+        if (n >= device_len)
+          n = device_len - 1;
+        memcpy(device, v + 1, n);
+        device[n] = '\0';
+      }
+    }
+  }
+  *t = r;
+  return MAM4B_OK;
+}
+
+mam4b_status read_tuning_file(const char *path, mam4b_tuning *t, char *device, size_t device_len) {
+  FILE *f = fopen(path, "rb");
+  if (!f)
+    return MAM4B_ERR_INVALID_ARGUMENT;
+  char buf[4096];
+  const size_t n = fread(buf, 1, sizeof(buf) - 1, f);
+  fclose(f);
+  buf[n] = '\0';
+  return parse_tuning(buf, t, device, device_len);
+}
+
+// The tuning a new context starts with: the file named by MAM4B_TUNING_FILE,
+// else mam4b_tuning.json next to this library, when it exists, parses and
+// was chosen on a device of the current device's name; else the defaults.
+void initial_tuning(int dev, mam4b_tuning *t) {
+  mam4b_default_tuning(t);
+  char path[1024] = {0};
+  const char *env = getenv("MAM4B_TUNING_FILE");
+  if (env && *env) {
+    snprintf(path, sizeof(path), "%s", env);
+  } else {
+    Dl_info info;
+    if (!dladdr((void *)&initial_tuning, &info) || !info.dli_fname)
+      return;
+    snprintf(path, sizeof(path), "%s", info.dli_fname);
+    char *slash = strrchr(path, '/');
+    if (!slash)
+      return;
+    snprintf(slash + 1, sizeof(path) - (size_t)(slash + 1 - path), "mam4b_tuning.json");
+  }
+  mam4b_tuning r;
+  char name[256];
+  if (read_tuning_file(path, &r, name, sizeof(name)) != MAM4B_OK)
+    return;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess || strcmp(prop.name, name) != 0)
+    return;
+  *t = r;
 }
 }  // namespace
 
 extern "C" {
 
 int mam4b_abi_version(void) { return MAM4B_ABI_VERSION; }
+
+void mam4b_default_tuning(mam4b_tuning *t) {
+  if (!t)
+    return;
+  t->size_block = 128;
+  t->size_regs = 128;
+  t->mode_block = 128;
+  t->pair_block = 128;
+  t->pre_block = 128;
+  t->pre_regs = 255;
+  t->post_block = 128;
+  t->post_regs = 128;
+  t->soa_block = 256;
+  t->soa_regs = 64;
+  t->soa_blocks_per_sm = 4;
+  t->cells_per_thread = 1;
+}
+
+mam4b_status mam4b_tuning_from_json(const char *path, mam4b_tuning *t, char *device,
+                                    size_t device_len) {
+  if (!path || !t)
+    return MAM4B_ERR_INVALID_ARGUMENT;
+  return read_tuning_file(path, t, device, device_len);
+}
+
+mam4b_status mam4b_get_tuning(const mam4b_ctx *ctx, mam4b_tuning *t) {
+  if (!ctx || !t)
+    return MAM4B_ERR_INVALID_ARGUMENT;
+  *t = ctx->tune;
+  return MAM4B_OK;
+}
+
+mam4b_status mam4b_set_tuning(mam4b_ctx *ctx, const mam4b_tuning *t) {
+  if (!ctx || !t || !valid_tuning(*t))
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_set_tuning", cudaSuccess);
+  ctx->tune = *t;
+  return MAM4B_OK;
+}
+
+mam4b_status mam4b_set_graph_mode(mam4b_ctx *ctx, int enable) {
+  if (!ctx)
+    return MAM4B_ERR_INVALID_ARGUMENT;
+  ctx->use_graph = enable != 0;
+  if (!ctx->use_graph)
+    drop_graph(ctx);
+  return MAM4B_OK;
+}
 
 void mam4b_default_config(mam4b_config *cfg) {
   if (!cfg)
@@ -3195,12 +3595,15 @@ mam4b_status mam4b_create(mam4b_ctx **out, const mam4b_config *cfg) {
     e = cudaMalloc(&ctx->d_flags, sizeof(unsigned));
   if (e == cudaSuccess)
     e = cudaMemset(ctx->d_flags, 0, sizeof(unsigned));
+  if (e == cudaSuccess)
+    e = cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, ctx->device);
   if (e != cudaSuccess) {
     if (ctx->d_flags)
       cudaFree(ctx->d_flags);
     delete ctx;
     return MAM4B_ERR_CUDA;
   }
+  initial_tuning(ctx->device, &ctx->tune);
   *out = ctx;
   return MAM4B_OK;
 }
@@ -3208,6 +3611,9 @@ mam4b_status mam4b_create(mam4b_ctx **out, const mam4b_config *cfg) {
 mam4b_status mam4b_destroy(mam4b_ctx *ctx) {
   if (!ctx)
     return MAM4B_ERR_INVALID_ARGUMENT;
+  drop_graph(ctx);
+  if (ctx->cap_stream)
+    cudaStreamDestroy(ctx->cap_stream);
   cudaFree(ctx->d_flags);
   cudaFree(ctx->d_in);
   cudaFree(ctx->d_out);
@@ -3296,7 +3702,7 @@ mam4b_status mam4b_step(mam4b_ctx *ctx, const mam4b_state_view *in, const mam4b_
   if (e != cudaSuccess)
     return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_step scratch", e);
   set_step_scratch(ctx, a, 0, 0);
-  e = launch_pipeline(ctx, a, s, precision);
+  e = launch_pipeline(ctx, a, s, precision, nullptr, true);
   if (e != cudaSuccess)
     return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_step launch", e);
   return MAM4B_OK;
@@ -3318,6 +3724,206 @@ mam4b_status mam4b_step_slab(mam4b_ctx *ctx, const double *in_slab, const double
   for (int f = 0; f < MAM4B_NOUT; ++f)
     ov.field[f] = out_slab + (size_t)f * ld;
   return mam4b_step(ctx, &iv, &ov, ncol, nlev, dt, precision, stream);
+}
+
+// Autotuner (include/mam4b.h): times every candidate launch shape of each
+// pipeline stage on the caller's batch, stage by stage from events
+// recorded between the launches (a stage's time does not depend on the
+// other stages' shapes), keeps the fastest shape of each stage, then the
+// fastest cells-per-thread of the whole-cell kernels, and adopts the result
+// when the whole pipeline is faster with it than with the defaults.
+mam4b_status mam4b_autotune(mam4b_ctx *ctx, const double *in_slab, const double *pblh,
+                            double *out_slab, size_t ld, int ncol, int nlev, double dt,
+                            int precision, int reps, void *stream, mam4b_tuning *best,
+                            float *default_ms, float *best_ms) {
+  const char *what = "mam4b_autotune";
+  if (!ctx || !in_slab || !pblh || !out_slab || ncol <= 0 || nlev <= 0 || !(dt > 0.0) ||
+      ld < (size_t)ncol * (size_t)nlev || reps < 1 || reps > 100 ||
+      (long long)ncol * nlev > 0x7fffffffLL ||
+      (precision != MAM4B_FP64 && precision != MAM4B_MIXED && precision != MAM4B_MIXED_FAST))
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, what, cudaSuccess);
+  if (!ctx->cfg.do_cond)
+    return set_err(ctx, MAM4B_ERR_NOT_SUPPORTED, "mam4b_autotune: condensation off (one kernel)",
+                   cudaSuccess);
+  StepArgs a;
+  memset(&a, 0, sizeof(a));
+  for (int f = 0; f < MAM4B_NIN; ++f)
+    a.in[f] = in_slab + (size_t)f * ld;
+  a.pblh = pblh;
+  for (int f = 0; f < MAM4B_NOUT; ++f)
+    a.out[f] = out_slab + (size_t)f * ld;
+  set_step_config(ctx, a, (long long)ncol * nlev, nlev, dt);
+  cudaError_t e = ensure_solver_scratch(ctx, (size_t)a.ncell);
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, what, e);
+  set_step_scratch(ctx, a, 0, 0);
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaEvent_t ev[7];
+  int nev = 0;
+  for (; nev < 7; ++nev)
+    if ((e = cudaEventCreate(&ev[nev])) != cudaSuccess)
+      break;
+  // per-stage candidates
+  const int blocks[3] = {64, 128, 256};
+  std::vector<mam4b_tuning> cand[6];
+  mam4b_tuning d;
+  mam4b_default_tuning(&d);
+  for (int b : blocks) {
+    for (int r : {255, 128, 96}) {
+      mam4b_tuning t = d;
+      t.size_block = b;
+      t.size_regs = r;
+      if (valid_tuning(t))
+        cand[0].push_back(t);
+    }
+    mam4b_tuning t = d;
+    t.mode_block = b;
+    cand[1].push_back(t);
+    t = d;
+    t.pair_block = b;
+    cand[2].push_back(t);
+    for (int r : {255, 168, 128}) {
+      t = d;
+      t.pre_block = b;
+      t.pre_regs = r;
+      if (valid_tuning(t))
+        cand[3].push_back(t);
+      t = d;
+      t.post_block = b;
+      t.post_regs = r;
+      if (valid_tuning(t))
+        cand[5].push_back(t);
+    }
+  }
+  for (int b : {128, 256})
+    for (int r : {64, 96, 128}) {
+      const int resident = (int)(65536 / ((long long)b * r));
+      for (int bps : {resident, resident / 2}) {
+        mam4b_tuning t = d;
+        t.soa_block = b;
+        t.soa_regs = r;
+        t.soa_blocks_per_sm = bps < 1 ? 1 : (bps > 16 ? 16 : bps);
+        if (valid_tuning(t))
+          cand[4].push_back(t);
+      }
+    }
+  size_t kmax = 0;
+  for (auto &c : cand)
+    kmax = std::max(kmax, c.size());
+  std::vector<float> stage_ms[6];
+  for (int k = 0; k < 6; ++k)
+    stage_ms[k].assign(cand[k].size(), 1e30f);
+  auto combine = [&](size_t i) {
+    // stage k of the combined shape from candidate i of stage k
+    mam4b_tuning t = d;
+    const mam4b_tuning &c0 = cand[0][i % cand[0].size()];
+    t.size_block = c0.size_block;
+    t.size_regs = c0.size_regs;
+    t.mode_block = cand[1][i % cand[1].size()].mode_block;
+    t.pair_block = cand[2][i % cand[2].size()].pair_block;
+    const mam4b_tuning &c3 = cand[3][i % cand[3].size()];
+    t.pre_block = c3.pre_block;
+    t.pre_regs = c3.pre_regs;
+    const mam4b_tuning &c4 = cand[4][i % cand[4].size()];
+    t.soa_block = c4.soa_block;
+    t.soa_regs = c4.soa_regs;
+    t.soa_blocks_per_sm = c4.soa_blocks_per_sm;
+    const mam4b_tuning &c5 = cand[5][i % cand[5].size()];
+    t.post_block = c5.post_block;
+    t.post_regs = c5.post_regs;
+    return t;
+  };
+  auto run = [&](const mam4b_tuning &t, float *stages, float *total) -> cudaError_t {
+    cudaError_t r = launch_pipeline_t(t, ctx->sms, a, s, precision, nullptr, ev, nullptr);
+    if (r == cudaSuccess)
+      r = cudaEventSynchronize(ev[6]);
+    float ms;
+    for (int k = 0; r == cudaSuccess && k < 6; ++k) {
+      r = cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+      if (stages)
+        stages[k] = ms;
+    }
+    if (r == cudaSuccess && total)
+      r = cudaEventElapsedTime(total, ev[0], ev[6]);
+    return r;
+  };
+  // warm-up
+  if (e == cudaSuccess)
+    e = run(d, nullptr, nullptr);
+  for (size_t i = 0; e == cudaSuccess && i < kmax; ++i) {
+    const mam4b_tuning t = combine(i);
+    for (int r = 0; e == cudaSuccess && r < reps; ++r) {
+      float st[6];
+      e = run(t, st, nullptr);
+      for (int k = 0; e == cudaSuccess && k < 6; ++k) {
+        const size_t j = i % cand[k].size();
+        if (i < cand[k].size())
+          stage_ms[k][j] = std::min(stage_ms[k][j], st[k]);
+      }
+    }
+  }
+  mam4b_tuning b = d;
+  if (e == cudaSuccess) {
+    size_t arg[6];
+    for (int k = 0; k < 6; ++k)
+      arg[k] = (size_t)(std::min_element(stage_ms[k].begin(), stage_ms[k].end()) -
+                        stage_ms[k].begin());
+    b.size_block = cand[0][arg[0]].size_block;
+    b.size_regs = cand[0][arg[0]].size_regs;
+    b.mode_block = cand[1][arg[1]].mode_block;
+    b.pair_block = cand[2][arg[2]].pair_block;
+    b.pre_block = cand[3][arg[3]].pre_block;
+    b.pre_regs = cand[3][arg[3]].pre_regs;
+    b.soa_block = cand[4][arg[4]].soa_block;
+    b.soa_regs = cand[4][arg[4]].soa_regs;
+    b.soa_blocks_per_sm = cand[4][arg[4]].soa_blocks_per_sm;
+    b.post_block = cand[5][arg[5]].post_block;
+    b.post_regs = cand[5][arg[5]].post_regs;
+  }
+  // cells per thread of the whole-cell kernels, then whole-pipeline times
+  auto total_of = [&](const mam4b_tuning &t, float &ms) -> cudaError_t {
+    ms = 1e30f;
+    cudaError_t r = cudaSuccess;
+    for (int k = 0; r == cudaSuccess && k < reps; ++k) {
+      float x;
+      r = run(t, nullptr, &x);
+      ms = std::min(ms, x);
+    }
+    return r;
+  };
+  float t_best = 1e30f;
+  for (int cpt : {1, 2, 4}) {
+    mam4b_tuning t = b;
+    t.cells_per_thread = cpt;
+    float ms = 1e30f;
+    if (e == cudaSuccess)
+      e = total_of(t, ms);
+    if (e == cudaSuccess && ms < t_best) {
+      t_best = ms;
+      b.cells_per_thread = cpt;
+    }
+  }
+  float t_def = 1e30f;
+  if (e == cudaSuccess)
+    e = total_of(d, t_def);
+  if (e == cudaSuccess)
+    e = total_of(b, t_best);
+  for (int k = 0; k < nev; ++k)
+    cudaEventDestroy(ev[k]);
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, what, e);
+  if (!(t_best < t_def)) {
+    b = d;
+    t_best = t_def;
+  }
+  ctx->tune = b;
+  if (best)
+    *best = b;
+  if (default_ms)
+    *default_ms = t_def;
+  if (best_ms)
+    *best_ms = t_best;
+  return MAM4B_OK;
 }
 
 // The step with gas-phase and aqueous chemistry ahead of amicphys (FP64):
@@ -3536,12 +4142,15 @@ mam4b_status mam4b_step_slab_noalloc(const mam4b_config *cfg, const double *in_s
     // no SOA loop to pipeline (and no scratch used)
     full_kernel<false><<<grid, block, 0, s>>>(a);
   } else {
-    size_kernel<<<grid, block, 0, s>>>(a);
-    mode_kernel<false><<<dim3(grid, NMODE), block, 0, s>>>(a);
-    pair_kernel<false><<<dim3(grid, 3), block, 0, s>>>(a);
-    pre_kernel<<<grid, block, 0, s>>>(a);
-    soa_kernel<false><<<nd.soa_grid, kSoaBlock, 0, s>>>(a);
-    post_kernel<<<grid, block, 0, s>>>(a);
+    // the default launch shape (mam4b_default_tuning)
+    mam4b_tuning t;
+    mam4b_default_tuning(&t);
+    launch_size(t, a, s);
+    launch_mode(t, a, s, false);
+    launch_pair(t, a, s, false);
+    launch_pre(t, a, s);
+    launch_soa(t, nd.sms, a, s, false);
+    launch_post(t, a, s);
   }
   e = cudaGetLastError();
   return e == cudaSuccess ? MAM4B_OK : MAM4B_ERR_CUDA;

@@ -78,6 +78,17 @@ class OpticsSwTables(ctypes.Structure):
                                                "refitab", "extp", "absp", "asmp")]
 
 
+class Tuning(ctypes.Structure):
+    """mam4b_tuning: launch shape of the forward step's kernels."""
+    _fields_ = [(k, ctypes.c_int) for k in (
+        "size_block", "size_regs", "mode_block", "pair_block", "pre_block", "pre_regs",
+        "post_block", "post_regs", "soa_block", "soa_regs", "soa_blocks_per_sm",
+        "cells_per_thread")]
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
 class CalcSizeConfig(ctypes.Structure):
     """mam4b_calcsize_config: CalcSize::Config (src/mam4xx/calcsize.hpp:835-842)."""
     _fields_ = [("do_aitacc_transfer", ctypes.c_int), ("do_adjust", ctypes.c_int)]
@@ -147,6 +158,19 @@ def lib():
         L.mam4b_coagulation_process.restype = I
         L.mam4b_launch_count.argtypes = [P]
         L.mam4b_launch_count.restype = ctypes.c_uint64
+        TP = ctypes.POINTER(Tuning)
+        L.mam4b_default_tuning.argtypes = [TP]
+        L.mam4b_get_tuning.argtypes = [P, TP]
+        L.mam4b_get_tuning.restype = I
+        L.mam4b_set_tuning.argtypes = [P, TP]
+        L.mam4b_set_tuning.restype = I
+        L.mam4b_tuning_from_json.argtypes = [ctypes.c_char_p, TP, ctypes.c_char_p, S]
+        L.mam4b_tuning_from_json.restype = I
+        FP = ctypes.POINTER(ctypes.c_float)
+        L.mam4b_autotune.argtypes = [P, P, P, P, S, I, I, D, I, I, P, TP, FP, FP]
+        L.mam4b_autotune.restype = I
+        L.mam4b_set_graph_mode.argtypes = [P, I]
+        L.mam4b_set_graph_mode.restype = I
         _lib = L
     return _lib
 
@@ -159,7 +183,24 @@ EXPORTED = ["mam4b_abi_version", "mam4b_default_config", "mam4b_create", "mam4b_
             "mam4b_activate",
             "mam4b_optics_lw_set_tables", "mam4b_optics_lw", "mam4b_optics_sw_set_tables",
             "mam4b_optics_sw", "mam4b_aero_rad_props_sw", "mam4b_aero_rad_props_lw",
-            "mam4b_dropmixnuc"]
+            "mam4b_dropmixnuc", "mam4b_default_tuning", "mam4b_get_tuning", "mam4b_set_tuning",
+            "mam4b_tuning_from_json", "mam4b_autotune", "mam4b_set_graph_mode"]
+
+
+def default_tuning():
+    t = Tuning()
+    lib().mam4b_default_tuning(ctypes.byref(t))
+    return t
+
+
+def tuning_from_json(path):
+    """(Tuning, device name) of a tuning file (mam4b_tuning_from_json)."""
+    t = Tuning()
+    dev = ctypes.create_string_buffer(256)
+    st = lib().mam4b_tuning_from_json(path.encode(), ctypes.byref(t), dev, 256)
+    if st != 0:
+        raise MicrophysicsError("mam4b_tuning_from_json(%s): %s" % (path, STATUS.get(st, st)))
+    return t, dev.value.decode()
 
 
 def default_config(**overrides):
@@ -374,6 +415,30 @@ class Context:
                                                  ctypes.byref(tends), int(ncol), int(nlev),
                                                  float(dt), ctypes.c_void_p(stream))
         self._check(st, "mam4b_coagulation_process")
+
+    def tuning(self):
+        t = Tuning()
+        self._check(self._lib.mam4b_get_tuning(self._h, ctypes.byref(t)), "mam4b_get_tuning")
+        return t
+
+    def set_tuning(self, t):
+        self._check(self._lib.mam4b_set_tuning(self._h, ctypes.byref(t)), "mam4b_set_tuning")
+
+    def set_graph_mode(self, enable):
+        self._check(self._lib.mam4b_set_graph_mode(self._h, int(bool(enable))),
+                    "mam4b_set_graph_mode")
+
+    def autotune(self, in_ptr, pblh_ptr, out_ptr, ld, ncol, nlev, dt, precision=FP64, reps=3,
+                 stream=0):
+        """Runs mam4b_autotune; returns (Tuning, default ms, tuned ms)."""
+        t = Tuning()
+        d_ms, b_ms = ctypes.c_float(0), ctypes.c_float(0)
+        st = self._lib.mam4b_autotune(self._h, in_ptr, pblh_ptr, out_ptr, int(ld), int(ncol),
+                                      int(nlev), float(dt), int(precision), int(reps),
+                                      ctypes.c_void_p(stream), ctypes.byref(t), ctypes.byref(d_ms),
+                                      ctypes.byref(b_ms))
+        self._check(st, "mam4b_autotune")
+        return t, float(d_ms.value), float(b_ms.value)
 
     def last_status(self):
         f = ctypes.c_uint32(0)

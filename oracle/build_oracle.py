@@ -15,6 +15,11 @@
                              when the reference tree exists (no cmake, no
                              Kokkos/EKAT: the shim stands in for the small
                              surface the headers use)
+  oracle/_ref/libmam4ref_gpu.so  nvcc, the same reference headers compiled
+                             unchanged for the GPU (sm_100a) against the
+                             same shim in its device mode, CUDA libm, no FMA
+                             contraction (oracle/ref/ref_step_gpu.cu): the
+                             libm-matched layer of the reference itself
   oracle/_ref/libmam4ref_tuned.so  the same reference build tuned for speed
                              (-O3 -march=x86-64-v3: AVX2 and FMA, FP
                              contraction allowed): the timed CPU baseline;
@@ -37,6 +42,7 @@ PORT_SO = os.path.join(HERE, "libmam4oracle.so")
 ULP_SO = os.path.join(HERE, "libmam4oracle_ulp.so")
 REF_SO = os.path.join(HERE, "_ref", "libmam4ref.so")
 REF_TUNED_SO = os.path.join(HERE, "_ref", "libmam4ref_tuned.so")
+REF_GPU_SO = os.path.join(HERE, "_ref", "libmam4ref_gpu.so")
 GPU_SO = os.path.join(HERE, "libmam4oracle_gpu.so")
 COUNT_SO = os.path.join(HERE, "libmam4oracle_count.so")
 DEFAULT_REF = "/root/reference"  # default checkout of the mam4xx tree
@@ -89,6 +95,14 @@ def build(ref=None, force=False):
         if force or _stale(REF_TUNED_SO, rdeps):
             _run(["g++", "-std=c++17"] + TUNED + ["-I", shim, "-I", src,
                   os.path.join(HERE, "ref", "ref_step.cpp"), "-o", REF_TUNED_SO])
+        gdeps = [os.path.join(HERE, "ref", "ref_step_gpu.cu"),
+                 os.path.join(shim, "kokkos_ekat_shim.hpp"), os.path.join(HERE, "oracle_api.h")]
+        if force or _stale(REF_GPU_SO, gdeps):
+            _run([os.environ.get("NVCC", "nvcc"), "-x", "cu",
+                  "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17",
+                  "--fmad=false", "--expt-relaxed-constexpr", "-diag-suppress", "20012,20014",
+                  "-Xcompiler", "-fPIC", "-shared", "-I", shim, "-I", src,
+                  os.path.join(HERE, "ref", "ref_step_gpu.cu"), "-o", REF_GPU_SO])
     return PORT_SO
 
 

@@ -17,6 +17,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_SO = os.path.join(HERE, "_ref", "libmam4ref.so")
 REF_TUNED_SO = os.path.join(HERE, "_ref", "libmam4ref_tuned.so")
+REF_GPU_SO = os.path.join(HERE, "_ref", "libmam4ref_gpu.so")
 # compiler flags of the two reference builds (oracle/build_oracle.py)
 REF_FLAGS = "g++ -O3 -ffp-contract=off -fopenmp (parity build)"
 REF_TUNED_FLAGS = "g++ -O3 -march=x86-64-v3 -ffp-contract=fast -fopenmp (tuned build)"
@@ -405,6 +406,40 @@ class GpuOracle:
         if rc != 0:
             raise RuntimeError("GPU oracle failed: %d" % rc)
         return (out, dg) if diag else out
+
+
+class RefGpuOracle:
+    """The mam4xx reference headers compiled unchanged for the GPU (CUDA
+    libm, no FMA contraction; oracle/ref/ref_step_gpu.cu): the reference
+    itself with the product's math library. step() returns the outputs and
+    checks that no reference kernel assert failed."""
+
+    def __init__(self):
+        if not os.path.exists(REF_GPU_SO):
+            raise FileNotFoundError(REF_GPU_SO)
+        self.lib = ctypes.CDLL(REF_GPU_SO)
+        self.lib.mam4refgpu_step.argtypes = [_I, _P, _S, _P, _P, _S, _D, ctypes.POINTER(Config),
+                                             ctypes.POINTER(ctypes.c_ulonglong)]
+        self.lib.mam4refgpu_step.restype = _I
+
+    def step(self, in_slab, pblh_cell, dt, cfg=None):
+        x = np.ascontiguousarray(in_slab, dtype=np.float64)
+        n = x.shape[1]
+        pb = np.ascontiguousarray(pblh_cell, dtype=np.float64)
+        out = np.zeros((NOUT, n))
+        cfg = cfg or default_config()
+        na = ctypes.c_ulonglong(0)
+        rc = self.lib.mam4refgpu_step(n, _ptr(x), n, _ptr(pb), _ptr(out), n, dt,
+                                      ctypes.byref(cfg), ctypes.byref(na))
+        if rc != 0:
+            raise RuntimeError("GPU reference build failed: %d" % rc)
+        if na.value:
+            raise RuntimeError("%d reference kernel asserts failed" % na.value)
+        return out
+
+
+def reference_gpu_available():
+    return os.path.exists(REF_GPU_SO)
 
 
 def reference_available():

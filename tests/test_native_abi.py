@@ -59,3 +59,28 @@ def test_invalid_arguments_are_rejected_without_a_device(lib):
     h = ctypes.c_void_p()
     bad = native.Config(1, 1, 1, 1, 7, 2, 8)  # optaa must be 1 or 2
     assert L.mam4b_create(ctypes.byref(h), ctypes.byref(bad)) == 1
+
+
+def test_tuning_file_round_trip_and_validation(tmp_path):
+    """Tuning files are parsed on the host (no CUDA call): the committed one
+    (when present) is valid, a written one reads back, and invalid shapes
+    or incomplete files are rejected."""
+    import json
+    from mam4xx_b200 import native
+    committed = os.path.join(ROOT, "mam4xx_b200", "mam4b_tuning.json")
+    if os.path.exists(committed):
+        t, dev = native.tuning_from_json(committed)
+        assert dev and t.as_dict() == {k: json.load(open(committed))[k] for k in t.as_dict()}
+    d = native.default_tuning().as_dict()
+    d.update(pre_regs=168, post_block=64, soa_blocks_per_sm=3, cells_per_thread=2)
+    p = tmp_path / "t.json"
+    p.write_text(json.dumps(dict(d, device="NVIDIA B200", chosen_on={"tuned_ms": 1.0})))
+    t, dev = native.tuning_from_json(str(p))
+    assert t.as_dict() == d and dev == "NVIDIA B200"
+    for bad in (dict(d, pre_regs=200), dict(d, size_block=512), dict(d, soa_blocks_per_sm=0),
+                dict(d, cells_per_thread=3), {k: v for k, v in d.items() if k != "soa_regs"}):
+        p.write_text(json.dumps(bad))
+        with pytest.raises(native.MicrophysicsError):
+            native.tuning_from_json(str(p))
+    with pytest.raises(native.MicrophysicsError):
+        native.tuning_from_json(str(tmp_path / "missing.json"))

@@ -187,3 +187,31 @@ def test_counting_build_matches_and_counts():
     fresh = count(cells=2304)
     for name, v in fresh.items():
         assert abs(v["flops_per_cell"] / committed[name]["flops_per_cell"] - 1) < 0.15, name
+
+
+def test_reference_device_build_host_path_equals_reference_build(ref_oracle):
+    """oracle/_ref/libmam4ref_gpu.so compiles the reference headers with nvcc
+    against the shim's device mode; its composition run on the host (glibc
+    libm) must equal the g++ build of the same headers bit for bit, which
+    checks the shim's device mode and the device driver's composition
+    without a GPU."""
+    import ctypes
+    from oracle import pyoracle
+    if not pyoracle.reference_gpu_available():
+        pytest.skip("reference headers not compiled for the GPU")
+    lib = ctypes.CDLL(pyoracle.REF_GPU_SO)
+    f = lib.mam4refgpu_step_on_host
+    P = ctypes.c_void_p
+    f.argtypes = [ctypes.c_int, P, ctypes.c_size_t, P, P, ctypes.c_size_t, ctypes.c_double,
+                  ctypes.POINTER(pyoracle.Config)]
+    for name, ncol, cfg in (("c1", None, {}), ("c2", 24, {}), ("c4", 24, {}),
+                            ("c2", 8, {"do_cond": 0}), ("c2", 8, {"gaexch_h2so4_uptake_optaa": 1})):
+        w = make_workload(name, ncol=ncol)
+        x = np.ascontiguousarray(w["in_slab"])
+        pb = pblh_per_cell(w)
+        n = x.shape[1]
+        out = np.zeros((68, n))
+        c = pyoracle.default_config(**cfg)
+        f(n, x.ctypes.data, n, pb.ctypes.data, out.ctypes.data, n, w["dt"], ctypes.byref(c))
+        ref = ref_oracle.step(x, pb, w["dt"], cfg=c)
+        np.testing.assert_array_equal(out, ref)
