@@ -131,14 +131,18 @@ typedef enum mam4b_status {
  * coagulation coefficients) and keep FP64 in calcsize, the H2SO4 implicit
  * exponential update, the renaming transfer fractions, the nucleation rate
  * fits (their polynomials cancel to a few digits in FP32), aging and every
- * state update and sum that carries species mass. MAM4B_MIXED keeps the
- * SOA sub-stepping in FP64 too; MAM4B_MIXED_FAST runs it in FP32, which is
+ * state update and sum that carries species mass. Where an FP32 value
+ * decides a branch at its threshold (the SOA loop's 1e-15 uptake cut-off,
+ * the coagulation table index), the FP64 value is used. MAM4B_MIXED runs
+ * the SOA sub-stepping with an FP64 state and FP64 semi-implicit update and
+ * FP32 step control (saturation ratios, departures from equilibrium, the
+ * sub-step length); MAM4B_MIXED_FAST runs the whole loop in FP32, which is
  * faster but leaves the results of many cells 1e-4..1e-2 away from FP64
  * (the loop amplifies rounding near equilibrium). Per-process diagnostics
  * are FP64 only. */
 typedef enum mam4b_precision {
   MAM4B_FP64 = 0,       /* plain double precision throughout              */
-  MAM4B_MIXED = 1,      /* FP32 bulk, FP64 condensation                   */
+  MAM4B_MIXED = 1,      /* FP32 bulk, FP64 condensation state and update  */
   MAM4B_MIXED_FAST = 2  /* FP32 bulk and FP32 SOA sub-stepping            */
 } mam4b_precision;
 
@@ -267,6 +271,46 @@ mam4b_status mam4b_autotune(mam4b_ctx *ctx, const double *in_slab, const double 
  * launches.
  */
 mam4b_status mam4b_set_graph_mode(mam4b_ctx *ctx, int enable);
+
+/*
+ * One column of a host model that keeps one array per field and column
+ * (mam4::Atmosphere / Prognostics / Diagnostics / Tendencies ColumnViews,
+ * src/mam4xx/atmosphere.hpp:70-118, aero_config.hpp:74-130): device
+ * pointers to nlev doubles each.
+ *   in[MAM4B_NIN]   the step's inputs in MAM4B_IN_* order (populations in
+ *                   the E3SM state_q order of the header's table)
+ *   pblh            the column's boundary-layer height [m]
+ *   tend[52]        tendency columns of the 52 prognostics (H2SO4, SOAG, 25
+ *                   interstitial, 25 cloud-borne); the step ADDS its
+ *                   tendency to each (as processes add to a shared
+ *                   Tendencies); NULL: not written
+ *   mode_out[16]    dry diameter, wet diameter, wet density and aerosol water
+ *                   of the 4 interstitial modes (outputs 52..67), written;
+ *                   NULL: not written
+ */
+typedef struct mam4b_column {
+  const double *in[MAM4B_NIN];
+  double pblh;
+  double *tend[MAM4B_NUM_PROG];
+  double *mode_out[MAM4B_NOUT - MAM4B_NUM_PROG];
+} mam4b_column;
+
+/*
+ * The step on ncol such columns (cols: a host array): gathers them into the
+ * context's staging slabs, runs the step and adds/writes the results into
+ * the columns, on `stream`. This is the batched entry behind the C++
+ * mam4::MicrophysicsProcess (include/mam4b_microphysics.hpp): it replaces
+ * the host's parallel_for(team_policy, ...) over columns of
+ * AeroProcess::compute_tendencies (src/validation/aero_process.hpp:114).
+ * Copies the column tables to the device synchronously; the kernels are
+ * asynchronous on `stream`.
+ */
+mam4b_status mam4b_step_columns(mam4b_ctx *ctx, const mam4b_column *cols, int ncol, int nlev,
+                                double dt, int precision, void *stream);
+
+/* Waits for the work of the context's last call (its stream); returns
+ * MAM4B_ERR_CUDA when that work failed. */
+mam4b_status mam4b_synchronize(mam4b_ctx *ctx);
 
 /*
  * Host-buffer convenience: copies the host slabs to the device, runs the

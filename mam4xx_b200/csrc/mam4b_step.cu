@@ -1336,11 +1336,19 @@ __device__ __forceinline__ void size_cell(const StepArgs &a, const long long c) 
   a.aux[AUX_FPATH * n + c] = fp;
 }
 
-template <int R>
+// LOOP: grid-stride loop over cells (cells_per_thread > 1); without it one
+// cell per thread, which leaves the register allocation of the body as is.
+template <int R, bool LOOP>
 __global__ void __maxnreg__(R) size_kernel(const __grid_constant__ StepArgs a) {
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < a.ncell; c += stride)
-    size_cell(a, c);
+  const long long c0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if constexpr (LOOP) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+#pragma unroll 1
+    for (long long c = c0; c < a.ncell; c += stride)
+      size_cell(a, c);
+  } else if (c0 < a.ncell) {
+    size_cell(a, c0);
+  }
 }
 
 // Stage 2, one thread per (cell, mode): water uptake of the mode (Kohler
@@ -1445,12 +1453,18 @@ __global__ void pair_kernel(const __grid_constant__ StepArgs a) {
   cc[(9 + p) * n] = bjj0;
 }
 
-template <int R, bool MIXED>
+template <int R, bool MIXED, bool LOOP>
 __global__ void __maxnreg__(R) pre_kernel(const __grid_constant__ StepArgs a) {
   const ChemArgs none = {nullptr, nullptr, 0};
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < a.ncell; c += stride)
-    cell_pre<false, MIXED>(a, none, c);
+  const long long c0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if constexpr (LOOP) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+#pragma unroll 1
+    for (long long c = c0; c < a.ncell; c += stride)
+      cell_pre<false, MIXED>(a, none, c);
+  } else if (c0 < a.ncell) {
+    cell_pre<false, MIXED>(a, none, c0);
+  }
 }
 
 // The pre stage of the step with chemistry (mam4b_step_chem_slab).
@@ -1463,12 +1477,18 @@ __global__ void __launch_bounds__(128) pre_chem_kernel(const __grid_constant__ S
 
 // (the 128-register cap, 4 blocks of 128 per SM with a few hundred bytes
 // spilled to L1, was 2 % faster than the unconstrained 231-register build)
-template <int R>
+template <int R, bool LOOP>
 __global__ void __maxnreg__(R) post_kernel(const __grid_constant__ StepArgs a) {
   const long long nq = (long long)a.counters[CNT_QUEUED];
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += stride)
-    cell_post(a, (unsigned)i);
+  const long long i0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if constexpr (LOOP) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+#pragma unroll 1
+    for (long long i = i0; i < nq; i += stride)
+      cell_post(a, (unsigned)i);
+  } else if (i0 < nq) {
+    cell_post(a, (unsigned)i0);
+  }
 }
 
 // SOA sub-stepping of the queued cells. Persistent warps; every lane owns
@@ -1482,9 +1502,21 @@ __global__ void __maxnreg__(R) post_kernel(const __grid_constant__ StepArgs a) {
 // Launched with any block size that is a multiple of 32 and one grid of
 // persistent blocks (SMs x blocks per SM).
 constexpr int kSoaBlock = 256;
-template <bool MIXED, int R>
+template <int SOA, class State>
+__device__ __forceinline__ bool soa_pass(State &st) {
+  if constexpr (SOA == 1)
+    return f32::soa_step_mx(st);
+  else
+    return soa_step(st);
+}
+
+// SOA: 0 the FP64 loop (soa_step), 1 FP64 state with FP32 step control
+// (f32::soa_step_mx, MAM4B_MIXED), 2 the FP32 loop (f32::soa_step,
+// MAM4B_MIXED_FAST).
+template <int SOA, int R>
 __global__ void __maxnreg__(R) soa_kernel(const __grid_constant__ StepArgs a) {
-  using State = typename std::conditional<MIXED, f32::SoaStateF, SoaState>::type;
+  constexpr bool F32 = SOA == 2;
+  using State = typename std::conditional<F32, f32::SoaStateF, SoaState>::type;
   const unsigned ntask = a.counters[CNT_QUEUED];
   const unsigned nlong = a.counters[CNT_LONG];
   const int lane = threadIdx.x & 31;
@@ -1523,7 +1555,7 @@ __global__ void __maxnreg__(R) soa_kernel(const __grid_constant__ StepArgs a) {
     }
     if (!__any_sync(0xffffffffu, active))
       break;
-    if (active && !soa_step(st)) {
+    if (active && !soa_pass<SOA>(st)) {
       double *q = a.soa + slot;
       q[SOA_G * n] = st.g;
 #pragma unroll
@@ -2940,6 +2972,37 @@ __global__ void __launch_bounds__(128) dropmix_kernel(const __grid_constant__ Dr
 }  // namespace mam4b
 
 // =============================================================== C ABI
+namespace mam4b {
+// Column gather/scatter of mam4b_step_columns: tab[f * ncol + col] points
+// at column col of field f (nlev doubles); slab is [nfield][ncol * nlev].
+__global__ void __launch_bounds__(128) gather_columns_kernel(const double *const *tab, double *slab,
+                                                             int ncol, int nlev) {
+  const long long ncell = (long long)ncol * nlev;
+  const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (cell >= ncell)
+    return;
+  const int f = blockIdx.y;
+  const int col = (int)(cell / nlev), lev = (int)(cell - (long long)col * nlev);
+  slab[(size_t)f * ncell + cell] = tab[(size_t)f * ncol + col][lev];
+}
+// first nadd fields added to their columns, the rest written; null columns skipped
+__global__ void __launch_bounds__(128) scatter_columns_kernel(double *const *tab,
+                                                              const double *slab, int ncol,
+                                                              int nlev, int nadd) {
+  const long long ncell = (long long)ncol * nlev;
+  const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (cell >= ncell)
+    return;
+  const int f = blockIdx.y;
+  const int col = (int)(cell / nlev), lev = (int)(cell - (long long)col * nlev);
+  double *p = tab[(size_t)f * ncol + col];
+  if (!p)
+    return;
+  const double v = slab[(size_t)f * ncell + cell];
+  p[lev] = (f < nadd) ? p[lev] + v : v;
+}
+}  // namespace mam4b
+
 using namespace mam4b;
 
 // Host-buffer path: columns are processed in chunks of about kHostChunkCells
@@ -2999,6 +3062,11 @@ struct mam4b_ctx {
   double *d_dmx;        // dropmixnuc activation results (DA_FIELDS per cell), grown
   size_t cap_dmx;
   unsigned *d_bins;     // [2 kPassBins]: loops per pass count, start offsets
+  // mam4b_step_columns: device pointer tables of the columns (grown) and
+  // their host staging
+  void **d_coltab;
+  size_t cap_coltab;
+  std::vector<void *> h_coltab;
   int adj_soa_grid;
   size_t cap_adj;
   // host path: copy/compute streams and their events (created on first use)
@@ -3131,14 +3199,21 @@ unsigned grid_for(long long n, int block, int cpt) {
 }
 
 // Stage launchers. Stage order: 0 size, 1 mode, 2 pair, 3 pre, 4 soa, 5 post.
-void launch_size(const mam4b_tuning &t, const StepArgs &a, cudaStream_t s) {
+template <bool LOOP>
+void launch_size_t(const mam4b_tuning &t, const StepArgs &a, cudaStream_t s) {
   const unsigned g = grid_for(a.ncell, t.size_block, t.cells_per_thread);
   if (t.size_regs == 96)
-    size_kernel<96><<<g, t.size_block, 0, s>>>(a);
+    size_kernel<96, LOOP><<<g, t.size_block, 0, s>>>(a);
   else if (t.size_regs == 128)
-    size_kernel<128><<<g, t.size_block, 0, s>>>(a);
+    size_kernel<128, LOOP><<<g, t.size_block, 0, s>>>(a);
   else
-    size_kernel<255><<<g, t.size_block, 0, s>>>(a);
+    size_kernel<255, LOOP><<<g, t.size_block, 0, s>>>(a);
+}
+void launch_size(const mam4b_tuning &t, const StepArgs &a, cudaStream_t s) {
+  if (t.cells_per_thread > 1)
+    launch_size_t<true>(t, a, s);
+  else
+    launch_size_t<false>(t, a, s);
 }
 void launch_mode(const mam4b_tuning &t, const StepArgs &a, cudaStream_t s, bool mixed) {
   const dim3 g(grid_for(a.ncell, t.mode_block, 1), NMODE);
@@ -3154,47 +3229,59 @@ void launch_pair(const mam4b_tuning &t, const StepArgs &a, cudaStream_t s, bool 
   else
     pair_kernel<false><<<g, t.pair_block, 0, s>>>(a);
 }
-template <bool MIXED>
+template <bool MIXED, bool LOOP>
 void launch_pre_t(const mam4b_tuning &t, const StepArgs &a, cudaStream_t s) {
   const unsigned g = grid_for(a.ncell, t.pre_block, t.cells_per_thread);
   if (t.pre_regs == 128)
-    pre_kernel<128, MIXED><<<g, t.pre_block, 0, s>>>(a);
+    pre_kernel<128, MIXED, LOOP><<<g, t.pre_block, 0, s>>>(a);
   else if (t.pre_regs == 168)
-    pre_kernel<168, MIXED><<<g, t.pre_block, 0, s>>>(a);
+    pre_kernel<168, MIXED, LOOP><<<g, t.pre_block, 0, s>>>(a);
   else
-    pre_kernel<255, MIXED><<<g, t.pre_block, 0, s>>>(a);
+    pre_kernel<255, MIXED, LOOP><<<g, t.pre_block, 0, s>>>(a);
 }
 void launch_pre(const mam4b_tuning &t, const StepArgs &a, cudaStream_t s, bool mixed = false) {
+  const bool loop = t.cells_per_thread > 1;
   if (mixed)
-    launch_pre_t<true>(t, a, s);
+    loop ? launch_pre_t<true, true>(t, a, s) : launch_pre_t<true, false>(t, a, s);
   else
-    launch_pre_t<false>(t, a, s);
+    loop ? launch_pre_t<false, true>(t, a, s) : launch_pre_t<false, false>(t, a, s);
 }
-template <bool MIXED>
+template <int SOA>
 void launch_soa_t(const mam4b_tuning &t, int sms, const StepArgs &a, cudaStream_t s) {
   const unsigned g = (unsigned)(sms * t.soa_blocks_per_sm);
   if (t.soa_regs == 128)
-    soa_kernel<MIXED, 128><<<g, t.soa_block, 0, s>>>(a);
+    soa_kernel<SOA, 128><<<g, t.soa_block, 0, s>>>(a);
   else if (t.soa_regs == 96)
-    soa_kernel<MIXED, 96><<<g, t.soa_block, 0, s>>>(a);
+    soa_kernel<SOA, 96><<<g, t.soa_block, 0, s>>>(a);
   else
-    soa_kernel<MIXED, 64><<<g, t.soa_block, 0, s>>>(a);
+    soa_kernel<SOA, 64><<<g, t.soa_block, 0, s>>>(a);
 }
-void launch_soa(const mam4b_tuning &t, int sms, const StepArgs &a, cudaStream_t s, bool fast) {
-  if (fast)
-    launch_soa_t<true>(t, sms, a, s);
+// the SOA loop of each precision (mam4b_precision)
+void launch_soa(const mam4b_tuning &t, int sms, const StepArgs &a, cudaStream_t s,
+                int precision) {
+  if (precision == MAM4B_MIXED_FAST)
+    launch_soa_t<2>(t, sms, a, s);
+  else if (precision == MAM4B_MIXED)
+    launch_soa_t<1>(t, sms, a, s);
   else
-    launch_soa_t<false>(t, sms, a, s);
+    launch_soa_t<0>(t, sms, a, s);
 }
-void launch_post(const mam4b_tuning &t, const StepArgs &a, cudaStream_t s) {
+template <bool LOOP>
+void launch_post_t(const mam4b_tuning &t, const StepArgs &a, cudaStream_t s) {
   // one thread per queued slot at most; the kernel reads the queue length
   const unsigned g = grid_for(a.ncell, t.post_block, t.cells_per_thread);
   if (t.post_regs == 255)
-    post_kernel<255><<<g, t.post_block, 0, s>>>(a);
+    post_kernel<255, LOOP><<<g, t.post_block, 0, s>>>(a);
   else if (t.post_regs == 168)
-    post_kernel<168><<<g, t.post_block, 0, s>>>(a);
+    post_kernel<168, LOOP><<<g, t.post_block, 0, s>>>(a);
   else
-    post_kernel<128><<<g, t.post_block, 0, s>>>(a);
+    post_kernel<128, LOOP><<<g, t.post_block, 0, s>>>(a);
+}
+void launch_post(const mam4b_tuning &t, const StepArgs &a, cudaStream_t s) {
+  if (t.cells_per_thread > 1)
+    launch_post_t<true>(t, a, s);
+  else
+    launch_post_t<false>(t, a, s);
 }
 
 // Clears the counters and queues the pipeline kernels on s in the
@@ -3242,7 +3329,7 @@ cudaError_t launch_pipeline_t(const mam4b_tuning &t, int sms, const StepArgs &a_
     launch_pre(t, a, s, mixed);
   }
   mark(4);
-  launch_soa(t, sms, a, s, precision == MAM4B_MIXED_FAST);
+  launch_soa(t, sms, a, s, precision);
   mark(5);
   launch_post(t, a, s);
   mark(6);
@@ -3614,6 +3701,7 @@ mam4b_status mam4b_destroy(mam4b_ctx *ctx) {
   drop_graph(ctx);
   if (ctx->cap_stream)
     cudaStreamDestroy(ctx->cap_stream);
+  cudaFree(ctx->d_coltab);
   cudaFree(ctx->d_flags);
   cudaFree(ctx->d_in);
   cudaFree(ctx->d_out);
@@ -4075,6 +4163,94 @@ mam4b_status mam4b_step_host(mam4b_ctx *ctx, const double *in_slab, const double
   return MAM4B_OK;
 }
 
+// The step on per-column arrays (include/mam4b.h, mam4b_step_columns):
+// gather the columns into the context's staging slabs, the pipeline, then
+// add the tendencies to (and write the mode outputs into) the caller's
+// columns. Two pointer tables go to the device per call, synchronously.
+mam4b_status mam4b_step_columns(mam4b_ctx *ctx, const mam4b_column *cols, int ncol, int nlev,
+                                double dt, int precision, void *stream) {
+  const char *what = "mam4b_step_columns";
+  if (!ctx || !cols || ncol < 0 || nlev <= 0 || !(dt > 0.0) || !isfinite(dt) ||
+      (long long)ncol * nlev > 0x7fffffffLL ||
+      (precision != MAM4B_FP64 && precision != MAM4B_MIXED && precision != MAM4B_MIXED_FAST))
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, what, cudaSuccess);
+  for (int c = 0; c < ncol; ++c)
+    for (int f = 0; f < MAM4B_NIN; ++f)
+      if (!cols[c].in[f])
+        return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_step_columns: null input column",
+                       cudaSuccess);
+  if (ncol == 0)
+    return MAM4B_OK;
+  const size_t ncell = (size_t)ncol * nlev;
+  cudaStream_t s = (cudaStream_t)stream;
+  ctx->last_stream = s;
+  cudaError_t e = grow(&ctx->d_in, &ctx->cap_in, (size_t)MAM4B_NIN * ncell);
+  if (e == cudaSuccess)
+    e = grow(&ctx->d_out, &ctx->cap_out, (size_t)MAM4B_NOUT * ncell);
+  if (e == cudaSuccess)
+    e = grow(&ctx->d_pblh, &ctx->cap_pblh, (size_t)ncol);
+  const size_t ntab = (size_t)(MAM4B_NIN + MAM4B_NOUT) * ncol;
+  if (e == cudaSuccess && ctx->cap_coltab < ntab) {
+    cudaFree(ctx->d_coltab);
+    ctx->d_coltab = nullptr;
+    ctx->cap_coltab = 0;
+    e = cudaMalloc(&ctx->d_coltab, ntab * sizeof(void *));
+    if (e == cudaSuccess)
+      ctx->cap_coltab = ntab;
+  }
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, "mam4b_step_columns scratch", e);
+  // tables [input fields][col], then [output fields][col]; pblh per column
+  ctx->h_coltab.assign(ntab + (size_t)ncol, nullptr);
+  double *pb = reinterpret_cast<double *>(ctx->h_coltab.data() + ntab);
+  for (int c = 0; c < ncol; ++c) {
+    for (int f = 0; f < MAM4B_NIN; ++f)
+      ctx->h_coltab[(size_t)f * ncol + c] = const_cast<double *>(cols[c].in[f]);
+    for (int f = 0; f < MAM4B_NUM_PROG; ++f)
+      ctx->h_coltab[(size_t)(MAM4B_NIN + f) * ncol + c] = cols[c].tend[f];
+    for (int f = 0; f < MAM4B_NOUT - MAM4B_NUM_PROG; ++f)
+      ctx->h_coltab[(size_t)(MAM4B_NIN + MAM4B_NUM_PROG + f) * ncol + c] = cols[c].mode_out[f];
+    pb[c] = cols[c].pblh;
+  }
+  static_assert(sizeof(double) == sizeof(void *), "pblh shares the pointer staging");
+  e = cudaMemcpyAsync(ctx->d_coltab, ctx->h_coltab.data(), ntab * sizeof(void *),
+                      cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(ctx->d_pblh, pb, (size_t)ncol * sizeof(double), cudaMemcpyHostToDevice, s);
+  // the host staging is reused by the next call: wait for the copies
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(s);
+  const int block = 128;
+  const unsigned gx = (unsigned)((ncell + block - 1) / block);
+  if (e == cudaSuccess) {
+    gather_columns_kernel<<<dim3(gx, MAM4B_NIN), block, 0, s>>>(
+        reinterpret_cast<const double *const *>(ctx->d_coltab), ctx->d_in, ncol, nlev);
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, what, e);
+  ctx->launches += 1;
+  const mam4b_status st = mam4b_step_slab(ctx, ctx->d_in, ctx->d_pblh, ctx->d_out, ncell, ncol,
+                                          nlev, dt, precision, stream);
+  if (st != MAM4B_OK)
+    return st;
+  scatter_columns_kernel<<<dim3(gx, MAM4B_NOUT), block, 0, s>>>(
+      reinterpret_cast<double *const *>(ctx->d_coltab) + (size_t)MAM4B_NIN * ncol, ctx->d_out,
+      ncol, nlev, MAM4B_NUM_PROG);
+  e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, what, e);
+  ctx->launches += 1;
+  return MAM4B_OK;
+}
+
+mam4b_status mam4b_synchronize(mam4b_ctx *ctx) {
+  if (!ctx)
+    return MAM4B_ERR_INVALID_ARGUMENT;
+  const cudaError_t e = cudaStreamSynchronize(ctx->last_stream);
+  return e == cudaSuccess ? MAM4B_OK : set_err(ctx, MAM4B_ERR_CUDA, "mam4b_synchronize", e);
+}
+
 // Allocation-free step for callers that cannot call cudaMalloc (a host
 // model whose memory pool owns the GPU's memory, or that forbids the
 // device-wide synchronisation of cudaMalloc/cudaFree once it runs). Same
@@ -4149,7 +4325,7 @@ mam4b_status mam4b_step_slab_noalloc(const mam4b_config *cfg, const double *in_s
     launch_mode(t, a, s, false);
     launch_pair(t, a, s, false);
     launch_pre(t, a, s);
-    launch_soa(t, nd.sms, a, s, false);
+    launch_soa(t, nd.sms, a, s, MAM4B_FP64);
     launch_post(t, a, s);
   }
   e = cudaGetLastError();

@@ -184,7 +184,8 @@ EXPORTED = ["mam4b_abi_version", "mam4b_default_config", "mam4b_create", "mam4b_
             "mam4b_optics_lw_set_tables", "mam4b_optics_lw", "mam4b_optics_sw_set_tables",
             "mam4b_optics_sw", "mam4b_aero_rad_props_sw", "mam4b_aero_rad_props_lw",
             "mam4b_dropmixnuc", "mam4b_default_tuning", "mam4b_get_tuning", "mam4b_set_tuning",
-            "mam4b_tuning_from_json", "mam4b_autotune", "mam4b_set_graph_mode"]
+            "mam4b_tuning_from_json", "mam4b_autotune", "mam4b_set_graph_mode",
+            "mam4b_step_columns", "mam4b_synchronize"]
 
 
 def default_tuning():

@@ -174,6 +174,7 @@ MAM4SHIM_HD inline double pow(A x, B y) {
   return ::pow(static_cast<double>(x), static_cast<double>(y));
 }
 MAM4SHIM_HD inline double nan(const char *s) { return ::nan(s); }
+MAM4SHIM_HD inline double copysign(double x, double y) { return ::copysign(x, y); }
 #else
 using std::abs;
 using std::atan;
@@ -189,6 +190,7 @@ using std::pow;
 using std::round;
 using std::sin;
 using std::sqrt;
+using std::copysign;
 inline double nan(const char *s) { return std::nan(s); }
 #endif
 template <class T> MAM4SHIM_HD constexpr const T &min(const T &a, const T &b) {
@@ -699,6 +701,10 @@ template <class F, class... P> void parallel_for(const RangePolicy<P...> &r, con
   for (int i = r.b; i < r.e; ++i)
     f(i);
 }
+template <class F, class... P>
+void parallel_for(const std::string &, const RangePolicy<P...> &r, const F &f) {
+  parallel_for(r, f);
+}
 
 template <class T> struct Sum {
   T &ref;
@@ -766,6 +772,7 @@ template <class Dev> struct KokkosTypes {
   using MemSpace = Kokkos::HostSpace;
   using TeamPolicy = Kokkos::TeamPolicy;
   using MemberType = Kokkos::TeamMember;
+  using RangePolicy = Kokkos::RangePolicy<>;
   template <class T> using view = Kokkos::View<T>;
   template <class T> using view_1d = Kokkos::View<T *>;
   template <class T> using view_2d = Kokkos::View<T **>;
