@@ -654,6 +654,23 @@ def mixed_leg(native, torch, dev, stream, args, ws, rank):
             res["fp64"] = {"value": ws * nm / (times[name] * 1e-3), "ms_per_step": times[name]}
             continue
         r = error_report_device(got, ref, xm, wm["dt"], tol=1e-5)
+        if name == "mixed":
+            # the FP64 step's own sensitivity: its results for inputs moved
+            # by one ulp and by 1e-7 (the size of FP32 rounding), against
+            # its results for the unperturbed inputs
+            pert = {}
+            for lab, eps in (("1ulp", 2.0 ** -52), ("1e-7", 1e-7)):
+                xq = xm * (1.0 + eps)
+                ctx.step_slab(xq.data_ptr(), pbm.data_ptr(), got.data_ptr(), nm, wm["ncol"], NLEV,
+                              wm["dt"], precision=native.FP64, stream=stream.cuda_stream)
+                torch.cuda.synchronize()
+                rq = error_report_device(got, ref, xm, wm["dt"], tol=1e-5)
+                pert[lab] = {"cells_within_1e-5": rq["cells_within_tol"], "max": rq["max"],
+                             "cell_err_quantiles": rq["cell_err_quantiles"]}
+                del xq
+            res["fp64_input_perturbation"] = pert
+            f()  # the mixed results again, for the report below
+            torch.cuda.synchronize()
         worst = sorted(range(native.NOUT), key=lambda k: -r["per_output_max"][k])[:6]
         res[name] = {"value": ws * nm / (times[name] * 1e-3), "unit": "cells/s",
                      "ms_per_step": times[name],

@@ -214,9 +214,13 @@ mam4b_status mam4b_step_slab(mam4b_ctx *ctx, const double *in_slab,
  * register cap of a kernel (size 255, 128 or 96; pre and post 255, 168 or 128;
  * soa 64, 96 or 128; block x regs <= 65536); soa_blocks_per_sm sizes the
  * solver's persistent grid (1..16 blocks per SM); cells_per_thread (1, 2,
- * 4) is how many cells each thread of size, pre and post steps, i.e.
- * 32 x cells_per_thread cells per warp. Every shape computes the same
- * results bit for bit; only the speed differs.
+ * 4) is how many cells each thread of size and post steps, i.e.
+ * 32 x cells_per_thread cells per warp; inline_scale (0 = off, 1, 4, 16,
+ * 64): cells whose first SOA sub-step is at least 1/inline_scale of the time
+ * step (short loops, predicted from the first sub-step) run their loop and
+ * finish inside pre, without the hand-off to the solver and post kernels
+ * (FP64 and MAM4B_MIXED; not in the adjoint's forward). Every shape computes
+ * the same results bit for bit; only the speed differs.
  */
 typedef struct mam4b_tuning {
   int size_block, size_regs;
@@ -225,10 +229,11 @@ typedef struct mam4b_tuning {
   int post_block, post_regs;
   int soa_block, soa_regs, soa_blocks_per_sm;
   int cells_per_thread;
+  int inline_scale;
 } mam4b_tuning;
 
 /* The built-in shape (size 128/128, mode 128, pair 128, pre 128/255, post
- * 128/128, soa 256/64 x 4 per SM, one cell per thread). */
+ * 128/128, soa 256/64 x 4 per SM, one cell per thread, no inline loops). */
 void mam4b_default_tuning(mam4b_tuning *t);
 
 /* A context starts with the shape in the file named by the environment

@@ -63,6 +63,8 @@ struct StepArgs {
   unsigned *counters;
   int *npass;        // [ncell] or null: passes of each slot's loop (adjoint only)
   int mixed;         // the mode/pair stages ran in FP32 (MAM4B_MIXED, _FAST)
+  double inline_scale;  // pre_kernel<.., FUSE>: cells whose first SOA sub-step
+                        // is at least 1/inline_scale of the step finish in pre
 };
 
 // The step runs as a pipeline of three kernels when condensation is on and
@@ -1010,7 +1012,31 @@ __device__ __forceinline__ void guard_soa_threshold(const StepArgs &a, const lon
   }
 }
 
-template <bool CHEM, bool MIXED = false>
+template <class Src>
+__device__ __forceinline__ void cell_finish(const StepArgs &a, const long long c, double temp,
+                                            double pmid, double zm, double cld, double pblh,
+                                            double relhum, double dgn_pc, Sub &s, ClearMid &cm,
+                                            const Src &src);
+// cell_finish's late inputs held in registers (the fused path of pre)
+struct FinishRegs {
+  const double (&oc_)[NPOP];
+  const double (&ci_)[NPOP];
+  const double (&cg_)[2];
+  const double (&ai_)[NPOP];
+  const double (&ac_)[NPOP];
+  double h2so4_, soag_;
+  __device__ double oc(int p) const { return oc_[p]; }
+  __device__ double ci(int p) const { return ci_[p]; }
+  __device__ double cg(int g) const { return cg_[g]; }
+  __device__ double ai(int p) const { return ai_[p]; }
+  __device__ double ac(int p) const { return ac_[p]; }
+  __device__ double h2so4() const { return h2so4_; }
+  __device__ double soag() const { return soag_; }
+};
+template <int SOA, class State>
+__device__ __forceinline__ bool soa_pass(State &st);
+
+template <bool CHEM, bool MIXED = false, bool FUSE = false>
 __device__ __forceinline__ void cell_pre(const StepArgs &a, const ChemArgs &ch,
                                          const long long c) {
   const StepConsts &C = c_k;
@@ -1032,7 +1058,10 @@ __device__ __forceinline__ void cell_pre(const StepArgs &a, const ChemArgs &ch,
   }
   const bool partly = !(f.cld < 1.0e-5);
   Sub s;
-  double rh, oc[NPOP], ci[NPOP], cg[2];
+  double rh, oc[NPOP], ci[NPOP], cg[2] = {0.0, 0.0};
+#pragma unroll
+  for (int p = 0; p < NPOP; ++p)
+    ci[p] = 0.0;
   if (!partly) {
     load_sub_plain(s, f.qi);
     s.gas[0] = f.g_soag * fsoag;
@@ -1067,7 +1096,26 @@ __device__ __forceinline__ void cell_pre(const StepArgs &a, const ChemArgs &ch,
   // queue the cell: solver state and hand-off at the start of the SOA loop
   SoaState st;
   soa_init(st, (double)(int)(dt / 1), f.temp, f.pmid, s, uptk0);
-  const bool long_loop = soa_first_rate(st) * st.dtfull > 0.05 * kLongLoopSteps;
+  const double first_rate = soa_first_rate(st) * st.dtfull;
+  if constexpr (FUSE) {
+    // a short loop (first sub-step at least 1/inline_scale of the step)
+    // runs here and the cell finishes without the hand-off, with the same
+    // arithmetic as the solver and post kernels
+    if (first_rate <= 0.05 * a.inline_scale) {
+      while (soa_pass<MIXED ? 1 : 0>(st)) {
+      }
+      if (st.niter > 1000)
+        atomicOr(a.flags, MAM4B_FLAG_SOA_NITER_LIMIT);
+      s.gas[0] = st.g;
+#pragma unroll
+      for (int k = 0; k < NMODE; ++k)
+        s.aer[0][k] = st.a[k];
+      const FinishRegs src{oc, ci, cg, f.ai, f.ac, f.h2so4, f.soag};
+      cell_finish(a, c, f.temp, f.pmid, f.zm, f.cld, f.pblh, rh, f.dgn_a[3], s, cm, src);
+      return;
+    }
+  }
+  const bool long_loop = first_rate > 0.05 * kLongLoopSteps;
   // warp-aggregated appends: the slot (in discovery order, which keeps the
   // post kernel's cell accesses coalesced) and the solver order entry
   const unsigned m = __activemask();
@@ -1130,11 +1178,93 @@ __device__ __forceinline__ void cell_pre(const StepArgs &a, const ChemArgs &ch,
   }
 }
 
-// Second half of a queued cell: the state at the SOA loop (hand-off), the
-// loop's result (solver), the rest of the clear subarea, recombination with
-// the cloudy subarea's contributions, tendencies.
-__device__ __forceinline__ void cell_post(const StepArgs &a, unsigned slot) {
+// Second half of a cell after its SOA loop: the rest of the clear subarea
+// (H2SO4 update, renaming, nucleation, coagulation with the coefficients of
+// pair_kernel, aging), recombination with the cloudy subarea's
+// contributions (ci, cg; partly cloudy cells) and the outgoing cloud-borne
+// grid means oc, tendencies. s holds the clear subarea with the loop's
+// result, cm the values saved before condensation.
+// src supplies the values read late (src.oc(p), ci(p), cg(g), ai(p), ac(p),
+// h2so4(), soag()): from registers in pre's fused path, from the hand-off
+// and the inputs in post_kernel, where reading them only when needed keeps
+// them out of registers during the suffix.
+template <class Src>
+__device__ __forceinline__ void cell_finish(const StepArgs &a, const long long c, double temp,
+                                            double pmid, double zm, double cld, double pblh,
+                                            double relhum, double dgn_pc, Sub &s, ClearMid &cm,
+                                            const Src &src) {
   const StepConsts &C = c_k;
+  const size_t n = (size_t)a.ncell;
+  const double dt = a.dt;
+  // wet sizes enter the suffix only through the coagulation coefficients,
+  // which pair_kernel computed
+  const double unused[NMODE] = {0, 0, 0, 0};
+  clear_suffix<false, true>(a, dt, temp, pmid, zm, pblh, relhum, dgn_pc, unused, unused, cm, s,
+                            nullptr, 0.0, a.aux + AUX_COAG * n + c, n);
+  // recombination (form_gcm_of_gases_and_aerosols_from_subareas)
+  const double fsoag = C.fcvt_soag;
+  double o_h2so4, o_soag, oi[NPOP];
+  double po[NPOP];
+  sub_to_pop(s, po);
+  if (cld < 1.0e-5) {
+    const double f = 1.0 - 0.0;
+    o_soag = dmax(0.0, 0.0 + (s.gas[0] / fsoag) * f);
+    o_h2so4 = dmax(0.0, 0.0 + (s.gas[1] / 1.0) * f);
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      oi[K::numslot(m)] = dmax(0.0, 0.0 + (po[K::numslot(m)] / 1.0) * f);
+#pragma unroll
+      for (int x = 0; x < NAER; ++x) {
+        const int sl = K::aer_slot(x, m);
+        if (sl >= 0)
+          oi[sl] = dmax(0.0, 0.0 + (po[sl] / K::fcvt_aer(x)) * f);
+      }
+    }
+  } else {
+    const double fclea = 1.0 - cld;
+    o_soag = dmax(0.0, (0.0 + (s.gas[0] / fsoag) * fclea) + src.cg(0));
+    o_h2so4 = dmax(0.0, (0.0 + (s.gas[1] / 1.0) * fclea) + src.cg(1));
+#pragma unroll
+    for (int m = 0; m < NMODE; ++m) {
+      oi[K::numslot(m)] =
+          dmax(0.0, (0.0 + (po[K::numslot(m)] / 1.0) * fclea) + src.ci(K::numslot(m)));
+#pragma unroll
+      for (int x = 0; x < NAER; ++x) {
+        const int sl = K::aer_slot(x, m);
+        if (sl >= 0)
+          oi[sl] = dmax(0.0, (0.0 + (po[sl] / K::fcvt_aer(x)) * fclea) + src.ci(sl));
+      }
+    }
+  }
+  double oc[NPOP], ai[NPOP], ac[NPOP];
+#pragma unroll
+  for (int p = 0; p < NPOP; ++p) {
+    oc[p] = src.oc(p);
+    ai[p] = src.ai(p);
+    ac[p] = src.ac(p);
+  }
+  store_outputs(a, c, o_h2so4, o_soag, oi, oc, src.h2so4(), src.soag(), ai, ac);
+}
+
+// cell_finish's late inputs read from the hand-off of queue slot `slot`
+// and the cell's inputs (post_kernel)
+struct FinishLoads {
+  const StepArgs &a;
+  long long c;
+  const double *h;
+  size_t n;
+  __device__ double oc(int p) const { return h[(H_OC + p) * n]; }
+  __device__ double ci(int p) const { return h[(H_CI + p) * n]; }
+  __device__ double cg(int g) const { return h[(H_CG + g) * n]; }
+  __device__ double ai(int p) const { return __ldg(a.in[MAM4B_IN_AER_I + p] + c); }
+  __device__ double ac(int p) const { return __ldg(a.in[MAM4B_IN_AER_C + p] + c); }
+  __device__ double h2so4() const { return __ldg(a.in[MAM4B_IN_H2SO4] + c); }
+  __device__ double soag() const { return __ldg(a.in[MAM4B_IN_SOAG] + c); }
+};
+
+// Second half of a queued cell: the state at the SOA loop (hand-off), the
+// loop's result (solver), then cell_finish.
+__device__ __forceinline__ void cell_post(const StepArgs &a, unsigned slot) {
   const size_t n = (size_t)a.ncell;
   const long long c = a.task[slot];
   const double temp = __ldg(a.in[MAM4B_IN_T] + c);
@@ -1142,7 +1272,6 @@ __device__ __forceinline__ void cell_post(const StepArgs &a, unsigned slot) {
   const double zm = __ldg(a.in[MAM4B_IN_ZM] + c);
   const double cld = __ldg(a.in[MAM4B_IN_CLD] + c);
   const double pblh = __ldg(a.pblh + c / a.nlev);
-  const double dt = a.dt;
   const double *h = a.hand + slot;
   const double *q = a.soa + slot;
   Sub s;
@@ -1162,60 +1291,11 @@ __device__ __forceinline__ void cell_post(const StepArgs &a, unsigned slot) {
   cm.netprod1 = h[H_NETPROD * n];
   cm.sv_so4_ait = h[H_SV_SO4 * n];
   cm.sv_soa_ait = h[H_SV_SOA * n];
-  // wet sizes enter the suffix only through the coagulation coefficients,
-  // which pair_kernel computed
-  const double unused[NMODE] = {0, 0, 0, 0};
 #pragma unroll
   for (int k = 0; k < NMODE; ++k)
     cm.uptk1[k] = h[(H_UPTK + k) * n];
-  clear_suffix<false, true>(a, dt, temp, pmid, zm, pblh, h[H_RELHUM * n], h[H_DGN_PC * n], unused,
-                            unused, cm, s, nullptr, 0.0, a.aux + AUX_COAG * n + c, n);
-  // recombination (form_gcm_of_gases_and_aerosols_from_subareas)
-  const double fsoag = C.fcvt_soag;
-  double o_h2so4, o_soag, oi[NPOP], oc[NPOP];
-#pragma unroll
-  for (int p = 0; p < NPOP; ++p)
-    oc[p] = h[(H_OC + p) * n];
-  double po[NPOP];
-  sub_to_pop(s, po);
-  if (cld < 1.0e-5) {
-    const double f = 1.0 - 0.0;
-    o_soag = dmax(0.0, 0.0 + (s.gas[0] / fsoag) * f);
-    o_h2so4 = dmax(0.0, 0.0 + (s.gas[1] / 1.0) * f);
-#pragma unroll
-    for (int m = 0; m < NMODE; ++m) {
-      oi[K::numslot(m)] = dmax(0.0, 0.0 + (po[K::numslot(m)] / 1.0) * f);
-#pragma unroll
-      for (int x = 0; x < NAER; ++x) {
-        const int sl = K::aer_slot(x, m);
-        if (sl >= 0)
-          oi[sl] = dmax(0.0, 0.0 + (po[sl] / K::fcvt_aer(x)) * f);
-      }
-    }
-  } else {
-    const double fclea = 1.0 - cld;
-    o_soag = dmax(0.0, (0.0 + (s.gas[0] / fsoag) * fclea) + h[H_CG * n]);
-    o_h2so4 = dmax(0.0, (0.0 + (s.gas[1] / 1.0) * fclea) + h[(H_CG + 1) * n]);
-#pragma unroll
-    for (int m = 0; m < NMODE; ++m) {
-      oi[K::numslot(m)] = dmax(0.0, (0.0 + (po[K::numslot(m)] / 1.0) * fclea) +
-                                        h[(H_CI + K::numslot(m)) * n]);
-#pragma unroll
-      for (int x = 0; x < NAER; ++x) {
-        const int sl = K::aer_slot(x, m);
-        if (sl >= 0)
-          oi[sl] = dmax(0.0, (0.0 + (po[sl] / K::fcvt_aer(x)) * fclea) + h[(H_CI + sl) * n]);
-      }
-    }
-  }
-  double ai[NPOP], ac[NPOP];
-#pragma unroll
-  for (int p = 0; p < NPOP; ++p) {
-    ai[p] = __ldg(a.in[MAM4B_IN_AER_I + p] + c);
-    ac[p] = __ldg(a.in[MAM4B_IN_AER_C + p] + c);
-  }
-  store_outputs(a, c, o_h2so4, o_soag, oi, oc, __ldg(a.in[MAM4B_IN_H2SO4] + c),
-                __ldg(a.in[MAM4B_IN_SOAG] + c), ai, ac);
+  const FinishLoads src{a, c, h, n};
+  cell_finish(a, c, temp, pmid, zm, cld, pblh, h[H_RELHUM * n], h[H_DGN_PC * n], s, cm, src);
 }
 
 template <bool DIAG>
@@ -1453,18 +1533,13 @@ __global__ void pair_kernel(const __grid_constant__ StepArgs a) {
   cc[(9 + p) * n] = bjj0;
 }
 
-template <int R, bool MIXED, bool LOOP>
+// FUSE: cells with short SOA loops finish here (StepArgs::inline_scale)
+template <int R, bool MIXED, bool FUSE>
 __global__ void __maxnreg__(R) pre_kernel(const __grid_constant__ StepArgs a) {
   const ChemArgs none = {nullptr, nullptr, 0};
-  const long long c0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if constexpr (LOOP) {
-    const long long stride = (long long)gridDim.x * blockDim.x;
-#pragma unroll 1
-    for (long long c = c0; c < a.ncell; c += stride)
-      cell_pre<false, MIXED>(a, none, c);
-  } else if (c0 < a.ncell) {
-    cell_pre<false, MIXED>(a, none, c0);
-  }
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < a.ncell)
+    cell_pre<false, MIXED, FUSE>(a, none, c);
 }
 
 // The pre stage of the step with chemistry (mam4b_step_chem_slab).
@@ -3189,7 +3264,9 @@ bool valid_tuning(const mam4b_tuning &t) {
          (t.soa_block == 128 || t.soa_block == 256) &&
          (long long)t.soa_block * t.soa_regs <= 65536 && t.soa_blocks_per_sm >= 1 &&
          t.soa_blocks_per_sm <= 16 &&
-         (t.cells_per_thread == 1 || t.cells_per_thread == 2 || t.cells_per_thread == 4);
+         (t.cells_per_thread == 1 || t.cells_per_thread == 2 || t.cells_per_thread == 4) &&
+         (t.inline_scale == 0 || t.inline_scale == 1 || t.inline_scale == 4 ||
+          t.inline_scale == 16 || t.inline_scale == 64);
 }
 
 unsigned grid_for(long long n, int block, int cpt) {
@@ -3229,22 +3306,23 @@ void launch_pair(const mam4b_tuning &t, const StepArgs &a, cudaStream_t s, bool 
   else
     pair_kernel<false><<<g, t.pair_block, 0, s>>>(a);
 }
-template <bool MIXED, bool LOOP>
+template <bool MIXED, bool FUSE>
 void launch_pre_t(const mam4b_tuning &t, const StepArgs &a, cudaStream_t s) {
-  const unsigned g = grid_for(a.ncell, t.pre_block, t.cells_per_thread);
+  const unsigned g = grid_for(a.ncell, t.pre_block, 1);
   if (t.pre_regs == 128)
-    pre_kernel<128, MIXED, LOOP><<<g, t.pre_block, 0, s>>>(a);
+    pre_kernel<128, MIXED, FUSE><<<g, t.pre_block, 0, s>>>(a);
   else if (t.pre_regs == 168)
-    pre_kernel<168, MIXED, LOOP><<<g, t.pre_block, 0, s>>>(a);
+    pre_kernel<168, MIXED, FUSE><<<g, t.pre_block, 0, s>>>(a);
   else
-    pre_kernel<255, MIXED, LOOP><<<g, t.pre_block, 0, s>>>(a);
+    pre_kernel<255, MIXED, FUSE><<<g, t.pre_block, 0, s>>>(a);
 }
-void launch_pre(const mam4b_tuning &t, const StepArgs &a, cudaStream_t s, bool mixed = false) {
-  const bool loop = t.cells_per_thread > 1;
+// fuse: cells with short SOA loops finish in pre (a.inline_scale > 0)
+void launch_pre(const mam4b_tuning &t, const StepArgs &a, cudaStream_t s, bool mixed = false,
+                bool fuse = false) {
   if (mixed)
-    loop ? launch_pre_t<true, true>(t, a, s) : launch_pre_t<true, false>(t, a, s);
+    fuse ? launch_pre_t<true, true>(t, a, s) : launch_pre_t<true, false>(t, a, s);
   else
-    loop ? launch_pre_t<false, true>(t, a, s) : launch_pre_t<false, false>(t, a, s);
+    fuse ? launch_pre_t<false, true>(t, a, s) : launch_pre_t<false, false>(t, a, s);
 }
 template <int SOA>
 void launch_soa_t(const mam4b_tuning &t, int sms, const StepArgs &a, cudaStream_t s) {
@@ -3294,6 +3372,10 @@ cudaError_t launch_pipeline_t(const mam4b_tuning &t, int sms, const StepArgs &a_
                               std::atomic<unsigned long long> *launches) {
   StepArgs a = a_in;
   a.mixed = precision != MAM4B_FP64;
+  // short SOA loops finish in pre unless the adjoint needs every loop's
+  // pass count (npass) or the loop runs in FP32 (MIXED_FAST)
+  const bool fuse = t.inline_scale > 0 && !a.npass && precision != MAM4B_MIXED_FAST;
+  a.inline_scale = fuse ? (double)t.inline_scale : 0.0;
   cudaError_t e = cudaMemsetAsync(a.counters, 0, CNT_WORDS * sizeof(unsigned), s);
   if (e != cudaSuccess)
     return e;
@@ -3326,7 +3408,7 @@ cudaError_t launch_pipeline_t(const mam4b_tuning &t, int sms, const StepArgs &a_
     const int block = 128;
     pre_chem_kernel<<<(unsigned)((a.ncell + block - 1) / block), block, 0, s>>>(a, *ch);
   } else {
-    launch_pre(t, a, s, mixed);
+    launch_pre(t, a, s, mixed, fuse);
   }
   mark(4);
   launch_soa(t, sms, a, s, precision);
@@ -3496,11 +3578,11 @@ cudaError_t noalloc_setup(int dev) {
 const char *const kTuningKeys[] = {"size_block", "size_regs", "mode_block", "pair_block",
                                    "pre_block", "pre_regs", "post_block", "post_regs",
                                    "soa_block", "soa_regs", "soa_blocks_per_sm",
-                                   "cells_per_thread"};
+                                   "cells_per_thread", "inline_scale"};
 int *tuning_field(mam4b_tuning &t, int k) {
   int *f[] = {&t.size_block, &t.size_regs, &t.mode_block, &t.pair_block, &t.pre_block,
               &t.pre_regs, &t.post_block, &t.post_regs, &t.soa_block, &t.soa_regs,
-              &t.soa_blocks_per_sm, &t.cells_per_thread};
+              &t.soa_blocks_per_sm, &t.cells_per_thread, &t.inline_scale};
   return f[k];
 }
 
@@ -3615,6 +3697,7 @@ void mam4b_default_tuning(mam4b_tuning *t) {
   t->soa_regs = 64;
   t->soa_blocks_per_sm = 4;
   t->cells_per_thread = 1;
+  t->inline_scale = 0;
 }
 
 mam4b_status mam4b_tuning_from_json(const char *path, mam4b_tuning *t, char *device,
@@ -3989,6 +4072,19 @@ mam4b_status mam4b_autotune(mam4b_ctx *ctx, const double *in_slab, const double 
     if (e == cudaSuccess && ms < t_best) {
       t_best = ms;
       b.cells_per_thread = cpt;
+    }
+  }
+  // short SOA loops finished in pre: changes the work of pre, soa and post
+  // together, so it is chosen on the whole step
+  for (int sc : {1, 4, 16, 64}) {
+    mam4b_tuning t = b;
+    t.inline_scale = sc;
+    float ms = 1e30f;
+    if (e == cudaSuccess)
+      e = total_of(t, ms);
+    if (e == cudaSuccess && ms < t_best) {
+      t_best = ms;
+      b.inline_scale = sc;
     }
   }
   float t_def = 1e30f;

@@ -83,7 +83,7 @@ class Tuning(ctypes.Structure):
     _fields_ = [(k, ctypes.c_int) for k in (
         "size_block", "size_regs", "mode_block", "pair_block", "pre_block", "pre_regs",
         "post_block", "post_regs", "soa_block", "soa_regs", "soa_blocks_per_sm",
-        "cells_per_thread")]
+        "cells_per_thread", "inline_scale")]
 
     def as_dict(self):
         return {k: int(getattr(self, k)) for k, _ in self._fields_}

@@ -39,7 +39,7 @@ def _shapes():
                     ("pair_block", (64, 256)), ("pre_regs", (168, 128)), ("pre_block", (64, 256)),
                     ("post_regs", (255, 168)), ("post_block", (64, 256)),
                     ("soa_regs", (96, 128)), ("soa_block", (128,)), ("soa_blocks_per_sm", (1, 2)),
-                    ("cells_per_thread", (2, 4))):
+                    ("cells_per_thread", (2, 4)), ("inline_scale", (1, 4, 16, 64))):
         for v in vals:
             t = dict(d)
             t[k] = v
@@ -63,11 +63,15 @@ def test_every_launch_shape_is_bitwise_equal(cuda_device, name, ncol):
         ctx.set_tuning(t)
         got = _step(ctx, w, x, pb)
         assert np.array_equal(got, ref), shape
-    # mixed precision through a non-default shape
+    # mixed precision through non-default shapes (the last ones finish
+    # short SOA loops inside pre)
     ctx.set_tuning(native.default_tuning())
     mref = _step(ctx, w, x, pb, native.MIXED)
-    ctx.set_tuning(native.Tuning(**_shapes()[-1]))
-    assert np.array_equal(_step(ctx, w, x, pb, native.MIXED), mref)
+    fref = _step(ctx, w, x, pb, native.MIXED_FAST)
+    for shape in _shapes()[-3:]:
+        ctx.set_tuning(native.Tuning(**shape))
+        assert np.array_equal(_step(ctx, w, x, pb, native.MIXED), mref), shape
+        assert np.array_equal(_step(ctx, w, x, pb, native.MIXED_FAST), fref), shape
     ctx.close()
 
 

@@ -72,13 +72,15 @@ def test_tuning_file_round_trip_and_validation(tmp_path):
         t, dev = native.tuning_from_json(committed)
         assert dev and t.as_dict() == {k: json.load(open(committed))[k] for k in t.as_dict()}
     d = native.default_tuning().as_dict()
-    d.update(pre_regs=168, post_block=64, soa_blocks_per_sm=3, cells_per_thread=2)
+    d.update(pre_regs=168, post_block=64, soa_blocks_per_sm=3, cells_per_thread=2,
+             inline_scale=16)
     p = tmp_path / "t.json"
     p.write_text(json.dumps(dict(d, device="NVIDIA B200", chosen_on={"tuned_ms": 1.0})))
     t, dev = native.tuning_from_json(str(p))
     assert t.as_dict() == d and dev == "NVIDIA B200"
     for bad in (dict(d, pre_regs=200), dict(d, size_block=512), dict(d, soa_blocks_per_sm=0),
-                dict(d, cells_per_thread=3), {k: v for k, v in d.items() if k != "soa_regs"}):
+                dict(d, cells_per_thread=3), dict(d, inline_scale=8),
+                {k: v for k, v in d.items() if k != "soa_regs"}):
         p.write_text(json.dumps(bad))
         with pytest.raises(native.MicrophysicsError):
             native.tuning_from_json(str(p))
