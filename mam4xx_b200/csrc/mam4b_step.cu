@@ -3413,11 +3413,15 @@ cudaError_t launch_pipeline_t(const mam4b_tuning &t, int sms, const StepArgs &a_
   mark(4);
   launch_soa(t, sms, a, s, precision);
   mark(5);
-  launch_post(t, a, s);
+  // the adjoint's forward (npass set) has no post stage: adj_post_kernel
+  // recomputes the suffix from the hand-off, and the forward's outputs are
+  // not returned
+  if (!a.npass)
+    launch_post(t, a, s);
   mark(6);
   e = cudaGetLastError();
   if (e == cudaSuccess && launches)
-    *launches += 6;
+    *launches += a.npass ? 5 : 6;
   return e;
 }
 

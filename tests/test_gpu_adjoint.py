@@ -65,7 +65,46 @@ def objective_bar(wts, dt, n):
     return ybar
 
 
-def test_adjoint_against_finite_differences(cuda_device):
+def _fd_entries(J, x, g, J0, cells, fields, h_rel=1e-6):
+    """Central and one-sided differences of the per-cell objective J(x)
+    (a function of the whole input slab) for every (field, cell); returns
+    arrays of (field, cell, err_central, err_left, err_right, kink) in units
+    of |g - fd| |x| / |J0|, kink = |fd_left - fd_right| |x| / |J0|."""
+    rows = []
+    Jx = J(x)
+    for f in fields:
+        h = h_rel * np.abs(x[f])
+        xp = x.copy()
+        xm = x.copy()
+        xp[f] += h
+        xm[f] -= h
+        Jp, Jm = J(xp), J(xm)
+        hs = np.where(h > 0, h, 1.0)
+        fd_c = (Jp - Jm) / (2 * hs)
+        fd_r = (Jp - Jx) / hs
+        fd_l = (Jx - Jm) / hs
+        for c in cells:
+            if x[f, c] == 0.0:
+                continue
+            sc = abs(x[f, c]) / abs(J0[c])
+            rows.append((f, c, abs(g[f, c] - fd_c[c]) * sc, abs(g[f, c] - fd_l[c]) * sc,
+                         abs(g[f, c] - fd_r[c]) * sc, abs(fd_l[c] - fd_r[c]) * sc))
+    return np.array(rows)
+
+
+def test_adjoint_against_finite_differences(cuda_device, port_oracle):
+    """Central differences of the GPU forward at relative step 1e-6 on 64
+    cells. Entries that miss 1e-6 are of two kinds:
+      * branch straddles: the forward is not differentiable inside
+        [x - h, x + h], shown per entry by a different SOA sub-step count at
+        x - h and x + h (counted on the CPU restatement) or by a kink (the
+        one-sided differences disagree by more than 1e-5); the adjoint then
+        matches the one-sided difference of one side (the derivative of a
+        branch the forward takes next to x);
+      * smooth disagreements (both one-sided differences agree with the
+        central one but not with the adjoint): a known inaccuracy of the
+        temperature derivative through renaming in partly cloudy cells,
+        bounded here at 1e-4 and 0.1 % of the entries."""
     w = make_workload("c5", ncol=32, seed=5150)
     x = w["in_slab"]
     n = x.shape[1]
@@ -78,30 +117,69 @@ def test_adjoint_against_finite_differences(cuda_device):
         g[5 + k] += wts  # the state itself enters J (after = before + tend dt)
     rng = np.random.default_rng(64)
     cells = rng.choice(n, 64, replace=False)
-    errs = []
-    for f in DIFF_FIELDS:
-        h = 1e-6 * np.abs(x[f])
-        xp = x.copy()
-        xm = x.copy()
-        xp[f] += h
-        xm[f] -= h
-        fd = (objective_cells(xp, forward(ctx, xp, w["pblh"], w), wts, w["dt"]) -
-              objective_cells(xm, forward(ctx, xm, w["pblh"], w), wts, w["dt"])) / np.where(h > 0, 2 * h, 1.0)
-        for c in cells:
-            if x[f, c] == 0.0:
-                continue
-            errs.append(abs(g[f, c] - fd[c]) * abs(x[f, c]) / abs(J0[c]))
-    errs = np.array(errs)
-    summary = {"entries": errs.size, "median": float(np.median(errs)),
+
+    def J(xv):
+        return objective_cells(xv, forward(ctx, xv, w["pblh"], w), wts, w["dt"])
+
+    rows = _fd_entries(J, x, g, J0, cells, DIFF_FIELDS)
+    errs = rows[:, 2]
+    summary = {"entries": int(errs.size), "median": float(np.median(errs)),
                "q999": float(np.quantile(errs, 0.999)), "max": float(errs.max()),
                "within_1e-6": float((errs <= 1e-6).mean())}
     assert errs.size > 3000
-    # a central difference that straddles a branch of the forward (an SOA
-    # sub-step count, a clip) is not a derivative; those rare entries are
-    # bounded by the step itself
     assert summary["median"] <= 1e-9, summary
     assert summary["within_1e-6"] >= 0.997, summary
-    assert summary["max"] <= 1e-3, summary
+    pb_cell = pblh_per_cell(w)
+    straddles, smooth = [], []
+    for f, c, ec, el, er, kink in rows[errs > 1e-6]:
+        f, c = int(f), int(c)
+        h = 1e-6 * abs(x[f, c])
+        xs = x[:, [c]].copy()
+        xp, xm = xs.copy(), xs.copy()
+        xp[f] += h
+        xm[f] -= h
+        np_, nm_ = (int(port_oracle.soa_niter(v, pb_cell[[c]], w["dt"])[0]) for v in (xp, xm))
+        if np_ != nm_ or kink > 1e-5:
+            assert min(el, er) <= 1e-5, ("straddle without a matching side", f, c, ec, el, er)
+            straddles.append((f, c))
+        else:
+            smooth.append((f, c, ec))
+    print("FD", summary, "straddles", len(straddles), "smooth", smooth)
+    assert len(smooth) <= 0.001 * errs.size, smooth
+    assert all(e <= 1e-4 for _, _, e in smooth), smooth
+
+
+def test_adjoint_against_reference_forward_differences(cuda_device, ref_oracle):
+    """The gradient of the FP64 reference forward itself (the mam4xx headers
+    compiled for the host): central differences of the reference build's
+    step on 16 cells agree with the adjoint to 1e-6 on 99 % of entries; the
+    rest differ by at most what the libm spread between the two builds makes
+    of a 1e-6 step."""
+    w = make_workload("c5", ncol=8, seed=5151)
+    x = w["in_slab"]
+    n = x.shape[1]
+    wts = pdel_over_g(w)
+    ctx = native.Context()
+    pbc = pblh_per_cell(w)
+    rng = np.random.default_rng(65)
+    cells = np.sort(rng.choice(n, 16, replace=False))
+    out = forward(ctx, x, w["pblh"], w)
+    J0 = objective_cells(x, out, wts, w["dt"])
+    g = adjoint(ctx, x, w["pblh"], objective_bar(wts, w["dt"], n), w)
+    for k in J_STATE:
+        g[5 + k] += wts
+
+    def J(xv):
+        # only the chosen cells are stepped on the host
+        o = np.zeros((native.NOUT, n))
+        o[:, cells] = ref_oracle.step(xv[:, cells], pbc[cells], w["dt"])
+        return objective_cells(xv, o, wts, w["dt"])
+
+    rows = _fd_entries(J, x, g, J0, cells, DIFF_FIELDS)
+    errs = rows[:, 2]
+    assert errs.size > 700
+    assert float((errs <= 1e-6).mean()) >= 0.99, float((errs <= 1e-6).mean())
+    assert float(np.median(errs)) <= 1e-8
 
 
 def test_adjoint_fixed_rows_and_determinism(cuda_device):
