@@ -501,9 +501,26 @@ def adjoint_leg(native, torch, dev, stream, args, ws):
         actx.adjoint_slab(xa.data_ptr(), pba.data_ptr(), ybar.data_ptr(), xbar.data_ptr(), na,
                           wa["ncol"], wa["nlev"], wa["dt"], stream=stream.cuda_stream)
 
+    def adj_ck4():
+        actx.set_adjoint_checkpoint(4)
+        adj()
+
+    xbar_mx = torch.empty_like(xbar)
+
+    def fwd_mixed():
+        actx.step_slab(xa.data_ptr(), pba.data_ptr(), outa.data_ptr(), na, wa["ncol"], wa["nlev"],
+                       wa["dt"], precision=native.MIXED, stream=stream.cuda_stream)
+
+    def adj_mixed():
+        actx.adjoint_slab(xa.data_ptr(), pba.data_ptr(), ybar.data_ptr(), xbar_mx.data_ptr(), na,
+                          wa["ncol"], wa["nlev"], wa["dt"], stream=stream.cuda_stream,
+                          precision=native.MIXED)
+
     times = {}
     ka = max(2, min(args.steps, 5))
-    for name, f in (("forward", fwd), ("adjoint", adj)):
+    for name, f in (("forward", fwd), ("forward_mixed", fwd_mixed), ("adjoint_mixed", adj_mixed),
+                    ("adjoint_ck4", adj_ck4), ("adjoint", adj)):
+        actx.set_adjoint_checkpoint(1)
         for _ in range(args.warmup):
             f()
         if ws > 1:
@@ -518,6 +535,29 @@ def adjoint_leg(native, torch, dev, stream, args, ws):
         e1.record(stream)
         torch.cuda.synchronize()
         times[name] = e0.elapsed_time(e1) / ka
+    # the mixed-precision adjoint's gradient against the FP64 one, per
+    # entry in units of relative sensitivity |g_mixed - g| |x| / |J_cell|
+    fwd()
+    torch.cuda.synchronize()
+    jcell = torch.from_numpy(wts).to(dev) * sum(xa[5 + k] + outa[k] * wa["dt"] for k in jstate)
+    gfull = xbar.clone()
+    gmix = xbar_mx.clone()
+    for k in jstate:
+        gfull[5 + k] += torch.from_numpy(wts).to(dev)
+        gmix[5 + k] += torch.from_numpy(wts).to(dev)
+    rows = [0, 3, 5, 6] + list(range(7, 57))
+    emx = ((gmix[rows] - gfull[rows]).abs() * xa[rows].abs() / jcell.abs().clamp(min=1e-300))
+    emx = emx.flatten()
+    samp = emx[torch.randperm(emx.numel(), generator=torch.Generator().manual_seed(7))[:1 << 20]
+               .to(dev)]
+    qs = torch.quantile(samp, torch.tensor([0.999, 0.9999], dtype=samp.dtype, device=dev))
+    mixed_vs_fp64 = {"entries": int(emx.numel()), "units": "|g_mixed - g_fp64| |x| / |J_cell|",
+                     "median": float(samp.median()), "q999": float(qs[0]),
+                     "q9999": float(qs[1]), "entries_above_1": int((emx > 1.0).sum()),
+                     "max": float(emx.max()),
+                     "within_1e-6": float((emx <= 1e-6).double().mean()),
+                     "within_1e-5": float((emx <= 1e-5).double().mean())}
+    del gfull, gmix, emx, samp
     # finite-difference check on 64 cells (first 8 columns x 8 levels)
     g = xbar.cpu().numpy()
     x_h = wa["in_slab"]
@@ -565,6 +605,15 @@ def adjoint_leg(native, torch, dev, stream, args, ws):
                          "weights pdel/g; gradient w.r.t. T, qv, H2SO4, SOAG, 50 populations",
             "forward_ms": times["forward"], "adjoint_ms": times["adjoint"],
             "adjoint_over_forward": times["adjoint"] / times["forward"],
+            "adjoint_ck4_ms": times["adjoint_ck4"],
+            "mixed": {"forward_ms": times["forward_mixed"], "adjoint_ms": times["adjoint_mixed"],
+                      "adjoint_over_forward": times["adjoint_mixed"] / times["forward_mixed"],
+                      "adjoint_vs_fp64_adjoint": times["adjoint_mixed"] / times["adjoint"],
+                      "gradient_vs_fp64": mixed_vs_fp64},
+            "adjoint_ck4_over_forward": times["adjoint_ck4"] / times["forward"],
+            "soa_states": "stored before every sub-step (adjoint_ms; 3.64 GB on 148 SMs) or a "
+                          "checkpoint every 4 sub-steps with the others recomputed "
+                          "(adjoint_ck4_ms; 0.93 GB); same gradient",
             "fd_check": {"cells": 64, "entries": int(errs.size), "rel_step": 1e-6,
                          "units": "|g - fd| |x| / |J_cell|",
                          "median": float(np.median(errs)), "max": float(errs.max()),
@@ -630,7 +679,7 @@ def mixed_leg(native, torch, dev, stream, args, ws, rank):
     the same resident inputs; every cell's error against this run's FP64
     result (mam4xx_b200.precision.error_report_device)."""
     from mam4xx_b200.distributed import EventClock, max_over_ranks, timed_steps
-    from mam4xx_b200.precision import error_report_device
+    from mam4xx_b200.precision import cell_errors_device, conditioning_split, error_report_device
     from mam4xx_b200.workloads import make_workload
     wm = make_workload("c3", ncol=args.ncol, seed=20261203 + 2 + 1000 * rank)
     xm = torch.from_numpy(wm["in_slab"]).to(dev)
@@ -668,9 +717,22 @@ def mixed_leg(native, torch, dev, stream, args, ws, rank):
                 pert[lab] = {"cells_within_1e-5": rq["cells_within_tol"], "max": rq["max"],
                              "cell_err_quantiles": rq["cell_err_quantiles"]}
                 del xq
+            # per cell: the FP64 step for its inputs rounded to single
+            # precision against the FP64 step for the exact inputs
+            xq = xm.float().double()
+            ctx.step_slab(xq.data_ptr(), pbm.data_ptr(), got.data_ptr(), nm, wm["ncol"], NLEV,
+                          wm["dt"], precision=native.FP64, stream=stream.cuda_stream)
+            torch.cuda.synchronize()
+            del xq
+            cond = cell_errors_device(got, ref, xm, wm["dt"])
+            rq = error_report_device(got, ref, xm, wm["dt"], tol=1e-5)
+            pert["fp32_rounded_inputs"] = {"cells_within_1e-5": rq["cells_within_tol"],
+                                           "max": rq["max"],
+                                           "cell_err_quantiles": rq["cell_err_quantiles"]}
             res["fp64_input_perturbation"] = pert
             f()  # the mixed results again, for the report below
             torch.cuda.synchronize()
+        split = conditioning_split(cell_errors_device(got, ref, xm, wm["dt"]), cond, tol=1e-5)
         worst = sorted(range(native.NOUT), key=lambda k: -r["per_output_max"][k])[:6]
         res[name] = {"value": ws * nm / (times[name] * 1e-3), "unit": "cells/s",
                      "ms_per_step": times[name],
@@ -679,6 +741,7 @@ def mixed_leg(native, torch, dev, stream, args, ws, rank):
                                      "cells_within_1e-5": r["cells_within_tol"],
                                      "cells_outside_1e-5": r["cells_outside_tol"],
                                      "cell_err_quantiles": r["cell_err_quantiles"],
+                                     "conditioning": split,
                                      "worst_outputs": {str(k): r["per_output_max"][k] for k in worst},
                                      "per_output_max": r["per_output_max"],
                                      "per_output_median": r["per_output_median"]}}
@@ -837,9 +900,28 @@ def main():
     alg_bytes = n * BYTES_PER_CELL + ncol * 8
     achieved = alg_bytes / (kernel_ms * 1e-3) / 1e9
     traffic = _traffic_per_launch(WORKLOAD, n)
+    # the other legs' key figures, first in the line (the full reports go last)
+    legs = {}
+    if precisions:
+        for k in ("mixed", "mixed_fast"):
+            if k in precisions:
+                e = precisions[k]["err_vs_fp64"]
+                legs[k] = {"speedup_vs_fp64": round(precisions[k]["speedup_vs_fp64"], 3),
+                           "cells_within_1e-5": round(e["cells_within_1e-5"], 5),
+                           "well_conditioned_within_1e-5":
+                               round(e["conditioning"]["well_conditioned_within_tol"], 6)}
+    if adjoint:
+        legs["adjoint"] = {k: round(adjoint[k], 3) for k in
+                           ("adjoint_over_forward", "adjoint_ck4_over_forward") if k in adjoint}
+        legs["adjoint"]["fd_within_1e-6"] = round(adjoint["fd_check"]["within_1e-6"], 5)
+        if "mixed" in adjoint:
+            legs["adjoint"]["mixed_over_fp64_adjoint"] = round(
+                adjoint["mixed"]["adjoint_vs_fp64_adjoint"], 3)
+            legs["adjoint"]["mixed_gradient_within_1e-5"] = round(
+                adjoint["mixed"]["gradient_vs_fp64"]["within_1e-5"], 5)
     line = {
         "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": ws, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "legs": legs, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded draws with the configuration's distributions)",
         "config": {"workload": _workload_name(ncol),

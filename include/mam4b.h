@@ -374,14 +374,44 @@ mam4b_status mam4b_step_slab_noalloc(const mam4b_config *cfg, const double *in_s
  * zero (these are held fixed), and the boundary-layer height has no
  * cotangent. The derivative is that of the branch the forward takes at the
  * given state (max/min clips, process thresholds and the SOA sub-step count
- * are not differentiated across). With condensation on, the SOA loop's
- * state is stored before every sub-step; without it, states are recomputed
- * from checkpoints kept every 4 sub-steps. Uses the context's config;
- * asynchronous on `stream`. Device pointers.
+ * are not differentiated across). With condensation on, the SOA loops are
+ * reversed by a persistent kernel whose threads keep the loop state (6
+ * doubles) before every sub-step (the default) or only a checkpoint every
+ * 4 sub-steps, recomputing each block of 4 from its checkpoint
+ * (mam4b_set_adjoint_checkpoint). Memory of those states, allocated on
+ * the first call and kept by the context: 6 x 1,001 doubles per thread
+ * (every sub-step) or 6 x 255 (every 4), for SMs x 2 x 256 threads; on a
+ * 148-SM B200, 3.64 GB or 0.93 GB, whatever the batch size. Without
+ * condensation, one thread per cell recomputes from checkpoints every 4
+ * sub-steps. Uses the context's config; asynchronous on `stream`. Device
+ * pointers.
  */
 mam4b_status mam4b_adjoint_slab(mam4b_ctx *ctx, const double *in_slab, const double *pblh,
                                 const double *out_bar, double *in_bar, size_t ld, int ncol,
                                 int nlev, double dt, void *stream);
+
+/*
+ * The adjoint of one precision form of the step (no counterpart in the
+ * reference): MAM4B_FP64 is mam4b_adjoint_slab. MAM4B_MIXED (condensation
+ * on) runs the forward sweep as the MAM4B_MIXED step does (single-precision
+ * water uptake, uptake and coagulation coefficients; the SOA loop in double
+ * precision with approximate reciprocals and fused multiply-adds) and
+ * reverses its SOA loops with the same arithmetic; every other reverse
+ * process is the FP64 one. Its gradient is that of the MAM4B_MIXED step up
+ * to rounding. MAM4B_MIXED_FAST: MAM4B_ERR_NOT_SUPPORTED.
+ */
+mam4b_status mam4b_adjoint_slab_ex(mam4b_ctx *ctx, const double *in_slab, const double *pblh,
+                                   const double *out_bar, double *in_bar, size_t ld, int ncol,
+                                   int nlev, double dt, int precision, void *stream);
+
+/*
+ * SOA sub-step states of the adjoint (no counterpart in the reference):
+ * interval 1 stores the state before every sub-step (fastest), interval 4
+ * keeps a checkpoint every 4 sub-steps and recomputes the others in the
+ * reverse sweep (a quarter of the memory, more arithmetic). The gradient
+ * is the same bit for bit. MAM4B_ERR_INVALID_ARGUMENT for other intervals.
+ */
+mam4b_status mam4b_set_adjoint_checkpoint(mam4b_ctx *ctx, int interval);
 
 /*
  * Step on tracer arrays (E3SM state_q tracer order, the layout of

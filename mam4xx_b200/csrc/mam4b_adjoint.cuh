@@ -16,6 +16,7 @@
 #pragma once
 
 #include "mam4b_physics.cuh"
+#include "mam4b_physics_mixed.cuh"
 
 namespace mam4b {
 namespace adj {
@@ -1310,7 +1311,31 @@ struct SoaBar {
   double opoa[NMODE], uptk[NMODE], g0;
 };
 
-MAM4B_HD void soa_step_rev(const SoaState &st, SoaBar &b) {
+// x / d (FP64 arithmetic of the step), or x * mx::rcp(d) with FAST (the
+// mixed-precision loop's arithmetic, f32::soa_step_mx); on the host always
+// x / d.
+template <bool FAST>
+MAM4B_HD double qdiv(double x, double d) {
+#ifdef __CUDA_ARCH__
+  if constexpr (FAST)
+    return x * f32::mx::rcp(d);
+#endif
+  return x / d;
+}
+// x * y + z, rounded once with FAST, twice (as the FP64 step) without
+template <bool FAST>
+MAM4B_HD double fmadd(double x, double y, double z) {
+  if constexpr (FAST)
+    return fma(x, y, z);
+  return z + x * y;
+}
+
+// FAST = false: the FP64 loop's arithmetic (reverse of soa_step). FAST =
+// true: the reverse of f32::soa_step_mx, the mixed-precision step's loop:
+// the same double-precision values with every quotient x / d taken as
+// x * mx::rcp(d) and the sums fused (the mixed-precision adjoint).
+template <bool FAST>
+MAM4B_HD void soa_step_rev_t(const SoaState &st, SoaBar &b) {
   const double g_prev = st.g;
   const double g = dmax(g_prev, 0.0);
   double tot = g;
@@ -1331,16 +1356,16 @@ MAM4B_HD void soa_step_rev(const SoaState &st, SoaBar &b) {
     if (skip[n])
       continue;
     aoa[n] = st.opoa[n] + a[n];
-    sat[n] = st.g0 / dmax(aoa[n], 1.0e-20);
+    sat[n] = qdiv<FAST>(st.g0, dmax(aoa[n], 1.0e-20));
     gs[n] = sat[n] * a[n];
     M1[n] = dmax(g, dmax(gs[n], 1.0e-20));
-    phi[n] = (g - gs[n]) / M1[n];
-    tmpb += st.uptk[n] * fabs(phi[n]);
+    phi[n] = qdiv<FAST>(g - gs[n], M1[n]);
+    tmpb = fmadd<FAST>(st.uptk[n], fabs(phi[n]), tmpb);
   }
   const double tmpa = dmax(0.0, tmpb);
   const double dtmax = st.dtfull - st.tcur;
   const bool last = dtmax * tmpa <= 0.05;
-  const double dtcur = last ? dtmax : 0.05 / tmpa;
+  const double dtcur = last ? dtmax : qdiv<FAST>(0.05, tmpa);
   double beta[NMODE], del[NMODE], sat2[NMODE], den[NMODE];
   double ta = 0.0, tbs = 0.0;
 #pragma unroll
@@ -1351,22 +1376,28 @@ MAM4B_HD void soa_step_rev(const SoaState &st, SoaBar &b) {
     del[n] = g - gs[n];
     sat2[n] = sat[n];
     if (del[n] > 0.0) {
-      const double a_tmp = a[n] + beta[n] * del[n];
-      sat2[n] = st.g0 / dmax(st.opoa[n] + a_tmp, 1.0e-20);
+      const double a_tmp = fmadd<FAST>(beta[n], del[n], a[n]);
+      sat2[n] = qdiv<FAST>(st.g0, dmax(st.opoa[n] + a_tmp, 1.0e-20));
     }
-    den[n] = 1.0 + beta[n] * sat2[n];
-    ta += a[n] / den[n];
-    tbs += beta[n] / den[n];
+    den[n] = fmadd<FAST>(beta[n], sat2[n], 1.0);
+    if constexpr (FAST) {
+      const double rd = qdiv<FAST>(1.0, den[n]);
+      ta = fmadd<FAST>(a[n], rd, ta);
+      tbs = fmadd<FAST>(beta[n], rd, tbs);
+    } else {
+      ta += a[n] / den[n];
+      tbs += beta[n] / den[n];
+    }
   }
-  const double q = (tot - ta) / (1.0 + tbs);
+  const double q = qdiv<FAST>(tot - ta, 1.0 + tbs);
   const double gn = dmax(0.0, q);
   // ---- reverse (reciprocals taken once: the cotangents need not round as
   // the forward does)
   double rden[NMODE];
 #pragma unroll
   for (int n = 0; n < NMODE; ++n)
-    rden[n] = skip[n] ? 0.0 : 1.0 / den[n];
-  const double r1 = 1.0 / (1.0 + tbs);
+    rden[n] = skip[n] ? 0.0 : qdiv<FAST>(1.0, den[n]);
+  const double r1 = qdiv<FAST>(1.0, 1.0 + tbs);
   double gnb = b.g, ab_[NMODE], betab[NMODE], denb[NMODE], sat2b[NMODE], satb[NMODE], gsb[NMODE];
   double gb = 0.0, totb = 0.0, tab = 0.0, tbb = 0.0, dtcurb = 0.0, tcurb = 0.0;
 #pragma unroll
@@ -1387,7 +1418,7 @@ MAM4B_HD void soa_step_rev(const SoaState &st, SoaBar &b) {
   for (int n = 0; n < NMODE; ++n) {
     if (skip[n])
       continue;  // a'[n] = 0
-    const double an = (a[n] + beta[n] * gn) * rden[n];
+    const double an = fmadd<FAST>(beta[n], gn, a[n]) * rden[n];
     const double numb = b.a[n] * rden[n];
     denb[n] -= numb * an;
     ab_[n] += numb;
@@ -1409,9 +1440,9 @@ MAM4B_HD void soa_step_rev(const SoaState &st, SoaBar &b) {
     betab[n] += denb[n] * sat2[n];
     sat2b[n] += denb[n] * beta[n];
     if (del[n] > 0.0) {
-      const double a_tmp = a[n] + beta[n] * del[n];
+      const double a_tmp = fmadd<FAST>(beta[n], del[n], a[n]);
       const double aoa2 = st.opoa[n] + a_tmp;
-      const double rM2 = 1.0 / dmax(aoa2, 1.0e-20);
+      const double rM2 = qdiv<FAST>(1.0, dmax(aoa2, 1.0e-20));
       b.g0 += sat2b[n] * rM2;
       const double M2b = -sat2b[n] * sat2[n] * rM2;
       const double aoa2b = maxxc_rev(aoa2, 1.0e-20, M2b);
@@ -1432,7 +1463,7 @@ MAM4B_HD void soa_step_rev(const SoaState &st, SoaBar &b) {
   if (last)
     tcurb -= dtcurb;  // dtcur = dtfull - tcur
   else
-    tmpab -= dtcurb * dtcur / tmpa;
+    tmpab -= qdiv<FAST>(dtcurb * dtcur, tmpa);
   const double tmpbb = maxc_rev(0.0, tmpb, tmpab);
 #pragma unroll
   for (int n = 0; n < NMODE; ++n) {
@@ -1440,7 +1471,7 @@ MAM4B_HD void soa_step_rev(const SoaState &st, SoaBar &b) {
       continue;
     b.uptk[n] += tmpbb * fabs(phi[n]);
     const double phib = tmpbb * st.uptk[n] * (phi[n] < 0.0 ? -1.0 : 1.0);
-    const double rM1 = 1.0 / M1[n];
+    const double rM1 = qdiv<FAST>(1.0, M1[n]);
     gb += phib * rM1;
     gsb[n] -= phib * rM1;
     const double M1b = -phib * phi[n] * rM1;
@@ -1455,7 +1486,7 @@ MAM4B_HD void soa_step_rev(const SoaState &st, SoaBar &b) {
     satb[n] += gsb[n] * a[n];
     ab_[n] += gsb[n] * sat[n];
     // sat = g0 / dmax(aoa, 1e-20)
-    const double rM = 1.0 / dmax(aoa[n], 1.0e-20);
+    const double rM = qdiv<FAST>(1.0, dmax(aoa[n], 1.0e-20));
     b.g0 += satb[n] * rM;
     const double Mb = -satb[n] * sat[n] * rM;
     const double aoab = maxxc_rev(aoa[n], 1.0e-20, Mb);
@@ -1476,6 +1507,8 @@ MAM4B_HD void soa_step_rev(const SoaState &st, SoaBar &b) {
   b.g = maxxc_rev(g_prev, 0.0, gb);
   b.tcur = tcurb;
 }
+
+MAM4B_HD void soa_step_rev(const SoaState &st, SoaBar &b) { soa_step_rev_t<false>(st, b); }
 
 // soa_init (gasaerexch_soaexch.hpp:155-170): g0 from T (p fixed); opoa
 // from POM; initial g, a from the subarea

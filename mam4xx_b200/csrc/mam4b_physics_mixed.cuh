@@ -230,26 +230,33 @@ __device__ __forceinline__ void coag_pair_coefs(const StepConsts &C, const CoagT
 }
 
 // ------------------------------------------------- SOA sub-stepping, mixed
-// mam_soaexch_1subarea (gasaerexch_soaexch.hpp:80-341) with the state and
-// its implicit update in double precision and the step control in single
-// precision (MAM4B_MIXED):
-//  * FP64: the gas and particle SOA, their totals, the skip decision on the
-//    FP64 uptake rates, the elapsed time, the semi-implicit update
-//    g = (tot - sum a r) / (1 + sum beta r), a = (a + beta g) r with
-//    r = 1 / (1 + beta sat) and its sums;
-//  * FP32: the saturation ratios sat = g0 / (POA + a), the relative
-//    departures phi from equilibrium and the sub-step 0.05 / sum k |phi|;
-//  * each r starts from a single-precision reciprocal and takes one Newton
-//    step in FP64, r (2 - d r), which leaves a relative error of about
-//    1e-14; one IEEE division per pass (the gas update).
+// mam_soaexch_1subarea (gasaerexch_soaexch.hpp:80-341) for MAM4B_MIXED:
+// every value in double precision (state, saturation ratios, departures
+// phi, step control, the semi-implicit update), as in the FP64 loop, but
+// without IEEE divisions and with fused multiply-adds:
+//  * each quotient x / d is x * rcp(d), rcp the hardware's approximate
+//    double reciprocal refined by two Newton-Raphson steps (mx::rcp), one
+//    reciprocal shared by the three quotients over 1 + beta sat;
+//  * the products that feed a sum are fused with it (__fma_rn).
+// The results differ from the FP64 loop's by rounding only (a few ulps per
+// pass), so the loop takes the FP64 loop's sub-steps except where a step
+// decision sits within rounding of its threshold. No value changes type:
+// conversions between double and float issue at a quarter of the FP64 rate
+// on this GPU, so a loop that mixes the two types is no faster.
 // Conservation: the update conserves g + sum a for any values of r, as the
-// same r enter the sums and the particle update, so the FP32 inputs move
-// the equilibrium by about 1e-7 relative but leave the SOA mass exact to
-// rounding.
+// same r enter the sums and the particle update.
 namespace mx {
-__device__ __forceinline__ double recip(double d) {
-  const double r0 = (double)__fdividef(1.0f, (float)d);
-  return r0 * (2.0 - d * r0);
+// 1 / d for a positive, normal d without a division: the special-function
+// unit's approximate reciprocal (PTX rcp.approx.ftz.f64) and two steps of
+// Newton's iteration for 1/d, r <- r + r (1 - d r), each of which squares
+// the relative error; the result is within a few ulps of 1 / d.
+__device__ __forceinline__ double rcp(double d) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
+  double e = __fma_rn(-d, r, 1.0);
+  r = __fma_rn(r, e, r);
+  e = __fma_rn(-d, r, 1.0);
+  return __fma_rn(r, e, r);
 }
 }  // namespace mx
 
@@ -261,8 +268,7 @@ __device__ __forceinline__ bool soa_step_mx(SoaState &st) {
     return false;
   double g_soa = dmax(st.g, 0.0);
   double tot_soa = g_soa;
-  double a_soa[NMODE], g_star[NMODE];
-  float sat[NMODE];
+  double a_soa[NMODE], sat[NMODE], g_star[NMODE];
   bool skip[NMODE];
 #pragma unroll
   for (int n = 0; n < NMODE; ++n) {
@@ -270,25 +276,26 @@ __device__ __forceinline__ bool soa_step_mx(SoaState &st) {
     a_soa[n] = skip[n] ? 0.0 : dmax(st.a[n], 0.0);
     tot_soa += a_soa[n];
   }
-  const float g0 = (float)st.g0;
-  float tmpb = 0.0f;
+  double tmpb = 0.0;
 #pragma unroll
   for (int n = 0; n < NMODE; ++n) {
     if (skip[n])
       continue;
-    sat[n] = g0 * __fdividef(1.0f, (float)dmax(st.opoa[n] + a_soa[n], 1.0e-20));
-    g_star[n] = (double)sat[n] * a_soa[n];
-    const float phi = (float)(g_soa - g_star[n]) *
-                      __fdividef(1.0f, (float)dmax(g_soa, dmax(g_star[n], 1.0e-20)));
-    tmpb += (float)st.uptk[n] * fabsf(phi);
+    // both denominators are at least 1e-20: normal numbers
+    sat[n] = st.g0 * mx::rcp(dmax(st.opoa[n] + a_soa[n], 1.0e-20));
+    g_star[n] = sat[n] * a_soa[n];
+    const double phi = (g_soa - g_star[n]) * mx::rcp(dmax(g_soa, dmax(g_star[n], 1.0e-20)));
+    tmpb = __fma_rn(st.uptk[n], fabs(phi), tmpb);
   }
+  const double tmpa = dmax(0.0, tmpb);
   double dtcur;
   const double dtmax = st.dtfull - st.tcur;
-  if (dtmax * (double)tmpb <= 0.05) {
+  if (dtmax * tmpa <= 0.05) {
     dtcur = dtmax;
     st.tcur = st.dtfull;
   } else {
-    dtcur = (double)(0.05f * __fdividef(1.0f, tmpb));
+    // tmpa > 0.05 / dtmax here
+    dtcur = 0.05 * mx::rcp(tmpa);
     st.tcur += dtcur;
   }
   double beta[NMODE], r[NMODE], ta = 0.0, tb = 0.0;
@@ -299,17 +306,16 @@ __device__ __forceinline__ bool soa_step_mx(SoaState &st) {
     beta[n] = dtcur * st.uptk[n];
     const double del_g = g_soa - g_star[n];
     if (del_g > 0.0)
-      sat[n] = g0 * __fdividef(1.0f, (float)dmax(st.opoa[n] + (a_soa[n] + beta[n] * del_g),
-                                                   1.0e-20));
-    const double d = 1.0 + beta[n] * (double)sat[n];
-    r[n] = (d < 1.0e30) ? mx::recip(d) : 1.0 / d;
-    ta += a_soa[n] * r[n];
-    tb += beta[n] * r[n];
+      sat[n] = st.g0 * mx::rcp(dmax(st.opoa[n] + __fma_rn(beta[n], del_g, a_soa[n]), 1.0e-20));
+    // 1 + beta sat >= 1
+    r[n] = mx::rcp(__fma_rn(beta[n], sat[n], 1.0));
+    ta = __fma_rn(a_soa[n], r[n], ta);
+    tb = __fma_rn(beta[n], r[n], tb);
   }
-  g_soa = dmax(0.0, (tot_soa - ta) / (1.0 + tb));
+  g_soa = dmax(0.0, (tot_soa - ta) * mx::rcp(1.0 + tb));
 #pragma unroll
   for (int n = 0; n < NMODE; ++n)
-    st.a[n] = skip[n] ? 0.0 : (a_soa[n] + beta[n] * g_soa) * r[n];
+    st.a[n] = skip[n] ? 0.0 : __fma_rn(beta[n], g_soa, a_soa[n]) * r[n];
   st.g = g_soa;
   return true;
 }

@@ -1718,7 +1718,7 @@ struct AdjPipeArgs {
   size_t ld;
   double *abar;         // [AB_FIELDS][ncell]
   double *lbar;         // [LB_FIELDS][ncell]
-  double *ck;           // SOA states [6 kAdjSoaStates][nthreads of adj_soa_kernel]
+  double *ck;           // SOA states [6 adj_soa_slots(CK)][nthreads of adj_soa_kernel]
   unsigned *bins;       // [2 kPassBins]: loops per pass count, start offsets
   adj::AdjCfg cfg;
 };
@@ -1880,15 +1880,37 @@ __global__ void __launch_bounds__(256) adj_sort_kernel(const __grid_constant__ A
 
 // Reverse of the SOA loops. Warps take 32 loops at a time from the sorted
 // order list (one atomic per warp); every lane runs its loop forward,
-// storing the state (g, a[4], tcur) before each pass in its own column of
-// p.ck ([6 * pass + component][thread]: the lanes of a warp are at the
+// keeping the state (g, a[4], tcur) before passes in its own column of
+// p.ck ([6 * index + component][thread]: the lanes of a warp are at the
 // same pass, so a warp's stores and loads are coalesced), then the reverse
-// passes, last to first, each from its stored state, starting from the
-// loop-end cotangents left by adj_post_kernel. 2 blocks per SM (128
+// passes, last to first, starting from the loop-end cotangents left by
+// adj_post_kernel. CK = 1 stores the state before every pass (1,001 states
+// per thread). CK > 1 keeps a checkpoint every CK passes (the states
+// before passes 0, CK, 2 CK, ...: ceil(1001 / CK) per thread) and reverses
+// the loop block by block: it recomputes the block's states from its
+// checkpoint into a CK-state slice of the thread's column, then reverses
+// the block's passes from them. Both give the same gradient bit for bit
+// (the recomputed passes are the forward's arithmetic on the same state);
+// CK > 1 needs about 1/CK of the memory and recomputes up to CK - 1 passes
+// per block. FAST: the loop of the mixed-precision step (f32::soa_step_mx)
+// and its reverse (the mixed-precision adjoint). 2 blocks per SM (128
 // registers, some spilled to L1): the extra warps hide more FP64 latency
 // than the unconstrained 255-register build (10 % faster).
-constexpr int kAdjSoaStates = 1001;  // states stored per loop (passes <= 1000)
+constexpr int kAdjSoaStates = 1001;  // states before passes 0..1000 (passes <= 1000)
+// states kept per solver thread: checkpoints plus, with CK > 1, one block
+__host__ __device__ constexpr int adj_soa_slots(int ck) {
+  return ck == 1 ? kAdjSoaStates : (kAdjSoaStates + ck - 1) / ck + ck;
+}
 
+template <bool FAST>
+__device__ __forceinline__ bool adj_soa_pass(SoaState &st) {
+  if constexpr (FAST)
+    return f32::soa_step_mx(st);
+  else
+    return soa_step(st);
+}
+
+template <int CK, bool FAST>
 __global__ void __launch_bounds__(kSoaBlock, 2) adj_soa_kernel(const __grid_constant__ AdjPipeArgs p) {
   const StepArgs &a = p.s;
   const unsigned ntask = a.counters[CNT_QUEUED];
@@ -1896,6 +1918,22 @@ __global__ void __launch_bounds__(kSoaBlock, 2) adj_soa_kernel(const __grid_cons
   const size_t n = (size_t)a.ncell;
   const size_t nthreads = (size_t)gridDim.x * blockDim.x;
   double *ck = p.ck + (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  auto put = [&](int idx, const SoaState &x) {
+    double *e = ck + (size_t)6 * idx * nthreads;
+    e[0] = x.g;
+#pragma unroll
+    for (int j = 0; j < NMODE; ++j)
+      e[(1 + j) * nthreads] = x.a[j];
+    e[5 * nthreads] = x.tcur;
+  };
+  auto get = [&](int idx, SoaState &x) {
+    const double *e = ck + (size_t)6 * idx * nthreads;
+    x.g = e[0];
+#pragma unroll
+    for (int j = 0; j < NMODE; ++j)
+      x.a[j] = e[(1 + j) * nthreads];
+    x.tcur = e[5 * nthreads];
+  };
   while (true) {
     unsigned base = 0;
     if (lane == 0)
@@ -1931,15 +1969,12 @@ __global__ void __launch_bounds__(kSoaBlock, 2) adj_soa_kernel(const __grid_cons
     st.tcur = 0.0;
     st.dtfull = (double)(int)(a.dt / 1);
     st.niter = 0;
+    // forward: k passes (the states before passes 0..k-1 are reversed)
     int k = 0;
     while (true) {
-      double *e = ck + (size_t)6 * k * nthreads;
-      e[0] = st.g;
-#pragma unroll
-      for (int j = 0; j < NMODE; ++j)
-        e[(1 + j) * nthreads] = st.a[j];
-      e[5 * nthreads] = st.tcur;
-      if (!soa_step(st))
+      if (CK == 1 || k % CK == 0)
+        put(k / CK, st);
+      if (!adj_soa_pass<FAST>(st))
         break;
       ++k;
     }
@@ -1953,15 +1988,29 @@ __global__ void __launch_bounds__(kSoaBlock, 2) adj_soa_kernel(const __grid_cons
     }
     b.tcur = 0.0;
     b.g0 = 0.0;
-    while (k > 0) {
-      --k;
-      const double *e = ck + (size_t)6 * k * nthreads;
-      st.g = e[0];
-#pragma unroll
-      for (int j = 0; j < NMODE; ++j)
-        st.a[j] = e[(1 + j) * nthreads];
-      st.tcur = e[5 * nthreads];
-      adj::soa_step_rev(st, b);
+    if constexpr (CK == 1) {
+      while (k > 0) {
+        --k;
+        get(k, st);
+        adj::soa_step_rev_t<FAST>(st, b);
+      }
+    } else {
+      constexpr int kBlock = (kAdjSoaStates + CK - 1) / CK;  // first state of the block slice
+      for (int b0 = k > 0 ? ((k - 1) / CK) * CK : -1; b0 >= 0; b0 -= CK) {
+        const int nb = min(CK, k - b0);  // passes b0 .. b0 + nb - 1
+        get(b0 / CK, st);
+        // these passes all continued in the forward (niter only caps it)
+        st.niter = 0;
+        put(kBlock, st);
+        for (int j = 1; j < nb; ++j) {
+          adj_soa_pass<FAST>(st);
+          put(kBlock + j, st);
+        }
+        for (int j = nb - 1; j >= 0; --j) {
+          get(kBlock + j, st);
+          adj::soa_step_rev_t<FAST>(st, b);
+        }
+      }
     }
     const long long c = a.task[slot];
     double *lb = p.lbar + c;
@@ -3127,6 +3176,8 @@ struct mam4b_ctx {
   double *d_ck;
   int adj_grid;
   double *d_ck2, *d_abar, *d_lbar;
+  int adj_ck;           // SOA checkpoint interval of the pipelined adjoint (0 = 1)
+  int ck2_slots;        // SOA states per solver thread d_ck2 holds
   int *d_npass;         // [cap_adj]: passes of each SOA loop
   double *d_optics_lw;  // longwave optics tables (opt::kTableDoubles), set by the host
   double *d_optics_sw;  // shortwave optics tables (opt::kSwTableDoubles), set by the host
@@ -3722,6 +3773,14 @@ mam4b_status mam4b_set_tuning(mam4b_ctx *ctx, const mam4b_tuning *t) {
   if (!ctx || !t || !valid_tuning(*t))
     return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_set_tuning", cudaSuccess);
   ctx->tune = *t;
+  return MAM4B_OK;
+}
+
+mam4b_status mam4b_set_adjoint_checkpoint(mam4b_ctx *ctx, int interval) {
+  if (!ctx || (interval != 1 && interval != 4))
+    return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_set_adjoint_checkpoint: interval 1 or 4",
+                   cudaSuccess);
+  ctx->adj_ck = interval;
   return MAM4B_OK;
 }
 
@@ -4438,12 +4497,24 @@ mam4b_status mam4b_step_slab_noalloc(const mam4b_config *cfg, const double *in_s
 mam4b_status mam4b_adjoint_slab(mam4b_ctx *ctx, const double *in_slab, const double *pblh,
                                 const double *out_bar, double *in_bar, size_t ld, int ncol,
                                 int nlev, double dt, void *stream) {
+  return mam4b_adjoint_slab_ex(ctx, in_slab, pblh, out_bar, in_bar, ld, ncol, nlev, dt,
+                               MAM4B_FP64, stream);
+}
+
+mam4b_status mam4b_adjoint_slab_ex(mam4b_ctx *ctx, const double *in_slab, const double *pblh,
+                                   const double *out_bar, double *in_bar, size_t ld, int ncol,
+                                   int nlev, double dt, int precision, void *stream) {
   if (!ctx || !in_slab || !pblh || !out_bar || !in_bar || ncol < 0 || nlev <= 0 ||
-      ld < (size_t)ncol * (size_t)nlev || !(dt > 0.0) || !isfinite(dt))
+      ld < (size_t)ncol * (size_t)nlev || !(dt > 0.0) || !isfinite(dt) ||
+      (precision != MAM4B_FP64 && precision != MAM4B_MIXED && precision != MAM4B_MIXED_FAST))
     return set_err(ctx, MAM4B_ERR_INVALID_ARGUMENT, "mam4b_adjoint_slab", cudaSuccess);
   if (!ctx->cfg.do_cond && !ctx->cfg.do_newnuc)
     return set_err(ctx, MAM4B_ERR_NOT_SUPPORTED,
                    "mam4b_adjoint_slab: needs condensation or nucleation on", cudaSuccess);
+  if (precision == MAM4B_MIXED_FAST || (precision == MAM4B_MIXED && !ctx->cfg.do_cond))
+    return set_err(ctx, MAM4B_ERR_NOT_SUPPORTED,
+                   "mam4b_adjoint_slab: precision not supported (FP64; MIXED with condensation on)",
+                   cudaSuccess);
   cudaStream_t s = (cudaStream_t)stream;
   ctx->last_stream = s;
   const long long ncell = (long long)ncol * nlev;
@@ -4512,19 +4583,28 @@ mam4b_status mam4b_adjoint_slab(mam4b_ctx *ctx, const double *in_slab, const dou
     if (e == cudaSuccess)
       ctx->cap_adj = n;
   }
+  const int ck_interval = ctx->adj_ck > 1 ? ctx->adj_ck : 1;
+  if (e == cudaSuccess && ctx->d_ck2 && ctx->ck2_slots < adj_soa_slots(ck_interval)) {
+    cudaFree(ctx->d_ck2);
+    ctx->d_ck2 = nullptr;
+    ctx->ck2_slots = 0;
+  }
   if (e == cudaSuccess && !ctx->d_ck2) {
     int dev = 0, sms = 0, per_sm = 0;
     e = cudaGetDevice(&dev);
     if (e == cudaSuccess)
       e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e == cudaSuccess)
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adj_soa_kernel, kSoaBlock, 0);
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adj_soa_kernel<1, false>,
+                                                        kSoaBlock, 0);
     if (e == cudaSuccess) {
       ctx->adj_soa_grid = sms * (per_sm > 0 ? per_sm : 1);
-      e = cudaMalloc(&ctx->d_ck2,
-                     (size_t)6 * kAdjSoaStates * ctx->adj_soa_grid * kSoaBlock * sizeof(double));
+      const int slots = adj_soa_slots(ck_interval);
+      e = cudaMalloc(&ctx->d_ck2, (size_t)6 * slots * ctx->adj_soa_grid * kSoaBlock * sizeof(double));
       if (e != cudaSuccess)
         ctx->d_ck2 = nullptr;
+      else
+        ctx->ck2_slots = slots;
     }
   }
   if (e != cudaSuccess)
@@ -4547,7 +4627,7 @@ mam4b_status mam4b_adjoint_slab(mam4b_ctx *ctx, const double *in_slab, const dou
   p.bins = ctx->d_bins;
   p.cfg = cfg;
   p.s.npass = ctx->d_npass;
-  e = launch_pipeline(ctx, p.s, s, MAM4B_FP64);
+  e = launch_pipeline(ctx, p.s, s, precision);
   if (e == cudaSuccess)
     e = cudaMemsetAsync(ctx->d_bins, 0, kPassBins * sizeof(unsigned), s);
   if (e != cudaSuccess)
@@ -4559,7 +4639,15 @@ mam4b_status mam4b_adjoint_slab(mam4b_ctx *ctx, const double *in_slab, const dou
   adj_hist_kernel<<<sort_grid, 256, 0, s>>>(p);
   adj_scan_kernel<<<1, 1024, 0, s>>>(p);
   adj_sort_kernel<<<sort_grid, 256, 0, s>>>(p);
-  adj_soa_kernel<<<ctx->adj_soa_grid, kSoaBlock, 0, s>>>(p);
+  const bool fast = precision == MAM4B_MIXED;
+  if (ck_interval == 4 && fast)
+    adj_soa_kernel<4, true><<<ctx->adj_soa_grid, kSoaBlock, 0, s>>>(p);
+  else if (ck_interval == 4)
+    adj_soa_kernel<4, false><<<ctx->adj_soa_grid, kSoaBlock, 0, s>>>(p);
+  else if (fast)
+    adj_soa_kernel<1, true><<<ctx->adj_soa_grid, kSoaBlock, 0, s>>>(p);
+  else
+    adj_soa_kernel<1, false><<<ctx->adj_soa_grid, kSoaBlock, 0, s>>>(p);
   adj_pre_kernel<<<grid, block, 0, s>>>(p);
   adj_mode_kernel<<<dim3(grid, NMODE), block, 0, s>>>(p);
   adj_fin_kernel<<<grid, block, 0, s>>>(p);

@@ -124,6 +124,8 @@ def lib():
         L.mam4b_step_slab_noalloc.restype = I
         L.mam4b_adjoint_slab.argtypes = [P, P, P, P, P, S, I, I, D, P]
         L.mam4b_adjoint_slab.restype = I
+        L.mam4b_adjoint_slab_ex.argtypes = [P, P, P, P, P, S, I, I, D, I, P]
+        L.mam4b_adjoint_slab_ex.restype = I
         L.mam4b_step_tracers.argtypes = [P, P, P, S, P, P, P, P, P, P, P, P, S, I, I, D, I, P]
         L.mam4b_step_tracers.restype = I
         L.mam4b_optics_lw_set_tables.argtypes = [P, ctypes.POINTER(OpticsLwTables)]
@@ -171,6 +173,8 @@ def lib():
         L.mam4b_autotune.restype = I
         L.mam4b_set_graph_mode.argtypes = [P, I]
         L.mam4b_set_graph_mode.restype = I
+        L.mam4b_set_adjoint_checkpoint.argtypes = [P, I]
+        L.mam4b_set_adjoint_checkpoint.restype = I
         _lib = L
     return _lib
 
@@ -185,7 +189,8 @@ EXPORTED = ["mam4b_abi_version", "mam4b_default_config", "mam4b_create", "mam4b_
             "mam4b_optics_sw", "mam4b_aero_rad_props_sw", "mam4b_aero_rad_props_lw",
             "mam4b_dropmixnuc", "mam4b_default_tuning", "mam4b_get_tuning", "mam4b_set_tuning",
             "mam4b_tuning_from_json", "mam4b_autotune", "mam4b_set_graph_mode",
-            "mam4b_step_columns", "mam4b_synchronize"]
+            "mam4b_step_columns", "mam4b_synchronize", "mam4b_set_adjoint_checkpoint",
+            "mam4b_adjoint_slab_ex"]
 
 
 def default_tuning():
@@ -274,11 +279,19 @@ class Context:
         self._check(st, "mam4b_step_host")
 
     def adjoint_slab(self, in_ptr, pblh_ptr, out_bar_ptr, in_bar_ptr, ld, ncol, nlev, dt,
-                     stream=0):
-        """in_bar = (d out / d in)^T out_bar (mam4b_adjoint_slab)."""
-        st = self._lib.mam4b_adjoint_slab(self._h, in_ptr, pblh_ptr, out_bar_ptr, in_bar_ptr,
-                                          int(ld), int(ncol), int(nlev), float(dt),
-                                          ctypes.c_void_p(stream))
+                     stream=0, precision=FP64):
+        """in_bar = (d out / d in)^T out_bar (mam4b_adjoint_slab; with
+        precision=MIXED the adjoint of the mixed-precision step,
+        mam4b_adjoint_slab_ex)."""
+        if precision == FP64:
+            st = self._lib.mam4b_adjoint_slab(self._h, in_ptr, pblh_ptr, out_bar_ptr, in_bar_ptr,
+                                              int(ld), int(ncol), int(nlev), float(dt),
+                                              ctypes.c_void_p(stream))
+        else:
+            st = self._lib.mam4b_adjoint_slab_ex(self._h, in_ptr, pblh_ptr, out_bar_ptr,
+                                                 in_bar_ptr, int(ld), int(ncol), int(nlev),
+                                                 float(dt), int(precision),
+                                                 ctypes.c_void_p(stream))
         self._check(st, "mam4b_adjoint_slab")
 
     def step_tracers(self, q, qqcw, tracer_stride, temperature, pressure, height,
@@ -424,6 +437,12 @@ class Context:
 
     def set_tuning(self, t):
         self._check(self._lib.mam4b_set_tuning(self._h, ctypes.byref(t)), "mam4b_set_tuning")
+
+    def set_adjoint_checkpoint(self, interval):
+        """SOA states of the adjoint: 1 = every sub-step, 4 = a checkpoint
+        every 4 sub-steps (same gradient, a quarter of the memory)."""
+        self._check(self._lib.mam4b_set_adjoint_checkpoint(self._h, int(interval)),
+                    "mam4b_set_adjoint_checkpoint")
 
     def set_graph_mode(self, enable):
         self._check(self._lib.mam4b_set_graph_mode(self._h, int(bool(enable))),

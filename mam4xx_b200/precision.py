@@ -40,6 +40,47 @@ def error_report(out, ref, in_slab, dt, tol=1e-5):
     }
 
 
+def cell_errors_device(out, ref, in_slab, dt, chunk=1 << 20):
+    """Per-cell error (the largest of the cell's 68 output errors, as in
+    output_errors) of `out` against `ref`, on the device: torch tensors
+    (68, n), (68, n), (57, n) float64; returns a float64 tensor (n,)."""
+    import torch
+    n = out.shape[1]
+    cell_err = torch.empty(n, dtype=torch.float64, device=out.device)
+    for c0 in range(0, n, chunk):
+        c1 = min(n, c0 + chunk)
+        q0 = in_slab[STATE0:STATE0 + 52, c0:c1].abs()
+        q1 = (in_slab[STATE0:STATE0 + 52, c0:c1] + ref[:52, c0:c1] * dt).abs()
+        e_t = (out[:52, c0:c1] - ref[:52, c0:c1]).abs() * dt / torch.clamp(torch.maximum(q0, q1),
+                                                                            min=1e-30)
+        e_d = (out[52:, c0:c1] - ref[52:, c0:c1]).abs() / torch.clamp(ref[52:, c0:c1].abs(),
+                                                                      min=1e-300)
+        e = torch.cat([e_t, e_d], dim=0)
+        e = torch.where(torch.isnan(e), torch.full_like(e, float("inf")), e)
+        cell_err[c0:c1] = e.max(dim=0).values
+    return cell_err
+
+
+def conditioning_split(err, cond_err, tol=1e-5):
+    """Classifies the cells a form gets wrong by more than tol (err, per
+    cell) by the FP64 step's own sensitivity cond_err (per cell: its
+    results for its inputs rounded to single precision against its results
+    for the exact inputs): `ill_conditioned` cells, where that rounding
+    alone moves the FP64 result by more than tol, and the rest. Tensors (n,)
+    on one device; returns a dict of counts and fractions."""
+    out = err > tol
+    ill = cond_err > tol
+    n = int(err.numel())
+    n_out = int(out.sum())
+    n_ill_out = int((out & ill).sum())
+    return {"tol": tol, "cells": n,
+            "ill_conditioned_cells": int(ill.sum()),
+            "outside_tol": n_out,
+            "outside_tol_ill_conditioned": n_ill_out,
+            "outside_tol_well_conditioned": n_out - n_ill_out,
+            "well_conditioned_within_tol": float(1.0 - (n_out - n_ill_out) / max(1, int((~ill).sum())))}
+
+
 def error_report_device(out, ref, in_slab, dt, tol=1e-5, chunk=1 << 20):
     """error_report over every cell, computed on the device in chunks of
     cells (torch tensors (68, n), (68, n), (57, n) float64 on one device).

@@ -220,3 +220,88 @@ def test_adjoint_autograd_function(cuda_device):
     for k in J_STATE:
         direct[5 + k] += pdel_over_g(w)
     np.testing.assert_allclose(gx.cpu().numpy(), direct, rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize("name,ncol", [("c5", 64), ("c4_stress", 32)])
+def test_adjoint_checkpoint_interval_gives_the_same_gradient(cuda_device, name, ncol):
+    """A checkpoint every 4 SOA sub-steps with the others recomputed in the
+    reverse sweep gives the gradient of storing every sub-step, bit for bit
+    (loops of 1 to 1,000 sub-steps, so partial last blocks are covered),
+    and the context switches back and forth."""
+    w = make_workload(name, ncol=ncol, seed=91)
+    x = w["in_slab"]
+    n = x.shape[1]
+    rng = np.random.default_rng(2)
+    ybar = rng.standard_normal((native.NOUT, n))
+    ctx = native.Context()
+    every = adjoint(ctx, x, w["pblh"], ybar, w)
+    ctx.set_adjoint_checkpoint(4)
+    ck4 = adjoint(ctx, x, w["pblh"], ybar, w)
+    ctx.set_adjoint_checkpoint(1)
+    again = adjoint(ctx, x, w["pblh"], ybar, w)
+    assert np.isfinite(every).all()
+    assert np.array_equal(ck4, every)
+    assert np.array_equal(again, every)
+    with pytest.raises(native.MicrophysicsError):
+        ctx.set_adjoint_checkpoint(3)
+
+
+def test_mixed_adjoint_against_fp64_adjoint_and_differences(cuda_device):
+    """The adjoint of the MAM4B_MIXED step (mam4b_adjoint_slab_ex): its
+    gradient against the FP64 adjoint's on every entry, and against central
+    finite differences of the FP64 forward step, in units of relative
+    sensitivity |g - ref| |x| / |J_cell|; both checkpoint intervals give the
+    same gradient bit for bit."""
+    import torch
+    w = make_workload("c5", ncol=32, seed=93)
+    x = w["in_slab"]
+    n = x.shape[1]
+    wts = pdel_over_g(w)
+    ybar = objective_bar(wts, w["dt"], n)
+    ctx = native.Context()
+    g64 = adjoint(ctx, x, w["pblh"], ybar, w)
+
+    def adjoint_mixed():
+        xt = torch.from_numpy(np.ascontiguousarray(x)).cuda()
+        pt = torch.from_numpy(np.ascontiguousarray(w["pblh"])).cuda()
+        yt = torch.from_numpy(np.ascontiguousarray(ybar)).cuda()
+        xb = torch.full((native.NIN, n), float("nan"), dtype=torch.float64, device="cuda")
+        ctx.adjoint_slab(xt.data_ptr(), pt.data_ptr(), yt.data_ptr(), xb.data_ptr(), n,
+                         w["ncol"], w["nlev"], w["dt"], precision=native.MIXED)
+        torch.cuda.synchronize()
+        return xb.cpu().numpy()
+
+    gmx = adjoint_mixed()
+    ctx.set_adjoint_checkpoint(4)
+    assert np.array_equal(adjoint_mixed(), gmx)
+    ctx.set_adjoint_checkpoint(1)
+    assert np.isfinite(gmx).all()
+    for f in (1, 2, 4):
+        assert (gmx[f] == 0.0).all()
+    out = forward(ctx, x, w["pblh"], w)
+    J0 = objective_cells(x, out, wts, w["dt"])
+    for k in J_STATE:
+        g64[5 + k] += wts
+        gmx[5 + k] += wts
+    err = np.abs(gmx[DIFF_FIELDS] - g64[DIFF_FIELDS]) * np.abs(x[DIFF_FIELDS]) / np.abs(J0)
+    within = float((err <= 1e-5).mean())
+    print("MIXED_ADJOINT vs FP64 adjoint: median %.3g, 99%% %.3g, within 1e-5 %.5f, max %.3g"
+          % (np.median(err), np.quantile(err, 0.99), within, err.max()))
+    assert np.median(err) <= 1e-8
+    assert within >= 0.99
+    # central differences of the FP64 forward on 32 cells
+    rng = np.random.default_rng(93)
+    cells = rng.choice(n, 32, replace=False)
+
+    def J(xv):
+        return objective_cells(xv, forward(ctx, xv, w["pblh"], w), wts, w["dt"])
+
+    rows = _fd_entries(J, x, gmx, J0, cells, DIFF_FIELDS)
+    fd = rows[:, 2]
+    print("MIXED_ADJOINT vs FP64 differences: median %.3g, within 1e-6 %.5f, within 1e-5 %.5f"
+          % (np.median(fd), (fd <= 1e-6).mean(), (fd <= 1e-5).mean()))
+    assert np.median(fd) <= 1e-8
+    assert (fd <= 1e-5).mean() >= 0.99
+    with pytest.raises(native.MicrophysicsError):
+        ctx.adjoint_slab(0, 0, 0, 0, n, w["ncol"], w["nlev"], w["dt"],
+                         precision=native.MIXED_FAST)

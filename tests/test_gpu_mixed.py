@@ -7,7 +7,10 @@ below are the measured behaviour with margin, not the 1e-12 of the FP64
 path: FP32 rounding enters the bulk (water uptake, uptake and coagulation
 coefficients), and with MIXED_FAST also the SOA sub-stepping, which
 amplifies rounding near equilibrium (the FP64 algorithm does the same to
-1-ulp libm differences, at 1e-16 instead of 1e-7 scale).
+1-ulp libm differences, at 1e-16 instead of 1e-7 scale). MIXED keeps the
+SOA loop in double precision (division-free, fused) and its cells outside
+1e-5 are, but for 0.2 %, cells where the FP64 step itself moves by more
+than 1e-5 when its inputs are rounded to FP32.
 """
 
 import numpy as np
@@ -40,9 +43,9 @@ def test_mixed_against_fp64(cuda_device, cfg):
     mix = run(w, native.MIXED)
     assert np.isfinite(mix).all()
     r = error_report(mix, ref, w["in_slab"], w["dt"], tol=1e-5)
-    assert r["cells_within_tol"] >= 0.97, r
+    assert r["cells_within_tol"] >= 0.98, r
     assert r["cell_err_quantiles"]["0.5"] <= 2e-6, r
-    assert r["cell_err_quantiles"]["0.99"] <= 1e-4, r
+    assert r["cell_err_quantiles"]["0.99"] <= 5e-5, r
     assert max(r["per_output_median"]) <= 1e-6, r
 
 
@@ -114,3 +117,34 @@ def test_mixed_precision_arguments(cuda_device):
     with pytest.raises(native.MicrophysicsError, match="invalid argument"):
         ctx.step_slab(x.data_ptr(), pb.data_ptr(), out.data_ptr(), n, w["ncol"], w["nlev"],
                       w["dt"], precision=7)
+
+
+@pytest.mark.parametrize("cfg", ["c3", "c4"])
+def test_mixed_errors_against_the_steps_own_conditioning(cuda_device, cfg):
+    """Where the mixed form misses 1e-5 of the FP64 step, the FP64 step
+    itself is that sensitive: per cell, the FP64 step for its inputs rounded
+    to single precision (a relative change of at most 6e-8 per input)
+    against the FP64 step for the exact inputs. The FP64 algorithm's
+    results jump where a decision (an SOA sub-step count, a clip, a
+    threshold) changes with its inputs, so no form that rounds any input of
+    such a decision to FP32 can meet 1e-5 on those cells; on the others
+    (well-conditioned at FP32 rounding) the mixed form does, but for its own
+    FP32 rounding in the bulk (a few ulps over tens of operations, more
+    than the one rounding of each input): at least 99.5 % of them."""
+    from mam4xx_b200.precision import output_errors
+    w = make_workload(cfg, ncol=256, seed=310 + int(cfg[1]))
+    ref = run(w, native.FP64)
+    mix = run(w, native.MIXED)
+    w32 = dict(w)
+    w32["in_slab"] = w["in_slab"].astype(np.float32).astype(np.float64)
+    r32 = run(w32, native.FP64)
+    e_mix = output_errors(mix, ref, w["in_slab"], w["dt"]).max(axis=0)
+    e_cond = output_errors(r32, ref, w["in_slab"], w["dt"]).max(axis=0)
+    well = e_cond <= 1e-5
+    frac_well = float((e_mix[well] <= 1e-5).mean())
+    print("CONDITIONING %s: cells %d, ill-conditioned %d, mixed outside 1e-5 %d "
+          "(well-conditioned %d), well-conditioned within 1e-5 %.6f"
+          % (cfg, e_mix.size, int((~well).sum()), int((e_mix > 1e-5).sum()),
+             int((e_mix[well] > 1e-5).sum()), frac_well))
+    assert frac_well >= 0.995
+    assert float((e_mix <= 1e-5).mean()) >= 0.98

@@ -56,6 +56,7 @@ def test_invalid_arguments_are_rejected_without_a_device(lib):
     assert L.mam4b_step(None, None, None, 1, 1, 1.0, 0, None) == 1
     assert L.mam4b_step_slab(None, None, None, None, 0, 1, 1, 1.0, 0, None) == 1
     assert L.mam4b_destroy(None) == 1
+    assert L.mam4b_set_adjoint_checkpoint(None, 4) == 1
     h = ctypes.c_void_p()
     bad = native.Config(1, 1, 1, 1, 7, 2, 8)  # optaa must be 1 or 2
     assert L.mam4b_create(ctypes.byref(h), ctypes.byref(bad)) == 1
