@@ -338,7 +338,7 @@ mam4b_status mam4b_step_host(mam4b_ctx *ctx, const double *in_slab,
  * hand-off between the pipeline kernels, the work queue and its counters,
  * the per-cell auxiliaries) in one fixed device array inside the library
  * instead of context-owned allocations:
- * MAM4B_NOALLOC_MAX_CELLS cells at most, about 16 MB, held on every GPU
+ * MAM4B_NOALLOC_MAX_CELLS cells at most, about 13 MB, held on every GPU
  * that loads the library until the process exits. No context is needed.
  *
  *   cfg      process switches (NULL = mam4b_default_config)

@@ -67,8 +67,10 @@ struct StepArgs {
                         // is at least 1/inline_scale of the step finish in pre
 };
 
-// The step runs as a pipeline of three kernels when condensation is on and
-// no diagnostics are asked for: pre_kernel runs each cell up to the SOA
+// The step runs as a pipeline of six kernels when condensation is on and
+// no diagnostics are asked for: size_kernel, mode_kernel and pair_kernel
+// compute calcsize, water uptake, uptake rates and coagulation coefficients
+// into `aux` and the size outputs; pre_kernel runs each cell up to the SOA
 // condensation loop of its clear subarea, writes the loop's initial state
 // and the rest of the cell's state at that point to slot-indexed scratch
 // and queues the cell (cloudy cells finish there); soa_kernel runs the
@@ -113,12 +115,14 @@ enum {
   H_SV_SOA = 32,
   H_DGN_PC = 33,   // dry diameter of the primary-carbon mode
   H_RELHUM = 34,   // relative humidity of the clear subarea
-  H_OC = 35,       // 25 outgoing cloud-borne grid means
-  H_CI = 60,       // 25 interstitial contributions of the cloudy subarea
-  H_CG = 85,       // 2 gas contributions of the cloudy subarea (SOAG, H2SO4)
-  H_SOAG0 = 87,    // SOA gas at the start of the loop (read by the adjoint)
-  H_FIELDS = 88
+  H_CI = 35,       // 25 interstitial contributions of the cloudy subarea
+  H_CG = 60,       // 2 gas contributions of the cloudy subarea (SOAG, H2SO4)
+  H_SOAG0 = 62,    // SOA gas at the start of the loop (read by the adjoint)
+  H_FIELDS = 63
 };
+// (The outgoing cloud-borne grid means are final once pre has set up the
+// subareas: the clear subarea does not change them. pre writes their
+// tendencies itself, store_cloudborne, so they are not handed off.)
 
 // Clear subarea, mam_amicphys_1subarea (mam4_amicphys.hpp:1127-1697), part 1:
 // optaa-2 production split and H2SO4 uptake rates from the per-particle
@@ -365,20 +369,40 @@ __device__ __forceinline__ int clear_subarea(const StepArgs &a, double deltat, d
   return niter;
 }
 
-__device__ __forceinline__ void store_outputs(const StepArgs &a, long long c, double o_h2so4,
-                                              double o_soag, const double (&oi)[NPOP],
-                                              const double (&oc)[NPOP], double h2so4, double soag,
-                                              const double (&ai)[NPOP], const double (&ac)[NPOP]) {
+// Tendencies of the 25 cloud-borne populations from their outgoing grid
+// means oc (vmr) and incoming values ac (mmr).
+__device__ __forceinline__ void store_cloudborne(const StepArgs &a, long long c,
+                                                 const double (&oc)[NPOP],
+                                                 const double (&ac)[NPOP]) {
+  const StepConsts &C = c_k;
+  const double dt = a.dt;
+  double *const *out = a.out;
+#pragma unroll
+  for (int p = 0; p < NPOP; ++p)
+    out[MAM4B_OUT_TEND + 27 + p][c] = (oc[p] * C.to_mmr[2 + p] - ac[p]) / dt;
+}
+
+// Tendencies of the gases and the 25 interstitial populations.
+__device__ __forceinline__ void store_interstitial(const StepArgs &a, long long c, double o_h2so4,
+                                                   double o_soag, const double (&oi)[NPOP],
+                                                   double h2so4, double soag,
+                                                   const double (&ai)[NPOP]) {
   const StepConsts &C = c_k;
   const double dt = a.dt;
   double *const *out = a.out;
   out[MAM4B_OUT_TEND + 0][c] = (o_h2so4 * C.to_mmr[0] - h2so4) / dt;
   out[MAM4B_OUT_TEND + 1][c] = (o_soag * C.to_mmr[1] - soag) / dt;
 #pragma unroll
-  for (int p = 0; p < NPOP; ++p) {
+  for (int p = 0; p < NPOP; ++p)
     out[MAM4B_OUT_TEND + 2 + p][c] = (oi[p] * C.to_mmr[2 + p] - ai[p]) / dt;
-    out[MAM4B_OUT_TEND + 27 + p][c] = (oc[p] * C.to_mmr[2 + p] - ac[p]) / dt;
-  }
+}
+
+__device__ __forceinline__ void store_outputs(const StepArgs &a, long long c, double o_h2so4,
+                                              double o_soag, const double (&oi)[NPOP],
+                                              const double (&oc)[NPOP], double h2so4, double soag,
+                                              const double (&ai)[NPOP], const double (&ac)[NPOP]) {
+  store_interstitial(a, c, o_h2so4, o_soag, oi, h2so4, soag, ai);
+  store_cloudborne(a, c, oc, ac);
 }
 
 // Per-cell state after calcsize and water uptake (modal_aero_calcsize_sub,
@@ -1019,17 +1043,13 @@ __device__ __forceinline__ void cell_finish(const StepArgs &a, const long long c
                                             const Src &src);
 // cell_finish's late inputs held in registers (the fused path of pre)
 struct FinishRegs {
-  const double (&oc_)[NPOP];
   const double (&ci_)[NPOP];
   const double (&cg_)[2];
   const double (&ai_)[NPOP];
-  const double (&ac_)[NPOP];
   double h2so4_, soag_;
-  __device__ double oc(int p) const { return oc_[p]; }
   __device__ double ci(int p) const { return ci_[p]; }
   __device__ double cg(int g) const { return cg_[g]; }
   __device__ double ai(int p) const { return ai_[p]; }
-  __device__ double ac(int p) const { return ac_[p]; }
   __device__ double h2so4() const { return h2so4_; }
   __device__ double soag() const { return soag_; }
 };
@@ -1110,7 +1130,8 @@ __device__ __forceinline__ void cell_pre(const StepArgs &a, const ChemArgs &ch,
 #pragma unroll
       for (int k = 0; k < NMODE; ++k)
         s.aer[0][k] = st.a[k];
-      const FinishRegs src{oc, ci, cg, f.ai, f.ac, f.h2so4, f.soag};
+      store_cloudborne(a, c, oc, f.ac);
+      const FinishRegs src{ci, cg, f.ai, f.h2so4, f.soag};
       cell_finish(a, c, f.temp, f.pmid, f.zm, f.cld, f.pblh, rh, f.dgn_a[3], s, cm, src);
       return;
     }
@@ -1166,9 +1187,7 @@ __device__ __forceinline__ void cell_pre(const StepArgs &a, const ChemArgs &ch,
   h[H_DGN_PC * n] = f.dgn_a[3];
   h[H_RELHUM * n] = rh;
   h[H_SOAG0 * n] = s.gas[0];
-#pragma unroll
-  for (int p = 0; p < NPOP; ++p)
-    h[(H_OC + p) * n] = oc[p];
+  store_cloudborne(a, c, oc, f.ac);
   if (partly) {
 #pragma unroll
     for (int p = 0; p < NPOP; ++p)
@@ -1181,13 +1200,14 @@ __device__ __forceinline__ void cell_pre(const StepArgs &a, const ChemArgs &ch,
 // Second half of a cell after its SOA loop: the rest of the clear subarea
 // (H2SO4 update, renaming, nucleation, coagulation with the coefficients of
 // pair_kernel, aging), recombination with the cloudy subarea's
-// contributions (ci, cg; partly cloudy cells) and the outgoing cloud-borne
-// grid means oc, tendencies. s holds the clear subarea with the loop's
-// result, cm the values saved before condensation.
-// src supplies the values read late (src.oc(p), ci(p), cg(g), ai(p), ac(p),
-// h2so4(), soag()): from registers in pre's fused path, from the hand-off
-// and the inputs in post_kernel, where reading them only when needed keeps
-// them out of registers during the suffix.
+// contributions (ci, cg; partly cloudy cells), tendencies of the gases and
+// interstitial populations (the cloud-borne ones are written by the pre
+// stage). s holds the clear subarea with the loop's result, cm the values
+// saved before condensation.
+// src supplies the values read late (src.ci(p), cg(g), ai(p), h2so4(),
+// soag()): from registers in pre's fused path, from the hand-off and the
+// inputs in post_kernel, where reading them only when needed keeps them out
+// of registers during the suffix.
 template <class Src>
 __device__ __forceinline__ void cell_finish(const StepArgs &a, const long long c, double temp,
                                             double pmid, double zm, double cld, double pblh,
@@ -1236,14 +1256,11 @@ __device__ __forceinline__ void cell_finish(const StepArgs &a, const long long c
       }
     }
   }
-  double oc[NPOP], ai[NPOP], ac[NPOP];
+  double ai[NPOP];
 #pragma unroll
-  for (int p = 0; p < NPOP; ++p) {
-    oc[p] = src.oc(p);
+  for (int p = 0; p < NPOP; ++p)
     ai[p] = src.ai(p);
-    ac[p] = src.ac(p);
-  }
-  store_outputs(a, c, o_h2so4, o_soag, oi, oc, src.h2so4(), src.soag(), ai, ac);
+  store_interstitial(a, c, o_h2so4, o_soag, oi, src.h2so4(), src.soag(), ai);
 }
 
 // cell_finish's late inputs read from the hand-off of queue slot `slot`
@@ -1253,11 +1270,9 @@ struct FinishLoads {
   long long c;
   const double *h;
   size_t n;
-  __device__ double oc(int p) const { return h[(H_OC + p) * n]; }
   __device__ double ci(int p) const { return h[(H_CI + p) * n]; }
   __device__ double cg(int g) const { return h[(H_CG + g) * n]; }
   __device__ double ai(int p) const { return __ldg(a.in[MAM4B_IN_AER_I + p] + c); }
-  __device__ double ac(int p) const { return __ldg(a.in[MAM4B_IN_AER_C + p] + c); }
   __device__ double h2so4() const { return __ldg(a.in[MAM4B_IN_H2SO4] + c); }
   __device__ double soag() const { return __ldg(a.in[MAM4B_IN_SOAG] + c); }
 };
@@ -4492,8 +4507,10 @@ mam4b_status mam4b_step_slab_noalloc(const mam4b_config *cfg, const double *in_s
 }
 
 // Reverse-mode adjoint (include/mam4b.h). With condensation on: the
-// forward pipeline into the context's output scratch, then the three
-// reverse kernels; otherwise one thread per cell (adjoint_kernel).
+// forward pipeline (without its post stage) into the context's output
+// scratch, then eight reverse launches (suffix, the counting sort of the
+// SOA loops, the loops, front, water uptake, calcsize); otherwise one
+// thread per cell (adjoint_kernel).
 mam4b_status mam4b_adjoint_slab(mam4b_ctx *ctx, const double *in_slab, const double *pblh,
                                 const double *out_bar, double *in_bar, size_t ld, int ncol,
                                 int nlev, double dt, void *stream) {
