@@ -745,6 +745,31 @@ def mixed_leg(native, torch, dev, stream, args, ws, rank):
                                      "worst_outputs": {str(k): r["per_output_max"][k] for k in worst},
                                      "per_output_max": r["per_output_max"],
                                      "per_output_median": r["per_output_median"]}}
+    # the uneven-batching configuration c4 in FP64 and MIXED (speed and
+    # error; the full reports above are on c3)
+    del xm, pbm, ref, got
+    w4 = make_workload("c4", ncol=args.ncol, seed=20261203 + 1000 * rank)
+    x4 = torch.from_numpy(w4["in_slab"]).to(dev)
+    pb4 = torch.from_numpy(w4["pblh"]).to(dev)
+    n4 = x4.shape[1]
+    r64 = torch.empty((native.NOUT, n4), dtype=torch.float64, device=dev)
+    rmx = torch.empty_like(r64)
+    t4 = {}
+    for name, prec, o in (("fp64", native.FP64, r64), ("mixed", native.MIXED, rmx)):
+        def f4(prec=prec, o=o):
+            ctx4.step_slab(x4.data_ptr(), pb4.data_ptr(), o.data_ptr(), n4, w4["ncol"], NLEV,
+                           w4["dt"], precision=prec, stream=stream.cuda_stream)
+        ctx4 = ctx
+        ms, _, _ = timed_steps(f4, args.steps, args.warmup, EventClock(stream),
+                               sync=torch.cuda.synchronize, device=dev)
+        t4[name] = ms / args.steps
+    r4 = error_report_device(rmx, r64, x4, w4["dt"], tol=1e-5)
+    res["c4"] = {"workload": "c4: %d columns x %d levels (uneven batching)" % (w4["ncol"], NLEV),
+                 "fp64_ms_per_step": t4["fp64"], "mixed_ms_per_step": t4["mixed"],
+                 "mixed_speedup_vs_fp64": max_over_ranks(t4["fp64"] / t4["mixed"], dev),
+                 "mixed_err_vs_fp64": {"cells_within_1e-5": r4["cells_within_tol"],
+                                       "median": r4["median"], "max": r4["max"],
+                                       "cell_err_quantiles": r4["cell_err_quantiles"]}}
     ctx.close()
     return res
 
@@ -910,6 +935,10 @@ def main():
                            "cells_within_1e-5": round(e["cells_within_1e-5"], 5),
                            "well_conditioned_within_1e-5":
                                round(e["conditioning"]["well_conditioned_within_tol"], 6)}
+        if "c4" in precisions:
+            legs["mixed_c4"] = {
+                "speedup_vs_fp64": round(precisions["c4"]["mixed_speedup_vs_fp64"], 3),
+                "cells_within_1e-5": round(precisions["c4"]["mixed_err_vs_fp64"]["cells_within_1e-5"], 5)}
     if adjoint:
         legs["adjoint"] = {k: round(adjoint[k], 3) for k in
                            ("adjoint_over_forward", "adjoint_ck4_over_forward") if k in adjoint}

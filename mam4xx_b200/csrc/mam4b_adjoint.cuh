@@ -1330,10 +1330,13 @@ MAM4B_HD double fmadd(double x, double y, double z) {
   return z + x * y;
 }
 
-// FAST = false: the FP64 loop's arithmetic (reverse of soa_step). FAST =
-// true: the reverse of f32::soa_step_mx, the mixed-precision step's loop:
-// the same double-precision values with every quotient x / d taken as
-// x * mx::rcp(d) and the sums fused (the mixed-precision adjoint).
+// The forward values of the pass are recomputed with the arithmetic of the
+// loop being reversed, so that every branch (skip, last sub-step, del > 0,
+// the clips) is the forward's: FAST = false the FP64 loop's (soa_step),
+// FAST = true f32::soa_step_mx's, the mixed-precision step's loop (every
+// quotient x / d as x * mx::rcp(d), the sums fused; the mixed-precision
+// adjoint). The cotangent sweep takes each reciprocal once, as
+// mx::rcp(d), in both: cotangents need not round as the forward does.
 template <bool FAST>
 MAM4B_HD void soa_step_rev_t(const SoaState &st, SoaBar &b) {
   const double g_prev = st.g;
@@ -1396,8 +1399,8 @@ MAM4B_HD void soa_step_rev_t(const SoaState &st, SoaBar &b) {
   double rden[NMODE];
 #pragma unroll
   for (int n = 0; n < NMODE; ++n)
-    rden[n] = skip[n] ? 0.0 : qdiv<FAST>(1.0, den[n]);
-  const double r1 = qdiv<FAST>(1.0, 1.0 + tbs);
+    rden[n] = skip[n] ? 0.0 : qdiv<true>(1.0, den[n]);
+  const double r1 = qdiv<true>(1.0, 1.0 + tbs);
   double gnb = b.g, ab_[NMODE], betab[NMODE], denb[NMODE], sat2b[NMODE], satb[NMODE], gsb[NMODE];
   double gb = 0.0, totb = 0.0, tab = 0.0, tbb = 0.0, dtcurb = 0.0, tcurb = 0.0;
 #pragma unroll
@@ -1442,7 +1445,7 @@ MAM4B_HD void soa_step_rev_t(const SoaState &st, SoaBar &b) {
     if (del[n] > 0.0) {
       const double a_tmp = fmadd<FAST>(beta[n], del[n], a[n]);
       const double aoa2 = st.opoa[n] + a_tmp;
-      const double rM2 = qdiv<FAST>(1.0, dmax(aoa2, 1.0e-20));
+      const double rM2 = qdiv<true>(1.0, dmax(aoa2, 1.0e-20));
       b.g0 += sat2b[n] * rM2;
       const double M2b = -sat2b[n] * sat2[n] * rM2;
       const double aoa2b = maxxc_rev(aoa2, 1.0e-20, M2b);
@@ -1463,7 +1466,7 @@ MAM4B_HD void soa_step_rev_t(const SoaState &st, SoaBar &b) {
   if (last)
     tcurb -= dtcurb;  // dtcur = dtfull - tcur
   else
-    tmpab -= qdiv<FAST>(dtcurb * dtcur, tmpa);
+    tmpab -= qdiv<true>(dtcurb * dtcur, tmpa);
   const double tmpbb = maxc_rev(0.0, tmpb, tmpab);
 #pragma unroll
   for (int n = 0; n < NMODE; ++n) {
@@ -1471,7 +1474,7 @@ MAM4B_HD void soa_step_rev_t(const SoaState &st, SoaBar &b) {
       continue;
     b.uptk[n] += tmpbb * fabs(phi[n]);
     const double phib = tmpbb * st.uptk[n] * (phi[n] < 0.0 ? -1.0 : 1.0);
-    const double rM1 = qdiv<FAST>(1.0, M1[n]);
+    const double rM1 = qdiv<true>(1.0, M1[n]);
     gb += phib * rM1;
     gsb[n] -= phib * rM1;
     const double M1b = -phib * phi[n] * rM1;
@@ -1486,7 +1489,7 @@ MAM4B_HD void soa_step_rev_t(const SoaState &st, SoaBar &b) {
     satb[n] += gsb[n] * a[n];
     ab_[n] += gsb[n] * sat[n];
     // sat = g0 / dmax(aoa, 1e-20)
-    const double rM = qdiv<FAST>(1.0, dmax(aoa[n], 1.0e-20));
+    const double rM = qdiv<true>(1.0, dmax(aoa[n], 1.0e-20));
     b.g0 += satb[n] * rM;
     const double Mb = -satb[n] * sat[n] * rM;
     const double aoab = maxxc_rev(aoa[n], 1.0e-20, Mb);

@@ -1907,8 +1907,13 @@ __global__ void __launch_bounds__(256) adj_sort_kernel(const __grid_constant__ A
 // the block's passes from them. Both give the same gradient bit for bit
 // (the recomputed passes are the forward's arithmetic on the same state);
 // CK > 1 needs about 1/CK of the memory and recomputes up to CK - 1 passes
-// per block. FAST: the loop of the mixed-precision step (f32::soa_step_mx)
-// and its reverse (the mixed-precision adjoint). 2 blocks per SM (128
+// per block. The forward loop is the step's: soa_step (FP64), or with FAST
+// f32::soa_step_mx (the mixed-precision adjoint). The reverse of each pass
+// linearises it at the stored state with the division-free arithmetic of
+// f32::soa_step_mx (adj::soa_step_rev_t<true>): the trajectory is the
+// forward's exactly, its local derivative is computed to rounding (a
+// branch that sits within rounding of its threshold may be taken the other
+// way, like a finite difference across it). 2 blocks per SM (128
 // registers, some spilled to L1): the extra warps hide more FP64 latency
 // than the unconstrained 255-register build (10 % faster).
 constexpr int kAdjSoaStates = 1001;  // states before passes 0..1000 (passes <= 1000)
@@ -2007,7 +2012,7 @@ __global__ void __launch_bounds__(kSoaBlock, 2) adj_soa_kernel(const __grid_cons
       while (k > 0) {
         --k;
         get(k, st);
-        adj::soa_step_rev_t<FAST>(st, b);
+        adj::soa_step_rev_t<true>(st, b);
       }
     } else {
       constexpr int kBlock = (kAdjSoaStates + CK - 1) / CK;  // first state of the block slice
@@ -2023,7 +2028,7 @@ __global__ void __launch_bounds__(kSoaBlock, 2) adj_soa_kernel(const __grid_cons
         }
         for (int j = nb - 1; j >= 0; --j) {
           get(kBlock + j, st);
-          adj::soa_step_rev_t<FAST>(st, b);
+          adj::soa_step_rev_t<true>(st, b);
         }
       }
     }
