@@ -547,6 +547,23 @@ def adjoint_leg(native, torch, dev, stream, args, ws):
         gmix[5 + k] += torch.from_numpy(wts).to(dev)
     rows = [0, 3, 5, 6] + list(range(7, 57))
     emx = ((gmix[rows] - gfull[rows]).abs() * xa[rows].abs() / jcell.abs().clamp(min=1e-300))
+    # cells whose mixed forward step itself departs from the FP64 one by
+    # more than 1e-5 (a different sub-step count or branch): the gradients
+    # there are of different branches
+    from mam4xx_b200.precision import cell_errors_device
+    out64 = outa.clone()
+    fwd_mixed()
+    torch.cuda.synchronize()
+    fwd_err = cell_errors_device(outa, out64, xa, wa["dt"])
+    bad_entry = emx > 1e-5
+    bad_cells = bad_entry.any(dim=0)
+    departs = fwd_err > 1e-5
+    branch = {"cells_with_entries_above_1e-5": int(bad_cells.sum()),
+              "of_which_forward_departs": int((bad_cells & departs).sum()),
+              "cells_where_forward_departs": int(departs.sum()),
+              "entries_above_1e-5_in_cells_where_forward_departs":
+                  float(bad_entry[:, departs].sum()) / max(1.0, float(bad_entry.sum()))}
+    del out64, fwd_err
     emx = emx.flatten()
     samp = emx[torch.randperm(emx.numel(), generator=torch.Generator().manual_seed(7))[:1 << 20]
                .to(dev)]
@@ -556,7 +573,8 @@ def adjoint_leg(native, torch, dev, stream, args, ws):
                      "q9999": float(qs[1]), "entries_above_1": int((emx > 1.0).sum()),
                      "max": float(emx.max()),
                      "within_1e-6": float((emx <= 1e-6).double().mean()),
-                     "within_1e-5": float((emx <= 1e-5).double().mean())}
+                     "within_1e-5": float((emx <= 1e-5).double().mean()),
+                     "branches": branch}
     del gfull, gmix, emx, samp
     # finite-difference check on 64 cells (first 8 columns x 8 levels)
     g = xbar.cpu().numpy()
