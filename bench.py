@@ -517,7 +517,7 @@ def adjoint_leg(native, torch, dev, stream, args, ws):
                           precision=native.MIXED)
 
     times = {}
-    ka = max(2, min(args.steps, 5))
+    ka = max(5, min(args.steps, 10))
     for name, f in (("forward", fwd), ("forward_mixed", fwd_mixed), ("adjoint_mixed", adj_mixed),
                     ("adjoint_ck4", adj_ck4), ("adjoint", adj)):
         actx.set_adjoint_checkpoint(1)
