@@ -29,21 +29,50 @@ constexpr int kRefi = kRefr + 4 * kLwBands * kPrefr;          // [4][16][10]
 constexpr int kAbsp = kRefi + 4 * kLwBands * kPrefi;          // [4][16][5][7][10]
 constexpr int kTableDoubles = kAbsp + 4 * kLwBands * kNcoef * kPrefr * kPrefi;
 
+// Where the tables of one band sit. LwTables / SwTables: the whole device
+// table (the layouts here, read through the read-only data cache). SwBand:
+// one band's values staged in shared memory by the shortwave band kernel
+// (species and water indices, the two refractive-index grids and the
+// coefficient tables of the four modes, band index dropped). The functions
+// below read the same values in the same order through either, so their
+// results do not depend on where the tables are.
+struct LwTables {
+  static constexpr bool kShared = false;
+  MAM4B_HD static int spec_re(int m, int s, int b) { return kSpecRe + (m * 7 + s) * kLwBands + b; }
+  MAM4B_HD static int spec_im(int m, int s, int b) { return kSpecIm + (m * 7 + s) * kLwBands + b; }
+  MAM4B_HD static int water_re(int b) { return kWaterRe + b; }
+  MAM4B_HD static int water_im(int b) { return kWaterIm + b; }
+  MAM4B_HD static int refr(int m, int b) { return kRefr + (m * kLwBands + b) * kPrefr; }
+  MAM4B_HD static int refi(int m, int b) { return kRefi + (m * kLwBands + b) * kPrefi; }
+  MAM4B_HD static int absp(int m, int b) {
+    return kAbsp + (m * kLwBands + b) * kNcoef * kPrefr * kPrefi;
+  }
+};
+
+template <class L>
+MAM4B_HD double tld(const double *p) {
+  if constexpr (L::kShared)
+    return *p;
+  else
+    return MAM4B_LDG(p);
+}
+
 // position of ref in a table: index of the bracket and the fraction
 // (compute_factors)
+template <class L>
 MAM4B_HD void table_factors(int n, double ref, const double *tab, int &ix, double &tt) {
   ix = 1;
   tt = 0.0;
   if (n > 1) {
     int ii = 0;
     for (ii = 0; ii < n; ++ii)
-      if (ref < MAM4B_LDG(tab + ii))
+      if (ref < tld<L>(tab + ii))
         break;
     ix = (ii - 1 > 0) ? ii - 1 : 0;
     const int ip1 = (ix + 1 < n - 1) ? ix + 1 : n - 1;
-    const double dx = MAM4B_LDG(tab + ip1) - MAM4B_LDG(tab + ix);
+    const double dx = tld<L>(tab + ip1) - tld<L>(tab + ix);
     if (fabs(dx) > 1.e-20)
-      tt = (ref - MAM4B_LDG(tab + ix)) / dx;
+      tt = (ref - tld<L>(tab + ix)) / dx;
   }
 }
 
@@ -72,14 +101,15 @@ MAM4B_HD void mode_specvol(int m, const double (&ai)[NPOP], double (&specvol)[7]
     specvol[s] = ai[K::spec0(m) + s] / act::type_dens(act::spectype(m, s));
 }
 
+template <class L = LwTables>
 MAM4B_HD double mode_band_tau(const double *tables, int m, int b, const double (&specvol)[7],
                               double qaerwat, const double (&cheb)[kNcoef], double mass) {
   const int nspec = K::nspec(m);
   double dryvol = 0.0, cre = 0.0, cim = 0.0;
   for (int s = 0; s < nspec; ++s) {
     dryvol += specvol[s];
-    cre += specvol[s] * MAM4B_LDG(tables + kSpecRe + (m * 7 + s) * kLwBands + b);
-    cim += specvol[s] * MAM4B_LDG(tables + kSpecIm + (m * 7 + s) * kLwBands + b);
+    cre += specvol[s] * tld<L>(tables + L::spec_re(m, s, b));
+    cim += specvol[s] * tld<L>(tables + L::spec_im(m, s, b));
   }
   double watervol = qaerwat / 1.0e3;
   double wetvol = watervol + dryvol;
@@ -87,34 +117,34 @@ MAM4B_HD double mode_band_tau(const double *tables, int m, int b, const double (
     watervol = 0.0;
     wetvol = dryvol;
   }
-  cre += watervol * MAM4B_LDG(tables + kWaterRe + b);
-  cim += watervol * MAM4B_LDG(tables + kWaterIm + b);
+  cre += watervol * tld<L>(tables + L::water_re(b));
+  cim += watervol * tld<L>(tables + L::water_im(b));
   if (wetvol > 1.e-40) {
     cre /= wetvol;
     cim /= wetvol;
   }
   const double refr = cre, refi = fabs(cim);
-  const double *rt = tables + kRefr + (m * kLwBands + b) * kPrefr;
-  const double *it = tables + kRefi + (m * kLwBands + b) * kPrefi;
+  const double *rt = tables + L::refr(m, b);
+  const double *it = tables + L::refi(m, b);
   int itab, jtab;
   double ttab, utab;
-  table_factors(kPrefr, refr, rt, itab, ttab);
-  table_factors(kPrefi, refi, it, jtab, utab);
+  table_factors<L>(kPrefr, refr, rt, itab, ttab);
+  table_factors<L>(kPrefi, refi, it, jtab, utab);
   const double tu = ttab * utab;
   const double tuc = ttab - tu;
   const double tcuc = 1.0 - tuc - utab;
   const double tcu = utab - tu;
   const int jp1 = (jtab + 1 < kPrefi - 1) ? jtab + 1 : kPrefi - 1;
   const int ip1 = (itab + 1 < kPrefr - 1) ? itab + 1 : kPrefr - 1;
-  const double *tb = tables + kAbsp + (m * kLwBands + b) * kNcoef * kPrefr * kPrefi;
+  const double *tb = tables + L::absp(m, b);
   double pabs = 0.0;
 #pragma unroll
   for (int c = 0; c < kNcoef; ++c) {
     const double *tc = tb + c * kPrefr * kPrefi;
-    const double coef = tcuc * MAM4B_LDG(tc + itab * kPrefi + jtab) +
-                        tuc * MAM4B_LDG(tc + ip1 * kPrefi + jtab) +
-                        tu * MAM4B_LDG(tc + ip1 * kPrefi + jp1) +
-                        tcu * MAM4B_LDG(tc + itab * kPrefi + jp1);
+    const double coef = tcuc * tld<L>(tc + itab * kPrefi + jtab) +
+                        tuc * tld<L>(tc + ip1 * kPrefi + jtab) +
+                        tu * tld<L>(tc + ip1 * kPrefi + jp1) +
+                        tcu * tld<L>(tc + itab * kPrefi + jp1);
     pabs = (c == 0) ? 0.5 * coef : pabs + cheb[c] * coef;
   }
   pabs *= wetvol * 1.0e3;
@@ -145,6 +175,34 @@ constexpr int kSwAsm = kSwAbs + 4 * kSwBands * kSwTab;
 constexpr int kSwTableDoubles = kSwAsm + 4 * kSwBands * kSwTab;
 constexpr int kSwDiagBand = 9;  // visible band of the optical-depth diagnostic
 
+// the shortwave tables of one band: in the device table, or staged in
+// shared memory
+struct SwTables {
+  static constexpr bool kShared = false;
+  MAM4B_HD static int spec_re(int m, int s, int b) { return kSwSpecRe + (m * 7 + s) * kSwBands + b; }
+  MAM4B_HD static int spec_im(int m, int s, int b) { return kSwSpecIm + (m * 7 + s) * kSwBands + b; }
+  MAM4B_HD static int water_re(int b) { return kSwWaterRe + b; }
+  MAM4B_HD static int water_im(int b) { return kSwWaterIm + b; }
+  MAM4B_HD static int refr(int m, int b) { return kSwRefr + (m * kSwBands + b) * kPrefr; }
+  MAM4B_HD static int refi(int m, int b) { return kSwRefi + (m * kSwBands + b) * kPrefi; }
+  MAM4B_HD static int ext(int m, int b) { return kSwExt + (m * kSwBands + b) * kSwTab; }
+  MAM4B_HD static int abs_(int m, int b) { return kSwAbs + (m * kSwBands + b) * kSwTab; }
+  MAM4B_HD static int asm_(int m, int b) { return kSwAsm + (m * kSwBands + b) * kSwTab; }
+};
+struct SwBand {
+  static constexpr bool kShared = true;
+  MAM4B_HD static int spec_re(int m, int s, int) { return m * 7 + s; }
+  MAM4B_HD static int spec_im(int m, int s, int) { return 28 + m * 7 + s; }
+  MAM4B_HD static int water_re(int) { return 56; }
+  MAM4B_HD static int water_im(int) { return 57; }
+  MAM4B_HD static int refr(int m, int) { return 58 + m * kPrefr; }
+  MAM4B_HD static int refi(int m, int) { return 86 + m * kPrefi; }
+  MAM4B_HD static int ext(int m, int) { return 126 + m * kSwTab; }
+  MAM4B_HD static int abs_(int m, int) { return 126 + (4 + m) * kSwTab; }
+  MAM4B_HD static int asm_(int m, int) { return 126 + (8 + m) * kSwTab; }
+};
+constexpr int kSwBandDoubles = 126 + 12 * kSwTab;  // 4,326
+
 // surface-mode radius, its log (method 1: log of the radius) and the
 // Chebyshev polynomials (modal_size_parameters)
 MAM4B_HD void mode_cheb_sw(int m, double dgn_w, double &radsurf, double &logradsurf,
@@ -164,32 +222,33 @@ MAM4B_HD void mode_cheb_sw(int m, double dgn_w, double &radsurf, double &lograds
 }
 
 // bilinear weights of the three coefficient tables of (m, b)
+template <class L = SwTables>
 MAM4B_HD void sw_coefs(const double *tables, int m, int b, double refr, double refi,
                        double (&cext)[kNcoef], double (&cabs)[kNcoef],
                        double (&casm)[kNcoef]) {
-  const double *rt = tables + kSwRefr + (m * kSwBands + b) * kPrefr;
-  const double *it = tables + kSwRefi + (m * kSwBands + b) * kPrefi;
+  const double *rt = tables + L::refr(m, b);
+  const double *it = tables + L::refi(m, b);
   int itab, jtab;
   double ttab, utab;
-  table_factors(kPrefr, refr, rt, itab, ttab);
-  table_factors(kPrefi, refi, it, jtab, utab);
+  table_factors<L>(kPrefr, refr, rt, itab, ttab);
+  table_factors<L>(kPrefi, refi, it, jtab, utab);
   const double tu = ttab * utab;
   const double tuc = ttab - tu;
   const double tcuc = 1.0 - tuc - utab;
   const double tcu = utab - tu;
   const int jp1 = (jtab + 1 < kPrefi - 1) ? jtab + 1 : kPrefi - 1;
   const int ip1 = (itab + 1 < kPrefr - 1) ? itab + 1 : kPrefr - 1;
-  const size_t off = (size_t)(m * kSwBands + b) * kSwTab;
 #pragma unroll
   for (int c = 0; c < kNcoef; ++c) {
-    const size_t o = off + (size_t)c * kPrefr * kPrefi;
-    const double *e = tables + kSwExt + o, *a = tables + kSwAbs + o, *s = tables + kSwAsm + o;
-    cext[c] = tcuc * MAM4B_LDG(e + itab * kPrefi + jtab) + tuc * MAM4B_LDG(e + ip1 * kPrefi + jtab) +
-              tu * MAM4B_LDG(e + ip1 * kPrefi + jp1) + tcu * MAM4B_LDG(e + itab * kPrefi + jp1);
-    cabs[c] = tcuc * MAM4B_LDG(a + itab * kPrefi + jtab) + tuc * MAM4B_LDG(a + ip1 * kPrefi + jtab) +
-              tu * MAM4B_LDG(a + ip1 * kPrefi + jp1) + tcu * MAM4B_LDG(a + itab * kPrefi + jp1);
-    casm[c] = tcuc * MAM4B_LDG(s + itab * kPrefi + jtab) + tuc * MAM4B_LDG(s + ip1 * kPrefi + jtab) +
-              tu * MAM4B_LDG(s + ip1 * kPrefi + jp1) + tcu * MAM4B_LDG(s + itab * kPrefi + jp1);
+    const int o = c * kPrefr * kPrefi;
+    const double *e = tables + L::ext(m, b) + o, *a = tables + L::abs_(m, b) + o,
+                 *s = tables + L::asm_(m, b) + o;
+    cext[c] = tcuc * tld<L>(e + itab * kPrefi + jtab) + tuc * tld<L>(e + ip1 * kPrefi + jtab) +
+              tu * tld<L>(e + ip1 * kPrefi + jp1) + tcu * tld<L>(e + itab * kPrefi + jp1);
+    cabs[c] = tcuc * tld<L>(a + itab * kPrefi + jtab) + tuc * tld<L>(a + ip1 * kPrefi + jtab) +
+              tu * tld<L>(a + ip1 * kPrefi + jp1) + tcu * tld<L>(a + itab * kPrefi + jp1);
+    casm[c] = tcuc * tld<L>(s + itab * kPrefi + jtab) + tuc * tld<L>(s + ip1 * kPrefi + jtab) +
+              tu * tld<L>(s + ip1 * kPrefi + jp1) + tcu * tld<L>(s + itab * kPrefi + jp1);
   }
 }
 
@@ -203,6 +262,7 @@ MAM4B_HD double cheb_eval(const double (&coef)[kNcoef], const double (&cheb)[kNc
 
 // optical depth, single-scattering and asymmetry products of mode m in
 // band b for one cell: out = {tauxar, wa, ga, fa}
+template <class L = SwTables>
 MAM4B_HD void mode_band_sw(const double *tables, int m, int b, const double (&specvol)[7],
                            double qaerwat, const double (&cheb)[kNcoef], double radsurf,
                            double logradsurf, double mass, double (&out)[4]) {
@@ -218,8 +278,8 @@ MAM4B_HD void mode_band_sw(const double *tables, int m, int b, const double (&sp
   double dv = 0.0, cre = 0.0, cim = 0.0;
   for (int s = 0; s < nspec; ++s) {
     dv += specvol[s];
-    cre += specvol[s] * MAM4B_LDG(tables + kSwSpecRe + (m * 7 + s) * kSwBands + b);
-    cim += specvol[s] * MAM4B_LDG(tables + kSwSpecIm + (m * 7 + s) * kSwBands + b);
+    cre += specvol[s] * tld<L>(tables + L::spec_re(m, s, b));
+    cim += specvol[s] * tld<L>(tables + L::spec_im(m, s, b));
   }
   double watervol = qaerwat / 1.0e3;
   double wetvol = watervol + dv;
@@ -227,13 +287,13 @@ MAM4B_HD void mode_band_sw(const double *tables, int m, int b, const double (&sp
     watervol = 0.0;
     wetvol = dv;
   }
-  cre += watervol * MAM4B_LDG(tables + kSwWaterRe + b);
-  cim += watervol * MAM4B_LDG(tables + kSwWaterIm + b);
+  cre += watervol * tld<L>(tables + L::water_re(b));
+  cim += watervol * tld<L>(tables + L::water_im(b));
   const double den = dmax(wetvol, 1.e-40);
   cre /= den;
   cim /= den;
   double cext[kNcoef], cabs[kNcoef], casm[kNcoef];
-  sw_coefs(tables, m, b, cre, fabs(cim), cext, cabs, casm);
+  sw_coefs<L>(tables, m, b, cre, fabs(cim), cext, cabs, casm);
   double pext = cheb_eval(cext, cheb);
   double pabs = cheb_eval(cabs, cheb);
   const double pasm = cheb_eval(casm, cheb);
@@ -252,6 +312,40 @@ MAM4B_HD void mode_band_sw(const double *tables, int m, int b, const double (&sp
   out[2] = dopaer * palb * pasm;
   out[3] = dopaer * palb * pasm * pasm;
 }
+
+#ifdef __CUDACC__
+// Band b's values of the refractive-index mixing and the tables of the
+// four modes, copied from the device table (layout G) into the block's
+// shared slice s (layout S) by all threads of the block; the caller
+// synchronises the block before reading s.
+template <class G, class S>
+__device__ void stage_band_common(const double *g, int b, double *s) {
+  const int t = threadIdx.x, nt = blockDim.x;
+  for (int i = t; i < 28; i += nt) {
+    const int m = i / 7, k = i % 7;
+    s[S::spec_re(m, k, b)] = __ldg(g + G::spec_re(m, k, b));
+    s[S::spec_im(m, k, b)] = __ldg(g + G::spec_im(m, k, b));
+  }
+  if (t == 0) {
+    s[S::water_re(b)] = __ldg(g + G::water_re(b));
+    s[S::water_im(b)] = __ldg(g + G::water_im(b));
+  }
+  for (int i = t; i < 4 * kPrefr; i += nt)
+    s[S::refr(i / kPrefr, b) + i % kPrefr] = __ldg(g + G::refr(i / kPrefr, b) + i % kPrefr);
+  for (int i = t; i < 4 * kPrefi; i += nt)
+    s[S::refi(i / kPrefi, b) + i % kPrefi] = __ldg(g + G::refi(i / kPrefi, b) + i % kPrefi);
+}
+
+__device__ void stage_sw_band(const double *g, int b, double *s) {
+  stage_band_common<SwTables, SwBand>(g, b, s);
+  for (int i = threadIdx.x; i < 4 * kSwTab; i += blockDim.x) {
+    const int m = i / kSwTab, k = i % kSwTab;
+    s[SwBand::ext(m, b) + k] = __ldg(g + SwTables::ext(m, b) + k);
+    s[SwBand::abs_(m, b) + k] = __ldg(g + SwTables::abs_(m, b) + k);
+    s[SwBand::asm_(m, b) + k] = __ldg(g + SwTables::asm_(m, b) + k);
+  }
+}
+#endif
 
 }  // namespace opt
 }  // namespace mam4b
