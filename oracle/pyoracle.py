@@ -449,7 +449,7 @@ def reference_available():
 # ----------------------------------------------------------------------
 # Parity against the oracle
 # ----------------------------------------------------------------------
-TOL = 1e-12        # north-star tolerance, state-relative
+TOL = 1e-12        # the FP64 parity tolerance, state-relative
 QUANTILES = (0.5, 0.9, 0.99, 0.999)
 
 

@@ -11,7 +11,7 @@ Two layers:
 
 2. Math library. Against the canonical host oracle (glibc) the kernel must
    be as close as the oracle is to itself when every libm result is moved by
-   1..2 ulps (oracle.pyoracle.parity): the north-star tolerance of 1e-12
+   1..2 ulps (oracle.pyoracle.parity): the target tolerance of 1e-12
    (state-relative per tendency, absolute floor 1e-30; relative for the
    diameters, densities and water) holds on the same fraction of cells as in
    that baseline and the error quantiles stay within 3x of it. No tighter

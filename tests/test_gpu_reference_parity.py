@@ -12,7 +12,7 @@
    differences (SOA sub-stepping, the water-uptake quartic), so the bar is
    the one of oracle.pyoracle.parity: at least as close to the host build
    as the host build is to itself under 1..2-ulp libm perturbations. The
-   north-star metric, error relative per tendency (absolute floor 1e-30
+   target metric, error relative per tendency (absolute floor 1e-30
    kg/kg), is reported beside the state-relative one.
 
 3. Conservation on the GPU, per cell and per column (weights pdel/g), in
@@ -88,7 +88,7 @@ def test_edge_cases_bitwise_against_reference_headers(cuda_device, ref_gpu):
 
 
 def tendency_rel_err(got, ref, dt, floor=1e-30):
-    """The north-star error: |d tend| relative to |tend_ref|, where an error
+    """The per-tendency error: |d tend| relative to |tend_ref|, where an error
     below the absolute floor (1e-30 kg/kg over the step) counts as zero;
     the 16 size/density/water outputs relative to their value."""
     e_t = np.abs(got[:52] - ref[:52]) / np.maximum(np.abs(ref[:52]), floor / dt)
