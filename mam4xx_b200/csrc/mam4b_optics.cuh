@@ -30,8 +30,8 @@ constexpr int kAbsp = kRefi + 4 * kLwBands * kPrefi;          // [4][16][5][7][1
 constexpr int kTableDoubles = kAbsp + 4 * kLwBands * kNcoef * kPrefr * kPrefi;
 
 // Where the tables of one band sit. LwTables / SwTables: the whole device
-// table (the layouts here, read through the read-only data cache). SwBand:
-// one band's values staged in shared memory by the shortwave band kernel
+// table (the layouts here, read through the read-only data cache). LwBand /
+// SwBand: one band's values staged in shared memory by the band kernels
 // (species and water indices, the two refractive-index grids and the
 // coefficient tables of the four modes, band index dropped). The functions
 // below read the same values in the same order through either, so their
@@ -48,6 +48,18 @@ struct LwTables {
     return kAbsp + (m * kLwBands + b) * kNcoef * kPrefr * kPrefi;
   }
 };
+
+struct LwBand {
+  static constexpr bool kShared = true;
+  MAM4B_HD static int spec_re(int m, int s, int) { return m * 7 + s; }
+  MAM4B_HD static int spec_im(int m, int s, int) { return 28 + m * 7 + s; }
+  MAM4B_HD static int water_re(int) { return 56; }
+  MAM4B_HD static int water_im(int) { return 57; }
+  MAM4B_HD static int refr(int m, int) { return 58 + m * kPrefr; }
+  MAM4B_HD static int refi(int m, int) { return 86 + m * kPrefi; }
+  MAM4B_HD static int absp(int m, int) { return 126 + m * kNcoef * kPrefr * kPrefi; }
+};
+constexpr int kLwBandDoubles = 126 + 4 * kNcoef * kPrefr * kPrefi;
 
 template <class L>
 MAM4B_HD double tld(const double *p) {
@@ -334,6 +346,13 @@ __device__ void stage_band_common(const double *g, int b, double *s) {
     s[S::refr(i / kPrefr, b) + i % kPrefr] = __ldg(g + G::refr(i / kPrefr, b) + i % kPrefr);
   for (int i = t; i < 4 * kPrefi; i += nt)
     s[S::refi(i / kPrefi, b) + i % kPrefi] = __ldg(g + G::refi(i / kPrefi, b) + i % kPrefi);
+}
+
+__device__ void stage_lw_band(const double *g, int b, double *s) {
+  stage_band_common<LwTables, LwBand>(g, b, s);
+  constexpr int kT = kNcoef * kPrefr * kPrefi;
+  for (int i = threadIdx.x; i < 4 * kT; i += blockDim.x)
+    s[LwBand::absp(i / kT, b) + i % kT] = __ldg(g + LwTables::absp(i / kT, b) + i % kT);
 }
 
 __device__ void stage_sw_band(const double *g, int b, double *s) {
