@@ -36,6 +36,7 @@ struct CoagProcessArgs {
   ProgFields progs, tends;
   long long ncell;
   double dt;
+  double *cc;  // [12][ncell]: the coefficients, from the pair stage to the update
 };
 
 // CalcSize::compute_tendencies for one cell (level k of a column):
@@ -233,17 +234,27 @@ MAM4B_HD void calcsize_process_cell(const StepConsts &C, const CalcSizeArgs &a, 
 // (mam4_constants.hpp:45), as that routine computes it; the wet density is
 // used as given (no lower bound); tendencies += (after - before) / dt and
 // the prognostics are updated in place.
-MAM4B_HD void coag_process_cell(const StepConsts &C, const CoagTables &Tb,
-                                const CoagProcessArgs &a, long long c) {
-  constexpr double kRGasMole = 6.022214076e23 * 1.380649e-23;
-  const double temp = a.temp[c], pmid = a.pmid[c];
-  const double aircon = pmid / (kRGasMole * temp);
-  double dgn_awet[NMODE], wetdens[NMODE];
-#pragma unroll
-  for (int m = 0; m < NMODE; ++m) {
-    dgn_awet[m] = a.dgn_awet[m][c];
-    wetdens[m] = a.wet_density[m][c];
-  }
+constexpr double kRGasMole = 6.022214076e23 * 1.380649e-23;
+
+MAM4B_HD double coag_process_aircon(const CoagProcessArgs &a, long long c) {
+  return a.pmid[c] / (kRGasMole * a.temp[c]);
+}
+
+// The coefficients of mode pair p (coag_pair_coefs: bij0, bij3, bii0,
+// bjj0, the pair's entries of coag_all_coefs) for one cell.
+MAM4B_HD void coag_process_pair(const StepConsts &C, const CoagTables &Tb,
+                                const CoagProcessArgs &a, long long c, int p, double &bij0,
+                                double &bij3, double &bii0, double &bjj0) {
+  const int sm = coag_src(p), dm = coag_dst(p);
+  coag_pair_coefs(C, Tb, p, a.temp[c], a.pmid[c], coag_process_aircon(a, c), a.dgn_awet[sm][c],
+                  a.dgn_awet[dm][c], a.wet_density[sm][c], a.wet_density[dm][c], bij0, bij3,
+                  bii0, bjj0);
+}
+
+// The coagulation update of one cell with its 12 coefficients cc
+// (coag_all_coefs order) and the tendencies.
+MAM4B_HD void coag_process_update(const CoagProcessArgs &a, long long c,
+                                  const double (&cc)[12]) {
   Sub s, s0;
   s.gas[0] = s.gas[1] = 0.0;
 #pragma unroll
@@ -254,8 +265,7 @@ MAM4B_HD void coag_process_cell(const StepConsts &C, const CoagTables &Tb,
       s.aer[x][m] = a.progs.q_i[m][x][c];
   }
   s0 = s;
-  double cc[12], coag_in[NAER];
-  coag_all_coefs(C, Tb, temp, pmid, aircon, dgn_awet, wetdens, cc);
+  double coag_in[NAER];
   coagulation(a.dt, cc, s, coag_in);
 #pragma unroll
   for (int m = 0; m < NMODE; ++m) {
@@ -267,6 +277,16 @@ MAM4B_HD void coag_process_cell(const StepConsts &C, const CoagTables &Tb,
     a.tends.n_i[m][c] += (s.num[m] - s0.num[m]) / a.dt;
     a.progs.n_i[m][c] = s.num[m];
   }
+}
+
+// Both parts for one cell in one thread.
+MAM4B_HD void coag_process_cell(const StepConsts &C, const CoagTables &Tb,
+                                const CoagProcessArgs &a, long long c) {
+  double cc[12];
+#pragma unroll
+  for (int p = 0; p < 3; ++p)
+    coag_process_pair(C, Tb, a, c, p, cc[p], cc[3 + p], cc[6 + p], cc[9 + p]);
+  coag_process_update(a, c, cc);
 }
 
 }  // namespace mam4b

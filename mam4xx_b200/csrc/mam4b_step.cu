@@ -2316,11 +2316,34 @@ __global__ void __launch_bounds__(128) calcsize_process_kernel(const __grid_cons
     calcsize_process_cell(c_k, a, c);
 }
 
+// In two stages, as the step's pair_kernel and post_kernel: one thread per
+// (cell, mode pair) for the coefficients (the FP64 exp/pow/sqrt chains,
+// with many warps resident), then one thread per cell for the update.
+__global__ void __launch_bounds__(128) coag_pair_process_kernel(const __grid_constant__ CoagProcessArgs a) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncell)
+    return;
+  const CoagTables T = {kCoagBm0ij, kCoagBm3i, kCoagBm0};
+  const int p = blockIdx.y;
+  const size_t n = (size_t)a.ncell;
+  double bij0, bij3, bii0, bjj0;
+  coag_process_pair(c_k, T, a, c, p, bij0, bij3, bii0, bjj0);
+  a.cc[p * n + c] = bij0;
+  a.cc[(3 + p) * n + c] = bij3;
+  a.cc[(6 + p) * n + c] = bii0;
+  a.cc[(9 + p) * n + c] = bjj0;
+}
+
 __global__ void __launch_bounds__(128) coag_process_kernel(const __grid_constant__ CoagProcessArgs a) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const CoagTables T = {kCoagBm0ij, kCoagBm3i, kCoagBm0};
-  if (c < a.ncell)
-    coag_process_cell(c_k, T, a, c);
+  if (c >= a.ncell)
+    return;
+  const size_t n = (size_t)a.ncell;
+  double cc[12];
+#pragma unroll
+  for (int k = 0; k < 12; ++k)
+    cc[k] = a.cc[k * n + c];
+  coag_process_update(a, c, cc);
 }
 
 // ---- aqueous sulfate chemistry (setsox), one thread per cell
@@ -3221,6 +3244,8 @@ struct mam4b_ctx {
   int *d_trop;          // [cap_trop]: tropopause level per column (aero_rad_props)
   size_t cap_trop;
   double *d_dmx;        // dropmixnuc activation results (DA_FIELDS per cell), grown
+  double *d_coag_cc;    // coagulation process: 12 coefficients per cell, grown
+  size_t cap_coag_cc;
   size_t cap_dmx;
   unsigned *d_bins;     // [2 kPassBins]: loops per pass count, start offsets
   // mam4b_step_columns: device pointer tables of the columns (grown) and
@@ -3904,6 +3929,7 @@ mam4b_status mam4b_destroy(mam4b_ctx *ctx) {
   cudaFree(ctx->d_optics_sw);
   cudaFree(ctx->d_trop);
   cudaFree(ctx->d_dmx);
+  cudaFree(ctx->d_coag_cc);
   if (ctx->host_streams) {
     for (int k = 0; k < kHostStreams; ++k) {
       cudaStreamDestroy(ctx->hs[k]);
@@ -5271,12 +5297,18 @@ mam4b_status mam4b_coagulation_process(mam4b_ctx *ctx, const double *temperature
   ctx->last_stream = s;
   if (a.ncell == 0)
     return MAM4B_OK;
-  const int block = 128;
-  coag_process_kernel<<<(unsigned)((a.ncell + block - 1) / block), block, 0, s>>>(a);
-  const cudaError_t e = cudaGetLastError();
+  cudaError_t e = grow(&ctx->d_coag_cc, &ctx->cap_coag_cc, (size_t)12 * a.ncell);
   if (e != cudaSuccess)
     return set_err(ctx, MAM4B_ERR_CUDA, what, e);
-  ctx->launches += 1;
+  a.cc = ctx->d_coag_cc;
+  const int block = 128;
+  const unsigned grid = (unsigned)((a.ncell + block - 1) / block);
+  coag_pair_process_kernel<<<dim3(grid, 3), block, 0, s>>>(a);
+  coag_process_kernel<<<grid, block, 0, s>>>(a);
+  e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return set_err(ctx, MAM4B_ERR_CUDA, what, e);
+  ctx->launches += 2;
   return MAM4B_OK;
 }
 
