@@ -607,21 +607,26 @@ MAM4B_HD void water_uptake_mode(const StepConsts &C, const double (&sp)[7],
   const double dryvol = 1.0 / v2ncur_a;
   const double drymass = drydens * dryvol;
   const double dryrad = cbrt(dryvol / (K::pi * 4.0 / 3.0));
-  double wetrad = kohler(C, dryrad, hygro, rh);
-  wetrad = dmax(wetrad, dryrad);
-  double wetvol = (K::pi * 4.0 / 3.0) * cube(wetrad);
-  wetvol = dmax(wetvol, dryvol);
-  double wtrvol = wetvol - dryvol;
-  wtrvol = dmax(wtrvol, 0.0);
+  double wetrad, wetvol, wtrvol;
   if (rh < K::rh_cryst) {
+    // the reference computes the Kohler radius and then discards it below
+    // the crystallisation humidity: the values are those it keeps
     wetrad = dryrad;
     wetvol = dryvol;
     wtrvol = 0.0;
-  } else if (rh < K::rh_deliq) {
-    wtrvol = wtrvol * C.hystfac * (rh - K::rh_cryst);
+  } else {
+    wetrad = kohler(C, dryrad, hygro, rh);
+    wetrad = dmax(wetrad, dryrad);
+    wetvol = (K::pi * 4.0 / 3.0) * cube(wetrad);
+    wetvol = dmax(wetvol, dryvol);
+    wtrvol = wetvol - dryvol;
     wtrvol = dmax(wtrvol, 0.0);
-    wetvol = dryvol + wtrvol;
-    wetrad = cbrt(wetvol / (4.0 / 3.0 * K::pi));
+    if (rh < K::rh_deliq) {
+      wtrvol = wtrvol * C.hystfac * (rh - K::rh_cryst);
+      wtrvol = dmax(wtrvol, 0.0);
+      wetvol = dryvol + wtrvol;
+      wetrad = cbrt(wetvol / (4.0 / 3.0 * K::pi));
+    }
   }
   dgn_awet = dgn_a * (wetrad / dryrad);
   qaerwat = 1.0e3 * naer * wtrvol;

@@ -1485,9 +1485,45 @@ __device__ __forceinline__ void mode_work(const StepArgs &a, const long long c) 
       uptake_rate_mode(C, M, a.aux[AUX_GDIFF * n + c], a.aux[AUX_FPATH * n + c], dgn_awet);
 }
 
+// FP64: the block's cells are regrouped so that the cells below the
+// crystallisation humidity, whose water uptake needs no Kohler solve, fill
+// warps of their own (cell order kept within each group; blocks of at most
+// 256 threads, the launch shapes allowed).
 template <bool MIXED>
 __global__ void mode_kernel(const __grid_constant__ StepArgs a) {
-  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if constexpr (!MIXED) {
+    __shared__ int s_perm[256];
+    __shared__ unsigned s_cnt[8][2];
+    const long long c0 = (long long)blockIdx.x * blockDim.x;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5, nw = blockDim.x >> 5;
+    const bool valid = c < a.ncell;
+    const bool dry = valid && a.aux[AUX_RH * (size_t)a.ncell + c] < K::rh_cryst;
+    const unsigned bd = __ballot_sync(0xffffffffu, dry);
+    const unsigned bo = __ballot_sync(0xffffffffu, valid && !dry);
+    if (lane == 0) {
+      s_cnt[w][0] = __popc(bd);
+      s_cnt[w][1] = __popc(bo);
+    }
+    __syncthreads();
+    unsigned before_d = 0, before_o = 0, total_d = 0, total = 0;
+    for (int k = 0; k < nw; ++k) {
+      if (k < w) {
+        before_d += s_cnt[k][0];
+        before_o += s_cnt[k][1];
+      }
+      total_d += s_cnt[k][0];
+      total += s_cnt[k][0] + s_cnt[k][1];
+    }
+    if (valid) {
+      const unsigned below = (1u << lane) - 1u;
+      s_perm[dry ? before_d + __popc(bd & below) : total_d + before_o + __popc(bo & below)] = t;
+    }
+    __syncthreads();
+    if ((unsigned)t >= total)
+      return;
+    c = c0 + s_perm[t];
+  }
   if (c >= a.ncell)
     return;
   switch (blockIdx.y) {
