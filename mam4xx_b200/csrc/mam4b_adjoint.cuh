@@ -652,11 +652,17 @@ MAM4B_HD void water_uptake_mode_rev(const StepConsts &C, const double (&sp)[7], 
   const double dryvol = 1.0 / v2ncur_a;
   const double drymass = drydens * dryvol;
   const double dryrad = cbrt(dryvol / (K::pi * 4.0 / 3.0));
-  const double wr0 = kohler(C, dryrad, hygro, rh);
-  const double wr1 = dmax(wr0, dryrad);
-  const double wv0 = (K::pi * 4.0 / 3.0) * cube(wr1);
-  const double wv1 = dmax(wv0, dryvol);
-  const double wt0 = dmax(wv1 - dryvol, 0.0);
+  // below the crystallisation humidity the Kohler radius is discarded (the
+  // forward skips it): nothing of it enters the outputs or their cotangents
+  const bool dry = rh < K::rh_cryst;
+  double wr0 = dryrad, wr1 = dryrad, wv0 = dryvol, wv1 = dryvol, wt0 = 0.0;
+  if (!dry) {
+    wr0 = kohler(C, dryrad, hygro, rh);
+    wr1 = dmax(wr0, dryrad);
+    wv0 = (K::pi * 4.0 / 3.0) * cube(wr1);
+    wv1 = dmax(wv0, dryvol);
+    wt0 = dmax(wv1 - dryvol, 0.0);
+  }
   int hbranch = 0;
   double wetrad = wr1, wetvol = wv1, wtrvol = wt0, wt1 = 0.0;
   if (rh < K::rh_cryst) {
@@ -704,20 +710,22 @@ MAM4B_HD void water_uptake_mode_rev(const StepConsts &C, const double (&sp)[7], 
     wv1b += wetvolb;
     wr1b += wetradb;
   }
-  // wt0 = dmax(wv1 - dryvol, 0)
-  {
-    const double t = maxc_rev(0.0, wv1 - dryvol, wt0b);
-    wv1b += t;
-    dryvolb -= t;
+  if (!dry) {
+    // wt0 = dmax(wv1 - dryvol, 0)
+    {
+      const double t = maxc_rev(0.0, wv1 - dryvol, wt0b);
+      wv1b += t;
+      dryvolb -= t;
+    }
+    // wv1 = dmax(wv0, dryvol)
+    double wv0b = 0.0;
+    max_rev(wv0, dryvol, wv1b, wv0b, dryvolb);
+    wr1b += wv0b * (K::pi * 4.0 / 3.0) * 3.0 * wr1 * wr1;
+    // wr1 = dmax(wr0, dryrad)
+    double wr0b = 0.0;
+    max_rev(wr0, dryrad, wr1b, wr0b, dryradb);
+    kohler_rev(C, dryrad, hygro, rh, wr0b, dryradb, hygrob, rhb);
   }
-  // wv1 = dmax(wv0, dryvol)
-  double wv0b = 0.0;
-  max_rev(wv0, dryvol, wv1b, wv0b, dryvolb);
-  wr1b += wv0b * (K::pi * 4.0 / 3.0) * 3.0 * wr1 * wr1;
-  // wr1 = dmax(wr0, dryrad)
-  double wr0b = 0.0;
-  max_rev(wr0, dryrad, wr1b, wr0b, dryradb);
-  kohler_rev(C, dryrad, hygro, rh, wr0b, dryradb, hygrob, rhb);
   // dryrad = cbrt(dryvol / (4/3 pi))
   dryvolb += dryradb * dryrad / (3.0 * dryvol);
   // drymass = drydens * dryvol

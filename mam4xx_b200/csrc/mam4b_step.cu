@@ -2205,10 +2205,42 @@ __device__ __forceinline__ void adj_mode_work(const AdjPipeArgs &p, long long c)
     p.xbar[(size_t)(MAM4B_IN_AER_I + K::spec0(M) + s) * p.ld + c] += spb[s];
 }
 
+// Cells regrouped within the block as in mode_kernel: those below the
+// crystallisation humidity (no Kohler reverse) fill warps of their own.
+// Launched with 128 threads per block.
 __global__ void __launch_bounds__(128) adj_mode_kernel(const __grid_constant__ AdjPipeArgs p) {
-  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= p.s.ncell)
+  __shared__ int s_perm[128];
+  __shared__ unsigned s_cnt[4][2];
+  const StepArgs &a = p.s;
+  const long long c0 = (long long)blockIdx.x * blockDim.x;
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5, nw = blockDim.x >> 5;
+  long long c = c0 + t;
+  const bool valid = c < a.ncell;
+  const bool dry = valid && a.aux[AUX_RH * (size_t)a.ncell + c] < K::rh_cryst;
+  const unsigned bd = __ballot_sync(0xffffffffu, dry);
+  const unsigned bo = __ballot_sync(0xffffffffu, valid && !dry);
+  if (lane == 0) {
+    s_cnt[w][0] = __popc(bd);
+    s_cnt[w][1] = __popc(bo);
+  }
+  __syncthreads();
+  unsigned before_d = 0, before_o = 0, total_d = 0, total = 0;
+  for (int k = 0; k < nw; ++k) {
+    if (k < w) {
+      before_d += s_cnt[k][0];
+      before_o += s_cnt[k][1];
+    }
+    total_d += s_cnt[k][0];
+    total += s_cnt[k][0] + s_cnt[k][1];
+  }
+  if (valid) {
+    const unsigned below = (1u << lane) - 1u;
+    s_perm[dry ? before_d + __popc(bd & below) : total_d + before_o + __popc(bo & below)] = t;
+  }
+  __syncthreads();
+  if ((unsigned)t >= total)
     return;
+  c = c0 + s_perm[t];
   switch (blockIdx.y) {
   case 0: adj_mode_work<0>(p, c); break;
   case 1: adj_mode_work<1>(p, c); break;
